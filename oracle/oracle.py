@@ -1,0 +1,114 @@
+"""ctypes binding of the C oracle -- TEST INFRASTRUCTURE ONLY.
+
+Loads ``oracle/_build/libwaam_oracle.so`` (built by ``make -C oracle``) and
+exposes each restated reference kernel on numpy arrays.  Only the parity
+tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
+use this module; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libwaam_oracle.so")
+
+_F = C.POINTER(C.c_float)
+_I = C.POINTER(C.c_int32)
+_f = C.c_float
+_i = C.c_int
+_l = C.c_int64
+
+_SIGS = {
+    "wo_init_grid": ([_F] * 9 + [_I, _i, _i, _i, _f, _f, _f, _i, _i, _i, _i, _i], None),
+    "wo_clear_forces": ([_F, _F, _F, _l], None),
+    "wo_inject_arc_heat": ([_F, _I, _F, _i, _i, _i] + [_f] * 9 + [_i], C.c_double),
+    "wo_inject_goldak_heat": ([_F, _I, _F, _i, _i, _i] + [_f] * 15 + [_i], C.c_double),
+    "wo_clamp_enthalpy_ceiling_scalar": ([_F, _I, _l, _f, _f, _f, _f, _f], None),
+    "wo_advect_diffuse_temperature": ([_F, _F, _F, _F, _F, _I, _i, _i, _i, _f, _f, _f], None),
+    "wo_update_phase": ([_F, _F, _F, _l, _f, _f, _f, _f], None),
+    "wo_update_T_max": ([_F, _F, _I, _l], None),
+    "wo_update_cooling_rate": ([_F, _F, _F, _I, _l, _f], None),
+    "wo_apply_thermal_boundary_losses": ([_F, _F, _I, _i, _i, _i, _f, _f, _f, _i, _i, _f, _f, _f], None),
+    "wo_clamp_enthalpy_floor_scalar": ([_F, _f, _I, _l, _f], None),
+    "wo_advect_phi": ([_F, _F, _F, _F, _F, _I, _i, _i, _i], None),
+    "wo_reinitialize_phi": ([_F, _I, _l], None),
+    "wo_apply_contact_angle_phi_bc": ([_F, _I, _i, _i, _i, _f], None),
+    "wo_update_flags_from_phi": ([_F, _F, _I, _i, _i, _i, _i], None),
+    "wo_sync_phi_liquid_fraction": ([_F, _F, _I, _l], None),
+    "wo_compute_csf_tension": ([_F, _I, _F, _F, _F, _i, _i, _i, _f, _i, _f], None),
+    "wo_compute_marangoni_force": ([_F, _F, _F, _F, _F, _F, _I, _i, _i, _i, _f], None),
+    "wo_apply_arc_pressure": ([_F, _I, _F, _i, _i, _i] + [_f] * 8, None),
+    "wo_add_hydrostatic_gravity": ([_F, _F, _I, _l, _f, _f], None),
+    "wo_add_buoyancy": ([_F, _F, _F, _I, _l, _f, _f, _f, _f], None),
+    "wo_clamp_body_force_magnitude": ([_F, _F, _F, _I, _l, _f], None),
+    "wo_collide_mrt": ([_F] * 10 + [_I, _l, _f, _f, _f], None),
+    "wo_collide_srt": ([_F] * 10 + [_I, _l, _f, _f], None),
+    "wo_clamp_velocity_mach": ([_F, _F, _F, _I, _l, _f], None),
+    "wo_stream": ([_F, _F, _I, _i, _i, _i], None),
+    "wo_update_time_above_T": ([_F, _I, _F, _F, _F, _l, _f, _f, _f, _f], None),
+    "wo_snapshot_forces": ([_F] * 6 + [_l], None),
+    "wo_remelt_hot_solid_scalar": ([_F, _F, _F, _F, _I, _l, _f, _f, _f, _f], None),
+    "wo_solidify_trailing_pool_scalar": ([_F, _F, _F, _F, _I, _F, _F, _F, _i, _i, _i] + [_f] * 10, None),
+    "wo_solidify_cooled_metal": ([_F, _F, _F, _I, _F, _F, _F, _l, _f, _i], None),
+    "wo_surface_height_at": ([_F, _I, _i, _i, _i, _i, _i, _i], C.c_float),
+    "wo_feed_wire_surface": ([_F, _I, _F, _F, _F, _F, _F, _i, _i, _i] + [_f] * 10 + [_F, _F, _f], None),
+    "wo_feed_wire_momentum_impact": ([_F, _F, _F, _F, _F, _I, _F, _i, _i, _i] + [_f] * 7, None),
+    "wo_apply_droplet_impact_pressure": ([_F, _I, _F, _F, _i, _i, _i] + [_f] * 8, None),
+    "wo_elec_build_sigma": ([_F, _F, _I, _l, _f, _f], None),
+    "wo_elec_inject_arc_source": ([_F, _i, _i, _i] + [_f] * 6, None),
+    "wo_elec_normalize_source": ([_F, _l, _f, _f], None),
+    "wo_elec_jacobi_step": ([_F, _F, _F, _F, _I, _i, _i, _i, _f, _f, _i], None),
+    "wo_elec_l1_diff": ([_F, _F, _l, C.POINTER(C.c_double), C.POINTER(C.c_double)], None),
+    "wo_elec_compute_J": ([_F, _F, _F, _F, _F, _I, _i, _i, _i, _f], None),
+    "wo_elec_bins": ([_F, _F, _i, _i, _i, _f, _f, _f, _f, _i], None),
+    "wo_elec_B_axisymmetric": ([_F, _F, _F, _F, _i, _i, _i, _f, _f, _f, _f, _f, _i], None),
+    "wo_apply_lorentz_JxB": ([_F] * 10 + [_I, _l, _f, _f, _f], None),
+    "wo_num_threads": ([], C.c_int),
+    "wo_set_num_threads": ([C.c_int], None),
+}
+
+_lib = None
+
+
+def build():
+    """Compile the oracle with its Makefile (gcc; seconds)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    if a.dtype == np.float32:
+        assert a.flags.c_contiguous
+        return a.ctypes.data_as(_F)
+    if a.dtype == np.int32:
+        assert a.flags.c_contiguous
+        return a.ctypes.data_as(_I)
+    raise TypeError("oracle arrays must be float32 or int32, got %s" % a.dtype)
+
+
+def call(name, *args):
+    """Call oracle function ``name``; numpy arrays are passed by pointer."""
+    conv = []
+    for a in args:
+        if isinstance(a, np.ndarray):
+            conv.append(_ptr(a))
+        else:
+            conv.append(a)
+    return getattr(lib(), name)(*conv)

@@ -1,0 +1,248 @@
+"""Kernel-level golden cases, runnable on any backend.
+
+Each case in ``CASES`` loads ``tests/golden/k_<name>.npz`` (inputs produced by
+``state_gen.seeded_state``; outputs produced by the reference's own kernels),
+runs the same operation on a backend and returns the backend's outputs.  A
+backend exposes the operator set of ``include/waam_b200.h`` under the
+oracle's names (``wo_*`` without the prefix) and works on numpy arrays:
+``OracleBackend`` calls the C oracle directly, the CUDA backend in
+``tests/cuda_backend.py`` copies the arrays to the GPU and calls the C-ABI.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+# tolerance used for every float32 field comparison:
+#   |a - b| <= RTOL * |b| + RTOL * max|b over the field|
+RTOL = 1e-5
+
+
+def load_case(name):
+    z = np.load(os.path.join(GOLDEN, "k_%s.npz" % name))
+    args = json.loads(str(z["args"]))
+    fields = json.loads(str(z["fields"]))
+    ins = {f: np.ascontiguousarray(z["in_" + f]) for f in fields}
+    outs = {f: z["out_" + f] for f in fields}
+    return args, ins, outs
+
+
+def full_inputs(name):
+    """All state fields for a case (fields not in the fixture come from state_gen)."""
+    import state_gen
+
+    args, ins, outs = load_case(name)
+    seed_map = {"inject_goldak": 1, "thermal_s2": 2, "vof_wet": 3, "contact": 4,
+                "contact_s5": 5, "forces_wet": 6, "csf": 7, "csf_wet": 8, "collide_srt": 9,
+                "tail": 10, "heat_loss": 11, "surface_height": 12, "deposit": 13}
+    nx, ny, nz = ins[next(iter(ins))].shape[-3:]
+    st = state_gen.seeded_state(nx, ny, nz, seed=seed_map.get(name, 0))
+    st = {k: (np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v) for k, v in st.items()}
+    st["phi_tmp"] = np.zeros_like(st["phi"])
+    for f, v in ins.items():
+        if f in st and f != "phi_tmp" and name != "reset":
+            # the fixture was generated from this very seeded state
+            assert np.array_equal(st[f], v), "state_gen drifted from fixture %s (%s)" % (name, f)
+        st[f] = v.copy()
+    return args, st, outs
+
+
+def compare(name, got, want, field):
+    want = np.asarray(want)
+    got = np.asarray(got)
+    assert got.shape == want.shape, (name, field, got.shape, want.shape)
+    if want.dtype.kind in "iu":
+        bad = np.count_nonzero(got != want)
+        assert bad == 0, "%s: %s differs in %d cells" % (name, field, bad)
+        return 0.0
+    scale = float(np.max(np.abs(want))) if want.size else 0.0
+    err = np.abs(got.astype(np.float64) - want.astype(np.float64))
+    tol = RTOL * np.abs(want.astype(np.float64)) + RTOL * scale
+    bad = np.count_nonzero(err > tol)
+    assert bad == 0, "%s: %s has %d cells beyond tolerance (max err %.3e, scale %.3e)" % (
+        name, field, bad, float(err.max()), scale)
+    return float(err.max() / max(scale, 1e-30))
+
+
+def run_case(be, name, st, a):
+    """Run case ``name`` on backend ``be`` in place on state dict ``st``."""
+    nx, ny, nz = st["phi"].shape
+    n = nx * ny * nz
+    if name == "inject_gauss":
+        be.inject_arc_heat(st["H"], st["flags"], st["f_l"], nx, ny, nz, a["arc_i"], a["arc_j"],
+                           a["arc_k"], a["Q_w"], a["sigma"], a["dt"], a["dx3"], a["eta"],
+                           a["pen"], a["enable"])
+    elif name == "inject_goldak":
+        be.inject_goldak_heat(st["H"], st["flags"], st["f_l"], nx, ny, nz, a["arc_i"], a["arc_j"],
+                              a["arc_k"], a["Q_w"], a["dt"], a["dx3"], a["eta"], a["sign"],
+                              a["ff"], a["fr"], a["a_front"], a["a_rear"], a["b"], a["c"],
+                              a["pen"], a["enable"])
+    elif name == "ceiling":
+        be.clamp_enthalpy_ceiling_scalar(st["H"], st["flags"], n, a["cp_rho"], a["T_solidus"],
+                                         a["T_liquidus"], a["T_cap"], a["L_rho"])
+    elif name in ("thermal", "thermal_s2"):
+        be.advect_diffuse_temperature(st["H"], st["T"], st["ux"], st["uy"], st["uz"], st["flags"],
+                                      nx, ny, nz, a["alpha_lu"], 1.0, a["cp_rho"])
+    elif name == "phase":
+        be.update_phase(st["H"], st["T"], st["f_l"], n, a["cp_rho"], a["L_rho"], a["T_solidus"],
+                        a["T_liquidus"])
+    elif name == "tmax_cool":
+        be.update_T_max(st["T"], st["T_max"], st["flags"], n)
+        be.update_cooling_rate(st["T"], st["T_prev"], st["dT_dt"], st["flags"], n, a["dt"])
+    elif name in ("vof", "vof_wet"):
+        be.advect_phi(st["phi_tmp"], st["phi"], st["ux"], st["uy"], st["uz"], st["flags"],
+                      nx, ny, nz)
+        st["phi"][...] = st["phi_tmp"]
+        be.reinitialize_phi(st["phi"], st["flags"], n)
+        if a["wetting"]:
+            be.apply_contact_angle_phi_bc(st["phi"], st["flags"], nx, ny, nz, a["theta"])
+        be.update_flags_from_phi(st["phi"], st["f_l"], st["flags"], nx, ny, nz, a["nz_solid"])
+        be.sync_phi_liquid_fraction(st["phi"], st["f_l"], st["flags"], n)
+    elif name in ("contact", "contact_s5"):
+        be.apply_contact_angle_phi_bc(st["phi"], st["flags"], nx, ny, nz, a["theta"])
+    elif name in ("forces", "forces_wet"):
+        be.clear_forces(st["Fx"], st["Fy"], st["Fz"], n)
+        be.compute_csf_tension(st["phi"], st["flags"], st["Fx"], st["Fy"], st["Fz"], nx, ny, nz,
+                               a["gamma_lu"], a["wetting"], a["theta"])
+        be.compute_marangoni_force(st["T"], st["phi"], st["f_l"], st["Fx"], st["Fy"], st["Fz"],
+                                   st["flags"], nx, ny, nz, a["dgamma_lu"])
+        if a["welding"]:
+            be.apply_arc_pressure(st["Fz"], st["flags"], st["phi"], nx, ny, nz, a["arc_i"],
+                                  a["arc_j"], a["arc_k"], a["p_sigma"], a["pressure"], a["dt"],
+                                  a["dx"], a["rho_phys"])
+        if a["hydro"]:
+            be.add_hydrostatic_gravity(st["Fz"], st["f_l"], st["flags"], n, 1.0, a["g_lu"])
+        be.add_buoyancy(st["T"], st["Fz"], st["f_l"], st["flags"], n, a["g_lu"], a["beta"],
+                        a["T_liquidus"], 1.0)
+        be.clamp_body_force_magnitude(st["Fx"], st["Fy"], st["Fz"], st["flags"], n, a["F_cap"])
+    elif name in ("csf", "csf_wet"):
+        be.compute_csf_tension(st["phi"], st["flags"], st["Fx"], st["Fy"], st["Fz"], nx, ny, nz,
+                               a["gamma_lu"], a["wetting"], a["theta"])
+    elif name == "collide_mrt":
+        be.collide_mrt(st["f_a"], st["f_b"], st["rho"], st["ux"], st["uy"], st["uz"], st["Fx"],
+                       st["Fy"], st["Fz"], st["f_l"], st["flags"], n, a["omega"], a["omega_b"],
+                       a["C_darcy"])
+        be.clamp_velocity_mach(st["ux"], st["uy"], st["uz"], st["flags"], n, a["u_cap"])
+    elif name == "collide_srt":
+        be.collide_srt(st["f_a"], st["f_b"], st["rho"], st["ux"], st["uy"], st["uz"], st["Fx"],
+                       st["Fy"], st["Fz"], st["f_l"], st["flags"], n, a["omega"], a["C_darcy"])
+        be.clamp_velocity_mach(st["ux"], st["uy"], st["uz"], st["flags"], n, a["u_cap"])
+    elif name == "stream":
+        be.stream(st["f_b"], st["f_a"], st["flags"], nx, ny, nz)
+    elif name == "tail":
+        be.update_time_above_T(st["T"], st["flags"], st["time_above_800_s"],
+                               st["time_above_1100_s"], st["time_above_solidus_s"], n, a["dt"],
+                               800.0 + 273.15, 1100.0 + 273.15, a["T_solidus"])
+        be.snapshot_forces(st["Fx"], st["Fy"], st["Fz"], st["Fx_snap"], st["Fy_snap"],
+                           st["Fz_snap"], n)
+        be.remelt_hot_solid_scalar(st["T"], st["H"], st["f_l"], st["phi"], st["flags"], n,
+                                   a["cp_rho"], a["T_solidus"], a["T_liquidus"], a["L_rho"])
+        d = a["dir"]
+        be.solidify_trailing_pool_scalar(st["T"], st["H"], st["f_l"], st["phi"], st["flags"],
+                                         st["ux"], st["uy"], st["uz"], nx, ny, nz, a["cp_rho"],
+                                         a["arc_i"], a["arc_j"], a["arc_k"], d[0], d[1], d[2],
+                                         a["lookback"], a["T_freeze"], a["T_solidus"])
+        be.solidify_cooled_metal(st["T"], st["f_l"], st["phi"], st["flags"], st["ux"], st["uy"],
+                                 st["uz"], n, a["T_solidus"], 1)
+    elif name == "heat_loss":
+        be.apply_thermal_boundary_losses(st["H"], st["T"], st["flags"], nx, ny, nz, a["T_amb"],
+                                         a["h_conv"], a["eps_rad"], a["conv"], a["rad"], a["dt"],
+                                         a["dx"], a["sigma_sb"])
+        be.clamp_enthalpy_floor_scalar(st["H"], a["cp_rho"], st["flags"], n, a["T_amb"])
+    elif name == "surface_height":
+        got = {}
+        for key in a["heights"]:
+            i0, j0 = (int(v) for v in key.split("_"))
+            got[key] = float(be.surface_height_at(st["phi"], st["flags"], nx, ny, nz, i0, j0,
+                                                  a["nz_solid"]))
+        return got
+    elif name == "deposit":
+        placed = []
+        r_try = a["foot_r"]
+        placed_real = 0.0
+        for _ in range(3):
+            vol, real = be.feed_wire_surface(
+                st["f_a"], st["flags"], st["f_l"], st["phi"], st["H"], st["T"], st["rho"],
+                nx, ny, nz, a["arc_i"], a["arc_j"], a["arc_k"], r_try, a["drop_r"],
+                a["target_vol"], a["T_drop"], a["cp_rho"], a["L_rho"], 1.0, placed_real,
+                placed_real, a["cell_vol"])
+            placed_real = real
+            placed.append([r_try, real, vol])
+            r_try = min(r_try + 1.5, 16.0)
+        v = a["vel"]
+        be.feed_wire_momentum_impact(st["f_a"], st["rho"], st["ux"], st["uy"], st["uz"],
+                                     st["flags"], st["f_l"], nx, ny, nz, a["arc_i"], a["arc_j"],
+                                     a["arc_k"], a["drop_r"], v[0], v[1], v[2])
+        be.apply_droplet_impact_pressure(st["Fz"], st["flags"], st["phi"], st["f_l"], nx, ny, nz,
+                                         a["arc_i"], a["arc_j"], a["arc_k"], a["drop_r"],
+                                         a["impact_pa"], a["dt"], a["dx"], 7800.0)
+        return placed
+    elif name == "reset":
+        ny_ = ny
+        be.init_grid(st["f_a"], st["rho"], st["ux"], st["uy"], st["uz"], st["T"], st["H"],
+                     st["f_l"], st["phi"], st["flags"], nx, ny, nz, 300.0, 1.0, a["cp_rho"],
+                     a["nz_solid"], 0, nx, 0, ny_)
+        for f in ("T_max", "T_prev"):
+            st[f][...] = np.float32(300.0)
+        for f in ("dT_dt", "time_above_800_s", "Fx", "Fx_snap"):
+            st[f][...] = 0.0
+        be.stream(st["f_a"], st["f_b"], st["flags"], nx, ny, nz)
+    else:
+        raise KeyError(name)
+    return None
+
+
+CASES = ["inject_gauss", "inject_goldak", "ceiling", "thermal", "thermal_s2", "phase",
+         "tmax_cool", "vof", "vof_wet", "contact", "contact_s5", "forces", "forces_wet", "csf",
+         "csf_wet", "collide_mrt", "collide_srt", "stream", "tail", "heat_loss",
+         "surface_height", "deposit", "reset"]
+
+
+def check_case(be, name):
+    """Run ``name`` on ``be`` and assert parity with the golden outputs."""
+    a, st, outs = full_inputs(name)
+    extra = run_case(be, name, st, a)
+    worst = 0.0
+    for f, want in outs.items():
+        worst = max(worst, compare(name, st[f], want, f))
+    if name == "surface_height":
+        assert extra == a["heights"], (extra, a["heights"])
+    if name == "deposit":
+        for got, ref in zip(extra, a["placed"]):
+            assert abs(got[1] - ref[1]) <= 1e-6 * max(ref[1], 1e-30) + 1e-30, (extra, a["placed"])
+    return worst
+
+
+class OracleBackend:
+    """Backend over the C oracle (``oracle/oracle.py``)."""
+
+    def __init__(self):
+        import sys
+        root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+        if root not in sys.path:
+            sys.path.insert(0, root)
+        from oracle import oracle as O
+        self.O = O
+
+    def __getattr__(self, name):
+        O = self.__dict__["O"]
+        fn_name = "wo_" + name
+        if fn_name not in O._SIGS:
+            raise AttributeError(name)
+
+        def f(*args):
+            return O.call(fn_name, *args)
+        return f
+
+    def feed_wire_surface(self, *args):
+        args = list(args)
+        vol = np.array([args[20]], dtype=np.float32)
+        real = np.array([args[21]], dtype=np.float32)
+        args[20] = vol
+        args[21] = real
+        self.O.call("wo_feed_wire_surface", *args)
+        return float(vol[0]), float(real[0])

@@ -1,0 +1,504 @@
+"""Generate the golden fixtures in this folder from the waam_twin reference.
+
+TEST INFRASTRUCTURE ONLY.  Run in a container that has the reference
+checkout (``WAAM_REFERENCE_ROOT``, default ``/root/reference``)::
+
+    python tests/golden/make_golden.py
+
+Every fixture is produced by the reference's own, unmodified Taichi kernels
+(kernels.py, cumulant_kernel.py) or its own ``WAAMTwin.step`` /
+``coupled_step`` (twin.py:533-567, solvers/coupled_step.py:73-464), executed
+serially by the numpy stand-in in ``taichi_shim/`` with the deterministic
+semantics documented there.  Inputs are seeded synthetic states from
+``tests/state_gen.py``.  Outputs are small ``.npz`` files:
+
+* ``k_<case>.npz``: one kernel call -- ``in_<field>``/``out_<field>`` arrays,
+  ``args`` (JSON of the scalar arguments) and ``fields`` (JSON list).
+* ``step_<case>.npz``: a short ``WAAMTwin.step`` run -- the full state before
+  each step and after the last one (``s<n>_<field>``), the torch positions and
+  the twin's derived scalars.
+* ``kat_<case>.json``: known-answer values of the reference's validation
+  scripts executed on the stand-in (Poiseuille, VOF mass, Goldak energy).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.dirname(HERE))
+
+import refload  # noqa: E402
+from state_gen import MATERIAL, seeded_state  # noqa: E402
+
+wt = refload.load()
+from waam_twin import kernels as K  # noqa: E402
+from waam_twin.cumulant_kernel import collide_mrt  # noqa: E402
+from waam_twin.materials import MaterialProps  # noqa: E402
+from waam_twin.physics import arc as arc_mod  # noqa: E402
+
+FIELDS3 = ["rho", "ux", "uy", "uz", "T", "H", "f_l", "phi", "T_max", "T_prev", "dT_dt",
+           "time_above_800_s", "time_above_1100_s", "time_above_solidus_s",
+           "Fx", "Fy", "Fz", "Fx_snap", "Fy_snap", "Fz_snap", "flags"]
+
+
+def material(theta_deg=30.0):
+    m = MATERIAL
+    return MaterialProps(
+        name="ER70S-6-constants", k=m["k"], rho=m["rho"], cp=m["cp"],
+        alpha=m["k"] / (m["rho"] * m["cp"]), T_solidus=m["T_solidus"],
+        T_liquidus=m["T_liquidus"], L_fusion=m["L_fusion"], gamma_0=m["gamma_0"],
+        dgamma_dT=m["dgamma_dT"], T_ref_gamma=m["T_liquidus"], mu=m["mu"],
+        beta_T=m["beta_T"], contact_angle_deg=theta_deg, status="synthetic",
+    )
+
+
+def make_twin(nx, ny, nz, dx=2e-4, **kw):
+    kw.setdefault("use_srt", False)
+    kw.setdefault("enable_vof", True)
+    kw.setdefault("max_tracers", 64)
+    kw.setdefault("droplet_freq_hz", 0.0)
+    return wt.WAAMTwin(material=material(kw.pop("theta", 30.0)), nx=nx, ny=ny, nz=nz, dx=dx, **kw)
+
+
+def load_state(g, st):
+    for name in FIELDS3:
+        getattr(g, name).from_numpy(st[name])
+    g.f_a.from_numpy(st["f_a"])
+    g.f_b.from_numpy(st["f_b"])
+    if hasattr(g, "phi_tmp"):
+        g.phi_tmp.from_numpy(np.zeros_like(st["phi"]))
+
+
+def dump_state(g, prefix, out):
+    for name in FIELDS3:
+        out[prefix + name] = getattr(g, name).to_numpy()
+    out[prefix + "f_a"] = g.f_a.to_numpy()
+    out[prefix + "f_b"] = g.f_b.to_numpy()
+
+
+def save(name, payload):
+    path = os.path.join(HERE, name)
+    np.savez_compressed(path, **payload)
+    print("wrote", name, os.path.getsize(path), "bytes")
+
+
+# ---------------------------------------------------------------------------
+# kernel cases
+# ---------------------------------------------------------------------------
+NX, NY, NZ = 13, 11, 12
+
+
+def kernel_case(name, call, fields, seed=0, twin_kw=None, state_kw=None, extra_in=None):
+    tw = make_twin(NX, NY, NZ, **(twin_kw or {}))
+    g = tw.grid
+    st = seeded_state(NX, NY, NZ, seed=seed, **(state_kw or {}))
+    tw.nz_solid = st["nz_solid"]
+    load_state(g, st)
+    if extra_in:
+        extra_in(tw, g)
+    payload = {}
+    for f in fields:
+        payload["in_" + f] = getattr(g, f).to_numpy()
+    args = call(tw, g)
+    for f in fields:
+        payload["out_" + f] = getattr(g, f).to_numpy()
+    payload["args"] = np.array(json.dumps(args))
+    payload["fields"] = np.array(json.dumps(fields))
+    save("k_%s.npz" % name, payload)
+
+
+def scal(tw):
+    g = tw.grid
+    m = tw.mat
+    return dict(cp_rho=float(np.float32(tw.cp_rho)), L_rho=float(np.float32(tw.L_rho)),
+                T_solidus=m.T_solidus, T_liquidus=m.T_liquidus, T_cap=tw.T_vapor_cap_K,
+                alpha_lu=tw.alpha_lu, dt=g.dt, dx=g.dx, nz_solid=tw.nz_solid,
+                nx=g.nx, ny=g.ny, nz=g.nz)
+
+
+def c_inject_gauss(tw, g):
+    a = dict(arc_i=5.3, arc_j=4.6, arc_k=float(tw.nz_solid + 1), Q_w=3000.0, sigma=3.2,
+             dt=g.dt, dx3=g.dx ** 3, eta=0.75, pen=tw.arc_penetration_m / g.dx, enable=1)
+    K.inject_arc_heat(g.H, g.flags, g.phi, g.f_l, g.arc_norm_buf, a["arc_i"], a["arc_j"], a["arc_k"],
+                      a["Q_w"], a["sigma"], a["dt"], a["dx3"], a["eta"], a["pen"], a["enable"],
+                      g.FLAG_SOLID, g.FLAG_GAS)
+    a["norm"] = float(g.arc_norm_buf[None])
+    return a
+
+
+def c_inject_goldak(tw, g):
+    a = dict(arc_i=6.1, arc_j=5.2, arc_k=float(tw.nz_solid + 1), Q_w=4000.0, dt=g.dt,
+             dx3=g.dx ** 3, eta=0.78, sign=-1.0, ff=0.6, fr=1.4, a_front=3.0, a_rear=6.5,
+             b=2.5, c=2.0, pen=tw.arc_penetration_m / g.dx, enable=1)
+    K.inject_goldak_heat(g.H, g.flags, g.phi, g.f_l, g.arc_norm_buf, a["arc_i"], a["arc_j"], a["arc_k"],
+                         a["Q_w"], a["dt"], a["dx3"], a["eta"], a["sign"], a["ff"], a["fr"],
+                         a["a_front"], a["a_rear"], a["b"], a["c"], a["pen"], a["enable"],
+                         g.FLAG_SOLID, g.FLAG_GAS)
+    a["norm"] = float(g.arc_norm_buf[None])
+    return a
+
+
+def c_ceiling(tw, g):
+    a = scal(tw)
+    a["T_cap"] = 2500.0
+    K.clamp_enthalpy_ceiling_scalar(g.H, g.flags, tw.cp_rho, a["T_solidus"], a["T_liquidus"],
+                                    a["T_cap"], tw.L_rho, g.FLAG_GAS)
+    return a
+
+
+def c_thermal(tw, g):
+    a = scal(tw)
+    K.advect_diffuse_temperature(g.H, g.T, g.ux, g.uy, g.uz, g.flags, tw.alpha_lu, 1.0,
+                                 g.FLAG_SOLID, g.FLAG_GAS, tw.cp_rho, g.nx, g.ny, g.nz)
+    return a
+
+
+def c_phase(tw, g):
+    a = scal(tw)
+    K.update_phase(g.H, g.T, g.f_l, tw.cp_rho, tw.L_rho, a["T_solidus"], a["T_liquidus"])
+    return a
+
+
+def c_tmax_cool(tw, g):
+    a = scal(tw)
+    K.update_T_max(g.T, g.T_max, g.flags, g.FLAG_GAS)
+    K.update_cooling_rate(g.T, g.T_prev, g.dT_dt, g.flags, g.dt, g.FLAG_GAS)
+    return a
+
+
+def c_vof_chain(wetting):
+    def run(tw, g):
+        a = scal(tw)
+        a["theta"] = tw.theta_rad
+        a["wetting"] = int(wetting)
+        K.advect_phi(g.phi_tmp, g.phi, g.ux, g.uy, g.uz, g.flags, g.FLAG_SOLID, g.FLAG_GAS,
+                     g.nx, g.ny, g.nz)
+        g.phi.copy_from(g.phi_tmp)
+        K.reinitialize_phi(g.phi, g.flags, g.FLAG_SOLID, g.FLAG_GAS, g.FLAG_FLUID)
+        if wetting:
+            K.apply_contact_angle_phi_bc(g.phi, g.flags, tw.theta_rad, g.FLAG_SOLID, g.FLAG_GAS,
+                                         g.nx, g.ny, g.nz)
+        K.update_flags_from_phi(g.phi, g.f_l, g.flags, tw.nz_solid, g.FLAG_FLUID, g.FLAG_SOLID,
+                                g.FLAG_GAS, g.FLAG_IFACE)
+        K.sync_phi_liquid_fraction(g.phi, g.f_l, g.flags, g.FLAG_GAS, g.FLAG_SOLID)
+        return a
+    return run
+
+
+def c_contact(tw, g):
+    a = scal(tw)
+    a["theta"] = tw.theta_rad
+    K.apply_contact_angle_phi_bc(g.phi, g.flags, tw.theta_rad, g.FLAG_SOLID, g.FLAG_GAS,
+                                 g.nx, g.ny, g.nz)
+    return a
+
+
+def c_forces(wetting, welding=True, hydro=True):
+    def run(tw, g):
+        a = scal(tw)
+        a.update(gamma_lu=tw.gamma_lu, dgamma_lu=tw.dgamma_dT_lu, theta=tw.theta_rad,
+                 wetting=int(wetting), arc_i=6.4, arc_j=5.1, arc_k=float(tw.nz_solid + 1),
+                 p_sigma=3.0, pressure=500.0, rho_phys=tw.mat.rho, g_lu=tw.g_lu,
+                 beta=tw.beta_T, F_cap=0.05, welding=int(welding), hydro=int(hydro))
+        K.clear_forces(g.Fx, g.Fy, g.Fz)
+        K.compute_csf_tension(g.phi, g.flags, g.Fx, g.Fy, g.Fz, tw.gamma_lu, g.FLAG_SOLID,
+                              g.FLAG_GAS, g.nx, g.ny, g.nz, int(wetting), float(tw.theta_rad))
+        K.compute_marangoni_force(g.T, g.phi, g.f_l, g.Fx, g.Fy, g.Fz, g.flags, tw.dgamma_dT_lu,
+                                  g.dx, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+        if welding:
+            K.apply_arc_pressure(g.Fz, g.flags, g.phi, a["arc_i"], a["arc_j"], a["arc_k"],
+                                 a["p_sigma"], a["pressure"], g.dt, g.dx, tw.mat.rho,
+                                 g.FLAG_SOLID, g.FLAG_GAS)
+        if hydro:
+            K.add_hydrostatic_gravity(g.Fz, g.f_l, g.flags, 1.0, tw.g_lu, g.FLAG_SOLID, g.FLAG_GAS)
+        K.add_buoyancy(g.T, g.Fz, g.f_l, g.flags, tw.g_lu, tw.beta_T, tw.mat.T_liquidus, 1.0,
+                       g.FLAG_SOLID, g.FLAG_GAS)
+        K.clamp_body_force_magnitude(g.Fx, g.Fy, g.Fz, g.flags, 0.05, g.FLAG_SOLID, g.FLAG_GAS)
+        return a
+    return run
+
+
+def c_csf_only(wetting):
+    def run(tw, g):
+        a = scal(tw)
+        a.update(gamma_lu=tw.gamma_lu * 50.0, theta=tw.theta_rad, wetting=int(wetting))
+        K.compute_csf_tension(g.phi, g.flags, g.Fx, g.Fy, g.Fz, a["gamma_lu"], g.FLAG_SOLID,
+                              g.FLAG_GAS, g.nx, g.ny, g.nz, int(wetting), float(tw.theta_rad))
+        return a
+    return run
+
+
+def c_collide(kind):
+    def run(tw, g):
+        a = scal(tw)
+        a.update(omega=tw.omega, omega_b=tw.omega_bulk, C_darcy=tw.C_darcy, tau=g.tau, u_cap=0.08)
+        if kind == "mrt":
+            collide_mrt(g.f_a, g.f_b, g.rho, g.ux, g.uy, g.uz, g.Fx, g.Fy, g.Fz, g.f_l, g.flags,
+                        g.ex, g.ey, g.ez, g.w, g.opp, tw.omega, tw.omega_bulk, tw.C_darcy,
+                        g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+        else:
+            K.collide_srt(g.f_a, g.f_b, g.rho, g.ux, g.uy, g.uz, g.Fx, g.Fy, g.Fz, g.f_l, g.flags,
+                          g.tau, tw.omega, 1.0, tw.C_darcy, g.FLAG_SOLID, g.FLAG_GAS,
+                          g.nx, g.ny, g.nz)
+        K.clamp_velocity_mach(g.ux, g.uy, g.uz, g.flags, 0.08, g.FLAG_SOLID, g.FLAG_GAS)
+        return a
+    return run
+
+
+def c_stream(tw, g):
+    a = scal(tw)
+    K.stream(g.f_b, g.f_a, g.flags, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+    return a
+
+
+def c_tail(tw, g):
+    a = scal(tw)
+    a.update(arc_i=9.5, arc_j=5.0, arc_k=float(tw.nz_solid + 1), dir=[1.0, 0.0, 0.0],
+             lookback=2.0, T_freeze=tw.mat.T_liquidus + 35.0)
+    K.update_time_above_T(g.T, g.flags, g.time_above_800_s, g.time_above_1100_s,
+                          g.time_above_solidus_s, g.dt, 800.0 + 273.15, 1100.0 + 273.15,
+                          tw.mat.T_solidus, g.FLAG_GAS)
+    K.snapshot_forces(g.Fx, g.Fy, g.Fz, g.Fx_snap, g.Fy_snap, g.Fz_snap)
+    K.remelt_hot_solid_scalar(g.T, g.H, g.f_l, g.phi, g.flags, tw.cp_rho, tw.mat.T_solidus,
+                              tw.mat.T_liquidus, tw.L_rho, g.FLAG_SOLID, g.FLAG_FLUID)
+    K.solidify_trailing_pool_scalar(g.T, g.H, g.f_l, g.phi, g.flags, g.ux, g.uy, g.uz, tw.cp_rho,
+                                    a["arc_i"], a["arc_j"], a["arc_k"], 1.0, 0.0, 0.0,
+                                    a["lookback"], a["T_freeze"], tw.mat.T_solidus,
+                                    g.FLAG_SOLID, g.FLAG_FLUID, g.FLAG_GAS)
+    K.solidify_cooled_metal(g.T, g.f_l, g.phi, g.flags, g.ux, g.uy, g.uz, tw.mat.T_solidus, 1,
+                            g.FLAG_SOLID, g.FLAG_FLUID, g.FLAG_GAS)
+    return a
+
+
+def c_heat_loss(tw, g):
+    a = scal(tw)
+    a.update(T_amb=300.0, h_conv=25.0, eps_rad=0.3, conv=1, rad=1, sigma_sb=5.670374419e-8)
+    K.apply_thermal_boundary_losses(g.H, g.T, g.flags, 300.0, 25.0, 0.3, 1, 1, tw.cp_rho, g.dt,
+                                    g.dx, a["sigma_sb"], g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+    K.clamp_enthalpy_floor_scalar(g.H, tw.cp_rho, g.flags, 300.0, g.FLAG_GAS)
+    return a
+
+
+def c_surface_height(tw, g):
+    out = {}
+    for (i0, j0) in [(3, 4), (7, 2), (12, 10), (0, 0)]:
+        K.surface_height_at(g.phi, g.flags, g.surface_k_buf, i0, j0, tw.nz_solid, g.FLAG_GAS, g.nz)
+        out["%d_%d" % (i0, j0)] = float(g.surface_k_buf[None])
+    a = scal(tw)
+    a["heights"] = out
+    return a
+
+
+def c_deposit(tw, g):
+    a = scal(tw)
+    a.update(arc_i=6.2, arc_j=5.4, arc_k=float(tw.nz_solid + 1), foot_r=3.5, drop_r=2.2,
+             T_drop=tw.mat.T_liquidus + 500.0, cell_vol=g.dx ** 3)
+    a["target_vol"] = 30.0 * g.dx ** 3
+    placed = []
+    r_try = a["foot_r"]
+    placed_real = 0.0
+    for _ in range(3):
+        g.deposit_vol_buf[None] = placed_real
+        g.deposit_real_buf[None] = placed_real
+        K.feed_wire_surface(g.f_a, g.flags, g.f_l, g.phi, g.H, g.T, g.rho, a["arc_i"], a["arc_j"],
+                            a["arc_k"], r_try, a["drop_r"], a["target_vol"], a["T_drop"], tw.cp_rho,
+                            tw.L_rho, 1.0, g.deposit_vol_buf, g.deposit_real_buf, g.dx ** 3,
+                            g.FLAG_GAS, g.FLAG_FLUID, g.FLAG_SOLID, g.nx, g.ny, g.nz)
+        placed_real = float(g.deposit_real_buf[None])
+        placed.append([r_try, placed_real, float(g.deposit_vol_buf[None])])
+        r_try = min(r_try + 1.5, 16.0)
+    a["placed"] = placed
+    a.update(vel=[0.004, -0.002, -0.03])
+    K.feed_wire_momentum_impact(g.f_a, g.rho, g.ux, g.uy, g.uz, g.flags, g.f_l, a["arc_i"],
+                                a["arc_j"], a["arc_k"], a["drop_r"], 0.004, -0.002, -0.03,
+                                g.FLAG_GAS, g.nx, g.ny, g.nz)
+    a.update(impact_pa=2.0e4)
+    K.apply_droplet_impact_pressure(g.Fz, g.flags, g.phi, g.f_l, a["arc_i"], a["arc_j"], a["arc_k"],
+                                    a["drop_r"], a["impact_pa"], g.dt, g.dx, tw.mat.rho,
+                                    g.FLAG_SOLID, g.FLAG_GAS)
+    return a
+
+
+def c_reset(tw, g):
+    a = scal(tw)
+    tw.reset()
+    a["nz_solid"] = tw.nz_solid
+    return a
+
+
+def kernel_cases():
+    base = ["H", "T", "f_l", "phi", "flags"]
+    kernel_case("inject_gauss", c_inject_gauss, ["H"])
+    kernel_case("inject_goldak", c_inject_goldak, ["H"], seed=1)
+    kernel_case("ceiling", c_ceiling, ["H"])
+    kernel_case("thermal", c_thermal, ["H"])
+    kernel_case("thermal_s2", c_thermal, ["H"], seed=2)
+    kernel_case("phase", c_phase, ["H", "T", "f_l"])
+    kernel_case("tmax_cool", c_tmax_cool, ["T_max", "T_prev", "dT_dt"])
+    kernel_case("vof", c_vof_chain(False), ["phi", "flags", "f_l", "phi_tmp"])
+    kernel_case("vof_wet", c_vof_chain(True), ["phi", "flags", "f_l", "phi_tmp"], seed=3)
+    kernel_case("contact", c_contact, ["phi"], seed=4)
+    kernel_case("contact_s5", c_contact, ["phi"], seed=5, twin_kw=dict(theta=60.0))
+    kernel_case("forces", c_forces(False), ["Fx", "Fy", "Fz"])
+    kernel_case("forces_wet", c_forces(True), ["Fx", "Fy", "Fz"], seed=6)
+    kernel_case("csf", c_csf_only(False), ["Fx", "Fy", "Fz"], seed=7)
+    kernel_case("csf_wet", c_csf_only(True), ["Fx", "Fy", "Fz"], seed=8)
+    kernel_case("collide_mrt", c_collide("mrt"), ["f_b", "rho", "ux", "uy", "uz"])
+    kernel_case("collide_srt", c_collide("srt"), ["f_b", "rho", "ux", "uy", "uz"], seed=9)
+    kernel_case("stream", c_stream, ["f_a"])
+    kernel_case("tail", c_tail, base + ["time_above_800_s", "time_above_1100_s",
+                                        "time_above_solidus_s", "Fx_snap", "Fy_snap", "Fz_snap",
+                                        "ux", "uy", "uz"], seed=10)
+    kernel_case("heat_loss", c_heat_loss, ["H"], seed=11)
+    kernel_case("surface_height", c_surface_height, ["phi"], seed=12)
+    kernel_case("deposit", c_deposit, base + ["rho", "f_a", "ux", "uy", "uz", "Fz"], seed=13)
+    kernel_case("reset", c_reset, base + ["rho", "ux", "uy", "uz", "f_a", "f_b", "T_max",
+                                          "T_prev", "dT_dt", "time_above_800_s", "Fx", "Fx_snap"])
+
+
+# ---------------------------------------------------------------------------
+# full-step cases
+# ---------------------------------------------------------------------------
+def twin_scalars(tw):
+    g = tw.grid
+    return dict(
+        nx=g.nx, ny=g.ny, nz=g.nz, dx=g.dx, dt=g.dt, tau=g.tau, alpha_lu=tw.alpha_lu,
+        omega=tw.omega, omega_bulk=tw.omega_bulk, cp_rho=tw.cp_rho, L_rho=tw.L_rho,
+        sigma_cells=tw.sigma_cells, g_lu=tw.g_lu, gamma_lu=tw.gamma_lu,
+        dgamma_dT_lu=tw.dgamma_dT_lu, theta_rad=tw.theta_rad, nz_solid=tw.nz_solid,
+        Q_w=tw.Q_w, eta=tw.eta, C_darcy=tw.C_darcy,
+    )
+
+
+def step_case(name, nx, ny, nz, n_steps, positions, twin_kw, setup=None, seeded=None):
+    tw = make_twin(nx, ny, nz, **twin_kw)
+    if setup:
+        setup(tw)
+    tw.reset()
+    g = tw.grid
+    if seeded is not None:
+        st = seeded_state(nx, ny, nz, seed=seeded, nz_solid=tw.nz_solid)
+        load_state(g, st)
+    payload = {}
+    log = []
+    for s in range(n_steps):
+        dump_state(g, "s%d_" % s, payload)
+        payload["s%d_read_is_a" % s] = np.array(g.f_src is g.f_a)
+        x, y = positions[s]
+        tw.step(x, y, True)
+        log.append(dict(arc=list(tw._last_arc_ijk), droplets=tw._n_droplets_fired,
+                        deposited=tw._deposited_volume_m3, dir=list(tw._torch_dir_xyz),
+                        last_drop=tw._last_droplet_time))
+    dump_state(g, "s%d_" % n_steps, payload)
+    payload["s%d_read_is_a" % n_steps] = np.array(g.f_src is g.f_a)
+    payload["positions"] = np.array(positions, dtype=np.float64)
+    payload["scalars"] = np.array(json.dumps(twin_scalars(tw)))
+    payload["twin_kw"] = np.array(json.dumps(twin_kw))
+    payload["log"] = np.array(json.dumps(log))
+    save("step_%s.npz" % name, payload)
+
+
+def step_cases():
+    # Config-1-like: Gaussian2D arc, MRT, VOF, no wire feed, plate 4 cells.
+    nx, ny, nz = 16, 12, 12
+    dx = 2.5e-4
+    cy = (ny // 2) * dx
+    pos = [(0.0012 + s * 0.008 * dx * 0.1, cy) for s in range(4)]
+    kw1 = dict(dx=dx, heat_source="gaussian2d", arc_power_W=3000.0, arc_efficiency=0.75,
+               arc_sigma_mm=0.75, travel_speed_m_s=0.008)
+    step_case("c1_plate", nx, ny, nz, 3, pos, kw1,
+              setup=lambda tw: setattr(tw, "plate_thickness_mm", 1.0))
+    # Same config from a seeded molten state (exercises collide/stream/forces).
+    step_case("c1_seeded", nx, ny, nz, 3, pos, kw1,
+              setup=lambda tw: setattr(tw, "plate_thickness_mm", 1.0), seeded=21)
+
+    # Config-2-like: Goldak, 100 Hz droplets (first fires at step 0), wetting 30 deg,
+    # CSF, hydrostatic gravity, buoyancy, Marangoni, MRT.
+    dx2 = 2e-4
+    cy2 = (ny // 2) * dx2
+    pos2 = [(0.0014 + s * 0.008 * dx2 * 0.1, cy2) for s in range(4)]
+    kw2 = dict(dx=dx2, heat_source="goldak", arc_power_W=4000.0, arc_efficiency=0.78,
+               arc_sigma_mm=0.6, droplet_freq_hz=100.0, enable_wetting=True,
+               enable_csf_tension=True, enable_hydrostatic_gravity=True,
+               travel_speed_m_s=0.008)
+
+    def setup2(tw):
+        tw.plate_thickness_mm = 0.8
+        tw.wire_feed_m_s = 0.1
+        tw.droplet_transfer_mode = "pulsed"
+        tw.pulse_frequency_hz = 100.0
+        tw.droplet_size_jitter = 0.0
+        tw.arc_source = arc_mod.Goldak3D(ff=0.6, fr=1.4, a_front=3.0 / (dx2 * 1e3) / 4,
+                                         a_rear=9.0 / (dx2 * 1e3) / 4, b=3.0 / (dx2 * 1e3) / 4,
+                                         c=3.0 / (dx2 * 1e3) / 4)
+
+    def run2(name, seeded):
+        tw_setup = setup2
+
+        def s(tw):
+            tw_setup(tw)
+        tw = make_twin(nx, ny, nz, **kw2)
+        s(tw)
+        tw.reset()
+        tw._last_droplet_time = -1.0  # first step fires a droplet
+        g = tw.grid
+        if seeded is not None:
+            st = seeded_state(nx, ny, nz, seed=seeded, nz_solid=tw.nz_solid)
+            load_state(g, st)
+        payload = {}
+        log = []
+        for step in range(3):
+            dump_state(g, "s%d_" % step, payload)
+            payload["s%d_read_is_a" % step] = np.array(g.f_src is g.f_a)
+            payload["s%d_last_drop" % step] = np.array(tw._last_droplet_time)
+            payload["s%d_n_drops" % step] = np.array(tw._n_droplets_fired)
+            x, y = pos2[step]
+            tw.step(x, y, True)
+            log.append(dict(arc=list(tw._last_arc_ijk), droplets=tw._n_droplets_fired,
+                            deposited=tw._deposited_volume_m3, dir=list(tw._torch_dir_xyz),
+                            last_drop=tw._last_droplet_time))
+        dump_state(g, "s3_", payload)
+        payload["s3_read_is_a"] = np.array(g.f_src is g.f_a)
+        payload["positions"] = np.array(pos2, dtype=np.float64)
+        sc = twin_scalars(tw)
+        sc.update(goldak=dict(ff=tw.arc_source.ff, fr=tw.arc_source.fr,
+                              a_front=tw.arc_source.a_front, a_rear=tw.arc_source.a_rear,
+                              b=tw.arc_source.b, c=tw.arc_source.c))
+        payload["scalars"] = np.array(json.dumps(sc))
+        payload["twin_kw"] = np.array(json.dumps(kw2))
+        payload["log"] = np.array(json.dumps(log))
+        save("step_%s.npz" % name, payload)
+
+    run2("c2_drop", None)
+    run2("c2_seeded", 22)
+
+
+# ---------------------------------------------------------------------------
+# known-answer values of the reference validation scripts
+# ---------------------------------------------------------------------------
+def kats():
+    import importlib
+    out = {}
+    for name, kw in [("test_vof_mass", {}), ("test_goldak_energy", {}),
+                     ("test_lbm_poiseuille", {}), ("test_stefan_solidification", {})]:
+        mod = importlib.import_module("waam_twin.validation." + name)
+        out[name] = float(mod.run(**kw))
+    with open(os.path.join(HERE, "kat_reference.json"), "w") as fh:
+        json.dump(out, fh, indent=1, sort_keys=True)
+    print("kats", out)
+
+
+if __name__ == "__main__":
+    what = sys.argv[1:] or ["kernels", "steps", "kats"]
+    if "kernels" in what:
+        kernel_cases()
+    if "steps" in what:
+        step_cases()
+    if "kats" in what:
+        kats()
