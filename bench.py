@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Throughput of the coupled melt-pool step on B200 (MLUPS, HBM roofline).
+
+Workload (default): the standard-size bead-on-plate case -- 256x128x96 D3Q19
+lattice, dx = 0.2 mm, constants-only ER70S-6-like steel, Goldak double
+ellipsoid (a_f 3 / a_r 9 / b 3 / c 3 mm, ff 0.6 / fr 1.4), 4 kW, eta 0.78,
+1.2 mm wire at 6 m/min as pulsed 100 Hz droplets, VOF with 30 deg wetting,
+CSF, Marangoni, buoyancy, hydrostatic gravity, two-rate central-moment
+collision, torch on a straight 40 mm line at 8 mm/s.  Synthetic inputs: the
+run starts from the reference's reset state and spins up (droplets deposit a
+bead) before timing.  One step = one ``WAAMTwin.step``.
+
+``python bench.py [--gpus N] [--steps K] [--warmup W]`` prints one JSON line.
+Under torchrun every rank runs an independent replica (the step has no
+cross-GPU exchange), timing is the max over ranks.
+``--impl reference`` times the CPU restatement of the reference step (the
+oracle, all host cores) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    "standard": dict(
+        workload="bead-on-plate 256x128x96 D3Q19, dx 0.2 mm, Goldak 4 kW, 100 Hz wire droplets, "
+                 "VOF+wetting 30deg+CSF+Marangoni+buoyancy+gravity, central-moment MRT",
+        nx=256, ny=128, nz=96, dx=2e-4, heat_source="goldak", arc_power_W=4000.0,
+        arc_efficiency=0.78, goldak_mm=dict(a_front_mm=3.0, a_rear_mm=9.0, b_mm=3.0, c_mm=3.0,
+                                            ff=0.6, fr=1.4),
+        droplet_freq_hz=100.0, wire_feed_m_s=0.1, wire_diameter_mm=1.2, enable_vof=True,
+        enable_wetting=True, contact_angle_deg=30.0, enable_csf_tension=True,
+        enable_hydrostatic_gravity=True, use_srt=False, travel_speed_m_s=0.008,
+        path_mm=((5.6, 12.8), (45.6, 12.8)), spinup=1200),
+    "small": dict(
+        workload="bead-on-plate 64x32x32 D3Q19, dx 0.25 mm, Gaussian 3 kW r 3 mm, no wire, VOF, "
+                 "central-moment MRT",
+        nx=64, ny=32, nz=32, dx=2.5e-4, heat_source="gaussian2d", arc_power_W=3000.0,
+        arc_efficiency=0.75, arc_sigma_mm=3.0, droplet_freq_hz=0.0, enable_vof=True,
+        plate_thickness_mm=4.0, use_srt=False, travel_speed_m_s=0.008,
+        path_mm=((4.0, 4.0), (14.0, 4.0)), spinup=200),
+}
+
+MATERIAL = dict(k=30.0, rho=7800.0, cp=680.0, T_solidus=1723.0, T_liquidus=1783.0,
+                L_fusion=2.7e5, gamma_0=1.8, dgamma_dT=-4.3e-4, mu=0.0065, beta_T=1.2e-4)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def twin_kwargs(w):
+    keys = ("heat_source", "arc_power_W", "arc_efficiency", "droplet_freq_hz", "enable_vof",
+            "enable_wetting", "contact_angle_deg", "enable_csf_tension",
+            "enable_hydrostatic_gravity", "use_srt", "travel_speed_m_s", "arc_sigma_mm",
+            "wire_diameter_mm")
+    return {k: w[k] for k in keys if k in w}
+
+
+def build_twin(w, device):
+    from waam_solver_b200 import WAAMTwin
+    from waam_solver_b200.materials import from_constants
+    from waam_solver_b200.physics.arc import goldak_from_job_mm
+    mat = from_constants("ER70S-6-constants", MATERIAL, contact_angle_deg=w.get("contact_angle_deg", 30.0))
+    tw = WAAMTwin(material=mat, nx=w["nx"], ny=w["ny"], nz=w["nz"], dx=w["dx"], max_tracers=1024,
+                  device=device, **twin_kwargs(w))
+    if w.get("plate_thickness_mm"):
+        tw.plate_thickness_mm = w["plate_thickness_mm"]
+    if w.get("wire_feed_m_s"):
+        tw.wire_feed_m_s = w["wire_feed_m_s"]
+        tw.droplet_transfer_mode = "pulsed"
+        tw.pulse_frequency_hz = w["droplet_freq_hz"]
+        tw.droplet_size_jitter = 0.0
+    if w.get("goldak_mm"):
+        tw.arc_source = goldak_from_job_mm(tw, w["goldak_mm"])
+    tw.reset()
+    return tw
+
+
+def positions(w, dt, n, start=0):
+    (x0, y0), (x1, y1) = w["path_mm"]
+    L = math.hypot(x1 - x0, y1 - y0) * 1e-3
+    out = []
+    for s in range(start, start + n):
+        d = min(s * dt * w["travel_speed_m_s"], L)
+        u = d / L
+        out.append((x0 * 1e-3 + u * (x1 - x0) * 1e-3, y0 * 1e-3 + u * (y1 - y0) * 1e-3))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def census(twin):
+    import torch
+    f = twin.grid.flags
+    n = f.numel()
+    solid = int((f == 1).sum().item())
+    gas = int((f == 2).sum().item())
+    return dict(n=n, solid=solid, gas=gas, fluid=n - solid - gas)
+
+
+def algorithmic_bytes(c):
+    """Compulsory DRAM bytes per launch of each fused stage (FP32 fields, int32
+    flags), from the cell census; each field element counted once."""
+    n, ns, ng, nf = c["n"], c["n"] - c["solid"], c["n"] - c["gas"], c["fluid"]
+    return {
+        "thermal": 20 * n + 24 * ng + 12 * nf,
+        "vof_advect": 12 * n + 12 * ng,
+        "column": 20 * n + 28 * ng,
+        "collide": 4 * n + 12 * (n - nf) + 344 * nf,
+        "stream": 4 * n + 304 * ns,
+        "tail": 0,
+    }
+
+
+STAGES = ["thermal", "vof_advect", "column", "collide", "stream", "tail"]
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def dist_max(x):
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier():
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier()
+
+
+def cpu_baseline(w, budget_s=15.0, max_steps=12):
+    """The CPU oracle (C restatement, OpenMP on all host cores) on the same
+    workload: reset, then as many full steps as fit the time budget."""
+    from oracle.oracle_step import OracleTwin
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.lib()
+    O.call("wo_set_num_threads", threads)
+    kw = twin_kwargs(w)
+    kw.pop("wire_diameter_mm", None)
+    g = None
+    if w.get("goldak_mm"):
+        gm = w["goldak_mm"]
+        dxmm = w["dx"] * 1e3
+        g = dict(ff=gm["ff"], fr=gm["fr"], a_front=gm["a_front_mm"] / dxmm,
+                 a_rear=gm["a_rear_mm"] / dxmm, b=gm["b_mm"] / dxmm, c=gm["c_mm"] / dxmm)
+    extra = {}
+    if w.get("wire_feed_m_s"):
+        extra = dict(wire_feed_m_s=w["wire_feed_m_s"], droplet_transfer_mode="pulsed",
+                     pulse_frequency_hz=w["droplet_freq_hz"], droplet_size_jitter=0.0)
+    if w.get("plate_thickness_mm"):
+        extra["plate_thickness_mm"] = w["plate_thickness_mm"]
+    mat = dict(MATERIAL, contact_angle_deg=w.get("contact_angle_deg", 30.0))
+    ot = OracleTwin(w["nx"], w["ny"], w["nz"], w["dx"], mat, goldak=g, **kw, **extra)
+    ot.reset()
+    pos = positions(w, ot.dt, max_steps + 1)
+    ot.step(*pos[0], True)  # warm-up (page-in, thread pool)
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps and (time.perf_counter() - t0) < budget_s:
+        ot.step(*pos[n + 1], True)
+        n += 1
+    el = time.perf_counter() - t0
+    cells = w["nx"] * w["ny"] * w["nz"]
+    return {"value": cells * n / el / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": "%d full steps of the %dx%dx%d workload after reset (%.1f s)" % (
+                n, w["nx"], w["ny"], w["nz"], el)}
+
+
+def run_reference(args, w):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    budget = max(5.0, min(60.0, 2.0 * args.steps))
+    cb = cpu_baseline(w, budget_s=budget, max_steps=max(args.steps, 3))
+    line = {"impl": "reference", "metric": "coupled step throughput (MLUPS)", "value": cb["value"],
+            "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": w["workload"]}, "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, w):
+    import torch
+    from waam_solver_b200 import _native
+    world, rank, local = dist_setup()
+    device = torch.device("cuda", local)
+    tw = build_twin(w, device)
+    g = tw.grid
+    cells = g.n_cells
+    total = w["spinup"] + args.warmup + 2 * args.steps + 4
+    pos = positions(w, g.dt, total)
+    s = 0
+    for _ in range(w["spinup"] + args.warmup):
+        tw.step(*pos[s], True)
+        s += 1
+    torch.cuda.synchronize()
+
+    # ---- device-resident run (value): positions staged on the device ----
+    K = args.steps
+    dev_pos = torch.tensor([[x / g.dx, y / g.dx] for x, y in pos[s:s + K]], dtype=torch.float32,
+                           device=device)
+    ev_sets = [[torch.cuda.Event(enable_timing=True) for _ in range(7)] for _ in range(K)]
+    for es in ev_sets:
+        for e in es:
+            e.record()
+    drops0 = tw._n_droplets_fired
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record()
+        for k in range(K):
+            tw._device_position = dev_pos[k]
+            tw._stage_events = ev_sets[k]
+            tw.step(*pos[s], True)
+            s += 1
+        stop.record()
+        torch.cuda.synchronize()
+    tw._device_position = None
+    tw._stage_events = None
+    barrier()
+    ms_local = start.elapsed_time(stop)
+    ms = dist_max(ms_local)
+    drops = tw._n_droplets_fired - drops0
+    stage_ms = {}
+    for i, name in enumerate(STAGES):
+        stage_ms[name] = statistics.fmean(es[i].elapsed_time(es[i + 1]) for es in ev_sets)
+    c = census(tw)
+    algo = algorithmic_bytes(c)
+    hbm, hbm_src = peaks()
+    dom = max(("stream", "collide", "thermal", "column", "vof_advect"),
+              key=lambda k: stage_ms[k])
+    achieved = algo[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_%s.json" % dom)
+    if os.path.exists(tpath):
+        with open(tpath) as fh:
+            t = json.load(fh)
+        traffic = t["dram_bytes_per_cell"] * c["n"]
+    step_bytes = sum(algo.values())
+    lib = _native.lib()
+    launches_per_step = lib.waam_step_launch_count(tw._fused_params, 0) + \
+        lib.waam_step_launch_count(tw._fused_params, 1)
+
+    # ---- end-to-end run through the public API with host inputs / outputs ----
+    probe = (g.nx // 2) * g.ny * g.nz + (g.ny // 2) * g.nz + tw.nz_solid - 1
+    host_out = torch.zeros(K, dtype=torch.float32, pin_memory=True)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(K):
+        tw.step(*pos[s], True)           # torch position from the host (pinned H2D, 8 B)
+        s += 1
+        host_out[k:k + 1].copy_(g.T.view(-1)[probe:probe + 1], non_blocking=True)  # D2H, 4 B
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    ms_e2e = dist_max(e0.elapsed_time(e1))
+
+    value = world * cells * K / (ms * 1e-3) / 1e6
+    e2e = world * cells * K / (ms_e2e * 1e-3) / 1e6
+    line = {
+        "metric": "coupled step throughput (MLUPS)", "value": value, "unit": "MLUPS",
+        "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (reference reset state + %d spin-up steps)" % w["spinup"],
+        "config": {"workload": w["workload"], "cells": cells, "global_batch": world,
+                   "parallelism": "replicas x%d" % world, "l2": "inputs larger than L2 "
+                   "(populations %.0f MB)" % (2 * 19 * cells * 4 / 1e6),
+                   "droplets_in_timed_region": drops},
+        "roofline": {"bound": "hbm", "kernel": "k_" + ("stream" if dom == "stream" else dom),
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic, "peak_source": hbm_src,
+                     "algorithmic_bytes_per_launch": algo[dom]},
+        "stages_ms": stage_ms,
+        "step_algorithmic_GBps": step_bytes / (ms / K * 1e-3) / 1e9,
+        "cell_census": c,
+        "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 4},
+        "gpu_launches": int(launches_per_step * 2 * K),
+        "clocks": clocks.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="standard", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_b200(args, w)
+
+
+if __name__ == "__main__":
+    main()

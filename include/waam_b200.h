@@ -1,0 +1,274 @@
+/* waam_b200 -- C ABI of the B200 (sm_100a) coupled melt-pool step.
+ *
+ * Drop-in native backend for the waam_twin operator API (physics/*.py) and
+ * its step driver (solvers/coupled_step.py:73-464) of THEDARKDEACON/waam_solver.
+ * All pointers are DEVICE pointers to memory owned by the caller (torch
+ * tensors in the Python host); the library never allocates or frees on these
+ * paths.  `stream` is a cudaStream_t passed as void*; every call is
+ * asynchronous and stream-ordered.  Sizes: scalar fields hold nx*ny*nz
+ * elements (k fastest), population fields 19*nx*ny*nz, flags are int32 with
+ * FLUID=0, SOLID=1, GAS=2, IFACE=4 (grid.py:63-66).
+ *
+ * Every call returns WAAM_OK (0) or a negative status; waam_last_error()
+ * gives the message of the last failure on the calling thread.  Entry points
+ * that reduce over the grid need a workspace of waam_workspace_bytes(n)
+ * bytes (device memory, 256-byte aligned), which the caller allocates once.
+ */
+#ifndef WAAM_B200_H
+#define WAAM_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define WAAM_OK 0
+#define WAAM_ERR_INVALID -1   /* bad argument (null pointer, size, workspace) */
+#define WAAM_ERR_CUDA -2      /* CUDA launch / runtime error */
+#define WAAM_ERR_DEVICE -3    /* a kernel reported a failed device-side check */
+
+const char* waam_last_error(void);
+int waam_abi_version(void);
+/* Bytes of device workspace needed by the reducing entry points for a grid
+ * of n cells (a field-sized snapshot plus block partial sums). */
+size_t waam_workspace_bytes(int64_t n);
+
+/* ---- operator API: one entry per reference Taichi kernel ---------------- */
+
+/* kernels.py:62-120 init_grid (called by WAAMTwin.reset, twin.py:486-531) */
+int waam_init_grid(float* f, float* rho, float* ux, float* uy, float* uz, float* T, float* H,
+                   float* f_l, float* phi, int32_t* flags, int nx, int ny, int nz, float T_amb,
+                   float rho0, float cp_rho, int nz_solid, int pi0, int pi1, int pj0, int pj1,
+                   void* stream);
+/* kernels.py:161-170 clear_forces (physics/forces.py:104) */
+int waam_clear_forces(float* Fx, float* Fy, float* Fz, int64_t n, void* stream);
+/* kernels.py:443-510 inject_arc_heat (physics/arc.py:63-72 Gaussian2D, 128-137 conical).
+ * Writes the weight sum to norm_buf (device float, grid.py:163 arc_norm_buf). */
+int waam_inject_arc_heat(float* H, const int32_t* flags, const float* f_l, float* norm_buf,
+                         int nx, int ny, int nz, float arc_i, float arc_j, float arc_k, float Q_w,
+                         float sigma, float dt, float dx3, float eta, float pen, int enable,
+                         void* workspace, size_t workspace_bytes, void* stream);
+/* kernels.py:548-622 inject_goldak_heat (physics/arc.py:106-119 Goldak3D) */
+int waam_inject_goldak_heat(float* H, const int32_t* flags, const float* f_l, float* norm_buf,
+                            int nx, int ny, int nz, float arc_i, float arc_j, float arc_k,
+                            float Q_w, float dt, float dx3, float eta, float sign, float ff,
+                            float fr, float a_f, float a_r, float b, float c, float pen,
+                            int enable, void* workspace, size_t workspace_bytes, void* stream);
+/* kernels.py:1953-1984 clamp_enthalpy_ceiling_scalar (physics/thermal.py:30) */
+int waam_clamp_enthalpy_ceiling_scalar(float* H, const int32_t* flags, int64_t n, float cp_rho,
+                                       float Ts, float Tl, float T_cap, float L_rho, void* stream);
+/* kernels.py:1611-1682 advect_diffuse_temperature (physics/thermal.py:16); neighbour
+ * reads see H from before the call (snapshot kept in the workspace). */
+int waam_advect_diffuse_temperature(float* H, const float* T, const float* ux, const float* uy,
+                                    const float* uz, const int32_t* flags, int nx, int ny, int nz,
+                                    float alpha_lu, float dt, float cp_rho, void* workspace,
+                                    size_t workspace_bytes, void* stream);
+/* kernels.py:1519-1556 update_phase (physics/phase_change.py:5) */
+int waam_update_phase(const float* H, float* T, float* f_l, int64_t n, float cp_rho,
+                      float L_rho, float Ts, float Tl, void* stream);
+/* kernels.py:3016-3032 update_T_max (physics/thermal.py:21) */
+int waam_update_T_max(const float* T, float* T_max, const int32_t* flags, int64_t n,
+                      void* stream);
+/* kernels.py:2013-2027 update_cooling_rate (physics/thermal.py:22) */
+int waam_update_cooling_rate(const float* T, float* T_prev, float* dT_dt, const int32_t* flags,
+                             int64_t n, float dt_phys, void* stream);
+/* kernels.py:2030-2082 apply_thermal_boundary_losses (physics/thermal.py:18) */
+int waam_apply_thermal_boundary_losses(float* H, const float* T, const int32_t* flags, int nx,
+                                       int ny, int nz, float T_amb, float h_conv, float eps_rad,
+                                       int conv, int rad, float dt, float dx, float sigma_sb,
+                                       void* stream);
+/* kernels.py:1937-1950 clamp_enthalpy_floor_scalar (physics/thermal.py:29) */
+int waam_clamp_enthalpy_floor_scalar(float* H, float cp_rho, const int32_t* flags, int64_t n,
+                                     float T_floor, void* stream);
+/* kernels.py:2320-2361 advect_phi (physics/free_surface.py:62) */
+int waam_advect_phi(float* phi_dst, const float* phi_src, const float* ux, const float* uy,
+                    const float* uz, const int32_t* flags, int nx, int ny, int nz, void* stream);
+/* kernels.py:2364-2391 reinitialize_phi (physics/free_surface.py:63) */
+int waam_reinitialize_phi(float* phi, const int32_t* flags, int64_t n, void* stream);
+/* kernels.py:933-991 apply_contact_angle_phi_bc (physics/free_surface.py:67); sequential
+ * in k inside a column, other columns read from the pre-call snapshot. */
+int waam_apply_contact_angle_phi_bc(float* phi, const int32_t* flags, int nx, int ny, int nz,
+                                    float theta, void* workspace, size_t workspace_bytes,
+                                    void* stream);
+/* kernels.py:2394-2419 update_flags_from_phi (physics/free_surface.py:64) */
+int waam_update_flags_from_phi(const float* phi, const float* f_l, int32_t* flags, int nx,
+                               int ny, int nz, int nz_solid, void* stream);
+/* kernels.py:3484-3504 sync_phi_liquid_fraction (physics/free_surface.py:65) */
+int waam_sync_phi_liquid_fraction(const float* phi, float* f_l, const int32_t* flags, int64_t n,
+                                  void* stream);
+/* kernels.py:858-926 compute_csf_tension (physics/forces.py:114-133) */
+int waam_compute_csf_tension(const float* phi, const int32_t* flags, float* Fx, float* Fy,
+                             float* Fz, int nx, int ny, int nz, float gamma_lu, int wetting,
+                             float theta, void* stream);
+/* kernels.py:2158-2217 compute_marangoni_force (physics/forces.py:105) */
+int waam_compute_marangoni_force(const float* T, const float* phi, const float* f_l, float* Fx,
+                                 float* Fy, float* Fz, const int32_t* flags, int nx, int ny,
+                                 int nz, float dgamma, void* stream);
+/* kernels.py:3038-3083 apply_arc_pressure (physics/forces.py:110) */
+int waam_apply_arc_pressure(float* Fz, const int32_t* flags, const float* phi, int nx, int ny,
+                            int nz, float arc_i, float arc_j, float arc_k, float sigma,
+                            float pressure, float dt, float dx, float rho_ref, void* stream);
+/* kernels.py:2756-2772 add_hydrostatic_gravity (physics/forces.py:109) */
+int waam_add_hydrostatic_gravity(float* Fz, const float* f_l, const int32_t* flags, int64_t n,
+                                 float rho_ref, float g_lu, void* stream);
+/* kernels.py:2729-2753 add_buoyancy (physics/forces.py:108) */
+int waam_add_buoyancy(const float* T, float* Fz, const float* f_l, const int32_t* flags,
+                      int64_t n, float g_lu, float beta, float T_ref, float rho_ref,
+                      void* stream);
+/* kernels.py:3286-3309 clamp_body_force_magnitude (solvers/coupled_step.py:356-362) */
+int waam_clamp_body_force_magnitude(float* Fx, float* Fy, float* Fz, const int32_t* flags,
+                                    int64_t n, float F_max, void* stream);
+/* cumulant_kernel.py:28-209 collide_mrt (physics/lbm.py:9) */
+int waam_collide_mrt(const float* f_src, float* f_dst, float* rho, float* ux, float* uy,
+                     float* uz, const float* Fx, const float* Fy, const float* Fz,
+                     const float* f_l, const int32_t* flags, int64_t n, float omega_s,
+                     float omega_b, float C_darcy, void* stream);
+/* kernels.py:2778-2885 collide_srt (physics/lbm.py:6) */
+int waam_collide_srt(const float* f_src, float* f_dst, float* rho, float* ux, float* uy,
+                     float* uz, const float* Fx, const float* Fy, const float* Fz,
+                     const float* f_l, const int32_t* flags, int64_t n, float omega,
+                     float C_darcy, void* stream);
+/* kernels.py:3312-3335 clamp_velocity_mach (solvers/coupled_step.py:398-402) */
+int waam_clamp_velocity_mach(float* ux, float* uy, float* uz, const int32_t* flags, int64_t n,
+                             float u_max, void* stream);
+/* kernels.py:2971-3010 stream (physics/lbm.py:8) */
+int waam_stream(const float* f_src, float* f_dst, const int32_t* flags, int nx, int ny, int nz,
+                void* stream);
+/* kernels.py:3261-3283 update_time_above_T (solvers/coupled_step.py:418-423) */
+int waam_update_time_above_T(const float* T, const int32_t* flags, float* t800, float* t1100,
+                             float* tsol, int64_t n, float dt, float T800, float T1100,
+                             float Tsol, void* stream);
+/* kernels.py:3338-3350 snapshot_forces (solvers/coupled_step.py:424) */
+int waam_snapshot_forces(const float* Fx, const float* Fy, const float* Fz, float* Sx, float* Sy,
+                         float* Sz, int64_t n, void* stream);
+/* kernels.py:2489-2520 remelt_hot_solid_scalar (physics/free_surface.py:69) */
+int waam_remelt_hot_solid_scalar(const float* T, float* H, float* f_l, float* phi,
+                                 int32_t* flags, int64_t n, float cp_rho, float Ts, float Tl,
+                                 float L_rho, void* stream);
+/* kernels.py:2573-2617 solidify_trailing_pool_scalar (solvers/coupled_step.py:452-457) */
+int waam_solidify_trailing_pool_scalar(float* T, float* H, float* f_l, float* phi,
+                                       int32_t* flags, float* ux, float* uy, float* uz, int nx,
+                                       int ny, int nz, float cp_rho, float arc_i, float arc_j,
+                                       float arc_k, float dir_x, float dir_y, float dir_z,
+                                       float lookback, float T_freeze, float Ts, void* stream);
+/* kernels.py:2422-2450 solidify_cooled_metal (physics/free_surface.py:73-91) */
+int waam_solidify_cooled_metal(const float* T, float* f_l, float* phi, int32_t* flags,
+                               float* ux, float* uy, float* uz, int64_t n, float Ts,
+                               int zero_velocity, void* stream);
+/* kernels.py:625-641 surface_height_at (physics/free_surface.py:66); writes the
+ * height to out (device float, grid.py:160 surface_k_buf). */
+int waam_surface_height_at(const float* phi, const int32_t* flags, float* out, int nx, int ny,
+                           int nz, int i0, int j0, int nz_fallback, void* stream);
+/* kernels.py:278-400 feed_wire_surface (physics/deposition.py:247); serial
+ * lexicographic budget order; vol_acc / real_acc are device floats
+ * (grid.py:161-162 deposit_vol_buf / deposit_real_buf). */
+int waam_feed_wire_surface(float* f_src, int32_t* flags, float* f_l, float* phi, float* H,
+                           float* T, float* rho, int nx, int ny, int nz, float arc_i, float arc_j,
+                           float arc_k, float foot_r, float drop_r, float target_vol,
+                           float T_drop, float cp_rho, float L_rho, float rho0, float* vol_acc,
+                           float* real_acc, float cell_vol, void* stream);
+/* kernels.py:1176-1233 feed_wire_momentum_impact (physics/weld_forces.py:534-542) */
+int waam_feed_wire_momentum_impact(float* f_src, const float* rho, float* ux, float* uy,
+                                   float* uz, const int32_t* flags, const float* f_l, int nx,
+                                   int ny, int nz, float arc_i, float arc_j, float arc_k,
+                                   float drop_r, float vx, float vy, float vz, void* stream);
+/* kernels.py:1142-1173 apply_droplet_impact_pressure (physics/weld_forces.py:543-550) */
+int waam_apply_droplet_impact_pressure(float* Fz, const int32_t* flags, const float* phi,
+                                       const float* f_l, int nx, int ny, int nz, float arc_i,
+                                       float arc_j, float arc_k, float drop_r, float impact_pa,
+                                       float dt, float dx, float rho_ref, void* stream);
+
+/* ---- fused step: the B200 pipeline of solvers/coupled_step.py:73-464 ----- */
+
+typedef struct WaamFields {
+    float* f_src;   /* populations read by this step's collide (grid.f_src) */
+    float* f_dst;   /* populations written by collide, streamed back into f_src */
+    float* rho;
+    float* ux;
+    float* uy;
+    float* uz;
+    float* T;       /* temperature at step start ... */
+    float* T_next;  /* ... and after the step (buffers swap on the host) */
+    float* H;
+    float* H_next;
+    float* f_l;
+    float* phi;
+    float* phi_tmp;
+    int32_t* flags;
+    float* T_max;
+    float* T_prev;
+    float* dT_dt;
+    float* t800;
+    float* t1100;
+    float* tsol;
+    float* Fx;      /* body force of the step (== the reference's F_snap) */
+    float* Fy;
+    float* Fz;
+    float* step_scalars; /* device float[16]: [0] arc k, [1] weight sum, [2] energy/weight,
+                            [4], [5] torch position (arc_i, arc_j) in cells -- written by
+                            the caller before waam_step_pre (a 2-float H2D copy per step) */
+    int nx, ny, nz;
+} WaamFields;
+
+typedef struct WaamStepParams {
+    /* torch position (solvers/coupled_step.py:92-94); the kernels read it from
+     * step_scalars[4..5], these copies are informational */
+    float arc_i, arc_j;
+    int welding;
+    int nz_solid;
+    /* arc source (physics/arc.py): kind 0 Gaussian/conical, 1 Goldak */
+    int arc_kind;
+    float arc_k_offset;  /* conical source: -1.5 (physics/arc.py:132) */
+    float Q_w, eta, dt, dx, dx3, sigma_heat, sign, ff, fr, a_f, a_r, gb, gc, pen;
+    int surface_weighting;
+    /* thermal / phase (twin.py:244-274) */
+    float cp_rho, L_rho, Ts, Tl, T_cap, alpha_lu;
+    int cap_enabled;
+    int heat_loss;
+    float T_amb, h_conv, eps_rad, sigma_sb;
+    int conv, rad;
+    /* VOF */
+    int vof, wetting;
+    float theta;
+    /* forces */
+    int csf, hydro, forces_from_buffer;
+    float gamma_lu, dgamma_lu, p_sigma, pressure, rho_phys, g_lu, beta, T_ref, F_cap;
+    /* collision */
+    int collision;  /* 0 MRT, 1 SRT */
+    float omega, omega_b, C_darcy, u_cap;
+    /* diagnostics and tail */
+    float T800, T1100;
+    int substrate_growth, bead_freeze;
+    float dir_x, dir_y, dir_z, lookback, T_freeze;
+} WaamStepParams;
+
+/* Stages of one fused step.  waam_step_pre runs the surface-height query,
+ * the arc weight sum, the arc heat injection and the enthalpy cap
+ * (solvers/coupled_step.py:34-108).  The host then performs droplet
+ * deposition if one is due, and calls waam_step_main for the rest of the
+ * step (coupled_step.py:168-458). */
+int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
+                  size_t workspace_bytes, void* stream);
+int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace,
+                   size_t workspace_bytes, void* stream);
+/* waam_step_main that also records events[0..6] (cudaEvent_t handles) on the
+ * stream at the stage boundaries: before thermal, after thermal, after VOF
+ * advection, after the column pass, after collide, after stream, after the
+ * remelt/solidify tail (a skipped stage has zero duration). */
+int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* workspace,
+                          size_t workspace_bytes, void* const* events, int n_events,
+                          void* stream);
+/* Number of kernels the fused stages launch (for launch accounting). */
+int waam_step_launch_count(const WaamStepParams* p, int stage);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,332 @@
+"""CPU oracle of the whole coupled step -- TEST INFRASTRUCTURE ONLY.
+
+``OracleTwin`` restates the reference step driver
+(solvers/coupled_step.py:73-464), the twin's derived lattice scalars
+(twin.py:244-274, grid.py:93-105), its reset (twin.py:486-531) and the host
+droplet arithmetic (physics/deposition_balance.py:12-86,
+physics/weld_forces.py:61-193, physics/electrical_stickout.py:23-36) on
+numpy float32 state, calling the C oracle kernels in ``waam_oracle.c``.
+It is the CPU reference for the GPU parity tests and the CPU baseline of
+``bench.py``; the product never imports it.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import oracle as O
+
+FLUID, SOLID, GAS, IFACE = 0, 1, 2, 4
+_W = np.array([1.0 / 3.0] + [1.0 / 18.0] * 6 + [1.0 / 36.0] * 12, dtype=np.float32)
+
+
+class OracleTwin:
+    """Constants-only material, Gaussian2D / Goldak / conical arc, MRT or SRT."""
+
+    def __init__(self, nx, ny, nz, dx, mat, **kw):
+        self.nx, self.ny, self.nz, self.dx = nx, ny, nz, dx
+        self.mat = dict(mat)
+        m = self.mat
+        m.setdefault("alpha", m["k"] / (m["rho"] * m["cp"]))
+        self.cfg = dict(
+            arc_power_W=2800.0, arc_efficiency=0.8, T_ambient=300.0, use_srt=True,
+            C_darcy=1.6e5, arc_pressure_pa=500.0, droplet_freq_hz=50.0, heat_source="gaussian2d",
+            enable_vof=False, enable_csf_tension=False, enable_wetting=False,
+            enable_hydrostatic_gravity=False, enable_heat_loss=False, h_conv=25.0, eps_rad=0.3,
+            enable_convection=True, enable_radiation=False, enable_deposition_momentum=True,
+            enable_droplet_impact_pressure=True, enable_substrate_growth=False,
+            enable_bead_freeze=False, contact_angle_deg=None, deposition_superheat_K=500.0,
+            deposition_footprint_sigma_scale=1.0, welding_current_A=140.0, travel_speed_m_s=0.0,
+            enable_enthalpy_cap=True, T_vapor_cap_K=3200.0, arc_surface_weighting=True,
+            arc_penetration_mm=2.0, wire_diameter_mm=1.2, arc_sigma_mm=2.0, bulk_tau=None,
+            wire_feed_m_s=0.0, droplet_transfer_mode="auto", pulse_frequency_hz=0.0,
+            droplet_size_jitter=0.12, plate_thickness_mm=None, goldak=None,
+            impact_lead_angle_deg=0.0, trailing_solidify_lookback_mm=2.5,
+            trailing_solidify_temp_margin_K=35.0)
+        unknown = set(kw) - set(self.cfg)
+        if unknown:
+            raise KeyError("unknown OracleTwin options: %s" % sorted(unknown))
+        self.cfg.update(kw)
+        c = self.cfg
+        # grid.py:93-105
+        self.dt = dx * 0.05 / 0.5
+        nu_lu = (m["mu"] / m["rho"]) * self.dt / dx ** 2
+        self.tau = 3.0 * nu_lu + 0.5
+        # twin.py:244-274
+        self.cp_rho = m["rho"] * m["cp"]
+        self.L_rho = m["rho"] * m["L_fusion"]
+        self.alpha_lu = m["alpha"] * self.dt / dx ** 2
+        self.omega = 1.0 / self.tau
+        self.omega_bulk = 1.0 / c["bulk_tau"] if c["bulk_tau"] else self.omega
+        self.arc_sigma_m = c["arc_sigma_mm"] * 1e-3
+        self.sigma_cells = self.arc_sigma_m / dx
+        self.g_lu = 9.81 * self.dt ** 2 / dx
+        scale_F = self.dt ** 2 / (m["rho"] * dx ** 2)
+        self.dgamma_dT_lu = m["dgamma_dT"] * scale_F / dx
+        self.gamma_lu = m["gamma_0"] * scale_F / dx
+        theta = c["contact_angle_deg"] if c["contact_angle_deg"] is not None else m.get("contact_angle_deg", 80.0)
+        self.theta = math.radians(theta)
+        headroom = max(6, nz // 4)
+        max_solid = max(1, nz - headroom)
+        t = c["plate_thickness_mm"]
+        if t is not None and t > 0:
+            self.nz_solid = max(1, min(int(round(t / (dx * 1000.0))), max_solid))
+        else:
+            self.nz_solid = max(1, min(nz // 5, max_solid))
+        self.step_n = 0
+        self.last_drop = 0.0
+        self.n_drops = 0
+        self.deposited = 0.0
+        self.dir = (1.0, 0.0, 0.0)
+        self.last_pos = None
+        self.arc_k = None
+        self.s = None
+
+    # ---------------------------------------------------------------- state --
+    def reset(self):
+        nx, ny, nz = self.nx, self.ny, self.nz
+        sh = (nx, ny, nz)
+        z = lambda: np.zeros(sh, np.float32)  # noqa: E731
+        s = dict(f_a=np.zeros((19,) + sh, np.float32), f_b=np.zeros((19,) + sh, np.float32),
+                 rho=z(), ux=z(), uy=z(), uz=z(), T=z(), H=z(), f_l=z(), phi=z(), phi_tmp=z(),
+                 flags=np.zeros(sh, np.int32), T_max=z(), T_prev=z(), dT_dt=z(),
+                 time_above_800_s=z(), time_above_1100_s=z(), time_above_solidus_s=z(),
+                 Fx=z(), Fy=z(), Fz=z())
+        T0 = self.cfg["T_ambient"]
+        O.call("wo_init_grid", s["f_a"], s["rho"], s["ux"], s["uy"], s["uz"], s["T"], s["H"],
+               s["f_l"], s["phi"], s["flags"], nx, ny, nz, T0, 1.0, self.cp_rho, self.nz_solid,
+               0, nx, 0, ny)
+        s["T_max"][...] = np.float32(T0)
+        s["T_prev"][...] = np.float32(T0)
+        O.call("wo_stream", s["f_a"], s["f_b"], s["flags"], nx, ny, nz)
+        s["read_is_a"] = True
+        self.s = s
+        self.step_n = 0
+        self.last_drop = 0.0
+        self.n_drops = 0
+        self.deposited = 0.0
+
+    def load(self, st):
+        """Adopt a state dict (numpy arrays named like the reference grid)."""
+        self.s = {k: (np.ascontiguousarray(v).copy() if isinstance(v, np.ndarray) else v)
+                  for k, v in st.items()}
+        self.s.setdefault("phi_tmp", np.zeros_like(self.s["phi"]))
+        self.s.setdefault("read_is_a", True)
+
+    def fsrc(self):
+        return self.s["f_a"] if self.s["read_is_a"] else self.s["f_b"]
+
+    def fdst(self):
+        return self.s["f_b"] if self.s["read_is_a"] else self.s["f_a"]
+
+    # ------------------------------------------------------- host arithmetic --
+    def _mode(self):
+        c = self.cfg
+        mode = str(c["droplet_transfer_mode"]).lower()
+        if mode in ("globular", "spray", "pulsed"):
+            return mode
+        if c["pulse_frequency_hz"] > 0:
+            return "pulsed"
+        return "globular" if c["welding_current_A"] < 180.0 else "spray"
+
+    def _mdot(self):
+        d = self.cfg["wire_diameter_mm"] * 1e-3
+        return self.mat["rho"] * math.pi * (d * 0.5) ** 2 * self.cfg["wire_feed_m_s"]
+
+    def _period(self):
+        c = self.cfg
+        f = c["droplet_freq_hz"]
+        base = 1.0 / max(f, 1e-9) if f > 0 else 1.0 / 50.0
+        mode = self._mode()
+        if mode == "globular":
+            sc = 1.55
+        elif mode == "spray":
+            sc = 0.72
+        elif mode == "pulsed":
+            sc = max(0.25, min(4.0, (1.0 / max(c["pulse_frequency_hz"], 1e-9)) / base))
+        else:
+            sc = 1.0
+        amp = max(0.0, min(c["droplet_size_jitter"], 0.35))
+        jit = 1.0 + amp * math.sin(0.73 * float(self.n_drops + 1) + 0.31)
+        return max(base * 0.2, base * sc * jit)
+
+    def _drop_mass_nominal(self):
+        return max(0.0, self._mdot() * max(self._period(), 0.0)) if self.cfg["droplet_freq_hz"] > 0 else 0.0
+
+    def _impact_velocity(self, m):
+        c = self.cfg
+        L = 3e-3
+        if c["droplet_freq_hz"] > 0 and c["wire_feed_m_s"] > 0:
+            L = c["wire_feed_m_s"] / c["droplet_freq_hz"]
+        v_feed = max(c["wire_feed_m_s"], 0.0)
+        v_grav = math.sqrt(max(0.0, 2.0 * 9.81 * L))
+        d = max(c["wire_diameter_mm"] * 1e-3, 1e-6)
+        pinch = 0.35 * math.sqrt(max(c["welding_current_A"], 0.0) / 200.0) * math.sqrt(1.2e-3 / d)
+        sc = {"globular": 0.78, "spray": 1.18, "pulsed": 1.05}.get(self._mode(), 1.0)
+        mt = 1.0
+        if m > 0:
+            mt = max(0.8, min(1.25, math.sqrt(self._drop_mass_nominal() / m)))
+        return min(5.0, sc * max(v_feed, v_grav + pinch) * mt)
+
+    # ------------------------------------------------------------------ step --
+    def step(self, x, y, welding=True):
+        c, s, m = self.cfg, self.s, self.mat
+        nx, ny, nz = self.nx, self.ny, self.nz
+        n = nx * ny * nz
+        if self.last_pos is not None:
+            d = (x - self.last_pos[0], y - self.last_pos[1], 0.0 - self.last_pos[2])
+            nrm = math.sqrt(sum(v * v for v in d))
+            if nrm > 1e-12:
+                self.dir = tuple(v / nrm for v in d)
+        self.last_pos = (x, y, 0.0)
+        arc_i, arc_j = x / self.dx, y / self.dx
+        i0 = max(0, min(int(arc_i), nx - 1))
+        j0 = max(0, min(int(arc_j), ny - 1))
+        k = float(O.call("wo_surface_height_at", s["phi"], s["flags"], nx, ny, nz, i0, j0,
+                         self.nz_solid))
+        if k < 1.0:
+            k = float(max(1, self.nz_solid - 1))
+        arc_k = self.arc_k = k
+        Ts, Tl = m["T_solidus"], m["T_liquidus"]
+        O.call("wo_clear_forces", s["Fx"], s["Fy"], s["Fz"], n)
+        pen = c["arc_penetration_mm"] * 1e-3 / self.dx
+        en = 1 if c["arc_surface_weighting"] else 0
+        cap = c["enable_enthalpy_cap"]
+        if welding:
+            hs = str(c["heat_source"]).lower().replace("-", "").replace("_", "")
+            if hs in ("goldak", "goldak3d", "doubleellipsoid"):
+                g = c["goldak"]
+                sign = 1.0 if c["travel_speed_m_s"] >= 0.0 else -1.0
+                O.call("wo_inject_goldak_heat", s["H"], s["flags"], s["f_l"], nx, ny, nz, arc_i,
+                       arc_j, arc_k, c["arc_power_W"], self.dt, self.dx ** 3,
+                       c["arc_efficiency"], sign, g["ff"], g["fr"], g["a_front"], g["a_rear"],
+                       g["b"], g["c"], pen, en)
+            elif hs in ("conical", "conicalvolume", "cone"):
+                O.call("wo_inject_arc_heat", s["H"], s["flags"], s["f_l"], nx, ny, nz, arc_i,
+                       arc_j, arc_k - 1.5, c["arc_power_W"], self.sigma_cells * 1.2, self.dt,
+                       self.dx ** 3, c["arc_efficiency"], pen, en)
+            else:
+                O.call("wo_inject_arc_heat", s["H"], s["flags"], s["f_l"], nx, ny, nz, arc_i,
+                       arc_j, arc_k, c["arc_power_W"], self.sigma_cells, self.dt, self.dx ** 3,
+                       c["arc_efficiency"], pen, en)
+            if cap:
+                O.call("wo_clamp_enthalpy_ceiling_scalar", s["H"], s["flags"], n, self.cp_rho,
+                       Ts, Tl, c["T_vapor_cap_K"], self.L_rho)
+            self._maybe_droplet(arc_i, arc_j, arc_k)
+        O.call("wo_advect_diffuse_temperature", s["H"], s["T"], s["ux"], s["uy"], s["uz"],
+               s["flags"], nx, ny, nz, self.alpha_lu, 1.0, self.cp_rho)
+        if c["enable_heat_loss"]:
+            O.call("wo_apply_thermal_boundary_losses", s["H"], s["T"], s["flags"], nx, ny, nz,
+                   c["T_ambient"], c["h_conv"], c["eps_rad"], int(c["enable_convection"]),
+                   int(c["enable_radiation"]), self.dt, self.dx, 5.670374419e-8)
+            O.call("wo_clamp_enthalpy_floor_scalar", s["H"], self.cp_rho, s["flags"], n,
+                   c["T_ambient"])
+        O.call("wo_update_phase", s["H"], s["T"], s["f_l"], n, self.cp_rho, self.L_rho, Ts, Tl)
+        if cap:
+            O.call("wo_clamp_enthalpy_ceiling_scalar", s["H"], s["flags"], n, self.cp_rho, Ts,
+                   Tl, c["T_vapor_cap_K"], self.L_rho)
+        O.call("wo_update_phase", s["H"], s["T"], s["f_l"], n, self.cp_rho, self.L_rho, Ts, Tl)
+        O.call("wo_update_T_max", s["T"], s["T_max"], s["flags"], n)
+        O.call("wo_update_cooling_rate", s["T"], s["T_prev"], s["dT_dt"], s["flags"], n, self.dt)
+        if c["enable_vof"]:
+            O.call("wo_advect_phi", s["phi_tmp"], s["phi"], s["ux"], s["uy"], s["uz"],
+                   s["flags"], nx, ny, nz)
+            s["phi"][...] = s["phi_tmp"]
+            O.call("wo_reinitialize_phi", s["phi"], s["flags"], n)
+            if c["enable_wetting"]:
+                O.call("wo_apply_contact_angle_phi_bc", s["phi"], s["flags"], nx, ny, nz,
+                       self.theta)
+            O.call("wo_update_flags_from_phi", s["phi"], s["f_l"], s["flags"], nx, ny, nz,
+                   self.nz_solid)
+            O.call("wo_sync_phi_liquid_fraction", s["phi"], s["f_l"], s["flags"], n)
+        if c["enable_csf_tension"]:
+            O.call("wo_compute_csf_tension", s["phi"], s["flags"], s["Fx"], s["Fy"], s["Fz"], nx,
+                   ny, nz, self.gamma_lu, int(c["enable_wetting"]), self.theta)
+        O.call("wo_compute_marangoni_force", s["T"], s["phi"], s["f_l"], s["Fx"], s["Fy"],
+               s["Fz"], s["flags"], nx, ny, nz, self.dgamma_dT_lu)
+        if welding:
+            O.call("wo_apply_arc_pressure", s["Fz"], s["flags"], s["phi"], nx, ny, nz, arc_i,
+                   arc_j, arc_k, self.arc_sigma_m / self.dx, c["arc_pressure_pa"], self.dt,
+                   self.dx, m["rho"])
+        if c["enable_hydrostatic_gravity"]:
+            O.call("wo_add_hydrostatic_gravity", s["Fz"], s["f_l"], s["flags"], n, 1.0, self.g_lu)
+        O.call("wo_add_buoyancy", s["T"], s["Fz"], s["f_l"], s["flags"], n, self.g_lu,
+               m["beta_T"], Tl, 1.0)
+        O.call("wo_clamp_body_force_magnitude", s["Fx"], s["Fy"], s["Fz"], s["flags"], n, 0.05)
+        if c["use_srt"]:
+            O.call("wo_collide_srt", self.fsrc(), self.fdst(), s["rho"], s["ux"], s["uy"],
+                   s["uz"], s["Fx"], s["Fy"], s["Fz"], s["f_l"], s["flags"], n, self.omega,
+                   c["C_darcy"])
+        else:
+            O.call("wo_collide_mrt", self.fsrc(), self.fdst(), s["rho"], s["ux"], s["uy"],
+                   s["uz"], s["Fx"], s["Fy"], s["Fz"], s["f_l"], s["flags"], n, self.omega,
+                   self.omega_bulk, c["C_darcy"])
+        O.call("wo_clamp_velocity_mach", s["ux"], s["uy"], s["uz"], s["flags"], n, 0.08)
+        O.call("wo_stream", self.fdst(), self.fsrc(), s["flags"], nx, ny, nz)
+        O.call("wo_update_time_above_T", s["T"], s["flags"], s["time_above_800_s"],
+               s["time_above_1100_s"], s["time_above_solidus_s"], n, self.dt, 800.0 + 273.15,
+               1100.0 + 273.15, Ts)
+        if c["enable_substrate_growth"] or c["enable_bead_freeze"]:
+            O.call("wo_remelt_hot_solid_scalar", s["T"], s["H"], s["f_l"], s["phi"], s["flags"],
+                   n, self.cp_rho, Ts, Tl, self.L_rho)
+            if welding and c["enable_bead_freeze"]:
+                lb = max(2.0, c["trailing_solidify_lookback_mm"] / (self.dx * 1000.0))
+                O.call("wo_solidify_trailing_pool_scalar", s["T"], s["H"], s["f_l"], s["phi"],
+                       s["flags"], s["ux"], s["uy"], s["uz"], nx, ny, nz, self.cp_rho, arc_i,
+                       arc_j, arc_k, self.dir[0], self.dir[1], self.dir[2], lb,
+                       Tl + c["trailing_solidify_temp_margin_K"], Ts)
+            O.call("wo_solidify_cooled_metal", s["T"], s["f_l"], s["phi"], s["flags"], s["ux"],
+                   s["uy"], s["uz"], n, Ts, 1)
+        s["read_is_a"] = not s["read_is_a"]
+        self.step_n += 1
+
+    def _maybe_droplet(self, arc_i, arc_j, arc_k):
+        c, s, m = self.cfg, self.s, self.mat
+        if c["droplet_freq_hz"] <= 0:
+            return
+        t = self.step_n * self.dt
+        if t - self.last_drop < self._period():
+            return
+        drop_dt = t - self.last_drop
+        self.last_drop = t
+        mass = max(0.0, self._mdot() * max(drop_dt, 0.0))
+        if mass <= 0:
+            r = 3.0
+        else:
+            cells = mass / m["rho"] / self.dx ** 3
+            r = max(1.0, min((3.0 * cells / (4.0 * math.pi)) ** (1.0 / 3.0), 10.0))
+        vol = mass / m["rho"]
+        T_drop = m["T_liquidus"] + c["deposition_superheat_K"]
+        r_try = max(r, self.sigma_cells * c["deposition_footprint_sigma_scale"])
+        placed = 0.0
+        nx, ny, nz = self.nx, self.ny, self.nz
+        for _ in range(10):
+            va = np.array([placed], np.float32)
+            ra = np.array([placed], np.float32)
+            O.call("wo_feed_wire_surface", self.fsrc(), s["flags"], s["f_l"], s["phi"], s["H"],
+                   s["T"], s["rho"], nx, ny, nz, arc_i, arc_j, arc_k, r_try, r, vol, T_drop,
+                   self.cp_rho, self.L_rho, 1.0, va, ra, self.dx ** 3)
+            placed = float(ra[0])
+            if placed >= vol * 0.98:
+                break
+            r_try = min(r_try + 1.5, 16.0)
+        self.deposited += placed
+        self.n_drops += 1
+        if c["enable_deposition_momentum"]:
+            v = self._impact_velocity(mass)
+            lead = math.radians(c["impact_lead_angle_deg"])
+            dxy = math.hypot(self.dir[0], self.dir[1])
+            ddx, ddy = (self.dir[0] / dxy, self.dir[1] / dxy) if dxy >= 1e-9 else (1.0, 0.0)
+            v_xy = min(v * 0.65, max(c["travel_speed_m_s"], abs(v) * math.tan(lead)))
+            v_z = -math.sqrt(max(v * v - v_xy * v_xy, v * v * 0.2))
+            k = self.dt / self.dx
+            O.call("wo_feed_wire_momentum_impact", self.fsrc(), s["rho"], s["ux"], s["uy"],
+                   s["uz"], s["flags"], s["f_l"], nx, ny, nz, arc_i, arc_j, arc_k, r,
+                   v_xy * ddx * k, v_xy * ddy * k, v_z * k)
+            if c["enable_droplet_impact_pressure"]:
+                rm = r * self.dx
+                pa = 0.5 * mass * v * v / max(math.pi * rm * rm, 1e-12) if mass > 0 else 0.0
+                O.call("wo_apply_droplet_impact_pressure", s["Fz"], s["flags"], s["phi"],
+                       s["f_l"], nx, ny, nz, arc_i, arc_j, arc_k, r, pa, self.dt, self.dx,
+                       m["rho"])

@@ -8,6 +8,9 @@
  * (OpenMP) are used only where every cell writes only itself.
  */
 #include "waam_oracle.h"
+/* The same float exponential the CUDA kernels use (Cody-Waite + Taylor), so
+ * that exp rounding does not blur the oracle/GPU comparison. */
+#include "../waam_solver_b200/csrc/waam_expf.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -34,6 +37,11 @@ static inline int imin(int a, int b) { return a < b ? a : b; }
 static inline int imax(int a, int b) { return a > b ? a : b; }
 static inline float fminf_(float a, float b) { return a < b ? a : b; }
 static inline float fmaxf_(float a, float b) { return a > b ? a : b; }
+
+/* Exposes the shared exponential for accuracy tests. */
+void wo_expf_array(const float* x, float* y, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) y[i] = waam_expf(x[i]);
+}
 
 int wo_num_threads(void) {
 #ifdef _OPENMP
@@ -104,7 +112,7 @@ static float arc_weight(int k, float arc_k, float fl, float pen, int enable) {
             } else {
                 float depth = fmaxf_(0.0f, dz);
                 float inv_pen = 1.0f / (pen + 1e-6f);
-                w = expf(-depth * inv_pen);
+                w = waam_expf(-depth * inv_pen);
             }
         }
     }
@@ -129,7 +137,7 @@ double wo_inject_arc_heat(float* H, const int32_t* flags, const float* f_l, int 
                 if (wd < 1e-6f) continue;
                 float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - arc_k;
                 float r2 = di * di + dj * dj + dk * dk * 0.25f;
-                acc += (double)(expf(-r2 * inv2s2) * wd);
+                acc += (double)(waam_expf(-r2 * inv2s2) * wd);
             }
     float w_total = (float)acc;
     float epw = 0.0f;
@@ -145,7 +153,7 @@ double wo_inject_arc_heat(float* H, const int32_t* flags, const float* f_l, int 
                 if (wd < 1e-6f) continue;
                 float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - arc_k;
                 float r2 = di * di + dj * dj + dk * dk * 0.25f;
-                H[c] += epw * expf(-r2 * inv2s2) * wd;
+                H[c] += epw * waam_expf(-r2 * inv2s2) * wd;
             }
     return acc;
 }
@@ -158,7 +166,7 @@ static float goldak_w(float di, float dj, float dk, float sign, float ff, float 
     int front = xt >= 0.0f;
     float a = front ? a_f : a_r;
     float frac = front ? ff : fr;
-    return frac * expf(-3.0f * ((xt * xt) / (a * a + eps) + (dj * dj) / (b * b + eps) +
+    return frac * waam_expf(-3.0f * ((xt * xt) / (a * a + eps) + (dj * dj) / (b * b + eps) +
                                 (dk * dk) / (c * c + eps)));
 }
 
@@ -449,7 +457,7 @@ void wo_apply_contact_angle_phi_bc(float* phi, const int32_t* flags, int nx, int
     int64_t n = (int64_t)nx * ny * nz;
     float* P0 = (float*)malloc(n * sizeof(float));
     memcpy(P0, phi, n * sizeof(float));
-    float cos_t = cosf(theta), sin_t = sinf(theta);
+    float cos_t = (float)cos((double)theta), sin_t = (float)sin((double)theta);
     float film = 0.5f * (1.0f - cos_t);
     float spread = film * (0.85f + 0.15f * sin_t);
 #pragma omp parallel for collapse(2)
@@ -550,7 +558,7 @@ void wo_compute_csf_tension(const float* phi, const int32_t* flags, float* Fx, f
                             float* Fz, int nx, int ny, int nz, float gamma_lu, int wetting,
                             float theta) {
     const float eps = 1e-6f;
-    float cos_t = cosf(theta), sin_t = sinf(theta);
+    float cos_t = (float)cos((double)theta), sin_t = (float)sin((double)theta);
 #pragma omp parallel for collapse(2)
     for (int i = 0; i < nx; ++i)
         for (int j = 0; j < ny; ++j)
@@ -688,7 +696,7 @@ void wo_apply_arc_pressure(float* Fz, const int32_t* flags, const float* phi, in
                 if (fabsf(dpz) > 0.05f) {
                     float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - arc_k;
                     float r2 = di * di + dj * dj + dk * dk * 0.1f;
-                    Fz[c] += -Flu * expf(-r2 * inv2s2);
+                    Fz[c] += -Flu * waam_expf(-r2 * inv2s2);
                 }
             }
 }
@@ -1136,7 +1144,7 @@ void wo_apply_droplet_impact_pressure(float* Fz, const int32_t* flags, const flo
                 float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - arc_k;
                 float r2 = di * di + dj * dj + dk * dk;
                 if (r2 > drop_r * drop_r * 4.0f) continue;
-                Fz[c] += -Flu * expf(-r2 * inv2s2);
+                Fz[c] += -Flu * waam_expf(-r2 * inv2s2);
             }
 }
 
@@ -1173,7 +1181,7 @@ void wo_elec_inject_arc_source(float* src, int nx, int ny, int nz, float arc_i, 
                 if (k < kmin || k > kmax) continue;
                 float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - arc_k;
                 float r2 = di * di + dj * dj + 0.25f * dk * dk;
-                float wgt = expf(-r2 * inv2s2);
+                float wgt = waam_expf(-r2 * inv2s2);
                 src[c] = current * wgt / (cell_vol + eps);
             }
 }

@@ -26,6 +26,7 @@ extern "C" {
 #endif
 
 int wo_num_threads(void);
+void wo_expf_array(const float* x, float* y, int64_t n);
 void wo_set_num_threads(int n);
 
 void wo_init_grid(float* f, float* rho, float* ux, float* uy, float* uz, float* T, float* H,

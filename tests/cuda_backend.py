@@ -1,0 +1,81 @@
+"""Kernel-case backend over the native C ABI (GPU tests only).
+
+Every call copies the numpy arguments to fresh CUDA tensors, calls the
+``waam_*`` entry point through ctypes exactly as an FFI user would, and
+copies the results back into the numpy arrays (in place), so the golden
+cases in ``cases.py`` run unchanged against the CUDA kernels.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from waam_solver_b200 import _native
+
+_WS_FUNCS = {"inject_arc_heat", "inject_goldak_heat", "advect_diffuse_temperature",
+             "apply_contact_angle_phi_bc"}
+_NORM_FUNCS = {"inject_arc_heat", "inject_goldak_heat"}
+
+
+class CudaBackend:
+    def __init__(self, device="cuda"):
+        self.device = torch.device(device)
+        self.launched = []
+
+    def _up(self, a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+
+    def _run(self, name, args, n_cells):
+        dev_args, back = [], []
+        for a in args:
+            if isinstance(a, np.ndarray):
+                t = self._up(a)
+                dev_args.append(t.data_ptr())
+                back.append((a, t))
+            else:
+                dev_args.append(a)
+        extra_tail = []
+        norm = None
+        if name in _NORM_FUNCS:
+            norm = torch.zeros((), dtype=torch.float32, device=self.device)
+            dev_args.insert(3, norm.data_ptr())
+        if name in _WS_FUNCS:
+            nbytes = int(_native.lib().waam_workspace_bytes(n_cells))
+            ws = torch.zeros(nbytes, dtype=torch.uint8, device=self.device)
+            extra_tail = [ws.data_ptr(), nbytes]
+        stream = torch.cuda.current_stream().cuda_stream
+        _native.call("waam_" + name, *(dev_args + extra_tail + [stream]))
+        torch.cuda.synchronize()
+        self.launched.append(name)
+        for host, t in back:
+            host[...] = t.cpu().numpy()
+        return None if norm is None else float(norm.item())
+
+    def __getattr__(self, name):
+        if name.startswith("_"):
+            raise AttributeError(name)
+
+        def f(*args):
+            n_cells = None
+            for a in args:
+                if isinstance(a, np.ndarray) and a.ndim == 3:
+                    n_cells = a.size
+                    break
+            return self._run(name, list(args), n_cells)
+        return f
+
+    def surface_height_at(self, phi, flags, nx, ny, nz, i0, j0, nz_fallback):
+        out = torch.zeros((), dtype=torch.float32, device=self.device)
+        tp, tf = self._up(phi), self._up(flags)
+        _native.call("waam_surface_height_at", tp.data_ptr(), tf.data_ptr(), out.data_ptr(), nx,
+                     ny, nz, i0, j0, nz_fallback, torch.cuda.current_stream().cuda_stream)
+        return float(out.item())
+
+    def feed_wire_surface(self, *args):
+        args = list(args)
+        vol = np.array([args[20]], dtype=np.float32).reshape(())
+        real = np.array([args[21]], dtype=np.float32).reshape(())
+        va, ra = np.array(vol).reshape(1), np.array(real).reshape(1)
+        args[20], args[21] = va, ra
+        self._run("feed_wire_surface", args, None)
+        return float(va[0]), float(ra[0])

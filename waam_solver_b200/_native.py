@@ -1,0 +1,111 @@
+"""Loader of the native library ``_lib/libwaam_b200.so``.
+
+The ctypes signatures are derived from the C header ``include/waam_b200.h``
+(the single definition of the ABI), so the Python host and any other FFI
+binding read the same declarations.  The product path has no fallback: if
+the library is missing or fails to load, every operator raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+HEADER = os.path.join(ROOT, "include", "waam_b200.h")
+LIB_PATH = os.path.join(HERE, "_lib", "libwaam_b200.so")
+
+
+class WaamError(RuntimeError):
+    """A native entry point returned a non-zero status."""
+
+
+class WaamFields(C.Structure):
+    _fields_ = [(name, C.c_void_p) for name in (
+        "f_src", "f_dst", "rho", "ux", "uy", "uz", "T", "T_next", "H", "H_next", "f_l", "phi",
+        "phi_tmp", "flags", "T_max", "T_prev", "dT_dt", "t800", "t1100", "tsol", "Fx", "Fy",
+        "Fz", "step_scalars")] + [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int)]
+
+
+def _params_fields():
+    """Field list of WaamStepParams, parsed from the header."""
+    src = open(HEADER).read()
+    body = re.search(r"typedef struct WaamStepParams \{(.*?)\} WaamStepParams;", src, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    out = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        typ, names = decl.split(None, 1)
+        ctype = {"int": C.c_int, "float": C.c_float}[typ]
+        for nm in names.split(","):
+            out.append((nm.strip(), ctype))
+    return out
+
+
+class WaamStepParams(C.Structure):
+    _fields_ = _params_fields()
+
+
+_CTYPES = {
+    "float*": C.c_void_p, "const float*": C.c_void_p, "int32_t*": C.c_void_p,
+    "const int32_t*": C.c_void_p, "void*": C.c_void_p, "float": C.c_float, "int": C.c_int,
+    "int64_t": C.c_int64, "size_t": C.c_size_t, "const WaamFields*": C.POINTER(WaamFields),
+    "const WaamStepParams*": C.POINTER(WaamStepParams), "const char*": C.c_char_p,
+    "void* const*": C.c_void_p,
+}
+
+
+def parse_header(path: str = HEADER):
+    """Return {function name: (restype, [argtypes])} for every declaration."""
+    src = open(path).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"typedef struct \w+ \{.*?\} \w+;", "", src, flags=re.S)
+    decls = {}
+    for m in re.finditer(r"(const char\*|int|size_t)\s+(waam_\w+)\s*\(([^)]*)\)\s*;", src):
+        ret, name, args = m.group(1), m.group(2), m.group(3)
+        types = []
+        args = args.strip()
+        if args and args != "void":
+            for a in args.split(","):
+                a = " ".join(a.split())
+                typ = a.rsplit(" ", 1)[0].replace(" *", "*")
+                types.append(_CTYPES[typ])
+        decls[name] = (_CTYPES[ret] if ret != "int" else C.c_int, types)
+    return decls
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """Load the native library (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise WaamError(
+                    "native library %s is missing; build it with "
+                    "`python -m waam_solver_b200.build`" % LIB_PATH)
+            L = C.CDLL(LIB_PATH)
+            for name, (res, args) in parse_header().items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+    return _lib
+
+
+def call(name: str, *args) -> int:
+    """Call entry point ``name``; raise WaamError on a non-zero status."""
+    rc = getattr(lib(), name)(*args)
+    if rc != 0:
+        msg = lib().waam_last_error().decode(errors="replace")
+        raise WaamError("%s failed (%d): %s" % (name, rc, msg))
+    return rc

@@ -1,0 +1,367 @@
+"""One coupled physics timestep (reference solvers/coupled_step.py:73-464).
+
+Two drivers produce the same state:
+
+* ``coupled_step_operators`` calls the operator API one kernel at a time in
+  the reference's order -- the drop-in path for callers that interleave
+  their own operators;
+* ``coupled_step_fused`` runs the B200 pipeline of ``waam_step_pre`` /
+  ``waam_step_main`` (about eight kernels per step, no host synchronisation
+  except on droplet steps, where the deposition budget is read back exactly
+  as the reference does).
+
+``coupled_step`` dispatches on ``twin.step_mode`` ("fused" by default).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _native, kernels
+from .physics import deposition, forces, free_surface, lbm, phase_change, thermal, weld_forces
+from .physics.electrical_stickout import droplet_entry_temperature_K
+
+T_800 = 800.0 + 273.15
+T_1100 = 1100.0 + 273.15
+
+
+def _clamp_ceiling(twin, g):
+    if twin.enable_enthalpy_cap:
+        thermal.clamp_enthalpy_ceiling_scalar(g.H, g.flags, twin.cp_rho, twin.mat.T_solidus,
+                                              twin.mat.T_liquidus, twin.T_vapor_cap_K, twin.L_rho,
+                                              g.FLAG_GAS)
+
+
+def _resolve_arc_k(twin, g, arc_i, arc_j, torch_z_m=None):
+    """solvers/coupled_step.py:34-59 (host read of the surface height)."""
+    i0 = max(0, min(int(arc_i), g.nx - 1))
+    j0 = max(0, min(int(arc_j), g.ny - 1))
+    free_surface.surface_height_at(g.phi, g.flags, g.surface_k_buf, i0, j0, twin.nz_solid,
+                                   g.FLAG_GAS, g.nz)
+    k = float(g.surface_k_buf.item())
+    if k < 1.0:
+        k = float(max(1, twin.nz_solid - 1))
+    return _robot_z(twin, g, k, torch_z_m)
+
+
+def _robot_z(twin, g, k_surface, torch_z_m):
+    if getattr(twin, "use_torch_z", False) and torch_z_m is not None:
+        z_bead = max(twin.substrate_z_m, torch_z_m - twin.ctwd_m)
+        k_robot = twin.nz_solid + (z_bead - twin.substrate_z_m) / g.dx - 1.0
+        k_robot = max(float(twin.nz_solid) + 0.5, min(k_robot, float(g.nz) - 2.0))
+        return max(k_surface, k_robot)
+    return k_surface
+
+
+def _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m):
+    """Droplet schedule and deposition (solvers/coupled_step.py:110-166).
+
+    Returns True when a droplet fired this step."""
+    if twin.droplet_freq <= 0:
+        return False
+    sim_time = twin._step_n * g.dt
+    period = deposition.droplet_period_s(twin)
+    if sim_time - twin._last_droplet_time < period:
+        return False
+    drop_dt = sim_time - twin._last_droplet_time
+    twin._last_droplet_time = sim_time
+    drop_mass = deposition.droplet_mass_for_interval_kg(twin, drop_dt)
+    drop_r = deposition.droplet_radius_cells_from_mass_kg(twin, drop_mass)
+    drop_vol = drop_mass / twin.mat.rho
+    T_drop = droplet_entry_temperature_K(twin)
+    r_try = deposition.deposition_footprint_cells(twin, drop_r)
+    placed_real = 0.0
+    for _ in range(10):
+        g.deposit_vol_buf.fill_(placed_real)
+        g.deposit_real_buf.fill_(placed_real)
+        deposition.feed_wire_surface(
+            g.f_src, g.flags, g.f_l, g.phi, g.H, g.T, g.rho, arc_i, arc_j, arc_k, r_try, drop_r,
+            drop_vol, T_drop, twin.cp_rho, twin.L_rho, 1.0, g.deposit_vol_buf,
+            g.deposit_real_buf, g.dx ** 3, g.FLAG_GAS, g.FLAG_FLUID, g.FLAG_SOLID, g.nx, g.ny,
+            g.nz)
+        placed_real = float(g.deposit_real_buf.item())
+        if placed_real >= drop_vol * 0.98:
+            break
+        r_try = min(r_try + 1.5, 16.0)
+    if placed_real < drop_vol * 0.98:
+        twin._deposition_overflow += 1
+    twin._deposited_volume_m3 += placed_real
+    twin._n_droplets_fired += 1
+    weld_forces.apply_droplet_impact(twin, g, arc_i, arc_j, arc_k, drop_r, drop_mass)
+    return True
+
+
+def coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
+    """The reference step, operator by operator (scalar-material path)."""
+    g = twin.grid
+    arc_i = torch_x_m / g.dx
+    arc_j = torch_y_m / g.dx
+    arc_k = _resolve_arc_k(twin, g, arc_i, arc_j, torch_z_m)
+    twin._last_arc_ijk = (float(arc_i), float(arc_j), float(arc_k))
+    forces.clear_forces(g.Fx, g.Fy, g.Fz)
+    pressure = weld_forces.arc_pressure_peak_pa(twin)
+    p_sigma = weld_forces.arc_pressure_sigma_cells(twin)
+    if is_welding:
+        twin.arc_source.inject(twin, g, arc_i, arc_j, arc_k)
+        _clamp_ceiling(twin, g)
+        _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m)
+    thermal.advect_diffuse_temperature(g.H, g.T, g.ux, g.uy, g.uz, g.flags, twin.alpha_lu, 1.0,
+                                       g.FLAG_SOLID, g.FLAG_GAS, twin.cp_rho, g.nx, g.ny, g.nz)
+    if twin.enable_heat_loss:
+        thermal.apply_boundary_losses(g.H, g.T, g.flags, twin.T_amb, twin.h_conv, twin.eps_rad,
+                                      int(twin.enable_convection), int(twin.enable_radiation),
+                                      twin.cp_rho, g.dt, g.dx, twin.sigma_sb, g.FLAG_SOLID,
+                                      g.FLAG_GAS, g.nx, g.ny, g.nz)
+        thermal.clamp_enthalpy_floor_scalar(g.H, twin.cp_rho, g.flags, twin.T_amb, g.FLAG_GAS)
+    phase_change.update_phase(g.H, g.T, g.f_l, twin.cp_rho, twin.L_rho, twin.mat.T_solidus,
+                              twin.mat.T_liquidus)
+    _clamp_ceiling(twin, g)
+    phase_change.update_phase(g.H, g.T, g.f_l, twin.cp_rho, twin.L_rho, twin.mat.T_solidus,
+                              twin.mat.T_liquidus)
+    thermal.update_T_max(g.T, g.T_max, g.flags, g.FLAG_GAS)
+    thermal.update_cooling_rate(g.T, g.T_prev, g.dT_dt, g.flags, g.dt, g.FLAG_GAS)
+    if twin.enable_vof:
+        g.ensure_vof_buffers()
+        free_surface.advect_phi(g.phi_tmp, g.phi, g.ux, g.uy, g.uz, g.flags, g.FLAG_SOLID,
+                                g.FLAG_GAS, g.nx, g.ny, g.nz)
+        g.phi.copy_(g.phi_tmp)
+        free_surface.reinitialize_phi(g.phi, g.flags, g.FLAG_SOLID, g.FLAG_GAS, g.FLAG_FLUID)
+        if twin.enable_wetting:
+            free_surface.apply_contact_angle_phi_bc(g.phi, g.flags, twin.theta_rad, g.FLAG_SOLID,
+                                                    g.FLAG_GAS, g.nx, g.ny, g.nz)
+        free_surface.update_flags_from_phi(g.phi, g.f_l, g.flags, twin.nz_solid, g.FLAG_FLUID,
+                                           g.FLAG_SOLID, g.FLAG_GAS, g.FLAG_IFACE)
+        free_surface.sync_phi_liquid_fraction(g.phi, g.f_l, g.flags, g.FLAG_GAS, g.FLAG_SOLID)
+    if twin.enable_csf_tension:
+        forces.compute_csf_tension(g.phi, g.flags, g.Fx, g.Fy, g.Fz, twin.gamma_lu, g.FLAG_SOLID,
+                                   g.FLAG_GAS, g.nx, g.ny, g.nz,
+                                   enable_wetting=twin.enable_wetting, theta_rad=twin.theta_rad)
+    forces.compute_marangoni_force(g.T, g.phi, g.f_l, g.Fx, g.Fy, g.Fz, g.flags,
+                                   twin.dgamma_dT_lu, g.dx, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny,
+                                   g.nz)
+    if is_welding:
+        weld_forces.apply_gas_shear(twin, g, arc_i, arc_j, arc_k)
+        forces.apply_arc_pressure(g.Fz, g.flags, g.phi, arc_i, arc_j, arc_k, p_sigma, pressure,
+                                  g.dt, g.dx, twin.mat.rho, g.FLAG_SOLID, g.FLAG_GAS)
+        weld_forces.apply_recoil(twin, g, arc_i, arc_j, arc_k)
+    if twin.enable_hydrostatic_gravity:
+        forces.add_hydrostatic_gravity(g.Fz, g.f_l, g.flags, 1.0, twin.g_lu, g.FLAG_SOLID,
+                                       g.FLAG_GAS)
+    forces.add_buoyancy(g.T, g.Fz, g.f_l, g.flags, twin.g_lu, twin.beta_T, twin.mat.T_liquidus,
+                        1.0, g.FLAG_SOLID, g.FLAG_GAS)
+    if is_welding and twin.enable_lorentz:
+        weld_forces.solve_lorentz(twin, g, arc_i, arc_j, arc_k)
+    u_cap = float(getattr(twin, "u_mach_limit_lu", 0.08))
+    F_cap = float(getattr(twin, "force_limit_lu", 0.05))
+    if F_cap > 0.0:
+        kernels.clamp_body_force_magnitude(g.Fx, g.Fy, g.Fz, g.flags, F_cap, g.FLAG_SOLID,
+                                           g.FLAG_GAS)
+    if twin.use_srt:
+        lbm.collide_srt(g.f_src, g.f_dst, g.rho, g.ux, g.uy, g.uz, g.Fx, g.Fy, g.Fz, g.f_l,
+                        g.flags, g.tau, twin.omega, 1.0, twin.C_darcy, g.FLAG_SOLID, g.FLAG_GAS,
+                        g.nx, g.ny, g.nz)
+    else:
+        lbm.collide_mrt(g.f_src, g.f_dst, g.rho, g.ux, g.uy, g.uz, g.Fx, g.Fy, g.Fz, g.f_l,
+                        g.flags, g.ex, g.ey, g.ez, g.w, g.opp, twin.omega, twin.omega_bulk,
+                        twin.C_darcy, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+    if u_cap > 0.0:
+        kernels.clamp_velocity_mach(g.ux, g.uy, g.uz, g.flags, u_cap, g.FLAG_SOLID, g.FLAG_GAS)
+    lbm.stream(g.f_dst, g.f_src, g.flags, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+    kernels.update_time_above_T(g.T, g.flags, g.time_above_800_s, g.time_above_1100_s,
+                                g.time_above_solidus_s, g.dt, T_800, T_1100, twin.mat.T_solidus,
+                                g.FLAG_GAS)
+    kernels.snapshot_forces(g.Fx, g.Fy, g.Fz, g.Fx_snap, g.Fy_snap, g.Fz_snap)
+    if twin.enable_substrate_growth or twin.enable_bead_freeze:
+        free_surface.remelt_hot_solid_scalar(g.T, g.H, g.f_l, g.phi, g.flags, twin.cp_rho,
+                                             twin.mat.T_solidus, twin.mat.T_liquidus, twin.L_rho,
+                                             g.FLAG_SOLID, g.FLAG_FLUID)
+        if is_welding and twin.enable_bead_freeze:
+            dx_, dy_, dz_ = getattr(twin, "_torch_dir_xyz", (1.0, 0.0, 0.0))
+            lookback = max(2.0, twin.trailing_solidify_lookback_mm / (g.dx * 1000.0))
+            T_freeze = twin.mat.T_liquidus + twin.trailing_solidify_temp_margin_K
+            kernels.solidify_trailing_pool_scalar(g.T, g.H, g.f_l, g.phi, g.flags, g.ux, g.uy,
+                                                  g.uz, twin.cp_rho, arc_i, arc_j, arc_k, dx_,
+                                                  dy_, dz_, lookback, T_freeze,
+                                                  twin.mat.T_solidus, g.FLAG_SOLID, g.FLAG_FLUID,
+                                                  g.FLAG_GAS)
+        free_surface.solidify_cooled_metal(g.T, g.f_l, g.phi, g.flags, g.ux, g.uy, g.uz,
+                                           twin.mat.T_solidus, True, g.FLAG_SOLID, g.FLAG_FLUID,
+                                           g.FLAG_GAS)
+    g.swap_buffers()
+    twin._step_n += 1
+
+
+def _fields(g):
+    f = _native.WaamFields()
+    g.ensure_vof_buffers()
+    for name, t in (("f_src", g.f_src), ("f_dst", g.f_dst), ("rho", g.rho), ("ux", g.ux),
+                    ("uy", g.uy), ("uz", g.uz), ("T", g.T), ("T_next", g.T_next), ("H", g.H),
+                    ("H_next", g.H_next), ("f_l", g.f_l), ("phi", g.phi),
+                    ("phi_tmp", g.phi_tmp), ("flags", g.flags), ("T_max", g.T_max),
+                    ("T_prev", g.T_prev), ("dT_dt", g.dT_dt), ("t800", g.time_above_800_s),
+                    ("t1100", g.time_above_1100_s), ("tsol", g.time_above_solidus_s),
+                    ("Fx", g.Fx), ("Fy", g.Fy), ("Fz", g.Fz), ("step_scalars", g.step_scalars)):
+        setattr(f, name, t.data_ptr())
+    f.nx, f.ny, f.nz = g.nx, g.ny, g.nz
+    return f
+
+
+def step_params(twin):
+    """WaamStepParams with every per-twin constant (per-step fields filled later)."""
+    g = twin.grid
+    m = twin.mat
+    p = _native.WaamStepParams()
+    p.nz_solid = twin.nz_solid
+    terms = twin.arc_source.fused_terms(twin)
+    for k, v in terms.items():
+        setattr(p, k, v)
+    p.Q_w, p.eta, p.dt, p.dx, p.dx3 = twin.Q_w, twin.eta, g.dt, g.dx, g.dx ** 3
+    p.pen = twin.arc_penetration_m / g.dx
+    p.surface_weighting = 1 if twin.arc_surface_weighting else 0
+    p.cp_rho, p.L_rho, p.Ts, p.Tl = twin.cp_rho, twin.L_rho, m.T_solidus, m.T_liquidus
+    p.T_cap, p.alpha_lu = twin.T_vapor_cap_K, twin.alpha_lu
+    p.cap_enabled = 1 if twin.enable_enthalpy_cap else 0
+    p.heat_loss = 1 if twin.enable_heat_loss else 0
+    p.T_amb, p.h_conv, p.eps_rad, p.sigma_sb = twin.T_amb, twin.h_conv, twin.eps_rad, twin.sigma_sb
+    p.conv, p.rad = int(twin.enable_convection), int(twin.enable_radiation)
+    p.vof, p.wetting, p.theta = int(twin.enable_vof), int(twin.enable_wetting), twin.theta_rad
+    p.csf, p.hydro = int(twin.enable_csf_tension), int(twin.enable_hydrostatic_gravity)
+    p.gamma_lu, p.dgamma_lu = twin.gamma_lu, twin.dgamma_dT_lu
+    p.p_sigma = weld_forces.arc_pressure_sigma_cells(twin)
+    p.pressure = weld_forces.arc_pressure_peak_pa(twin)
+    p.rho_phys, p.g_lu, p.beta, p.T_ref = m.rho, twin.g_lu, twin.beta_T, m.T_liquidus
+    p.F_cap = float(getattr(twin, "force_limit_lu", 0.05))
+    p.collision = 1 if twin.use_srt else 0
+    p.omega = twin.omega
+    p.omega_b = twin.omega_bulk
+    p.C_darcy = twin.C_darcy
+    p.u_cap = float(getattr(twin, "u_mach_limit_lu", 0.08))
+    p.T800, p.T1100 = T_800, T_1100
+    p.substrate_growth, p.bead_freeze = int(twin.enable_substrate_growth), int(twin.enable_bead_freeze)
+    p.lookback = max(2.0, twin.trailing_solidify_lookback_mm / (g.dx * 1000.0))
+    p.T_freeze = m.T_liquidus + twin.trailing_solidify_temp_margin_K
+    return p
+
+
+def _check_fused_supported(twin):
+    if twin.enable_lorentz or twin.enable_recoil or twin.enable_gas_shear:
+        return False
+    if getattr(twin, "use_torch_z", False):
+        return False
+    return True
+
+
+class _PositionRing:
+    """Pinned host slots for the per-step torch position (a 2-float H2D copy).
+
+    A slot is rewritten only after the copy that last read it has completed,
+    so the host can run ahead of the GPU without racing its own copies."""
+
+    SLOTS = 1024
+
+    def __init__(self, device):
+        self.host = torch.zeros((self.SLOTS, 2), dtype=torch.float32, pin_memory=True)
+        self.events = [None] * self.SLOTS
+        self.i = 0
+
+    def upload(self, dst, arc_i, arc_j):
+        slot = self.i % self.SLOTS
+        self.i += 1
+        ev = self.events[slot]
+        if ev is not None:
+            ev.synchronize()
+        self.host[slot, 0] = arc_i
+        self.host[slot, 1] = arc_j
+        dst.copy_(self.host[slot], non_blocking=True)
+        if ev is None:
+            ev = self.events[slot] = torch.cuda.Event()
+        ev.record()
+
+
+def upload_position(twin, arc_i, arc_j):
+    g = twin.grid
+    src = getattr(twin, "_device_position", None)
+    if src is not None:
+        # caller-provided device tensor with the position (cells); no host copy
+        g.step_scalars[4:6].copy_(src)
+        return
+    ring = getattr(g, "_pos_ring", None)
+    if ring is None:
+        ring = g._pos_ring = _PositionRing(g.device)
+    ring.upload(g.step_scalars[4:6], arc_i, arc_j)
+
+
+def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
+    """The B200 pipeline (waam_step_pre -> [droplet] -> waam_step_main)."""
+    if not _check_fused_supported(twin):
+        return coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m)
+    g = twin.grid
+    arc_i = torch_x_m / g.dx
+    arc_j = torch_y_m / g.dx
+    p = twin._fused_params
+    if p is None:
+        p = twin._fused_params = step_params(twin)
+    p.arc_i, p.arc_j = arc_i, arc_j
+    p.welding = 1 if is_welding else 0
+    p.forces_from_buffer = 0
+    dx_, dy_, dz_ = getattr(twin, "_torch_dir_xyz", (1.0, 0.0, 0.0))
+    p.dir_x, p.dir_y, p.dir_z = dx_, dy_, dz_
+    f = _fields(g)
+    ws = g.workspace
+    stream = torch.cuda.current_stream().cuda_stream
+    upload_position(twin, arc_i, arc_j)
+    _native.call("waam_step_pre", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(), ws.numel(),
+                 stream)
+    twin._last_arc_ijk = _LazyArc(g, arc_i, arc_j)
+    if is_welding and twin.droplet_freq > 0:
+        sim_time = twin._step_n * g.dt
+        if sim_time - twin._last_droplet_time >= deposition.droplet_period_s(twin):
+            arc_k = float(g.step_scalars[0].item())
+            forces.clear_forces(g.Fx, g.Fy, g.Fz)
+            _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m)
+            p.forces_from_buffer = 1
+    events = getattr(twin, "_stage_events", None)
+    if events is None:
+        _native.call("waam_step_main", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(),
+                     ws.numel(), stream)
+    else:
+        # stage timing for measurement: 7 cudaEvent handles recorded in-stream
+        handles = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
+        _native.call("waam_step_main_events", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(),
+                     ws.numel(), handles, len(events), stream)
+        cb = getattr(twin, "_stage_callback", None)
+        if cb is not None:
+            cb()
+    g.flip_thermal()
+    g.swap_buffers()
+    twin._step_n += 1
+
+
+class _LazyArc(tuple):
+    """(arc_i, arc_j, arc_k) whose arc_k is read from the device on first use."""
+
+    def __new__(cls, g, arc_i, arc_j):
+        obj = super().__new__(cls, (arc_i, arc_j, None))
+        obj._g = g
+        return obj
+
+    def __getitem__(self, idx):
+        if idx == 2 or idx == -1:
+            return float(self._g.step_scalars[0].item())
+        return tuple.__getitem__(self, idx)
+
+    def __iter__(self):
+        yield self[0]
+        yield self[1]
+        yield self[2]
+
+
+def coupled_step(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
+    if getattr(twin, "step_mode", "fused") == "operators":
+        coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m)
+    else:
+        coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m)
+    rec = getattr(twin, "probe_recorder", None)
+    if rec is not None:
+        rec.record_step(twin)

@@ -1,0 +1,68 @@
+// Internal declarations shared by the CUDA translation units.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "waam_common.cuh"
+
+namespace waam {
+
+constexpr int kThreads = 256;
+constexpr int kMaxElemBlocks = 148 * 16;  // grid-stride cap: 16 CTAs per SM
+constexpr int kRedBlocks = 592;           // fixed so reduction order never depends on the GPU
+
+// Caller-provided workspace layout (waam_workspace_bytes):
+//   [0, 256)            unsigned counter of the last-block reduction
+//   [256, 8192)         double partial sums, one per reduction block
+//   [8192, 16384)       float scalars (arc k, weight sum, energy per weight, ...)
+//   [16384, ...)        one field-sized float scratch (snapshots)
+constexpr size_t kWsPartialsOffset = 256;
+constexpr size_t kWsScalarsOffset = 8192;
+constexpr size_t kWsFieldOffset = 16384;
+
+// Slots of the fused step's device scalars (WaamFields::step_scalars).
+constexpr int kScalarArcK = 0;   // resolved arc k (written by the surface query)
+constexpr int kScalarWsum = 1;   // arc weight sum
+constexpr int kScalarEpw = 2;    // energy per unit weight
+constexpr int kScalarArcI = 4;   // torch x in cells (copied in by the host every step)
+constexpr int kScalarArcJ = 5;   // torch y in cells
+
+struct Workspace {
+    unsigned* counter;
+    double* partials;
+    float* scalars;
+    float* field;
+    static Workspace at(void* base) {
+        char* b = static_cast<char*>(base);
+        Workspace w;
+        w.counter = reinterpret_cast<unsigned*>(b);
+        w.partials = reinterpret_cast<double*>(b + kWsPartialsOffset);
+        w.scalars = reinterpret_cast<float*>(b + kWsScalarsOffset);
+        w.field = reinterpret_cast<float*>(b + kWsFieldOffset);
+        return w;
+    }
+};
+
+int fail(int code, const char* what);
+int check_launch(const char* what);
+int elem_blocks(int64_t n);
+int red_blocks(int64_t n);
+bool dims_ok(int nx, int ny, int nz);
+bool workspace_ok(void* ws, size_t bytes, int64_t n);
+
+__global__ void k_arc_norm(Dims d, const int32_t* __restrict__ flags, const float* __restrict__ f_l,
+                           ArcParams p, const float* arc_k_dev, float arc_k_offset, float Qe_dt,
+                           float dx3, float* norm_out, float* scalars, Workspace ws);
+__global__ void k_arc_inject(Dims d, float* __restrict__ H, const int32_t* __restrict__ flags,
+                             const float* __restrict__ f_l, ArcParams p, const float* arc_k_dev,
+                             float arc_k_offset, const float* scalars, int cap, PhaseParams ph);
+
+int launch_contact_columns(Dims d, const float* snap, float* phi, const int32_t* flags,
+                           float theta, void* stream);
+int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags, void* stream);
+int launch_deposit(Dims d, float* f_src, int32_t* flags, float* f_l, float* phi, float* H, float* T,
+                   float* rho, float arc_i, float arc_j, float arc_k, float foot_r, float drop_r,
+                   float target_vol, float T_drop, float cp_rho, float L_rho, float rho0,
+                   float* vol_acc, float* real_acc, float cell_vol, void* stream);
+
+}  // namespace waam

@@ -1,0 +1,491 @@
+"""Operator API of the coupled step, reference names and signatures.
+
+Each function here has the name and positional arguments of the waam_twin
+Taichi kernel it replaces (kernels.py / cumulant_kernel.py of the reference)
+and runs the matching sm_100a entry point of ``libwaam_b200.so`` on the
+current torch CUDA stream.  Fields are torch CUDA tensors laid out like the
+reference grid.  The ``FLAG_*`` arguments are accepted for signature
+compatibility and must carry the reference values (FLUID=0, SOLID=1, GAS=2,
+IFACE=4).  There is no CPU path: a missing library or a non-CUDA tensor
+raises.
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+
+from . import _native
+from ._native import WaamError
+
+FLAG_VALUES = {"FLAG_FLUID": 0, "FLAG_SOLID": 1, "FLAG_GAS": 2, "FLAG_IFACE": 4}
+_W = [1.0 / 3.0] + [1.0 / 18.0] * 6 + [1.0 / 36.0] * 12
+
+
+def _flags_ok(**kw):
+    for k, v in kw.items():
+        if int(v) != FLAG_VALUES[k]:
+            raise WaamError("%s=%s differs from the built-in value %d" % (k, v, FLAG_VALUES[k]))
+
+
+def _f(t, n=None):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise WaamError("expected a CUDA tensor, got %r" % type(t))
+    if t.dtype != torch.float32 or not t.is_contiguous():
+        raise WaamError("expected a contiguous float32 CUDA tensor, got %s" % t.dtype)
+    if n is not None and t.numel() != n:
+        raise WaamError("field has %d elements, expected %d" % (t.numel(), n))
+    return t.data_ptr()
+
+
+def _i(t, n=None):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise WaamError("expected a CUDA tensor, got %r" % type(t))
+    if t.dtype != torch.int32 or not t.is_contiguous():
+        raise WaamError("expected a contiguous int32 CUDA tensor (flags), got %s" % t.dtype)
+    if n is not None and t.numel() != n:
+        raise WaamError("flags has %d elements, expected %d" % (t.numel(), n))
+    return t.data_ptr()
+
+
+def _dims(t):
+    if t.dim() == 4:
+        return tuple(t.shape[1:])
+    return tuple(t.shape)
+
+
+def _stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+_WORKSPACES = {}
+
+
+def workspace_for(t):
+    """Device workspace for reducing entry points (cached per device and size)."""
+    n = t.numel() if t.dim() == 3 else t[0].numel()
+    key = (t.device, n)
+    ws = _WORKSPACES.get(key)
+    if ws is None:
+        nbytes = int(_native.lib().waam_workspace_bytes(n))
+        ws = torch.zeros(nbytes, dtype=torch.uint8, device=t.device)
+        _WORKSPACES[key] = ws
+    return ws.data_ptr(), ws.numel()
+
+
+def _call(name, *args):
+    return _native.call(name, *args)
+
+
+# ---------------------------------------------------------------- init ----
+def init_grid(f, rho, ux, uy, uz, T, H, f_l, phi, flags, T_ambient, rho0, cp_rho, nz_solid,
+              plate_i0, plate_i1, plate_j0, plate_j1, FLAG_FLUID, FLAG_SOLID, FLAG_GAS):
+    _flags_ok(FLAG_FLUID=FLAG_FLUID, FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(rho)
+    n = nx * ny * nz
+    _call("waam_init_grid", _f(f, 19 * n), _f(rho, n), _f(ux, n), _f(uy, n), _f(uz, n), _f(T, n),
+          _f(H, n), _f(f_l, n), _f(phi, n), _i(flags, n), nx, ny, nz, float(T_ambient),
+          float(rho0), float(cp_rho), int(nz_solid), int(plate_i0), int(plate_i1),
+          int(plate_j0), int(plate_j1), _stream())
+
+
+def init_aux_fields(T_max, T_prev, dT_dt, time_above_800, time_above_1100, time_above_solidus,
+                    Fx_snap, Fy_snap, Fz_snap, Fx, Fy, Fz, T_ambient, porosity_active,
+                    tracer_head, max_tracers):
+    """kernels.py:123-158 (state reset; not on the step path)."""
+    tracer_head.zero_()
+    porosity_active.zero_()
+    T_max.fill_(float(T_ambient))
+    T_prev.fill_(float(T_ambient))
+    for t in (dT_dt, time_above_800, time_above_1100, time_above_solidus, Fx_snap, Fy_snap,
+              Fz_snap, Fx, Fy, Fz):
+        t.zero_()
+
+
+def clear_forces(Fx, Fy, Fz):
+    n = Fx.numel()
+    _call("waam_clear_forces", _f(Fx, n), _f(Fy, n), _f(Fz, n), n, _stream())
+
+
+# ----------------------------------------------------------------- arc ----
+def inject_arc_heat(H, flags, phi, f_l, norm_buf, arc_i, arc_j, arc_k, Q_w, sigma, dt, dx3, eta,
+                    penetration_cells, enable_surface_weight, FLAG_SOLID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(H)
+    n = H.numel()
+    ws, wsb = workspace_for(H)
+    _call("waam_inject_arc_heat", _f(H, n), _i(flags, n), _f(f_l, n), _f(norm_buf, 1), nx, ny, nz,
+          float(arc_i), float(arc_j), float(arc_k), float(Q_w), float(sigma), float(dt),
+          float(dx3), float(eta), float(penetration_cells), int(enable_surface_weight), ws, wsb,
+          _stream())
+
+
+def inject_goldak_heat(H, flags, phi, f_l, norm_buf, arc_i, arc_j, arc_k, Q_w, dt, dx3, eta,
+                       travel_sign, ff, fr, a_front, a_rear, b_axis, c_axis, penetration_cells,
+                       enable_surface_weight, FLAG_SOLID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(H)
+    n = H.numel()
+    ws, wsb = workspace_for(H)
+    _call("waam_inject_goldak_heat", _f(H, n), _i(flags, n), _f(f_l, n), _f(norm_buf, 1), nx, ny,
+          nz, float(arc_i), float(arc_j), float(arc_k), float(Q_w), float(dt), float(dx3),
+          float(eta), float(travel_sign), float(ff), float(fr), float(a_front), float(a_rear),
+          float(b_axis), float(c_axis), float(penetration_cells), int(enable_surface_weight), ws,
+          wsb, _stream())
+
+
+def surface_height_at(phi, flags, out, i0, j0, nz_fallback, FLAG_GAS, nz):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    nx, ny, nz_ = _dims(phi)
+    if int(nz) != nz_:
+        raise WaamError("surface_height_at: nz=%s does not match the field (%d)" % (nz, nz_))
+    n = phi.numel()
+    _call("waam_surface_height_at", _f(phi, n), _i(flags, n), _f(out, 1), nx, ny, nz_, int(i0),
+          int(j0), int(nz_fallback), _stream())
+
+
+# ---------------------------------------------------------- deposition ----
+def feed_wire_surface(f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j, arc_k, footprint_r,
+                      droplet_radius, target_vol, T_drop, cp_rho, L_rho, rho0, vol_acc, real_acc,
+                      cell_vol, FLAG_GAS, FLAG_FLUID, FLAG_SOLID, nx, ny, nz):
+    _flags_ok(FLAG_GAS=FLAG_GAS, FLAG_FLUID=FLAG_FLUID, FLAG_SOLID=FLAG_SOLID)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_feed_wire_surface", _f(f_src, 19 * n), _i(flags, n), _f(f_l, n), _f(phi, n),
+          _f(H, n), _f(T, n), _f(rho, n), int(nx), int(ny), int(nz), float(arc_i), float(arc_j),
+          float(arc_k), float(footprint_r), float(droplet_radius), float(target_vol),
+          float(T_drop), float(cp_rho), float(L_rho), float(rho0), _f(vol_acc, 1),
+          _f(real_acc, 1), float(cell_vol), _stream())
+
+
+def feed_wire_momentum_impact(f_src, rho, ux, uy, uz, flags, f_l, arc_i, arc_j, arc_k,
+                              droplet_radius, vx_lu, vy_lu, vz_lu, FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_feed_wire_momentum_impact", _f(f_src, 19 * n), _f(rho, n), _f(ux, n), _f(uy, n),
+          _f(uz, n), _i(flags, n), _f(f_l, n), int(nx), int(ny), int(nz), float(arc_i),
+          float(arc_j), float(arc_k), float(droplet_radius), float(vx_lu), float(vy_lu),
+          float(vz_lu), _stream())
+
+
+def apply_droplet_impact_pressure(Fz, flags, phi, f_l, arc_i, arc_j, arc_k, drop_radius,
+                                  impact_pa, dt, dx, rho_ref, FLAG_SOLID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(Fz)
+    n = Fz.numel()
+    _call("waam_apply_droplet_impact_pressure", _f(Fz, n), _i(flags, n), _f(phi, n), _f(f_l, n),
+          nx, ny, nz, float(arc_i), float(arc_j), float(arc_k), float(drop_radius),
+          float(impact_pa), float(dt), float(dx), float(rho_ref), _stream())
+
+
+# ------------------------------------------------------------- thermal ----
+def advect_diffuse_temperature(H, T, ux, uy, uz, flags, alpha_lu, dt, FLAG_SOLID, FLAG_GAS,
+                               cp_rho, nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    ws, wsb = workspace_for(H)
+    _call("waam_advect_diffuse_temperature", _f(H, n), _f(T, n), _f(ux, n), _f(uy, n), _f(uz, n),
+          _i(flags, n), int(nx), int(ny), int(nz), float(alpha_lu), float(dt), float(cp_rho), ws,
+          wsb, _stream())
+
+
+def update_phase(H, T, f_l, cp_rho, L_rho, T_solidus, T_liquidus):
+    n = H.numel()
+    _call("waam_update_phase", _f(H, n), _f(T, n), _f(f_l, n), n, float(cp_rho), float(L_rho),
+          float(T_solidus), float(T_liquidus), _stream())
+
+
+def clamp_enthalpy_ceiling_scalar(H, flags, cp_rho, T_solidus, T_liquidus, T_vapor_cap, L_rho,
+                                  FLAG_GAS):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = H.numel()
+    _call("waam_clamp_enthalpy_ceiling_scalar", _f(H, n), _i(flags, n), n, float(cp_rho),
+          float(T_solidus), float(T_liquidus), float(T_vapor_cap), float(L_rho), _stream())
+
+
+def clamp_enthalpy_floor_scalar(H, cp_rho, flags, T_floor, FLAG_GAS):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = H.numel()
+    _call("waam_clamp_enthalpy_floor_scalar", _f(H, n), float(cp_rho), _i(flags, n), n,
+          float(T_floor), _stream())
+
+
+def update_T_max(T, T_max, flags, FLAG_GAS):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = T.numel()
+    _call("waam_update_T_max", _f(T, n), _f(T_max, n), _i(flags, n), n, _stream())
+
+
+def update_cooling_rate(T, T_prev, dT_dt, flags, dt_phys, FLAG_GAS):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = T.numel()
+    _call("waam_update_cooling_rate", _f(T, n), _f(T_prev, n), _f(dT_dt, n), _i(flags, n), n,
+          float(dt_phys), _stream())
+
+
+def apply_thermal_boundary_losses(H, T, flags, T_amb, h_conv, eps_rad, enable_conv, enable_rad,
+                                  cp_rho, dt, dx, sigma_sb, FLAG_SOLID, FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_apply_thermal_boundary_losses", _f(H, n), _f(T, n), _i(flags, n), int(nx),
+          int(ny), int(nz), float(T_amb), float(h_conv), float(eps_rad), int(enable_conv),
+          int(enable_rad), float(dt), float(dx), float(sigma_sb), _stream())
+
+
+def update_time_above_T(T, flags, time_above_800, time_above_1100, time_above_solidus, dt, T_800,
+                        T_1100, T_solidus, FLAG_GAS):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = T.numel()
+    _call("waam_update_time_above_T", _f(T, n), _i(flags, n), _f(time_above_800, n),
+          _f(time_above_1100, n), _f(time_above_solidus, n), n, float(dt), float(T_800),
+          float(T_1100), float(T_solidus), _stream())
+
+
+# ----------------------------------------------------------------- VOF ----
+def advect_phi(phi_dst, phi_src, ux, uy, uz, flags, FLAG_SOLID, FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_advect_phi", _f(phi_dst, n), _f(phi_src, n), _f(ux, n), _f(uy, n), _f(uz, n),
+          _i(flags, n), int(nx), int(ny), int(nz), _stream())
+
+
+def reinitialize_phi(phi, flags, FLAG_SOLID, FLAG_GAS, FLAG_FLUID):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS, FLAG_FLUID=FLAG_FLUID)
+    n = phi.numel()
+    _call("waam_reinitialize_phi", _f(phi, n), _i(flags, n), n, _stream())
+
+
+def apply_contact_angle_phi_bc(phi, flags, theta_rad, FLAG_SOLID, FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    ws, wsb = workspace_for(phi)
+    _call("waam_apply_contact_angle_phi_bc", _f(phi, n), _i(flags, n), int(nx), int(ny), int(nz),
+          float(theta_rad), ws, wsb, _stream())
+
+
+def update_flags_from_phi(phi, f_l, flags, nz_solid, FLAG_FLUID, FLAG_SOLID, FLAG_GAS, FLAG_IFACE):
+    _flags_ok(FLAG_FLUID=FLAG_FLUID, FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS,
+              FLAG_IFACE=FLAG_IFACE)
+    nx, ny, nz = _dims(phi)
+    n = phi.numel()
+    _call("waam_update_flags_from_phi", _f(phi, n), _f(f_l, n), _i(flags, n), nx, ny, nz,
+          int(nz_solid), _stream())
+
+
+def sync_phi_liquid_fraction(phi, f_l, flags, FLAG_GAS, FLAG_SOLID):
+    _flags_ok(FLAG_GAS=FLAG_GAS, FLAG_SOLID=FLAG_SOLID)
+    n = phi.numel()
+    _call("waam_sync_phi_liquid_fraction", _f(phi, n), _f(f_l, n), _i(flags, n), n, _stream())
+
+
+def remelt_hot_solid_scalar(T, H, f_l, phi, flags, cp_rho, T_solidus, T_liquidus, L_rho,
+                            FLAG_SOLID, FLAG_FLUID):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_FLUID=FLAG_FLUID)
+    n = T.numel()
+    _call("waam_remelt_hot_solid_scalar", _f(T, n), _f(H, n), _f(f_l, n), _f(phi, n),
+          _i(flags, n), n, float(cp_rho), float(T_solidus), float(T_liquidus), float(L_rho),
+          _stream())
+
+
+def solidify_trailing_pool_scalar(T, H, f_l, phi, flags, ux, uy, uz, cp_rho, arc_i, arc_j, arc_k,
+                                  dir_x, dir_y, dir_z, lookback_cells, T_freeze, T_solidus,
+                                  FLAG_SOLID, FLAG_FLUID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_FLUID=FLAG_FLUID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(T)
+    n = T.numel()
+    _call("waam_solidify_trailing_pool_scalar", _f(T, n), _f(H, n), _f(f_l, n), _f(phi, n),
+          _i(flags, n), _f(ux, n), _f(uy, n), _f(uz, n), nx, ny, nz, float(cp_rho), float(arc_i),
+          float(arc_j), float(arc_k), float(dir_x), float(dir_y), float(dir_z),
+          float(lookback_cells), float(T_freeze), float(T_solidus), _stream())
+
+
+def solidify_cooled_metal(T, f_l, phi, flags, ux, uy, uz, T_solidus, zero_velocity, FLAG_SOLID,
+                          FLAG_FLUID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_FLUID=FLAG_FLUID, FLAG_GAS=FLAG_GAS)
+    n = T.numel()
+    _call("waam_solidify_cooled_metal", _f(T, n), _f(f_l, n), _f(phi, n), _i(flags, n), _f(ux, n),
+          _f(uy, n), _f(uz, n), n, float(T_solidus), int(zero_velocity), _stream())
+
+
+# -------------------------------------------------------------- forces ----
+def compute_csf_tension(phi, flags, Fx, Fy, Fz, gamma_lu, FLAG_SOLID, FLAG_GAS, nx, ny, nz,
+                        enable_wetting, theta_rad):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_compute_csf_tension", _f(phi, n), _i(flags, n), _f(Fx, n), _f(Fy, n), _f(Fz, n),
+          int(nx), int(ny), int(nz), float(gamma_lu), int(enable_wetting), float(theta_rad),
+          _stream())
+
+
+compute_csf_wetting = compute_csf_tension
+
+
+def compute_marangoni_force(T, phi, f_l, Fx, Fy, Fz, flags, dgamma_dT, dx, FLAG_SOLID, FLAG_GAS,
+                            nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_compute_marangoni_force", _f(T, n), _f(phi, n), _f(f_l, n), _f(Fx, n), _f(Fy, n),
+          _f(Fz, n), _i(flags, n), int(nx), int(ny), int(nz), float(dgamma_dT), _stream())
+
+
+def apply_arc_pressure(Fz, flags, phi, arc_i, arc_j, arc_k, sigma, pressure_pa, dt, dx, rho_ref,
+                       FLAG_SOLID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(Fz)
+    n = Fz.numel()
+    _call("waam_apply_arc_pressure", _f(Fz, n), _i(flags, n), _f(phi, n), nx, ny, nz,
+          float(arc_i), float(arc_j), float(arc_k), float(sigma), float(pressure_pa), float(dt),
+          float(dx), float(rho_ref), _stream())
+
+
+def add_buoyancy(T, Fz, f_l, flags, g_lu, beta, T_ref, rho_ref, FLAG_SOLID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = T.numel()
+    _call("waam_add_buoyancy", _f(T, n), _f(Fz, n), _f(f_l, n), _i(flags, n), n, float(g_lu),
+          float(beta), float(T_ref), float(rho_ref), _stream())
+
+
+def add_hydrostatic_gravity(Fz, f_l, flags, rho_ref, g_lu, FLAG_SOLID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = Fz.numel()
+    _call("waam_add_hydrostatic_gravity", _f(Fz, n), _f(f_l, n), _i(flags, n), n, float(rho_ref),
+          float(g_lu), _stream())
+
+
+def clamp_body_force_magnitude(Fx, Fy, Fz, flags, F_max_lu, FLAG_SOLID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = Fx.numel()
+    _call("waam_clamp_body_force_magnitude", _f(Fx, n), _f(Fy, n), _f(Fz, n), _i(flags, n), n,
+          float(F_max_lu), _stream())
+
+
+def snapshot_forces(Fx, Fy, Fz, Fx_snap, Fy_snap, Fz_snap):
+    if Fx_snap.data_ptr() == Fx.data_ptr():
+        return  # the snapshot aliases the force field
+    n = Fx.numel()
+    _call("waam_snapshot_forces", _f(Fx, n), _f(Fy, n), _f(Fz, n), _f(Fx_snap, n),
+          _f(Fy_snap, n), _f(Fz_snap, n), n, _stream())
+
+
+# ------------------------------------------------------------------ LBM ----
+def collide_srt(f_src, f_dst, rho, ux, uy, uz, Fx, Fy, Fz, f_l, flags, tau, omega, dt_lu, C_darcy,
+                FLAG_SOLID, FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_collide_srt", _f(f_src, 19 * n), _f(f_dst, 19 * n), _f(rho, n), _f(ux, n),
+          _f(uy, n), _f(uz, n), _f(Fx, n), _f(Fy, n), _f(Fz, n), _f(f_l, n), _i(flags, n), n,
+          float(omega), float(C_darcy), _stream())
+
+
+def collide_mrt(f_src, f_dst, rho, ux, uy, uz, Fx, Fy, Fz, f_l, flags, EX, EY, EZ, W, OPP,
+                omega_s, omega_b, C_darcy, FLAG_SOLID, FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_collide_mrt", _f(f_src, 19 * n), _f(f_dst, 19 * n), _f(rho, n), _f(ux, n),
+          _f(uy, n), _f(uz, n), _f(Fx, n), _f(Fy, n), _f(Fz, n), _f(f_l, n), _i(flags, n), n,
+          float(omega_s), float(omega_b), float(C_darcy), _stream())
+
+
+def clamp_velocity_mach(ux, uy, uz, flags, u_max_lu, FLAG_SOLID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = ux.numel()
+    _call("waam_clamp_velocity_mach", _f(ux, n), _f(uy, n), _f(uz, n), _i(flags, n), n,
+          float(u_max_lu), _stream())
+
+
+def stream(f_src, f_dst, flags, FLAG_SOLID, FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_stream", _f(f_src, 19 * n), _f(f_dst, 19 * n), _i(flags, n), int(nx), int(ny),
+          int(nz), _stream())
+
+
+# ---------------------------------------------- verification set-ups ------
+# The reference's validation scripts build their cases with these kernels
+# (kernels.py:2085-2155, 3089-3179); they are set-up code, not step code.
+def init_poiseuille_channel(f, rho, ux, uy, uz, f_l, phi, flags, rho0, ny, nz, fx_lu, nu_lu,
+                            FLAG_FLUID, FLAG_SOLID):
+    nx = rho.shape[0]
+    dev = rho.device
+    j = torch.arange(ny, device=dev).view(1, ny, 1).expand(nx, ny, nz)
+    k = torch.arange(nz, device=dev).view(1, 1, nz).expand(nx, ny, nz)
+    wall = (j == 0) | (j == ny - 1) | (k == 0) | (k == nz - 1)
+    flags.copy_(torch.where(wall, torch.full_like(flags, FLAG_SOLID), torch.full_like(flags, FLAG_FLUID)))
+    rho.fill_(float(rho0))
+    uy.zero_()
+    uz.zero_()
+    f_l.fill_(1.0)
+    phi.fill_(1.0)
+    h = torch.tensor(float(ny - 2), dtype=torch.float32, device=dev)
+    y = (j - 1).to(torch.float32)
+    c = torch.tensor(float(fx_lu), dtype=torch.float32) / (torch.tensor(2.0) * torch.tensor(float(nu_lu), dtype=torch.float32))
+    prof = c.to(dev) * y * (h - 1.0 - y)
+    ux.copy_(torch.where(wall, torch.zeros_like(prof), prof))
+    u2 = ux * ux + uy * uy + uz * uz
+    from .grid import EX as _EX, EY as _EY, EZ as _EZ
+    for q in range(19):
+        wq = torch.tensor(_W[q], dtype=torch.float32)
+        eu = _EX[q] * ux + _EY[q] * uy + _EZ[q] * uz
+        eq = wq.to(dev) * float(rho0) * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * u2)
+        f[q].copy_(torch.where(wall, (wq * float(rho0)).to(dev).expand_as(eq), eq))
+
+
+def set_uniform_Fx(Fx, Fy, Fz, fx_lu, flags, FLAG_FLUID):
+    fluid = flags == FLAG_FLUID
+    Fx.copy_(torch.where(fluid, torch.full_like(Fx, float(fx_lu)), torch.zeros_like(Fx)))
+    Fy.zero_()
+    Fz.zero_()
+
+
+def prescribe_gaussian_pulse(T, H, f_l, flags, T_bg, A, sigma_m, cx, cy, cz, dx, cp_rho, FLAG_GAS):
+    nx, ny, nz = T.shape
+    dev = T.device
+    f32 = dict(dtype=torch.float32, device=dev)
+    inv2s2 = torch.tensor(1.0, dtype=torch.float32) / (torch.tensor(2.0) * torch.tensor(float(sigma_m), dtype=torch.float32) ** 2)
+    dxv = float(dx)
+    px = torch.arange(nx, **f32).view(nx, 1, 1) * dxv - float(cx)
+    py = torch.arange(ny, **f32).view(1, ny, 1) * dxv - float(cy)
+    pz = torch.arange(nz, **f32).view(1, 1, nz) * dxv - float(cz)
+    r2 = px * px + py * py + pz * pz
+    Tc = float(T_bg) + float(A) * torch.exp(-r2 * inv2s2.to(dev))
+    keep = flags == FLAG_GAS
+    T.copy_(torch.where(keep, T, Tc))
+    H.copy_(torch.where(keep, H, float(cp_rho) * Tc))
+    f_l.copy_(torch.where(keep, f_l, torch.ones_like(f_l)))
+
+
+def sync_T_from_H(H, T, cp_rho):
+    T.copy_(H / float(cp_rho))
+
+
+def init_stefan_liquid_column(T, H, f_l, phi, flags, nz_solid, T_amb, T_init, cp_rho, L_rho,
+                              T_solidus, T_liquidus, FLAG_FLUID, FLAG_SOLID):
+    nx, ny, nz = T.shape
+    k = torch.arange(nz, device=T.device).view(1, 1, nz).expand(nx, ny, nz)
+    sol = k < int(nz_solid)
+    cp = torch.tensor(float(cp_rho), dtype=torch.float32)
+    H_liq = cp * float(T_liquidus) + torch.tensor(float(L_rho), dtype=torch.float32)
+    flags.copy_(torch.where(sol, torch.full_like(flags, FLAG_SOLID), torch.full_like(flags, FLAG_FLUID)))
+    phi.fill_(1.0)
+    f_l.copy_(torch.where(sol, torch.zeros_like(f_l), torch.ones_like(f_l)))
+    T.copy_(torch.where(sol, torch.full_like(T, float(T_amb)), torch.full_like(T, float(T_init))))
+    h_liq_val = (H_liq + cp * (torch.tensor(float(T_init), dtype=torch.float32) - float(T_liquidus))).item()
+    h_sol_val = (cp * float(T_amb)).item()
+    H.copy_(torch.where(sol, torch.full_like(H, h_sol_val), torch.full_like(H, h_liq_val)))
+
+
+def clamp_substrate_enthalpy(H, T, f_l, flags, nz_solid, T_amb, cp_rho, FLAG_SOLID):
+    nx, ny, nz = T.shape
+    k = torch.arange(nz, device=T.device).view(1, 1, nz).expand(nx, ny, nz)
+    m = (k < int(nz_solid)) & (flags == FLAG_SOLID)
+    h = (torch.tensor(float(cp_rho), dtype=torch.float32) * float(T_amb)).item()
+    H.copy_(torch.where(m, torch.full_like(H, h), H))
+    T.copy_(torch.where(m, torch.full_like(T, float(T_amb)), T))
+    f_l.copy_(torch.where(m, torch.zeros_like(f_l), f_l))
+
+
+def bind_velocity_set(grid):
+    """Kept for API compatibility (kernels.py:54-56)."""
+    return None
+
+
+__all__ = [n for n in dir() if not n.startswith("_") and n not in ("math", "torch")]

@@ -1,0 +1,362 @@
+"""WAAMTwin driver on the B200 backend (reference twin.py:37-869, the parts on
+the step path: construction, derived lattice scalars, reset, step, run,
+run_path, telemetry).
+
+The constructor takes the reference's keyword arguments.  Features outside
+the accelerated path (material tables, vapour recoil, gas shear, moving
+window) raise instead of silently changing the physics.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import kernels
+from .coupled_step import coupled_step
+from .grid import WAAMGrid
+from .materials import MaterialProps, load_material
+from .physics.arc import create_heat_source
+from .physics.deposition_balance import droplet_mass_kg, expected_deposited_mass_kg
+from .torch_path import TorchPathDriver, clamp_torch_to_domain, parse_torch_path
+
+RHO_LATTICE = 1.0
+
+
+class WAAMTwin:
+    def __init__(self, material="ER70S-6", nx=256, ny=128, nz=64, dx=2e-4, arc_power_W=2800.0,
+                 arc_efficiency=0.8, high_sulphur=False, T_ambient=300.0, use_srt=True,
+                 C_darcy=1.6e5, arc_pressure_pa=500.0, droplet_freq_hz=50.0, max_tracers=None,
+                 enable_heat_loss=False, h_conv=25.0, eps_rad=0.3, enable_convection=True,
+                 enable_radiation=False, heat_source="gaussian2d", enable_vof=False,
+                 enable_recoil=False, enable_csf_tension=False, enable_deposition_momentum=True,
+                 enable_lorentz=False, enable_gas_shear=False,
+                 enable_droplet_impact_pressure=True, use_recoil_clausius_clapeyron=True,
+                 enable_substrate_growth=False, enable_moving_window=False, enable_wetting=False,
+                 enable_hydrostatic_gravity=False, enable_bead_freeze=False, enable_ctwd=False,
+                 contact_angle_deg=None, deposition_superheat_K=500.0,
+                 deposition_footprint_sigma_scale=1.0, stickout_mm=12.0, ctwd_mm=15.0,
+                 layer_height_mm=1.2, recoil_pressure_pa=5000.0, welding_current_A=140.0,
+                 sigma_liquid_Sm=1.0e6, sigma_solid_Sm=1.0e5, lorentz_jacobi_iters=40,
+                 lorentz_jacobi_omega=0.85, gas_jet_velocity_m_s=12.0, gas_shear_coeff=1.0,
+                 T_boiling_K=3100.0, P_vapor_ref_Pa=101325.0, L_vapor_J_kg=6.0e6,
+                 R_spec_vapor_J_kgK=450.0, travel_speed_m_s=0.0, use_variable_tau=True,
+                 enable_enthalpy_cap=True, T_vapor_cap_K=3200.0, arc_surface_weighting=True,
+                 arc_penetration_mm=2.0, wire_diameter_mm=1.2, arc_sigma_mm=2.0, bulk_tau=None,
+                 step_mode="fused", device=None):
+        if arc_power_W < 0:
+            raise ValueError("arc_power_W must be >= 0, got %s" % arc_power_W)
+        if not 0.0 < arc_efficiency <= 1.0:
+            raise ValueError("arc_efficiency must be in (0, 1], got %s" % arc_efficiency)
+        if wire_diameter_mm <= 0:
+            raise ValueError("wire_diameter_mm must be > 0, got %s" % wire_diameter_mm)
+        if arc_sigma_mm <= 0:
+            raise ValueError("arc_sigma_mm must be > 0, got %s" % arc_sigma_mm)
+        if contact_angle_deg is not None and not 0.0 < contact_angle_deg < 180.0:
+            raise ValueError("contact_angle_deg must be in (0, 180), got %s" % contact_angle_deg)
+        if enable_moving_window:
+            raise NotImplementedError("moving window is not supported by this backend")
+        self.mat = material if isinstance(material, MaterialProps) else load_material(material, high_sulphur)
+        if self.mat.has_tables:
+            raise NotImplementedError("temperature-dependent material tables are not supported")
+        self.use_material_tables = False
+        self.Q_w = arc_power_W
+        self.eta = arc_efficiency
+        self.T_amb = T_ambient
+        self.use_srt = use_srt
+        self.C_darcy = C_darcy
+        self.arc_pressure = arc_pressure_pa
+        self.arc_pressure_model = "constant"
+        self.pressure_sigma_m = None
+        self.strict_mode = False
+        self.u_mach_limit_lu = 0.08
+        self.force_limit_lu = 0.05
+        self.droplet_freq = droplet_freq_hz
+        self.enable_heat_loss = enable_heat_loss
+        self.h_conv = h_conv
+        self.eps_rad = eps_rad
+        self.enable_convection = enable_convection
+        self.enable_radiation = enable_radiation
+        self.sigma_sb = 5.670374419e-8
+        self.heat_source_name = heat_source
+        self.enable_vof = enable_vof
+        self.enable_recoil = enable_recoil
+        self.enable_csf_tension = enable_csf_tension
+        self.enable_deposition_momentum = enable_deposition_momentum
+        self.enable_lorentz = enable_lorentz
+        self.enable_gas_shear = enable_gas_shear
+        self.grid = WAAMGrid(nx, ny, nz, dx, self.mat, max_tracers=max_tracers or 50_000,
+                             allocate_lorentz=enable_lorentz, allocate_vof=True, device=device)
+        self.enable_droplet_impact_pressure = enable_droplet_impact_pressure
+        self.use_recoil_clausius_clapeyron = use_recoil_clausius_clapeyron
+        self.enable_substrate_growth = enable_substrate_growth
+        self.enable_moving_window = enable_moving_window
+        self.enable_wetting = enable_wetting
+        self.enable_hydrostatic_gravity = enable_hydrostatic_gravity
+        self.enable_bead_freeze = enable_bead_freeze
+        self.enable_ctwd = enable_ctwd
+        self.contact_angle_deg = (contact_angle_deg if contact_angle_deg is not None
+                                  else self.mat.contact_angle_deg)
+        self.theta_rad = math.radians(self.contact_angle_deg)
+        self.deposition_superheat_K = deposition_superheat_K
+        self.deposition_footprint_sigma_scale = deposition_footprint_sigma_scale
+        self.stickout_m = stickout_mm * 1e-3
+        self.ctwd_nominal_m = ctwd_mm * 1e-3
+        self.ctwd_m = ctwd_mm * 1e-3
+        self.layer_height_m = layer_height_mm * 1e-3
+        self.rho_e_ohm_m = self.mat.rho_e_ohm_m
+        self.eta_stick = self.mat.eta_stick
+        self.recoil_pressure_pa = recoil_pressure_pa
+        self.welding_current_A = welding_current_A
+        self.sigma_liquid_Sm = sigma_liquid_Sm
+        self.sigma_solid_Sm = sigma_solid_Sm
+        self.lorentz_jacobi_iters = lorentz_jacobi_iters
+        self.lorentz_jacobi_omega = lorentz_jacobi_omega
+        self.gas_jet_velocity_m_s = gas_jet_velocity_m_s
+        self.gas_shear_coeff = gas_shear_coeff
+        self.T_boiling_K = T_boiling_K
+        self.P_vapor_ref_Pa = P_vapor_ref_Pa
+        self.L_vapor_J_kg = L_vapor_J_kg
+        self.R_spec_vapor_J_kgK = R_spec_vapor_J_kgK
+        self.travel_speed_m_s = travel_speed_m_s
+        self.marangoni_scale = 1.0
+        self.use_variable_tau = use_variable_tau
+        self.enable_enthalpy_cap = enable_enthalpy_cap
+        self.T_vapor_cap_K = T_vapor_cap_K
+        self.arc_surface_weighting = arc_surface_weighting
+        self.arc_penetration_m = arc_penetration_mm * 1e-3
+        self.wire_diameter_m = wire_diameter_mm * 1e-3
+        self.wire_feed_m_s = 0.0
+        self.droplet_transfer_mode = "auto"
+        self.pulse_frequency_hz = 0.0
+        self.droplet_size_jitter = 0.12
+        self.impact_lead_angle_deg = 0.0
+        self.trailing_solidify_lookback_mm = 2.5
+        self.trailing_solidify_temp_margin_K = 35.0
+        self._deposited_volume_m3 = 0.0
+        self._n_droplets_fired = 0
+        self._deposition_overflow = 0
+        self.plate_thickness_mm = None
+        self.plate_size_mm = None
+        self.plate_origin_mm = None
+        self.nz_solid = max(1, nz // 5)
+        self._step_n = 0
+        self._last_droplet_time = 0.0
+        self._window_offset_x_m = 0.0
+        self._interpass_cooling_steps = 0
+        self.probe_recorder = None
+        self.use_torch_z = False
+        self.substrate_z_m = 0.0
+        self._sim_origin_offset_x_m = 0.0
+        self._sim_origin_offset_y_m = 0.0
+        self._last_torch_pos_m = None
+        self._torch_dir_xyz = (1.0, 0.0, 0.0)
+        self._last_arc_ijk = None
+        self.step_mode = step_mode
+        self._fused_params = None
+
+        # Derived lattice scalars (twin.py:244-274).
+        g = self.grid
+        mat = self.mat
+        self.cp_rho = mat.rho * mat.cp
+        self.L_rho = mat.rho * mat.L_fusion
+        self.alpha_lu = mat.alpha * g.dt / (g.dx ** 2)
+        self.omega = 1.0 / g.tau
+        self.omega_bulk = 1.0 / bulk_tau if bulk_tau else self.omega
+        self.arc_sigma_m = arc_sigma_mm * 1e-3
+        self.sigma_cells = self.arc_sigma_m / g.dx
+        self.g_lu = 9.81 * (g.dt ** 2) / g.dx
+        self.beta_T = mat.beta_T
+        scale_F = (g.dt ** 2) / (mat.rho * g.dx ** 2)
+        self.force_scale = scale_F
+        self.dgamma_dT_lu = mat.dgamma_dT * scale_F / g.dx
+        self.gamma_lu = mat.gamma_0 * scale_F / g.dx
+        self.H_sol = mat.rho * mat.cp * mat.T_solidus
+        self.H_liq = self.H_sol + self.L_rho
+        self.arc_source = create_heat_source(heat_source)
+
+    # -- configuration ----------------------------------------------------
+    def invalidate(self):
+        """Drop cached step parameters after changing a twin attribute."""
+        self._fused_params = None
+
+    def resolve_nz_solid(self, test_fluid_domain=False):
+        """Substrate layers from plate thickness (else nz//5), leaving gas headroom."""
+        if test_fluid_domain:
+            return 0
+        g = self.grid
+        headroom = max(6, g.nz // 4)
+        max_solid = max(1, g.nz - headroom)
+        thick = self.plate_thickness_mm
+        if thick is not None and float(thick) > 0.0:
+            n = int(round(float(thick) / (g.dx * 1000.0)))
+            return max(1, min(n, max_solid))
+        return max(1, min(g.nz // 5, max_solid))
+
+    def resolve_plate_ij(self):
+        g = self.grid
+        if not self.plate_size_mm:
+            return 0, g.nx, 0, g.ny
+        dx_mm = g.dx * 1000.0
+        ni = min(max(1, int(round(float(self.plate_size_mm[0]) / dx_mm))), g.nx)
+        nj = min(max(1, int(round(float(self.plate_size_mm[1]) / dx_mm))), g.ny)
+        if self.plate_origin_mm is not None:
+            i0 = int(round(float(self.plate_origin_mm[0]) / dx_mm))
+            j0 = int(round(float(self.plate_origin_mm[1]) / dx_mm))
+        else:
+            i0, j0 = (g.nx - ni) // 2, (g.ny - nj) // 2
+        i0 = max(0, min(i0, g.nx - ni))
+        j0 = max(0, min(j0, g.ny - nj))
+        return i0, i0 + ni, j0, j0 + nj
+
+    def apply_plate_geometry(self, *, plate_thickness_mm=None, plate_size_mm=None,
+                             plate_origin_mm=None):
+        if plate_thickness_mm is not None:
+            self.plate_thickness_mm = float(plate_thickness_mm)
+            self.nz_solid = self.resolve_nz_solid()
+        if plate_size_mm is not None:
+            self.plate_size_mm = (float(plate_size_mm[0]), float(plate_size_mm[1]))
+        if plate_origin_mm is not None:
+            self.plate_origin_mm = (float(plate_origin_mm[0]), float(plate_origin_mm[1]))
+        self.invalidate()
+
+    # -- state ------------------------------------------------------------
+    def reset(self, T_ambient=None, test_fluid_domain=False):
+        """twin.py:486-531: quiescent plate + gas, aux fields, one initial stream."""
+        T0 = T_ambient or self.T_amb
+        g = self.grid
+        if test_fluid_domain:
+            nz_solid = -1
+            self.nz_solid = 0
+            i0, i1, j0, j1 = 0, g.nx, 0, g.ny
+        else:
+            self.nz_solid = self.resolve_nz_solid(False)
+            nz_solid = self.nz_solid
+            i0, i1, j0, j1 = self.resolve_plate_ij()
+        kernels.init_grid(g.f_a, g.rho, g.ux, g.uy, g.uz, g.T, g.H, g.f_l, g.phi, g.flags, T0,
+                          RHO_LATTICE, self.cp_rho, nz_solid, i0, i1, j0, j1, g.FLAG_FLUID,
+                          g.FLAG_SOLID, g.FLAG_GAS)
+        kernels.init_aux_fields(g.T_max, g.T_prev, g.dT_dt, g.time_above_800_s,
+                                g.time_above_1100_s, g.time_above_solidus_s, g.Fx_snap, g.Fy_snap,
+                                g.Fz_snap, g.Fx, g.Fy, g.Fz, T0, g.porosity_active,
+                                g.tracer_head, g.max_tracers)
+        kernels.stream(g.f_a, g.f_b, g.flags, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+        self._step_n = 0
+        self._last_droplet_time = 0.0
+        self._deposited_volume_m3 = 0.0
+        self._n_droplets_fired = 0
+        self._deposition_overflow = 0
+        self._last_torch_pos_m = None
+        self._torch_dir_xyz = (1.0, 0.0, 0.0)
+        g.deposit_vol_buf.zero_()
+        g.deposit_real_buf.zero_()
+        self.invalidate()
+
+    def step(self, torch_x_m, torch_y_m, is_welding=True, torch_z_m=None):
+        """twin.py:533-567."""
+        z_now = 0.0 if torch_z_m is None else float(torch_z_m)
+        if self._last_torch_pos_m is not None:
+            px, py, pz = self._last_torch_pos_m
+            d = (torch_x_m - px, torch_y_m - py, z_now - pz)
+            norm = math.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
+            if norm > 1e-12:
+                self._torch_dir_xyz = (d[0] / norm, d[1] / norm, d[2] / norm)
+        self._last_torch_pos_m = (torch_x_m, torch_y_m, z_now)
+        sim_x = torch_x_m - self._window_offset_x_m - self._sim_origin_offset_x_m
+        sim_y = torch_y_m - self._sim_origin_offset_y_m
+        coupled_step(self, sim_x, sim_y, is_welding, torch_z_m)
+        self._check_strict_mode()
+
+    def _check_strict_mode(self):
+        if not self.strict_mode or self._n_droplets_fired < 20:
+            return
+        ratio = self._deposited_volume_m3 * self.mat.rho / max(
+            self._n_droplets_fired * droplet_mass_kg(self), 1e-12)
+        if not 0.95 <= ratio <= 1.05:
+            raise RuntimeError("[strict_mode] mass_balance_ratio=%.3f outside [0.95, 1.05] after "
+                               "%d droplets" % (ratio, self._n_droplets_fired))
+
+    def run(self, n_steps, torch_x_m=0.0, torch_y_m=0.0, is_welding=True):
+        for _ in range(n_steps):
+            self.step(torch_x_m, torch_y_m, is_welding)
+
+    def path_positions(self, job, n_steps=None):
+        """(x, y, z) torch positions of run_path, as a list (twin.py:632-704)."""
+        waypoints = parse_torch_path(job) if isinstance(job, dict) else list(job)
+        g = self.grid
+        if not waypoints:
+            waypoints = [(0.01, (g.ny // 2) * g.dx, 0.0)]
+        driver = TorchPathDriver(waypoints, self.travel_speed_m_s)
+        if n_steps is None:
+            n_steps = max(400, int(driver.total_length / max(self.travel_speed_m_s * g.dt, 1e-12)))
+        if driver.segments:
+            s0 = driver.segments[0]
+            d = (s0.x1 - s0.x0, s0.y1 - s0.y0, s0.z1 - s0.z0)
+            norm = math.sqrt(sum(v * v for v in d))
+            if norm > 1e-12:
+                self._torch_dir_xyz = tuple(v / norm for v in d)
+        out = []
+        for step, x, y, z in driver.positions_for_steps(n_steps, g.dt):
+            seg = driver.segment_index_at_distance(driver.distance_at_step(step, g.dt))
+            out.append((step, seg, x, y, z))
+        return driver, out
+
+    def run_path(self, job, n_steps=None, is_welding=True, interpass_steps=0):
+        """Follow the job's torch path at travel speed, with interpass parking."""
+        driver, pos = self.path_positions(job, n_steps)
+        g = self.grid
+        interpass = int(interpass_steps) if interpass_steps else int(self._interpass_cooling_steps or 0)
+        prev_seg = -1
+
+        def clamp(x, y):
+            off = self._window_offset_x_m
+            cx, cy = clamp_torch_to_domain(x - off, y, g.nx, g.ny, g.dx)
+            return cx + off, cy
+
+        for step, seg, x, y, z in pos:
+            if interpass > 0 and seg > prev_seg >= 0:
+                park = driver.segment_end(prev_seg) or (x, y, z)
+                for _ in range(interpass):
+                    cx, cy = clamp(park[0], park[1])
+                    self.step(cx, cy, is_welding=False, torch_z_m=park[2])
+            prev_seg = seg
+            cx, cy = clamp(x, y)
+            self.step(cx, cy, is_welding, torch_z_m=z)
+
+    # -- telemetry (twin.py:706-821, pool metrics) -------------------------
+    def get_telemetry(self):
+        g = self.grid
+        fl = g.f_l
+        liquid = fl > 0.5
+        n_liquid = int(liquid.sum().item())
+        tele = {"step": self._step_n, "sim_time_s": self._step_n * g.dt, "n_liquid_cells": n_liquid}
+        nongas = g.flags != g.FLAG_GAS
+        if n_liquid > 0:
+            T_peak = float(torch.where(liquid, g.T, torch.full_like(g.T, -1e30)).max().item())
+            ii = torch.nonzero(liquid)[:, 0].to(torch.float64)
+            i_c = int(round(float(ii.mean().item())))
+            i_c = max(0, min(g.nx - 1, i_c))
+            sect = (fl[i_c] > 0.5).cpu().numpy()
+            if sect.any():
+                y_idx = np.where(sect.any(axis=1))[0]
+                z_idx = np.where(sect.any(axis=0))[0]
+                width = (y_idx[-1] - y_idx[0] + 1) * g.dx
+                depth = max(0, self.nz_solid - z_idx[0]) * g.dx
+            else:
+                width = depth = 0.0
+            length = (float(ii.max().item()) - float(ii.min().item()) + 1.0) * g.dx
+            u2 = (g.ux * g.ux + g.uy * g.uy + g.uz * g.uz)[liquid].max().item()
+            u_max = math.sqrt(u2) * g.dx / g.dt
+        else:
+            T_peak = float(torch.where(nongas, g.T, torch.full_like(g.T, -1e30)).max().item())
+            width = depth = length = u_max = 0.0
+        dep_mass = self._deposited_volume_m3 * self.mat.rho
+        exp_drop = self._n_droplets_fired * droplet_mass_kg(self)
+        tele.update(T_peak_K=T_peak, pool_width_mm=width * 1e3, pool_depth_mm=depth * 1e3,
+                    pool_length_mm=length * 1e3, u_max_m_s=u_max,
+                    deposited_mass_kg=dep_mass, expected_mass_kg=expected_deposited_mass_kg(self),
+                    mass_balance_ratio=dep_mass / max(exp_drop, 1e-12),
+                    n_droplets=self._n_droplets_fired,
+                    total_enthalpy_J=float(g.H.double().sum().item()) * g.dx ** 3)
+        return tele
