@@ -295,6 +295,7 @@ def run_b200(args, w):
     torch.cuda.synchronize()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
+        t_host = time.perf_counter()
         start.record()
         for k in range(K):
             tw._device_position = dev_pos[k]
@@ -302,6 +303,7 @@ def run_b200(args, w):
             tw.step(*pos[s], True)
             s += 1
         stop.record()
+        host_ms = (time.perf_counter() - t_host) * 1e3 / K
         torch.cuda.synchronize()
     tw._device_position = None
     tw._stage_events = None
@@ -363,6 +365,7 @@ def run_b200(args, w):
                      "algorithmic_bytes_per_launch": algo[dom]},
         "stages_ms": stage_ms,
         "step_algorithmic_GBps": step_bytes / (ms / K * 1e-3) / 1e9,
+        "host_enqueue_ms_per_step": host_ms,
         "cell_census": c,
         "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 4},
         "gpu_launches": int(launches_per_step * 2 * K),
@@ -385,10 +388,14 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="standard", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spinup", type=int, default=None,
+                    help="steps run before warm-up (default: the workload's spin-up)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    w = WORKLOADS[args.workload]
+    w = dict(WORKLOADS[args.workload])
+    if args.spinup is not None:
+        w["spinup"] = args.spinup
     if args.impl == "reference":
         run_reference(args, w)
     else:
