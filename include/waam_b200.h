@@ -58,6 +58,20 @@ int waam_inject_goldak_heat(float* H, const int32_t* flags, const float* f_l, fl
                             float Q_w, float dt, float dx3, float eta, float sign, float ff,
                             float fr, float a_f, float a_r, float b, float c, float pen,
                             int enable, void* workspace, size_t workspace_bytes, void* stream);
+/* Same operation and result as waam_inject_goldak_heat, for callers that
+ * cannot allocate device memory (an FFI host without a CUDA allocator, or a
+ * step loop under a fixed device-memory budget): its reduction scratch is a
+ * static device array inside the library, so it takes no workspace.  No
+ * counterpart in the reference.  Grids above 16,777,216 cells are rejected
+ * with WAAM_ERR_INVALID; calls that overlap on the GPU race on the shared
+ * scratch; the first call on a device resolves the scratch address and
+ * should come before any stream capture. */
+int waam_inject_goldak_heat_noalloc(float* H, const int32_t* flags, const float* f_l,
+                                    float* norm_buf, int nx, int ny, int nz, float arc_i,
+                                    float arc_j, float arc_k, float Q_w, float dt, float dx3,
+                                    float eta, float sign, float ff, float fr, float a_f,
+                                    float a_r, float b, float c, float pen, int enable,
+                                    void* stream);
 /* kernels.py:1953-1984 clamp_enthalpy_ceiling_scalar (physics/thermal.py:30) */
 int waam_clamp_enthalpy_ceiling_scalar(float* H, const int32_t* flags, int64_t n, float cp_rho,
                                        float Ts, float Tl, float T_cap, float L_rho, void* stream);
