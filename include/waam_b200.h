@@ -248,8 +248,11 @@ typedef struct WaamStepParams {
     /* VOF */
     int vof, wetting;
     float theta;
-    /* forces */
-    int csf, hydro, forces_from_buffer;
+    /* forces.  The fused step keeps F == 0 outside FLUID/IFACE cells; set
+     * forces_from_buffer when F holds this step's droplet impact load (then F is
+     * the starting force of active cells and stays untouched elsewhere), and
+     * clear_forces when the previous step left F != 0 outside active cells. */
+    int csf, hydro, forces_from_buffer, clear_forces;
     float gamma_lu, dgamma_lu, p_sigma, pressure, rho_phys, g_lu, beta, T_ref, F_cap;
     /* collision */
     int collision;  /* 0 MRT, 1 SRT */

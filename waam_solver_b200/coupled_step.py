@@ -190,6 +190,7 @@ def coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=Non
                                            g.FLAG_GAS)
     g.swap_buffers()
     twin._step_n += 1
+    g._forces_dirty = True
 
 
 def _fields(g):
@@ -260,8 +261,10 @@ class _PositionRing:
 
     SLOTS = 1024
 
-    def __init__(self, device):
+    def __init__(self):
         self.host = torch.zeros((self.SLOTS, 2), dtype=torch.float32, pin_memory=True)
+        self.host_np = self.host.numpy()
+        self.views = [self.host[i] for i in range(self.SLOTS)]
         self.events = [None] * self.SLOTS
         self.i = 0
 
@@ -271,9 +274,9 @@ class _PositionRing:
         ev = self.events[slot]
         if ev is not None:
             ev.synchronize()
-        self.host[slot, 0] = arc_i
-        self.host[slot, 1] = arc_j
-        dst.copy_(self.host[slot], non_blocking=True)
+        self.host_np[slot, 0] = arc_i
+        self.host_np[slot, 1] = arc_j
+        dst.copy_(self.views[slot], non_blocking=True)
         if ev is None:
             ev = self.events[slot] = torch.cuda.Event()
         ev.record()
@@ -284,16 +287,63 @@ def upload_position(twin, arc_i, arc_j):
     src = getattr(twin, "_device_position", None)
     if src is not None:
         # caller-provided device tensor with the position (cells); no host copy
-        g.step_scalars[4:6].copy_(src)
+        g._pos_dst.copy_(src)
         return
     ring = getattr(g, "_pos_ring", None)
     if ring is None:
-        ring = g._pos_ring = _PositionRing(g.device)
-    ring.upload(g.step_scalars[4:6], arc_i, arc_j)
+        ring = g._pos_ring = _PositionRing()
+    ring.upload(g._pos_dst, arc_i, arc_j)
+
+
+def _fields_cached(g):
+    """WaamFields for the current buffer parity (device pointers never move)."""
+    key = (g._read_buf is g.f_a, g._cur)
+    cache = g.__dict__.setdefault("_fields_cache", {})
+    f = cache.get(key)
+    if f is None:
+        f = cache[key] = _fields(g)
+        g._pos_dst = g.step_scalars[4:6]
+    return f
+
+
+def _droplet_due(twin, g, is_welding):
+    if not is_welding or twin.droplet_freq <= 0:
+        return False
+    sim_time = twin._step_n * g.dt
+    return sim_time - twin._last_droplet_time >= deposition.droplet_period_s(twin)
+
+
+def _run_graph(twin, g, f, p, ws, key):
+    """Replay (capturing on first reuse) the CUDA graph of one non-droplet step."""
+    graphs = twin.__dict__.setdefault("_graphs", {})
+    entry = graphs.get(key)
+    if entry is None:
+        graphs[key] = entry = {"seen": 0, "graph": None}
+    if entry["graph"] is None:
+        entry["seen"] += 1
+        if entry["seen"] < 3:      # eager the first two times: modules load outside capture
+            return False
+        graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.graph(graph, stream=side):
+            st = torch.cuda.current_stream().cuda_stream
+            _native.call("waam_step_pre", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(),
+                         ws.numel(), st)
+            _native.call("waam_step_main", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(),
+                         ws.numel(), st)
+        torch.cuda.current_stream().wait_stream(side)
+        entry["graph"] = graph
+    entry["graph"].replay()
+    return True
 
 
 def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
-    """The B200 pipeline (waam_step_pre -> [droplet] -> waam_step_main)."""
+    """The B200 pipeline (waam_step_pre -> [droplet] -> waam_step_main).
+
+    Steps without a droplet replay a captured CUDA graph of the two stages
+    (``twin.use_cuda_graphs``); droplet steps and instrumented steps run the
+    stages eagerly because they read back or record events in between."""
     if not _check_fused_supported(twin):
         return coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m)
     g = twin.grid
@@ -302,37 +352,44 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     p = twin._fused_params
     if p is None:
         p = twin._fused_params = step_params(twin)
+        twin.__dict__["_graphs"] = {}
     p.arc_i, p.arc_j = arc_i, arc_j
     p.welding = 1 if is_welding else 0
     p.forces_from_buffer = 0
+    p.clear_forces = 1 if getattr(g, "_forces_dirty", True) else 0
     dx_, dy_, dz_ = getattr(twin, "_torch_dir_xyz", (1.0, 0.0, 0.0))
     p.dir_x, p.dir_y, p.dir_z = dx_, dy_, dz_
-    f = _fields(g)
+    f = _fields_cached(g)
     ws = g.workspace
-    stream = torch.cuda.current_stream().cuda_stream
     upload_position(twin, arc_i, arc_j)
-    _native.call("waam_step_pre", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(), ws.numel(),
-                 stream)
     twin._last_arc_ijk = _LazyArc(g, arc_i, arc_j)
-    if is_welding and twin.droplet_freq > 0:
-        sim_time = twin._step_n * g.dt
-        if sim_time - twin._last_droplet_time >= deposition.droplet_period_s(twin):
+    events = getattr(twin, "_stage_events", None)
+    due = _droplet_due(twin, g, is_welding)
+    done = False
+    if not due and events is None and getattr(twin, "use_cuda_graphs", True):
+        key = (g._read_buf is g.f_a, g._cur, p.welding, p.clear_forces,
+               (dx_, dy_, dz_) if twin.enable_bead_freeze else None)
+        done = _run_graph(twin, g, f, p, ws, key)
+    if not done:
+        stream = torch.cuda.current_stream().cuda_stream
+        _native.call("waam_step_pre", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(),
+                     ws.numel(), stream)
+        if due:
             arc_k = float(g.step_scalars[0].item())
             forces.clear_forces(g.Fx, g.Fy, g.Fz)
             _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m)
             p.forces_from_buffer = 1
-    events = getattr(twin, "_stage_events", None)
-    if events is None:
-        _native.call("waam_step_main", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(),
-                     ws.numel(), stream)
-    else:
-        # stage timing for measurement: 7 cudaEvent handles recorded in-stream
-        handles = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
-        _native.call("waam_step_main_events", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(),
-                     ws.numel(), handles, len(events), stream)
-        cb = getattr(twin, "_stage_callback", None)
-        if cb is not None:
-            cb()
+            p.clear_forces = 0
+        if events is None:
+            _native.call("waam_step_main", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(),
+                         ws.numel(), stream)
+        else:
+            # stage timing for measurement: 7 cudaEvent handles recorded in-stream
+            handles = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
+            _native.call("waam_step_main_events", ctypes.byref(f), ctypes.byref(p),
+                         ws.data_ptr(), ws.numel(), handles, len(events), stream)
+    # the droplet impact load stays in F outside the active cells until the next step
+    g._forces_dirty = bool(p.forces_from_buffer)
     g.flip_thermal()
     g.swap_buffers()
     twin._step_n += 1

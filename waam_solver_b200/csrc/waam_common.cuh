@@ -39,12 +39,12 @@ __host__ __device__ constexpr float wq(int q) {
     return q == 0 ? 0.333333343f : (q < 7 ? 0.0555555560f : 0.0277777780f);
 }
 
+// Grids are limited to fewer than 2^31 cells (checked on the host), so a cell
+// index fits an int; population offsets q*n + c are formed in 64 bits.
 struct Dims {
     int nx, ny, nz;
     __host__ __device__ int64_t n() const { return (int64_t)nx * ny * nz; }
-    __host__ __device__ int64_t idx(int i, int j, int k) const {
-        return ((int64_t)i * ny + j) * nz + k;
-    }
+    __host__ __device__ int idx(int i, int j, int k) const { return (i * ny + j) * nz + k; }
     __device__ void ijk(int64_t c, int& i, int& j, int& k) const {
         k = (int)(c % nz);
         int64_t r = c / nz;
@@ -210,7 +210,7 @@ __device__ __forceinline__ float thermal_dh(const Dims d, const float* __restric
         ii = imax(0, imin(ii, d.nx - 1));
         jj = imax(0, imin(jj, d.ny - 1));
         kk = imax(0, imin(kk, d.nz - 1));
-        int64_t c = d.idx(ii, jj, kk);
+        int c = d.idx(ii, jj, kk);
         float val = f[c];
         if (flags[c] == GAS) val = fb;
         return val;
@@ -251,11 +251,13 @@ __device__ __forceinline__ float vof_flux(const Dims d, const float* __restrict_
                                           const int32_t* __restrict__ flags, int i0, int j0,
                                           int k0, int i1, int j1, int k1) {
     float flux = 0.0f;
-    int ii0 = (i0 + d.nx) % d.nx, ii1 = (i1 + d.nx) % d.nx;
+    // x is periodic: i0, i1 lie in [-1, nx]
+    int ii0 = i0 < 0 ? i0 + d.nx : (i0 >= d.nx ? i0 - d.nx : i0);
+    int ii1 = i1 < 0 ? i1 + d.nx : (i1 >= d.nx ? i1 - d.nx : i1);
     bool in0 = j0 >= 0 && k0 >= 0 && j0 < d.ny && k0 < d.nz;
     bool in1 = j1 >= 0 && k1 >= 0 && j1 < d.ny && k1 < d.nz;
     if (in0 && in1) {
-        int64_t c0 = d.idx(ii0, j0, k0), c1 = d.idx(ii1, j1, k1);
+        int c0 = d.idx(ii0, j0, k0), c1 = d.idx(ii1, j1, k1);
         int fl0 = flags[c0], fl1 = flags[c1];
         if (fl0 != SOLID && fl1 != SOLID) {
             float u0 = 0.0f, u1 = 0.0f;

@@ -2,10 +2,15 @@
 // plus the column, streaming and deposition kernels shared with the
 // operator API.
 //
-// Per step (no droplet):  surface-height -> arc weight sum -> inject + cap
+// Per step (no droplet):  surface height -> arc weight sum -> inject + cap
 // -> thermal (advect/diffuse, losses, phase, T_max, cooling rate)
-// -> VOF advect+reinit -> column pass (contact angle, flags, sync, time above)
-// -> forces + collide + Mach clamp -> stream -> [remelt / solidify].
+// -> VOF advect+reinit -> column pass (contact angle, flags, sync, time above,
+//    active-cell list) -> forces + collide + Mach clamp over the active list
+// -> stream -> [remelt / solidify].
+//
+// Cell kernels use 32x8 (k, j) tiles with one grid z-slice per i, so the cell
+// coordinates come from the launch geometry without integer division, and
+// consecutive lanes touch consecutive k (coalesced, k is the fastest axis).
 #include <cmath>
 
 #include "../../include/waam_b200.h"
@@ -18,6 +23,25 @@ namespace waam {
 
 #define STREAM(s) reinterpret_cast<cudaStream_t>(s)
 constexpr int kMainEvents = 7;
+constexpr int kTileK = 32;
+constexpr int kTileJ = 8;
+constexpr int kTileRedBlocks = 592;   // <= kWsMaxPartials
+constexpr int kListThreads = 128;
+constexpr int kListBlocks = 148 * 6;
+
+inline dim3 tile_grid(const Dims& d) {
+    return dim3((d.nz + kTileK - 1) / kTileK, (d.ny + kTileJ - 1) / kTileJ, d.nx);
+}
+inline dim3 tile_block() { return dim3(kTileK, kTileJ, 1); }
+
+__device__ __forceinline__ bool tile_cell(const Dims& d, int& i, int& j, int& k, int& c) {
+    k = blockIdx.x * kTileK + threadIdx.x;
+    j = blockIdx.y * kTileJ + threadIdx.y;
+    i = blockIdx.z;
+    if (k >= d.nz || j >= d.ny) return false;
+    c = (i * d.ny + j) * d.nz + k;
+    return true;
+}
 
 // ---------------------------------------------------------------------------
 // Contact-angle ghost-phi BC (kernels.py:933-991), one warp per (i, j)
@@ -67,8 +91,9 @@ __device__ __forceinline__ float contact_rules(const ContactConst& cc, float sta
     return v;
 }
 
-// Runs the column pass for one warp; `emit(k, c, value, flag_old)` is called
-// for every cell of the column (value = final phi, or snap for solid cells).
+// Runs the column pass for one warp; `emit(k, c, value, flag_old, valid)` is
+// called by every lane of every chunk (convergent), value = final phi (snap
+// for solid cells).
 template <class Emit>
 __device__ __forceinline__ void contact_column(const Dims d, const float* __restrict__ snap,
                                                const int32_t* __restrict__ flags, int i, int j,
@@ -77,14 +102,15 @@ __device__ __forceinline__ void contact_column(const Dims d, const float* __rest
     int carry_flag = SOLID;      // old flag of the cell below the chunk
     float carry_final = 0.0f;    // final phi of the cell below the chunk
     float carry_ghost = -1.0f;   // ghost value written into the chunk's first cell (<0: none)
+    const int sx = d.ny * d.nz;
     for (int k0 = 0; k0 < d.nz; k0 += 32) {
         int k = k0 + lane;
         bool valid = k < d.nz;
-        int64_t c = d.idx(i, j, valid ? k : d.nz - 1);
+        int c = d.idx(i, j, valid ? k : d.nz - 1);
         float s = valid ? snap[c] : 0.0f;
         int flag = valid ? flags[c] : SOLID;
         if (!wetting) {
-            if (valid) emit(k, c, s, flag);
+            emit(k, c, s, flag, valid);
             continue;
         }
         int flag_up = (valid && k + 1 < d.nz) ? flags[c + 1] : SOLID;
@@ -96,7 +122,6 @@ __device__ __forceinline__ void contact_column(const Dims d, const float* __rest
         if (valid && flag != SOLID) {
             if (j - 1 >= 0 && snap[c - d.nz] > 0.55f) any_nb = true;
             if (j + 1 < d.ny && snap[c + d.nz] > 0.55f) any_nb = true;
-            int64_t sx = (int64_t)d.ny * d.nz;
             if (i - 1 >= 0 && snap[c - sx] > 0.55f) any_nb = true;
             if (i + 1 < d.nx && snap[c + sx] > 0.55f) any_nb = true;
         }
@@ -127,7 +152,7 @@ __device__ __forceinline__ void contact_column(const Dims d, const float* __rest
             cur = nv;
             if (!__any_sync(0xffffffffu, changed)) break;
         }
-        if (valid) emit(k, c, cur, flag);
+        emit(k, c, cur, flag, valid);
         carry_flag = __shfl_sync(0xffffffffu, flag, 31);
         carry_final = __shfl_sync(0xffffffffu, cur, 31);
         carry_ghost = __shfl_sync(0xffffffffu, ghost_out, 31);
@@ -140,8 +165,8 @@ __global__ void k_contact_op(Dims d, const float* __restrict__ snap, float* __re
     if (warp >= d.nx * d.ny) return;
     int i = warp / d.ny, j = warp % d.ny;
     ContactConst cc = contact_const(cos_t, sin_t);
-    contact_column(d, snap, flags, i, j, true, cc, [&](int k, int64_t c, float v, int flag) {
-        if (flag != SOLID) phi[c] = v;
+    contact_column(d, snap, flags, i, j, true, cc, [&](int k, int c, float v, int flag, bool valid) {
+        if (valid && flag != SOLID) phi[c] = v;
     });
 }
 
@@ -157,25 +182,31 @@ int launch_contact_columns(Dims d, const float* snap, float* phi, const int32_t*
 
 // ---------------------------------------------------------------------------
 // Pull streaming (kernels.py:2971-3010): x periodic, y/z clamped, bounce-back
-// from SOLID sources for non-gas cells.  One thread per cell, k fastest.
+// from SOLID sources for non-gas cells.  Interior cells (no wrap or clamp on
+// any axis) use fixed neighbour offsets; boundary cells take the general path.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_stream(Dims d, const float* __restrict__ f_src,
-                                                     float* __restrict__ f_dst,
-                                                     const int32_t* __restrict__ flags) {
-    const int64_t n = d.n();
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
+__global__ void __launch_bounds__(256) k_stream(Dims d, const float* __restrict__ f_src,
+                                                float* __restrict__ f_dst,
+                                                const int32_t* __restrict__ flags) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
     const int flag = flags[c];
     if (flag == SOLID) return;
-    int i, j, k;
-    d.ijk(c, i, j, k);
+    const size_t n = (size_t)d.n();
+    const int sy = d.nz, sx = d.ny * d.nz;
+    const bool interior = i > 0 && i < d.nx - 1 && j > 0 && j < d.ny - 1 && k > 0 && k < d.nz - 1;
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
-        int ni = i - ex(q);
-        ni = ni < 0 ? ni + d.nx : (ni >= d.nx ? ni - d.nx : ni);
-        int nj = imax(0, imin(j - ey(q), d.ny - 1));
-        int nk = imax(0, imin(k - ez(q), d.nz - 1));
-        int64_t s = d.idx(ni, nj, nk);
+        int s;
+        if (interior) {
+            s = c - (ex(q) * sx + ey(q) * sy + ez(q));
+        } else {
+            int ni = i - ex(q);
+            ni = ni < 0 ? ni + d.nx : (ni >= d.nx ? ni - d.nx : ni);
+            int nj = imax(0, imin(j - ey(q), d.ny - 1));
+            int nk = imax(0, imin(k - ez(q), d.nz - 1));
+            s = (ni * d.ny + nj) * d.nz + nk;
+        }
         float v;
         if (flag == GAS || flags[s] != SOLID)
             v = f_src[q * n + s];
@@ -186,9 +217,7 @@ __global__ void __launch_bounds__(kThreads) k_stream(Dims d, const float* __rest
 }
 
 int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags, void* stream) {
-    int64_t n = d.n();
-    int blocks = (int)((n + kThreads - 1) / kThreads);
-    k_stream<<<blocks, kThreads, 0, STREAM(stream)>>>(d, f_src, f_dst, flags);
+    k_stream<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(d, f_src, f_dst, flags);
     return check_launch("k_stream");
 }
 
@@ -205,7 +234,7 @@ __device__ bool has_metal_nb(const Dims d, const float* phi, const int32_t* flag
     for (int m = 0; m < 6; ++m) {
         int ii = i + dd[m][0], jj = j + dd[m][1], kk = k + dd[m][2];
         if (ii >= 0 && jj >= 0 && kk >= 0 && ii < d.nx && jj < d.ny && kk < d.nz) {
-            int64_t c = d.idx(ii, jj, kk);
+            int c = d.idx(ii, jj, kk);
             if (flags[c] == FLUID || flags[c] == SOLID)
                 found = true;
             else if (phi[c] > 0.35f || f_l[c] > 0.2f)
@@ -220,7 +249,7 @@ __global__ void k_deposit(Dims d, float* f_src, int32_t* flags, float* f_l, floa
                           float drop_r, float target_vol, float T_drop, float cp_rho, float L_rho,
                           float rho0, float* vol_acc, float* real_acc, float cell_vol) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const int64_t n = d.n();
+    const size_t n = (size_t)d.n();
     float sr = fmax_(foot_r, drop_r);
     int i0 = imax(0, (int)(arc_i - sr)), i1 = imin(d.nx, (int)(arc_i + sr) + 1);
     int j0 = imax(0, (int)(arc_j - sr)), j1 = imin(d.ny, (int)(arc_j + sr) + 1);
@@ -236,7 +265,7 @@ __global__ void k_deposit(Dims d, float* f_src, int32_t* flags, float* f_l, floa
             for (int j = j0; j < j1; ++j)
                 for (int k = k0; k < k1; ++k) {
                     if (vol >= target_vol) continue;
-                    int64_t c = d.idx(i, j, k);
+                    int c = d.idx(i, j, k);
                     if (flags[c] != GAS) continue;
                     if (!has_metal_nb(d, phi, flags, f_l, i, j, k)) continue;
                     float di = (float)i - arc_i, dj = (float)j - arc_j;
@@ -266,7 +295,7 @@ __global__ void k_deposit(Dims d, float* f_src, int32_t* flags, float* f_l, floa
     for (int i = i0; i < i1; ++i)
         for (int j = j0; j < j1; ++j)
             for (int k = k0; k < k1; ++k) {
-                int64_t c = d.idx(i, j, k);
+                int c = d.idx(i, j, k);
                 if (flags[c] != FLUID || f_l[c] < 0.45f) continue;
                 float di = (float)i - arc_i, dj = (float)j - arc_j;
                 if (di * di + dj * dj > foot2 * 1.44f) continue;
@@ -294,7 +323,7 @@ int launch_deposit(Dims d, float* f_src, int32_t* flags, float* f_l, float* phi,
 // ---------------------------------------------------------------------------
 
 // Surface height at the torch column + the arc-k fallback of
-// solvers/coupled_step.py:34-59 -> scalars[0].
+// solvers/coupled_step.py:34-59 -> scalars[kScalarArcK].
 __global__ void k_surface_arc(Dims d, const float* phi, const int32_t* flags, float* scalars,
                               int nz_solid) {
     float arc_i = scalars[kScalarArcI], arc_j = scalars[kScalarArcJ];
@@ -302,7 +331,7 @@ __global__ void k_surface_arc(Dims d, const float* phi, const int32_t* flags, fl
     int j0 = imax(0, imin((int)arc_j, d.ny - 1));
     int best = -1;
     for (int k = threadIdx.x; k < d.nz; k += 32) {
-        int64_t c = d.idx(i0, j0, k);
+        int c = d.idx(i0, j0, k);
         if (flags[c] != GAS && phi[c] > 0.05f) best = k;
     }
     for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_down_sync(0xffffffffu, best, o));
@@ -310,8 +339,96 @@ __global__ void k_surface_arc(Dims d, const float* phi, const int32_t* flags, fl
         int ks = best >= 0 ? best : imax(1, nz_solid - 1);
         float kf = (float)ks;
         if (kf < 1.0f) kf = (float)imax(1, nz_solid - 1);
-        scalars[0] = kf;
+        scalars[kScalarArcK] = kf;
     }
+}
+
+__device__ double tile_block_sum(double v) {
+    __shared__ double sh[(kTileK * kTileJ) / 32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int t = threadIdx.y * kTileK + threadIdx.x;
+    if ((t & 31) == 0) sh[t >> 5] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (t == 0)
+        for (int w = 0; w < (kTileK * kTileJ) / 32; ++w) s += sh[w];
+    __syncthreads();
+    return s;
+}
+
+// Arc weight sum over 32x8 tiles (pass 1 of kernels.py:443-510 / 548-622),
+// deterministic: fixed tile-to-block assignment, double partials, the last
+// block sums them in order.  Writes the weight sum and the energy per weight.
+__global__ void __launch_bounds__(256) k_arc_norm_tiles(Dims d, const int32_t* __restrict__ flags,
+                                                        const float* __restrict__ f_l, ArcParams p,
+                                                        float* scalars, float arc_k_offset,
+                                                        float Qe_dt, float dx3, Workspace ws) {
+    p.arc_k = scalars[kScalarArcK] + arc_k_offset;
+    p.arc_i = scalars[kScalarArcI];
+    p.arc_j = scalars[kScalarArcJ];
+    const int kt = (d.nz + kTileK - 1) / kTileK, jt = (d.ny + kTileJ - 1) / kTileJ;
+    const int tiles = kt * jt * d.nx;
+    double part = 0.0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        int a = t % kt, r = t / kt;
+        int b = r % jt, i = r / jt;
+        int k = a * kTileK + threadIdx.x, j = b * kTileJ + threadIdx.y;
+        if (k >= d.nz || j >= d.ny) continue;
+        int c = (i * d.ny + j) * d.nz + k;
+        int flag = flags[c];
+        if (flag == GAS) continue;
+        part += (double)arc_cell_weight(p, i, j, k, flag, f_l[c]);
+    }
+    part = tile_block_sum(part);
+    __shared__ bool last;
+    int t0 = threadIdx.y * kTileK + threadIdx.x;
+    if (t0 == 0) {
+        ws.partials[blockIdx.x] = part;
+        __threadfence();
+        unsigned prev = atomicAdd(ws.counter, 1u);
+        last = prev == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    // the last block sums the partials: fixed strided assignment + fixed tree
+    __threadfence();
+    double acc = 0.0;
+    for (unsigned bb = t0; bb < gridDim.x; bb += kTileK * kTileJ)
+        acc += ((volatile double*)ws.partials)[bb];
+    double tot = tile_block_sum(acc);
+    if (t0 == 0) {
+        *ws.counter = 0u;
+        float w_total = (float)tot;
+        float epw = 0.0f;
+        if (w_total > 1e-9f) epw = Qe_dt / (w_total * dx3);
+        scalars[kScalarWsum] = w_total;
+        scalars[kScalarEpw] = epw;
+    }
+}
+
+// Pass 2: H += epw * weight (non-gas cells), then the enthalpy ceiling
+// (solvers/coupled_step.py:107-108).
+__global__ void __launch_bounds__(256) k_arc_inject_tiles(Dims d, float* __restrict__ H,
+                                                          const int32_t* __restrict__ flags,
+                                                          const float* __restrict__ f_l,
+                                                          ArcParams p, const float* scalars,
+                                                          float arc_k_offset, int cap,
+                                                          PhaseParams ph) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
+    int flag = flags[c];
+    if (flag == GAS) return;
+    p.arc_k = scalars[kScalarArcK] + arc_k_offset;
+    p.arc_i = scalars[kScalarArcI];
+    p.arc_j = scalars[kScalarArcJ];
+    float epw = scalars[kScalarEpw];
+    float dh;
+    bool hit = arc_cell_heat(p, epw, i, j, k, flag, f_l[c], dh);
+    if (!hit && !cap) return;
+    float h = H[c];
+    if (hit) h = h + dh;
+    if (cap) h = cap_h(ph, h);
+    H[c] = h;
 }
 
 struct ThermalArgs {
@@ -325,21 +442,22 @@ struct ThermalArgs {
 // 2030-2082 + 1937-1950 (losses, floor), 1519-1556 twice around the ceiling
 // 1953-1984 (only the second update_phase is observable), 3016-3032 (T_max),
 // 2013-2027 (cooling rate).  H and T are double-buffered so neighbour reads
-// see the pre-stage values.
-__global__ void __launch_bounds__(kThreads) k_thermal_fused(
+// see the pre-stage values.  Also resets the active-cell shard counters of the step.
+__global__ void __launch_bounds__(256) k_thermal_fused(
     Dims d, const float* __restrict__ H, float* __restrict__ H_next, const float* __restrict__ T,
     float* __restrict__ T_next, float* __restrict__ f_l, const float* __restrict__ ux,
     const float* __restrict__ uy, const float* __restrict__ uz, const int32_t* __restrict__ flags,
     float* __restrict__ T_max, float* __restrict__ T_prev, float* __restrict__ dT_dt,
-    ThermalArgs a) {
-    const int64_t n = d.n();
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
+    unsigned* active_count, ThermalArgs a) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
+        const int t = threadIdx.y * kTileK + threadIdx.x;
+        if (t < kActiveShards) active_count[t] = 0u;
+    }
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
     const int flag = flags[c];
     float h = H[c];
     if (flag != GAS) {
-        int i, j, k;
-        d.ijk(c, i, j, k);
         float u = 0.0f, v = 0.0f, w = 0.0f;
         if (flag != SOLID) {
             u = ux[c];
@@ -349,10 +467,10 @@ __global__ void __launch_bounds__(kThreads) k_thermal_fused(
         h = h + thermal_dh(d, H, T, flags, u, v, w, i, j, k, flag, h, a.cpa, a.dt_lu);
         if (a.heat_loss) {
             int ne = 0;
+            const int sx = d.ny * d.nz;
             if (k + 1 < d.nz && flags[c + 1] == GAS) ne++;
             if (j + 1 < d.ny && flags[c + d.nz] == GAS) ne++;
             if (j - 1 >= 0 && flags[c - d.nz] == GAS) ne++;
-            int64_t sx = (int64_t)d.ny * d.nz;
             if (i + 1 < d.nx && flags[c + sx] == GAS) ne++;
             if (i - 1 >= 0 && flags[c - sx] == GAS) ne++;
             if (ne != 0) {
@@ -383,19 +501,33 @@ __global__ void __launch_bounds__(kThreads) k_thermal_fused(
     }
 }
 
-// VOF advection + reinitialisation (kernels.py:2320-2391) -> phi_tmp.
-__global__ void __launch_bounds__(kThreads) k_vof_advect(Dims d, const float* __restrict__ phi,
-                                                         float* __restrict__ phi_tmp,
-                                                         const float* __restrict__ ux,
-                                                         const float* __restrict__ uy,
-                                                         const float* __restrict__ uz,
-                                                         const int32_t* __restrict__ flags) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= d.n()) return;
-    int i, j, k;
-    d.ijk(c, i, j, k);
-    int flag = flags[c];
-    float p = advect_phi_cell(d, phi, ux, uy, uz, flags, i, j, k, flag);
+// VOF advection + reinitialisation (kernels.py:2320-2391) -> phi_tmp.  A gas
+// cell whose six face neighbours are gas (or outside y/z) has zero velocity on
+// every face, so all fluxes vanish and phi_tmp = reinit(phi) exactly.
+__global__ void __launch_bounds__(256) k_vof_advect(Dims d, const float* __restrict__ phi,
+                                                    float* __restrict__ phi_tmp,
+                                                    const float* __restrict__ ux,
+                                                    const float* __restrict__ uy,
+                                                    const float* __restrict__ uz,
+                                                    const int32_t* __restrict__ flags) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
+    const int flag = flags[c];
+    float p = phi[c];
+    if (flag == GAS) {
+        const int sx = d.ny * d.nz;
+        int im = i > 0 ? c - sx : c + (d.nx - 1) * sx;
+        int ip = i < d.nx - 1 ? c + sx : c - (d.nx - 1) * sx;
+        // all six loads issued together (no short-circuit chain of dependent loads)
+        const int fa = flags[im], fb = flags[ip];
+        const int fc = j > 0 ? flags[c - d.nz] : GAS, fd = j < d.ny - 1 ? flags[c + d.nz] : GAS;
+        const int fe = k > 0 ? flags[c - 1] : GAS, ff = k < d.nz - 1 ? flags[c + 1] : GAS;
+        const bool quiet = ((fa == GAS) & (fb == GAS) & (fc == GAS) & (fd == GAS) & (fe == GAS) &
+                            (ff == GAS)) != 0;
+        if (!quiet) p = advect_phi_cell(d, phi, ux, uy, uz, flags, i, j, k, flag);
+    } else if (flag != SOLID) {
+        p = advect_phi_cell(d, phi, ux, uy, uz, flags, i, j, k, flag);
+    }
     phi_tmp[c] = reinit_phi(p, flag);
 }
 
@@ -403,42 +535,75 @@ struct ColumnArgs {
     int vof, wetting, nz_solid;
     float cos_t, sin_t;
     float dt_phys, T800, T1100, Ts;
+    int zero_forces;  // keep F == 0 outside the active cells (see k_collide_list)
+    int clear_all;    // the previous step left forces outside the active set
+    int shard_cap;    // list slots per shard: ceil(nx*ny / kActiveShards) * nz
 };
+
+__device__ __forceinline__ bool is_active(int flag) { return flag == FLUID || flag == IFACE; }
 
 // Column pass: contact-angle BC (kernels.py:933-991) on phi_tmp, flags from
 // phi (2394-2419), phi/f_l sync (3484-3504) and time-above-T (3261-3283,
 // which runs after collide/stream in the reference but only reads T and the
-// post-VOF flags).
-__global__ void __launch_bounds__(kThreads) k_column(Dims d, const float* __restrict__ phi_tmp,
-                                                     float* __restrict__ phi,
-                                                     int32_t* __restrict__ flags,
-                                                     float* __restrict__ f_l,
-                                                     const float* __restrict__ T,
-                                                     float* __restrict__ t800,
-                                                     float* __restrict__ t1100,
-                                                     float* __restrict__ tsol, ColumnArgs a) {
+// post-VOF flags).  Appends every FLUID/IFACE cell to the active list
+// (column c goes to shard c % 64, in k order within a warp) and zeroes the
+// force of cells leaving the active set.
+__global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict__ phi_tmp,
+                                                float* __restrict__ phi,
+                                                int32_t* __restrict__ flags,
+                                                float* __restrict__ f_l,
+                                                const float* __restrict__ T,
+                                                float* __restrict__ t800,
+                                                float* __restrict__ t1100,
+                                                float* __restrict__ tsol, float* __restrict__ Fx,
+                                                float* __restrict__ Fy, float* __restrict__ Fz,
+                                                int* __restrict__ active_list,
+                                                unsigned* __restrict__ active_count,
+                                                ColumnArgs a) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (warp >= d.nx * d.ny) return;
+    const int lane = threadIdx.x & 31;
     int i = warp / d.ny, j = warp % d.ny;
     ContactConst cc = contact_const(a.cos_t, a.sin_t);
     const float* src = a.vof ? phi_tmp : phi;
     contact_column(d, src, flags, i, j, a.vof && a.wetting, cc,
-                   [&](int k, int64_t c, float v, int flag_old) {
+                   [&](int k, int c, float v, int flag_old, bool valid) {
                        int flag = flag_old;
-                       if (a.vof) {
-                           float fl = f_l[c];
-                           flag = flag_from(v, fl, k, a.nz_solid);
-                           phi[c] = v;
-                           flags[c] = flag;
-                           if (flag == GAS || v < 0.05f || flag == SOLID) {
-                               if (fl != 0.0f) f_l[c] = 0.0f;
+                       if (valid) {
+                           if (a.vof) {
+                               float fl = f_l[c];
+                               flag = flag_from(v, fl, k, a.nz_solid);
+                               phi[c] = v;
+                               flags[c] = flag;
+                               if (flag == GAS || v < 0.05f || flag == SOLID) {
+                                   if (fl != 0.0f) f_l[c] = 0.0f;
+                               }
+                           }
+                           if (flag != GAS) {
+                               float t = T[c];
+                               if (t >= a.T800) t800[c] += a.dt_phys;
+                               if (t >= a.T1100) t1100[c] += a.dt_phys;
+                               if (t >= a.Ts) tsol[c] += a.dt_phys;
+                           }
+                           if (a.zero_forces && !is_active(flag) &&
+                               (a.clear_all || is_active(flag_old))) {
+                               Fx[c] = 0.0f;
+                               Fy[c] = 0.0f;
+                               Fz[c] = 0.0f;
                            }
                        }
-                       if (flag != GAS) {
-                           float t = T[c];
-                           if (t >= a.T800) t800[c] += a.dt_phys;
-                           if (t >= a.T1100) t1100[c] += a.dt_phys;
-                           if (t >= a.Ts) tsol[c] += a.dt_phys;
+                       bool act = valid && is_active(flag);
+                       unsigned m = __ballot_sync(0xffffffffu, act);
+                       if (m) {
+                           // one counter per shard of columns keeps the atomics spread out
+                           const int shard = warp & (kActiveShards - 1);
+                           unsigned base = 0;
+                           if (lane == 0)
+                               base = atomicAdd(active_count + shard, (unsigned)__popc(m));
+                           base = __shfl_sync(0xffffffffu, base, 0);
+                           if (act)
+                               active_list[(int64_t)shard * a.shard_cap + base +
+                                           __popc(m & ((1u << lane) - 1u))] = c;
                        }
                    });
 }
@@ -449,75 +614,94 @@ struct CollideArgs {
     float omega, omega_b, C_darcy, u_cap;
 };
 
-// Body forces + collision + Mach clamp for FLUID/IFACE cells
-// (solvers/coupled_step.py:298-402); forces stay in registers and are
-// written once as the step's force field (== the reference's F_snap).
-__global__ void __launch_bounds__(kThreads) k_collide_fused(
+// Body forces + collision + Mach clamp over the active (FLUID/IFACE) cells
+// listed by k_column, shard after shard (solvers/coupled_step.py:298-402).  Forces stay in
+// registers and are written once as the step's force field (== the
+// reference's F_snap); every other cell keeps F == 0.
+__global__ void __launch_bounds__(kListThreads) k_collide_list(
     Dims d, const float* __restrict__ f_src, float* __restrict__ f_dst, float* __restrict__ rho,
     float* __restrict__ ux, float* __restrict__ uy, float* __restrict__ uz,
     float* __restrict__ Fx, float* __restrict__ Fy, float* __restrict__ Fz,
     const float* __restrict__ phi, const float* __restrict__ T, const float* __restrict__ f_l,
-    const int32_t* __restrict__ flags, const float* __restrict__ scalars, CollideArgs a) {
-    const int64_t n = d.n();
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    const int flag = flags[c];
-    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-    if (a.from_buffer) {
-        fx = Fx[c];
-        fy = Fy[c];
-        fz = Fz[c];
-    }
-    if (flag == SOLID || flag == GAS) {
-        if (!a.from_buffer) {
-            Fx[c] = 0.0f;
-            Fy[c] = 0.0f;
-            Fz[c] = 0.0f;
+    const int32_t* __restrict__ flags, const float* __restrict__ scalars,
+    const int* __restrict__ active_list, const unsigned* __restrict__ active_count,
+    int shard_cap, CollideArgs a) {
+    const size_t n = (size_t)d.n();
+    __shared__ unsigned start[kActiveShards + 1];
+    if (threadIdx.x < 32) {
+        // exclusive prefix of the 64 shard counts (two per lane)
+        unsigned c0 = active_count[2 * threadIdx.x], c1 = active_count[2 * threadIdx.x + 1];
+        unsigned v = c0 + c1, incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (threadIdx.x >= o) incl += y;
         }
-        return;
+        unsigned excl = incl - v;
+        start[2 * threadIdx.x] = excl;
+        start[2 * threadIdx.x + 1] = excl + c0;
+        if (threadIdx.x == 31) start[kActiveShards] = incl;
     }
-    int i, j, k;
-    d.ijk(c, i, j, k);
+    __syncthreads();
+    const unsigned cnt = start[kActiveShards];
     ForceParams P = a.P;
     P.arc_k = scalars[kScalarArcK];
     P.arc_i = scalars[kScalarArcI];
     P.arc_j = scalars[kScalarArcJ];
-    float fl = f_l[c];
-    cell_forces(d, P, phi, T, flags, i, j, k, fl, fx, fy, fz);
-    float f[19], o[19];
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt;
+         t += gridDim.x * blockDim.x) {
+        int lo = 0, hi = kActiveShards;  // last shard with start <= t
+        while (hi - lo > 1) {
+            int mid = (lo + hi) >> 1;
+            if (start[mid] <= t) lo = mid; else hi = mid;
+        }
+        const int c = active_list[(int64_t)lo * shard_cap + (t - start[lo])];
+        const int k = c % d.nz;
+        const int r = c / d.nz;
+        const int j = r % d.ny;
+        const int i = r / d.ny;
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        if (a.from_buffer) {
+            fx = Fx[c];
+            fy = Fy[c];
+            fz = Fz[c];
+        }
+        float fl = f_l[c];
+        cell_forces(d, P, phi, T, flags, i, j, k, fl, fx, fy, fz);
+        float f[19], o[19];
 #pragma unroll
-    for (int q = 0; q < 19; ++q) f[q] = f_src[q * n + c];
-    float r, u, v, w;
-    if (a.kind == 0)
-        collide_mrt_cell(f, fl, fx, fy, fz, a.omega, a.omega_b, a.C_darcy, o, r, u, v, w);
-    else
-        collide_srt_cell(f, fl, fx, fy, fz, a.omega, a.C_darcy, o, r, u, v, w);
+        for (int q = 0; q < 19; ++q) f[q] = f_src[q * n + c];
+        float rr, u, v, w;
+        if (a.kind == 0)
+            collide_mrt_cell(f, fl, fx, fy, fz, a.omega, a.omega_b, a.C_darcy, o, rr, u, v, w);
+        else
+            collide_srt_cell(f, fl, fx, fy, fz, a.omega, a.C_darcy, o, rr, u, v, w);
 #pragma unroll
-    for (int q = 0; q < 19; ++q) f_dst[q * n + c] = o[q];
-    if (a.u_cap > 0.0f) clamp_mach(u, v, w, a.u_cap);
-    rho[c] = r;
-    ux[c] = u;
-    uy[c] = v;
-    uz[c] = w;
-    Fx[c] = fx;
-    Fy[c] = fy;
-    Fz[c] = fz;
+        for (int q = 0; q < 19; ++q) f_dst[q * n + c] = o[q];
+        if (a.u_cap > 0.0f) clamp_mach(u, v, w, a.u_cap);
+        rho[c] = rr;
+        ux[c] = u;
+        uy[c] = v;
+        uz[c] = w;
+        Fx[c] = fx;
+        Fy[c] = fy;
+        Fz[c] = fz;
+    }
 }
 
 struct TailArgs {
     float cp_rho, Ts, Tl, L_rho;
     int remelt, trailing, cooled;
-    float arc_i, arc_j, dir_x, dir_y, dir_z, lookback, T_freeze;
+    float dir_x, dir_y, dir_z, lookback, T_freeze;
 };
 
 // solvers/coupled_step.py:426-458: remelt_hot_solid_scalar (kernels.py:2489),
 // solidify_trailing_pool_scalar (2573), solidify_cooled_metal (2422); all
 // per cell, applied in the reference order.
-__global__ void k_tail(Dims d, float* T, float* H, float* f_l, float* phi, int32_t* flags,
-                       float* ux, float* uy, float* uz, const float* scalars, TailArgs a) {
-    const int64_t n = d.n();
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
+__global__ void __launch_bounds__(256) k_tail(Dims d, float* T, float* H, float* f_l, float* phi,
+                                              int32_t* flags, float* ux, float* uy, float* uz,
+                                              const float* scalars, TailArgs a) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
     int flag = flags[c];
     if (a.remelt && flag == SOLID) {
         float Tc = T[c];
@@ -538,8 +722,6 @@ __global__ void k_tail(Dims d, float* T, float* H, float* f_l, float* phi, int32
         }
     }
     if (a.trailing && flag != GAS && !(phi[c] < 0.85f || f_l[c] < 0.05f)) {
-        int i, j, k;
-        d.ijk(c, i, j, k);
         float arc_k = scalars[kScalarArcK];
         float di = (float)i - scalars[kScalarArcI], dj = (float)j - scalars[kScalarArcJ];
         float dk = (float)k - arc_k;
@@ -567,9 +749,6 @@ __global__ void k_tail(Dims d, float* T, float* H, float* f_l, float* phi, int32
 static ArcParams arc_params(const WaamStepParams* p) {
     ArcParams a{};
     a.kind = p->arc_kind;
-    a.arc_i = p->arc_i;
-    a.arc_j = p->arc_j;
-    a.arc_k = 0.0f;  // taken from the device scalar
     a.inv2s2 = 1.0f / (2.0f * p->sigma_heat * p->sigma_heat);
     a.sign = p->sign;
     a.ff = p->ff;
@@ -616,16 +795,16 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     if (e || !p->welding) return e;
     ArcParams a = arc_params(p);
     float Qe_dt = p->Q_w * p->eta * p->dt;
-    k_arc_norm<<<red_blocks(d.n()), kThreads, 0, STREAM(stream)>>>(
-        d, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, Qe_dt, p->dx3, nullptr,
-        f->step_scalars, ws);
-    e = check_launch("k_arc_norm");
+    const int tiles = (int)tile_grid(d).x * (int)tile_grid(d).y * d.nx;
+    const int blocks = tiles < kTileRedBlocks ? tiles : kTileRedBlocks;
+    k_arc_norm_tiles<<<blocks, tile_block(), 0, STREAM(stream)>>>(
+        d, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, Qe_dt, p->dx3, ws);
+    e = check_launch("k_arc_norm_tiles");
     if (e) return e;
     PhaseParams ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
-    k_arc_inject<<<elem_blocks(d.n()), kThreads, 0, STREAM(stream)>>>(
-        d, f->H, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, f->step_scalars,
-        p->cap_enabled, ph);
-    return check_launch("k_arc_inject");
+    k_arc_inject_tiles<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
+        d, f->H, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, p->cap_enabled, ph);
+    return check_launch("k_arc_inject_tiles");
 }
 
 int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace,
@@ -645,8 +824,13 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     Dims d{f->nx, f->ny, f->nz};
     if (!workspace_ok(workspace, workspace_bytes, d.n()))
         return fail(WAAM_ERR_INVALID, "step_main: workspace too small or misaligned");
-    const int64_t n = d.n();
-    const int cell_blocks = (int)((n + kThreads - 1) / kThreads);
+    Workspace ws = Workspace::at(workspace);
+    unsigned* active_count = ws.counter + kActiveShardSlot;
+    int* active_list = reinterpret_cast<int*>(ws.field);
+    const int64_t shard_cap =
+        ((int64_t)d.nx * d.ny + kActiveShards - 1) / kActiveShards * (int64_t)d.nz;
+    if (shard_cap * kActiveShards > d.n() + kFieldSlack || shard_cap > INT32_MAX)
+        return fail(WAAM_ERR_INVALID, "step_main: nz too large for the active-cell list");
     const int col_blocks = (int)(((int64_t)d.nx * d.ny * 32 + kThreads - 1) / kThreads);
     cudaStream_t s = STREAM(stream);
 
@@ -666,16 +850,16 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     ta.sigma_sb = p->sigma_sb;
     ta.h_floor = p->cp_rho * p->T_amb;
     mark(0);
-    k_thermal_fused<<<cell_blocks, kThreads, 0, s>>>(d, f->H, f->H_next, f->T, f->T_next, f->f_l,
-                                                     f->ux, f->uy, f->uz, f->flags, f->T_max,
-                                                     f->T_prev, f->dT_dt, ta);
+    k_thermal_fused<<<tile_grid(d), tile_block(), 0, s>>>(
+        d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
+        f->T_prev, f->dT_dt, active_count, ta);
     int e = check_launch("k_thermal_fused");
     if (e) return e;
     mark(1);
 
     if (p->vof) {
-        k_vof_advect<<<cell_blocks, kThreads, 0, s>>>(d, f->phi, f->phi_tmp, f->ux, f->uy, f->uz,
-                                                      f->flags);
+        k_vof_advect<<<tile_grid(d), tile_block(), 0, s>>>(d, f->phi, f->phi_tmp, f->ux, f->uy,
+                                                            f->uz, f->flags);
         e = check_launch("k_vof_advect");
         if (e) return e;
     }
@@ -690,8 +874,12 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     ca.T800 = p->T800;
     ca.T1100 = p->T1100;
     ca.Ts = p->Ts;
+    ca.zero_forces = p->forces_from_buffer ? 0 : 1;
+    ca.clear_all = p->clear_forces;
+    ca.shard_cap = (int)shard_cap;
     k_column<<<col_blocks, kThreads, 0, s>>>(d, f->phi_tmp, f->phi, f->flags, f->f_l, f->T_next,
-                                             f->t800, f->t1100, f->tsol, ca);
+                                             f->t800, f->t1100, f->tsol, f->Fx, f->Fy, f->Fz,
+                                             active_list, active_count, ca);
     e = check_launch("k_column");
     if (e) return e;
     mark(3);
@@ -706,9 +894,7 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     P.cos_t = (float)cos((double)p->theta);
     P.sin_t = (float)sin((double)p->theta);
     P.dgamma = p->dgamma_lu;
-    P.arc_i = p->arc_i;
-    P.arc_j = p->arc_j;
-    P.arc_k = 0.0f;
+    P.arc_i = P.arc_j = P.arc_k = 0.0f;  // from the device scalars
     P.p_inv2s2 = 1.0f / (2.0f * p->p_sigma * p->p_sigma + 1e-6f);
     float Fphys = p->pressure / (p->rho_phys * p->dx);
     P.p_Flu = Fphys * (p->dt * p->dt) / p->dx;
@@ -723,10 +909,11 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     cl.omega_b = p->omega_b;
     cl.C_darcy = p->C_darcy;
     cl.u_cap = p->u_cap;
-    k_collide_fused<<<cell_blocks, kThreads, 0, s>>>(d, f->f_src, f->f_dst, f->rho, f->ux, f->uy,
-                                                     f->uz, f->Fx, f->Fy, f->Fz, f->phi, f->T_next,
-                                                     f->f_l, f->flags, f->step_scalars, cl);
-    e = check_launch("k_collide_fused");
+    k_collide_list<<<kListBlocks, kListThreads, 0, s>>>(
+        d, f->f_src, f->f_dst, f->rho, f->ux, f->uy, f->uz, f->Fx, f->Fy, f->Fz, f->phi,
+        f->T_next, f->f_l, f->flags, f->step_scalars, active_list, active_count, (int)shard_cap,
+        cl);
+    e = check_launch("k_collide_list");
     if (e) return e;
     mark(4);
 
@@ -743,15 +930,14 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
         t.remelt = 1;
         t.trailing = p->welding && p->bead_freeze;
         t.cooled = 1;
-        t.arc_i = p->arc_i;
-        t.arc_j = p->arc_j;
         t.dir_x = p->dir_x;
         t.dir_y = p->dir_y;
         t.dir_z = p->dir_z;
         t.lookback = p->lookback;
         t.T_freeze = p->T_freeze;
-        k_tail<<<cell_blocks, kThreads, 0, s>>>(d, f->T_next, f->H_next, f->f_l, f->phi, f->flags,
-                                                f->ux, f->uy, f->uz, f->step_scalars, t);
+        k_tail<<<tile_grid(d), tile_block(), 0, s>>>(d, f->T_next, f->H_next, f->f_l, f->phi,
+                                                      f->flags, f->ux, f->uy, f->uz,
+                                                      f->step_scalars, t);
         e = check_launch("k_tail");
     }
     mark(6);

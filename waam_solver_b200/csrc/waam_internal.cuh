@@ -12,13 +12,19 @@ constexpr int kMaxElemBlocks = 148 * 16;  // grid-stride cap: 16 CTAs per SM
 constexpr int kRedBlocks = 592;           // fixed so reduction order never depends on the GPU
 
 // Caller-provided workspace layout (waam_workspace_bytes):
-//   [0, 256)            unsigned counter of the last-block reduction
-//   [256, 8192)         double partial sums, one per reduction block
-//   [8192, 16384)       float scalars (arc k, weight sum, energy per weight, ...)
-//   [16384, ...)        one field-sized float scratch (snapshots)
-constexpr size_t kWsPartialsOffset = 256;
-constexpr size_t kWsScalarsOffset = 8192;
-constexpr size_t kWsFieldOffset = 16384;
+//   [0, 512)            unsigned counters: [0] last-block reduction,
+//                       [kActiveShardSlot, +kActiveShards) active-cell counts per shard
+//   [512, 1024)         float scalars of the operator-level reductions
+//   [1024, 33792)       double partial sums, one per reduction block (<= 4096)
+//   [33792, ...)        one field-sized scratch (n + kFieldSlack elements): a float
+//                       snapshot (operator API) or the int32 active-cell list (fused step)
+constexpr size_t kWsScalarsOffset = 512;
+constexpr size_t kWsPartialsOffset = 1024;
+constexpr int kWsMaxPartials = 4096;
+constexpr size_t kWsFieldOffset = 33792;
+constexpr int64_t kFieldSlack = 65536;
+constexpr int kActiveShards = 64;     // power of two
+constexpr int kActiveShardSlot = 64;  // first shard counter in the counter block
 
 // Slots of the fused step's device scalars (WaamFields::step_scalars).
 constexpr int kScalarArcK = 0;   // resolved arc k (written by the surface query)
@@ -28,7 +34,7 @@ constexpr int kScalarArcI = 4;   // torch x in cells (copied in by the host ever
 constexpr int kScalarArcJ = 5;   // torch y in cells
 
 struct Workspace {
-    unsigned* counter;
+    unsigned* counter;        // counter[0]: reduction, counter[kActiveCountSlot]: active cells
     double* partials;
     float* scalars;
     float* field;

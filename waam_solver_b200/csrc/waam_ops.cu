@@ -46,7 +46,10 @@ int red_blocks(int64_t n) {
     return (int)b;
 }
 
-bool dims_ok(int nx, int ny, int nz) { return nx > 0 && ny > 0 && nz > 0; }
+bool dims_ok(int nx, int ny, int nz) {
+    return nx > 0 && ny > 0 && nz > 0 && nx <= 65535 &&
+           (int64_t)nx * ny * nz < ((int64_t)1 << 31);
+}
 
 bool workspace_ok(void* ws, size_t bytes, int64_t n) {
     return ws != nullptr && bytes >= waam_workspace_bytes(n) &&
@@ -645,7 +648,7 @@ const char* waam_last_error(void) { return waam::g_last_error.c_str(); }
 int waam_abi_version(void) { return 1; }
 
 size_t waam_workspace_bytes(int64_t n) {
-    size_t field = (size_t)(n > 0 ? n : 0) * sizeof(float);
+    size_t field = (size_t)((n > 0 ? n : 0) + waam::kFieldSlack) * sizeof(float);
     field = (field + 255) & ~(size_t)255;
     return waam::kWsFieldOffset + field;
 }

@@ -128,6 +128,9 @@ class WAAMGrid:
             self.ensure_export_buffers()
         self._read_buf = self.f_a
         self._write_buf = self.f_b
+        # True when F may be non-zero outside FLUID/IFACE cells (the fused step
+        # then clears it; see WaamStepParams.clear_forces)
+        self._forces_dirty = True
 
     # -- optional fields (grid.py:228-262) --------------------------------
     def ensure_vof_buffers(self):
@@ -223,6 +226,7 @@ class WAAMGrid:
 
     def load_state(self, st):
         """Inverse of state_dict (numpy arrays or tensors)."""
+        self._forces_dirty = True
         for k, v in st.items():
             if k == "read_is_a":
                 self._read_buf, self._write_buf = (self.f_a, self.f_b) if v else (self.f_b, self.f_a)

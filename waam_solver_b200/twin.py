@@ -154,6 +154,8 @@ class WAAMTwin:
         self._torch_dir_xyz = (1.0, 0.0, 0.0)
         self._last_arc_ijk = None
         self.step_mode = step_mode
+        # non-droplet fused steps replay a captured CUDA graph of the step
+        self.use_cuda_graphs = True
         self._fused_params = None
 
         # Derived lattice scalars (twin.py:244-274).
