@@ -179,12 +179,24 @@ int waam_surface_height_at(const float* phi, const int32_t* flags, float* out, i
                            int nz, int i0, int j0, int nz_fallback, void* stream);
 /* kernels.py:278-400 feed_wire_surface (physics/deposition.py:247); serial
  * lexicographic budget order; vol_acc / real_acc are device floats
- * (grid.py:161-162 deposit_vol_buf / deposit_real_buf). */
+ * (grid.py:161-162 deposit_vol_buf / deposit_real_buf).  One CTA per call. */
 int waam_feed_wire_surface(float* f_src, int32_t* flags, float* f_l, float* phi, float* H,
                            float* T, float* rho, int nx, int ny, int nz, float arc_i, float arc_j,
                            float arc_k, float foot_r, float drop_r, float target_vol,
                            float T_drop, float cp_rho, float L_rho, float rho0, float* vol_acc,
                            float* real_acc, float cell_vol, void* stream);
+/* The droplet's whole deposition, solvers/coupled_step.py:126-151: attempt t
+ * is feed_wire_surface with footprint radius foot_radii[t]; attempt 0 starts
+ * from *vol_acc / *real_acc, attempt t > 0 runs only while the converted
+ * volume *real_acc is below accept_volume (compared in double) and starts
+ * with both budgets at that volume.  One launch, no host round trip between
+ * attempts; read *real_acc afterwards for the placed volume. */
+#define WAAM_DEPOSIT_MAX_TRIES 16
+int waam_deposit_droplet(float* f_src, int32_t* flags, float* f_l, float* phi, float* H, float* T,
+                         float* rho, int nx, int ny, int nz, float arc_i, float arc_j, float arc_k,
+                         const float* foot_radii, int n_tries, double accept_volume, float drop_r,
+                         float target_vol, float T_drop, float cp_rho, float L_rho, float rho0,
+                         float* vol_acc, float* real_acc, float cell_vol, void* stream);
 /* kernels.py:1176-1233 feed_wire_momentum_impact (physics/weld_forces.py:534-542) */
 int waam_feed_wire_momentum_impact(float* f_src, const float* rho, float* ux, float* uy,
                                    float* uz, const int32_t* flags, const float* f_l, int nx,

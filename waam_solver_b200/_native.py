@@ -53,7 +53,7 @@ class WaamStepParams(C.Structure):
 _CTYPES = {
     "float*": C.c_void_p, "const float*": C.c_void_p, "int32_t*": C.c_void_p,
     "const int32_t*": C.c_void_p, "void*": C.c_void_p, "float": C.c_float, "int": C.c_int,
-    "int64_t": C.c_int64, "size_t": C.c_size_t, "const WaamFields*": C.POINTER(WaamFields),
+    "int64_t": C.c_int64, "size_t": C.c_size_t, "double": C.c_double, "const WaamFields*": C.POINTER(WaamFields),
     "const WaamStepParams*": C.POINTER(WaamStepParams), "const char*": C.c_char_p,
     "void* const*": C.c_void_p,
 }

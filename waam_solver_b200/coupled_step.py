@@ -54,10 +54,22 @@ def _robot_z(twin, g, k_surface, torch_z_m):
     return k_surface
 
 
-def _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m):
+def _footprint_radii(r_try):
+    """The retry radii of solvers/coupled_step.py:130-151 (10 attempts)."""
+    radii = []
+    for _ in range(10):
+        radii.append(r_try)
+        r_try = min(r_try + 1.5, 16.0)
+    return radii
+
+
+def _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m, device_retries=False):
     """Droplet schedule and deposition (solvers/coupled_step.py:110-166).
 
-    Returns True when a droplet fired this step."""
+    ``device_retries`` runs the footprint retry loop in one launch
+    (``kernels.deposit_droplet``) instead of one ``feed_wire_surface`` call and
+    one read-back per attempt; the results are identical.  Returns True when a
+    droplet fired this step."""
     if twin.droplet_freq <= 0:
         return False
     sim_time = twin._step_n * g.dt
@@ -72,7 +84,16 @@ def _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m):
     T_drop = droplet_entry_temperature_K(twin)
     r_try = deposition.deposition_footprint_cells(twin, drop_r)
     placed_real = 0.0
-    for _ in range(10):
+    if device_retries:
+        g.deposit_vol_buf.zero_()
+        g.deposit_real_buf.zero_()
+        kernels.deposit_droplet(
+            g.f_src, g.flags, g.f_l, g.phi, g.H, g.T, g.rho, arc_i, arc_j, arc_k,
+            _footprint_radii(r_try), drop_vol * 0.98, drop_r, drop_vol, T_drop, twin.cp_rho,
+            twin.L_rho, 1.0, g.deposit_vol_buf, g.deposit_real_buf, g.dx ** 3, g.FLAG_GAS,
+            g.FLAG_FLUID, g.FLAG_SOLID, g.nx, g.ny, g.nz)
+        placed_real = float(g.deposit_real_buf.item())
+    for _ in range(0 if device_retries else 10):
         g.deposit_vol_buf.fill_(placed_real)
         g.deposit_real_buf.fill_(placed_real)
         deposition.feed_wire_surface(
@@ -377,7 +398,7 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
         if due:
             arc_k = float(g.step_scalars[0].item())
             forces.clear_forces(g.Fx, g.Fy, g.Fz)
-            _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m)
+            _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m, device_retries=True)
             p.forces_from_buffer = 1
             p.clear_forces = 0
         if events is None:

@@ -1,5 +1,5 @@
 // Fused B200 pipeline of one coupled step (solvers/coupled_step.py:73-464)
-// plus the column, streaming and deposition kernels shared with the
+// plus the column and streaming kernels shared with the
 // operator API.
 //
 // Per step (no droplet):  surface height -> arc weight sum -> inject + cap
@@ -219,103 +219,6 @@ __global__ void __launch_bounds__(256) k_stream(Dims d, const float* __restrict_
 int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags, void* stream) {
     k_stream<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(d, f_src, f_dst, flags);
     return check_launch("k_stream");
-}
-
-// ---------------------------------------------------------------------------
-// Droplet deposition (kernels.py:278-400).  The reference's reserve-then-
-// commit budget is order dependent; this kernel fixes the order to the serial
-// lexicographic (i, j, k) one with a single thread.  The search box is at
-// most (2*16+1)^2 x ~20 cells and the kernel runs once per droplet.
-// ---------------------------------------------------------------------------
-__device__ bool has_metal_nb(const Dims d, const float* phi, const int32_t* flags,
-                             const float* f_l, int i, int j, int k) {
-    const int dd[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
-    bool found = false;
-    for (int m = 0; m < 6; ++m) {
-        int ii = i + dd[m][0], jj = j + dd[m][1], kk = k + dd[m][2];
-        if (ii >= 0 && jj >= 0 && kk >= 0 && ii < d.nx && jj < d.ny && kk < d.nz) {
-            int c = d.idx(ii, jj, kk);
-            if (flags[c] == FLUID || flags[c] == SOLID)
-                found = true;
-            else if (phi[c] > 0.35f || f_l[c] > 0.2f)
-                found = true;
-        }
-    }
-    return found;
-}
-
-__global__ void k_deposit(Dims d, float* f_src, int32_t* flags, float* f_l, float* phi, float* H,
-                          float* T, float* rho, float arc_i, float arc_j, float arc_k, float foot_r,
-                          float drop_r, float target_vol, float T_drop, float cp_rho, float L_rho,
-                          float rho0, float* vol_acc, float* real_acc, float cell_vol) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const size_t n = (size_t)d.n();
-    float sr = fmax_(foot_r, drop_r);
-    int i0 = imax(0, (int)(arc_i - sr)), i1 = imin(d.nx, (int)(arc_i + sr) + 1);
-    int j0 = imax(0, (int)(arc_j - sr)), j1 = imin(d.ny, (int)(arc_j + sr) + 1);
-    int k0 = imax(0, (int)(arc_k - 1.0f));
-    float k_span = fmax_(drop_r + 3.0f, 4.0f);
-    int k1 = imin(d.nz, (int)(arc_k + k_span) + 1);
-    float drop_cz = arc_k + drop_r + 0.5f;
-    float rd2 = drop_r * drop_r, foot2 = sr * sr;
-    float vol = *vol_acc, real = *real_acc;
-    const float hdrop = cp_rho * T_drop + L_rho;
-    for (int pass = 0; pass < 2; ++pass)
-        for (int i = i0; i < i1; ++i)
-            for (int j = j0; j < j1; ++j)
-                for (int k = k0; k < k1; ++k) {
-                    if (vol >= target_vol) continue;
-                    int c = d.idx(i, j, k);
-                    if (flags[c] != GAS) continue;
-                    if (!has_metal_nb(d, phi, flags, f_l, i, j, k)) continue;
-                    float di = (float)i - arc_i, dj = (float)j - arc_j;
-                    float rij2 = di * di + dj * dj;
-                    if (pass == 0) {
-                        float dk = (float)k - drop_cz;
-                        float r2 = di * di + dj * dj + dk * dk;
-                        if (rij2 > foot2 && r2 > rd2) continue;
-                    } else if (rij2 > foot2 * 1.44f) {
-                        continue;
-                    }
-                    float reserved = vol;
-                    vol = reserved + cell_vol;
-                    if (reserved >= target_vol) {
-                        vol = vol - cell_vol;
-                    } else {
-                        flags[c] = FLUID;
-                        f_l[c] = 1.0f;
-                        phi[c] = 1.0f;
-                        T[c] = T_drop;
-                        H[c] = hdrop;
-                        rho[c] = rho0;
-                        for (int q = 0; q < 19; ++q) f_src[q * n + c] = wq(q) * rho0;
-                        real = real + cell_vol;
-                    }
-                }
-    for (int i = i0; i < i1; ++i)
-        for (int j = j0; j < j1; ++j)
-            for (int k = k0; k < k1; ++k) {
-                int c = d.idx(i, j, k);
-                if (flags[c] != FLUID || f_l[c] < 0.45f) continue;
-                float di = (float)i - arc_i, dj = (float)j - arc_j;
-                if (di * di + dj * dj > foot2 * 1.44f) continue;
-                T[c] = T_drop;
-                H[c] = hdrop;
-                rho[c] = rho0;
-                for (int q = 0; q < 19; ++q) f_src[q * n + c] = wq(q) * rho0;
-            }
-    *vol_acc = vol;
-    *real_acc = real;
-}
-
-int launch_deposit(Dims d, float* f_src, int32_t* flags, float* f_l, float* phi, float* H, float* T,
-                   float* rho, float arc_i, float arc_j, float arc_k, float foot_r, float drop_r,
-                   float target_vol, float T_drop, float cp_rho, float L_rho, float rho0,
-                   float* vol_acc, float* real_acc, float cell_vol, void* stream) {
-    k_deposit<<<1, 32, 0, STREAM(stream)>>>(d, f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j,
-                                            arc_k, foot_r, drop_r, target_vol, T_drop, cp_rho,
-                                            L_rho, rho0, vol_acc, real_acc, cell_vol);
-    return check_launch("k_deposit");
 }
 
 // ---------------------------------------------------------------------------

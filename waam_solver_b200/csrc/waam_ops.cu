@@ -979,8 +979,23 @@ int waam_feed_wire_surface(float* f_src, int32_t* flags, float* f_l, float* phi,
     REQUIRE(f_src && flags && f_l && phi && H && T && rho && vol_acc && real_acc,
             "feed_wire_surface: null field");
     return waam::launch_deposit(Dims{nx, ny, nz}, f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j,
-                                arc_k, foot_r, drop_r, target_vol, T_drop, cp_rho, L_rho, rho0,
-                                vol_acc, real_acc, cell_vol, stream);
+                                arc_k, &foot_r, 1, 0.0, drop_r, target_vol, T_drop, cp_rho, L_rho,
+                                rho0, vol_acc, real_acc, cell_vol, stream);
+}
+
+int waam_deposit_droplet(float* f_src, int32_t* flags, float* f_l, float* phi, float* H, float* T,
+                         float* rho, int nx, int ny, int nz, float arc_i, float arc_j, float arc_k,
+                         const float* foot_radii, int n_tries, double accept_volume, float drop_r,
+                         float target_vol, float T_drop, float cp_rho, float L_rho, float rho0,
+                         float* vol_acc, float* real_acc, float cell_vol, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "deposit_droplet: bad dims");
+    REQUIRE(f_src && flags && f_l && phi && H && T && rho && vol_acc && real_acc,
+            "deposit_droplet: null field");
+    REQUIRE(foot_radii && n_tries >= 1 && n_tries <= WAAM_DEPOSIT_MAX_TRIES,
+            "deposit_droplet: need 1..WAAM_DEPOSIT_MAX_TRIES footprint radii");
+    return waam::launch_deposit(Dims{nx, ny, nz}, f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j,
+                                arc_k, foot_radii, n_tries, accept_volume, drop_r, target_vol,
+                                T_drop, cp_rho, L_rho, rho0, vol_acc, real_acc, cell_vol, stream);
 }
 
 int waam_feed_wire_momentum_impact(float* f_src, const float* rho, float* ux, float* uy, float* uz,

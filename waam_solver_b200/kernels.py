@@ -11,6 +11,7 @@ raises.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 
 import torch
@@ -155,6 +156,26 @@ def feed_wire_surface(f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j, arc_k, fo
           float(arc_k), float(footprint_r), float(droplet_radius), float(target_vol),
           float(T_drop), float(cp_rho), float(L_rho), float(rho0), _f(vol_acc, 1),
           _f(real_acc, 1), float(cell_vol), _stream())
+
+
+def deposit_droplet(f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j, arc_k, footprint_radii,
+                    accept_volume, droplet_radius, target_vol, T_drop, cp_rho, L_rho, rho0,
+                    vol_acc, real_acc, cell_vol, FLAG_GAS, FLAG_FLUID, FLAG_SOLID, nx, ny, nz):
+    """The footprint retry loop of solvers/coupled_step.py:126-151 in one launch.
+
+    Attempt ``t`` is ``feed_wire_surface`` with ``footprint_radii[t]``; attempt
+    ``t > 0`` runs only while ``real_acc`` is below ``accept_volume`` and starts
+    with both budgets at ``real_acc``.  ``vol_acc``/``real_acc`` hold the
+    starting budgets on entry and the final ones on return."""
+    _flags_ok(FLAG_GAS=FLAG_GAS, FLAG_FLUID=FLAG_FLUID, FLAG_SOLID=FLAG_SOLID)
+    n = int(nx) * int(ny) * int(nz)
+    radii = (ctypes.c_float * len(footprint_radii))(*[float(r) for r in footprint_radii])
+    _call("waam_deposit_droplet", _f(f_src, 19 * n), _i(flags, n), _f(f_l, n), _f(phi, n),
+          _f(H, n), _f(T, n), _f(rho, n), int(nx), int(ny), int(nz), float(arc_i), float(arc_j),
+          float(arc_k), ctypes.cast(radii, ctypes.c_void_p), len(footprint_radii),
+          float(accept_volume), float(droplet_radius), float(target_vol), float(T_drop),
+          float(cp_rho), float(L_rho), float(rho0), _f(vol_acc, 1), _f(real_acc, 1),
+          float(cell_vol), _stream())
 
 
 def feed_wire_momentum_impact(f_src, rho, ux, uy, uz, flags, f_l, arc_i, arc_j, arc_k,
