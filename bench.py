@@ -164,17 +164,30 @@ def census(twin):
     return dict(n=n, solid=solid, gas=gas, fluid=n - solid - gas)
 
 
-def algorithmic_bytes(c):
+def algorithmic_bytes(c, tail_on=False):
     """Compulsory DRAM bytes per launch of each fused stage (FP32 fields, int32
-    flags), from the cell census; each field element counted once."""
-    n, ns, ng, nf = c["n"], c["n"] - c["solid"], c["n"] - c["gas"], c["fluid"]
+    flags), from the cell census; each field element read or written once.
+
+    n cells, ns non-solid, ng non-gas, na active (FLUID/IFACE):
+      arc        norm: flags n, f_l ng; inject: flags n, f_l ng, H r+w ng (ceiling on)
+      thermal    flags, H, H_next, T_next, f_l: n; T, T_max r+w, T_prev r+w,
+                 dT_dt: ng; ux, uy, uz: na
+      vof_advect flags, phi, phi_tmp: n; ux, uy, uz: na
+      column     phi_tmp, phi, flags r+w, f_l: n; T, 3 time-above r+w: ng; list: na
+      collide    list, f_l, phi, T, flags, 19 f reads, 19 f writes, rho, u (3), F (3): na
+      stream     flags: n; 19 f reads + 19 f writes: ns
+      tail       flags: n; T, phi, f_l: ng (only when remelt / solidify run)
+    Neighbour reads of the stencils are cache hits and are not counted.
+    """
+    n, ns, ng, na = c["n"], c["n"] - c["solid"], c["n"] - c["gas"], c["fluid"]
     return {
-        "thermal": 20 * n + 24 * ng + 12 * nf,
-        "vof_advect": 12 * n + 12 * ng,
-        "column": 20 * n + 28 * ng,
-        "collide": 4 * n + 12 * (n - nf) + 344 * nf,
-        "stream": 4 * n + 304 * ns,
-        "tail": 0,
+        "arc": 8 * n + 16 * ng,
+        "thermal": 20 * n + 24 * ng + 12 * na,
+        "vof_advect": 12 * n + 12 * na,
+        "column": 20 * n + 28 * ng + 4 * na,
+        "collide": 200 * na,
+        "stream": 4 * n + 152 * ns,
+        "tail": (4 * n + 12 * ng) if tail_on else 0,
     }
 
 
@@ -324,7 +337,7 @@ def run_b200(args, w):
     for i, name in enumerate(STAGES):
         stage_ms[name] = statistics.fmean(es[i].elapsed_time(es[i + 1]) for es in ev_sets)
     c = census(tw)
-    algo = algorithmic_bytes(c)
+    algo = algorithmic_bytes(c, tw.enable_bead_freeze or tw.enable_substrate_growth)
     hbm, hbm_src = peaks()
     dom = max(("stream", "collide", "thermal", "column", "vof_advect"),
               key=lambda k: stage_ms[k])
@@ -334,7 +347,9 @@ def run_b200(args, w):
     if os.path.exists(tpath):
         with open(tpath) as fh:
             t = json.load(fh)
-        traffic = t["dram_bytes_per_cell"] * c["n"]
+        # one capture's DRAM bytes, scaled to this census by the cells the stage touches
+        per = {"stream": c["n"] - c["solid"], "collide": c["fluid"]}.get(dom, c["n"])
+        traffic = t["dram_bytes"] * per / t["cells_touched"]
     step_bytes = sum(algo.values())
     lib = _native.lib()
     launches_per_step = lib.waam_step_launch_count(tw._fused_params, 0) + \

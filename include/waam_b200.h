@@ -208,6 +208,54 @@ int waam_apply_droplet_impact_pressure(float* Fz, const int32_t* flags, const fl
                                        float arc_j, float arc_k, float drop_r, float impact_pa,
                                        float dt, float dx, float rho_ref, void* stream);
 
+/* ---- Lorentz force of the welding current (physics/weld_forces.py:196-281) -- */
+
+/* kernels.py:1237-1251 elec_build_sigma */
+int waam_elec_build_sigma(float* sigma, const float* f_l, const int32_t* flags, int64_t n,
+                          float sigma_liquid, float sigma_solid, void* stream);
+/* kernels.py:1255-1284 elec_clear_source + elec_inject_arc_source (one pass) */
+int waam_elec_inject_arc_source(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
+                                float arc_k, float sigma_cells, float current_A, float dx,
+                                void* stream);
+/* kernels.py:1288-1301 elec_normalize_source; the sum is taken in double */
+int waam_elec_normalize_source(float* source, int64_t n, float target_current_A, float dx,
+                               void* workspace, size_t workspace_bytes, void* stream);
+/* kernels.py:1304-1312 elec_init_ground (phi = 0) */
+int waam_elec_init_ground(float* phi, int64_t n, void* stream);
+/* kernels.py:1315-1355 elec_jacobi_step; phi_in and phi_out must differ */
+int waam_elec_jacobi_step(const float* phi_in, float* phi_out, const float* sigma,
+                          const float* source, const int32_t* flags, int nx, int ny, int nz,
+                          float dx, float omega_j, int nz_solid, void* stream);
+/* elec_jacobi_step followed by elec_l1_diff(phi_out, phi_in) (kernels.py:1387-1398)
+ * in the same pass: *diff_buf = sum|phi_out - phi_in|, *norm_buf = sum|phi_in|. */
+int waam_elec_jacobi_step_l1(const float* phi_in, float* phi_out, const float* sigma,
+                             const float* source, const int32_t* flags, int nx, int ny, int nz,
+                             float dx, float omega_j, int nz_solid, float* diff_buf,
+                             float* norm_buf, void* workspace, size_t workspace_bytes,
+                             void* stream);
+/* kernels.py:1387-1398 elec_l1_diff: *diff_buf = sum|a - b|, *norm_buf = sum|b| */
+int waam_elec_l1_diff(const float* a, const float* b, float* diff_buf, float* norm_buf, int nx,
+                      int ny, int nz, void* workspace, size_t workspace_bytes, void* stream);
+/* kernels.py:1358-1383 elec_compute_J */
+int waam_elec_compute_J(float* Jx, float* Jy, float* Jz, const float* phi, const float* sigma,
+                        const int32_t* flags, int nx, int ny, int nz, float dx, void* stream);
+/* kernels.py:1402-1421 elec_bin_axial_current: bins (nz, n_bins) of Jz dx^2 by
+ * radius; sums in double, stored as float */
+int waam_elec_bin_axial_current(const float* Jz, float* bins, int nx, int ny, int nz, float arc_i,
+                                float arc_j, float dx, float bin_dr_cells, int n_bins,
+                                void* workspace, size_t workspace_bytes, void* stream);
+/* kernels.py:1424-1435 elec_prefix_bins (float prefix over radius, in place) */
+int waam_elec_prefix_bins(float* bins, int n_bins, int nz, void* stream);
+/* kernels.py:1438-1475 elec_B_axisymmetric */
+int waam_elec_B_axisymmetric(float* Bx, float* By, float* Bz, const float* bins, int nx, int ny,
+                             int nz, float arc_i, float arc_j, float dx, float bin_dr_cells,
+                             float mu0, int n_bins, void* stream);
+/* kernels.py:1479-1513 apply_lorentz_JxB */
+int waam_apply_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* Jx, const float* Jy,
+                           const float* Jz, const float* Bx, const float* By, const float* Bz,
+                           const float* f_l, const int32_t* flags, int64_t n, float dt, float dx,
+                           float rho_ref, void* stream);
+
 /* ---- fused step: the B200 pipeline of solvers/coupled_step.py:73-464 ----- */
 
 typedef struct WaamFields {

@@ -43,7 +43,9 @@ class OracleTwin:
             wire_feed_m_s=0.0, droplet_transfer_mode="auto", pulse_frequency_hz=0.0,
             droplet_size_jitter=0.12, plate_thickness_mm=None, goldak=None,
             impact_lead_angle_deg=0.0, trailing_solidify_lookback_mm=2.5,
-            trailing_solidify_temp_margin_K=35.0)
+            trailing_solidify_temp_margin_K=35.0, enable_lorentz=False, sigma_liquid_Sm=1.0e6,
+            sigma_solid_Sm=1.0e5, lorentz_jacobi_iters=40, lorentz_jacobi_omega=0.85,
+            lorentz_jacobi_tol=1e-4)
         unknown = set(kw) - set(self.cfg)
         if unknown:
             raise KeyError("unknown OracleTwin options: %s" % sorted(unknown))
@@ -82,6 +84,8 @@ class OracleTwin:
         self.last_pos = None
         self.arc_k = None
         self.s = None
+        self.lorentz_warm = False
+        self.lorentz_iters = []
 
     # ---------------------------------------------------------------- state --
     def reset(self):
@@ -102,6 +106,7 @@ class OracleTwin:
         O.call("wo_stream", s["f_a"], s["f_b"], s["flags"], nx, ny, nz)
         s["read_is_a"] = True
         self.s = s
+        self.lorentz_warm = False
         self.step_n = 0
         self.last_drop = 0.0
         self.n_drops = 0
@@ -253,6 +258,8 @@ class OracleTwin:
             O.call("wo_add_hydrostatic_gravity", s["Fz"], s["f_l"], s["flags"], n, 1.0, self.g_lu)
         O.call("wo_add_buoyancy", s["T"], s["Fz"], s["f_l"], s["flags"], n, self.g_lu,
                m["beta_T"], Tl, 1.0)
+        if welding and c["enable_lorentz"]:
+            self._lorentz(arc_i, arc_j, arc_k)
         O.call("wo_clamp_body_force_magnitude", s["Fx"], s["Fy"], s["Fz"], s["flags"], n, 0.05)
         if c["use_srt"]:
             O.call("wo_collide_srt", self.fsrc(), self.fdst(), s["rho"], s["ux"], s["uy"],
@@ -280,6 +287,57 @@ class OracleTwin:
                    s["uy"], s["uz"], n, Ts, 1)
         s["read_is_a"] = not s["read_is_a"]
         self.step_n += 1
+
+    def _lorentz(self, arc_i, arc_j, arc_k):
+        """physics/weld_forces.py:196-281 on the oracle kernels."""
+        import ctypes
+        c, s = self.cfg, self.s
+        nx, ny, nz, n = self.nx, self.ny, self.nz, self.nx * self.ny * self.nz
+        sh = (nx, ny, nz)
+        for f in ("phi_elec", "phi_elec_tmp", "sigma_elec", "elec_source", "Jx", "Jy", "Jz", "Bx",
+                  "By", "Bz"):
+            s.setdefault(f, np.zeros(sh, np.float32))
+        n_bins = 64
+        s.setdefault("elec_rad_bins", np.zeros((nz, n_bins), np.float32))
+        I = c["welding_current_A"]
+        O.call("wo_elec_build_sigma", s["sigma_elec"], s["f_l"], s["flags"], n,
+               c["sigma_liquid_Sm"], c["sigma_solid_Sm"])
+        O.call("wo_elec_inject_arc_source", s["elec_source"], nx, ny, nz, arc_i, arc_j, arc_k,
+               self.sigma_cells, I, self.dx)
+        O.call("wo_elec_normalize_source", s["elec_source"], n, I, self.dx)
+        cold = not self.lorentz_warm
+        if cold:
+            s["phi_elec"][...] = 0.0
+            self.lorentz_warm = True
+        max_iters = max(int(c["lorentz_jacobi_iters"]), 20)
+        if cold:
+            nmax = max(nx, ny, nz)
+            max_iters = max(max_iters, 2 * nmax * nmax)
+        done = 0
+        d, m = ctypes.c_double(), ctypes.c_double()
+        while done < max_iters:
+            for _ in range(min(10, max_iters - done)):
+                O.call("wo_elec_jacobi_step", s["phi_elec"], s["phi_elec_tmp"], s["sigma_elec"],
+                       s["elec_source"], s["flags"], nx, ny, nz, self.dx,
+                       c["lorentz_jacobi_omega"], self.nz_solid)
+                O.call("wo_elec_l1_diff", s["phi_elec_tmp"], s["phi_elec"], n, ctypes.byref(d),
+                       ctypes.byref(m))
+                s["phi_elec"][...] = s["phi_elec_tmp"]
+                done += 1
+            rel = float(np.float32(d.value)) / max(float(np.float32(m.value)), 1e-30)
+            if rel < c["lorentz_jacobi_tol"]:
+                break
+        self.lorentz_iters.append(done)
+        O.call("wo_elec_compute_J", s["Jx"], s["Jy"], s["Jz"], s["phi_elec"], s["sigma_elec"],
+               s["flags"], nx, ny, nz, self.dx)
+        bin_dr = max(float(max(nx, ny)) / (2.0 * n_bins), 0.5)
+        O.call("wo_elec_bins", s["Jz"], s["elec_rad_bins"], nx, ny, nz, arc_i, arc_j, self.dx,
+               bin_dr, n_bins)
+        O.call("wo_elec_B_axisymmetric", s["Bx"], s["By"], s["Bz"], s["elec_rad_bins"], nx, ny,
+               nz, arc_i, arc_j, self.dx, bin_dr, 4.0e-7 * math.pi, n_bins)
+        O.call("wo_apply_lorentz_JxB", s["Fx"], s["Fy"], s["Fz"], s["Jx"], s["Jy"], s["Jz"],
+               s["Bx"], s["By"], s["Bz"], s["f_l"], s["flags"], n, self.dt, self.dx,
+               self.mat["rho"])
 
     def _maybe_droplet(self, arc_i, arc_j, arc_k):
         c, s, m = self.cfg, self.s, self.mat

@@ -45,7 +45,8 @@ def full_inputs(name):
     args, ins, outs = load_case(name)
     seed_map = {"inject_goldak": 1, "thermal_s2": 2, "vof_wet": 3, "contact": 4,
                 "contact_s5": 5, "forces_wet": 6, "csf": 7, "csf_wet": 8, "collide_srt": 9,
-                "tail": 10, "heat_loss": 11, "surface_height": 12, "deposit": 13}
+                "tail": 10, "heat_loss": 11, "surface_height": 12, "deposit": 13,
+                "lorentz": 14}
     nx, ny, nz = ins[next(iter(ins))].shape[-3:]
     st = state_gen.seeded_state(nx, ny, nz, seed=seed_map.get(name, 0))
     st = {k: (np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v) for k, v in st.items()}
@@ -189,6 +190,36 @@ def run_case(be, name, st, a):
                                          a["arc_i"], a["arc_j"], a["arc_k"], a["drop_r"],
                                          a["impact_pa"], a["dt"], a["dx"], 7800.0)
         return placed
+    elif name == "lorentz":
+        rng = np.random.default_rng(31)
+        for f in ("sigma_elec", "elec_source", "phi_elec_tmp", "Jx", "Jy", "Jz", "Bx", "By", "Bz"):
+            st.setdefault(f, np.zeros((nx, ny, nz), np.float32))
+        st.setdefault("phi_elec", rng.uniform(0.0, 0.05, (nx, ny, nz)).astype(np.float32))
+        st.setdefault("elec_rad_bins", np.zeros((nz, a["n_bins"]), np.float32))
+        be.elec_build_sigma(st["sigma_elec"], st["f_l"], st["flags"], n, a["s_liq"], a["s_sol"])
+        be.elec_inject_arc_source(st["elec_source"], nx, ny, nz, a["arc_i"], a["arc_j"],
+                                  a["arc_k"], a["sigma_cells"], a["current"], a["dx"])
+        be.elec_normalize_source(st["elec_source"], n, a["current"], a["dx"])
+        l1 = []
+        for it in range(a["iters"]):
+            be.elec_jacobi_step(st["phi_elec"], st["phi_elec_tmp"], st["sigma_elec"],
+                                st["elec_source"], st["flags"], nx, ny, nz, a["dx"], a["omega"],
+                                a["nz_solid"])
+            d, m = be.elec_l1(st["phi_elec_tmp"], st["phi_elec"])
+            st["phi_elec"][...] = st["phi_elec_tmp"]
+            if it % 10 == 9:
+                l1.append([d, m])
+        be.elec_compute_J(st["Jx"], st["Jy"], st["Jz"], st["phi_elec"], st["sigma_elec"],
+                          st["flags"], nx, ny, nz, a["dx"])
+        be.elec_bins(st["Jz"], st["elec_rad_bins"], nx, ny, nz, a["arc_i"], a["arc_j"], a["dx"],
+                     a["bin_dr"], a["n_bins"])
+        be.elec_B_axisymmetric(st["Bx"], st["By"], st["Bz"], st["elec_rad_bins"], nx, ny, nz,
+                               a["arc_i"], a["arc_j"], a["dx"], a["bin_dr"], a["mu0"],
+                               a["n_bins"])
+        be.apply_lorentz_JxB(st["Fx"], st["Fy"], st["Fz"], st["Jx"], st["Jy"], st["Jz"],
+                             st["Bx"], st["By"], st["Bz"], st["f_l"], st["flags"], n, a["dt"],
+                             a["dx"], a["rho_ref"])
+        return l1
     elif name == "reset":
         ny_ = ny
         be.init_grid(st["f_a"], st["rho"], st["ux"], st["uy"], st["uz"], st["T"], st["H"],
@@ -207,7 +238,7 @@ def run_case(be, name, st, a):
 CASES = ["inject_gauss", "inject_goldak", "ceiling", "thermal", "thermal_s2", "phase",
          "tmax_cool", "vof", "vof_wet", "contact", "contact_s5", "forces", "forces_wet", "csf",
          "csf_wet", "collide_mrt", "collide_srt", "stream", "tail", "heat_loss",
-         "surface_height", "deposit", "reset"]
+         "surface_height", "deposit", "lorentz", "reset"]
 
 
 def check_case(be, name):
@@ -219,6 +250,10 @@ def check_case(be, name):
         worst = max(worst, compare(name, st[f], want, f))
     if name == "surface_height":
         assert extra == a["heights"], (extra, a["heights"])
+    if name == "lorentz":
+        for got, ref in zip(extra, a["l1"]):
+            for g_, r_ in zip(got, ref):
+                assert abs(g_ - r_) <= RTOL * abs(r_), (extra, a["l1"])
     if name == "deposit":
         for got, ref in zip(extra, a["placed"]):
             assert abs(got[1] - ref[1]) <= 1e-6 * max(ref[1], 1e-30) + 1e-30, (extra, a["placed"])
@@ -245,6 +280,15 @@ class OracleBackend:
         def f(*args):
             return O.call(fn_name, *args)
         return f
+
+    def elec_l1(self, a, b):
+        import ctypes
+        d, m = ctypes.c_double(), ctypes.c_double()
+        self.O.call("wo_elec_l1_diff", a, b, a.size, ctypes.byref(d), ctypes.byref(m))
+        return float(np.float32(d.value)), float(np.float32(m.value))
+
+    def elec_bins(self, Jz, bins, nx, ny, nz, arc_i, arc_j, dx, bin_dr, n_bins):
+        self.O.call("wo_elec_bins", Jz, bins, nx, ny, nz, arc_i, arc_j, dx, bin_dr, n_bins)
 
     def feed_wire_surface(self, *args):
         args = list(args)

@@ -13,7 +13,7 @@ import torch
 from waam_solver_b200 import _native
 
 _WS_FUNCS = {"inject_arc_heat", "inject_goldak_heat", "advect_diffuse_temperature",
-             "apply_contact_angle_phi_bc"}
+             "apply_contact_angle_phi_bc", "elec_normalize_source"}
 _NORM_FUNCS = {"inject_arc_heat", "inject_goldak_heat"}
 
 
@@ -63,6 +63,33 @@ class CudaBackend:
                     break
             return self._run(name, list(args), n_cells)
         return f
+
+    def _ws(self, n_cells):
+        nbytes = int(_native.lib().waam_workspace_bytes(n_cells))
+        return torch.zeros(nbytes, dtype=torch.uint8, device=self.device), nbytes
+
+    def elec_l1(self, a, b):
+        nx, ny, nz = a.shape
+        ta, tb = self._up(a), self._up(b)
+        d = torch.zeros((), dtype=torch.float32, device=self.device)
+        m = torch.zeros((), dtype=torch.float32, device=self.device)
+        ws, nbytes = self._ws(a.size)
+        _native.call("waam_elec_l1_diff", ta.data_ptr(), tb.data_ptr(), d.data_ptr(),
+                     m.data_ptr(), nx, ny, nz, ws.data_ptr(), nbytes,
+                     torch.cuda.current_stream().cuda_stream)
+        self.launched.append("elec_l1_diff")
+        return float(d.item()), float(m.item())
+
+    def elec_bins(self, Jz, bins, nx, ny, nz, arc_i, arc_j, dx, bin_dr, n_bins):
+        tj, tb = self._up(Jz), self._up(bins)
+        ws, nbytes = self._ws(Jz.size)
+        st = torch.cuda.current_stream().cuda_stream
+        _native.call("waam_elec_bin_axial_current", tj.data_ptr(), tb.data_ptr(), nx, ny, nz,
+                     arc_i, arc_j, dx, bin_dr, n_bins, ws.data_ptr(), nbytes, st)
+        _native.call("waam_elec_prefix_bins", tb.data_ptr(), n_bins, nz, st)
+        torch.cuda.synchronize()
+        self.launched.append("elec_bins")
+        bins[...] = tb.cpu().numpy()
 
     def surface_height_at(self, phi, flags, nx, ny, nz, i0, j0, nz_fallback):
         out = torch.zeros((), dtype=torch.float32, device=self.device)

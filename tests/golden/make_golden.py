@@ -94,7 +94,12 @@ def save(name, payload):
 NX, NY, NZ = 13, 11, 12
 
 
+ONLY = set()   # kernel case names given as ``kernel=<name>`` on the command line
+
+
 def kernel_case(name, call, fields, seed=0, twin_kw=None, state_kw=None, extra_in=None):
+    if ONLY and name not in ONLY:
+        return
     tw = make_twin(NX, NY, NZ, **(twin_kw or {}))
     g = tw.grid
     st = seeded_state(NX, NY, NZ, seed=seed, **(state_kw or {}))
@@ -325,6 +330,52 @@ def c_deposit(tw, g):
     return a
 
 
+LORENTZ_FIELDS = ["sigma_elec", "elec_source", "phi_elec", "phi_elec_tmp", "Jx", "Jy", "Jz",
+                  "Bx", "By", "Bz", "elec_rad_bins", "Fx", "Fy", "Fz"]
+
+
+def lorentz_setup(tw, g):
+    g.ensure_lorentz_fields()
+    rng = np.random.default_rng(31)
+    g.phi_elec.from_numpy(rng.uniform(0.0, 0.05, (g.nx, g.ny, g.nz)).astype(np.float32))
+    g.phi_elec_tmp.from_numpy(np.zeros((g.nx, g.ny, g.nz), np.float32))
+
+
+def c_lorentz(tw, g):
+    """physics/weld_forces.py:196-281 with a fixed budget of 30 Jacobi sweeps."""
+    from waam_twin.physics.weld_forces import MU0
+    a = scal(tw)
+    a.update(arc_i=6.3, arc_j=5.4, arc_k=float(tw.nz_solid + 1), sigma_cells=2.5, current=200.0,
+             s_liq=1.0e6, s_sol=1.0e5, omega=0.85, iters=30, n_bins=int(g.n_elec_bins),
+             mu0=MU0, rho_ref=tw.mat.rho)
+    a["bin_dr"] = max(float(max(g.nx, g.ny)) / (2.0 * g.n_elec_bins), 0.5)
+    K.elec_build_sigma(g.sigma_elec, g.f_l, g.flags, a["s_liq"], a["s_sol"], g.FLAG_GAS)
+    K.elec_clear_source(g.elec_source)
+    K.elec_inject_arc_source(g.elec_source, a["arc_i"], a["arc_j"], a["arc_k"], a["sigma_cells"],
+                             a["current"], g.dx, g.nz)
+    K.elec_normalize_source(g.elec_source, a["current"], g.dx)
+    res = []
+    for it in range(a["iters"]):
+        K.elec_jacobi_step(g.phi_elec, g.phi_elec_tmp, g.sigma_elec, g.elec_source, g.flags,
+                           g.dx, a["omega"], g.FLAG_GAS, g.FLAG_SOLID, tw.nz_solid, g.nx, g.ny,
+                           g.nz)
+        K.elec_l1_diff(g.phi_elec_tmp, g.phi_elec, g.elec_res_buf, g.elec_norm_buf)
+        g.phi_elec.copy_from(g.phi_elec_tmp)
+        if it % 10 == 9:
+            res.append([float(g.elec_res_buf[None]), float(g.elec_norm_buf[None])])
+    a["l1"] = res
+    K.elec_compute_J(g.Jx, g.Jy, g.Jz, g.phi_elec, g.sigma_elec, g.flags, g.dx, g.FLAG_GAS,
+                     g.nx, g.ny, g.nz)
+    K.elec_bin_axial_current(g.Jz, g.elec_rad_bins, a["arc_i"], a["arc_j"], g.dx, a["bin_dr"],
+                             a["n_bins"], g.nz)
+    K.elec_prefix_bins(g.elec_rad_bins, a["n_bins"], g.nz)
+    K.elec_B_axisymmetric(g.Bx, g.By, g.Bz, g.elec_rad_bins, a["arc_i"], a["arc_j"], g.dx,
+                          a["bin_dr"], MU0, a["n_bins"], g.nz)
+    K.apply_lorentz_JxB(g.Fx, g.Fy, g.Fz, g.Jx, g.Jy, g.Jz, g.Bx, g.By, g.Bz, g.f_l, g.flags,
+                        g.dt, g.dx, tw.mat.rho, g.FLAG_GAS)
+    return a
+
+
 def c_reset(tw, g):
     a = scal(tw)
     tw.reset()
@@ -358,6 +409,7 @@ def kernel_cases():
     kernel_case("heat_loss", c_heat_loss, ["H"], seed=11)
     kernel_case("surface_height", c_surface_height, ["phi"], seed=12)
     kernel_case("deposit", c_deposit, base + ["rho", "f_a", "ux", "uy", "uz", "Fz"], seed=13)
+    kernel_case("lorentz", c_lorentz, LORENTZ_FIELDS, seed=14, extra_in=lorentz_setup)
     kernel_case("reset", c_reset, base + ["rho", "ux", "uy", "uz", "f_a", "f_b", "T_max",
                                           "T_prev", "dT_dt", "time_above_800_s", "Fx", "Fx_snap"])
 
@@ -496,7 +548,8 @@ def kats():
 
 if __name__ == "__main__":
     what = sys.argv[1:] or ["kernels", "steps", "kats"]
-    if "kernels" in what:
+    ONLY.update(w.split("=", 1)[1] for w in what if w.startswith("kernel="))
+    if "kernels" in what or ONLY:
         kernel_cases()
     if "steps" in what:
         step_cases()

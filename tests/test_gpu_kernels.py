@@ -46,12 +46,15 @@ def test_cuda_matches_oracle(cuda_backend, oracle_backend, name):
             cases.compare(name, v, st_o[f], f)
             if v.dtype.kind in "iu":
                 assert np.array_equal(v, st_o[f])
-    assert ex_c == ex_o or name in ("deposit",)
+    if name == "lorentz":   # grid sums in double, block order vs serial order
+        np.testing.assert_allclose(ex_c, ex_o, rtol=cases.RTOL)
+    else:
+        assert ex_c == ex_o or name in ("deposit",)
 
 
 BIG = ["inject_gauss", "inject_goldak", "thermal", "vof", "vof_wet", "contact", "contact_s5",
        "forces", "forces_wet", "csf_wet", "collide_mrt", "collide_srt", "stream", "tail",
-       "heat_loss", "deposit"]
+       "heat_loss", "deposit", "lorentz"]
 
 
 @pytest.mark.parametrize("shape", [(48, 40, 36), (33, 17, 70)])

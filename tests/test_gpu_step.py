@@ -43,7 +43,7 @@ def test_fused_matches_oracle_over_trajectory(name):
     steps.compare_state("%s fused vs oracle" % name, tw.grid.state_dict(), ot.s)
 
 
-def _config_twins(kind, nx, ny, nz):
+def _config_twins(kind, nx, ny, nz, **more):
     """A c1-like (Gaussian, no wire) or c2-like (Goldak, 100 Hz droplets, wetting,
     CSF, hydrostatic) run from reset, on the GPU and on the oracle."""
     from oracle.oracle_step import OracleTwin
@@ -64,6 +64,7 @@ def _config_twins(kind, nx, ny, nz):
         host = dict(wire_feed_m_s=0.1, droplet_transfer_mode="pulsed", pulse_frequency_hz=100.0,
                     droplet_size_jitter=0.0)
         goldak = dict(ff=0.6, fr=1.4, a_front=5.0, a_rear=12.0, b=5.0, c=4.0)
+    kw.update(more)
     mat = from_constants("m", steps.MATERIAL, contact_angle_deg=30.0)
     tw = WAAMTwin(material=mat, nx=nx, ny=ny, nz=nz, dx=dx, max_tracers=64, **kw)
     for k, v in host.items():
@@ -131,3 +132,32 @@ def test_graph_replay_matches_eager_launches():
     for k, v in states[0].items():
         if isinstance(v, np.ndarray):
             assert np.array_equal(v, states[1][k]), k
+
+
+LORENTZ_FIELDS = ("phi_elec", "Jx", "Jy", "Jz", "Bx", "By", "Bz", "elec_rad_bins")
+
+
+def test_lorentz_steps_match_oracle():
+    """Welding current on: the potential solve (cold start, then warm), J, B and
+    J x B through the CUDA operators, step by step against the oracle."""
+    shape = (40, 24, 24)
+    tw, ot, dx = _config_twins("c2", *shape, enable_lorentz=True, welding_current_A=180.0,
+                               lorentz_jacobi_iters=40)
+    import state_gen
+    st = state_gen.seeded_state(*shape, seed=9, nz_solid=tw.nz_solid)
+    st["read_is_a"] = True
+    tw.grid.load_state({k: v for k, v in st.items() if k != "nz_solid"})
+    ot.load({k: v for k, v in st.items() if k != "nz_solid"})
+    y = (shape[1] // 2) * dx
+    for s in range(5):
+        x = 0.3 * shape[0] * dx + s * 0.008 * dx * 0.1
+        tw.step(x, y, True)
+        ot.step(x, y, True)
+        torch.cuda.synchronize()
+        assert tw._lorentz_last_iters == ot.lorentz_iters[-1], (s, tw._lorentz_last_iters,
+                                                                ot.lorentz_iters)
+        g = tw.grid
+        got = {f: getattr(g, f).cpu().numpy() for f in LORENTZ_FIELDS}
+        steps.compare_state("lorentz step %d" % s, dict(tw.grid.state_dict(), **got),
+                            ot.s, fields=steps.FIELDS + list(LORENTZ_FIELDS))
+    assert ot.lorentz_iters[0] > ot.lorentz_iters[-1]    # cold start, then warm starts

@@ -23,25 +23,10 @@ namespace waam {
 
 #define STREAM(s) reinterpret_cast<cudaStream_t>(s)
 constexpr int kMainEvents = 7;
-constexpr int kTileK = 32;
-constexpr int kTileJ = 8;
 constexpr int kTileRedBlocks = 592;   // <= kWsMaxPartials
 constexpr int kListThreads = 128;
 constexpr int kListBlocks = 148 * 6;
 
-inline dim3 tile_grid(const Dims& d) {
-    return dim3((d.nz + kTileK - 1) / kTileK, (d.ny + kTileJ - 1) / kTileJ, d.nx);
-}
-inline dim3 tile_block() { return dim3(kTileK, kTileJ, 1); }
-
-__device__ __forceinline__ bool tile_cell(const Dims& d, int& i, int& j, int& k, int& c) {
-    k = blockIdx.x * kTileK + threadIdx.x;
-    j = blockIdx.y * kTileJ + threadIdx.y;
-    i = blockIdx.z;
-    if (k >= d.nz || j >= d.ny) return false;
-    c = (i * d.ny + j) * d.nz + k;
-    return true;
-}
 
 // ---------------------------------------------------------------------------
 // Contact-angle ghost-phi BC (kernels.py:933-991), one warp per (i, j)
@@ -182,9 +167,22 @@ int launch_contact_columns(Dims d, const float* snap, float* phi, const int32_t*
 
 // ---------------------------------------------------------------------------
 // Pull streaming (kernels.py:2971-3010): x periodic, y/z clamped, bounce-back
-// from SOLID sources for non-gas cells.  Interior cells (no wrap or clamp on
-// any axis) use fixed neighbour offsets; boundary cells take the general path.
+// from SOLID sources for non-gas cells.  Every thread first issues its 19
+// source loads back to back (independent addresses, so all are in flight at
+// once), then, for the few non-gas cells, replaces the populations whose
+// source is SOLID by the cell's own opposite population, then stores.
+// Interior cells (no wrap or clamp on any axis) use fixed neighbour offsets.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ int stream_source(const Dims& d, bool interior, int i, int j, int k,
+                                             int c, int q) {
+    if (interior) return c - (ex(q) * d.ny * d.nz + ey(q) * d.nz + ez(q));
+    int ni = i - ex(q);
+    ni = ni < 0 ? ni + d.nx : (ni >= d.nx ? ni - d.nx : ni);
+    const int nj = imax(0, imin(j - ey(q), d.ny - 1));
+    const int nk = imax(0, imin(k - ez(q), d.nz - 1));
+    return (ni * d.ny + nj) * d.nz + nk;
+}
+
 __global__ void __launch_bounds__(256) k_stream(Dims d, const float* __restrict__ f_src,
                                                 float* __restrict__ f_dst,
                                                 const int32_t* __restrict__ flags) {
@@ -193,27 +191,18 @@ __global__ void __launch_bounds__(256) k_stream(Dims d, const float* __restrict_
     const int flag = flags[c];
     if (flag == SOLID) return;
     const size_t n = (size_t)d.n();
-    const int sy = d.nz, sx = d.ny * d.nz;
     const bool interior = i > 0 && i < d.nx - 1 && j > 0 && j < d.ny - 1 && k > 0 && k < d.nz - 1;
+    float v[19];
 #pragma unroll
-    for (int q = 0; q < 19; ++q) {
-        int s;
-        if (interior) {
-            s = c - (ex(q) * sx + ey(q) * sy + ez(q));
-        } else {
-            int ni = i - ex(q);
-            ni = ni < 0 ? ni + d.nx : (ni >= d.nx ? ni - d.nx : ni);
-            int nj = imax(0, imin(j - ey(q), d.ny - 1));
-            int nk = imax(0, imin(k - ez(q), d.nz - 1));
-            s = (ni * d.ny + nj) * d.nz + nk;
-        }
-        float v;
-        if (flag == GAS || flags[s] != SOLID)
-            v = f_src[q * n + s];
-        else
-            v = f_src[opp(q) * n + c];
-        f_dst[q * n + c] = v;
+    for (int q = 0; q < 19; ++q) v[q] = f_src[q * n + stream_source(d, interior, i, j, k, c, q)];
+    if (flag != GAS) {
+#pragma unroll
+        for (int q = 1; q < 19; ++q)
+            if (flags[stream_source(d, interior, i, j, k, c, q)] == SOLID)
+                v[q] = f_src[opp(q) * n + c];
     }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f_dst[q * n + c] = v[q];
 }
 
 int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags, void* stream) {

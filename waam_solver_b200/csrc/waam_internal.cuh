@@ -26,6 +26,26 @@ constexpr int64_t kFieldSlack = 65536;
 constexpr int kActiveShards = 64;     // power of two
 constexpr int kActiveShardSlot = 64;  // first shard counter in the counter block
 
+// Cell tiles of the stencil kernels: 32 (k) x 8 (j) threads, one grid z-slice
+// per i, so a cell's coordinates come from the launch geometry without
+// integer division and consecutive lanes touch consecutive k (coalesced).
+constexpr int kTileK = 32;
+constexpr int kTileJ = 8;
+
+inline dim3 tile_grid(const Dims& d) {
+    return dim3((d.nz + kTileK - 1) / kTileK, (d.ny + kTileJ - 1) / kTileJ, d.nx);
+}
+inline dim3 tile_block() { return dim3(kTileK, kTileJ, 1); }
+
+__device__ __forceinline__ bool tile_cell(const Dims& d, int& i, int& j, int& k, int& c) {
+    k = blockIdx.x * kTileK + threadIdx.x;
+    j = blockIdx.y * kTileJ + threadIdx.y;
+    i = blockIdx.z;
+    if (k >= d.nz || j >= d.ny) return false;
+    c = (i * d.ny + j) * d.nz + k;
+    return true;
+}
+
 // Slots of the fused step's device scalars (WaamFields::step_scalars).
 constexpr int kScalarArcK = 0;   // resolved arc k (written by the surface query)
 constexpr int kScalarWsum = 1;   // arc weight sum

@@ -1,0 +1,506 @@
+// Electromagnetic (Lorentz) force of the welding current: kernels.py:1236-1513,
+// driven by physics/weld_forces.py:196-281 solve_lorentz.
+//
+//   sigma map -> Gaussian current source normalised to I -> damped Jacobi
+//   solve of div(sigma grad phi_e) = -source (the substrate below nz_solid
+//   grounded, gas insulating) -> J = -sigma grad phi_e -> axial current binned
+//   by radius per z slab, prefix-summed -> B_theta = mu0 I_enc / (2 pi r)
+//   -> F += f_l (J x B) dt^2 / (rho dx).
+//
+// The Jacobi sweep optionally accumulates the L1 change and the L1 norm of its
+// input (elec_l1_diff, kernels.py:1387-1398) in the same pass, so the host's
+// convergence check every ten sweeps costs no extra grid read.  Grid sums are
+// accumulated in double in a fixed block order (the reference's float atomics
+// have no fixed order); the radial bins use double atomics and are rounded to
+// float before the float prefix sum, as the oracle does.
+#include <cmath>
+
+#include "../../include/waam_b200.h"
+#include "waam_common.cuh"
+#include "waam_internal.cuh"
+
+namespace waam {
+
+#define STREAM(s) reinterpret_cast<cudaStream_t>(s)
+
+namespace {
+
+constexpr int kRedGridMax = kWsMaxPartials / 2;   // two sums share the partials
+constexpr int kMaxBins = 1024;
+constexpr int kOpScalarSourceScale = 16;          // ws.scalars slot of the source scale
+
+// Reduction tiles: the 32 x 8 (k, j) tiles with loops over the tiles and i,
+// so the grid stays at <= kRedGridMax blocks (one partial per block).
+inline dim3 red_tile_grid(const Dims& d) {
+    int gx = imin((d.nz + kTileK - 1) / kTileK, 16);
+    int gy = imin((d.ny + kTileJ - 1) / kTileJ, 16);
+    int gz = imax(1, imin(d.nx, kRedGridMax / (gx * gy)));
+    return dim3(gx, gy, gz);
+}
+
+__device__ __forceinline__ double2 block_sum2(double a, double b) {
+    __shared__ double sh[2][kTileK * kTileJ / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    const int lane = t & 31, wid = t >> 5;
+    if (lane == 0) {
+        sh[0][wid] = a;
+        sh[1][wid] = b;
+    }
+    __syncthreads();
+    double2 r = make_double2(0.0, 0.0);
+    if (t == 0)
+        for (int w = 0; w < kTileK * kTileJ / 32; ++w) {
+            r.x += sh[0][w];
+            r.y += sh[1][w];
+        }
+    __syncthreads();
+    return r;   // valid in thread 0
+}
+
+// Last-block combine of two per-block sums in block order; returns true in the
+// thread that holds the totals.
+__device__ bool finish_sum2(Workspace ws, double2 part, double2& total) {
+    __shared__ bool last;
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned b = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    if (t == 0) {
+        ws.partials[b] = part.x;
+        ws.partials[nb + b] = part.y;
+        __threadfence();
+        unsigned prev = atomicAdd(ws.counter, 1u);
+        last = prev == nb - 1;
+    }
+    __syncthreads();
+    if (!last || t != 0) return false;
+    __threadfence();
+    double x = 0.0, y = 0.0;
+    for (unsigned q = 0; q < nb; ++q) {
+        x += ((volatile double*)ws.partials)[q];
+        y += ((volatile double*)ws.partials)[nb + q];
+    }
+    total = make_double2(x, y);
+    *ws.counter = 0u;
+    return true;
+}
+
+// kernels.py:1237-1251
+__global__ void k_elec_sigma(float* sigma, const float* f_l, const int32_t* flags, int64_t n,
+                             float s_liq, float s_sol) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        int fl = flags[c];
+        sigma[c] = fl == GAS ? 1e-8f : (f_l[c] > 0.55f ? s_liq : s_sol);
+    }
+}
+
+// kernels.py:1255-1284 (clear + inject in one pass)
+__global__ void k_elec_source(Dims d, float* src, float arc_i, float arc_j, float arc_k,
+                              float inv2s2, float current, float vol_eps, int k_min, int k_max) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
+    float v = 0.0f;
+    if (k >= k_min && k <= k_max) {
+        float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - arc_k;
+        float r2 = di * di + dj * dj + 0.25f * dk * dk;
+        v = current * waam_expf(-r2 * inv2s2) / vol_eps;
+    }
+    src[c] = v;
+}
+
+// kernels.py:1288-1301, pass 1: sum(source * cell_vol) -> scale in ws scalars
+__global__ void k_elec_source_sum(const float* src, int64_t n, float cell_vol, float current,
+                                  Workspace ws) {
+    double part = 0.0;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x)
+        part += (double)(src[c] * cell_vol);
+    __shared__ double sh[kThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = part;
+    __syncthreads();
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) t += sh[w];
+        ws.partials[blockIdx.x] = t;
+        __threadfence();
+        last = atomicAdd(ws.counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    double t = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) t += ((volatile double*)ws.partials)[b];
+    float total = (float)t;
+    ws.scalars[kOpScalarSourceScale] = current / fmax_(total, 1e-12f);
+    *ws.counter = 0u;
+}
+
+// kernels.py:1288-1301, pass 2
+__global__ void k_elec_source_scale(float* src, int64_t n, Workspace ws) {
+    const float s = ws.scalars[kOpScalarSourceScale];
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x)
+        src[c] *= s;
+}
+
+// kernels.py:1315-1355 elec_jacobi_step (+ kernels.py:1387-1398 elec_l1_diff
+// of (phi_out, phi_in) when L1 is set).
+template <bool L1>
+__global__ void __launch_bounds__(kTileK* kTileJ)
+    k_elec_jacobi(Dims d, const float* __restrict__ phi_in, float* __restrict__ phi_out,
+                  const float* __restrict__ sigma, const float* __restrict__ src,
+                  const int32_t* __restrict__ flags, float dx, float omega_j, int nz_solid,
+                  float* diff_out, float* norm_out, Workspace ws) {
+    const float eps = 1e-12f;
+    const int sx = d.ny * d.nz, sy = d.nz;
+    double dsum = 0.0, nsum = 0.0;
+    for (int i = blockIdx.z; i < d.nx; i += gridDim.z)
+        for (int jt = blockIdx.y; jt * kTileJ < d.ny; jt += gridDim.y)
+            for (int kt = blockIdx.x; kt * kTileK < d.nz; kt += gridDim.x) {
+                const int k = kt * kTileK + threadIdx.x, j = jt * kTileJ + threadIdx.y;
+                if (k >= d.nz || j >= d.ny) continue;
+                const int c = (i * d.ny + j) * d.nz + k;
+                const int fl = flags[c];
+                const float pin = phi_in[c];
+                float out;
+                if (fl == GAS || (k <= nz_solid && fl == SOLID)) {
+                    out = 0.0f;
+                } else {
+                    const int ip = c + (i + 1 < d.nx ? sx : 0), im = c - (i > 0 ? sx : 0);
+                    const int jp = c + (j + 1 < d.ny ? sy : 0), jm = c - (j > 0 ? sy : 0);
+                    const int kp = c + (k + 1 < d.nz ? 1 : 0), km = c - (k > 0 ? 1 : 0);
+                    const float sp = sigma[ip], sm = sigma[im], sn = sigma[jp], ss = sigma[jm];
+                    const float st = sigma[kp], sb = sigma[km];
+                    const float denom = sp + sm + sn + ss + st + sb + eps;
+                    const float nb = sp * phi_in[ip] + sm * phi_in[im] + sn * phi_in[jp] +
+                                     ss * phi_in[jm] + st * phi_in[kp] + sb * phi_in[km];
+                    const float pn = (nb + src[c] * dx * dx) / denom;
+                    out = (1.0f - omega_j) * pin + omega_j * pn;
+                }
+                phi_out[c] = out;
+                if (L1) {
+                    dsum += (double)fabsf(out - pin);
+                    nsum += (double)fabsf(pin);
+                }
+            }
+    if (L1) {
+        double2 part = block_sum2(dsum, nsum);
+        double2 tot;
+        if (finish_sum2(ws, part, tot)) {
+            *diff_out = (float)tot.x;
+            *norm_out = (float)tot.y;
+        }
+    }
+}
+
+// kernels.py:1387-1398 elec_l1_diff as an operator
+__global__ void __launch_bounds__(kTileK* kTileJ)
+    k_elec_l1(Dims d, const float* __restrict__ a, const float* __restrict__ b, float* diff_out,
+              float* norm_out, Workspace ws) {
+    double dsum = 0.0, nsum = 0.0;
+    for (int i = blockIdx.z; i < d.nx; i += gridDim.z)
+        for (int jt = blockIdx.y; jt * kTileJ < d.ny; jt += gridDim.y)
+            for (int kt = blockIdx.x; kt * kTileK < d.nz; kt += gridDim.x) {
+                const int k = kt * kTileK + threadIdx.x, j = jt * kTileJ + threadIdx.y;
+                if (k >= d.nz || j >= d.ny) continue;
+                const int c = (i * d.ny + j) * d.nz + k;
+                const float bv = b[c];
+                dsum += (double)fabsf(a[c] - bv);
+                nsum += (double)fabsf(bv);
+            }
+    double2 part = block_sum2(dsum, nsum);
+    double2 tot;
+    if (finish_sum2(ws, part, tot)) {
+        *diff_out = (float)tot.x;
+        *norm_out = (float)tot.y;
+    }
+}
+
+// kernels.py:1358-1383 elec_compute_J
+__global__ void k_elec_J(Dims d, float* Jx, float* Jy, float* Jz, const float* __restrict__ phi,
+                         const float* __restrict__ sigma, const int32_t* __restrict__ flags,
+                         float dx) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
+    if (flags[c] == GAS) {
+        Jx[c] = 0.0f;
+        Jy[c] = 0.0f;
+        Jz[c] = 0.0f;
+        return;
+    }
+    const int sx = d.ny * d.nz, sy = d.nz;
+    const float sg = sigma[c];
+    const float two_dx = 2.0f * dx;
+    const float gx = (phi[c + (i + 1 < d.nx ? sx : 0)] - phi[c - (i > 0 ? sx : 0)]) / two_dx;
+    const float gy = (phi[c + (j + 1 < d.ny ? sy : 0)] - phi[c - (j > 0 ? sy : 0)]) / two_dx;
+    const float gz = (phi[c + (k + 1 < d.nz ? 1 : 0)] - phi[c - (k > 0 ? 1 : 0)]) / two_dx;
+    Jx[c] = -sg * gx;
+    Jy[c] = -sg * gy;
+    Jz[c] = -sg * gz;
+}
+
+__device__ __forceinline__ int radial_bin(float di, float dj, float bin_dr, int n_bins,
+                                          float& r) {
+    r = sqrtf(di * di + dj * dj);
+    return imin((int)(r / bin_dr), n_bins - 1);
+}
+
+// kernels.py:1402-1421 elec_bin_axial_current: per z slab, sum of Jz dx^2 by
+// radius bin.  Block (s, k) sums a strip of columns of slab k in shared
+// double bins, then adds them to the slab's double accumulators.
+__global__ void k_elec_bin(Dims d, const float* __restrict__ Jz, double* acc, float arc_i,
+                           float arc_j, float dx2, float bin_dr, int n_bins) {
+    extern __shared__ double sbin[];
+    const int k = blockIdx.y;
+    for (int b = threadIdx.x; b < n_bins; b += blockDim.x) sbin[b] = 0.0;
+    __syncthreads();
+    const int ncol = d.nx * d.ny;
+    for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < ncol;
+         col += gridDim.x * blockDim.x) {
+        const int i = col / d.ny, j = col - i * d.ny;
+        float r;
+        const int b = radial_bin((float)i - arc_i, (float)j - arc_j, bin_dr, n_bins, r);
+        atomicAdd(&sbin[b], (double)(Jz[(int64_t)col * d.nz + k] * dx2));
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < n_bins; b += blockDim.x)
+        if (sbin[b] != 0.0) atomicAdd(&acc[(int64_t)k * n_bins + b], sbin[b]);
+}
+
+__global__ void k_elec_bin_store(const double* acc, float* bins, int64_t m) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m;
+         q += (int64_t)gridDim.x * blockDim.x)
+        bins[q] = (float)acc[q];
+}
+
+// kernels.py:1424-1435 elec_prefix_bins (float, in place)
+__global__ void k_elec_prefix(float* bins, int n_bins, int nz) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nz) return;
+    float a = 0.0f;
+    for (int b = 0; b < n_bins; ++b) {
+        a += bins[(int64_t)k * n_bins + b];
+        bins[(int64_t)k * n_bins + b] = a;
+    }
+}
+
+// kernels.py:1438-1475 elec_B_axisymmetric
+__global__ void k_elec_B(Dims d, float* Bx, float* By, float* Bz, const float* __restrict__ bins,
+                         float arc_i, float arc_j, float dx, float bin_dr, float mu0,
+                         int n_bins) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
+    const float di = (float)i - arc_i, dj = (float)j - arc_j;
+    float rc;
+    const int b = radial_bin(di, dj, bin_dr, n_bins, rc);
+    float bx = 0.0f, by = 0.0f;
+    if (rc > 1e-3f) {
+        const float I = bins[(int64_t)k * n_bins + b];
+        const float rm = rc * dx;
+        const float two_pi = 6.28318530717958647692f;
+        const float Bt = mu0 * I / (two_pi * rm);
+        bx = -Bt * dj / rc;
+        by = Bt * di / rc;
+    }
+    Bx[c] = bx;
+    By[c] = by;
+    Bz[c] = 0.0f;
+}
+
+// kernels.py:1479-1513 apply_lorentz_JxB
+__global__ void k_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* __restrict__ Jx,
+                              const float* __restrict__ Jy, const float* __restrict__ Jz,
+                              const float* __restrict__ Bx, const float* __restrict__ By,
+                              const float* __restrict__ Bz, const float* __restrict__ f_l,
+                              const int32_t* __restrict__ flags, int64_t n, float dt, float dx,
+                              float rho_ref) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const float fl = f_l[c];
+        if (flags[c] == GAS || fl < 0.05f) continue;
+        const float jx = Jx[c], jy = Jy[c], jz = Jz[c], bx = Bx[c], by = By[c], bz = Bz[c];
+        const float fxp = jy * bz - jz * by, fyp = jz * bx - jx * bz, fzp = jx * by - jy * bx;
+        const float flw = fmin_(1.0f, fl);
+        const float scale = flw * dt * dt / (rho_ref * dx);
+        Fx[c] += fxp * scale;
+        Fy[c] += fyp * scale;
+        Fz[c] += fzp * scale;
+    }
+}
+
+}  // namespace
+}  // namespace waam
+
+using namespace waam;
+
+#define REQUIRE(cond, msg) \
+    if (!(cond)) return waam::fail(WAAM_ERR_INVALID, msg)
+
+extern "C" {
+
+int waam_elec_build_sigma(float* sigma, const float* f_l, const int32_t* flags, int64_t n,
+                          float sigma_liquid, float sigma_solid, void* stream) {
+    REQUIRE(sigma && f_l && flags && n > 0, "elec_build_sigma: null field or empty grid");
+    k_elec_sigma<<<elem_blocks(n), kThreads, 0, STREAM(stream)>>>(sigma, f_l, flags, n,
+                                                                  sigma_liquid, sigma_solid);
+    return check_launch("k_elec_sigma");
+}
+
+int waam_elec_inject_arc_source(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
+                                float arc_k, float sigma_cells, float current_A, float dx,
+                                void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_inject_arc_source: bad dims");
+    REQUIRE(source, "elec_inject_arc_source: null field");
+    REQUIRE(std::isfinite(arc_k) && std::isfinite(sigma_cells) && std::fabs(arc_k) < 1e6f &&
+                std::fabs(sigma_cells) < 1e6f,
+            "elec_inject_arc_source: arc k / sigma not finite");
+    const float eps = 1e-6f;
+    const float inv2s2 = 1.0f / (2.0f * sigma_cells * sigma_cells + eps);
+    const float cell_vol = dx * dx * dx;
+    const int k_max = imin(nz, (int)(arc_k + sigma_cells * 4.0f) + 1);
+    const int k_min = imax(0, (int)(arc_k - sigma_cells));
+    Dims d{nx, ny, nz};
+    k_elec_source<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
+        d, source, arc_i, arc_j, arc_k, inv2s2, current_A, cell_vol + eps, k_min, k_max);
+    return check_launch("k_elec_source");
+}
+
+int waam_elec_normalize_source(float* source, int64_t n, float target_current_A, float dx,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+    REQUIRE(source && n > 0, "elec_normalize_source: null field or empty grid");
+    REQUIRE(workspace_ok(workspace, workspace_bytes, n),
+            "elec_normalize_source: workspace too small or misaligned");
+    Workspace ws = Workspace::at(workspace);
+    const float cell_vol = dx * dx * dx;
+    k_elec_source_sum<<<red_blocks(n), kThreads, 0, STREAM(stream)>>>(source, n, cell_vol,
+                                                                      target_current_A, ws);
+    int rc = check_launch("k_elec_source_sum");
+    if (rc) return rc;
+    k_elec_source_scale<<<elem_blocks(n), kThreads, 0, STREAM(stream)>>>(source, n, ws);
+    return check_launch("k_elec_source_scale");
+}
+
+int waam_elec_init_ground(float* phi, int64_t n, void* stream) {
+    REQUIRE(phi && n > 0, "elec_init_ground: null field or empty grid");
+    cudaError_t e = cudaMemsetAsync(phi, 0, (size_t)n * sizeof(float), STREAM(stream));
+    if (e != cudaSuccess) return fail(WAAM_ERR_CUDA, cudaGetErrorString(e));
+    return WAAM_OK;
+}
+
+int waam_elec_jacobi_step(const float* phi_in, float* phi_out, const float* sigma,
+                          const float* source, const int32_t* flags, int nx, int ny, int nz,
+                          float dx, float omega_j, int nz_solid, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_jacobi_step: bad dims");
+    REQUIRE(phi_in && phi_out && sigma && source && flags && phi_in != phi_out,
+            "elec_jacobi_step: null or aliased field");
+    Dims d{nx, ny, nz};
+    k_elec_jacobi<false><<<red_tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
+        d, phi_in, phi_out, sigma, source, flags, dx, omega_j, nz_solid, nullptr, nullptr,
+        Workspace{});
+    return check_launch("k_elec_jacobi");
+}
+
+int waam_elec_jacobi_step_l1(const float* phi_in, float* phi_out, const float* sigma,
+                             const float* source, const int32_t* flags, int nx, int ny, int nz,
+                             float dx, float omega_j, int nz_solid, float* diff_buf,
+                             float* norm_buf, void* workspace, size_t workspace_bytes,
+                             void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_jacobi_step_l1: bad dims");
+    REQUIRE(phi_in && phi_out && sigma && source && flags && diff_buf && norm_buf &&
+                phi_in != phi_out,
+            "elec_jacobi_step_l1: null or aliased field");
+    Dims d{nx, ny, nz};
+    REQUIRE(workspace_ok(workspace, workspace_bytes, d.n()),
+            "elec_jacobi_step_l1: workspace too small or misaligned");
+    k_elec_jacobi<true><<<red_tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
+        d, phi_in, phi_out, sigma, source, flags, dx, omega_j, nz_solid, diff_buf, norm_buf,
+        Workspace::at(workspace));
+    return check_launch("k_elec_jacobi_l1");
+}
+
+int waam_elec_l1_diff(const float* a, const float* b, float* diff_buf, float* norm_buf, int nx,
+                      int ny, int nz, void* workspace, size_t workspace_bytes, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_l1_diff: bad dims");
+    REQUIRE(a && b && diff_buf && norm_buf, "elec_l1_diff: null field");
+    Dims d{nx, ny, nz};
+    REQUIRE(workspace_ok(workspace, workspace_bytes, d.n()),
+            "elec_l1_diff: workspace too small or misaligned");
+    k_elec_l1<<<red_tile_grid(d), tile_block(), 0, STREAM(stream)>>>(d, a, b, diff_buf, norm_buf,
+                                                                     Workspace::at(workspace));
+    return check_launch("k_elec_l1");
+}
+
+int waam_elec_compute_J(float* Jx, float* Jy, float* Jz, const float* phi, const float* sigma,
+                        const int32_t* flags, int nx, int ny, int nz, float dx, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_compute_J: bad dims");
+    REQUIRE(Jx && Jy && Jz && phi && sigma && flags, "elec_compute_J: null field");
+    Dims d{nx, ny, nz};
+    k_elec_J<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(d, Jx, Jy, Jz, phi, sigma, flags,
+                                                               dx);
+    return check_launch("k_elec_J");
+}
+
+int waam_elec_bin_axial_current(const float* Jz, float* bins, int nx, int ny, int nz, float arc_i,
+                                float arc_j, float dx, float bin_dr_cells, int n_bins,
+                                void* workspace, size_t workspace_bytes, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_bin_axial_current: bad dims");
+    REQUIRE(Jz && bins, "elec_bin_axial_current: null field");
+    REQUIRE(n_bins >= 1 && n_bins <= kMaxBins, "elec_bin_axial_current: n_bins out of range");
+    Dims d{nx, ny, nz};
+    REQUIRE(workspace_ok(workspace, workspace_bytes, d.n()),
+            "elec_bin_axial_current: workspace too small or misaligned");
+    // double accumulators in the workspace's field scratch
+    const int64_t m = (int64_t)nz * n_bins;
+    REQUIRE((size_t)m * sizeof(double) <= (size_t)(d.n() + kFieldSlack) * sizeof(float),
+            "elec_bin_axial_current: nz * n_bins accumulators exceed the workspace");
+    Workspace ws = Workspace::at(workspace);
+    double* acc = reinterpret_cast<double*>(ws.field);
+    cudaError_t e = cudaMemsetAsync(acc, 0, (size_t)m * sizeof(double), STREAM(stream));
+    if (e != cudaSuccess) return fail(WAAM_ERR_CUDA, cudaGetErrorString(e));
+    const int ncol = nx * ny;
+    const int strips = imax(1, imin((ncol + kThreads - 1) / kThreads, imax(1, 1184 / nz)));
+    k_elec_bin<<<dim3(strips, nz), kThreads, n_bins * sizeof(double), STREAM(stream)>>>(
+        d, Jz, acc, arc_i, arc_j, dx * dx, bin_dr_cells, n_bins);
+    int rc = check_launch("k_elec_bin");
+    if (rc) return rc;
+    k_elec_bin_store<<<elem_blocks(m), kThreads, 0, STREAM(stream)>>>(acc, bins, m);
+    return check_launch("k_elec_bin_store");
+}
+
+int waam_elec_prefix_bins(float* bins, int n_bins, int nz, void* stream) {
+    REQUIRE(bins && n_bins >= 1 && nz >= 1, "elec_prefix_bins: bad arguments");
+    k_elec_prefix<<<(nz + 127) / 128, 128, 0, STREAM(stream)>>>(bins, n_bins, nz);
+    return check_launch("k_elec_prefix");
+}
+
+int waam_elec_B_axisymmetric(float* Bx, float* By, float* Bz, const float* bins, int nx, int ny,
+                             int nz, float arc_i, float arc_j, float dx, float bin_dr_cells,
+                             float mu0, int n_bins, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_B_axisymmetric: bad dims");
+    REQUIRE(Bx && By && Bz && bins, "elec_B_axisymmetric: null field");
+    REQUIRE(n_bins >= 1, "elec_B_axisymmetric: n_bins out of range");
+    Dims d{nx, ny, nz};
+    k_elec_B<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(d, Bx, By, Bz, bins, arc_i, arc_j,
+                                                               dx, bin_dr_cells, mu0, n_bins);
+    return check_launch("k_elec_B");
+}
+
+int waam_apply_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* Jx, const float* Jy,
+                           const float* Jz, const float* Bx, const float* By, const float* Bz,
+                           const float* f_l, const int32_t* flags, int64_t n, float dt, float dx,
+                           float rho_ref, void* stream) {
+    REQUIRE(Fx && Fy && Fz && Jx && Jy && Jz && Bx && By && Bz && f_l && flags && n > 0,
+            "apply_lorentz_JxB: null field or empty grid");
+    k_lorentz_JxB<<<elem_blocks(n), kThreads, 0, STREAM(stream)>>>(Fx, Fy, Fz, Jx, Jy, Jz, Bx, By,
+                                                                   Bz, f_l, flags, n, dt, dx,
+                                                                   rho_ref);
+    return check_launch("k_lorentz_JxB");
+}
+
+}  // extern "C"

@@ -510,3 +510,101 @@ def bind_velocity_set(grid):
 
 
 __all__ = [n for n in dir() if not n.startswith("_") and n not in ("math", "torch")]
+
+
+# ------------------------------------------------------------- Lorentz ----
+# kernels.py:1236-1513 (electric potential, current density, self field, J x B)
+
+def elec_build_sigma(sigma, f_l, flags, sigma_liquid, sigma_solid, FLAG_GAS):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = sigma.numel()
+    _call("waam_elec_build_sigma", _f(sigma, n), _f(f_l, n), _i(flags, n), n,
+          float(sigma_liquid), float(sigma_solid), _stream())
+
+
+def elec_clear_source(source):
+    source.zero_()
+
+
+def elec_inject_arc_source(source, arc_i, arc_j, arc_k, sigma_cells, current_A, dx, nz):
+    nx, ny, nz_ = _dims(source)
+    if int(nz) != nz_:
+        raise WaamError("elec_inject_arc_source: nz=%d does not match the field (%d)" % (nz, nz_))
+    _call("waam_elec_inject_arc_source", _f(source), nx, ny, nz_, float(arc_i), float(arc_j),
+          float(arc_k), float(sigma_cells), float(current_A), float(dx), _stream())
+
+
+def elec_normalize_source(source, target_current_A, dx):
+    ws, wsb = workspace_for(source)
+    _call("waam_elec_normalize_source", _f(source), source.numel(), float(target_current_A),
+          float(dx), ws, wsb, _stream())
+
+
+def elec_init_ground(phi, flags, nz_solid, FLAG_SOLID):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID)
+    _call("waam_elec_init_ground", _f(phi), phi.numel(), _stream())
+
+
+def elec_jacobi_step(phi_in, phi_out, sigma, source, flags, dx, omega_j, FLAG_GAS, FLAG_SOLID,
+                     nz_solid, nx, ny, nz):
+    _flags_ok(FLAG_GAS=FLAG_GAS, FLAG_SOLID=FLAG_SOLID)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_elec_jacobi_step", _f(phi_in, n), _f(phi_out, n), _f(sigma, n), _f(source, n),
+          _i(flags, n), int(nx), int(ny), int(nz), float(dx), float(omega_j), int(nz_solid),
+          _stream())
+
+
+def elec_jacobi_step_l1(phi_in, phi_out, sigma, source, flags, dx, omega_j, nz_solid, diff_buf,
+                        norm_buf):
+    """elec_jacobi_step then elec_l1_diff(phi_out, phi_in, diff_buf, norm_buf), one pass."""
+    nx, ny, nz = _dims(phi_in)
+    n = phi_in.numel()
+    ws, wsb = workspace_for(phi_in)
+    _call("waam_elec_jacobi_step_l1", _f(phi_in, n), _f(phi_out, n), _f(sigma, n),
+          _f(source, n), _i(flags, n), nx, ny, nz, float(dx), float(omega_j), int(nz_solid),
+          _f(diff_buf, 1), _f(norm_buf, 1), ws, wsb, _stream())
+
+
+def elec_l1_diff(a, b, diff_buf, norm_buf):
+    nx, ny, nz = _dims(a)
+    ws, wsb = workspace_for(a)
+    _call("waam_elec_l1_diff", _f(a), _f(b, a.numel()), _f(diff_buf, 1), _f(norm_buf, 1), nx,
+          ny, nz, ws, wsb, _stream())
+
+
+def elec_compute_J(Jx, Jy, Jz, phi, sigma, flags, dx, FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_elec_compute_J", _f(Jx, n), _f(Jy, n), _f(Jz, n), _f(phi, n), _f(sigma, n),
+          _i(flags, n), int(nx), int(ny), int(nz), float(dx), _stream())
+
+
+def elec_bin_axial_current(Jz, bins, arc_i, arc_j, dx, bin_dr_cells, n_bins, nz):
+    nx, ny, nz_ = _dims(Jz)
+    if tuple(bins.shape) != (nz_, int(n_bins)):
+        raise WaamError("elec_bin_axial_current: bins must be (nz, n_bins)")
+    ws, wsb = workspace_for(Jz)
+    _call("waam_elec_bin_axial_current", _f(Jz), _f(bins, nz_ * int(n_bins)), nx, ny, nz_,
+          float(arc_i), float(arc_j), float(dx), float(bin_dr_cells), int(n_bins), ws, wsb,
+          _stream())
+
+
+def elec_prefix_bins(bins, n_bins, nz):
+    _call("waam_elec_prefix_bins", _f(bins, int(n_bins) * int(nz)), int(n_bins), int(nz),
+          _stream())
+
+
+def elec_B_axisymmetric(Bx, By, Bz, bins, arc_i, arc_j, dx, bin_dr_cells, mu0, n_bins, nz):
+    nx, ny, nz_ = _dims(Bx)
+    n = Bx.numel()
+    _call("waam_elec_B_axisymmetric", _f(Bx, n), _f(By, n), _f(Bz, n),
+          _f(bins, nz_ * int(n_bins)), nx, ny, nz_, float(arc_i), float(arc_j), float(dx),
+          float(bin_dr_cells), float(mu0), int(n_bins), _stream())
+
+
+def apply_lorentz_JxB(Fx, Fy, Fz, Jx, Jy, Jz, Bx, By, Bz, f_l, flags, dt, dx, rho_ref, FLAG_GAS):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = Fx.numel()
+    _call("waam_apply_lorentz_JxB", _f(Fx, n), _f(Fy, n), _f(Fz, n), _f(Jx, n), _f(Jy, n),
+          _f(Jz, n), _f(Bx, n), _f(By, n), _f(Bz, n), _f(f_l, n), _i(flags, n), n, float(dt),
+          float(dx), float(rho_ref), _stream())

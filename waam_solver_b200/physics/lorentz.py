@@ -1,0 +1,92 @@
+"""Electromagnetic force of the welding current (physics/weld_forces.py:196-281).
+
+The same sequence as the reference: conductivity map, Gaussian current source
+normalised to the welding current, a warm-started damped Jacobi solve of the
+electric potential with a relative-L1 convergence check every ten sweeps,
+current density, axisymmetric self field from the enclosed axial current and
+the f_l-weighted J x B body force added to F.
+
+Two differences of form, not of result: the potential ping-pongs between
+``phi_elec`` and ``phi_elec_tmp`` instead of copying the new iterate back
+(after the solve ``phi_elec`` holds the last iterate, ``phi_elec_tmp`` the one
+before it), and the L1 change is computed inside the last sweep of each chunk
+of ten -- the only sweep whose L1 the reference reads.
+"""
+from __future__ import annotations
+
+import math
+
+from .. import kernels
+
+MU0 = 4.0e-7 * math.pi
+
+
+def _jacobi_budget(twin, g, cold_start):
+    max_iters = max(int(twin.lorentz_jacobi_iters), 20)
+    if cold_start:
+        n_max = max(g.nx, g.ny, g.nz)
+        max_iters = max(max_iters, 2 * n_max * n_max)
+    return max_iters
+
+
+def solve_lorentz(twin, g, arc_i, arc_j, arc_k):
+    if not twin.enable_lorentz:
+        return
+    g.ensure_lorentz_fields()
+    kernels.elec_build_sigma(g.sigma_elec, g.f_l, g.flags, twin.sigma_liquid_Sm,
+                             twin.sigma_solid_Sm, g.FLAG_GAS)
+    kernels.elec_inject_arc_source(g.elec_source, arc_i, arc_j, arc_k, twin.sigma_cells,
+                                   twin.welding_current_A, g.dx, g.nz)
+    kernels.elec_normalize_source(g.elec_source, twin.welding_current_A, g.dx)
+
+    cold_start = not getattr(twin, "_lorentz_warm", False)
+    if cold_start:
+        kernels.elec_init_ground(g.phi_elec, g.flags, twin.nz_solid, g.FLAG_SOLID)
+        twin._lorentz_warm = True
+    max_iters = _jacobi_budget(twin, g, cold_start)
+    tol = float(getattr(twin, "lorentz_jacobi_tol", 1e-4))
+    check_every = 10
+    converged = False
+    iters_done = 0
+    rel = float("inf")
+    while iters_done < max_iters:
+        chunk = min(check_every, max_iters - iters_done)
+        for c in range(chunk):
+            if c == chunk - 1:
+                kernels.elec_jacobi_step_l1(g.phi_elec, g.phi_elec_tmp, g.sigma_elec,
+                                            g.elec_source, g.flags, g.dx,
+                                            twin.lorentz_jacobi_omega, twin.nz_solid,
+                                            g.elec_res_buf, g.elec_norm_buf)
+            else:
+                kernels.elec_jacobi_step(g.phi_elec, g.phi_elec_tmp, g.sigma_elec,
+                                         g.elec_source, g.flags, g.dx,
+                                         twin.lorentz_jacobi_omega, g.FLAG_GAS, g.FLAG_SOLID,
+                                         twin.nz_solid, g.nx, g.ny, g.nz)
+            g.phi_elec, g.phi_elec_tmp = g.phi_elec_tmp, g.phi_elec
+            iters_done += 1
+        rel = float(g.elec_res_buf.item()) / max(float(g.elec_norm_buf.item()), 1e-30)
+        if rel < tol:
+            converged = True
+            break
+    if not converged:
+        twin._lorentz_unconverged = getattr(twin, "_lorentz_unconverged", 0) + 1
+        twin._lorentz_unconverged_streak = getattr(twin, "_lorentz_unconverged_streak", 0) + 1
+        n_bad = twin._lorentz_unconverged
+        if n_bad in (1, 10, 100) or n_bad % 1000 == 0:
+            print("[weld_forces] WARNING: Lorentz Jacobi hit %d iters without converging "
+                  "(rel change=%.2e > %.0e); raise lorentz_jacobi_iters. (%d occurrences)"
+                  % (max_iters, rel, tol, n_bad))
+    else:
+        twin._lorentz_unconverged_streak = 0
+    twin._lorentz_last_iters = iters_done
+
+    kernels.elec_compute_J(g.Jx, g.Jy, g.Jz, g.phi_elec, g.sigma_elec, g.flags, g.dx, g.FLAG_GAS,
+                           g.nx, g.ny, g.nz)
+    bin_dr_cells = max(float(max(g.nx, g.ny)) / (2.0 * g.n_elec_bins), 0.5)
+    kernels.elec_bin_axial_current(g.Jz, g.elec_rad_bins, arc_i, arc_j, g.dx, bin_dr_cells,
+                                   g.n_elec_bins, g.nz)
+    kernels.elec_prefix_bins(g.elec_rad_bins, g.n_elec_bins, g.nz)
+    kernels.elec_B_axisymmetric(g.Bx, g.By, g.Bz, g.elec_rad_bins, arc_i, arc_j, g.dx,
+                                bin_dr_cells, MU0, g.n_elec_bins, g.nz)
+    kernels.apply_lorentz_JxB(g.Fx, g.Fy, g.Fz, g.Jx, g.Jy, g.Jz, g.Bx, g.By, g.Bz, g.f_l, g.flags,
+                              g.dt, g.dx, twin.mat.rho, g.FLAG_GAS)

@@ -137,6 +137,10 @@ class WAAMTwin:
         self._deposited_volume_m3 = 0.0
         self._n_droplets_fired = 0
         self._deposition_overflow = 0
+        self._lorentz_warm = False
+        self._lorentz_unconverged = 0
+        self._lorentz_unconverged_streak = 0
+        self.lorentz_jacobi_tol = 1e-4
         self.plate_thickness_mm = None
         self.plate_size_mm = None
         self.plate_origin_mm = None
@@ -251,6 +255,8 @@ class WAAMTwin:
         self._deposition_overflow = 0
         self._last_torch_pos_m = None
         self._torch_dir_xyz = (1.0, 0.0, 0.0)
+        self._lorentz_warm = False
+        self._lorentz_unconverged_streak = 0
         g.deposit_vol_buf.zero_()
         g.deposit_real_buf.zero_()
         self.invalidate()
@@ -271,7 +277,14 @@ class WAAMTwin:
         self._check_strict_mode()
 
     def _check_strict_mode(self):
-        if not self.strict_mode or self._n_droplets_fired < 20:
+        if not self.strict_mode:
+            return
+        streak = int(getattr(self, "_lorentz_unconverged_streak", 0) or 0)
+        if self.enable_lorentz and streak > 50:
+            raise RuntimeError("[strict_mode] Lorentz Jacobi failed to converge for %d "
+                               "consecutive steps -- raise lorentz_jacobi_iters or disable "
+                               "strict_mode" % streak)
+        if self._n_droplets_fired < 20:
             return
         ratio = self._deposited_volume_m3 * self.mat.rho / max(
             self._n_droplets_fired * droplet_mass_kg(self), 1e-12)
