@@ -352,8 +352,9 @@ def run_b200(args, w):
         traffic = t["dram_bytes"] * per / t["cells_touched"]
     step_bytes = sum(algo.values())
     lib = _native.lib()
-    launches_per_step = lib.waam_step_launch_count(tw._fused_params, 0) + \
-        lib.waam_step_launch_count(tw._fused_params, 1)
+    pre = lib.waam_step_launch_count(tw._fused_params, 0)
+    launches_graph = pre + lib.waam_step_launch_count(tw._fused_params, 1)
+    launches_events = pre + lib.waam_step_launch_count(tw._fused_params, 2)
 
     # ---- end-to-end run through the public API with host inputs / outputs ----
     probe = (g.nx // 2) * g.ny * g.nz + (g.ny // 2) * g.nz + tw.nz_solid - 1
@@ -392,7 +393,7 @@ def run_b200(args, w):
         "host_enqueue_ms_per_step": host_ms,
         "cell_census": c,
         "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 4},
-        "gpu_launches": int(launches_per_step * (2 * K + Ks)),
+        "gpu_launches": int(launches_graph * 2 * K + launches_events * Ks),
         "stage_timing": "events between the fused kernels over %d instrumented steps "
                         "(eager launches); value/e2e steps replay CUDA graphs" % Ks,
         "clocks": clocks.summary(),

@@ -33,8 +33,8 @@ extern "C" {
 
 const char* waam_last_error(void);
 int waam_abi_version(void);
-/* Bytes of device workspace needed by the reducing entry points for a grid
- * of n cells (a field-sized snapshot plus block partial sums). */
+/* Bytes of device workspace needed by the reducing entry points and the fused
+ * step for a grid of n cells (block partial sums and a field-sized scratch). */
 size_t waam_workspace_bytes(int64_t n);
 
 /* ---- operator API: one entry per reference Taichi kernel ---------------- */
@@ -327,7 +327,11 @@ typedef struct WaamStepParams {
  * the arc weight sum, the arc heat injection and the enthalpy cap
  * (solvers/coupled_step.py:34-108).  The host then performs droplet
  * deposition if one is due, and calls waam_step_main for the rest of the
- * step (coupled_step.py:168-458). */
+ * step (coupled_step.py:168-458).  waam_step_main forks independent kernels
+ * onto a second stream of the library's own (one per device, created on the
+ * first call -- make that call outside any stream capture) and joins it back
+ * into `stream` before returning; a capture of `stream` records the fork as
+ * graph branches. */
 int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
                   size_t workspace_bytes, void* stream);
 int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace,
@@ -339,7 +343,8 @@ int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace
 int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* workspace,
                           size_t workspace_bytes, void* const* events, int n_events,
                           void* stream);
-/* Number of kernels the fused stages launch (for launch accounting). */
+/* Number of kernels the fused stages launch (for launch accounting): stage 0
+ * waam_step_pre, 1 waam_step_main, 2 waam_step_main_events. */
 int waam_step_launch_count(const WaamStepParams* p, int stage);
 
 #if defined(__GNUC__)

@@ -161,3 +161,26 @@ def test_lorentz_steps_match_oracle():
         steps.compare_state("lorentz step %d" % s, dict(tw.grid.state_dict(), **got),
                             ot.s, fields=steps.FIELDS + list(LORENTZ_FIELDS))
     assert ot.lorentz_iters[0] > ot.lorentz_iters[-1]    # cold start, then warm starts
+
+
+def test_overlapped_step_matches_serial_stage_timing_path():
+    """The fused step with its second-stream overlap equals the serial path
+    that records stage events, bit for bit."""
+    states = []
+    for timed in (False, True):
+        tw, ot, dx = _config_twins("c2", 40, 24, 24)
+        tw.use_cuda_graphs = False
+        tw._last_droplet_time = -1.0
+        for s in range(8):
+            if timed:
+                evs = [torch.cuda.Event(enable_timing=True) for _ in range(7)]
+                for e in evs:
+                    e.record()      # torch creates the CUDA event on its first record
+                tw._stage_events = evs
+            tw.step(0.3 * 40 * dx + s * 1e-6, 12 * dx, True)
+        tw._stage_events = None
+        torch.cuda.synchronize()
+        states.append(tw.grid.state_dict())
+    for k, v in states[0].items():
+        if isinstance(v, np.ndarray):
+            assert np.array_equal(v, states[1][k]), k

@@ -12,6 +12,7 @@
 // coordinates come from the launch geometry without integer division, and
 // consecutive lanes touch consecutive k (coalesced, k is the fastest axis).
 #include <cmath>
+#include <mutex>
 
 #include "../../include/waam_b200.h"
 #include "waam_common.cuh"
@@ -23,6 +24,7 @@ namespace waam {
 
 #define STREAM(s) reinterpret_cast<cudaStream_t>(s)
 constexpr int kMainEvents = 7;
+constexpr int kMaxDevices = 64;
 constexpr int kTileRedBlocks = 592;   // <= kWsMaxPartials
 constexpr int kListThreads = 128;
 constexpr int kListBlocks = 148 * 6;
@@ -183,13 +185,11 @@ __device__ __forceinline__ int stream_source(const Dims& d, bool interior, int i
     return (ni * d.ny + nj) * d.nz + nk;
 }
 
-__global__ void __launch_bounds__(256) k_stream(Dims d, const float* __restrict__ f_src,
-                                                float* __restrict__ f_dst,
-                                                const int32_t* __restrict__ flags) {
-    int i, j, k, c;
-    if (!tile_cell(d, i, j, k, c)) return;
-    const int flag = flags[c];
-    if (flag == SOLID) return;
+// One cell of the pull (non-solid cells only).
+__device__ __forceinline__ void stream_cell(const Dims& d, const float* __restrict__ f_src,
+                                            float* __restrict__ f_dst,
+                                            const int32_t* __restrict__ flags, int i, int j, int k,
+                                            int c, int flag) {
     const size_t n = (size_t)d.n();
     const bool interior = i > 0 && i < d.nx - 1 && j > 0 && j < d.ny - 1 && k > 0 && k < d.nz - 1;
     float v[19];
@@ -203,6 +203,16 @@ __global__ void __launch_bounds__(256) k_stream(Dims d, const float* __restrict_
     }
 #pragma unroll
     for (int q = 0; q < 19; ++q) f_dst[q * n + c] = v[q];
+}
+
+__global__ void __launch_bounds__(256) k_stream(Dims d, const float* __restrict__ f_src,
+                                                float* __restrict__ f_dst,
+                                                const int32_t* __restrict__ flags) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
+    const int flag = flags[c];
+    if (flag == SOLID) return;
+    stream_cell(d, f_src, f_dst, flags, i, j, k, c, flag);
 }
 
 int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags, void* stream) {
@@ -551,6 +561,11 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
         const int r = c / d.nz;
         const int j = r % d.ny;
         const int i = r / d.ny;
+        // the populations (DRAM) are requested first so that their latency
+        // overlaps the force stencil (cache-resident phi, T, flags)
+        float f[19], o[19];
+#pragma unroll
+        for (int q = 0; q < 19; ++q) f[q] = f_src[q * n + c];
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
         if (a.from_buffer) {
             fx = Fx[c];
@@ -559,9 +574,6 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
         }
         float fl = f_l[c];
         cell_forces(d, P, phi, T, flags, i, j, k, fl, fx, fy, fz);
-        float f[19], o[19];
-#pragma unroll
-        for (int q = 0; q < 19; ++q) f[q] = f_src[q * n + c];
         float rr, u, v, w;
         if (a.kind == 0)
             collide_mrt_cell(f, fl, fx, fy, fz, a.omega, a.omega_b, a.C_darcy, o, rr, u, v, w);
@@ -654,6 +666,37 @@ static ArcParams arc_params(const WaamStepParams* p) {
     return a;
 }
 
+// Second stream and fork/join events of the fused step, one set per device
+// (created on the first step on that device, which should not be inside a
+// stream capture).  Calls on different host threads share them; every fork is
+// ordered by its own event record, so sharing only serialises.
+struct AuxStream {
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+static int aux_stream(AuxStream** out) {
+    static std::mutex mu;
+    static AuxStream table[kMaxDevices];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(WAAM_ERR_CUDA, cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return fail(WAAM_ERR_INVALID, "step_main: device index");
+    std::lock_guard<std::mutex> lock(mu);
+    AuxStream& a = table[dev];
+    if (!a.s2) {
+        e = cudaStreamCreateWithFlags(&a.s2, cudaStreamNonBlocking);
+        for (int q = 0; q < 2 && e == cudaSuccess; ++q)
+            e = cudaEventCreateWithFlags(&a.ev[q], cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            a.s2 = nullptr;
+            return fail(WAAM_ERR_CUDA, cudaGetErrorString(e));
+        }
+    }
+    *out = &a;
+    return WAAM_OK;
+}
+
 static bool fields_ok(const WaamFields* f) {
     return f && f->f_src && f->f_dst && f->rho && f->ux && f->uy && f->uz && f->T && f->T_next &&
            f->H && f->H_next && f->f_l && f->phi && f->phi_tmp && f->flags && f->T_max &&
@@ -669,7 +712,8 @@ extern "C" {
 int waam_step_launch_count(const WaamStepParams* p, int stage) {
     if (!p) return 0;
     if (stage == 0) return p->welding ? 3 : 1;
-    int n = 1 /*thermal*/ + (p->vof ? 1 : 0) + 1 /*column*/ + 1 /*collide*/ + 1 /*stream*/;
+    // thermal, [vof], column, collide, stream
+    int n = 1 + (p->vof ? 1 : 0) + 1 + 1 + 1;
     if (p->substrate_growth || p->bead_freeze) n += 1;
     return n;
 }
@@ -710,6 +754,8 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     if (!fields_ok(f) || !p) return fail(WAAM_ERR_INVALID, "step_main: bad fields or params");
     if (events && n_events < kMainEvents)
         return fail(WAAM_ERR_INVALID, "step_main: need 7 events");
+    for (int q = 0; events && q < kMainEvents; ++q)
+        if (!events[q]) return fail(WAAM_ERR_INVALID, "step_main: null event handle");
     auto mark = [&](int i) {
         if (events) cudaEventRecord(reinterpret_cast<cudaEvent_t>(events[i]), STREAM(stream));
     };
@@ -741,19 +787,48 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     ta.dx = p->dx;
     ta.sigma_sb = p->sigma_sb;
     ta.h_floor = p->cp_rho * p->T_amb;
+    // Without stage events, VOF advection (reads phi, u, flags; writes phi_tmp)
+    // runs on a second stream beside the thermal stage (reads H, T, u, flags;
+    // writes the thermal fields and f_l).
+    AuxStream* aux = nullptr;
+    const bool overlap = events == nullptr;
+    if (overlap) {
+        int ea = aux_stream(&aux);
+        if (ea) return ea;
+    }
+    auto fork = [&](int q) {
+        cudaEventRecord(aux->ev[q], s);
+        cudaStreamWaitEvent(aux->s2, aux->ev[q], 0);
+    };
+    auto join = [&](int q) {
+        cudaEventRecord(aux->ev[q], aux->s2);
+        cudaStreamWaitEvent(s, aux->ev[q], 0);
+    };
+    int e;
+    if (overlap && p->vof) {
+        fork(0);
+        k_vof_advect<<<tile_grid(d), tile_block(), 0, aux->s2>>>(d, f->phi, f->phi_tmp, f->ux,
+                                                                  f->uy, f->uz, f->flags);
+        e = check_launch("k_vof_advect");
+        if (e) return e;
+    }
     mark(0);
     k_thermal_fused<<<tile_grid(d), tile_block(), 0, s>>>(
         d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
         f->T_prev, f->dT_dt, active_count, ta);
-    int e = check_launch("k_thermal_fused");
+    e = check_launch("k_thermal_fused");
     if (e) return e;
     mark(1);
 
     if (p->vof) {
-        k_vof_advect<<<tile_grid(d), tile_block(), 0, s>>>(d, f->phi, f->phi_tmp, f->ux, f->uy,
-                                                            f->uz, f->flags);
-        e = check_launch("k_vof_advect");
-        if (e) return e;
+        if (overlap) {
+            join(1);
+        } else {
+            k_vof_advect<<<tile_grid(d), tile_block(), 0, s>>>(d, f->phi, f->phi_tmp, f->ux,
+                                                                f->uy, f->uz, f->flags);
+            e = check_launch("k_vof_advect");
+            if (e) return e;
+        }
     }
     mark(2);
     ColumnArgs ca;

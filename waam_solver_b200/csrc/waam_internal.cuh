@@ -24,6 +24,11 @@ constexpr int kWsMaxPartials = 4096;
 constexpr size_t kWsFieldOffset = 33792;
 constexpr int64_t kFieldSlack = 65536;
 constexpr int kActiveShards = 64;     // power of two
+
+inline size_t ws_total_bytes(int64_t n) {
+    size_t field = (size_t)((n > 0 ? n : 0) + kFieldSlack) * sizeof(float);
+    return kWsFieldOffset + ((field + 255) & ~(size_t)255);
+}
 constexpr int kActiveShardSlot = 64;  // first shard counter in the counter block
 
 // Cell tiles of the stencil kernels: 32 (k) x 8 (j) threads, one grid z-slice

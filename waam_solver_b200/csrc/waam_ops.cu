@@ -647,11 +647,7 @@ const char* waam_last_error(void) { return waam::g_last_error.c_str(); }
 
 int waam_abi_version(void) { return 1; }
 
-size_t waam_workspace_bytes(int64_t n) {
-    size_t field = (size_t)((n > 0 ? n : 0) + waam::kFieldSlack) * sizeof(float);
-    field = (field + 255) & ~(size_t)255;
-    return waam::kWsFieldOffset + field;
-}
+size_t waam_workspace_bytes(int64_t n) { return waam::ws_total_bytes(n); }
 
 int waam_init_grid(float* f, float* rho, float* ux, float* uy, float* uz, float* T, float* H,
                    float* f_l, float* phi, int32_t* flags, int nx, int ny, int nz, float T_amb,
