@@ -73,13 +73,13 @@ def twin_kwargs(w):
     return {k: w[k] for k in keys if k in w}
 
 
-def build_twin(w, device):
+def build_twin(w, device, population_dtype="float32"):
     from waam_solver_b200 import WAAMTwin
     from waam_solver_b200.materials import from_constants
     from waam_solver_b200.physics.arc import goldak_from_job_mm
     mat = from_constants("ER70S-6-constants", MATERIAL, contact_angle_deg=w.get("contact_angle_deg", 30.0))
     tw = WAAMTwin(material=mat, nx=w["nx"], ny=w["ny"], nz=w["nz"], dx=w["dx"], max_tracers=1024,
-                  device=device, **twin_kwargs(w))
+                  device=device, population_dtype=population_dtype, **twin_kwargs(w))
     if w.get("plate_thickness_mm"):
         tw.plate_thickness_mm = w["plate_thickness_mm"]
     if w.get("wire_feed_m_s"):
@@ -278,6 +278,54 @@ def run_reference(args, w):
     print(json.dumps(line), flush=True)
 
 
+def storage_forms(w, device, K, ref_ms):
+    """The same workload with 16-bit population storage (float16 / bfloat16
+    offsets from the rest weights): whole-step time over K device-resident
+    steps after the same spin-up, plus the stream stage alone."""
+    import torch
+    out = {}
+    for dtype in ("float16", "bfloat16"):
+        tw = build_twin(w, device, population_dtype=dtype)
+        g = tw.grid
+        pos = positions(w, g.dt, w["spinup"] + K + 204)
+        s = 0
+        for _ in range(w["spinup"]):
+            tw.step(*pos[s], True)
+            s += 1
+        dev_pos = torch.tensor([[x / g.dx, y / g.dx] for x, y in pos[s:s + K]],
+                               dtype=torch.float32, device=device)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(K):
+            tw._device_position = dev_pos[k]
+            tw.step(*pos[s], True)
+            s += 1
+        e1.record()
+        torch.cuda.synchronize()
+        tw._device_position = None
+        ms = e0.elapsed_time(e1) / K
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(7)] for _ in range(200)]
+        for es in evs:
+            for e in es:
+                e.record()
+        for es in evs:
+            tw._stage_events = es
+            tw.step(*pos[s], True)
+            s += 1
+        torch.cuda.synchronize()
+        tw._stage_events = None
+        stream_ms = statistics.fmean(es[4].elapsed_time(es[5]) for es in evs)
+        c = census(tw)
+        stream_bytes = 4 * c["n"] + 76 * (c["n"] - c["solid"])
+        out[dtype] = {"value": g.n_cells / (ms * 1e-3) / 1e6, "unit": "MLUPS", "ms_per_step": ms,
+                      "vs_float32": ref_ms / ms, "stream_ms": stream_ms,
+                      "stream_GBps": stream_bytes / (stream_ms * 1e-3) / 1e9, "steps": K}
+        del tw, g
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_b200(args, w):
     import torch
     from waam_solver_b200 import _native
@@ -398,6 +446,10 @@ def run_b200(args, w):
                         "(eager launches); value/e2e steps replay CUDA graphs" % Ks,
         "clocks": clocks.summary(),
     }
+    if world == 1:
+        line["precision_forms"] = storage_forms(w, device, min(K, 1000), ms / K)
+        line["precision_forms"]["storage"] = ("headline value: float32 populations; forms: "
+                                              "16-bit offsets f_q - w_q, float32 arithmetic")
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:

@@ -190,18 +190,28 @@ int waam_feed_wire_surface(float* f_src, int32_t* flags, float* f_l, float* phi,
  * from *vol_acc / *real_acc, attempt t > 0 runs only while the converted
  * volume *real_acc is below accept_volume (compared in double) and starts
  * with both budgets at that volume.  One launch, no host round trip between
- * attempts; read *real_acc afterwards for the placed volume. */
+ * attempts; read *real_acc afterwards for the placed volume.  f_src holds
+ * populations in the storage f_storage (as WaamStepParams.f_storage). */
 #define WAAM_DEPOSIT_MAX_TRIES 16
-int waam_deposit_droplet(float* f_src, int32_t* flags, float* f_l, float* phi, float* H, float* T,
-                         float* rho, int nx, int ny, int nz, float arc_i, float arc_j, float arc_k,
-                         const float* foot_radii, int n_tries, double accept_volume, float drop_r,
-                         float target_vol, float T_drop, float cp_rho, float L_rho, float rho0,
-                         float* vol_acc, float* real_acc, float cell_vol, void* stream);
+int waam_deposit_droplet(void* f_src, int f_storage, int32_t* flags, float* f_l, float* phi,
+                         float* H, float* T, float* rho, int nx, int ny, int nz, float arc_i,
+                         float arc_j, float arc_k, const float* foot_radii, int n_tries,
+                         double accept_volume, float drop_r, float target_vol, float T_drop,
+                         float cp_rho, float L_rho, float rho0, float* vol_acc, float* real_acc,
+                         float cell_vol, void* stream);
 /* kernels.py:1176-1233 feed_wire_momentum_impact (physics/weld_forces.py:534-542) */
 int waam_feed_wire_momentum_impact(float* f_src, const float* rho, float* ux, float* uy,
                                    float* uz, const int32_t* flags, const float* f_l, int nx,
                                    int ny, int nz, float arc_i, float arc_j, float arc_k,
                                    float drop_r, float vx, float vy, float vz, void* stream);
+/* feed_wire_momentum_impact on populations in any storage (f_storage as
+ * WaamStepParams.f_storage); no counterpart in the reference, which stores
+ * float32 only. */
+int waam_feed_wire_momentum_impact_stored(void* f_src, int f_storage, const float* rho, float* ux,
+                                          float* uy, float* uz, const int32_t* flags,
+                                          const float* f_l, int nx, int ny, int nz, float arc_i,
+                                          float arc_j, float arc_k, float drop_r, float vx,
+                                          float vy, float vz, void* stream);
 /* kernels.py:1142-1173 apply_droplet_impact_pressure (physics/weld_forces.py:543-550) */
 int waam_apply_droplet_impact_pressure(float* Fz, const int32_t* flags, const float* phi,
                                        const float* f_l, int nx, int ny, int nz, float arc_i,
@@ -259,8 +269,9 @@ int waam_apply_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* Jx, con
 /* ---- fused step: the B200 pipeline of solvers/coupled_step.py:73-464 ----- */
 
 typedef struct WaamFields {
-    float* f_src;   /* populations read by this step's collide (grid.f_src) */
-    float* f_dst;   /* populations written by collide, streamed back into f_src */
+    /* populations, elements per WaamStepParams.f_storage (float or 16-bit) */
+    void* f_src;    /* read by this step's collide (grid.f_src) */
+    void* f_dst;    /* written by collide, streamed back into f_src */
     float* rho;
     float* ux;
     float* uy;
@@ -321,6 +332,10 @@ typedef struct WaamStepParams {
     float T800, T1100;
     int substrate_growth, bead_freeze;
     float dir_x, dir_y, dir_z, lookback, T_freeze;
+    /* population storage of f_src / f_dst: 0 float32 f_q; 1 float16 and
+     * 2 bfloat16 offsets f_q - w_q (rho0 = 1), rounded to nearest; the
+     * arithmetic is float32 in every case */
+    int f_storage;
 } WaamStepParams;
 
 /* Stages of one fused step.  waam_step_pre runs the surface-height query,

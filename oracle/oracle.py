@@ -1,7 +1,8 @@
 """ctypes binding of the C oracle -- TEST INFRASTRUCTURE ONLY.
 
 Loads ``oracle/_build/libwaam_oracle.so`` (built by ``make -C oracle``) and
-exposes each restated reference kernel on numpy arrays.  Only the parity
+exposes each restated reference kernel on numpy arrays; ``fp64`` is the same
+source built in double precision.  Only the parity
 tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
 use this module; the product never imports it.
 """
@@ -15,6 +16,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libwaam_oracle.so")
+LIB64_PATH = os.path.join(HERE, "_build", "libwaam_oracle64.so")
 
 _F = C.POINTER(C.c_float)
 _I = C.POINTER(C.c_int32)
@@ -72,44 +74,59 @@ _SIGS = {
     "wo_set_num_threads": ([C.c_int], None),
 }
 
-_lib = None
-
-
 def build():
     """Compile the oracle with its Makefile (gcc; seconds)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
+class Oracle:
+    """One build of the oracle: float32 (``libwaam_oracle.so``) or the same
+    source in double precision (``libwaam_oracle64.so``, float -> double in
+    every signature)."""
+
+    def __init__(self, fp64=False):
+        self.fp64 = fp64
+        self.dtype = np.float64 if fp64 else np.float32
+        self.path = LIB64_PATH if fp64 else LIB_PATH
+        self._lib = None
+
+    def lib(self):
+        if self._lib is None:
+            if not os.path.exists(self.path):
+                build()
+            L = C.CDLL(self.path)
+            fptr, fval = (C.POINTER(C.c_double), C.c_double) if self.fp64 else (_F, _f)
+            for name, (args, res) in _SIGS.items():
+                fn = getattr(L, name)
+                fn.argtypes = [fptr if a is _F else (fval if a is _f else a) for a in args]
+                fn.restype = C.c_double if (self.fp64 and res is C.c_float) else res
+            self._lib = L
+        return self._lib
+
+    def _ptr(self, a):
+        if a.dtype == self.dtype:
+            assert a.flags.c_contiguous
+            return a.ctypes.data_as(C.POINTER(C.c_double) if self.fp64 else _F)
+        if a.dtype == np.int32:
+            assert a.flags.c_contiguous
+            return a.ctypes.data_as(_I)
+        raise TypeError("oracle arrays must be %s or int32, got %s" % (
+            np.dtype(self.dtype).name, a.dtype))
+
+    def call(self, name, *args):
+        """Call oracle function ``name``; numpy arrays are passed by pointer."""
+        conv = [self._ptr(a) if isinstance(a, np.ndarray) else a for a in args]
+        return getattr(self.lib(), name)(*conv)
+
+
+fp32 = Oracle(False)
+fp64 = Oracle(True)
+
+
 def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            build()
-        L = C.CDLL(LIB_PATH)
-        for name, (args, res) in _SIGS.items():
-            fn = getattr(L, name)
-            fn.argtypes = args
-            fn.restype = res
-        _lib = L
-    return _lib
-
-
-def _ptr(a):
-    if a.dtype == np.float32:
-        assert a.flags.c_contiguous
-        return a.ctypes.data_as(_F)
-    if a.dtype == np.int32:
-        assert a.flags.c_contiguous
-        return a.ctypes.data_as(_I)
-    raise TypeError("oracle arrays must be float32 or int32, got %s" % a.dtype)
+    return fp32.lib()
 
 
 def call(name, *args):
-    """Call oracle function ``name``; numpy arrays are passed by pointer."""
-    conv = []
-    for a in args:
-        if isinstance(a, np.ndarray):
-            conv.append(_ptr(a))
-        else:
-            conv.append(a)
-    return getattr(lib(), name)(*conv)
+    """Call float32 oracle function ``name``; numpy arrays are passed by pointer."""
+    return fp32.call(name, *args)

@@ -24,7 +24,11 @@ _W = np.array([1.0 / 3.0] + [1.0 / 18.0] * 6 + [1.0 / 36.0] * 12, dtype=np.float
 class OracleTwin:
     """Constants-only material, Gaussian2D / Goldak / conical arc, MRT or SRT."""
 
-    def __init__(self, nx, ny, nz, dx, mat, **kw):
+    def __init__(self, nx, ny, nz, dx, mat, precision="fp32", **kw):
+        if precision not in ("fp32", "fp64"):
+            raise ValueError("precision must be fp32 or fp64")
+        self.O = O.fp64 if precision == "fp64" else O.fp32
+        self.ft = self.O.dtype
         self.nx, self.ny, self.nz, self.dx = nx, ny, nz, dx
         self.mat = dict(mat)
         m = self.mat
@@ -91,19 +95,19 @@ class OracleTwin:
     def reset(self):
         nx, ny, nz = self.nx, self.ny, self.nz
         sh = (nx, ny, nz)
-        z = lambda: np.zeros(sh, np.float32)  # noqa: E731
-        s = dict(f_a=np.zeros((19,) + sh, np.float32), f_b=np.zeros((19,) + sh, np.float32),
+        z = lambda: np.zeros(sh, self.ft)  # noqa: E731
+        s = dict(f_a=np.zeros((19,) + sh, self.ft), f_b=np.zeros((19,) + sh, self.ft),
                  rho=z(), ux=z(), uy=z(), uz=z(), T=z(), H=z(), f_l=z(), phi=z(), phi_tmp=z(),
                  flags=np.zeros(sh, np.int32), T_max=z(), T_prev=z(), dT_dt=z(),
                  time_above_800_s=z(), time_above_1100_s=z(), time_above_solidus_s=z(),
                  Fx=z(), Fy=z(), Fz=z())
         T0 = self.cfg["T_ambient"]
-        O.call("wo_init_grid", s["f_a"], s["rho"], s["ux"], s["uy"], s["uz"], s["T"], s["H"],
+        self.O.call("wo_init_grid", s["f_a"], s["rho"], s["ux"], s["uy"], s["uz"], s["T"], s["H"],
                s["f_l"], s["phi"], s["flags"], nx, ny, nz, T0, 1.0, self.cp_rho, self.nz_solid,
                0, nx, 0, ny)
-        s["T_max"][...] = np.float32(T0)
-        s["T_prev"][...] = np.float32(T0)
-        O.call("wo_stream", s["f_a"], s["f_b"], s["flags"], nx, ny, nz)
+        s["T_max"][...] = self.ft(T0)
+        s["T_prev"][...] = self.ft(T0)
+        self.O.call("wo_stream", s["f_a"], s["f_b"], s["flags"], nx, ny, nz)
         s["read_is_a"] = True
         self.s = s
         self.lorentz_warm = False
@@ -114,8 +118,10 @@ class OracleTwin:
 
     def load(self, st):
         """Adopt a state dict (numpy arrays named like the reference grid)."""
-        self.s = {k: (np.ascontiguousarray(v).copy() if isinstance(v, np.ndarray) else v)
-                  for k, v in st.items()}
+        def own(v):
+            v = np.ascontiguousarray(v).copy()
+            return v.astype(self.ft) if v.dtype.kind == "f" else v
+        self.s = {k: (own(v) if isinstance(v, np.ndarray) else v) for k, v in st.items()}
         self.s.setdefault("phi_tmp", np.zeros_like(self.s["phi"]))
         self.s.setdefault("read_is_a", True)
 
@@ -188,13 +194,13 @@ class OracleTwin:
         arc_i, arc_j = x / self.dx, y / self.dx
         i0 = max(0, min(int(arc_i), nx - 1))
         j0 = max(0, min(int(arc_j), ny - 1))
-        k = float(O.call("wo_surface_height_at", s["phi"], s["flags"], nx, ny, nz, i0, j0,
+        k = float(self.O.call("wo_surface_height_at", s["phi"], s["flags"], nx, ny, nz, i0, j0,
                          self.nz_solid))
         if k < 1.0:
             k = float(max(1, self.nz_solid - 1))
         arc_k = self.arc_k = k
         Ts, Tl = m["T_solidus"], m["T_liquidus"]
-        O.call("wo_clear_forces", s["Fx"], s["Fy"], s["Fz"], n)
+        self.O.call("wo_clear_forces", s["Fx"], s["Fy"], s["Fz"], n)
         pen = c["arc_penetration_mm"] * 1e-3 / self.dx
         en = 1 if c["arc_surface_weighting"] else 0
         cap = c["enable_enthalpy_cap"]
@@ -203,87 +209,87 @@ class OracleTwin:
             if hs in ("goldak", "goldak3d", "doubleellipsoid"):
                 g = c["goldak"]
                 sign = 1.0 if c["travel_speed_m_s"] >= 0.0 else -1.0
-                O.call("wo_inject_goldak_heat", s["H"], s["flags"], s["f_l"], nx, ny, nz, arc_i,
+                self.O.call("wo_inject_goldak_heat", s["H"], s["flags"], s["f_l"], nx, ny, nz, arc_i,
                        arc_j, arc_k, c["arc_power_W"], self.dt, self.dx ** 3,
                        c["arc_efficiency"], sign, g["ff"], g["fr"], g["a_front"], g["a_rear"],
                        g["b"], g["c"], pen, en)
             elif hs in ("conical", "conicalvolume", "cone"):
-                O.call("wo_inject_arc_heat", s["H"], s["flags"], s["f_l"], nx, ny, nz, arc_i,
+                self.O.call("wo_inject_arc_heat", s["H"], s["flags"], s["f_l"], nx, ny, nz, arc_i,
                        arc_j, arc_k - 1.5, c["arc_power_W"], self.sigma_cells * 1.2, self.dt,
                        self.dx ** 3, c["arc_efficiency"], pen, en)
             else:
-                O.call("wo_inject_arc_heat", s["H"], s["flags"], s["f_l"], nx, ny, nz, arc_i,
+                self.O.call("wo_inject_arc_heat", s["H"], s["flags"], s["f_l"], nx, ny, nz, arc_i,
                        arc_j, arc_k, c["arc_power_W"], self.sigma_cells, self.dt, self.dx ** 3,
                        c["arc_efficiency"], pen, en)
             if cap:
-                O.call("wo_clamp_enthalpy_ceiling_scalar", s["H"], s["flags"], n, self.cp_rho,
+                self.O.call("wo_clamp_enthalpy_ceiling_scalar", s["H"], s["flags"], n, self.cp_rho,
                        Ts, Tl, c["T_vapor_cap_K"], self.L_rho)
             self._maybe_droplet(arc_i, arc_j, arc_k)
-        O.call("wo_advect_diffuse_temperature", s["H"], s["T"], s["ux"], s["uy"], s["uz"],
+        self.O.call("wo_advect_diffuse_temperature", s["H"], s["T"], s["ux"], s["uy"], s["uz"],
                s["flags"], nx, ny, nz, self.alpha_lu, 1.0, self.cp_rho)
         if c["enable_heat_loss"]:
-            O.call("wo_apply_thermal_boundary_losses", s["H"], s["T"], s["flags"], nx, ny, nz,
+            self.O.call("wo_apply_thermal_boundary_losses", s["H"], s["T"], s["flags"], nx, ny, nz,
                    c["T_ambient"], c["h_conv"], c["eps_rad"], int(c["enable_convection"]),
                    int(c["enable_radiation"]), self.dt, self.dx, 5.670374419e-8)
-            O.call("wo_clamp_enthalpy_floor_scalar", s["H"], self.cp_rho, s["flags"], n,
+            self.O.call("wo_clamp_enthalpy_floor_scalar", s["H"], self.cp_rho, s["flags"], n,
                    c["T_ambient"])
-        O.call("wo_update_phase", s["H"], s["T"], s["f_l"], n, self.cp_rho, self.L_rho, Ts, Tl)
+        self.O.call("wo_update_phase", s["H"], s["T"], s["f_l"], n, self.cp_rho, self.L_rho, Ts, Tl)
         if cap:
-            O.call("wo_clamp_enthalpy_ceiling_scalar", s["H"], s["flags"], n, self.cp_rho, Ts,
+            self.O.call("wo_clamp_enthalpy_ceiling_scalar", s["H"], s["flags"], n, self.cp_rho, Ts,
                    Tl, c["T_vapor_cap_K"], self.L_rho)
-        O.call("wo_update_phase", s["H"], s["T"], s["f_l"], n, self.cp_rho, self.L_rho, Ts, Tl)
-        O.call("wo_update_T_max", s["T"], s["T_max"], s["flags"], n)
-        O.call("wo_update_cooling_rate", s["T"], s["T_prev"], s["dT_dt"], s["flags"], n, self.dt)
+        self.O.call("wo_update_phase", s["H"], s["T"], s["f_l"], n, self.cp_rho, self.L_rho, Ts, Tl)
+        self.O.call("wo_update_T_max", s["T"], s["T_max"], s["flags"], n)
+        self.O.call("wo_update_cooling_rate", s["T"], s["T_prev"], s["dT_dt"], s["flags"], n, self.dt)
         if c["enable_vof"]:
-            O.call("wo_advect_phi", s["phi_tmp"], s["phi"], s["ux"], s["uy"], s["uz"],
+            self.O.call("wo_advect_phi", s["phi_tmp"], s["phi"], s["ux"], s["uy"], s["uz"],
                    s["flags"], nx, ny, nz)
             s["phi"][...] = s["phi_tmp"]
-            O.call("wo_reinitialize_phi", s["phi"], s["flags"], n)
+            self.O.call("wo_reinitialize_phi", s["phi"], s["flags"], n)
             if c["enable_wetting"]:
-                O.call("wo_apply_contact_angle_phi_bc", s["phi"], s["flags"], nx, ny, nz,
+                self.O.call("wo_apply_contact_angle_phi_bc", s["phi"], s["flags"], nx, ny, nz,
                        self.theta)
-            O.call("wo_update_flags_from_phi", s["phi"], s["f_l"], s["flags"], nx, ny, nz,
+            self.O.call("wo_update_flags_from_phi", s["phi"], s["f_l"], s["flags"], nx, ny, nz,
                    self.nz_solid)
-            O.call("wo_sync_phi_liquid_fraction", s["phi"], s["f_l"], s["flags"], n)
+            self.O.call("wo_sync_phi_liquid_fraction", s["phi"], s["f_l"], s["flags"], n)
         if c["enable_csf_tension"]:
-            O.call("wo_compute_csf_tension", s["phi"], s["flags"], s["Fx"], s["Fy"], s["Fz"], nx,
+            self.O.call("wo_compute_csf_tension", s["phi"], s["flags"], s["Fx"], s["Fy"], s["Fz"], nx,
                    ny, nz, self.gamma_lu, int(c["enable_wetting"]), self.theta)
-        O.call("wo_compute_marangoni_force", s["T"], s["phi"], s["f_l"], s["Fx"], s["Fy"],
+        self.O.call("wo_compute_marangoni_force", s["T"], s["phi"], s["f_l"], s["Fx"], s["Fy"],
                s["Fz"], s["flags"], nx, ny, nz, self.dgamma_dT_lu)
         if welding:
-            O.call("wo_apply_arc_pressure", s["Fz"], s["flags"], s["phi"], nx, ny, nz, arc_i,
+            self.O.call("wo_apply_arc_pressure", s["Fz"], s["flags"], s["phi"], nx, ny, nz, arc_i,
                    arc_j, arc_k, self.arc_sigma_m / self.dx, c["arc_pressure_pa"], self.dt,
                    self.dx, m["rho"])
         if c["enable_hydrostatic_gravity"]:
-            O.call("wo_add_hydrostatic_gravity", s["Fz"], s["f_l"], s["flags"], n, 1.0, self.g_lu)
-        O.call("wo_add_buoyancy", s["T"], s["Fz"], s["f_l"], s["flags"], n, self.g_lu,
+            self.O.call("wo_add_hydrostatic_gravity", s["Fz"], s["f_l"], s["flags"], n, 1.0, self.g_lu)
+        self.O.call("wo_add_buoyancy", s["T"], s["Fz"], s["f_l"], s["flags"], n, self.g_lu,
                m["beta_T"], Tl, 1.0)
         if welding and c["enable_lorentz"]:
             self._lorentz(arc_i, arc_j, arc_k)
-        O.call("wo_clamp_body_force_magnitude", s["Fx"], s["Fy"], s["Fz"], s["flags"], n, 0.05)
+        self.O.call("wo_clamp_body_force_magnitude", s["Fx"], s["Fy"], s["Fz"], s["flags"], n, 0.05)
         if c["use_srt"]:
-            O.call("wo_collide_srt", self.fsrc(), self.fdst(), s["rho"], s["ux"], s["uy"],
+            self.O.call("wo_collide_srt", self.fsrc(), self.fdst(), s["rho"], s["ux"], s["uy"],
                    s["uz"], s["Fx"], s["Fy"], s["Fz"], s["f_l"], s["flags"], n, self.omega,
                    c["C_darcy"])
         else:
-            O.call("wo_collide_mrt", self.fsrc(), self.fdst(), s["rho"], s["ux"], s["uy"],
+            self.O.call("wo_collide_mrt", self.fsrc(), self.fdst(), s["rho"], s["ux"], s["uy"],
                    s["uz"], s["Fx"], s["Fy"], s["Fz"], s["f_l"], s["flags"], n, self.omega,
                    self.omega_bulk, c["C_darcy"])
-        O.call("wo_clamp_velocity_mach", s["ux"], s["uy"], s["uz"], s["flags"], n, 0.08)
-        O.call("wo_stream", self.fdst(), self.fsrc(), s["flags"], nx, ny, nz)
-        O.call("wo_update_time_above_T", s["T"], s["flags"], s["time_above_800_s"],
+        self.O.call("wo_clamp_velocity_mach", s["ux"], s["uy"], s["uz"], s["flags"], n, 0.08)
+        self.O.call("wo_stream", self.fdst(), self.fsrc(), s["flags"], nx, ny, nz)
+        self.O.call("wo_update_time_above_T", s["T"], s["flags"], s["time_above_800_s"],
                s["time_above_1100_s"], s["time_above_solidus_s"], n, self.dt, 800.0 + 273.15,
                1100.0 + 273.15, Ts)
         if c["enable_substrate_growth"] or c["enable_bead_freeze"]:
-            O.call("wo_remelt_hot_solid_scalar", s["T"], s["H"], s["f_l"], s["phi"], s["flags"],
+            self.O.call("wo_remelt_hot_solid_scalar", s["T"], s["H"], s["f_l"], s["phi"], s["flags"],
                    n, self.cp_rho, Ts, Tl, self.L_rho)
             if welding and c["enable_bead_freeze"]:
                 lb = max(2.0, c["trailing_solidify_lookback_mm"] / (self.dx * 1000.0))
-                O.call("wo_solidify_trailing_pool_scalar", s["T"], s["H"], s["f_l"], s["phi"],
+                self.O.call("wo_solidify_trailing_pool_scalar", s["T"], s["H"], s["f_l"], s["phi"],
                        s["flags"], s["ux"], s["uy"], s["uz"], nx, ny, nz, self.cp_rho, arc_i,
                        arc_j, arc_k, self.dir[0], self.dir[1], self.dir[2], lb,
                        Tl + c["trailing_solidify_temp_margin_K"], Ts)
-            O.call("wo_solidify_cooled_metal", s["T"], s["f_l"], s["phi"], s["flags"], s["ux"],
+            self.O.call("wo_solidify_cooled_metal", s["T"], s["f_l"], s["phi"], s["flags"], s["ux"],
                    s["uy"], s["uz"], n, Ts, 1)
         s["read_is_a"] = not s["read_is_a"]
         self.step_n += 1
@@ -296,15 +302,15 @@ class OracleTwin:
         sh = (nx, ny, nz)
         for f in ("phi_elec", "phi_elec_tmp", "sigma_elec", "elec_source", "Jx", "Jy", "Jz", "Bx",
                   "By", "Bz"):
-            s.setdefault(f, np.zeros(sh, np.float32))
+            s.setdefault(f, np.zeros(sh, self.ft))
         n_bins = 64
-        s.setdefault("elec_rad_bins", np.zeros((nz, n_bins), np.float32))
+        s.setdefault("elec_rad_bins", np.zeros((nz, n_bins), self.ft))
         I = c["welding_current_A"]
-        O.call("wo_elec_build_sigma", s["sigma_elec"], s["f_l"], s["flags"], n,
+        self.O.call("wo_elec_build_sigma", s["sigma_elec"], s["f_l"], s["flags"], n,
                c["sigma_liquid_Sm"], c["sigma_solid_Sm"])
-        O.call("wo_elec_inject_arc_source", s["elec_source"], nx, ny, nz, arc_i, arc_j, arc_k,
+        self.O.call("wo_elec_inject_arc_source", s["elec_source"], nx, ny, nz, arc_i, arc_j, arc_k,
                self.sigma_cells, I, self.dx)
-        O.call("wo_elec_normalize_source", s["elec_source"], n, I, self.dx)
+        self.O.call("wo_elec_normalize_source", s["elec_source"], n, I, self.dx)
         cold = not self.lorentz_warm
         if cold:
             s["phi_elec"][...] = 0.0
@@ -317,25 +323,25 @@ class OracleTwin:
         d, m = ctypes.c_double(), ctypes.c_double()
         while done < max_iters:
             for _ in range(min(10, max_iters - done)):
-                O.call("wo_elec_jacobi_step", s["phi_elec"], s["phi_elec_tmp"], s["sigma_elec"],
+                self.O.call("wo_elec_jacobi_step", s["phi_elec"], s["phi_elec_tmp"], s["sigma_elec"],
                        s["elec_source"], s["flags"], nx, ny, nz, self.dx,
                        c["lorentz_jacobi_omega"], self.nz_solid)
-                O.call("wo_elec_l1_diff", s["phi_elec_tmp"], s["phi_elec"], n, ctypes.byref(d),
+                self.O.call("wo_elec_l1_diff", s["phi_elec_tmp"], s["phi_elec"], n, ctypes.byref(d),
                        ctypes.byref(m))
                 s["phi_elec"][...] = s["phi_elec_tmp"]
                 done += 1
-            rel = float(np.float32(d.value)) / max(float(np.float32(m.value)), 1e-30)
+            rel = float(self.ft(d.value)) / max(float(self.ft(m.value)), 1e-30)
             if rel < c["lorentz_jacobi_tol"]:
                 break
         self.lorentz_iters.append(done)
-        O.call("wo_elec_compute_J", s["Jx"], s["Jy"], s["Jz"], s["phi_elec"], s["sigma_elec"],
+        self.O.call("wo_elec_compute_J", s["Jx"], s["Jy"], s["Jz"], s["phi_elec"], s["sigma_elec"],
                s["flags"], nx, ny, nz, self.dx)
         bin_dr = max(float(max(nx, ny)) / (2.0 * n_bins), 0.5)
-        O.call("wo_elec_bins", s["Jz"], s["elec_rad_bins"], nx, ny, nz, arc_i, arc_j, self.dx,
+        self.O.call("wo_elec_bins", s["Jz"], s["elec_rad_bins"], nx, ny, nz, arc_i, arc_j, self.dx,
                bin_dr, n_bins)
-        O.call("wo_elec_B_axisymmetric", s["Bx"], s["By"], s["Bz"], s["elec_rad_bins"], nx, ny,
+        self.O.call("wo_elec_B_axisymmetric", s["Bx"], s["By"], s["Bz"], s["elec_rad_bins"], nx, ny,
                nz, arc_i, arc_j, self.dx, bin_dr, 4.0e-7 * math.pi, n_bins)
-        O.call("wo_apply_lorentz_JxB", s["Fx"], s["Fy"], s["Fz"], s["Jx"], s["Jy"], s["Jz"],
+        self.O.call("wo_apply_lorentz_JxB", s["Fx"], s["Fy"], s["Fz"], s["Jx"], s["Jy"], s["Jz"],
                s["Bx"], s["By"], s["Bz"], s["f_l"], s["flags"], n, self.dt, self.dx,
                self.mat["rho"])
 
@@ -360,9 +366,9 @@ class OracleTwin:
         placed = 0.0
         nx, ny, nz = self.nx, self.ny, self.nz
         for _ in range(10):
-            va = np.array([placed], np.float32)
-            ra = np.array([placed], np.float32)
-            O.call("wo_feed_wire_surface", self.fsrc(), s["flags"], s["f_l"], s["phi"], s["H"],
+            va = np.array([placed], self.ft)
+            ra = np.array([placed], self.ft)
+            self.O.call("wo_feed_wire_surface", self.fsrc(), s["flags"], s["f_l"], s["phi"], s["H"],
                    s["T"], s["rho"], nx, ny, nz, arc_i, arc_j, arc_k, r_try, r, vol, T_drop,
                    self.cp_rho, self.L_rho, 1.0, va, ra, self.dx ** 3)
             placed = float(ra[0])
@@ -379,12 +385,12 @@ class OracleTwin:
             v_xy = min(v * 0.65, max(c["travel_speed_m_s"], abs(v) * math.tan(lead)))
             v_z = -math.sqrt(max(v * v - v_xy * v_xy, v * v * 0.2))
             k = self.dt / self.dx
-            O.call("wo_feed_wire_momentum_impact", self.fsrc(), s["rho"], s["ux"], s["uy"],
+            self.O.call("wo_feed_wire_momentum_impact", self.fsrc(), s["rho"], s["ux"], s["uy"],
                    s["uz"], s["flags"], s["f_l"], nx, ny, nz, arc_i, arc_j, arc_k, r,
                    v_xy * ddx * k, v_xy * ddy * k, v_z * k)
             if c["enable_droplet_impact_pressure"]:
                 rm = r * self.dx
                 pa = 0.5 * mass * v * v / max(math.pi * rm * rm, 1e-12) if mass > 0 else 0.0
-                O.call("wo_apply_droplet_impact_pressure", s["Fz"], s["flags"], s["phi"],
+                self.O.call("wo_apply_droplet_impact_pressure", s["Fz"], s["flags"], s["phi"],
                        s["f_l"], nx, ny, nz, arc_i, arc_j, arc_k, r, pa, self.dt, self.dx,
                        m["rho"])

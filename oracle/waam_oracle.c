@@ -7,16 +7,28 @@
  * reference source up to the rounding of exp/sin/cos.  Parallel loops
  * (OpenMP) are used only where every cell writes only itself.
  */
-#include "waam_oracle.h"
-/* The same float exponential the CUDA kernels use (Cody-Waite + Taylor), so
- * that exp rounding does not blur the oracle/GPU comparison. */
-#include "../waam_solver_b200/csrc/waam_expf.h"
-
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
 #include <omp.h>
+#endif
+
+#ifdef WAAM_ORACLE_FP64
+/* FP64 build (make fp64): every float of this file and of waam_oracle.h is a
+ * double and the exponential is the C library's -- the double-precision run
+ * that the reduced-precision population storage is measured against. */
+#define float double
+#define sqrtf sqrt
+#define fabsf fabs
+#define waam_expf exp
+#include "waam_oracle.h"
+#else
+#include "waam_oracle.h"
+/* The same float exponential the CUDA kernels use (Cody-Waite + Taylor), so
+ * that exp rounding does not blur the oracle/GPU comparison. */
+#include "../waam_solver_b200/csrc/waam_expf.h"
 #endif
 
 #define FLUID 0

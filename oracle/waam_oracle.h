@@ -8,7 +8,7 @@
  * row-major with k fastest, populations are (19, nx, ny, nz); flags are int32
  * with FLUID=0, SOLID=1, GAS=2, IFACE=4.
  *
- * Semantics pinned where the reference is racy (see DESIGN.md):
+ * Semantics pinned where the reference is racy:
  *   wo_advect_diffuse_temperature  -- neighbour reads of H see the value from
  *                                     before the kernel (snapshot);
  *   wo_apply_contact_angle_phi_bc  -- sequential in k within a column,

@@ -1,0 +1,159 @@
+"""16-bit population storage (float16 / bfloat16 offsets f_q - w_q).
+
+* One fused step from the same state in float32 and in 16-bit storage: every
+  field but the populations is bit-identical (the kernels compute in float32
+  on w_q + offset), the populations differ by at most the rounding of the
+  stored offset.
+* The c1 configuration (64x32x32, Gaussian 3 kW arc, VOF, MRT) in float32,
+  float16 and bfloat16 storage against the FP64 oracle: from reset for 2000
+  steps (the plate heats; no pool forms in 2000 steps, since the flag rules
+  keep every cell below nz_solid solid and there is no wire feed), and from a
+  seeded molten pool for 500 steps (flow, phase change and free surface
+  active).  Compared: peak T of the metal, pool width / depth, max |u| in the
+  liquid and total enthalpy; bounds for float32 and float16: peak T within
+  0.5 %, width / depth within one cell, total enthalpy within 0.1 %; bfloat16
+  (8-bit significand) within 3 %, two cells and 1 %.
+"""
+import numpy as np
+import pytest
+import torch
+
+import steps
+
+pytestmark = pytest.mark.gpu
+
+NON_F = [f for f in steps.FIELDS if f not in ("f_a", "f_b")]
+ULP_BITS = {"float16": 11, "bfloat16": 8}
+
+
+def _c2_twin(dtype, shape=(40, 24, 24)):
+    from waam_solver_b200 import WAAMTwin
+    from waam_solver_b200.materials import from_constants
+    from waam_solver_b200.physics.arc import Goldak3D
+    mat = from_constants("m", steps.MATERIAL, contact_angle_deg=30.0)
+    tw = WAAMTwin(material=mat, nx=shape[0], ny=shape[1], nz=shape[2], dx=2e-4, max_tracers=64,
+                  use_srt=False, enable_vof=True, travel_speed_m_s=0.008, heat_source="goldak",
+                  arc_power_W=4000.0, arc_efficiency=0.78, arc_sigma_mm=1.0,
+                  droplet_freq_hz=100.0, enable_wetting=True, enable_csf_tension=True,
+                  enable_hydrostatic_gravity=True, population_dtype=dtype)
+    tw.wire_feed_m_s = 0.1
+    tw.droplet_transfer_mode = "pulsed"
+    tw.pulse_frequency_hz = 100.0
+    tw.droplet_size_jitter = 0.0
+    tw.arc_source = Goldak3D(ff=0.6, fr=1.4, a_front=5.0, a_rear=12.0, b=5.0, c=4.0)
+    tw.reset()
+    return tw
+
+
+@pytest.mark.parametrize("dtype", ["float16", "bfloat16"])
+def test_one_step_matches_float32_up_to_storage_rounding(dtype):
+    import state_gen
+    shape = (40, 24, 24)
+    t16 = _c2_twin(dtype, shape)
+    st = state_gen.seeded_state(*shape, seed=5, nz_solid=t16.nz_solid)
+    st["read_is_a"] = True
+    t16.grid.load_state({k: v for k, v in st.items() if k != "nz_solid"})
+    # the float32 twin starts from exactly the populations the 16-bit twin holds
+    start = t16.grid.state_dict()
+    t32 = _c2_twin("float32", shape)
+    t32.grid.load_state(start)
+    dx = 2e-4
+    for tw in (t16, t32):
+        tw._last_droplet_time = 1e9     # no droplet: compare the plain step
+        tw.step(0.3 * shape[0] * dx, (shape[1] // 2) * dx, True)
+    torch.cuda.synchronize()
+    a, b = t16.grid.state_dict(), t32.grid.state_dict()
+    for f in NON_F:
+        assert np.array_equal(a[f], b[f]), f
+    w = t32.grid.w.cpu().numpy().reshape(19, 1, 1, 1)
+    for f in ("f_a", "f_b"):
+        off = np.abs(b[f].astype(np.float64) - w)
+        # half an ulp of the stored offset (relative 2^-11 / 2^-8; 2^-25 absolute for
+        # float16 subnormals) plus the float32 rounding of w_q + offset (2^-25 below 0.5)
+        bound = off * 2.0 ** -ULP_BITS[dtype] + 2.0 ** -24
+        err = np.abs(a[f].astype(np.float64) - b[f].astype(np.float64))
+        assert np.all(err <= bound), (f, float((err - bound).max()))
+
+
+def _c1_run(storage, case):
+    import state_gen
+    from oracle.oracle_step import OracleTwin
+    from waam_solver_b200 import WAAMTwin
+    from waam_solver_b200.materials import from_constants
+    nx, ny, nz, dx = 64, 32, 32, 2.5e-4
+    seeded = case == "seeded_pool"
+    n_steps = 500 if seeded else 2000
+    kw = dict(use_srt=False, enable_vof=True, travel_speed_m_s=0.008, heat_source="gaussian2d",
+              arc_power_W=3000.0, arc_efficiency=0.75, arc_sigma_mm=1.0 if seeded else 3.0,
+              droplet_freq_hz=0.0)
+    y = (ny // 2) * dx
+    xs = [0.004 + s * 0.008 * dx * 0.1 for s in range(n_steps)]
+    start = None
+    if seeded:
+        start = state_gen.seeded_state(nx, ny, nz, seed=3, nz_solid=16)
+        start = {k: v for k, v in start.items() if k != "nz_solid"}
+        start["read_is_a"] = True
+    if storage == "fp64_oracle":
+        ot = OracleTwin(nx, ny, nz, dx, steps.MATERIAL, precision="fp64",
+                        plate_thickness_mm=4.0, **kw)
+        ot.reset()
+        if start:
+            ot.load(start)
+        for x in xs:
+            ot.step(x, y, True)
+        return ot.s, ot.nz_solid
+    mat = from_constants("m", steps.MATERIAL, contact_angle_deg=80.0)
+    tw = WAAMTwin(material=mat, nx=nx, ny=ny, nz=nz, dx=dx, max_tracers=64,
+                  population_dtype=storage, **kw)
+    tw.plate_thickness_mm = 4.0
+    tw.reset()
+    if start:
+        tw.grid.load_state(start)
+    for x in xs:
+        tw.step(x, y, True)
+    torch.cuda.synchronize()
+    return tw.grid.state_dict(), tw.nz_solid
+
+
+def _summary(st, nz_solid, dx=2.5e-4):
+    fl = st["f_l"] > 0.5
+    metal = st["flags"] != 2
+    out = {"T_peak": float(st["T"].astype(np.float64)[metal].max()),
+           "H_total": float(st["H"].astype(np.float64).sum()) * dx ** 3,
+           "u_max": 0.0, "width_cells": 0, "depth_cells": 0, "n_liquid": int(fl.sum())}
+    if fl.any():
+        u = np.sqrt(st["ux"].astype(np.float64) ** 2 + st["uy"].astype(np.float64) ** 2 +
+                    st["uz"].astype(np.float64) ** 2)
+        out["u_max"] = float(u[fl].max())
+        ii = np.nonzero(fl)[0]
+        sect = fl[int(round(ii.mean()))]
+        ys, zs = np.nonzero(sect.any(axis=1))[0], np.nonzero(sect.any(axis=0))[0]
+        if ys.size:
+            out["width_cells"] = int(ys[-1] - ys[0] + 1)
+            out["depth_cells"] = max(0, nz_solid - int(zs[0]))
+    return out
+
+
+# (peak T relative, width / depth cells, total enthalpy relative): the targets
+# for float32 and float16 storage; bfloat16 (8-bit significand) is reported
+# against looser bounds.
+BOUNDS = {"float32": (5e-3, 1, 1e-3), "float16": (5e-3, 1, 1e-3), "bfloat16": (3e-2, 2, 1e-2)}
+
+
+@pytest.mark.parametrize("case", ["reset", "seeded_pool"])
+def test_storage_forms_against_fp64_oracle(case):
+    ref_state, nzs = _c1_run("fp64_oracle", case)
+    ref = _summary(ref_state, nzs)
+    if case == "seeded_pool":
+        assert ref["n_liquid"] > 0
+    report = {"fp64_oracle": ref}
+    for storage in ("float32", "float16", "bfloat16"):
+        st, nzs = _c1_run(storage, case)
+        report[storage] = _summary(st, nzs)
+    print("storage-form report (%s):" % case, report)
+    for storage, (t_rel, cells, h_rel) in BOUNDS.items():
+        s = report[storage]
+        assert abs(s["T_peak"] - ref["T_peak"]) <= t_rel * ref["T_peak"], (storage, s, ref)
+        assert abs(s["width_cells"] - ref["width_cells"]) <= cells, (storage, s, ref)
+        assert abs(s["depth_cells"] - ref["depth_cells"]) <= cells, (storage, s, ref)
+        assert abs(s["H_total"] - ref["H_total"]) <= h_rel * abs(ref["H_total"]), (storage, s, ref)

@@ -19,6 +19,7 @@ import ctypes
 import torch
 
 from . import _native, kernels
+from ._native import WaamError
 from .physics import deposition, forces, free_surface, lbm, phase_change, thermal, weld_forces
 from .physics.electrical_stickout import droplet_entry_temperature_K
 
@@ -263,15 +264,17 @@ def step_params(twin):
     p.substrate_growth, p.bead_freeze = int(twin.enable_substrate_growth), int(twin.enable_bead_freeze)
     p.lookback = max(2.0, twin.trailing_solidify_lookback_mm / (g.dx * 1000.0))
     p.T_freeze = m.T_liquidus + twin.trailing_solidify_temp_margin_K
+    p.f_storage = g.population_storage
     return p
 
 
 def _check_fused_supported(twin):
-    if twin.enable_lorentz or twin.enable_recoil or twin.enable_gas_shear:
-        return False
-    if getattr(twin, "use_torch_z", False):
-        return False
-    return True
+    supported = not (twin.enable_lorentz or twin.enable_recoil or twin.enable_gas_shear or
+                     getattr(twin, "use_torch_z", False))
+    if not supported and twin.grid.population_storage:
+        raise WaamError("16-bit population storage runs on the fused step only; this "
+                        "configuration needs the operator path")
+    return supported
 
 
 class _PositionRing:

@@ -10,6 +10,8 @@
 // order of global sums.
 #pragma once
 #include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "waam_expf.h"
@@ -37,6 +39,47 @@ __host__ __device__ constexpr int opp(int q) { return q == 0 ? 0 : (q & 1 ? q + 
 // kernels.py:45-50: Python 1/3, 1/18, 1/36 rounded to float32.
 __host__ __device__ constexpr float wq(int q) {
     return q == 0 ? 0.333333343f : (q < 7 ? 0.0555555560f : 0.0277777780f);
+}
+
+// Population storage.  kStoreF32 keeps f_q; kStoreF16 / kStoreBF16 keep the
+// offset f_q - w_q (rho0 = 1) in 16 bits, rounded to nearest, and every
+// kernel computes in float on w_q + offset.
+enum PopStorage { kStoreF32 = 0, kStoreF16 = 1, kStoreBF16 = 2 };
+
+template <int S>
+struct Pop;
+template <>
+struct Pop<kStoreF32> {
+    typedef float T;
+    __device__ static __forceinline__ float get(T v, int) { return v; }
+    __device__ static __forceinline__ T put(float f, int) { return f; }
+};
+template <>
+struct Pop<kStoreF16> {
+    typedef __half T;
+    __device__ static __forceinline__ float get(T v, int q) { return wq(q) + __half2float(v); }
+    __device__ static __forceinline__ T put(float f, int q) { return __float2half_rn(f - wq(q)); }
+};
+template <>
+struct Pop<kStoreBF16> {
+    typedef __nv_bfloat16 T;
+    __device__ static __forceinline__ float get(T v, int q) {
+        return wq(q) + __bfloat162float(v);
+    }
+    __device__ static __forceinline__ T put(float f, int q) {
+        return __float2bfloat16_rn(f - wq(q));
+    }
+};
+
+// Store one population value at element index idx in any storage (for the
+// sparse writers: deposition, droplet impact).
+__device__ __forceinline__ void pop_store(void* f, size_t idx, int q, float v, int storage) {
+    if (storage == kStoreF16)
+        static_cast<__half*>(f)[idx] = Pop<kStoreF16>::put(v, q);
+    else if (storage == kStoreBF16)
+        static_cast<__nv_bfloat16*>(f)[idx] = Pop<kStoreBF16>::put(v, q);
+    else
+        static_cast<float*>(f)[idx] = v;
 }
 
 // Grids are limited to fewer than 2^31 cells (checked on the host), so a cell

@@ -79,7 +79,7 @@ __host__ __device__ inline DepBox deposit_box(const Dims& d, float arc_i, float 
 }
 
 struct DepFields {
-    float* f_src;
+    void* f_src;      // populations, elements per DepConsts::storage
     int32_t* flags;
     float* f_l;
     float* phi;
@@ -90,6 +90,7 @@ struct DepFields {
 
 struct DepConsts {
     float arc_i, arc_j, arc_k, drop_r, target_vol, T_drop, hdrop, rho0, cell_vol;
+    int storage;   // PopStorage of f_src
 };
 
 // kernels.py:255-275 _has_metal_neighbor: a 6-neighbour in the grid that is
@@ -125,7 +126,7 @@ __device__ __forceinline__ void write_liquid(const DepFields& F, const DepConsts
     F.H[c] = K.hdrop;
     F.rho[c] = K.rho0;
 #pragma unroll
-    for (int q = 0; q < 19; ++q) F.f_src[q * n + c] = wq(q) * K.rho0;
+    for (int q = 0; q < 19; ++q) pop_store(F.f_src, q * n + c, q, wq(q) * K.rho0, K.storage);
 }
 
 // Bits of e reachable from a bit of g by walking up (towards larger k) through
@@ -460,11 +461,13 @@ __global__ void k_deposit_serial(Dims d, DepFields F, DepConsts K, DepositTries 
 
 }  // namespace
 
-int launch_deposit(Dims d, float* f_src, int32_t* flags, float* f_l, float* phi, float* H, float* T,
-                   float* rho, float arc_i, float arc_j, float arc_k, const float* foot_radii,
-                   int n_tries, double accept_volume, float drop_r, float target_vol, float T_drop,
-                   float cp_rho, float L_rho, float rho0, float* vol_acc, float* real_acc,
-                   float cell_vol, void* stream) {
+int launch_deposit(Dims d, void* f_src, int f_storage, int32_t* flags, float* f_l, float* phi,
+                   float* H, float* T, float* rho, float arc_i, float arc_j, float arc_k,
+                   const float* foot_radii, int n_tries, double accept_volume, float drop_r,
+                   float target_vol, float T_drop, float cp_rho, float L_rho, float rho0,
+                   float* vol_acc, float* real_acc, float cell_vol, void* stream) {
+    if (f_storage < kStoreF32 || f_storage > kStoreBF16)
+        return fail(WAAM_ERR_INVALID, "deposit: f_storage must be 0, 1 or 2");
     if (n_tries < 1 || n_tries > WAAM_DEPOSIT_MAX_TRIES || !foot_radii)
         return fail(WAAM_ERR_INVALID, "deposit: footprint radii missing or too many tries");
     // the search box is cast to int: keep every coordinate well inside int range
@@ -491,7 +494,7 @@ int launch_deposit(Dims d, float* f_src, int32_t* flags, float* f_l, float* phi,
     }
     const DepFields F{f_src, flags, f_l, phi, H, T, rho};
     const DepConsts K{arc_i, arc_j, arc_k, drop_r, target_vol, T_drop, cp_rho * T_drop + L_rho,
-                      rho0, cell_vol};
+                      rho0, cell_vol, f_storage};
     const size_t smem = words * kDepWordBytes;
     if (smem <= (size_t)kDepMaxSmem) {
         if (smem > 48 * 1024) {

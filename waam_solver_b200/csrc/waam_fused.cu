@@ -185,14 +185,16 @@ __device__ __forceinline__ int stream_source(const Dims& d, bool interior, int i
     return (ni * d.ny + nj) * d.nz + nk;
 }
 
-// One cell of the pull (non-solid cells only).
-__device__ __forceinline__ void stream_cell(const Dims& d, const float* __restrict__ f_src,
-                                            float* __restrict__ f_dst,
+// One cell of the pull (non-solid cells only).  T is the stored element:
+// streaming moves stored values unchanged, whatever the population storage.
+template <typename T>
+__device__ __forceinline__ void stream_cell(const Dims& d, const T* __restrict__ f_src,
+                                            T* __restrict__ f_dst,
                                             const int32_t* __restrict__ flags, int i, int j, int k,
                                             int c, int flag) {
     const size_t n = (size_t)d.n();
     const bool interior = i > 0 && i < d.nx - 1 && j > 0 && j < d.ny - 1 && k > 0 && k < d.nz - 1;
-    float v[19];
+    T v[19];
 #pragma unroll
     for (int q = 0; q < 19; ++q) v[q] = f_src[q * n + stream_source(d, interior, i, j, k, c, q)];
     if (flag != GAS) {
@@ -205,8 +207,9 @@ __device__ __forceinline__ void stream_cell(const Dims& d, const float* __restri
     for (int q = 0; q < 19; ++q) f_dst[q * n + c] = v[q];
 }
 
-__global__ void __launch_bounds__(256) k_stream(Dims d, const float* __restrict__ f_src,
-                                                float* __restrict__ f_dst,
+template <typename T>
+__global__ void __launch_bounds__(256) k_stream(Dims d, const T* __restrict__ f_src,
+                                                T* __restrict__ f_dst,
                                                 const int32_t* __restrict__ flags) {
     int i, j, k, c;
     if (!tile_cell(d, i, j, k, c)) return;
@@ -216,7 +219,19 @@ __global__ void __launch_bounds__(256) k_stream(Dims d, const float* __restrict_
 }
 
 int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags, void* stream) {
-    k_stream<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(d, f_src, f_dst, flags);
+    k_stream<float><<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(d, f_src, f_dst, flags);
+    return check_launch("k_stream");
+}
+
+// The fused step's stream: 4-byte or 2-byte stored populations.
+static int launch_stream_stored(Dims d, const void* f_src, void* f_dst, const int32_t* flags,
+                                int storage, cudaStream_t s) {
+    if (storage == kStoreF32)
+        k_stream<float><<<tile_grid(d), tile_block(), 0, s>>>(
+            d, static_cast<const float*>(f_src), static_cast<float*>(f_dst), flags);
+    else
+        k_stream<uint16_t><<<tile_grid(d), tile_block(), 0, s>>>(
+            d, static_cast<const uint16_t*>(f_src), static_cast<uint16_t*>(f_dst), flags);
     return check_launch("k_stream");
 }
 
@@ -520,8 +535,10 @@ struct CollideArgs {
 // listed by k_column, shard after shard (solvers/coupled_step.py:298-402).  Forces stay in
 // registers and are written once as the step's force field (== the
 // reference's F_snap); every other cell keeps F == 0.
+template <int S>
 __global__ void __launch_bounds__(kListThreads) k_collide_list(
-    Dims d, const float* __restrict__ f_src, float* __restrict__ f_dst, float* __restrict__ rho,
+    Dims d, const typename Pop<S>::T* __restrict__ f_src, typename Pop<S>::T* __restrict__ f_dst,
+    float* __restrict__ rho,
     float* __restrict__ ux, float* __restrict__ uy, float* __restrict__ uz,
     float* __restrict__ Fx, float* __restrict__ Fy, float* __restrict__ Fz,
     const float* __restrict__ phi, const float* __restrict__ T, const float* __restrict__ f_l,
@@ -565,7 +582,7 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
         // overlaps the force stencil (cache-resident phi, T, flags)
         float f[19], o[19];
 #pragma unroll
-        for (int q = 0; q < 19; ++q) f[q] = f_src[q * n + c];
+        for (int q = 0; q < 19; ++q) f[q] = Pop<S>::get(f_src[q * n + c], q);
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
         if (a.from_buffer) {
             fx = Fx[c];
@@ -580,7 +597,7 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
         else
             collide_srt_cell(f, fl, fx, fy, fz, a.omega, a.C_darcy, o, rr, u, v, w);
 #pragma unroll
-        for (int q = 0; q < 19; ++q) f_dst[q * n + c] = o[q];
+        for (int q = 0; q < 19; ++q) f_dst[q * n + c] = Pop<S>::put(o[q], q);
         if (a.u_cap > 0.0f) clamp_mach(u, v, w, a.u_cap);
         rho[c] = rr;
         ux[c] = u;
@@ -752,6 +769,8 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
                           size_t workspace_bytes, void* const* events, int n_events,
                           void* stream) {
     if (!fields_ok(f) || !p) return fail(WAAM_ERR_INVALID, "step_main: bad fields or params");
+    if (p->f_storage < kStoreF32 || p->f_storage > kStoreBF16)
+        return fail(WAAM_ERR_INVALID, "step_main: f_storage must be 0 (f32), 1 (f16) or 2 (bf16)");
     if (events && n_events < kMainEvents)
         return fail(WAAM_ERR_INVALID, "step_main: need 7 events");
     for (int q = 0; events && q < kMainEvents; ++q)
@@ -876,15 +895,23 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     cl.omega_b = p->omega_b;
     cl.C_darcy = p->C_darcy;
     cl.u_cap = p->u_cap;
-    k_collide_list<<<kListBlocks, kListThreads, 0, s>>>(
-        d, f->f_src, f->f_dst, f->rho, f->ux, f->uy, f->uz, f->Fx, f->Fy, f->Fz, f->phi,
-        f->T_next, f->f_l, f->flags, f->step_scalars, active_list, active_count, (int)shard_cap,
-        cl);
+#define WAAM_COLLIDE(S)                                                                    \
+    k_collide_list<S><<<kListBlocks, kListThreads, 0, s>>>(                                \
+        d, static_cast<const Pop<S>::T*>(f->f_src), static_cast<Pop<S>::T*>(f->f_dst),           \
+        f->rho, f->ux, f->uy, f->uz, f->Fx, f->Fy, f->Fz, f->phi, f->T_next, f->f_l, f->flags,    \
+        f->step_scalars, active_list, active_count, (int)shard_cap, cl)
+    if (p->f_storage == kStoreF16)
+        WAAM_COLLIDE(kStoreF16);
+    else if (p->f_storage == kStoreBF16)
+        WAAM_COLLIDE(kStoreBF16);
+    else
+        WAAM_COLLIDE(kStoreF32);
+#undef WAAM_COLLIDE
     e = check_launch("k_collide_list");
     if (e) return e;
     mark(4);
 
-    e = launch_stream(d, f->f_dst, f->f_src, f->flags, stream);
+    e = launch_stream_stored(d, f->f_dst, f->f_src, f->flags, p->f_storage, s);
     if (e) return e;
     mark(5);
 

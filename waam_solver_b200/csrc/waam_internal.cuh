@@ -93,10 +93,10 @@ int launch_contact_columns(Dims d, const float* snap, float* phi, const int32_t*
 int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags, void* stream);
 // Droplet deposition with up to WAAM_DEPOSIT_MAX_TRIES footprint radii; attempt
 // t > 0 runs only while the converted volume is below accept_volume.
-int launch_deposit(Dims d, float* f_src, int32_t* flags, float* f_l, float* phi, float* H, float* T,
-                   float* rho, float arc_i, float arc_j, float arc_k, const float* foot_radii,
-                   int n_tries, double accept_volume, float drop_r, float target_vol, float T_drop,
-                   float cp_rho, float L_rho, float rho0, float* vol_acc, float* real_acc,
-                   float cell_vol, void* stream);
+int launch_deposit(Dims d, void* f_src, int f_storage, int32_t* flags, float* f_l, float* phi,
+                   float* H, float* T, float* rho, float arc_i, float arc_j, float arc_k,
+                   const float* foot_radii, int n_tries, double accept_volume, float drop_r,
+                   float target_vol, float T_drop, float cp_rho, float L_rho, float rho0,
+                   float* vol_acc, float* real_acc, float cell_vol, void* stream);
 
 }  // namespace waam

@@ -579,10 +579,11 @@ __global__ void k_surface_height(Dims d, const float* phi, const int32_t* flags,
     }
 }
 
-__global__ void k_momentum_impact(Dims d, float* f_src, const float* rho, float* ux, float* uy,
-                                  float* uz, const int32_t* flags, const float* f_l, float arc_i,
-                                  float arc_j, float arc_k, float drop_r, float vx, float vy,
-                                  float vz, int i0, int i1, int j0, int j1, int k0, int k1) {
+__global__ void k_momentum_impact(Dims d, void* f_src, int storage, const float* rho, float* ux,
+                                  float* uy, float* uz, const int32_t* flags, const float* f_l,
+                                  float arc_i, float arc_j, float arc_k, float drop_r, float vx,
+                                  float vy, float vz, int i0, int i1, int j0, int j1, int k0,
+                                  int k1) {
     int64_t n = d.n();
     int ni = i1 - i0, nj = j1 - j0, nk = k1 - k0;
     int64_t m = (int64_t)ni * nj * nk;
@@ -607,7 +608,8 @@ __global__ void k_momentum_impact(Dims d, float* f_src, const float* rho, float*
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
             float eu = (float)ex(q) * vx + (float)ey(q) * vy + (float)ez(q) * vz;
-            f_src[q * n + c] = wq(q) * rl * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * u2);
+            pop_store(f_src, q * n + c, q,
+                      wq(q) * rl * (1.0f + 3.0f * eu + 4.5f * eu * eu - 1.5f * u2), storage);
         }
     }
 }
@@ -974,32 +976,37 @@ int waam_feed_wire_surface(float* f_src, int32_t* flags, float* f_l, float* phi,
     REQUIRE(dims_ok(nx, ny, nz), "feed_wire_surface: bad dims");
     REQUIRE(f_src && flags && f_l && phi && H && T && rho && vol_acc && real_acc,
             "feed_wire_surface: null field");
-    return waam::launch_deposit(Dims{nx, ny, nz}, f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j,
-                                arc_k, &foot_r, 1, 0.0, drop_r, target_vol, T_drop, cp_rho, L_rho,
-                                rho0, vol_acc, real_acc, cell_vol, stream);
+    return waam::launch_deposit(Dims{nx, ny, nz}, f_src, waam::kStoreF32, flags, f_l, phi, H, T,
+                                rho, arc_i, arc_j, arc_k, &foot_r, 1, 0.0, drop_r, target_vol,
+                                T_drop, cp_rho, L_rho, rho0, vol_acc, real_acc, cell_vol, stream);
 }
 
-int waam_deposit_droplet(float* f_src, int32_t* flags, float* f_l, float* phi, float* H, float* T,
-                         float* rho, int nx, int ny, int nz, float arc_i, float arc_j, float arc_k,
-                         const float* foot_radii, int n_tries, double accept_volume, float drop_r,
-                         float target_vol, float T_drop, float cp_rho, float L_rho, float rho0,
-                         float* vol_acc, float* real_acc, float cell_vol, void* stream) {
+int waam_deposit_droplet(void* f_src, int f_storage, int32_t* flags, float* f_l, float* phi,
+                         float* H, float* T, float* rho, int nx, int ny, int nz, float arc_i,
+                         float arc_j, float arc_k, const float* foot_radii, int n_tries,
+                         double accept_volume, float drop_r, float target_vol, float T_drop,
+                         float cp_rho, float L_rho, float rho0, float* vol_acc, float* real_acc,
+                         float cell_vol, void* stream) {
     REQUIRE(dims_ok(nx, ny, nz), "deposit_droplet: bad dims");
     REQUIRE(f_src && flags && f_l && phi && H && T && rho && vol_acc && real_acc,
             "deposit_droplet: null field");
     REQUIRE(foot_radii && n_tries >= 1 && n_tries <= WAAM_DEPOSIT_MAX_TRIES,
             "deposit_droplet: need 1..WAAM_DEPOSIT_MAX_TRIES footprint radii");
-    return waam::launch_deposit(Dims{nx, ny, nz}, f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j,
-                                arc_k, foot_radii, n_tries, accept_volume, drop_r, target_vol,
-                                T_drop, cp_rho, L_rho, rho0, vol_acc, real_acc, cell_vol, stream);
+    return waam::launch_deposit(Dims{nx, ny, nz}, f_src, f_storage, flags, f_l, phi, H, T, rho,
+                                arc_i, arc_j, arc_k, foot_radii, n_tries, accept_volume, drop_r,
+                                target_vol, T_drop, cp_rho, L_rho, rho0, vol_acc, real_acc,
+                                cell_vol, stream);
 }
 
-int waam_feed_wire_momentum_impact(float* f_src, const float* rho, float* ux, float* uy, float* uz,
-                                   const int32_t* flags, const float* f_l, int nx, int ny, int nz,
-                                   float arc_i, float arc_j, float arc_k, float drop_r, float vx,
-                                   float vy, float vz, void* stream) {
+int waam_feed_wire_momentum_impact_stored(void* f_src, int f_storage, const float* rho, float* ux,
+                                          float* uy, float* uz, const int32_t* flags,
+                                          const float* f_l, int nx, int ny, int nz, float arc_i,
+                                          float arc_j, float arc_k, float drop_r, float vx,
+                                          float vy, float vz, void* stream) {
     REQUIRE(dims_ok(nx, ny, nz), "momentum_impact: bad dims");
     REQUIRE(f_src && rho && ux && uy && uz && flags && f_l, "momentum_impact: null field");
+    REQUIRE(f_storage >= waam::kStoreF32 && f_storage <= waam::kStoreBF16,
+            "momentum_impact: f_storage must be 0, 1 or 2");
     Dims d{nx, ny, nz};
     int i0 = imax(0, (int)(arc_i - drop_r * 2.5f)), i1 = imin(nx, (int)(arc_i + drop_r * 2.5f) + 1);
     int j0 = imax(0, (int)(arc_j - drop_r * 2.5f)), j1 = imin(ny, (int)(arc_j + drop_r * 2.5f) + 1);
@@ -1007,9 +1014,18 @@ int waam_feed_wire_momentum_impact(float* f_src, const float* rho, float* ux, fl
     if (i1 <= i0 || j1 <= j0 || k1 <= k0) return WAAM_OK;
     int64_t m = (int64_t)(i1 - i0) * (j1 - j0) * (k1 - k0);
     k_momentum_impact<<<waam::elem_blocks(m), kThreads, 0, STREAM(stream)>>>(
-        d, f_src, rho, ux, uy, uz, flags, f_l, arc_i, arc_j, arc_k, drop_r, vx, vy, vz, i0, i1, j0,
-        j1, k0, k1);
+        d, f_src, f_storage, rho, ux, uy, uz, flags, f_l, arc_i, arc_j, arc_k, drop_r, vx, vy, vz,
+        i0, i1, j0, j1, k0, k1);
     return waam::check_launch("k_momentum_impact");
+}
+
+int waam_feed_wire_momentum_impact(float* f_src, const float* rho, float* ux, float* uy, float* uz,
+                                   const int32_t* flags, const float* f_l, int nx, int ny, int nz,
+                                   float arc_i, float arc_j, float arc_k, float drop_r, float vx,
+                                   float vy, float vz, void* stream) {
+    return waam_feed_wire_momentum_impact_stored(f_src, waam::kStoreF32, rho, ux, uy, uz, flags,
+                                                 f_l, nx, ny, nz, arc_i, arc_j, arc_k, drop_r, vx,
+                                                 vy, vz, stream);
 }
 
 int waam_apply_droplet_impact_pressure(float* Fz, const int32_t* flags, const float* phi,

@@ -15,6 +15,10 @@ Differences that matter to a caller:
 * ``Fx_snap``/``Fy_snap``/``Fz_snap`` alias ``Fx``/``Fy``/``Fz`` unless the grid is
   created with ``separate_force_snapshot=True``: at every step boundary the
   reference's snapshot equals the force field (kernels.py:3338-3350).
+* ``population_dtype=torch.float16`` or ``torch.bfloat16`` stores ``f_a`` /
+  ``f_b`` as 16-bit offsets f_q - w_q from the rest weights (rho0 = 1); the
+  kernels compute in float32.  ``populations(t)`` returns float32 f_q of
+  either buffer, ``state_dict`` / ``load_state`` convert.
 """
 from __future__ import annotations
 
@@ -46,7 +50,7 @@ class WAAMGrid:
 
     def __init__(self, nx, ny, nz, dx, mat, max_tracers=50_000, allocate_lorentz=False,
                  allocate_vof=False, allocate_export=False, device=None,
-                 separate_force_snapshot=False, verbose=False):
+                 separate_force_snapshot=False, verbose=False, population_dtype=torch.float32):
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.dx = float(dx)
         self.mat = mat
@@ -76,8 +80,14 @@ class WAAMGrid:
         def vol():
             return torch.zeros(shape3, **f32)
 
-        self.f_a = torch.zeros((Q,) + shape3, **f32)
-        self.f_b = torch.zeros((Q,) + shape3, **f32)
+        pop_dtype = {"float32": torch.float32, "float16": torch.float16,
+                     "bfloat16": torch.bfloat16}.get(population_dtype, population_dtype)
+        if pop_dtype not in (torch.float32, torch.float16, torch.bfloat16):
+            raise ValueError("population_dtype must be float32, float16 or bfloat16")
+        self.population_dtype = pop_dtype
+        self.population_storage = {torch.float32: 0, torch.float16: 1, torch.bfloat16: 2}[pop_dtype]
+        self.f_a = torch.zeros((Q,) + shape3, dtype=pop_dtype, device=dev)
+        self.f_b = torch.zeros((Q,) + shape3, dtype=pop_dtype, device=dev)
         self.rho = vol()
         self._T = [vol(), vol()]
         self._H = [vol(), vol()]
@@ -202,6 +212,27 @@ class WAAMGrid:
     def f_dst(self):
         return self._write_buf
 
+    # -- population storage -------------------------------------------------
+    def _rest_weights(self):
+        w = getattr(self, "_w_col", None)
+        if w is None:
+            w = self._w_col = self.w.view(Q, 1, 1, 1)
+        return w
+
+    def populations(self, t):
+        """float32 f_q of population buffer ``t`` (f_a, f_b, f_src or f_dst)."""
+        if t.dtype == torch.float32:
+            return t
+        return t.float() + self._rest_weights()
+
+    def store_populations(self, dst, f):
+        """Write float32 f_q into population buffer ``dst`` in its storage."""
+        f = torch.as_tensor(f, device=self.device).to(torch.float32).reshape(dst.shape)
+        if dst.dtype == torch.float32:
+            dst.copy_(f)
+        else:
+            dst.copy_((f - self._rest_weights()).to(dst.dtype))
+
     @property
     def n_cells(self):
         return self.nx * self.ny * self.nz
@@ -220,7 +251,12 @@ class WAAMGrid:
         names = ["rho", "T", "H", "T_max", "f_l", "phi", "dT_dt", "T_prev", "time_above_800_s",
                  "time_above_1100_s", "time_above_solidus_s", "ux", "uy", "uz", "Fx", "Fy",
                  "Fz", "flags", "f_a", "f_b"]
-        out = {k: getattr(self, k).detach().cpu().numpy() for k in names}
+        out = {}
+        for k in names:
+            t = getattr(self, k)
+            if k in ("f_a", "f_b"):
+                t = self.populations(t)
+            out[k] = t.detach().cpu().numpy()
         out["read_is_a"] = self._read_buf is self.f_a
         return out
 
@@ -237,6 +273,9 @@ class WAAMGrid:
                 continue
             else:
                 dst = getattr(self, k)
+            if k in ("f_a", "f_b"):
+                self.store_populations(dst, v)
+                continue
             dst.copy_(torch.as_tensor(v).to(dst.dtype).reshape(dst.shape))
 
 

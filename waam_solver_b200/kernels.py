@@ -39,6 +39,22 @@ def _f(t, n=None):
     return t.data_ptr()
 
 
+POP_STORAGE = {torch.float32: 0, torch.float16: 1, torch.bfloat16: 2}
+
+
+def _pop(t, n=None):
+    """(pointer, storage code) of a population tensor: float32 f_q, or float16 /
+    bfloat16 offsets f_q - w_q (see WaamStepParams.f_storage)."""
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise WaamError("expected a CUDA tensor, got %r" % type(t))
+    if t.dtype not in POP_STORAGE or not t.is_contiguous():
+        raise WaamError("populations must be a contiguous float32, float16 or bfloat16 CUDA "
+                        "tensor, got %s" % t.dtype)
+    if n is not None and t.numel() != n:
+        raise WaamError("populations have %d elements, expected %d" % (t.numel(), n))
+    return t.data_ptr(), POP_STORAGE[t.dtype]
+
+
 def _i(t, n=None):
     if not isinstance(t, torch.Tensor) or not t.is_cuda:
         raise WaamError("expected a CUDA tensor, got %r" % type(t))
@@ -170,7 +186,8 @@ def deposit_droplet(f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j, arc_k, foot
     _flags_ok(FLAG_GAS=FLAG_GAS, FLAG_FLUID=FLAG_FLUID, FLAG_SOLID=FLAG_SOLID)
     n = int(nx) * int(ny) * int(nz)
     radii = (ctypes.c_float * len(footprint_radii))(*[float(r) for r in footprint_radii])
-    _call("waam_deposit_droplet", _f(f_src, 19 * n), _i(flags, n), _f(f_l, n), _f(phi, n),
+    fp, storage = _pop(f_src, 19 * n)
+    _call("waam_deposit_droplet", fp, storage, _i(flags, n), _f(f_l, n), _f(phi, n),
           _f(H, n), _f(T, n), _f(rho, n), int(nx), int(ny), int(nz), float(arc_i), float(arc_j),
           float(arc_k), ctypes.cast(radii, ctypes.c_void_p), len(footprint_radii),
           float(accept_volume), float(droplet_radius), float(target_vol), float(T_drop),
@@ -182,7 +199,8 @@ def feed_wire_momentum_impact(f_src, rho, ux, uy, uz, flags, f_l, arc_i, arc_j, 
                               droplet_radius, vx_lu, vy_lu, vz_lu, FLAG_GAS, nx, ny, nz):
     _flags_ok(FLAG_GAS=FLAG_GAS)
     n = int(nx) * int(ny) * int(nz)
-    _call("waam_feed_wire_momentum_impact", _f(f_src, 19 * n), _f(rho, n), _f(ux, n), _f(uy, n),
+    fp, storage = _pop(f_src, 19 * n)
+    _call("waam_feed_wire_momentum_impact_stored", fp, storage, _f(rho, n), _f(ux, n), _f(uy, n),
           _f(uz, n), _i(flags, n), _f(f_l, n), int(nx), int(ny), int(nz), float(arc_i),
           float(arc_j), float(arc_k), float(droplet_radius), float(vx_lu), float(vy_lu),
           float(vz_lu), _stream())

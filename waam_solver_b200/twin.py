@@ -44,7 +44,7 @@ class WAAMTwin:
                  R_spec_vapor_J_kgK=450.0, travel_speed_m_s=0.0, use_variable_tau=True,
                  enable_enthalpy_cap=True, T_vapor_cap_K=3200.0, arc_surface_weighting=True,
                  arc_penetration_mm=2.0, wire_diameter_mm=1.2, arc_sigma_mm=2.0, bulk_tau=None,
-                 step_mode="fused", device=None):
+                 step_mode="fused", population_dtype="float32", device=None):
         if arc_power_W < 0:
             raise ValueError("arc_power_W must be >= 0, got %s" % arc_power_W)
         if not 0.0 < arc_efficiency <= 1.0:
@@ -87,7 +87,11 @@ class WAAMTwin:
         self.enable_lorentz = enable_lorentz
         self.enable_gas_shear = enable_gas_shear
         self.grid = WAAMGrid(nx, ny, nz, dx, self.mat, max_tracers=max_tracers or 50_000,
-                             allocate_lorentz=enable_lorentz, allocate_vof=True, device=device)
+                             allocate_lorentz=enable_lorentz, allocate_vof=True, device=device,
+                             population_dtype=population_dtype)
+        if self.grid.population_storage and (step_mode != "fused" or enable_lorentz):
+            raise NotImplementedError("16-bit population storage runs on the fused step only "
+                                      "(step_mode='fused', no Lorentz force)")
         self.enable_droplet_impact_pressure = enable_droplet_impact_pressure
         self.use_recoil_clausius_clapeyron = use_recoil_clausius_clapeyron
         self.enable_substrate_growth = enable_substrate_growth
@@ -240,14 +244,22 @@ class WAAMTwin:
             self.nz_solid = self.resolve_nz_solid(False)
             nz_solid = self.nz_solid
             i0, i1, j0, j1 = self.resolve_plate_ij()
-        kernels.init_grid(g.f_a, g.rho, g.ux, g.uy, g.uz, g.T, g.H, g.f_l, g.phi, g.flags, T0,
+        f_a, f_b = g.f_a, g.f_b
+        if g.population_storage:   # initialise and stream in float32, then store offsets
+            f_a, f_b = torch.empty(f_a.shape, device=g.device), torch.empty(f_b.shape,
+                                                                              device=g.device)
+        kernels.init_grid(f_a, g.rho, g.ux, g.uy, g.uz, g.T, g.H, g.f_l, g.phi, g.flags, T0,
                           RHO_LATTICE, self.cp_rho, nz_solid, i0, i1, j0, j1, g.FLAG_FLUID,
                           g.FLAG_SOLID, g.FLAG_GAS)
         kernels.init_aux_fields(g.T_max, g.T_prev, g.dT_dt, g.time_above_800_s,
                                 g.time_above_1100_s, g.time_above_solidus_s, g.Fx_snap, g.Fy_snap,
                                 g.Fz_snap, g.Fx, g.Fy, g.Fz, T0, g.porosity_active,
                                 g.tracer_head, g.max_tracers)
-        kernels.stream(g.f_a, g.f_b, g.flags, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+        kernels.stream(f_a, f_b, g.flags, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+        if g.population_storage:
+            g.store_populations(g.f_a, f_a)
+            g.store_populations(g.f_b, f_b)
+            del f_a, f_b
         self._step_n = 0
         self._last_droplet_time = 0.0
         self._deposited_volume_m3 = 0.0
