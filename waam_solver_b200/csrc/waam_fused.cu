@@ -173,8 +173,31 @@ int launch_contact_columns(Dims d, const float* snap, float* phi, const int32_t*
 // source loads back to back (independent addresses, so all are in flight at
 // once), then, for the few non-gas cells, replaces the populations whose
 // source is SOLID by the cell's own opposite population, then stores.
-// Interior cells (no wrap or clamp on any axis) use fixed neighbour offsets.
+// The per-population base pointers come precomputed in the launch
+// parameters -- for interior cells (no wrap or clamp on any axis) already
+// shifted by the pull offset -- so an address costs one multiply-add.
 // ---------------------------------------------------------------------------
+template <typename T>
+struct StreamPtrs {
+    const T* src[19];    // population q shifted by the interior pull offset
+    const T* base[19];   // population q of the input
+    T* dst[19];          // population q of the output
+};
+
+template <typename T>
+static StreamPtrs<T> stream_ptrs(const Dims& d, const void* f_src, void* f_dst) {
+    StreamPtrs<T> P;
+    const int64_t n = d.n(), sx = (int64_t)d.ny * d.nz, sy = d.nz;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(f_src), b = reinterpret_cast<uintptr_t>(f_dst);
+    for (int q = 0; q < 19; ++q) {
+        const int64_t off = ex(q) * sx + ey(q) * sy + ez(q);   // < n for every q >= 1, 0 for q = 0
+        P.src[q] = reinterpret_cast<const T*>(a + (uintptr_t)((q * n - off) * (int64_t)sizeof(T)));
+        P.base[q] = reinterpret_cast<const T*>(a + (uintptr_t)(q * n * (int64_t)sizeof(T)));
+        P.dst[q] = reinterpret_cast<T*>(b + (uintptr_t)(q * n * (int64_t)sizeof(T)));
+    }
+    return P;
+}
+
 __device__ __forceinline__ int stream_source(const Dims& d, bool interior, int i, int j, int k,
                                              int c, int q) {
     if (interior) return c - (ex(q) * d.ny * d.nz + ey(q) * d.nz + ez(q));
@@ -185,41 +208,41 @@ __device__ __forceinline__ int stream_source(const Dims& d, bool interior, int i
     return (ni * d.ny + nj) * d.nz + nk;
 }
 
-// One cell of the pull (non-solid cells only).  T is the stored element:
-// streaming moves stored values unchanged, whatever the population storage.
+// T is the stored element: streaming moves stored values unchanged, whatever
+// the population storage.
 template <typename T>
-__device__ __forceinline__ void stream_cell(const Dims& d, const T* __restrict__ f_src,
-                                            T* __restrict__ f_dst,
-                                            const int32_t* __restrict__ flags, int i, int j, int k,
-                                            int c, int flag) {
-    const size_t n = (size_t)d.n();
-    const bool interior = i > 0 && i < d.nx - 1 && j > 0 && j < d.ny - 1 && k > 0 && k < d.nz - 1;
-    T v[19];
-#pragma unroll
-    for (int q = 0; q < 19; ++q) v[q] = f_src[q * n + stream_source(d, interior, i, j, k, c, q)];
-    if (flag != GAS) {
-#pragma unroll
-        for (int q = 1; q < 19; ++q)
-            if (flags[stream_source(d, interior, i, j, k, c, q)] == SOLID)
-                v[q] = f_src[opp(q) * n + c];
-    }
-#pragma unroll
-    for (int q = 0; q < 19; ++q) f_dst[q * n + c] = v[q];
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) k_stream(Dims d, const T* __restrict__ f_src,
-                                                T* __restrict__ f_dst,
+__global__ void __launch_bounds__(256) k_stream(Dims d, const __grid_constant__ StreamPtrs<T> P,
                                                 const int32_t* __restrict__ flags) {
     int i, j, k, c;
     if (!tile_cell(d, i, j, k, c)) return;
     const int flag = flags[c];
     if (flag == SOLID) return;
-    stream_cell(d, f_src, f_dst, flags, i, j, k, c, flag);
+    const bool interior = i > 0 && i < d.nx - 1 && j > 0 && j < d.ny - 1 && k > 0 && k < d.nz - 1;
+    T v[19];
+    if (interior) {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) v[q] = P.src[q][c];
+    } else {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) v[q] = P.base[q][stream_source(d, false, i, j, k, c, q)];
+    }
+    if (flag != GAS) {
+#pragma unroll
+        for (int q = 1; q < 19; ++q)
+            if (flags[stream_source(d, interior, i, j, k, c, q)] == SOLID) v[q] = P.base[opp(q)][c];
+    }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) P.dst[q][c] = v[q];
+}
+
+template <typename T>
+static void launch_stream_t(const Dims& d, const void* f_src, void* f_dst, const int32_t* flags,
+                            cudaStream_t s) {
+    k_stream<T><<<tile_grid(d), tile_block(), 0, s>>>(d, stream_ptrs<T>(d, f_src, f_dst), flags);
 }
 
 int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags, void* stream) {
-    k_stream<float><<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(d, f_src, f_dst, flags);
+    launch_stream_t<float>(d, f_src, f_dst, flags, STREAM(stream));
     return check_launch("k_stream");
 }
 
@@ -227,11 +250,9 @@ int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags
 static int launch_stream_stored(Dims d, const void* f_src, void* f_dst, const int32_t* flags,
                                 int storage, cudaStream_t s) {
     if (storage == kStoreF32)
-        k_stream<float><<<tile_grid(d), tile_block(), 0, s>>>(
-            d, static_cast<const float*>(f_src), static_cast<float*>(f_dst), flags);
+        launch_stream_t<float>(d, f_src, f_dst, flags, s);
     else
-        k_stream<uint16_t><<<tile_grid(d), tile_block(), 0, s>>>(
-            d, static_cast<const uint16_t*>(f_src), static_cast<uint16_t*>(f_dst), flags);
+        launch_stream_t<uint16_t>(d, f_src, f_dst, flags, s);
     return check_launch("k_stream");
 }
 
