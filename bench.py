@@ -223,7 +223,7 @@ def barrier():
         dist.barrier()
 
 
-def cpu_baseline(w, budget_s=15.0, max_steps=12):
+def cpu_baseline(w, budget_s=15.0, max_steps=400):
     """The CPU oracle (C restatement, OpenMP on all host cores) on the same
     workload: reset, then as many full steps as fit the time budget."""
     from oracle.oracle_step import OracleTwin
@@ -446,7 +446,7 @@ def run_b200(args, w):
                         "(eager launches); value/e2e steps replay CUDA graphs" % Ks,
         "clocks": clocks.summary(),
     }
-    if world == 1:
+    if world == 1 and not args.no_precision_forms:
         line["precision_forms"] = storage_forms(w, device, min(K, 1000), ms / K)
         line["precision_forms"]["storage"] = ("headline value: float32 populations; forms: "
                                               "16-bit offsets f_q - w_q, float32 arithmetic")
@@ -466,6 +466,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="standard", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-precision-forms", action="store_true",
+                    help="skip the float16 / bfloat16 population-storage timings")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spinup", type=int, default=None,
                     help="steps run before warm-up (default: the workload's spin-up)")
