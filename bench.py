@@ -12,7 +12,7 @@ bead) before timing.  One step = one ``WAAMTwin.step``.
 
 ``python bench.py [--gpus N] [--steps K] [--warmup W]`` prints one JSON line.
 Under torchrun every rank runs an independent replica (the step has no
-cross-GPU exchange; see DESIGN.md), timing is the max over ranks.
+cross-GPU exchange), timing is the max over ranks.
 ``--impl reference`` times the CPU restatement of the reference step (the
 oracle, all host cores) on the same workload.
 """

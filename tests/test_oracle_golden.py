@@ -2,7 +2,7 @@
 
 The fixtures in tests/golden/ were produced by the reference's unmodified
 Taichi kernels executed serially (tests/golden/make_golden.py); this pins the
-oracle before it is used to judge the CUDA path.
+oracle before it is used to check the CUDA path.
 """
 import pytest
 
