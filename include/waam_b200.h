@@ -266,6 +266,21 @@ int waam_apply_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* Jx, con
                            const float* f_l, const int32_t* flags, int64_t n, float dt, float dx,
                            float rho_ref, void* stream);
 
+/* ---- porosity tracers (kernels.py:3182-3255) ---------------------------- */
+
+/* kernels.py:3182-3205 inject_tracers: spawn_count particles into consecutive
+ * ring-buffer slots from *head (then *head += spawn_count), at random offsets
+ * within +-sigma_m of (arc_x, arc_y), z = arc_z.  pos is (max_tracers, 3).
+ * The offsets come from a counter-based hash of (seed, spawn index): the
+ * reference's ti.random() stream is not reproducible, so a seed is added. */
+int waam_inject_tracers(float* pos, int32_t* active, int32_t* head, int max_tracers, float arc_x,
+                        float arc_y, float arc_z, float sigma_m, int spawn_count, uint64_t seed,
+                        void* stream);
+/* kernels.py:3207-3255 advect_tracers (nearest-cell velocity, pos += u*dx) */
+int waam_advect_tracers(float* pos, int32_t* active, const float* ux, const float* uy,
+                        const float* uz, const float* f_l, const int32_t* flags, int nx, int ny,
+                        int nz, float dx, int max_tracers, void* stream);
+
 /* ---- fused step: the B200 pipeline of solvers/coupled_step.py:73-464 ----- */
 
 typedef struct WaamFields {
@@ -297,6 +312,11 @@ typedef struct WaamFields {
                             [4], [5] torch position (arc_i, arc_j) in cells -- written by
                             the caller before waam_step_pre (a 2-float H2D copy per step) */
     int nx, ny, nz;
+    /* porosity tracers advected after the stream (kernels.py:3207-3255); a
+     * null pos or max_tracers == 0 skips them */
+    float* tracer_pos;        /* (max_tracers, 3) */
+    int32_t* tracer_active;   /* (max_tracers) */
+    int max_tracers;
 } WaamFields;
 
 typedef struct WaamStepParams {

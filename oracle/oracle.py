@@ -69,6 +69,8 @@ _SIGS = {
     "wo_elec_bins": ([_F, _F, _i, _i, _i, _f, _f, _f, _f, _i], None),
     "wo_elec_B_axisymmetric": ([_F, _F, _F, _F, _i, _i, _i, _f, _f, _f, _f, _f, _i], None),
     "wo_apply_lorentz_JxB": ([_F] * 10 + [_I, _l, _f, _f, _f], None),
+    "wo_inject_tracers": ([_F, _I, _I, _i, _f, _f, _f, _f, _i, C.c_uint64], None),
+    "wo_advect_tracers": ([_F, _I, _F, _F, _F, _F, _I, _i, _i, _i, _f, _i], None),
     "wo_num_threads": ([], C.c_int),
     "wo_expf_array": ([_F, _F, _l], None),
     "wo_set_num_threads": ([C.c_int], None),

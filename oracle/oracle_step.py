@@ -49,7 +49,7 @@ class OracleTwin:
             impact_lead_angle_deg=0.0, trailing_solidify_lookback_mm=2.5,
             trailing_solidify_temp_margin_K=35.0, enable_lorentz=False, sigma_liquid_Sm=1.0e6,
             sigma_solid_Sm=1.0e5, lorentz_jacobi_iters=40, lorentz_jacobi_omega=0.85,
-            lorentz_jacobi_tol=1e-4)
+            lorentz_jacobi_tol=1e-4, max_tracers=64)
         unknown = set(kw) - set(self.cfg)
         if unknown:
             raise KeyError("unknown OracleTwin options: %s" % sorted(unknown))
@@ -110,6 +110,7 @@ class OracleTwin:
         self.O.call("wo_stream", s["f_a"], s["f_b"], s["flags"], nx, ny, nz)
         s["read_is_a"] = True
         self.s = s
+        self._tracer_fields()
         self.lorentz_warm = False
         self.step_n = 0
         self.last_drop = 0.0
@@ -124,6 +125,13 @@ class OracleTwin:
         self.s = {k: (own(v) if isinstance(v, np.ndarray) else v) for k, v in st.items()}
         self.s.setdefault("phi_tmp", np.zeros_like(self.s["phi"]))
         self.s.setdefault("read_is_a", True)
+        self._tracer_fields()
+
+    def _tracer_fields(self):
+        m = int(self.cfg["max_tracers"])
+        self.s.setdefault("porosity_pos", np.zeros((m, 3), self.ft))
+        self.s.setdefault("porosity_active", np.zeros(m, np.int32))
+        self.s.setdefault("tracer_head", np.zeros(1, np.int32))
 
     def fsrc(self):
         return self.s["f_a"] if self.s["read_is_a"] else self.s["f_b"]
@@ -191,6 +199,7 @@ class OracleTwin:
             if nrm > 1e-12:
                 self.dir = tuple(v / nrm for v in d)
         self.last_pos = (x, y, 0.0)
+        self._pos = (x, y)
         arc_i, arc_j = x / self.dx, y / self.dx
         i0 = max(0, min(int(arc_i), nx - 1))
         j0 = max(0, min(int(arc_j), ny - 1))
@@ -277,6 +286,8 @@ class OracleTwin:
                    self.omega_bulk, c["C_darcy"])
         self.O.call("wo_clamp_velocity_mach", s["ux"], s["uy"], s["uz"], s["flags"], n, 0.08)
         self.O.call("wo_stream", self.fdst(), self.fsrc(), s["flags"], nx, ny, nz)
+        self.O.call("wo_advect_tracers", s["porosity_pos"], s["porosity_active"], s["ux"], s["uy"],
+                    s["uz"], s["f_l"], s["flags"], nx, ny, nz, self.dx, int(c["max_tracers"]))
         self.O.call("wo_update_time_above_T", s["T"], s["flags"], s["time_above_800_s"],
                s["time_above_1100_s"], s["time_above_solidus_s"], n, self.dt, 800.0 + 273.15,
                1100.0 + 273.15, Ts)
@@ -362,6 +373,11 @@ class OracleTwin:
             r = max(1.0, min((3.0 * cells / (4.0 * math.pi)) ** (1.0 / 3.0), 10.0))
         vol = mass / m["rho"]
         T_drop = m["T_liquidus"] + c["deposition_superheat_K"]
+        # solvers/coupled_step.py:120-125 (seeded by the step number, as the library does)
+        self.O.call("wo_inject_tracers", s["porosity_pos"], s["porosity_active"],
+                    s["tracer_head"], int(c["max_tracers"]), self._pos[0], self._pos[1],
+                    float(arc_k + 1) * self.dx, float(self.sigma_cells * self.dx), 50,
+                    int(self.step_n))
         r_try = max(r, self.sigma_cells * c["deposition_footprint_sigma_scale"])
         placed = 0.0
         nx, ny, nz = self.nx, self.ny, self.nz

@@ -1338,3 +1338,49 @@ void wo_apply_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* Jx, cons
         Fz[c] += fzp * scale;
     }
 }
+
+/* ---------------- tracers (kernels.py:3182-3255) ---------------- */
+
+static uint64_t wo_mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static float wo_uniform01(uint64_t seed, uint64_t index, int component) {
+    uint64_t h = wo_mix64(seed ^ wo_mix64(index * 2ull + (uint64_t)component));
+    return (float)(uint32_t)(h >> 40) * (1.0f / 16777216.0f);
+}
+
+void wo_inject_tracers(float* pos, int32_t* active, int32_t* head, int max_tracers, float arc_x,
+                       float arc_y, float arc_z, float sigma_m, int spawn_count, uint64_t seed) {
+    int base = *head;
+    for (int t = 0; t < spawn_count; ++t) {
+        uint64_t index = (uint64_t)(uint32_t)base + (uint64_t)t;
+        int slot = (int)(index % (uint64_t)max_tracers);
+        active[slot] = 1;
+        float rdx = (wo_uniform01(seed, index, 0) * 2.0f - 1.0f) * sigma_m;
+        float rdy = (wo_uniform01(seed, index, 1) * 2.0f - 1.0f) * sigma_m;
+        pos[3 * slot + 0] = arc_x + rdx;
+        pos[3 * slot + 1] = arc_y + rdy;
+        pos[3 * slot + 2] = arc_z;
+    }
+    *head = base + spawn_count;
+}
+
+void wo_advect_tracers(float* pos, int32_t* active, const float* ux, const float* uy,
+                       const float* uz, const float* f_l, const int32_t* flags, int nx, int ny,
+                       int nz, float dx, int max_tracers) {
+    for (int p = 0; p < max_tracers; ++p) {
+        if (active[p] != 1) continue;
+        int i = (int)(pos[3 * p] / dx), j = (int)(pos[3 * p + 1] / dx), k = (int)(pos[3 * p + 2] / dx);
+        if (i < 0 || i >= nx || j < 0 || j >= ny || k < 0 || k >= nz) { active[p] = 0; continue; }
+        int64_t c = IX(i, j, k);
+        if (flags[c] == GAS) { active[p] = 0; continue; }
+        if (f_l[c] < 0.05f || flags[c] == SOLID) { active[p] = 2; continue; }
+        pos[3 * p] = pos[3 * p] + ux[c] * dx;
+        pos[3 * p + 1] = pos[3 * p + 1] + uy[c] * dx;
+        pos[3 * p + 2] = pos[3 * p + 2] + uz[c] * dx;
+    }
+}

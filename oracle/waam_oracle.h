@@ -138,6 +138,15 @@ void wo_apply_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* Jx, cons
                           const float* f_l, const int32_t* flags, int64_t n, float dt, float dx,
                           float rho_ref);
 
+/* kernels.py:3182-3205 inject_tracers with the library's counter-based hash
+ * (the reference's ti.random() is not reproducible) */
+void wo_inject_tracers(float* pos, int32_t* active, int32_t* head, int max_tracers, float arc_x,
+                       float arc_y, float arc_z, float sigma_m, int spawn_count, uint64_t seed);
+/* kernels.py:3207-3255 advect_tracers */
+void wo_advect_tracers(float* pos, int32_t* active, const float* ux, const float* uy,
+                       const float* uz, const float* f_l, const int32_t* flags, int nx, int ny,
+                       int nz, float dx, int max_tracers);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,8 +46,9 @@ def full_inputs(name):
     seed_map = {"inject_goldak": 1, "thermal_s2": 2, "vof_wet": 3, "contact": 4,
                 "contact_s5": 5, "forces_wet": 6, "csf": 7, "csf_wet": 8, "collide_srt": 9,
                 "tail": 10, "heat_loss": 11, "surface_height": 12, "deposit": 13,
-                "lorentz": 14}
-    nx, ny, nz = ins[next(iter(ins))].shape[-3:]
+                "lorentz": 14, "tracers": 15}
+    grids = [v.shape[-3:] for v in ins.values() if v.ndim >= 3 and v.shape[-1] != 3]
+    nx, ny, nz = grids[0] if grids else (13, 11, 12)   # tracer-only cases: the kernel-case grid
     st = state_gen.seeded_state(nx, ny, nz, seed=seed_map.get(name, 0))
     st = {k: (np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v) for k, v in st.items()}
     st["phi_tmp"] = np.zeros_like(st["phi"])
@@ -220,6 +221,9 @@ def run_case(be, name, st, a):
                              st["Bx"], st["By"], st["Bz"], st["f_l"], st["flags"], n, a["dt"],
                              a["dx"], a["rho_ref"])
         return l1
+    elif name == "tracers":
+        be.advect_tracers(st["porosity_pos"], st["porosity_active"], st["ux"], st["uy"], st["uz"],
+                          st["f_l"], st["flags"], nx, ny, nz, a["dx"], a["max_tracers"])
     elif name == "reset":
         ny_ = ny
         be.init_grid(st["f_a"], st["rho"], st["ux"], st["uy"], st["uz"], st["T"], st["H"],
@@ -238,7 +242,7 @@ def run_case(be, name, st, a):
 CASES = ["inject_gauss", "inject_goldak", "ceiling", "thermal", "thermal_s2", "phase",
          "tmax_cool", "vof", "vof_wet", "contact", "contact_s5", "forces", "forces_wet", "csf",
          "csf_wet", "collide_mrt", "collide_srt", "stream", "tail", "heat_loss",
-         "surface_height", "deposit", "lorentz", "reset"]
+         "surface_height", "deposit", "lorentz", "tracers", "reset"]
 
 
 def check_case(be, name):

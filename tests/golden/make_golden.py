@@ -376,6 +376,26 @@ def c_lorentz(tw, g):
     return a
 
 
+def tracer_setup(tw, g):
+    rng = np.random.default_rng(41)
+    m = g.max_tracers
+    ext = np.array([g.nx, g.ny, g.nz], np.float64) * g.dx
+    pos = rng.uniform(-0.05, 1.05, (m, 3)) * ext          # some outside the grid
+    hot = np.array([0.45 * g.nx, 0.5 * g.ny, tw.nz_solid + 1.0]) * g.dx
+    pos[: m // 2] = hot + rng.uniform(-3.0, 3.0, (m // 2, 3)) * g.dx   # near the melt
+    act = rng.choice([0, 1, 1, 1, 2], size=m).astype(np.int32)
+    g.porosity_pos.from_numpy(pos.astype(np.float32))
+    g.porosity_active.from_numpy(act)
+
+
+def c_tracers(tw, g):
+    a = scal(tw)
+    a["max_tracers"] = int(g.max_tracers)
+    K.advect_tracers(g.porosity_pos, g.porosity_active, g.ux, g.uy, g.uz, g.f_l, g.flags, g.dx,
+                     g.dt, g.max_tracers, g.FLAG_SOLID, g.FLAG_GAS)
+    return a
+
+
 def c_reset(tw, g):
     a = scal(tw)
     tw.reset()
@@ -410,6 +430,8 @@ def kernel_cases():
     kernel_case("surface_height", c_surface_height, ["phi"], seed=12)
     kernel_case("deposit", c_deposit, base + ["rho", "f_a", "ux", "uy", "uz", "Fz"], seed=13)
     kernel_case("lorentz", c_lorentz, LORENTZ_FIELDS, seed=14, extra_in=lorentz_setup)
+    kernel_case("tracers", c_tracers, ["porosity_pos", "porosity_active"], seed=15,
+                extra_in=tracer_setup)
     kernel_case("reset", c_reset, base + ["rho", "ux", "uy", "uz", "f_a", "f_b", "T_max",
                                           "T_prev", "dT_dt", "time_above_800_s", "Fx", "Fx_snap"])
 

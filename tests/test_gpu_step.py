@@ -100,6 +100,12 @@ def test_fused_matches_oracle_from_reset(kind, shape, n_steps):
     if kind == "c2":
         assert tw._n_droplets_fired == ot.n_drops >= 1
         assert abs(tw._deposited_volume_m3 - ot.deposited) <= 1e-6 * max(ot.deposited, 1e-30)
+        # porosity tracers spawned by the droplets and advected every step
+        g = tw.grid
+        assert int(g.tracer_head.item()) == int(ot.s["tracer_head"][0]) >= 50
+        assert np.array_equal(g.porosity_active.cpu().numpy(), ot.s["porosity_active"])
+        steps.compare("tracers", g.porosity_pos.cpu().numpy(), ot.s["porosity_pos"],
+                      "porosity_pos")
 
 
 def test_fused_is_deterministic():

@@ -26,7 +26,9 @@ class WaamFields(C.Structure):
     _fields_ = [(name, C.c_void_p) for name in (
         "f_src", "f_dst", "rho", "ux", "uy", "uz", "T", "T_next", "H", "H_next", "f_l", "phi",
         "phi_tmp", "flags", "T_max", "T_prev", "dT_dt", "t800", "t1100", "tsol", "Fx", "Fy",
-        "Fz", "step_scalars")] + [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int)]
+        "Fz", "step_scalars")] + [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                                  ("tracer_pos", C.c_void_p), ("tracer_active", C.c_void_p),
+                                  ("max_tracers", C.c_int)]
 
 
 def _params_fields():
@@ -53,7 +55,7 @@ class WaamStepParams(C.Structure):
 _CTYPES = {
     "float*": C.c_void_p, "const float*": C.c_void_p, "int32_t*": C.c_void_p,
     "const int32_t*": C.c_void_p, "void*": C.c_void_p, "float": C.c_float, "int": C.c_int,
-    "int64_t": C.c_int64, "size_t": C.c_size_t, "double": C.c_double, "const WaamFields*": C.POINTER(WaamFields),
+    "int64_t": C.c_int64, "size_t": C.c_size_t, "double": C.c_double, "uint64_t": C.c_uint64, "const WaamFields*": C.POINTER(WaamFields),
     "const WaamStepParams*": C.POINTER(WaamStepParams), "const char*": C.c_char_p,
     "void* const*": C.c_void_p,
 }

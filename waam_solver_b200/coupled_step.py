@@ -83,6 +83,7 @@ def _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m, device_retries=
     drop_r = deposition.droplet_radius_cells_from_mass_kg(twin, drop_mass)
     drop_vol = drop_mass / twin.mat.rho
     T_drop = droplet_entry_temperature_K(twin)
+    _spawn_tracers(twin, g, torch_x_m, torch_y_m, arc_k)
     r_try = deposition.deposition_footprint_cells(twin, drop_r)
     placed_real = 0.0
     if device_retries:
@@ -190,6 +191,8 @@ def coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=Non
     if u_cap > 0.0:
         kernels.clamp_velocity_mach(g.ux, g.uy, g.uz, g.flags, u_cap, g.FLAG_SOLID, g.FLAG_GAS)
     lbm.stream(g.f_dst, g.f_src, g.flags, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+    kernels.advect_tracers(g.porosity_pos, g.porosity_active, g.ux, g.uy, g.uz, g.f_l, g.flags,
+                           g.dx, g.dt, g.max_tracers, g.FLAG_SOLID, g.FLAG_GAS)
     kernels.update_time_above_T(g.T, g.flags, g.time_above_800_s, g.time_above_1100_s,
                                 g.time_above_solidus_s, g.dt, T_800, T_1100, twin.mat.T_solidus,
                                 g.FLAG_GAS)
@@ -227,7 +230,21 @@ def _fields(g):
                     ("Fx", g.Fx), ("Fy", g.Fy), ("Fz", g.Fz), ("step_scalars", g.step_scalars)):
         setattr(f, name, t.data_ptr())
     f.nx, f.ny, f.nz = g.nx, g.ny, g.nz
+    if getattr(g, "_tracers_live", False):   # advected once the first droplet spawned some
+        f.tracer_pos, f.tracer_active = g.porosity_pos.data_ptr(), g.porosity_active.data_ptr()
+        f.max_tracers = g.max_tracers
     return f
+
+
+def _spawn_tracers(twin, g, torch_x_m, torch_y_m, arc_k):
+    """solvers/coupled_step.py:120-125: 50 porosity tracers per droplet."""
+    kernels.inject_tracers(g.porosity_pos, g.porosity_active, g.tracer_head, g.max_tracers,
+                           torch_x_m, torch_y_m, float(arc_k + 1) * g.dx,
+                           float(twin.sigma_cells * g.dx), 50, seed=twin._step_n)
+    if not getattr(g, "_tracers_live", False):
+        g._tracers_live = True
+        g.__dict__.pop("_fields_cache", None)    # the fused step now advects them
+        twin.__dict__["_graphs"] = {}
 
 
 def step_params(twin):
@@ -402,6 +419,7 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
             arc_k = float(g.step_scalars[0].item())
             forces.clear_forces(g.Fx, g.Fy, g.Fz)
             _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m, device_retries=True)
+            f = _fields_cached(g)     # the first droplet switches tracer advection on
             p.forces_from_buffer = 1
             p.clear_forces = 0
         if events is None:

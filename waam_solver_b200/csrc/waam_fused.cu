@@ -750,7 +750,7 @@ extern "C" {
 int waam_step_launch_count(const WaamStepParams* p, int stage) {
     if (!p) return 0;
     if (stage == 0) return p->welding ? 3 : 1;
-    // thermal, [vof], column, collide, stream
+    // thermal, [vof], column, collide, stream (tracers counted by the caller)
     int n = 1 + (p->vof ? 1 : 0) + 1 + 1 + 1;
     if (p->substrate_growth || p->bead_freeze) n += 1;
     return n;
@@ -934,6 +934,11 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
 
     e = launch_stream_stored(d, f->f_dst, f->f_src, f->flags, p->f_storage, s);
     if (e) return e;
+    if (f->tracer_pos && f->tracer_active && f->max_tracers > 0) {
+        e = launch_advect_tracers(d, f->tracer_pos, f->tracer_active, f->ux, f->uy, f->uz,
+                                  f->f_l, f->flags, p->dx, f->max_tracers, stream);
+        if (e) return e;
+    }
     mark(5);
 
     if (p->substrate_growth || p->bead_freeze) {

@@ -91,6 +91,9 @@ __global__ void k_arc_inject(Dims d, float* __restrict__ H, const int32_t* __res
 int launch_contact_columns(Dims d, const float* snap, float* phi, const int32_t* flags,
                            float theta, void* stream);
 int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags, void* stream);
+int launch_advect_tracers(Dims d, float* pos, int32_t* active, const float* ux, const float* uy,
+                          const float* uz, const float* f_l, const int32_t* flags, float dx,
+                          int max_tracers, void* stream);
 // Droplet deposition with up to WAAM_DEPOSIT_MAX_TRIES footprint radii; attempt
 // t > 0 runs only while the converted volume is below accept_volume.
 int launch_deposit(Dims d, void* f_src, int f_storage, int32_t* flags, float* f_l, float* phi,

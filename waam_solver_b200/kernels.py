@@ -626,3 +626,38 @@ def apply_lorentz_JxB(Fx, Fy, Fz, Jx, Jy, Jz, Bx, By, Bz, f_l, flags, dt, dx, rh
     _call("waam_apply_lorentz_JxB", _f(Fx, n), _f(Fy, n), _f(Fz, n), _f(Jx, n), _f(Jy, n),
           _f(Jz, n), _f(Bx, n), _f(By, n), _f(Bz, n), _f(f_l, n), _i(flags, n), n, float(dt),
           float(dx), float(rho_ref), _stream())
+
+
+# ------------------------------------------------------------- tracers ----
+# kernels.py:3182-3255 (porosity tracers; no feedback into the fields)
+_tracer_calls = [0]
+
+
+def inject_tracers(pos, active, head, max_tracers, arc_x, arc_y, arc_z, sigma_m, spawn_count,
+                   seed=None):
+    """Spawn ``spawn_count`` tracers into the ring buffer (kernels.py:3182-3205).
+
+    ``seed`` selects the random offsets (a counter-based hash; the reference's
+    ti.random() is not reproducible); by default successive calls use 0, 1, 2..."""
+    if seed is None:
+        seed = _tracer_calls[0]
+        _tracer_calls[0] += 1
+    m = int(max_tracers)
+    if pos.shape != (m, 3) or active.numel() != m:
+        raise WaamError("inject_tracers: pos must be (max_tracers, 3), active (max_tracers,)")
+    _call("waam_inject_tracers", _f(pos), _i(active), _i(head, 1), m, float(arc_x),
+          float(arc_y), float(arc_z), float(sigma_m), int(spawn_count),
+          int(seed) & 0xFFFFFFFFFFFFFFFF, _stream())
+
+
+def advect_tracers(pos, active, ux, uy, uz, f_l, flags, dx, dt, max_tracers, FLAG_SOLID,
+                   FLAG_GAS):
+    """kernels.py:3207-3255: nearest-cell velocity, pos += u * dx."""
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(ux)
+    n = ux.numel()
+    m = int(max_tracers)
+    if pos.shape != (m, 3) or active.numel() != m:
+        raise WaamError("advect_tracers: pos must be (max_tracers, 3), active (max_tracers,)")
+    _call("waam_advect_tracers", _f(pos), _i(active), _f(ux, n), _f(uy, n), _f(uz, n),
+          _f(f_l, n), _i(flags, n), nx, ny, nz, float(dx), m, _stream())

@@ -190,6 +190,7 @@ class WAAMTwin:
     def invalidate(self):
         """Drop cached step parameters after changing a twin attribute."""
         self._fused_params = None
+        self.grid.__dict__.pop("_fields_cache", None)
 
     def resolve_nz_solid(self, test_fluid_domain=False):
         """Substrate layers from plate thickness (else nz//5), leaving gas headroom."""
@@ -271,6 +272,7 @@ class WAAMTwin:
         self._lorentz_unconverged_streak = 0
         g.deposit_vol_buf.zero_()
         g.deposit_real_buf.zero_()
+        g._tracers_live = False
         self.invalidate()
 
     def step(self, torch_x_m, torch_y_m, is_welding=True, torch_z_m=None):
