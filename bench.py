@@ -371,17 +371,23 @@ def run_b200(args, w):
     # ---- stage timing: the same step with events between the fused kernels ----
     Ks = min(K, 400)
     ev_sets = [[torch.cuda.Event(enable_timing=True) for _ in range(7)] for _ in range(Ks)]
+    ev_pre = [torch.cuda.Event(enable_timing=True) for _ in range(Ks)]
     for es in ev_sets:
         for e in es:
             e.record()
     torch.cuda.synchronize()
+    pre_steps = []
     for k in range(Ks):
         tw._stage_events = ev_sets[k]
+        due = tw._n_droplets_fired
+        ev_pre[k].record()
         tw.step(*pos[s], True)
+        if tw._n_droplets_fired == due:
+            pre_steps.append(k)     # the pre stage of droplet steps includes the deposition
         s += 1
     torch.cuda.synchronize()
     tw._stage_events = None
-    stage_ms = {}
+    stage_ms = {"pre": statistics.fmean(ev_pre[k].elapsed_time(ev_sets[k][0]) for k in pre_steps)}
     for i, name in enumerate(STAGES):
         stage_ms[name] = statistics.fmean(es[i].elapsed_time(es[i + 1]) for es in ev_sets)
     c = census(tw)

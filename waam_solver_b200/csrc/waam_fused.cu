@@ -25,7 +25,7 @@ namespace waam {
 #define STREAM(s) reinterpret_cast<cudaStream_t>(s)
 constexpr int kMainEvents = 7;
 constexpr int kMaxDevices = 64;
-constexpr int kTileRedBlocks = 592;   // <= kWsMaxPartials
+constexpr int kTileRedBlocks = 592;   // <= kWsMaxPartials; a fixed grid keeps the sum order fixed
 constexpr int kListThreads = 128;
 constexpr int kListBlocks = 148 * 6;
 
@@ -262,23 +262,31 @@ static int launch_stream_stored(Dims d, const void* f_src, void* f_dst, const in
 
 // Surface height at the torch column + the arc-k fallback of
 // solvers/coupled_step.py:34-59 -> scalars[kScalarArcK].
-__global__ void k_surface_arc(Dims d, const float* phi, const int32_t* flags, float* scalars,
-                              int nz_solid) {
+// Top metal cell of the torch column and the arc-k fallback of
+// solvers/coupled_step.py:34-59, computed by one warp (every lane returns it).
+__device__ __forceinline__ float surface_arc_k(const Dims& d, const float* phi,
+                                               const int32_t* flags, const float* scalars,
+                                               int nz_solid) {
+    const int lane = threadIdx.x & 31;
     float arc_i = scalars[kScalarArcI], arc_j = scalars[kScalarArcJ];
     int i0 = imax(0, imin((int)arc_i, d.nx - 1));
     int j0 = imax(0, imin((int)arc_j, d.ny - 1));
     int best = -1;
-    for (int k = threadIdx.x; k < d.nz; k += 32) {
+    for (int k = lane; k < d.nz; k += 32) {
         int c = d.idx(i0, j0, k);
         if (flags[c] != GAS && phi[c] > 0.05f) best = k;
     }
-    for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_down_sync(0xffffffffu, best, o));
-    if (threadIdx.x == 0) {
-        int ks = best >= 0 ? best : imax(1, nz_solid - 1);
-        float kf = (float)ks;
-        if (kf < 1.0f) kf = (float)imax(1, nz_solid - 1);
-        scalars[kScalarArcK] = kf;
-    }
+    for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+    int ks = best >= 0 ? best : imax(1, nz_solid - 1);
+    float kf = (float)ks;
+    if (kf < 1.0f) kf = (float)imax(1, nz_solid - 1);
+    return kf;
+}
+
+__global__ void k_surface_arc(Dims d, const float* phi, const int32_t* flags, float* scalars,
+                              int nz_solid) {
+    const float kf = surface_arc_k(d, phi, flags, scalars, nz_solid);
+    if (threadIdx.x == 0) scalars[kScalarArcK] = kf;
 }
 
 __device__ double tile_block_sum(double v) {
@@ -298,24 +306,51 @@ __device__ double tile_block_sum(double v) {
 // deterministic: fixed tile-to-block assignment, double partials, the last
 // block sums them in order.  Writes the weight sum and the energy per weight.
 __global__ void __launch_bounds__(256) k_arc_norm_tiles(Dims d, const int32_t* __restrict__ flags,
-                                                        const float* __restrict__ f_l, ArcParams p,
-                                                        float* scalars, float arc_k_offset,
-                                                        float Qe_dt, float dx3, Workspace ws) {
-    p.arc_k = scalars[kScalarArcK] + arc_k_offset;
+                                                        const float* __restrict__ f_l,
+                                                        const float* __restrict__ phi, int nz_solid,
+                                                        ArcParams p, float* scalars,
+                                                        float arc_k_offset, float Qe_dt, float dx3,
+                                                        Workspace ws) {
+    // every block finds the arc k itself (one warp scans the torch column), so
+    // the surface query needs no launch of its own; block 0 publishes it
+    __shared__ float s_arc_k;
+    if (threadIdx.y == 0) {
+        const float kf = surface_arc_k(d, phi, flags, scalars, nz_solid);
+        if (threadIdx.x == 0) {
+            s_arc_k = kf;
+            if (blockIdx.x == 0) scalars[kScalarArcK] = kf;
+        }
+    }
+    __syncthreads();
+    p.arc_k = s_arc_k + arc_k_offset;
     p.arc_i = scalars[kScalarArcI];
     p.arc_j = scalars[kScalarArcJ];
     const int kt = (d.nz + kTileK - 1) / kTileK, jt = (d.ny + kTileJ - 1) / kTileJ;
     const int tiles = kt * jt * d.nx;
+    // four tiles per pass: their flags and liquid fractions are all requested
+    // before any weight is computed (f_l of gas cells is read and ignored)
+    constexpr int kU = 4;
     double part = 0.0;
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-        int a = t % kt, r = t / kt;
-        int b = r % jt, i = r / jt;
-        int k = a * kTileK + threadIdx.x, j = b * kTileJ + threadIdx.y;
-        if (k >= d.nz || j >= d.ny) continue;
-        int c = (i * d.ny + j) * d.nz + k;
-        int flag = flags[c];
-        if (flag == GAS) continue;
-        part += (double)arc_cell_weight(p, i, j, k, flag, f_l[c]);
+    for (int t0 = blockIdx.x; t0 < tiles; t0 += kU * gridDim.x) {
+        int fg[kU], ci[kU], cj[kU], ck[kU];
+        float fl[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int t = t0 + u * gridDim.x;
+            const int a = t % kt, r = t / kt;
+            const int b = r % jt, i = r / jt;
+            const int k = a * kTileK + threadIdx.x, j = b * kTileJ + threadIdx.y;
+            const bool ok = t < tiles && k < d.nz && j < d.ny;
+            const int c = ok ? (i * d.ny + j) * d.nz + k : 0;
+            fg[u] = ok ? flags[c] : GAS;
+            fl[u] = ok ? f_l[c] : 0.0f;
+            ci[u] = i;
+            cj[u] = j;
+            ck[u] = k;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            if (fg[u] != GAS) part += (double)arc_cell_weight(p, ci[u], cj[u], ck[u], fg[u], fl[u]);
     }
     part = tile_block_sum(part);
     __shared__ bool last;
@@ -354,16 +389,19 @@ __global__ void __launch_bounds__(256) k_arc_inject_tiles(Dims d, float* __restr
                                                           PhaseParams ph) {
     int i, j, k, c;
     if (!tile_cell(d, i, j, k, c)) return;
-    int flag = flags[c];
-    if (flag == GAS) return;
+    // the device scalars and the flag are requested together, then f_l and H
     p.arc_k = scalars[kScalarArcK] + arc_k_offset;
     p.arc_i = scalars[kScalarArcI];
     p.arc_j = scalars[kScalarArcJ];
-    float epw = scalars[kScalarEpw];
+    const float epw = scalars[kScalarEpw];
+    const int flag = flags[c];
+    const float fl = f_l[c];           // requested with the flag (ignored for gas cells)
+    float h = cap ? H[c] : 0.0f;
+    if (flag == GAS) return;
     float dh;
-    bool hit = arc_cell_heat(p, epw, i, j, k, flag, f_l[c], dh);
+    const bool hit = arc_cell_heat(p, epw, i, j, k, flag, fl, dh);
     if (!hit && !cap) return;
-    float h = H[c];
+    if (!cap) h = H[c];
     if (hit) h = h + dh;
     if (cap) h = cap_h(ph, h);
     H[c] = h;
@@ -749,7 +787,7 @@ extern "C" {
 
 int waam_step_launch_count(const WaamStepParams* p, int stage) {
     if (!p) return 0;
-    if (stage == 0) return p->welding ? 3 : 1;
+    if (stage == 0) return p->welding ? 2 : 1;
     // thermal, [vof], column, collide, stream (tracers counted by the caller)
     int n = 1 + (p->vof ? 1 : 0) + 1 + 1 + 1;
     if (p->substrate_growth || p->bead_freeze) n += 1;
@@ -763,17 +801,19 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     if (!workspace_ok(workspace, workspace_bytes, d.n()))
         return fail(WAAM_ERR_INVALID, "step_pre: workspace too small or misaligned");
     Workspace ws = Workspace::at(workspace);
-    k_surface_arc<<<1, 32, 0, STREAM(stream)>>>(d, f->phi, f->flags, f->step_scalars,
-                                                p->nz_solid);
-    int e = check_launch("k_surface_arc");
-    if (e || !p->welding) return e;
+    if (!p->welding) {
+        k_surface_arc<<<1, 32, 0, STREAM(stream)>>>(d, f->phi, f->flags, f->step_scalars,
+                                                    p->nz_solid);
+        return check_launch("k_surface_arc");
+    }
     ArcParams a = arc_params(p);
     float Qe_dt = p->Q_w * p->eta * p->dt;
     const int tiles = (int)tile_grid(d).x * (int)tile_grid(d).y * d.nx;
     const int blocks = tiles < kTileRedBlocks ? tiles : kTileRedBlocks;
     k_arc_norm_tiles<<<blocks, tile_block(), 0, STREAM(stream)>>>(
-        d, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, Qe_dt, p->dx3, ws);
-    e = check_launch("k_arc_norm_tiles");
+        d, f->flags, f->f_l, f->phi, p->nz_solid, a, f->step_scalars, p->arc_k_offset, Qe_dt,
+        p->dx3, ws);
+    int e = check_launch("k_arc_norm_tiles");
     if (e) return e;
     PhaseParams ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
     k_arc_inject_tiles<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(

@@ -15,13 +15,13 @@ constexpr int kRedBlocks = 592;           // fixed so reduction order never depe
 //   [0, 512)            unsigned counters: [0] last-block reduction,
 //                       [kActiveShardSlot, +kActiveShards) active-cell counts per shard
 //   [512, 1024)         float scalars of the operator-level reductions
-//   [1024, 33792)       double partial sums, one per reduction block (<= 4096)
-//   [33792, ...)        one field-sized scratch (n + kFieldSlack elements): a float
+//   [1024, 132096)      double partial sums, one per reduction block (<= 16384)
+//   [132096, ...)       one field-sized scratch (n + kFieldSlack elements): a float
 //                       snapshot (operator API) or the int32 active-cell list (fused step)
 constexpr size_t kWsScalarsOffset = 512;
 constexpr size_t kWsPartialsOffset = 1024;
-constexpr int kWsMaxPartials = 4096;
-constexpr size_t kWsFieldOffset = 33792;
+constexpr int kWsMaxPartials = 16384;
+constexpr size_t kWsFieldOffset = kWsPartialsOffset + kWsMaxPartials * sizeof(double);
 constexpr int64_t kFieldSlack = 65536;
 constexpr int kActiveShards = 64;     // power of two
 
