@@ -69,6 +69,16 @@ _SIGS = {
     "wo_elec_bins": ([_F, _F, _i, _i, _i, _f, _f, _f, _f, _i], None),
     "wo_elec_B_axisymmetric": ([_F, _F, _F, _F, _i, _i, _i, _f, _f, _f, _f, _f, _i], None),
     "wo_apply_lorentz_JxB": ([_F] * 10 + [_I, _l, _f, _f, _f], None),
+    "wo_refresh_thermal_properties": ([_F, _F, _F, _F, _F, _I, _l, _F, _I, _F, _F] + [_f] * 5,
+                                      None),
+    "wo_advect_diffuse_temperature_variable": ([_F] * 5 + [_I, _F, _F, _i, _i, _i, _f], None),
+    "wo_update_phase_variable_cp": ([_F] * 4 + [_l] + [_f] * 5, None),
+    "wo_clamp_enthalpy_ceiling_variable_cp": ([_F, _I, _F, _l, _f, _f, _f], None),
+    "wo_clamp_enthalpy_floor": ([_F, _F, _I, _l, _f], None),
+    "wo_compute_marangoni_force_variable": ([_F] * 6 + [_I, _F, _i, _i, _i], None),
+    "wo_collide_srt_variable_tau": ([_F] * 10 + [_I, _F, _l, _f], None),
+    "wo_remelt_hot_solid": ([_F] * 4 + [_I, _F, _l, _f, _f, _f], None),
+    "wo_solidify_trailing_pool": ([_F] * 4 + [_I] + [_F] * 4 + [_i, _i, _i] + [_f] * 9, None),
     "wo_inject_tracers": ([_F, _I, _I, _i, _f, _f, _f, _f, _i, C.c_uint64], None),
     "wo_advect_tracers": ([_F, _I, _F, _F, _F, _F, _I, _i, _i, _i, _f, _i], None),
     "wo_num_threads": ([], C.c_int),

@@ -268,9 +268,30 @@ static inline float masked(const float* fld, const int32_t* flags, int nx, int n
 }
 
 /* kernels.py:1611-1682 advect_diffuse_temperature, snapshot semantics on H */
+static void advect_diffuse_impl(float* H, const float* T, const float* ux, const float* uy,
+                                const float* uz, const int32_t* flags, int nx, int ny, int nz,
+                                float alpha_lu, float dt, float cp_rho, const float* alpha_f,
+                                const float* cp_f);
+
 void wo_advect_diffuse_temperature(float* H, const float* T, const float* ux, const float* uy,
                                    const float* uz, const int32_t* flags, int nx, int ny, int nz,
                                    float alpha_lu, float dt, float cp_rho) {
+    advect_diffuse_impl(H, T, ux, uy, uz, flags, nx, ny, nz, alpha_lu, dt, cp_rho, NULL, NULL);
+}
+
+/* kernels.py:1775-1836 advect_diffuse_temperature_variable: the same scheme
+ * with the cell's own cp*rho and alpha_lu */
+void wo_advect_diffuse_temperature_variable(float* H, const float* T, const float* ux,
+                                            const float* uy, const float* uz,
+                                            const int32_t* flags, const float* alpha_f,
+                                            const float* cp_f, int nx, int ny, int nz, float dt) {
+    advect_diffuse_impl(H, T, ux, uy, uz, flags, nx, ny, nz, 0.0f, dt, 0.0f, alpha_f, cp_f);
+}
+
+static void advect_diffuse_impl(float* H, const float* T, const float* ux, const float* uy,
+                                const float* uz, const int32_t* flags, int nx, int ny, int nz,
+                                float alpha_lu, float dt, float cp_rho, const float* alpha_f,
+                                const float* cp_f) {
     int64_t n = (int64_t)nx * ny * nz;
     float* H0 = (float*)malloc(n * sizeof(float));
     memcpy(H0, H, n * sizeof(float));
@@ -289,7 +310,8 @@ void wo_advect_diffuse_temperature(float* H, const float* T, const float* ux, co
                 float Tkm = masked(T, flags, nx, ny, nz, i, j, k - 1, Tc);
                 float Tkp = masked(T, flags, nx, ny, nz, i, j, k + 1, Tc);
                 float lap = Tip + Tim + Tjp + Tjm + Tkp + Tkm - 6.0f * Tc;
-                float dH = cp_rho * alpha_lu * lap * dt;
+                float cr = cp_f ? cp_f[c] : cp_rho, al = alpha_f ? alpha_f[c] : alpha_lu;
+                float dH = cr * al * lap * dt;
                 if (flag != SOLID) {
                     float u = ux[c], v = uy[c], w = uz[c];
                     float Him = masked(H0, flags, nx, ny, nz, i - 1, j, k, Hc);
@@ -660,9 +682,26 @@ void wo_compute_csf_tension(const float* phi, const int32_t* flags, float* Fx, f
 }
 
 /* kernels.py:2158-2217 compute_marangoni_force */
+static void marangoni_impl(const float* T, const float* phi, const float* f_l, float* Fx,
+                           float* Fy, float* Fz, const int32_t* flags, int nx, int ny, int nz,
+                           float dgamma, const float* dg_f);
+
 void wo_compute_marangoni_force(const float* T, const float* phi, const float* f_l, float* Fx,
                                 float* Fy, float* Fz, const int32_t* flags, int nx, int ny, int nz,
                                 float dgamma) {
+    marangoni_impl(T, phi, f_l, Fx, Fy, Fz, flags, nx, ny, nz, dgamma, NULL);
+}
+
+/* kernels.py:2221-2269 compute_marangoni_force_variable (per-cell dgamma) */
+void wo_compute_marangoni_force_variable(const float* T, const float* phi, const float* f_l,
+                                         float* Fx, float* Fy, float* Fz, const int32_t* flags,
+                                         const float* dg_f, int nx, int ny, int nz) {
+    marangoni_impl(T, phi, f_l, Fx, Fy, Fz, flags, nx, ny, nz, 0.0f, dg_f);
+}
+
+static void marangoni_impl(const float* T, const float* phi, const float* f_l, float* Fx,
+                           float* Fy, float* Fz, const int32_t* flags, int nx, int ny, int nz,
+                           float dgamma, const float* dg_f) {
 #pragma omp parallel for collapse(2)
     for (int i = 0; i < nx; ++i)
         for (int j = 0; j < ny; ++j)
@@ -684,7 +723,7 @@ void wo_compute_marangoni_force(const float* T, const float* phi, const float* f
                 float tz = 0.5f * (T[IX(i, j, kp)] - T[IX(i, j, km)]);
                 float nd = nxn * tx + nyn * ty + nzn * tz;
                 float sx = tx - nd * nxn, sy = ty - nd * nyn, sz = tz - nd * nzn;
-                float scale = dgamma * g;
+                float scale = (dg_f ? dg_f[c] : dgamma) * g;
                 Fx[c] += scale * sx;
                 Fy[c] += scale * sy;
                 Fz[c] += scale * sz;
@@ -834,14 +873,37 @@ void wo_collide_mrt(const float* f_src, float* f_dst, float* rho, float* ux, flo
 }
 
 /* kernels.py:2778-2885 collide_srt (BGK + Guo + Carman-Kozeny) */
+static void collide_srt_impl(const float* f_src, float* f_dst, float* rho, float* ux, float* uy,
+                             float* uz, const float* Fx, const float* Fy, const float* Fz,
+                             const float* f_l, const int32_t* flags, int64_t n, float omega_c,
+                             float C_darcy, const float* tau_f);
+
 void wo_collide_srt(const float* f_src, float* f_dst, float* rho, float* ux, float* uy, float* uz,
                     const float* Fx, const float* Fy, const float* Fz, const float* f_l,
                     const int32_t* flags, int64_t n, float omega, float C_darcy) {
+    collide_srt_impl(f_src, f_dst, rho, ux, uy, uz, Fx, Fy, Fz, f_l, flags, n, omega, C_darcy,
+                     NULL);
+}
+
+/* kernels.py:2889-2965 collide_srt_variable_tau: omega = 1/(tau + 1e-6) per cell */
+void wo_collide_srt_variable_tau(const float* f_src, float* f_dst, float* rho, float* ux,
+                                 float* uy, float* uz, const float* Fx, const float* Fy,
+                                 const float* Fz, const float* f_l, const int32_t* flags,
+                                 const float* tau_f, int64_t n, float C_darcy) {
+    collide_srt_impl(f_src, f_dst, rho, ux, uy, uz, Fx, Fy, Fz, f_l, flags, n, 0.0f, C_darcy,
+                     tau_f);
+}
+
+static void collide_srt_impl(const float* f_src, float* f_dst, float* rho, float* ux, float* uy,
+                             float* uz, const float* Fx, const float* Fy, const float* Fz,
+                             const float* f_l, const int32_t* flags, int64_t n, float omega_c,
+                             float C_darcy, const float* tau_f) {
     const float eps = 1e-6f;
 #pragma omp parallel for
     for (int64_t c = 0; c < n; ++c) {
         if (flags[c] == SOLID || flags[c] == GAS) continue;
         float fl = f_l[c];
+        float omega = tau_f ? 1.0f / (tau_f[c] + eps) : omega_c;
         float r = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
         for (int q = 0; q < 19; ++q) {
             float fq = f_src[q * n + c];
@@ -1383,4 +1445,166 @@ void wo_advect_tracers(float* pos, int32_t* active, const float* ux, const float
         pos[3 * p + 1] = pos[3 * p + 1] + uy[c] * dx;
         pos[3 * p + 2] = pos[3 * p + 2] + uz[c] * dx;
     }
+}
+
+/* ---------------- material-table path (kernels.py:1686-2010, 2454-2570) ---------------- */
+
+/* kernels.py:1686-1707 lookup_table_1d (the last matching segment wins) */
+static float lookup_1d(float T, const float* t, const float* v, int n, float fallback) {
+    float result = fallback;
+    if (n > 0) {
+        if (T <= t[0]) {
+            result = v[0];
+        } else if (T >= t[n - 1]) {
+            result = v[n - 1];
+        } else {
+            for (int idx = 0; idx < 7; ++idx) {
+                if (idx < n - 1) {
+                    float t0 = t[idx], t1 = t[idx + 1];
+                    if (T >= t0 && T <= t1) {
+                        float w = (T - t0) / (t1 - t0 + 1e-8f);
+                        result = v[idx] + w * (v[idx + 1] - v[idx]);
+                    }
+                }
+            }
+        }
+    }
+    return result;
+}
+
+/* kernels.py:1710-1772 refresh_thermal_properties (use_tables = 1).  tab holds
+ * cp_T, cp_V, k_T, k_V, mu_T, mu_V, dgamma_T, dgamma_V (8 knots each), cnt the
+ * four knot counts, fb the four fallbacks, ref cp_rho, alpha_lu, dgamma_lu,
+ * tau of the constants path. */
+void wo_refresh_thermal_properties(const float* T, float* cp_f, float* alpha_f, float* dg_f,
+                                   float* tau_f, const int32_t* flags, int64_t n,
+                                   const float* tab, const int32_t* cnt, const float* fb,
+                                   const float* ref, float rho, float dt, float dx,
+                                   float force_scale, float marangoni_scale) {
+#pragma omp parallel for
+    for (int64_t c = 0; c < n; ++c) {
+        if (flags[c] == SOLID || flags[c] == GAS) {
+            cp_f[c] = ref[0];
+            alpha_f[c] = ref[1];
+            dg_f[c] = ref[2];
+            tau_f[c] = ref[3];
+            continue;
+        }
+        float Tc = T[c];
+        float cp = lookup_1d(Tc, tab + 0, tab + 8, cnt[0], fb[0]);
+        float kv = lookup_1d(Tc, tab + 16, tab + 24, cnt[1], fb[1]);
+        float mu = lookup_1d(Tc, tab + 32, tab + 40, cnt[2], fb[2]);
+        float dg = lookup_1d(Tc, tab + 48, tab + 56, cnt[3], fb[3]);
+        float cp_r = rho * cp;
+        float alpha_phys = kv / (rho * cp + 1e-9f);
+        float nu_phys = mu / (rho + 1e-9f);
+        float nu_lu = nu_phys * dt / (dx * dx);
+        cp_f[c] = cp_r;
+        alpha_f[c] = alpha_phys * dt / (dx * dx);
+        dg_f[c] = dg * force_scale * marangoni_scale;
+        tau_f[c] = 3.0f * nu_lu + 0.5f;
+    }
+}
+
+/* kernels.py:1839-1863 update_phase_variable_cp */
+void wo_update_phase_variable_cp(const float* H, float* T, float* f_l, const float* cp_f,
+                                 int64_t n, float L_rho, float Ts, float Tl, float H_sol,
+                                 float H_liq) {
+#pragma omp parallel for
+    for (int64_t c = 0; c < n; ++c) {
+        float h = H[c], cp = cp_f[c];
+        if (h <= H_sol) {
+            f_l[c] = 0.0f;
+            T[c] = h / (cp + 1e-9f);
+        } else if (h >= H_liq) {
+            f_l[c] = 1.0f;
+            T[c] = Tl + (h - H_liq) / (cp + 1e-9f);
+        } else {
+            float fl = (h - H_sol) / L_rho;
+            f_l[c] = fl;
+            T[c] = Ts + fl * (Tl - Ts);
+        }
+    }
+}
+
+/* kernels.py:1988-2010 clamp_enthalpy_ceiling_variable_cp */
+void wo_clamp_enthalpy_ceiling_variable_cp(float* H, const int32_t* flags, const float* cp_f,
+                                           int64_t n, float H_liq, float Tl, float T_cap) {
+#pragma omp parallel for
+    for (int64_t c = 0; c < n; ++c) {
+        if (flags[c] == GAS) continue;
+        float cp_r = cp_f[c];
+        float cap_l = H_liq + cp_r * (T_cap - Tl);
+        float cap_s = cp_r * T_cap;
+        float h = H[c];
+        if (h > H_liq) {
+            if (h > cap_l) H[c] = cap_l;
+        } else {
+            if (h > cap_s) H[c] = cap_s;
+        }
+    }
+}
+
+/* kernels.py:1922-1935 clamp_enthalpy_floor (per-cell cp*rho) */
+void wo_clamp_enthalpy_floor(float* H, const float* cp_f, const int32_t* flags, int64_t n,
+                             float T_floor) {
+#pragma omp parallel for
+    for (int64_t c = 0; c < n; ++c) {
+        if (flags[c] == GAS) continue;
+        float h_min = cp_f[c] * T_floor;
+        if (H[c] < h_min) H[c] = h_min;
+    }
+}
+
+/* kernels.py:2454-2485 remelt_hot_solid (per-cell cp*rho) */
+void wo_remelt_hot_solid(float* T, float* H, float* f_l, float* phi, int32_t* flags,
+                         const float* cp_f, int64_t n, float Ts, float Tl, float L_rho) {
+#pragma omp parallel for
+    for (int64_t c = 0; c < n; ++c) {
+        if (flags[c] != SOLID) continue;
+        float Tc = T[c];
+        if (Tc <= Ts + 5.0f) continue;
+        float cp_r = cp_f[c];
+        float H_sol = cp_r * Ts;
+        float fl;
+        if (Tc >= Tl) {
+            fl = 1.0f;
+            H[c] = cp_r * Tl + L_rho + cp_r * (Tc - Tl);
+        } else {
+            fl = (Tc - Ts) / (Tl - Ts + 1e-6f);
+            H[c] = H_sol + fl * L_rho;
+        }
+        f_l[c] = fl;
+        phi[c] = 1.0f;
+        flags[c] = FLUID;
+    }
+}
+
+/* kernels.py:2524-2570 solidify_trailing_pool (per-cell cp*rho) */
+void wo_solidify_trailing_pool(float* T, float* H, float* f_l, float* phi, int32_t* flags,
+                               float* ux, float* uy, float* uz, const float* cp_f, int nx, int ny,
+                               int nz, float arc_i, float arc_j, float arc_k, float dir_x,
+                               float dir_y, float dir_z, float lookback, float T_freeze,
+                               float Ts) {
+#pragma omp parallel for collapse(2)
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                int64_t c = IX(i, j, k);
+                if (flags[c] == GAS) continue;
+                if (phi[c] < 0.85f || f_l[c] < 0.05f) continue;
+                float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - arc_k;
+                float proj = di * dir_x + dj * dir_y + dk * dir_z;
+                if (proj > -lookback) continue;
+                if (T[c] >= T_freeze) continue;
+                float cp_r = cp_f[c];
+                H[c] = cp_r * (Ts - 1.0f);
+                T[c] = Ts - 1.0f;
+                f_l[c] = 0.0f;
+                phi[c] = 1.0f;
+                flags[c] = SOLID;
+                ux[c] = 0.0f;
+                uy[c] = 0.0f;
+                uz[c] = 0.0f;
+            }
 }

@@ -138,6 +138,38 @@ void wo_apply_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* Jx, cons
                           const float* f_l, const int32_t* flags, int64_t n, float dt, float dx,
                           float rho_ref);
 
+/* material-table path (kernels.py:1686-2010, 2221-2269, 2454-2570, 2889-2965) */
+void wo_refresh_thermal_properties(const float* T, float* cp_f, float* alpha_f, float* dg_f,
+                                   float* tau_f, const int32_t* flags, int64_t n,
+                                   const float* tab, const int32_t* cnt, const float* fb,
+                                   const float* ref, float rho, float dt, float dx,
+                                   float force_scale, float marangoni_scale);
+void wo_advect_diffuse_temperature_variable(float* H, const float* T, const float* ux,
+                                            const float* uy, const float* uz,
+                                            const int32_t* flags, const float* alpha_f,
+                                            const float* cp_f, int nx, int ny, int nz, float dt);
+void wo_update_phase_variable_cp(const float* H, float* T, float* f_l, const float* cp_f,
+                                 int64_t n, float L_rho, float Ts, float Tl, float H_sol,
+                                 float H_liq);
+void wo_clamp_enthalpy_ceiling_variable_cp(float* H, const int32_t* flags, const float* cp_f,
+                                           int64_t n, float H_liq, float Tl, float T_cap);
+void wo_clamp_enthalpy_floor(float* H, const float* cp_f, const int32_t* flags, int64_t n,
+                             float T_floor);
+void wo_compute_marangoni_force_variable(const float* T, const float* phi, const float* f_l,
+                                         float* Fx, float* Fy, float* Fz, const int32_t* flags,
+                                         const float* dg_f, int nx, int ny, int nz);
+void wo_collide_srt_variable_tau(const float* f_src, float* f_dst, float* rho, float* ux,
+                                 float* uy, float* uz, const float* Fx, const float* Fy,
+                                 const float* Fz, const float* f_l, const int32_t* flags,
+                                 const float* tau_f, int64_t n, float C_darcy);
+void wo_remelt_hot_solid(float* T, float* H, float* f_l, float* phi, int32_t* flags,
+                         const float* cp_f, int64_t n, float Ts, float Tl, float L_rho);
+void wo_solidify_trailing_pool(float* T, float* H, float* f_l, float* phi, int32_t* flags,
+                               float* ux, float* uy, float* uz, const float* cp_f, int nx, int ny,
+                               int nz, float arc_i, float arc_j, float arc_k, float dir_x,
+                               float dir_y, float dir_z, float lookback, float T_freeze,
+                               float Ts);
+
 /* kernels.py:3182-3205 inject_tracers with the library's counter-based hash
  * (the reference's ti.random() is not reproducible) */
 void wo_inject_tracers(float* pos, int32_t* active, int32_t* head, int max_tracers, float arc_x,

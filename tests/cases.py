@@ -46,7 +46,8 @@ def full_inputs(name):
     seed_map = {"inject_goldak": 1, "thermal_s2": 2, "vof_wet": 3, "contact": 4,
                 "contact_s5": 5, "forces_wet": 6, "csf": 7, "csf_wet": 8, "collide_srt": 9,
                 "tail": 10, "heat_loss": 11, "surface_height": 12, "deposit": 13,
-                "lorentz": 14, "tracers": 15}
+                "lorentz": 14, "tracers": 15, "refresh": 16, "thermal_var": 17, "phase_var": 18,
+                "forces_var": 19, "srt_var": 20, "tail_var": 21}
     grids = [v.shape[-3:] for v in ins.values() if v.ndim >= 3 and v.shape[-1] != 3]
     nx, ny, nz = grids[0] if grids else (13, 11, 12)   # tracer-only cases: the kernel-case grid
     st = state_gen.seeded_state(nx, ny, nz, seed=seed_map.get(name, 0))
@@ -76,6 +77,19 @@ def compare(name, got, want, field, rtol=None):
     assert bad == 0, "%s: %s has %d cells beyond tolerance (max err %.3e, scale %.3e)" % (
         name, field, bad, float(err.max()), scale)
     return float(err.max() / max(scale, 1e-30))
+
+
+def table_arrays(a):
+    """Oracle-style table arguments from a fixture's args: knots (64), counts,
+    fallbacks, constants-path reference values."""
+    tab = np.concatenate([np.asarray(a[key], np.float32) for key in (
+        "cp_T", "cp_V", "k_T", "k_V", "mu_T", "mu_V", "dgamma_T", "dgamma_V")])
+    cnt = np.array([a["n_cp"], a["n_k"], a["n_mu"], a["n_dgamma"]], np.int32)
+    fb = np.array([a["cp_fallback"], a["k_fallback"], a["mu_fallback"], a["dgamma_fallback"]],
+                  np.float32)
+    ref = np.array([a["cp_rho_ref"], a["alpha_lu_ref"], a["dgamma_lu_ref"], a["tau_ref"]],
+                   np.float32)
+    return tab, cnt, fb, ref
 
 
 def run_case(be, name, st, a):
@@ -221,6 +235,43 @@ def run_case(be, name, st, a):
                              st["Bx"], st["By"], st["Bz"], st["f_l"], st["flags"], n, a["dt"],
                              a["dx"], a["rho_ref"])
         return l1
+    elif name == "refresh":
+        tab, cnt, fb, ref = table_arrays(a)
+        be.refresh_thermal_properties(st["T"], st["cp_rho_field"], st["alpha_lu_field"],
+                                      st["dgamma_lu_field"], st["tau_field"], st["flags"], n, tab,
+                                      cnt, fb, ref, a["rho"], a["dt"], a["dx"], a["force_scale"],
+                                      a["marangoni_scale"])
+    elif name == "thermal_var":
+        be.advect_diffuse_temperature_variable(st["H"], st["T"], st["ux"], st["uy"], st["uz"],
+                                               st["flags"], st["alpha_lu_field"],
+                                               st["cp_rho_field"], nx, ny, nz, 1.0)
+    elif name == "phase_var":
+        be.clamp_enthalpy_floor(st["H"], st["cp_rho_field"], st["flags"], n, a["T_floor"])
+        for step in range(2):
+            be.update_phase_variable_cp(st["H"], st["T"], st["f_l"], st["cp_rho_field"], n,
+                                        a["L_rho_t"], a["T_solidus_t"], a["T_liquidus_t"],
+                                        a["H_sol_t"], a["H_liq_t"])
+            if step == 0:
+                be.clamp_enthalpy_ceiling_variable_cp(st["H"], st["flags"], st["cp_rho_field"], n,
+                                                      a["H_liq_t"], a["T_liquidus_t"],
+                                                      a["T_cap_case"])
+    elif name == "forces_var":
+        be.clear_forces(st["Fx"], st["Fy"], st["Fz"], n)
+        be.compute_marangoni_force_variable(st["T"], st["phi"], st["f_l"], st["Fx"], st["Fy"],
+                                            st["Fz"], st["flags"], st["dgamma_lu_field"], nx, ny,
+                                            nz)
+    elif name == "srt_var":
+        be.collide_srt_variable_tau(st["f_a"], st["f_b"], st["rho"], st["ux"], st["uy"],
+                                    st["uz"], st["Fx"], st["Fy"], st["Fz"], st["f_l"],
+                                    st["flags"], st["tau_field"], n, a["C_darcy"])
+    elif name == "tail_var":
+        be.remelt_hot_solid(st["T"], st["H"], st["f_l"], st["phi"], st["flags"],
+                            st["cp_rho_field"], n, a["T_solidus_t"], a["T_liquidus_t"],
+                            a["L_rho_t"])
+        be.solidify_trailing_pool(st["T"], st["H"], st["f_l"], st["phi"], st["flags"], st["ux"],
+                                  st["uy"], st["uz"], st["cp_rho_field"], nx, ny, nz, a["arc_i"],
+                                  a["arc_j"], a["arc_k"], 1.0, 0.0, 0.0, a["lookback"],
+                                  a["T_freeze"], a["T_solidus_t"])
     elif name == "tracers":
         be.advect_tracers(st["porosity_pos"], st["porosity_active"], st["ux"], st["uy"], st["uz"],
                           st["f_l"], st["flags"], nx, ny, nz, a["dx"], a["max_tracers"])
@@ -242,7 +293,8 @@ def run_case(be, name, st, a):
 CASES = ["inject_gauss", "inject_goldak", "ceiling", "thermal", "thermal_s2", "phase",
          "tmax_cool", "vof", "vof_wet", "contact", "contact_s5", "forces", "forces_wet", "csf",
          "csf_wet", "collide_mrt", "collide_srt", "stream", "tail", "heat_loss",
-         "surface_height", "deposit", "lorentz", "tracers", "reset"]
+         "surface_height", "deposit", "lorentz", "tracers", "refresh", "thermal_var",
+         "phase_var", "forces_var", "srt_var", "tail_var", "reset"]
 
 
 def check_case(be, name):

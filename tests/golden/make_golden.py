@@ -58,7 +58,49 @@ def material(theta_deg=30.0):
     )
 
 
+def table_material():
+    """The reference's validated ER70S-6 file: cp, k, mu and dgamma/dT tables."""
+    from waam_twin.materials import load_material
+    return load_material(os.path.join(refload.REFERENCE_ROOT, "materials", "validated",
+                                      "ER70S-6.v1.yaml"))
+
+
+def table_args(tw):
+    """The twin's GPU tables (float32 knots as uploaded) and reference values."""
+    t = tw.gpu_tables
+    out = {}
+    for name in ("cp", "k", "mu", "dgamma"):
+        out[name + "_T"] = [float(v) for v in getattr(t, name + "_T").to_numpy()]
+        out[name + "_V"] = [float(v) for v in getattr(t, name + "_V").to_numpy()]
+        out["n_" + name] = int(getattr(t, "n_" + name)[None])
+    out.update(cp_fallback=t.cp_fallback, k_fallback=t.k_fallback, mu_fallback=t.mu_fallback,
+               dgamma_fallback=t.dgamma_fallback, rho=tw.mat.rho,
+               force_scale=tw.force_scale / tw.grid.dx, cp_rho_ref=tw.cp_rho,
+               alpha_lu_ref=tw.alpha_lu, dgamma_lu_ref=tw.dgamma_dT_lu, tau_ref=tw.grid.tau,
+               marangoni_scale=tw.marangoni_scale, H_sol_t=tw.H_sol, H_liq_t=tw.H_liq,
+               T_solidus_t=tw.mat.T_solidus, T_liquidus_t=tw.mat.T_liquidus,
+               L_rho_t=tw.L_rho, T_cap=tw.T_vapor_cap_K, C_darcy=tw.C_darcy)
+    return out
+
+
+def refresh(tw, g):
+    t = tw.gpu_tables
+    K.refresh_thermal_properties(
+        g.T, g.cp_rho_field, g.alpha_lu_field, g.dgamma_lu_field, g.tau_field,
+        t.cp_T, t.cp_V, t.k_T, t.k_V, t.mu_T, t.mu_V, t.dgamma_T, t.dgamma_V,
+        t.n_cp, t.n_k, t.n_mu, t.n_dgamma, tw.mat.rho, g.dt, g.dx,
+        t.cp_fallback, t.k_fallback, t.mu_fallback, t.dgamma_fallback,
+        tw.force_scale / g.dx, tw.cp_rho, tw.alpha_lu, tw.dgamma_dT_lu, g.tau,
+        tw.marangoni_scale, 1, g.flags, g.FLAG_SOLID, g.FLAG_GAS)
+
+
 def make_twin(nx, ny, nz, dx=2e-4, **kw):
+    if kw.pop("tables", False):
+        kw.setdefault("use_srt", False)
+        kw.setdefault("enable_vof", True)
+        kw.setdefault("max_tracers", 64)
+        kw.setdefault("droplet_freq_hz", 0.0)
+        return wt.WAAMTwin(material=table_material(), nx=nx, ny=ny, nz=nz, dx=dx, **kw)
     kw.setdefault("use_srt", False)
     kw.setdefault("enable_vof", True)
     kw.setdefault("max_tracers", 64)
@@ -396,6 +438,77 @@ def c_tracers(tw, g):
     return a
 
 
+PROP_FIELDS = ["cp_rho_field", "alpha_lu_field", "dgamma_lu_field", "tau_field"]
+
+
+def c_refresh(tw, g):
+    a = scal(tw)
+    a.update(table_args(tw))
+    refresh(tw, g)
+    return a
+
+
+def props_setup(tw, g):
+    refresh(tw, g)        # realistic per-cell properties as the kernel inputs
+
+
+def c_thermal_var(tw, g):
+    a = scal(tw)
+    a.update(table_args(tw))
+    K.advect_diffuse_temperature_variable(g.H, g.T, g.ux, g.uy, g.uz, g.flags, g.alpha_lu_field,
+                                          g.cp_rho_field, 1.0, g.FLAG_SOLID, g.FLAG_GAS,
+                                          g.nx, g.ny, g.nz)
+    return a
+
+
+def c_phase_var(tw, g):
+    a = scal(tw)
+    a.update(table_args(tw))
+    K.clamp_enthalpy_floor(g.H, g.cp_rho_field, g.flags, 300.0, g.FLAG_GAS)
+    K.update_phase_variable_cp(g.H, g.T, g.f_l, g.cp_rho_field, tw.L_rho, tw.mat.T_solidus,
+                               tw.mat.T_liquidus, tw.H_sol, tw.H_liq)
+    K.clamp_enthalpy_ceiling_variable_cp(g.H, g.flags, g.cp_rho_field, tw.H_liq,
+                                         tw.mat.T_liquidus, 2500.0, g.FLAG_GAS)
+    K.update_phase_variable_cp(g.H, g.T, g.f_l, g.cp_rho_field, tw.L_rho, tw.mat.T_solidus,
+                               tw.mat.T_liquidus, tw.H_sol, tw.H_liq)
+    a["T_floor"] = 300.0
+    a["T_cap_case"] = 2500.0
+    return a
+
+
+def c_forces_var(tw, g):
+    a = scal(tw)
+    a.update(table_args(tw))
+    K.clear_forces(g.Fx, g.Fy, g.Fz)
+    K.compute_marangoni_force_variable(g.T, g.phi, g.f_l, g.Fx, g.Fy, g.Fz, g.flags,
+                                       g.dgamma_lu_field, g.FLAG_SOLID, g.FLAG_GAS,
+                                       g.nx, g.ny, g.nz)
+    return a
+
+
+def c_srt_var(tw, g):
+    a = scal(tw)
+    a.update(table_args(tw))
+    K.collide_srt_variable_tau(g.f_a, g.f_b, g.rho, g.ux, g.uy, g.uz, g.Fx, g.Fy, g.Fz, g.f_l,
+                               g.flags, g.tau_field, tw.C_darcy, g.FLAG_SOLID, g.FLAG_GAS,
+                               g.nx, g.ny, g.nz)
+    return a
+
+
+def c_tail_var(tw, g):
+    a = scal(tw)
+    a.update(table_args(tw))
+    a.update(arc_i=9.5, arc_j=5.0, arc_k=float(tw.nz_solid + 1), lookback=2.0,
+             T_freeze=tw.mat.T_liquidus + 35.0)
+    K.remelt_hot_solid(g.T, g.H, g.f_l, g.phi, g.flags, g.cp_rho_field, tw.mat.T_solidus,
+                       tw.mat.T_liquidus, tw.L_rho, g.FLAG_SOLID, g.FLAG_FLUID)
+    K.solidify_trailing_pool(g.T, g.H, g.f_l, g.phi, g.flags, g.ux, g.uy, g.uz, g.cp_rho_field,
+                             a["arc_i"], a["arc_j"], a["arc_k"], 1.0, 0.0, 0.0, a["lookback"],
+                             a["T_freeze"], tw.mat.T_solidus, g.FLAG_SOLID, g.FLAG_FLUID,
+                             g.FLAG_GAS)
+    return a
+
+
 def c_reset(tw, g):
     a = scal(tw)
     tw.reset()
@@ -432,6 +545,18 @@ def kernel_cases():
     kernel_case("lorentz", c_lorentz, LORENTZ_FIELDS, seed=14, extra_in=lorentz_setup)
     kernel_case("tracers", c_tracers, ["porosity_pos", "porosity_active"], seed=15,
                 extra_in=tracer_setup)
+    tb = dict(tables=True)
+    kernel_case("refresh", c_refresh, PROP_FIELDS, seed=16, twin_kw=tb)
+    kernel_case("thermal_var", c_thermal_var, ["H"] + PROP_FIELDS, seed=17, twin_kw=tb,
+                extra_in=props_setup)
+    kernel_case("phase_var", c_phase_var, ["H", "T", "f_l"] + PROP_FIELDS, seed=18,
+                twin_kw=tb, extra_in=props_setup)
+    kernel_case("forces_var", c_forces_var, ["Fx", "Fy", "Fz"] + PROP_FIELDS, seed=19,
+                twin_kw=tb, extra_in=props_setup)
+    kernel_case("srt_var", c_srt_var, ["f_b", "rho", "ux", "uy", "uz"] + PROP_FIELDS, seed=20,
+                twin_kw=tb, extra_in=props_setup)
+    kernel_case("tail_var", c_tail_var, base + ["ux", "uy", "uz"] + PROP_FIELDS, seed=21,
+                twin_kw=tb, extra_in=props_setup)
     kernel_case("reset", c_reset, base + ["rho", "ux", "uy", "uz", "f_a", "f_b", "T_max",
                                           "T_prev", "dT_dt", "time_above_800_s", "Fx", "Fx_snap"])
 

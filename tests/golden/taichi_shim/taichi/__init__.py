@@ -64,6 +64,7 @@ cfg = _Cfg()
 # kernel name -> {argument name: "cell" | "column"}
 SNAPSHOT_SEMANTICS = {
     "advect_diffuse_temperature": {"H": "cell"},
+    "advect_diffuse_temperature_variable": {"H": "cell"},
     "apply_contact_angle_phi_bc": {"phi": "column"},
 }
 
