@@ -36,6 +36,9 @@ int waam_abi_version(void);
 /* Bytes of device workspace needed by the reducing entry points and the fused
  * step for a grid of n cells (block partial sums and a field-sized scratch). */
 size_t waam_workspace_bytes(int64_t n);
+/* sizeof of the ABI structs, for FFI layout checks: 0 WaamFields,
+ * 1 WaamStepParams, 2 WaamMaterialTables (0 for any other value) */
+size_t waam_struct_size(int which);
 
 /* ---- operator API: one entry per reference Taichi kernel ---------------- */
 
@@ -281,6 +284,71 @@ int waam_advect_tracers(float* pos, int32_t* active, const float* ux, const floa
                         const float* uz, const float* f_l, const int32_t* flags, int nx, int ny,
                         int nz, float dx, int max_tracers, void* stream);
 
+/* ---- temperature-dependent material tables (kernels.py:1686-2010, 2454-2570) */
+
+/* gpu_tables.py:12-80 MaterialGPUTables: up to 8 (T [K], value) knots per
+ * property, sorted by T; a count of 0 selects the fallback constant.  The
+ * struct is read on the host and passed to the kernels by value. */
+#define WAAM_TABLE_KNOTS 8
+typedef struct WaamMaterialTables {
+    float cp_T[WAAM_TABLE_KNOTS], cp_V[WAAM_TABLE_KNOTS];
+    float k_T[WAAM_TABLE_KNOTS], k_V[WAAM_TABLE_KNOTS];
+    float mu_T[WAAM_TABLE_KNOTS], mu_V[WAAM_TABLE_KNOTS];
+    float dgamma_T[WAAM_TABLE_KNOTS], dgamma_V[WAAM_TABLE_KNOTS];
+    int32_t n_cp, n_k, n_mu, n_dgamma;
+    float cp_fallback, k_fallback, mu_fallback, dgamma_fallback;
+} WaamMaterialTables;
+
+/* kernels.py:1710-1772 refresh_thermal_properties: per-cell rho*cp(T),
+ * alpha_lu(T), dgamma_lu(T) (x force_scale x marangoni_scale) and SRT tau(T)
+ * from the tables (use_tables = 1) or the reference constants; SOLID and GAS
+ * cells take the reference constants.  `tables` is a host pointer. */
+int waam_refresh_thermal_properties(const float* T, float* cp_rho_f, float* alpha_f,
+                                    float* dgamma_f, float* tau_f, const int32_t* flags, int64_t n,
+                                    const WaamMaterialTables* tables, float rho, float dt,
+                                    float dx, float force_scale, float cp_rho_ref,
+                                    float alpha_lu_ref, float dgamma_lu_ref, float tau_ref,
+                                    float marangoni_scale, int use_tables, void* stream);
+/* kernels.py:1775-1836 advect_diffuse_temperature_variable (snapshot of H in
+ * the workspace, like waam_advect_diffuse_temperature) */
+int waam_advect_diffuse_temperature_variable(float* H, const float* T, const float* ux,
+                                             const float* uy, const float* uz,
+                                             const int32_t* flags, const float* alpha_f,
+                                             const float* cp_rho_f, int nx, int ny, int nz,
+                                             float dt, void* workspace, size_t workspace_bytes,
+                                             void* stream);
+/* kernels.py:1839-1863 update_phase_variable_cp */
+int waam_update_phase_variable_cp(const float* H, float* T, float* f_l, const float* cp_rho_f,
+                                  int64_t n, float L_rho, float T_solidus, float T_liquidus,
+                                  float H_sol, float H_liq, void* stream);
+/* kernels.py:1988-2010 clamp_enthalpy_ceiling_variable_cp */
+int waam_clamp_enthalpy_ceiling_variable_cp(float* H, const int32_t* flags, const float* cp_rho_f,
+                                            int64_t n, float H_liq, float T_liquidus,
+                                            float T_cap, void* stream);
+/* kernels.py:1922-1935 clamp_enthalpy_floor (per-cell rho*cp) */
+int waam_clamp_enthalpy_floor(float* H, const float* cp_rho_f, const int32_t* flags, int64_t n,
+                              float T_floor, void* stream);
+/* kernels.py:2221-2269 compute_marangoni_force_variable (per-cell dgamma) */
+int waam_compute_marangoni_force_variable(const float* T, const float* phi, const float* f_l,
+                                          float* Fx, float* Fy, float* Fz, const int32_t* flags,
+                                          const float* dgamma_f, int nx, int ny, int nz,
+                                          void* stream);
+/* kernels.py:2889-2965 collide_srt_variable_tau: omega = 1 / (tau + 1e-6) per cell */
+int waam_collide_srt_variable_tau(const float* f_src, float* f_dst, float* rho, float* ux,
+                                  float* uy, float* uz, const float* Fx, const float* Fy,
+                                  const float* Fz, const float* f_l, const int32_t* flags,
+                                  const float* tau_f, int64_t n, float C_darcy, void* stream);
+/* kernels.py:2454-2485 remelt_hot_solid (per-cell rho*cp) */
+int waam_remelt_hot_solid(float* T, float* H, float* f_l, float* phi, int32_t* flags,
+                          const float* cp_rho_f, int64_t n, float T_solidus, float T_liquidus,
+                          float L_rho, void* stream);
+/* kernels.py:2524-2570 solidify_trailing_pool (per-cell rho*cp) */
+int waam_solidify_trailing_pool(float* T, float* H, float* f_l, float* phi, int32_t* flags,
+                                float* ux, float* uy, float* uz, const float* cp_rho_f, int nx,
+                                int ny, int nz, float arc_i, float arc_j, float arc_k, float dir_x,
+                                float dir_y, float dir_z, float lookback, float T_freeze,
+                                float T_solidus, void* stream);
+
 /* ---- fused step: the B200 pipeline of solvers/coupled_step.py:73-464 ----- */
 
 typedef struct WaamFields {
@@ -317,6 +385,12 @@ typedef struct WaamFields {
     float* tracer_pos;        /* (max_tracers, 3) */
     int32_t* tracer_active;   /* (max_tracers) */
     int max_tracers;
+    /* per-cell material properties (grid.py:146-149), read and written when
+     * WaamStepParams.use_tables != 0, otherwise unused (may be null) */
+    float* cp_rho_f;
+    float* alpha_f;
+    float* dgamma_f;
+    float* tau_f;
 } WaamFields;
 
 typedef struct WaamStepParams {
@@ -356,6 +430,20 @@ typedef struct WaamStepParams {
      * 2 bfloat16 offsets f_q - w_q (rho0 = 1), rounded to nearest; the
      * arithmetic is float32 in every case */
     int f_storage;
+    /* temperature-dependent material tables (twin.py:269-273): the thermal
+     * stage refreshes WaamFields' property fields from T and then uses the
+     * cell's own rho*cp and alpha; the enthalpy ceiling (also the one after
+     * the arc injection, which reads the fields of the previous step), the
+     * floor, the phase update, Marangoni and the remelt / trailing-freeze
+     * tail use the fields; variable_tau replaces the collision by the
+     * variable-tau SRT (solvers/coupled_step.py:168-458). */
+    int use_tables, variable_tau;
+    float rho_mat;          /* rho of the material [kg/m^3] */
+    float force_scale_lu;   /* Marangoni prefactor force_scale / dx */
+    float marangoni_scale;
+    float H_sol_t, H_liq_t; /* rho * cp(T_solidus) * T_solidus, H_sol_t + L_rho */
+    float tau_ref;          /* grid tau (SOLID / GAS cells) */
+    WaamMaterialTables tables;
 } WaamStepParams;
 
 /* Stages of one fused step.  waam_step_pre runs the surface-height query,

@@ -22,7 +22,8 @@ _W = np.array([1.0 / 3.0] + [1.0 / 18.0] * 6 + [1.0 / 36.0] * 12, dtype=np.float
 
 
 class OracleTwin:
-    """Constants-only material, Gaussian2D / Goldak / conical arc, MRT or SRT."""
+    """Constants or temperature tables (``tables={"cp": [(T, v), ...], ...}``),
+    Gaussian2D / Goldak / conical arc, MRT, SRT or variable-tau SRT."""
 
     def __init__(self, nx, ny, nz, dx, mat, precision="fp32", **kw):
         if precision not in ("fp32", "fp64"):
@@ -49,7 +50,7 @@ class OracleTwin:
             impact_lead_angle_deg=0.0, trailing_solidify_lookback_mm=2.5,
             trailing_solidify_temp_margin_K=35.0, enable_lorentz=False, sigma_liquid_Sm=1.0e6,
             sigma_solid_Sm=1.0e5, lorentz_jacobi_iters=40, lorentz_jacobi_omega=0.85,
-            lorentz_jacobi_tol=1e-4, max_tracers=64)
+            lorentz_jacobi_tol=1e-4, max_tracers=64, tables=None, use_variable_tau=True)
         unknown = set(kw) - set(self.cfg)
         if unknown:
             raise KeyError("unknown OracleTwin options: %s" % sorted(unknown))
@@ -71,6 +72,8 @@ class OracleTwin:
         scale_F = self.dt ** 2 / (m["rho"] * dx ** 2)
         self.dgamma_dT_lu = m["dgamma_dT"] * scale_F / dx
         self.gamma_lu = m["gamma_0"] * scale_F / dx
+        self.force_scale = scale_F
+        self._setup_tables(c["tables"])
         theta = c["contact_angle_deg"] if c["contact_angle_deg"] is not None else m.get("contact_angle_deg", 80.0)
         self.theta = math.radians(theta)
         headroom = max(6, nz // 4)
@@ -91,6 +94,79 @@ class OracleTwin:
         self.lorentz_warm = False
         self.lorentz_iters = []
 
+    def _setup_tables(self, tables):
+        """gpu_tables.py:12-80 (knot upload) and twin.py:269-273 (H_sol / H_liq
+        from cp(T_solidus)); materials.py:48-58 cp_at is material_tables.py
+        interp_linear."""
+        m = self.mat
+        tables = {k: sorted((float(a), float(b)) for a, b in v)
+                  for k, v in (tables or {}).items() if v}
+        self.use_tables = bool(tables)
+        cols, cnt = [], []
+        fb = [m["cp"], m["k"], m["mu"], m["dgamma_dT"]]
+        for key, fallback in zip(("cp", "k", "mu", "dgamma_dT"), fb):
+            knots = tables.get(key, [])[:8]
+            t = np.zeros(8, np.float32)
+            v = np.zeros(8, np.float32)
+            if not knots:
+                t[0], v[0] = 300.0, fallback
+                n = 1
+            else:
+                n = len(knots)
+                for q, (a, b) in enumerate(knots):
+                    t[q], v[q] = a, b
+            cols += [t, v]
+            cnt.append(n)
+        self.tab = np.concatenate(cols).astype(self.ft)
+        self.cnt = np.array(cnt, np.int32)
+        self.fb = np.array(fb, self.ft)
+
+        def cp_at(T):
+            knots = tables.get("cp", [])
+            if not knots:
+                return m["cp"]
+            if T <= knots[0][0]:
+                return knots[0][1]
+            if T >= knots[-1][0]:
+                return knots[-1][1]
+            for (t0, v0), (t1, v1) in zip(knots[:-1], knots[1:]):
+                if t0 <= T <= t1:
+                    return v0 if t1 == t0 else v0 + (T - t0) / (t1 - t0) * (v1 - v0)
+            return m["cp"]
+        self.H_sol = m["rho"] * cp_at(m["T_solidus"]) * m["T_solidus"]
+        self.H_liq = self.H_sol + self.L_rho
+
+    def _refresh(self):
+        """solvers/coupled_step.py:168-181 refresh_properties (use_tables = 1)."""
+        s = self.s
+        ref = np.array([self.cp_rho, self.alpha_lu, self.dgamma_dT_lu, self.tau], self.ft)
+        self.O.call("wo_refresh_thermal_properties", s["T"], s["cp_rho_field"],
+                    s["alpha_lu_field"], s["dgamma_lu_field"], s["tau_field"], s["flags"],
+                    s["T"].size, self.tab, self.cnt, self.fb, ref, self.mat["rho"], self.dt,
+                    self.dx, self.force_scale / self.dx, 1.0)
+
+    def _ceiling(self):
+        """solvers/coupled_step.py:17-31 _clamp_enthalpy_ceiling."""
+        s, c, m = self.s, self.cfg, self.mat
+        n = s["H"].size
+        if self.use_tables:
+            self.O.call("wo_clamp_enthalpy_ceiling_variable_cp", s["H"], s["flags"],
+                        s["cp_rho_field"], n, self.H_liq, m["T_liquidus"], c["T_vapor_cap_K"])
+        else:
+            self.O.call("wo_clamp_enthalpy_ceiling_scalar", s["H"], s["flags"], n, self.cp_rho,
+                        m["T_solidus"], m["T_liquidus"], c["T_vapor_cap_K"], self.L_rho)
+
+    def _phase(self):
+        s, m = self.s, self.mat
+        n = s["H"].size
+        if self.use_tables:
+            self.O.call("wo_update_phase_variable_cp", s["H"], s["T"], s["f_l"],
+                        s["cp_rho_field"], n, self.L_rho, m["T_solidus"], m["T_liquidus"],
+                        self.H_sol, self.H_liq)
+        else:
+            self.O.call("wo_update_phase", s["H"], s["T"], s["f_l"], n, self.cp_rho, self.L_rho,
+                        m["T_solidus"], m["T_liquidus"])
+
     # ---------------------------------------------------------------- state --
     def reset(self):
         nx, ny, nz = self.nx, self.ny, self.nz
@@ -109,6 +185,10 @@ class OracleTwin:
         s["T_prev"][...] = self.ft(T0)
         self.O.call("wo_stream", s["f_a"], s["f_b"], s["flags"], nx, ny, nz)
         s["read_is_a"] = True
+        # the property fields are zero when the grid is made and are not
+        # touched by reset (grid.py:146-149, twin.py:486-531)
+        for key in ("cp_rho_field", "alpha_lu_field", "dgamma_lu_field", "tau_field"):
+            s[key] = self.s[key] if self.s is not None and key in self.s else z()
         self.s = s
         self._tracer_fields()
         self.lorentz_warm = False
@@ -124,6 +204,8 @@ class OracleTwin:
             return v.astype(self.ft) if v.dtype.kind == "f" else v
         self.s = {k: (own(v) if isinstance(v, np.ndarray) else v) for k, v in st.items()}
         self.s.setdefault("phi_tmp", np.zeros_like(self.s["phi"]))
+        for key in ("cp_rho_field", "alpha_lu_field", "dgamma_lu_field", "tau_field"):
+            self.s.setdefault(key, np.zeros_like(self.s["phi"]))
         self.s.setdefault("read_is_a", True)
         self._tracer_fields()
 
@@ -231,22 +313,30 @@ class OracleTwin:
                        arc_j, arc_k, c["arc_power_W"], self.sigma_cells, self.dt, self.dx ** 3,
                        c["arc_efficiency"], pen, en)
             if cap:
-                self.O.call("wo_clamp_enthalpy_ceiling_scalar", s["H"], s["flags"], n, self.cp_rho,
-                       Ts, Tl, c["T_vapor_cap_K"], self.L_rho)
+                self._ceiling()
             self._maybe_droplet(arc_i, arc_j, arc_k)
-        self.O.call("wo_advect_diffuse_temperature", s["H"], s["T"], s["ux"], s["uy"], s["uz"],
-               s["flags"], nx, ny, nz, self.alpha_lu, 1.0, self.cp_rho)
+        if self.use_tables:
+            self._refresh()
+            self.O.call("wo_advect_diffuse_temperature_variable", s["H"], s["T"], s["ux"],
+                        s["uy"], s["uz"], s["flags"], s["alpha_lu_field"], s["cp_rho_field"],
+                        nx, ny, nz, 1.0)
+        else:
+            self.O.call("wo_advect_diffuse_temperature", s["H"], s["T"], s["ux"], s["uy"],
+                        s["uz"], s["flags"], nx, ny, nz, self.alpha_lu, 1.0, self.cp_rho)
         if c["enable_heat_loss"]:
             self.O.call("wo_apply_thermal_boundary_losses", s["H"], s["T"], s["flags"], nx, ny, nz,
                    c["T_ambient"], c["h_conv"], c["eps_rad"], int(c["enable_convection"]),
                    int(c["enable_radiation"]), self.dt, self.dx, 5.670374419e-8)
-            self.O.call("wo_clamp_enthalpy_floor_scalar", s["H"], self.cp_rho, s["flags"], n,
-                   c["T_ambient"])
-        self.O.call("wo_update_phase", s["H"], s["T"], s["f_l"], n, self.cp_rho, self.L_rho, Ts, Tl)
+            if self.use_tables:
+                self.O.call("wo_clamp_enthalpy_floor", s["H"], s["cp_rho_field"], s["flags"], n,
+                            c["T_ambient"])
+            else:
+                self.O.call("wo_clamp_enthalpy_floor_scalar", s["H"], self.cp_rho, s["flags"], n,
+                            c["T_ambient"])
+        self._phase()
         if cap:
-            self.O.call("wo_clamp_enthalpy_ceiling_scalar", s["H"], s["flags"], n, self.cp_rho, Ts,
-                   Tl, c["T_vapor_cap_K"], self.L_rho)
-        self.O.call("wo_update_phase", s["H"], s["T"], s["f_l"], n, self.cp_rho, self.L_rho, Ts, Tl)
+            self._ceiling()
+        self._phase()
         self.O.call("wo_update_T_max", s["T"], s["T_max"], s["flags"], n)
         self.O.call("wo_update_cooling_rate", s["T"], s["T_prev"], s["dT_dt"], s["flags"], n, self.dt)
         if c["enable_vof"]:
@@ -263,8 +353,12 @@ class OracleTwin:
         if c["enable_csf_tension"]:
             self.O.call("wo_compute_csf_tension", s["phi"], s["flags"], s["Fx"], s["Fy"], s["Fz"], nx,
                    ny, nz, self.gamma_lu, int(c["enable_wetting"]), self.theta)
-        self.O.call("wo_compute_marangoni_force", s["T"], s["phi"], s["f_l"], s["Fx"], s["Fy"],
-               s["Fz"], s["flags"], nx, ny, nz, self.dgamma_dT_lu)
+        if self.use_tables:
+            self.O.call("wo_compute_marangoni_force_variable", s["T"], s["phi"], s["f_l"],
+                        s["Fx"], s["Fy"], s["Fz"], s["flags"], s["dgamma_lu_field"], nx, ny, nz)
+        else:
+            self.O.call("wo_compute_marangoni_force", s["T"], s["phi"], s["f_l"], s["Fx"],
+                        s["Fy"], s["Fz"], s["flags"], nx, ny, nz, self.dgamma_dT_lu)
         if welding:
             self.O.call("wo_apply_arc_pressure", s["Fz"], s["flags"], s["phi"], nx, ny, nz, arc_i,
                    arc_j, arc_k, self.arc_sigma_m / self.dx, c["arc_pressure_pa"], self.dt,
@@ -276,7 +370,11 @@ class OracleTwin:
         if welding and c["enable_lorentz"]:
             self._lorentz(arc_i, arc_j, arc_k)
         self.O.call("wo_clamp_body_force_magnitude", s["Fx"], s["Fy"], s["Fz"], s["flags"], n, 0.05)
-        if c["use_srt"]:
+        if self.use_tables and c["use_variable_tau"]:
+            self.O.call("wo_collide_srt_variable_tau", self.fsrc(), self.fdst(), s["rho"],
+                        s["ux"], s["uy"], s["uz"], s["Fx"], s["Fy"], s["Fz"], s["f_l"],
+                        s["flags"], s["tau_field"], n, c["C_darcy"])
+        elif c["use_srt"]:
             self.O.call("wo_collide_srt", self.fsrc(), self.fdst(), s["rho"], s["ux"], s["uy"],
                    s["uz"], s["Fx"], s["Fy"], s["Fz"], s["f_l"], s["flags"], n, self.omega,
                    c["C_darcy"])
@@ -292,14 +390,25 @@ class OracleTwin:
                s["time_above_1100_s"], s["time_above_solidus_s"], n, self.dt, 800.0 + 273.15,
                1100.0 + 273.15, Ts)
         if c["enable_substrate_growth"] or c["enable_bead_freeze"]:
-            self.O.call("wo_remelt_hot_solid_scalar", s["T"], s["H"], s["f_l"], s["phi"], s["flags"],
-                   n, self.cp_rho, Ts, Tl, self.L_rho)
+            if self.use_tables:
+                self.O.call("wo_remelt_hot_solid", s["T"], s["H"], s["f_l"], s["phi"],
+                            s["flags"], s["cp_rho_field"], n, Ts, Tl, self.L_rho)
+            else:
+                self.O.call("wo_remelt_hot_solid_scalar", s["T"], s["H"], s["f_l"], s["phi"],
+                            s["flags"], n, self.cp_rho, Ts, Tl, self.L_rho)
             if welding and c["enable_bead_freeze"]:
                 lb = max(2.0, c["trailing_solidify_lookback_mm"] / (self.dx * 1000.0))
-                self.O.call("wo_solidify_trailing_pool_scalar", s["T"], s["H"], s["f_l"], s["phi"],
-                       s["flags"], s["ux"], s["uy"], s["uz"], nx, ny, nz, self.cp_rho, arc_i,
-                       arc_j, arc_k, self.dir[0], self.dir[1], self.dir[2], lb,
-                       Tl + c["trailing_solidify_temp_margin_K"], Ts)
+                T_fr = Tl + c["trailing_solidify_temp_margin_K"]
+                if self.use_tables:
+                    self.O.call("wo_solidify_trailing_pool", s["T"], s["H"], s["f_l"], s["phi"],
+                                s["flags"], s["ux"], s["uy"], s["uz"], s["cp_rho_field"], nx, ny,
+                                nz, arc_i, arc_j, arc_k, self.dir[0], self.dir[1], self.dir[2],
+                                lb, T_fr, Ts)
+                else:
+                    self.O.call("wo_solidify_trailing_pool_scalar", s["T"], s["H"], s["f_l"],
+                                s["phi"], s["flags"], s["ux"], s["uy"], s["uz"], nx, ny, nz,
+                                self.cp_rho, arc_i, arc_j, arc_k, self.dir[0], self.dir[1],
+                                self.dir[2], lb, T_fr, Ts)
             self.O.call("wo_solidify_cooled_metal", s["T"], s["f_l"], s["phi"], s["flags"], s["ux"],
                    s["uy"], s["uz"], n, Ts, 1)
         s["read_is_a"] = not s["read_is_a"]

@@ -7,13 +7,16 @@ cases in ``cases.py`` run unchanged against the CUDA kernels.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
 from waam_solver_b200 import _native
 
 _WS_FUNCS = {"inject_arc_heat", "inject_goldak_heat", "advect_diffuse_temperature",
-             "apply_contact_angle_phi_bc", "elec_normalize_source"}
+             "apply_contact_angle_phi_bc", "elec_normalize_source",
+             "advect_diffuse_temperature_variable"}
 _NORM_FUNCS = {"inject_arc_heat", "inject_goldak_heat"}
 
 
@@ -90,6 +93,23 @@ class CudaBackend:
         torch.cuda.synchronize()
         self.launched.append("elec_bins")
         bins[...] = tb.cpu().numpy()
+
+    def refresh_thermal_properties(self, T, cp_f, alpha_f, dg_f, tau_f, flags, n, tab, cnt, fb,
+                                   ref, rho, dt, dx, force_scale, marangoni_scale):
+        """The oracle's flat table arguments packed into a WaamMaterialTables."""
+        from waam_solver_b200 import kernels
+        tb = kernels.material_tables_struct(*[tab[8 * q:8 * q + 8] for q in range(8)],
+                                            *[int(c) for c in cnt], *[float(v) for v in fb])
+        outs = [self._up(a) for a in (cp_f, alpha_f, dg_f, tau_f)]
+        tT, tf = self._up(T), self._up(flags)
+        _native.call("waam_refresh_thermal_properties", tT.data_ptr(),
+                     *[o.data_ptr() for o in outs], tf.data_ptr(), n, ctypes.byref(tb),
+                     rho, dt, dx, force_scale, float(ref[0]), float(ref[1]), float(ref[2]),
+                     float(ref[3]), marangoni_scale, 1, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        self.launched.append("refresh_thermal_properties")
+        for host, t in zip((cp_f, alpha_f, dg_f, tau_f), outs):
+            host[...] = t.cpu().numpy()
 
     def surface_height_at(self, phi, flags, nx, ny, nz, i0, j0, nz_fallback):
         out = torch.zeros((), dtype=torch.float32, device=self.device)

@@ -575,8 +575,20 @@ def twin_scalars(tw):
     )
 
 
-def step_case(name, nx, ny, nz, n_steps, positions, twin_kw, setup=None, seeded=None):
-    tw = make_twin(nx, ny, nz, **twin_kw)
+def material_record(tw):
+    """Constants and tables of the twin's material after the surfactant model."""
+    m = tw.mat
+    consts = {k: float(getattr(m, k)) for k in (
+        "k", "rho", "cp", "alpha", "T_solidus", "T_liquidus", "L_fusion", "gamma_0",
+        "dgamma_dT", "T_ref_gamma", "mu", "beta_T")}
+    tables = {k: [list(map(float, r)) for r in getattr(m.tables, k)]
+              for k in ("cp", "k", "mu", "dgamma_dT")}
+    return dict(constants=consts, tables=tables, contact_angle_deg=m.contact_angle_deg)
+
+
+def step_case(name, nx, ny, nz, n_steps, positions, twin_kw, setup=None, seeded=None,
+              after_load=None):
+    tw = make_twin(nx, ny, nz, **dict(twin_kw))
     if setup:
         setup(tw)
     tw.reset()
@@ -584,10 +596,16 @@ def step_case(name, nx, ny, nz, n_steps, positions, twin_kw, setup=None, seeded=
     if seeded is not None:
         st = seeded_state(nx, ny, nz, seed=seeded, nz_solid=tw.nz_solid)
         load_state(g, st)
+    if after_load:
+        after_load(tw, g)
+    props = bool(twin_kw.get("tables"))
     payload = {}
     log = []
     for s in range(n_steps):
         dump_state(g, "s%d_" % s, payload)
+        if props:
+            for f in PROP_FIELDS:
+                payload["s%d_%s" % (s, f)] = getattr(g, f).to_numpy()
         payload["s%d_read_is_a" % s] = np.array(g.f_src is g.f_a)
         x, y = positions[s]
         tw.step(x, y, True)
@@ -595,9 +613,15 @@ def step_case(name, nx, ny, nz, n_steps, positions, twin_kw, setup=None, seeded=
                         deposited=tw._deposited_volume_m3, dir=list(tw._torch_dir_xyz),
                         last_drop=tw._last_droplet_time))
     dump_state(g, "s%d_" % n_steps, payload)
+    if props:
+        for f in PROP_FIELDS:
+            payload["s%d_%s" % (n_steps, f)] = getattr(g, f).to_numpy()
     payload["s%d_read_is_a" % n_steps] = np.array(g.f_src is g.f_a)
     payload["positions"] = np.array(positions, dtype=np.float64)
-    payload["scalars"] = np.array(json.dumps(twin_scalars(tw)))
+    sc = twin_scalars(tw)
+    if props:
+        sc.update(material=material_record(tw), H_sol=tw.H_sol, H_liq=tw.H_liq)
+    payload["scalars"] = np.array(json.dumps(sc))
     payload["twin_kw"] = np.array(json.dumps(twin_kw))
     payload["log"] = np.array(json.dumps(log))
     save("step_%s.npz" % name, payload)
@@ -676,6 +700,28 @@ def step_cases():
 
     run2("c2_drop", None)
     run2("c2_seeded", 22)
+    table_step_cases()
+
+
+def table_step_cases():
+    """The material-table path (solvers/coupled_step.py:168-458 with
+    use_material_tables): the validated ER70S-6 file, c1-like Gaussian arc,
+    heat losses on.  t1_plate starts from reset, where the property fields
+    are still zero at the first enthalpy ceiling; t1_seeded starts from a
+    molten state with refreshed fields, with substrate growth and the
+    trailing freeze on, and runs the variable-tau SRT collision."""
+    nx, ny, nz = 16, 12, 12
+    dx = 2.5e-4
+    cy = (ny // 2) * dx
+    pos = [(0.0012 + s * 0.008 * dx * 0.1, cy) for s in range(4)]
+    kw = dict(dx=dx, heat_source="gaussian2d", arc_power_W=3000.0, arc_efficiency=0.75,
+              arc_sigma_mm=0.75, travel_speed_m_s=0.008, enable_heat_loss=True, tables=True)
+    step_case("t1_plate", nx, ny, nz, 3, pos, kw,
+              setup=lambda tw: setattr(tw, "plate_thickness_mm", 1.0))
+    kw2 = dict(kw, enable_substrate_growth=True, enable_bead_freeze=True)
+    step_case("t1_seeded", nx, ny, nz, 3, pos, kw2,
+              setup=lambda tw: setattr(tw, "plate_thickness_mm", 1.0), seeded=23,
+              after_load=refresh)
 
 
 # ---------------------------------------------------------------------------
@@ -700,5 +746,7 @@ if __name__ == "__main__":
         kernel_cases()
     if "steps" in what:
         step_cases()
+    if "table_steps" in what:
+        table_step_cases()
     if "kats" in what:
         kats()

@@ -5,7 +5,6 @@ import numpy as np
 
 import steps
 from waam_solver_b200 import WAAMTwin
-from waam_solver_b200.materials import from_constants
 from waam_solver_b200.physics.arc import Goldak3D
 
 
@@ -13,7 +12,7 @@ def twin_for_case(name, step_mode="fused"):
     sc, kw, states, positions = steps.load_step_case(name)
     opt, extra = steps.driver_options(name, sc, kw)
     plate = opt.pop("plate_thickness_mm")
-    mat = from_constants("ER70S-6-constants", steps.MATERIAL, contact_angle_deg=30.0)
+    mat = steps.material_for(name, extra)[0]
     tw = WAAMTwin(material=mat, nx=sc["nx"], ny=sc["ny"], nz=sc["nz"], max_tracers=64,
                   step_mode=step_mode, **opt)
     tw.plate_thickness_mm = plate

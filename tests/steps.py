@@ -23,7 +23,15 @@ MATERIAL = dict(k=30.0, rho=7800.0, cp=680.0, T_solidus=1723.0, T_liquidus=1783.
                 L_fusion=2.7e5, gamma_0=1.8, dgamma_dT=-4.3e-4, mu=0.0065, beta_T=1.2e-4,
                 contact_angle_deg=30.0)
 
-STEP_CASES = ["c1_plate", "c1_seeded", "c2_drop", "c2_seeded"]
+PROP_FIELDS = ["cp_rho_field", "alpha_lu_field", "dgamma_lu_field", "tau_field"]
+
+# c*: constants-only material; t*: the material-table path (validated
+# ER70S-6 file with cp, k, mu and Sahoo dgamma/dT tables)
+STEP_CASES = ["c1_plate", "c1_seeded", "c2_drop", "c2_seeded", "t1_plate", "t1_seeded"]
+
+
+def fields_for(name):
+    return FIELDS + PROP_FIELDS if name.startswith("t") else FIELDS
 
 
 def load_step_case(name):
@@ -34,7 +42,7 @@ def load_step_case(name):
                    and k.split("_")[0][1:].isdigit()) + 1
     states = []
     for s in range(n_states):
-        st = {f: np.ascontiguousarray(z["s%d_%s" % (s, f)]) for f in FIELDS}
+        st = {f: np.ascontiguousarray(z["s%d_%s" % (s, f)]) for f in fields_for(name)}
         st["read_is_a"] = bool(z["s%d_read_is_a" % s])
         states.append(st)
     positions = [tuple(p) for p in z["positions"]]
@@ -48,14 +56,31 @@ def driver_options(name, sc, kw):
     opt.setdefault("enable_vof", True)
     opt.setdefault("droplet_freq_hz", 0.0)
     opt.pop("max_tracers", None)
+    opt.pop("tables", None)
     extra = dict(nz_solid=sc["nz_solid"])
-    if name.startswith("c1"):
+    if "material" in sc:
+        extra["material"] = sc["material"]
+    if name.startswith(("c1", "t1")):
         opt["plate_thickness_mm"] = 1.0
     else:
         opt["plate_thickness_mm"] = 0.8
         extra.update(wire_feed_m_s=0.1, droplet_transfer_mode="pulsed", pulse_frequency_hz=100.0,
                      droplet_size_jitter=0.0, goldak=sc["goldak"], last_drop=-1.0)
     return opt, extra
+
+
+def material_for(name, extra):
+    """(MaterialProps of the B200 twin, oracle constants dict, oracle tables)."""
+    from waam_solver_b200.materials import from_constants, MaterialTables
+    rec = extra.get("material")
+    if rec is None:
+        return (from_constants("ER70S-6-constants", MATERIAL, contact_angle_deg=30.0),
+                MATERIAL, None)
+    c = dict(rec["constants"])
+    mat = from_constants("ER70S-6", c, contact_angle_deg=rec["contact_angle_deg"])
+    mat.tables = MaterialTables(**{k: [tuple(r) for r in v] for k, v in rec["tables"].items()})
+    oc = dict(c, contact_angle_deg=rec["contact_angle_deg"])
+    return mat, oc, {k: [tuple(r) for r in v] for k, v in rec["tables"].items()}
 
 
 def compare_state(tag, got, want, fields=FIELDS, reference=False):

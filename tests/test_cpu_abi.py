@@ -42,12 +42,23 @@ def test_abi_version_and_workspace():
     assert lib.waam_workspace_bytes(1000) % 256 == 0
 
 
+def test_ctypes_struct_layouts_match_the_library():
+    lib = _native.lib()
+    for which, cls in enumerate((_native.WaamFields, _native.WaamStepParams,
+                                 _native.WaamMaterialTables)):
+        assert lib.waam_struct_size(which) == ctypes.sizeof(cls), cls.__name__
+    assert lib.waam_struct_size(3) == 0
+
+
 @pytest.mark.parametrize("call", [
     ("waam_clear_forces", (None, None, None, 10, None)),
     ("waam_stream", (None, None, None, 4, 4, 4, None)),
     ("waam_stream", (1, 1, 1, 0, 4, 4, None)),
     ("waam_update_phase", (None, 1, 1, 10, 1.0, 1.0, 1.0, 1.0, None)),
     ("waam_surface_height_at", (1, 1, 1, 4, 4, 4, 7, 0, 1, None)),
+    ("waam_refresh_thermal_properties", (1, 1, 1, 1, 1, 1, 10, None, 1.0, 1.0, 1.0, 1.0, 1.0,
+                                         1.0, 1.0, 1.0, 1.0, 1, None)),
+    ("waam_clamp_enthalpy_floor", (1, None, 1, 10, 300.0, None)),
 ])
 def test_invalid_arguments_are_rejected_on_the_host(call):
     name, args = call

@@ -24,7 +24,8 @@ def test_single_steps_match_reference(name, mode):
         torch.cuda.synchronize()
         got = tw.grid.state_dict()
         assert got["read_is_a"] == states[s + 1]["read_is_a"]
-        steps.compare_state("%s/%s step %d" % (name, mode, s), got, states[s + 1], reference=True)
+        steps.compare_state("%s/%s step %d" % (name, mode, s), got, states[s + 1],
+                            fields=steps.fields_for(name), reference=True)
 
 
 @pytest.mark.parametrize("name", steps.STEP_CASES)
@@ -40,12 +41,14 @@ def test_fused_matches_oracle_over_trajectory(name):
         tw.step(float(x), float(y), True)
         ot.step(float(x), float(y), True)
     torch.cuda.synchronize()
-    steps.compare_state("%s fused vs oracle" % name, tw.grid.state_dict(), ot.s)
+    steps.compare_state("%s fused vs oracle" % name, tw.grid.state_dict(), ot.s,
+                        fields=steps.fields_for(name))
 
 
-def _config_twins(kind, nx, ny, nz, **more):
+def _config_twins(kind, nx, ny, nz, material=None, **more):
     """A c1-like (Gaussian, no wire) or c2-like (Goldak, 100 Hz droplets, wetting,
-    CSF, hydrostatic) run from reset, on the GPU and on the oracle."""
+    CSF, hydrostatic) run from reset, on the GPU and on the oracle.  ``material``:
+    (MaterialProps, oracle constants, oracle tables) of steps.material_for."""
     from oracle.oracle_step import OracleTwin
     from waam_solver_b200 import WAAMTwin
     from waam_solver_b200.materials import from_constants
@@ -66,13 +69,21 @@ def _config_twins(kind, nx, ny, nz, **more):
         goldak = dict(ff=0.6, fr=1.4, a_front=5.0, a_rear=12.0, b=5.0, c=4.0)
     kw.update(more)
     mat = from_constants("m", steps.MATERIAL, contact_angle_deg=30.0)
+    omat, otables = steps.MATERIAL, None
+    if material is not None:
+        import dataclasses
+        mat, omat, otables = material
+        mat = dataclasses.replace(mat, contact_angle_deg=30.0)
+        omat = {k: v for k, v in omat.items() if k != "contact_angle_deg"}
     tw = WAAMTwin(material=mat, nx=nx, ny=ny, nz=nz, dx=dx, max_tracers=64, **kw)
     for k, v in host.items():
         setattr(tw, k, v)
     if goldak:
         tw.arc_source = Goldak3D(**goldak)
     tw.reset()
-    ot = OracleTwin(nx, ny, nz, dx, steps.MATERIAL, goldak=goldak, **kw, **host)
+    okw = {k: v for k, v in kw.items() if k != "step_mode"}
+    ot = OracleTwin(nx, ny, nz, dx, omat, goldak=goldak, tables=otables, contact_angle_deg=30.0,
+                    **okw, **host)
     ot.reset()
     return tw, ot, dx
 
@@ -190,3 +201,59 @@ def test_overlapped_step_matches_serial_stage_timing_path():
     for k, v in states[0].items():
         if isinstance(v, np.ndarray):
             assert np.array_equal(v, states[1][k]), k
+
+
+def _table_material():
+    """The validated ER70S-6 file as the reference loads it (tables + Sahoo)."""
+    sc, kw, states, positions = steps.load_step_case("t1_plate")
+    opt, extra = steps.driver_options("t1_plate", sc, kw)
+    return steps.material_for("t1_plate", extra)
+
+
+@pytest.mark.parametrize("variable_tau", [True, False])
+def test_table_path_matches_oracle_from_seeded_pool(variable_tau):
+    """Material tables on a c2-like run (droplets, wetting, CSF, heat losses,
+    substrate growth and trailing freeze): every step of the fused pipeline
+    against the oracle, property fields included; the variable-tau SRT or,
+    with use_variable_tau off, the MRT collision."""
+    shape = (40, 24, 24)
+    tw, ot, dx = _config_twins("c2", *shape, material=_table_material(),
+                               use_variable_tau=variable_tau, enable_heat_loss=True,
+                               enable_substrate_growth=True, enable_bead_freeze=True)
+    assert tw.use_material_tables and ot.use_tables
+    assert tw.H_sol == pytest.approx(ot.H_sol, rel=1e-14)
+    import state_gen
+    st = state_gen.seeded_state(*shape, seed=11, nz_solid=tw.nz_solid)
+    st["read_is_a"] = True
+    tw.grid.load_state({k: v for k, v in st.items() if k != "nz_solid"})
+    ot.load({k: v for k, v in st.items() if k != "nz_solid"})
+    tw._last_droplet_time = -1.0
+    ot.last_drop = -1.0
+    y = (shape[1] // 2) * dx
+    fields = steps.FIELDS + steps.PROP_FIELDS
+    for s in range(16):
+        x = 0.3 * shape[0] * dx + s * 0.008 * dx * 0.1
+        tw.step(x, y, True)
+        ot.step(x, y, True)
+        torch.cuda.synchronize()
+        steps.compare_state("tables step %d" % s, tw.grid.state_dict(), ot.s, fields=fields)
+    assert tw._n_droplets_fired == ot.n_drops >= 1
+
+
+def test_table_path_operators_equal_fused():
+    """The operator-by-operator table path and the fused pipeline agree."""
+    shape = (40, 24, 24)
+    out = []
+    for mode in ("operators", "fused"):
+        tw, ot, dx = _config_twins("c1", *shape, material=_table_material(),
+                                   enable_heat_loss=True, step_mode=mode)
+        import state_gen
+        st = state_gen.seeded_state(*shape, seed=12, nz_solid=tw.nz_solid)
+        st["read_is_a"] = True
+        tw.grid.load_state({k: v for k, v in st.items() if k != "nz_solid"})
+        for s in range(6):
+            tw.step(0.3 * shape[0] * dx + s * 1e-6, (shape[1] // 2) * dx, True)
+        torch.cuda.synchronize()
+        out.append(tw.grid.state_dict())
+    steps.compare_state("operators vs fused (tables)", out[0], out[1],
+                        fields=steps.FIELDS + steps.PROP_FIELDS)

@@ -22,8 +22,9 @@ def make_oracle(name):
     dx = opt.pop("dx")
     host = {k: v for k, v in extra.items() if k in ("wire_feed_m_s", "droplet_transfer_mode",
                                                     "pulse_frequency_hz", "droplet_size_jitter")}
-    ot = OracleTwin(sc["nx"], sc["ny"], sc["nz"], dx, steps.MATERIAL, goldak=extra.get("goldak"),
-                    **opt, **host)
+    _, mat, tables = steps.material_for(name, extra)
+    ot = OracleTwin(sc["nx"], sc["ny"], sc["nz"], dx, mat, goldak=extra.get("goldak"),
+                    tables=tables, **opt, **host)
     assert ot.nz_solid == sc["nz_solid"]
     return ot, sc, extra, states, positions
 
@@ -54,7 +55,8 @@ def test_oracle_single_steps_match_reference(name):
         x, y = positions[s]
         ot.step(x, y, True)
         assert ot.s["read_is_a"] == states[s + 1]["read_is_a"]
-        steps.compare_state("%s step %d" % (name, s), ot.s, states[s + 1], reference=True)
+        steps.compare_state("%s step %d" % (name, s), ot.s, states[s + 1],
+                            fields=steps.fields_for(name), reference=True)
 
 
 @pytest.mark.parametrize("name", steps.STEP_CASES)
@@ -65,4 +67,5 @@ def test_oracle_trajectory_matches_reference(name, monkeypatch):
     monkeypatch.setattr(cases, "RTOL", 1e-4)
     for s, (x, y) in enumerate(positions[: len(states) - 1]):
         ot.step(x, y, True)
-    steps.compare_state("%s trajectory" % name, ot.s, states[-1], reference=True)
+    steps.compare_state("%s trajectory" % name, ot.s, states[-1],
+                        fields=steps.fields_for(name), reference=True)

@@ -28,7 +28,20 @@ class WaamFields(C.Structure):
         "phi_tmp", "flags", "T_max", "T_prev", "dT_dt", "t800", "t1100", "tsol", "Fx", "Fy",
         "Fz", "step_scalars")] + [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                                   ("tracer_pos", C.c_void_p), ("tracer_active", C.c_void_p),
-                                  ("max_tracers", C.c_int)]
+                                  ("max_tracers", C.c_int)] + [
+        (name, C.c_void_p) for name in ("cp_rho_f", "alpha_f", "dgamma_f", "tau_f")]
+
+
+TABLE_KNOTS = 8
+
+
+class WaamMaterialTables(C.Structure):
+    """gpu_tables.py MaterialGPUTables as the C struct of the header."""
+    _fields_ = ([(name, C.c_float * TABLE_KNOTS) for name in (
+        "cp_T", "cp_V", "k_T", "k_V", "mu_T", "mu_V", "dgamma_T", "dgamma_V")] +
+        [(name, C.c_int32) for name in ("n_cp", "n_k", "n_mu", "n_dgamma")] +
+        [(name, C.c_float) for name in ("cp_fallback", "k_fallback", "mu_fallback",
+                                        "dgamma_fallback")])
 
 
 def _params_fields():
@@ -42,7 +55,7 @@ def _params_fields():
         if not decl:
             continue
         typ, names = decl.split(None, 1)
-        ctype = {"int": C.c_int, "float": C.c_float}[typ]
+        ctype = {"int": C.c_int, "float": C.c_float, "WaamMaterialTables": WaamMaterialTables}[typ]
         for nm in names.split(","):
             out.append((nm.strip(), ctype))
     return out
@@ -55,9 +68,10 @@ class WaamStepParams(C.Structure):
 _CTYPES = {
     "float*": C.c_void_p, "const float*": C.c_void_p, "int32_t*": C.c_void_p,
     "const int32_t*": C.c_void_p, "void*": C.c_void_p, "float": C.c_float, "int": C.c_int,
-    "int64_t": C.c_int64, "size_t": C.c_size_t, "double": C.c_double, "uint64_t": C.c_uint64, "const WaamFields*": C.POINTER(WaamFields),
+    "int64_t": C.c_int64, "size_t": C.c_size_t, "double": C.c_double, "uint64_t": C.c_uint64,
+    "const WaamFields*": C.POINTER(WaamFields),
     "const WaamStepParams*": C.POINTER(WaamStepParams), "const char*": C.c_char_p,
-    "void* const*": C.c_void_p,
+    "void* const*": C.c_void_p, "const WaamMaterialTables*": C.POINTER(WaamMaterialTables),
 }
 
 

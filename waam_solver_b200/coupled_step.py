@@ -28,10 +28,38 @@ T_1100 = 1100.0 + 273.15
 
 
 def _clamp_ceiling(twin, g):
-    if twin.enable_enthalpy_cap:
+    """solvers/coupled_step.py:17-31."""
+    if not twin.enable_enthalpy_cap:
+        return
+    if twin.use_material_tables:
+        thermal.clamp_enthalpy_ceiling_variable_cp(g.H, g.flags, g.cp_rho_field, twin.H_liq,
+                                                   twin.mat.T_liquidus, twin.T_vapor_cap_K,
+                                                   g.FLAG_GAS)
+    else:
         thermal.clamp_enthalpy_ceiling_scalar(g.H, g.flags, twin.cp_rho, twin.mat.T_solidus,
                                               twin.mat.T_liquidus, twin.T_vapor_cap_K, twin.L_rho,
                                               g.FLAG_GAS)
+
+
+def _update_phase(twin, g):
+    if twin.use_material_tables:
+        thermal.update_phase_variable_cp(g.H, g.T, g.f_l, g.cp_rho_field, twin.L_rho,
+                                         twin.mat.T_solidus, twin.mat.T_liquidus, twin.H_sol,
+                                         twin.H_liq)
+    else:
+        phase_change.update_phase(g.H, g.T, g.f_l, twin.cp_rho, twin.L_rho, twin.mat.T_solidus,
+                                  twin.mat.T_liquidus)
+
+
+def _refresh_properties(twin, g):
+    """solvers/coupled_step.py:168-181 (the knots travel by value, no device read)."""
+    t = twin.gpu_tables
+    thermal.refresh_properties(
+        g.T, g.cp_rho_field, g.alpha_lu_field, g.dgamma_lu_field, g.tau_field, t.cp_T, t.cp_V,
+        t.k_T, t.k_V, t.mu_T, t.mu_V, t.dgamma_T, t.dgamma_V, t.n_cp, t.n_k, t.n_mu, t.n_dgamma,
+        g.mat.rho, g.dt, g.dx, t.cp_fallback, t.k_fallback, t.mu_fallback, t.dgamma_fallback,
+        twin.force_scale / g.dx, twin.cp_rho, twin.alpha_lu, twin.dgamma_dT_lu, g.tau,
+        twin.marangoni_scale, 1, g.flags, g.FLAG_SOLID, g.FLAG_GAS)
 
 
 def _resolve_arc_k(twin, g, arc_i, arc_j, torch_z_m=None):
@@ -116,7 +144,7 @@ def _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m, device_retries=
 
 
 def coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
-    """The reference step, operator by operator (scalar-material path)."""
+    """The reference step, operator by operator (constants or table path)."""
     g = twin.grid
     arc_i = torch_x_m / g.dx
     arc_j = torch_y_m / g.dx
@@ -129,19 +157,29 @@ def coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=Non
         twin.arc_source.inject(twin, g, arc_i, arc_j, arc_k)
         _clamp_ceiling(twin, g)
         _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m)
-    thermal.advect_diffuse_temperature(g.H, g.T, g.ux, g.uy, g.uz, g.flags, twin.alpha_lu, 1.0,
-                                       g.FLAG_SOLID, g.FLAG_GAS, twin.cp_rho, g.nx, g.ny, g.nz)
+    tables = twin.use_material_tables
+    if tables:
+        _refresh_properties(twin, g)
+        thermal.advect_diffuse_variable(g.H, g.T, g.ux, g.uy, g.uz, g.flags, g.alpha_lu_field,
+                                        g.cp_rho_field, 1.0, g.FLAG_SOLID, g.FLAG_GAS, g.nx,
+                                        g.ny, g.nz)
+    else:
+        thermal.advect_diffuse_temperature(g.H, g.T, g.ux, g.uy, g.uz, g.flags, twin.alpha_lu,
+                                           1.0, g.FLAG_SOLID, g.FLAG_GAS, twin.cp_rho, g.nx,
+                                           g.ny, g.nz)
     if twin.enable_heat_loss:
         thermal.apply_boundary_losses(g.H, g.T, g.flags, twin.T_amb, twin.h_conv, twin.eps_rad,
                                       int(twin.enable_convection), int(twin.enable_radiation),
                                       twin.cp_rho, g.dt, g.dx, twin.sigma_sb, g.FLAG_SOLID,
                                       g.FLAG_GAS, g.nx, g.ny, g.nz)
-        thermal.clamp_enthalpy_floor_scalar(g.H, twin.cp_rho, g.flags, twin.T_amb, g.FLAG_GAS)
-    phase_change.update_phase(g.H, g.T, g.f_l, twin.cp_rho, twin.L_rho, twin.mat.T_solidus,
-                              twin.mat.T_liquidus)
+        if tables:
+            thermal.clamp_enthalpy_floor(g.H, g.cp_rho_field, g.flags, twin.T_amb, g.FLAG_GAS)
+        else:
+            thermal.clamp_enthalpy_floor_scalar(g.H, twin.cp_rho, g.flags, twin.T_amb,
+                                                g.FLAG_GAS)
+    _update_phase(twin, g)
     _clamp_ceiling(twin, g)
-    phase_change.update_phase(g.H, g.T, g.f_l, twin.cp_rho, twin.L_rho, twin.mat.T_solidus,
-                              twin.mat.T_liquidus)
+    _update_phase(twin, g)
     thermal.update_T_max(g.T, g.T_max, g.flags, g.FLAG_GAS)
     thermal.update_cooling_rate(g.T, g.T_prev, g.dT_dt, g.flags, g.dt, g.FLAG_GAS)
     if twin.enable_vof:
@@ -160,9 +198,14 @@ def coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=Non
         forces.compute_csf_tension(g.phi, g.flags, g.Fx, g.Fy, g.Fz, twin.gamma_lu, g.FLAG_SOLID,
                                    g.FLAG_GAS, g.nx, g.ny, g.nz,
                                    enable_wetting=twin.enable_wetting, theta_rad=twin.theta_rad)
-    forces.compute_marangoni_force(g.T, g.phi, g.f_l, g.Fx, g.Fy, g.Fz, g.flags,
-                                   twin.dgamma_dT_lu, g.dx, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny,
-                                   g.nz)
+    if tables:
+        forces.compute_marangoni_force_variable(g.T, g.phi, g.f_l, g.Fx, g.Fy, g.Fz, g.flags,
+                                                g.dgamma_lu_field, g.FLAG_SOLID, g.FLAG_GAS,
+                                                g.nx, g.ny, g.nz)
+    else:
+        forces.compute_marangoni_force(g.T, g.phi, g.f_l, g.Fx, g.Fy, g.Fz, g.flags,
+                                       twin.dgamma_dT_lu, g.dx, g.FLAG_SOLID, g.FLAG_GAS, g.nx,
+                                       g.ny, g.nz)
     if is_welding:
         weld_forces.apply_gas_shear(twin, g, arc_i, arc_j, arc_k)
         forces.apply_arc_pressure(g.Fz, g.flags, g.phi, arc_i, arc_j, arc_k, p_sigma, pressure,
@@ -180,7 +223,11 @@ def coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=Non
     if F_cap > 0.0:
         kernels.clamp_body_force_magnitude(g.Fx, g.Fy, g.Fz, g.flags, F_cap, g.FLAG_SOLID,
                                            g.FLAG_GAS)
-    if twin.use_srt:
+    if tables and twin.use_variable_tau:
+        lbm.collide_srt_variable_tau(g.f_src, g.f_dst, g.rho, g.ux, g.uy, g.uz, g.Fx, g.Fy, g.Fz,
+                                     g.f_l, g.flags, g.tau_field, twin.C_darcy, g.FLAG_SOLID,
+                                     g.FLAG_GAS, g.nx, g.ny, g.nz)
+    elif twin.use_srt:
         lbm.collide_srt(g.f_src, g.f_dst, g.rho, g.ux, g.uy, g.uz, g.Fx, g.Fy, g.Fz, g.f_l,
                         g.flags, g.tau, twin.omega, 1.0, twin.C_darcy, g.FLAG_SOLID, g.FLAG_GAS,
                         g.nx, g.ny, g.nz)
@@ -198,18 +245,29 @@ def coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=Non
                                 g.FLAG_GAS)
     kernels.snapshot_forces(g.Fx, g.Fy, g.Fz, g.Fx_snap, g.Fy_snap, g.Fz_snap)
     if twin.enable_substrate_growth or twin.enable_bead_freeze:
-        free_surface.remelt_hot_solid_scalar(g.T, g.H, g.f_l, g.phi, g.flags, twin.cp_rho,
-                                             twin.mat.T_solidus, twin.mat.T_liquidus, twin.L_rho,
-                                             g.FLAG_SOLID, g.FLAG_FLUID)
+        if tables:
+            free_surface.remelt_hot_solid(g.T, g.H, g.f_l, g.phi, g.flags, g.cp_rho_field,
+                                          twin.mat.T_solidus, twin.mat.T_liquidus, twin.L_rho,
+                                          g.FLAG_SOLID, g.FLAG_FLUID)
+        else:
+            free_surface.remelt_hot_solid_scalar(g.T, g.H, g.f_l, g.phi, g.flags, twin.cp_rho,
+                                                 twin.mat.T_solidus, twin.mat.T_liquidus,
+                                                 twin.L_rho, g.FLAG_SOLID, g.FLAG_FLUID)
         if is_welding and twin.enable_bead_freeze:
             dx_, dy_, dz_ = getattr(twin, "_torch_dir_xyz", (1.0, 0.0, 0.0))
             lookback = max(2.0, twin.trailing_solidify_lookback_mm / (g.dx * 1000.0))
             T_freeze = twin.mat.T_liquidus + twin.trailing_solidify_temp_margin_K
-            kernels.solidify_trailing_pool_scalar(g.T, g.H, g.f_l, g.phi, g.flags, g.ux, g.uy,
-                                                  g.uz, twin.cp_rho, arc_i, arc_j, arc_k, dx_,
-                                                  dy_, dz_, lookback, T_freeze,
-                                                  twin.mat.T_solidus, g.FLAG_SOLID, g.FLAG_FLUID,
-                                                  g.FLAG_GAS)
+            if tables:
+                kernels.solidify_trailing_pool(g.T, g.H, g.f_l, g.phi, g.flags, g.ux, g.uy, g.uz,
+                                               g.cp_rho_field, arc_i, arc_j, arc_k, dx_, dy_, dz_,
+                                               lookback, T_freeze, twin.mat.T_solidus,
+                                               g.FLAG_SOLID, g.FLAG_FLUID, g.FLAG_GAS)
+            else:
+                kernels.solidify_trailing_pool_scalar(g.T, g.H, g.f_l, g.phi, g.flags, g.ux,
+                                                      g.uy, g.uz, twin.cp_rho, arc_i, arc_j,
+                                                      arc_k, dx_, dy_, dz_, lookback, T_freeze,
+                                                      twin.mat.T_solidus, g.FLAG_SOLID,
+                                                      g.FLAG_FLUID, g.FLAG_GAS)
         free_surface.solidify_cooled_metal(g.T, g.f_l, g.phi, g.flags, g.ux, g.uy, g.uz,
                                            twin.mat.T_solidus, True, g.FLAG_SOLID, g.FLAG_FLUID,
                                            g.FLAG_GAS)
@@ -233,6 +291,8 @@ def _fields(g):
     if getattr(g, "_tracers_live", False):   # advected once the first droplet spawned some
         f.tracer_pos, f.tracer_active = g.porosity_pos.data_ptr(), g.porosity_active.data_ptr()
         f.max_tracers = g.max_tracers
+    f.cp_rho_f, f.alpha_f = g.cp_rho_field.data_ptr(), g.alpha_lu_field.data_ptr()
+    f.dgamma_f, f.tau_f = g.dgamma_lu_field.data_ptr(), g.tau_field.data_ptr()
     return f
 
 
@@ -282,6 +342,14 @@ def step_params(twin):
     p.lookback = max(2.0, twin.trailing_solidify_lookback_mm / (g.dx * 1000.0))
     p.T_freeze = m.T_liquidus + twin.trailing_solidify_temp_margin_K
     p.f_storage = g.population_storage
+    p.use_tables = 1 if twin.use_material_tables else 0
+    p.variable_tau = 1 if twin.use_variable_tau else 0
+    p.rho_mat = m.rho
+    p.force_scale_lu = twin.force_scale / g.dx
+    p.marangoni_scale = twin.marangoni_scale
+    p.H_sol_t, p.H_liq_t = twin.H_sol, twin.H_liq
+    p.tau_ref = g.tau
+    p.tables = twin.gpu_tables.struct
     return p
 
 

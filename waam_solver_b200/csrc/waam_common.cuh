@@ -14,6 +14,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include "../../include/waam_b200.h"
 #include "waam_expf.h"
 
 namespace waam {
@@ -197,6 +198,121 @@ __host__ inline PhaseParams make_phase(float cp_rho, float L_rho, float Ts, floa
     p.cap_s = cp_rho * T_cap;
     p.cap_enabled = cap_enabled;
     return p;
+}
+
+// ---- temperature-dependent material tables (kernels.py:1686-2010) ----
+
+// Constants of the property refresh (kernels.py:1710-1772): the values of
+// SOLID / GAS cells (and of every cell without tables) and the unit factors.
+struct TableConsts {
+    float rho, dt, dx, force_scale, marangoni_scale;
+    float cp_rho_ref, alpha_ref, dgamma_ref, tau_ref;
+    int use_tables;
+};
+
+// Phase constants of the table path (twin.py:271-273): H_sol, H_liq come
+// from cp(T_solidus), not from the per-cell rho*cp.
+struct VarPhase {
+    float H_sol, H_liq, L_rho, Ts, Tl, T_cap;
+};
+
+// kernels.py:1686-1707 lookup_table_1d: clamped to the end knots, linear
+// inside; where knots repeat, the last segment containing T wins.  Every
+// index is a compile-time constant, so the knots stay in parameter space.
+__device__ __forceinline__ float table_lookup(float T, const float (&t)[WAAM_TABLE_KNOTS],
+                                              const float (&v)[WAAM_TABLE_KNOTS], int n,
+                                              float fallback) {
+    float result = fallback;
+    if (n > 0) {
+        float t_last = t[0], v_last = v[0];
+#pragma unroll
+        for (int q = 1; q < WAAM_TABLE_KNOTS; ++q) {
+            if (q == n - 1) {
+                t_last = t[q];
+                v_last = v[q];
+            }
+        }
+        if (T <= t[0]) {
+            result = v[0];
+        } else if (T >= t_last) {
+            result = v_last;
+        } else {
+#pragma unroll
+            for (int idx = 0; idx < WAAM_TABLE_KNOTS - 1; ++idx) {
+                if (idx < n - 1) {
+                    const float t0 = t[idx], t1 = t[idx + 1];
+                    if (T >= t0 && T <= t1) {
+                        const float w = (T - t0) / (t1 - t0 + 1e-8f);
+                        result = v[idx] + w * (v[idx + 1] - v[idx]);
+                    }
+                }
+            }
+        }
+    }
+    return result;
+}
+
+struct CellProps {
+    float cp_rho, alpha, dgamma, tau;
+};
+
+// kernels.py:1710-1772 refresh_thermal_properties for one cell
+__device__ __forceinline__ CellProps refresh_cell(const WaamMaterialTables& tb,
+                                                  const TableConsts& k, int flag, float T) {
+    CellProps p;
+    if (flag == SOLID || flag == GAS) {
+        p.cp_rho = k.cp_rho_ref;
+        p.alpha = k.alpha_ref;
+        p.dgamma = k.dgamma_ref;
+        p.tau = k.tau_ref;
+    } else if (k.use_tables == 1) {
+        const float cp = table_lookup(T, tb.cp_T, tb.cp_V, tb.n_cp, tb.cp_fallback);
+        const float kv = table_lookup(T, tb.k_T, tb.k_V, tb.n_k, tb.k_fallback);
+        const float mu = table_lookup(T, tb.mu_T, tb.mu_V, tb.n_mu, tb.mu_fallback);
+        const float dg = table_lookup(T, tb.dgamma_T, tb.dgamma_V, tb.n_dgamma,
+                                      tb.dgamma_fallback);
+        const float alpha_phys = kv / (k.rho * cp + 1e-9f);
+        const float nu_phys = mu / (k.rho + 1e-9f);
+        const float nu_lu = nu_phys * k.dt / (k.dx * k.dx);
+        p.cp_rho = k.rho * cp;
+        p.alpha = alpha_phys * k.dt / (k.dx * k.dx);
+        p.dgamma = dg * k.force_scale * k.marangoni_scale;
+        p.tau = 3.0f * nu_lu + 0.5f;
+    } else {
+        p.cp_rho = k.cp_rho_ref;
+        p.alpha = k.alpha_ref;
+        p.dgamma = k.dgamma_ref * k.marangoni_scale;
+        p.tau = k.tau_ref;
+    }
+    return p;
+}
+
+// kernels.py:1988-2010 clamp_enthalpy_ceiling_variable_cp (one non-gas cell)
+__device__ __forceinline__ float cap_h_var(const VarPhase& p, float cp_r, float h) {
+    const float cap_l = p.H_liq + cp_r * (p.T_cap - p.Tl);
+    const float cap_s = cp_r * p.T_cap;
+    if (h > p.H_liq) {
+        if (h > cap_l) h = cap_l;
+    } else {
+        if (h > cap_s) h = cap_s;
+    }
+    return h;
+}
+
+// kernels.py:1839-1863 update_phase_variable_cp (one cell)
+__device__ __forceinline__ void phase_var(const VarPhase& p, float cp, float h, float& T,
+                                          float& fl) {
+    if (h <= p.H_sol) {
+        fl = 0.0f;
+        T = h / (cp + 1e-9f);
+    } else if (h >= p.H_liq) {
+        fl = 1.0f;
+        T = p.Tl + (h - p.H_liq) / (cp + 1e-9f);
+    } else {
+        const float f = (h - p.H_sol) / p.L_rho;
+        fl = f;
+        T = p.Ts + f * (p.Tl - p.Ts);
+    }
 }
 
 // kernels.py:1953-1984 clamp_enthalpy_ceiling_scalar (one cell, non-gas)

@@ -386,7 +386,9 @@ __global__ void __launch_bounds__(256) k_arc_inject_tiles(Dims d, float* __restr
                                                           const float* __restrict__ f_l,
                                                           ArcParams p, const float* scalars,
                                                           float arc_k_offset, int cap,
-                                                          PhaseParams ph) {
+                                                          PhaseParams ph,
+                                                          const float* __restrict__ cp_f,
+                                                          VarPhase vp) {
     int i, j, k, c;
     if (!tile_cell(d, i, j, k, c)) return;
     // the device scalars and the flag are requested together, then f_l and H
@@ -403,7 +405,9 @@ __global__ void __launch_bounds__(256) k_arc_inject_tiles(Dims d, float* __restr
     if (!hit && !cap) return;
     if (!cap) h = H[c];
     if (hit) h = h + dh;
-    if (cap) h = cap_h(ph, h);
+    // table path: the ceiling with the rho*cp fields of the previous step
+    // (kernels.py:1988-2010)
+    if (cap) h = cp_f ? cap_h_var(vp, cp_f[c], h) : cap_h(ph, h);
     H[c] = h;
 }
 
@@ -414,17 +418,34 @@ struct ThermalArgs {
     float T_amb, h_conv, eps_rad, dt_phys, dx, sigma_sb, h_floor;
 };
 
+// Table path of the thermal stage: the property refresh (kernels.py:1710-1772)
+// is computed per cell from T before the cell's own enthalpy update and
+// written to the property fields; the update uses the cell's rho*cp and alpha.
+struct TableArgs {
+    VarPhase vp;
+    TableConsts tc;
+    WaamMaterialTables tb;
+    float* cp_f;
+    float* alpha_f;
+    float* dg_f;
+    float* tau_f;
+};
+
 // Thermal stage for every cell: kernels.py:1611-1682 (advect/diffuse),
 // 2030-2082 + 1937-1950 (losses, floor), 1519-1556 twice around the ceiling
 // 1953-1984 (only the second update_phase is observable), 3016-3032 (T_max),
 // 2013-2027 (cooling rate).  H and T are double-buffered so neighbour reads
 // see the pre-stage values.  Also resets the active-cell shard counters of the step.
+// TABLES: refresh_thermal_properties, advect_diffuse_temperature_variable,
+// clamp_enthalpy_floor and update_phase_variable_cp / the variable ceiling
+// (kernels.py:1710-1863, 1922-1935, 1988-2010) instead of the scalar forms.
+template <bool TABLES>
 __global__ void __launch_bounds__(256) k_thermal_fused(
     Dims d, const float* __restrict__ H, float* __restrict__ H_next, const float* __restrict__ T,
     float* __restrict__ T_next, float* __restrict__ f_l, const float* __restrict__ ux,
     const float* __restrict__ uy, const float* __restrict__ uz, const int32_t* __restrict__ flags,
     float* __restrict__ T_max, float* __restrict__ T_prev, float* __restrict__ dT_dt,
-    unsigned* active_count, ThermalArgs a) {
+    unsigned* active_count, ThermalArgs a, TableArgs tba) {
     if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
         const int t = threadIdx.y * kTileK + threadIdx.x;
         if (t < kActiveShards) active_count[t] = 0u;
@@ -433,6 +454,14 @@ __global__ void __launch_bounds__(256) k_thermal_fused(
     if (!tile_cell(d, i, j, k, c)) return;
     const int flag = flags[c];
     float h = H[c];
+    CellProps pr{};
+    if (TABLES) {
+        pr = refresh_cell(tba.tb, tba.tc, flag, T[c]);
+        tba.cp_f[c] = pr.cp_rho;
+        tba.alpha_f[c] = pr.alpha;
+        tba.dg_f[c] = pr.dgamma;
+        tba.tau_f[c] = pr.tau;
+    }
     if (flag != GAS) {
         float u = 0.0f, v = 0.0f, w = 0.0f;
         if (flag != SOLID) {
@@ -440,7 +469,8 @@ __global__ void __launch_bounds__(256) k_thermal_fused(
             v = uy[c];
             w = uz[c];
         }
-        h = h + thermal_dh(d, H, T, flags, u, v, w, i, j, k, flag, h, a.cpa, a.dt_lu);
+        const float cpa = TABLES ? pr.cp_rho * pr.alpha : a.cpa;
+        h = h + thermal_dh(d, H, T, flags, u, v, w, i, j, k, flag, h, cpa, a.dt_lu);
         if (a.heat_loss) {
             int ne = 0;
             const int sx = d.ny * d.nz;
@@ -460,12 +490,16 @@ __global__ void __launch_bounds__(256) k_thermal_fused(
                 }
                 h -= q * (float)ne * a.dt_phys / a.dx;
             }
-            if (h < a.h_floor) h = a.h_floor;
+            const float h_floor = TABLES ? pr.cp_rho * a.T_amb : a.h_floor;
+            if (h < h_floor) h = h_floor;
         }
-        if (a.ph.cap_enabled) h = cap_h(a.ph, h);
+        if (a.ph.cap_enabled) h = TABLES ? cap_h_var(tba.vp, pr.cp_rho, h) : cap_h(a.ph, h);
     }
     float t, fl;
-    phase(a.ph, h, t, fl);
+    if (TABLES)
+        phase_var(tba.vp, pr.cp_rho, h, t, fl);
+    else
+        phase(a.ph, h, t, fl);
     H_next[c] = h;
     T_next[c] = t;
     f_l[c] = fl;
@@ -586,8 +620,10 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
 
 struct CollideArgs {
     ForceParams P;
-    int kind, from_buffer;
+    int kind, from_buffer;  // kind 0 MRT, 1 SRT, 2 SRT with the per-cell tau_f
     float omega, omega_b, C_darcy, u_cap;
+    const float* dgamma_f;  // non-null: Marangoni with the per-cell dgamma (table path)
+    const float* tau_f;
 };
 
 // Body forces + collision + Mach clamp over the active (FLUID/IFACE) cells
@@ -642,6 +678,8 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
         float f[19], o[19];
 #pragma unroll
         for (int q = 0; q < 19; ++q) f[q] = Pop<S>::get(f_src[q * n + c], q);
+        const float tau_c = a.kind == 2 ? a.tau_f[c] : 0.0f;
+        if (a.dgamma_f) P.dgamma = a.dgamma_f[c];
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
         if (a.from_buffer) {
             fx = Fx[c];
@@ -653,8 +691,9 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
         float rr, u, v, w;
         if (a.kind == 0)
             collide_mrt_cell(f, fl, fx, fy, fz, a.omega, a.omega_b, a.C_darcy, o, rr, u, v, w);
-        else
-            collide_srt_cell(f, fl, fx, fy, fz, a.omega, a.C_darcy, o, rr, u, v, w);
+        else  // kernels.py:2889-2965: omega = 1 / (tau + 1e-6) per cell
+            collide_srt_cell(f, fl, fx, fy, fz, a.kind == 2 ? 1.0f / (tau_c + 1e-6f) : a.omega,
+                             a.C_darcy, o, rr, u, v, w);
 #pragma unroll
         for (int q = 0; q < 19; ++q) f_dst[q * n + c] = Pop<S>::put(o[q], q);
         if (a.u_cap > 0.0f) clamp_mach(u, v, w, a.u_cap);
@@ -672,6 +711,7 @@ struct TailArgs {
     float cp_rho, Ts, Tl, L_rho;
     int remelt, trailing, cooled;
     float dir_x, dir_y, dir_z, lookback, T_freeze;
+    const float* cp_f;  // non-null: the per-cell rho*cp (kernels.py:2454-2570)
 };
 
 // solvers/coupled_step.py:426-458: remelt_hot_solid_scalar (kernels.py:2489),
@@ -686,11 +726,12 @@ __global__ void __launch_bounds__(256) k_tail(Dims d, float* T, float* H, float*
     if (a.remelt && flag == SOLID) {
         float Tc = T[c];
         if (!(Tc <= a.Ts + 5.0f)) {
-            float H_sol = a.cp_rho * a.Ts;
+            const float cp_rho = a.cp_f ? a.cp_f[c] : a.cp_rho;
+            float H_sol = cp_rho * a.Ts;
             float fl;
             if (Tc >= a.Tl) {
                 fl = 1.0f;
-                H[c] = a.cp_rho * a.Tl + a.L_rho + a.cp_rho * (Tc - a.Tl);
+                H[c] = cp_rho * a.Tl + a.L_rho + cp_rho * (Tc - a.Tl);
             } else {
                 fl = (Tc - a.Ts) / (a.Tl - a.Ts + 1e-6f);
                 H[c] = H_sol + fl * a.L_rho;
@@ -707,7 +748,7 @@ __global__ void __launch_bounds__(256) k_tail(Dims d, float* T, float* H, float*
         float dk = (float)k - arc_k;
         float proj = di * a.dir_x + dj * a.dir_y + dk * a.dir_z;
         if (!(proj > -a.lookback) && !(T[c] >= a.T_freeze)) {
-            H[c] = a.cp_rho * (a.Ts - 1.0f);
+            H[c] = (a.cp_f ? a.cp_f[c] : a.cp_rho) * (a.Ts - 1.0f);
             T[c] = a.Ts - 1.0f;
             f_l[c] = 0.0f;
             phi[c] = 1.0f;
@@ -781,6 +822,18 @@ static bool fields_ok(const WaamFields* f) {
            f->H != f->H_next && f->T != f->T_next;
 }
 
+static bool tables_fields_ok(const WaamFields* f, const WaamStepParams* p) {
+    if (!p->use_tables) return true;
+    const int32_t cnt[4] = {p->tables.n_cp, p->tables.n_k, p->tables.n_mu, p->tables.n_dgamma};
+    for (int q = 0; q < 4; ++q)
+        if (cnt[q] < 0 || cnt[q] > WAAM_TABLE_KNOTS) return false;
+    return f->cp_rho_f && f->alpha_f && f->dgamma_f && f->tau_f;
+}
+
+static VarPhase var_phase(const WaamStepParams* p) {
+    return VarPhase{p->H_sol_t, p->H_liq_t, p->L_rho, p->Ts, p->Tl, p->T_cap};
+}
+
 }  // namespace waam
 
 extern "C" {
@@ -797,6 +850,7 @@ int waam_step_launch_count(const WaamStepParams* p, int stage) {
 int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
                   size_t workspace_bytes, void* stream) {
     if (!fields_ok(f) || !p) return fail(WAAM_ERR_INVALID, "step_pre: bad fields or params");
+    if (!tables_fields_ok(f, p)) return fail(WAAM_ERR_INVALID, "step_pre: bad material tables");
     Dims d{f->nx, f->ny, f->nz};
     if (!workspace_ok(workspace, workspace_bytes, d.n()))
         return fail(WAAM_ERR_INVALID, "step_pre: workspace too small or misaligned");
@@ -817,7 +871,8 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     if (e) return e;
     PhaseParams ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
     k_arc_inject_tiles<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
-        d, f->H, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, p->cap_enabled, ph);
+        d, f->H, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, p->cap_enabled, ph,
+        p->use_tables ? f->cp_rho_f : nullptr, var_phase(p));
     return check_launch("k_arc_inject_tiles");
 }
 
@@ -830,6 +885,7 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
                           size_t workspace_bytes, void* const* events, int n_events,
                           void* stream) {
     if (!fields_ok(f) || !p) return fail(WAAM_ERR_INVALID, "step_main: bad fields or params");
+    if (!tables_fields_ok(f, p)) return fail(WAAM_ERR_INVALID, "step_main: bad material tables");
     if (p->f_storage < kStoreF32 || p->f_storage > kStoreBF16)
         return fail(WAAM_ERR_INVALID, "step_main: f_storage must be 0 (f32), 1 (f16) or 2 (bf16)");
     if (events && n_events < kMainEvents)
@@ -867,6 +923,17 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     ta.dx = p->dx;
     ta.sigma_sb = p->sigma_sb;
     ta.h_floor = p->cp_rho * p->T_amb;
+    TableArgs tba{};
+    if (p->use_tables) {
+        tba.vp = var_phase(p);
+        tba.tc = TableConsts{p->rho_mat, p->dt, p->dx, p->force_scale_lu, p->marangoni_scale,
+                             p->cp_rho, p->alpha_lu, p->dgamma_lu, p->tau_ref, 1};
+        tba.tb = p->tables;
+        tba.cp_f = f->cp_rho_f;
+        tba.alpha_f = f->alpha_f;
+        tba.dg_f = f->dgamma_f;
+        tba.tau_f = f->tau_f;
+    }
     // Without stage events, VOF advection (reads phi, u, flags; writes phi_tmp)
     // runs on a second stream beside the thermal stage (reads H, T, u, flags;
     // writes the thermal fields and f_l).
@@ -893,9 +960,14 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
         if (e) return e;
     }
     mark(0);
-    k_thermal_fused<<<tile_grid(d), tile_block(), 0, s>>>(
-        d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
-        f->T_prev, f->dT_dt, active_count, ta);
+    if (p->use_tables)
+        k_thermal_fused<true><<<tile_grid(d), tile_block(), 0, s>>>(
+            d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
+            f->T_prev, f->dT_dt, active_count, ta, tba);
+    else
+        k_thermal_fused<false><<<tile_grid(d), tile_block(), 0, s>>>(
+            d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
+            f->T_prev, f->dT_dt, active_count, ta, tba);
     e = check_launch("k_thermal_fused");
     if (e) return e;
     mark(1);
@@ -950,7 +1022,9 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     P.T_ref = p->T_ref;
     P.rho_ref = 1.0f;
     P.F_cap = p->F_cap;
-    cl.kind = p->collision;
+    cl.kind = p->use_tables && p->variable_tau ? 2 : p->collision;
+    cl.dgamma_f = p->use_tables ? f->dgamma_f : nullptr;
+    cl.tau_f = f->tau_f;
     cl.from_buffer = p->forces_from_buffer;
     cl.omega = p->omega;
     cl.omega_b = p->omega_b;
@@ -995,6 +1069,7 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
         t.dir_z = p->dir_z;
         t.lookback = p->lookback;
         t.T_freeze = p->T_freeze;
+        t.cp_f = p->use_tables ? f->cp_rho_f : nullptr;
         k_tail<<<tile_grid(d), tile_block(), 0, s>>>(d, f->T_next, f->H_next, f->f_l, f->phi,
                                                       f->flags, f->ux, f->uy, f->uz,
                                                       f->step_scalars, t);

@@ -214,9 +214,10 @@ __global__ void k_copy(float* dst, const float* src, int64_t n) {
     GRID_LOOP(c, n) { dst[c] = src[c]; }
 }
 
+// cp_f / alpha_f non-null: the cell's own rho*cp and alpha_lu (kernels.py:1775-1836)
 __global__ void k_thermal_op(Dims d, float* H, const float* Hs, const float* T, const float* ux,
                              const float* uy, const float* uz, const int32_t* flags, float cpa,
-                             float dt) {
+                             float dt, const float* cp_f, const float* alpha_f) {
     int64_t n = d.n();
     GRID_LOOP(c, n) {
         int flag = flags[c];
@@ -230,7 +231,8 @@ __global__ void k_thermal_op(Dims d, float* H, const float* Hs, const float* T, 
             v = uy[c];
             w = uz[c];
         }
-        float dH = thermal_dh(d, Hs, T, flags, u, v, w, i, j, k, flag, Hc, cpa, dt);
+        const float cpa_c = cp_f ? cp_f[c] * alpha_f[c] : cpa;
+        float dH = thermal_dh(d, Hs, T, flags, u, v, w, i, j, k, flag, Hc, cpa_c, dt);
         H[c] = Hc + dH;
     }
 }
@@ -307,6 +309,46 @@ __global__ void k_floor(float* H, float h_min, const int32_t* flags, int64_t n) 
     }
 }
 
+__global__ void k_floor_var(float* H, const float* cp_f, const int32_t* flags, int64_t n,
+                            float T_floor) {
+    GRID_LOOP(c, n) {
+        if (flags[c] == GAS) continue;
+        const float h_min = cp_f[c] * T_floor;
+        if (H[c] < h_min) H[c] = h_min;
+    }
+}
+
+__global__ void k_refresh(const float* T, float* cp_f, float* alpha_f, float* dg_f, float* tau_f,
+                          const int32_t* flags, int64_t n, WaamMaterialTables tb, TableConsts k) {
+    GRID_LOOP(c, n) {
+        const CellProps p = refresh_cell(tb, k, flags[c], T[c]);
+        cp_f[c] = p.cp_rho;
+        alpha_f[c] = p.alpha;
+        dg_f[c] = p.dgamma;
+        tau_f[c] = p.tau;
+    }
+}
+
+__global__ void k_phase_var(const float* H, float* T, float* f_l, const float* cp_f, int64_t n,
+                            VarPhase vp) {
+    GRID_LOOP(c, n) {
+        float t, fl;
+        phase_var(vp, cp_f[c], H[c], t, fl);
+        f_l[c] = fl;
+        T[c] = t;
+    }
+}
+
+__global__ void k_ceiling_var(float* H, const int32_t* flags, const float* cp_f, int64_t n,
+                              VarPhase vp) {
+    GRID_LOOP(c, n) {
+        if (flags[c] == GAS) continue;
+        const float h = H[c];
+        const float h2 = cap_h_var(vp, cp_f[c], h);
+        if (h2 != h) H[c] = h2;
+    }
+}
+
 __global__ void k_advect_phi(Dims d, float* phi_dst, const float* phi, const float* ux,
                              const float* uy, const float* uz, const int32_t* flags) {
     int64_t n = d.n();
@@ -359,8 +401,10 @@ __global__ void k_csf(Dims d, const float* phi, const int32_t* flags, float* Fx,
     }
 }
 
+// dg_f non-null: the cell's own dgamma (kernels.py:2221-2269)
 __global__ void k_marangoni(Dims d, const float* T, const float* phi, const float* f_l, float* Fx,
-                            float* Fy, float* Fz, const int32_t* flags, float dgamma) {
+                            float* Fy, float* Fz, const int32_t* flags, float dgamma,
+                            const float* dg_f) {
     int64_t n = d.n();
     GRID_LOOP(c, n) {
         int flag = flags[c];
@@ -383,7 +427,7 @@ __global__ void k_marangoni(Dims d, const float* T, const float* phi, const floa
         float tz = 0.5f * (T[d.idx(i, j, kp)] - T[d.idx(i, j, km)]);
         float nd = nxn * tx + nyn * ty + nzn * tz;
         float sx = tx - nd * nxn, sy = ty - nd * nyn, sz = tz - nd * nzn;
-        float scale = dgamma * g;
+        float scale = (dg_f ? dg_f[c] : dgamma) * g;
         Fx[c] += scale * sx;
         Fy[c] += scale * sy;
         Fz[c] += scale * sz;
@@ -447,7 +491,7 @@ template <int KIND>
 __global__ void k_collide(const float* __restrict__ f_src, float* __restrict__ f_dst, float* rho,
                           float* ux, float* uy, float* uz, const float* Fx, const float* Fy,
                           const float* Fz, const float* f_l, const int32_t* flags, int64_t n,
-                          float omega_s, float omega_b, float C_darcy) {
+                          float omega_s, float omega_b, float C_darcy, const float* tau_f) {
     GRID_LOOP(c, n) {
         int flag = flags[c];
         if (flag == SOLID || flag == GAS) continue;
@@ -459,7 +503,9 @@ __global__ void k_collide(const float* __restrict__ f_src, float* __restrict__ f
             collide_mrt_cell(f, f_l[c], Fx[c], Fy[c], Fz[c], omega_s, omega_b, C_darcy, o, r, u, v,
                              w);
         else
-            collide_srt_cell(f, f_l[c], Fx[c], Fy[c], Fz[c], omega_s, C_darcy, o, r, u, v, w);
+            // tau_f non-null: omega = 1 / (tau + 1e-6) per cell (kernels.py:2889-2965)
+            collide_srt_cell(f, f_l[c], Fx[c], Fy[c], Fz[c],
+                             tau_f ? 1.0f / (tau_f[c] + 1e-6f) : omega_s, C_darcy, o, r, u, v, w);
 #pragma unroll
         for (int q = 0; q < 19; ++q) f_dst[q * n + c] = o[q];
         rho[c] = r;
@@ -505,12 +551,14 @@ __global__ void k_snapshot(const float* Fx, const float* Fy, const float* Fz, fl
     }
 }
 
+// cp_f non-null: the cell's own rho*cp (kernels.py:2454-2485)
 __global__ void k_remelt(const float* T, float* H, float* f_l, float* phi, int32_t* flags, int64_t n,
-                         float cp_rho, float Ts, float Tl, float L_rho) {
+                         float cp_rho_c, float Ts, float Tl, float L_rho, const float* cp_f) {
     GRID_LOOP(c, n) {
         if (flags[c] != SOLID) continue;
         float Tc = T[c];
         if (Tc <= Ts + 5.0f) continue;
+        const float cp_rho = cp_f ? cp_f[c] : cp_rho_c;
         float H_sol = cp_rho * Ts;
         float fl;
         if (Tc >= Tl) {
@@ -529,7 +577,7 @@ __global__ void k_remelt(const float* T, float* H, float* f_l, float* phi, int32
 __global__ void k_trailing(Dims d, float* T, float* H, float* f_l, float* phi, int32_t* flags,
                            float* ux, float* uy, float* uz, float cp_rho, float arc_i, float arc_j,
                            float arc_k, float dir_x, float dir_y, float dir_z, float lookback,
-                           float T_freeze, float Ts) {
+                           float T_freeze, float Ts, const float* cp_f) {
     int64_t n = d.n();
     GRID_LOOP(c, n) {
         if (flags[c] == GAS) continue;
@@ -540,7 +588,8 @@ __global__ void k_trailing(Dims d, float* T, float* H, float* f_l, float* phi, i
         float proj = di * dir_x + dj * dir_y + dk * dir_z;
         if (proj > -lookback) continue;
         if (T[c] >= T_freeze) continue;
-        H[c] = cp_rho * (Ts - 1.0f);
+        // cp_f non-null: the cell's own rho*cp (kernels.py:2524-2570)
+        H[c] = (cp_f ? cp_f[c] : cp_rho) * (Ts - 1.0f);
         T[c] = Ts - 1.0f;
         f_l[c] = 0.0f;
         phi[c] = 1.0f;
@@ -651,6 +700,15 @@ int waam_abi_version(void) { return 1; }
 
 size_t waam_workspace_bytes(int64_t n) { return waam::ws_total_bytes(n); }
 
+size_t waam_struct_size(int which) {
+    switch (which) {
+        case 0: return sizeof(WaamFields);
+        case 1: return sizeof(WaamStepParams);
+        case 2: return sizeof(WaamMaterialTables);
+        default: return 0;
+    }
+}
+
 int waam_init_grid(float* f, float* rho, float* ux, float* uy, float* uz, float* T, float* H,
                    float* f_l, float* phi, int32_t* flags, int nx, int ny, int nz, float T_amb,
                    float rho0, float cp_rho, int nz_solid, int pi0, int pi1, int pj0, int pj1,
@@ -747,7 +805,8 @@ int waam_advect_diffuse_temperature(float* H, const float* T, const float* ux, c
     int e = waam::check_launch("k_copy");
     if (e) return e;
     float cpa = cp_rho * alpha_lu;
-    k_thermal_op<<<b, kThreads, 0, STREAM(stream)>>>(d, H, Hs, T, ux, uy, uz, flags, cpa, dt);
+    k_thermal_op<<<b, kThreads, 0, STREAM(stream)>>>(d, H, Hs, T, ux, uy, uz, flags, cpa, dt,
+                                                     nullptr, nullptr);
     return waam::check_launch("k_thermal_op");
 }
 
@@ -851,7 +910,7 @@ int waam_compute_marangoni_force(const float* T, const float* phi, const float* 
     REQUIRE(dims_ok(nx, ny, nz), "marangoni: bad dims");
     REQUIRE(T && phi && f_l && Fx && Fy && Fz && flags, "marangoni: null field");
     Dims d{nx, ny, nz};
-    EW(k_marangoni, d.n(), stream, d, T, phi, f_l, Fx, Fy, Fz, flags, dgamma);
+    EW(k_marangoni, d.n(), stream, d, T, phi, f_l, Fx, Fy, Fz, flags, dgamma, nullptr);
 }
 
 int waam_apply_arc_pressure(float* Fz, const int32_t* flags, const float* phi, int nx, int ny,
@@ -892,7 +951,7 @@ int waam_collide_mrt(const float* f_src, float* f_dst, float* rho, float* ux, fl
             "collide_mrt: null field");
     REQUIRE(f_src != f_dst, "collide_mrt: f_src must not alias f_dst");
     EW(k_collide<0>, n, stream, f_src, f_dst, rho, ux, uy, uz, Fx, Fy, Fz, f_l, flags, n, omega_s,
-       omega_b, C_darcy);
+       omega_b, C_darcy, nullptr);
 }
 
 int waam_collide_srt(const float* f_src, float* f_dst, float* rho, float* ux, float* uy, float* uz,
@@ -902,7 +961,7 @@ int waam_collide_srt(const float* f_src, float* f_dst, float* rho, float* ux, fl
             "collide_srt: null field");
     REQUIRE(f_src != f_dst, "collide_srt: f_src must not alias f_dst");
     EW(k_collide<1>, n, stream, f_src, f_dst, rho, ux, uy, uz, Fx, Fy, Fz, f_l, flags, n, omega,
-       0.0f, C_darcy);
+       0.0f, C_darcy, nullptr);
 }
 
 int waam_clamp_velocity_mach(float* ux, float* uy, float* uz, const int32_t* flags, int64_t n,
@@ -936,7 +995,7 @@ int waam_remelt_hot_solid_scalar(const float* T, float* H, float* f_l, float* ph
                                  int64_t n, float cp_rho, float Ts, float Tl, float L_rho,
                                  void* stream) {
     REQUIRE(T && H && f_l && phi && flags, "remelt: null field");
-    EW(k_remelt, n, stream, T, H, f_l, phi, flags, n, cp_rho, Ts, Tl, L_rho);
+    EW(k_remelt, n, stream, T, H, f_l, phi, flags, n, cp_rho, Ts, Tl, L_rho, nullptr);
 }
 
 int waam_solidify_trailing_pool_scalar(float* T, float* H, float* f_l, float* phi, int32_t* flags,
@@ -948,7 +1007,116 @@ int waam_solidify_trailing_pool_scalar(float* T, float* H, float* f_l, float* ph
     REQUIRE(T && H && f_l && phi && flags && ux && uy && uz, "trailing: null field");
     Dims d{nx, ny, nz};
     EW(k_trailing, d.n(), stream, d, T, H, f_l, phi, flags, ux, uy, uz, cp_rho, arc_i, arc_j, arc_k,
-       dir_x, dir_y, dir_z, lookback, T_freeze, Ts);
+       dir_x, dir_y, dir_z, lookback, T_freeze, Ts, nullptr);
+}
+
+static bool tables_ok(const WaamMaterialTables* t) {
+    const int32_t cnt[4] = {t->n_cp, t->n_k, t->n_mu, t->n_dgamma};
+    for (int q = 0; q < 4; ++q)
+        if (cnt[q] < 0 || cnt[q] > WAAM_TABLE_KNOTS) return false;
+    return true;
+}
+
+int waam_refresh_thermal_properties(const float* T, float* cp_rho_f, float* alpha_f,
+                                    float* dgamma_f, float* tau_f, const int32_t* flags, int64_t n,
+                                    const WaamMaterialTables* tables, float rho, float dt,
+                                    float dx, float force_scale, float cp_rho_ref,
+                                    float alpha_lu_ref, float dgamma_lu_ref, float tau_ref,
+                                    float marangoni_scale, int use_tables, void* stream) {
+    REQUIRE(T && cp_rho_f && alpha_f && dgamma_f && tau_f && flags, "refresh: null field");
+    REQUIRE(use_tables != 1 || (tables && tables_ok(tables)), "refresh: bad tables");
+    WaamMaterialTables tb{};
+    if (tables) tb = *tables;
+    TableConsts k{rho, dt, dx, force_scale, marangoni_scale, cp_rho_ref, alpha_lu_ref,
+                  dgamma_lu_ref, tau_ref, use_tables};
+    EW(k_refresh, n, stream, T, cp_rho_f, alpha_f, dgamma_f, tau_f, flags, n, tb, k);
+}
+
+int waam_advect_diffuse_temperature_variable(float* H, const float* T, const float* ux,
+                                             const float* uy, const float* uz,
+                                             const int32_t* flags, const float* alpha_f,
+                                             const float* cp_rho_f, int nx, int ny, int nz,
+                                             float dt, void* workspace, size_t workspace_bytes,
+                                             void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "thermal_variable: bad dims");
+    REQUIRE(H && T && ux && uy && uz && flags && alpha_f && cp_rho_f,
+            "thermal_variable: null field");
+    Dims d{nx, ny, nz};
+    REQUIRE(waam::workspace_ok(workspace, workspace_bytes, d.n()),
+            "thermal_variable: workspace too small");
+    float* Hs = Workspace::at(workspace).field;
+    int b = waam::elem_blocks(d.n());
+    k_copy<<<b, kThreads, 0, STREAM(stream)>>>(Hs, H, d.n());
+    int e = waam::check_launch("k_copy");
+    if (e) return e;
+    k_thermal_op<<<b, kThreads, 0, STREAM(stream)>>>(d, H, Hs, T, ux, uy, uz, flags, 0.0f, dt,
+                                                     cp_rho_f, alpha_f);
+    return waam::check_launch("k_thermal_op");
+}
+
+int waam_update_phase_variable_cp(const float* H, float* T, float* f_l, const float* cp_rho_f,
+                                  int64_t n, float L_rho, float T_solidus, float T_liquidus,
+                                  float H_sol, float H_liq, void* stream) {
+    REQUIRE(H && T && f_l && cp_rho_f, "phase_variable: null field");
+    VarPhase vp{H_sol, H_liq, L_rho, T_solidus, T_liquidus, 0.0f};
+    EW(k_phase_var, n, stream, H, T, f_l, cp_rho_f, n, vp);
+}
+
+int waam_clamp_enthalpy_ceiling_variable_cp(float* H, const int32_t* flags, const float* cp_rho_f,
+                                            int64_t n, float H_liq, float T_liquidus,
+                                            float T_cap, void* stream) {
+    REQUIRE(H && flags && cp_rho_f, "ceiling_variable: null field");
+    VarPhase vp{0.0f, H_liq, 0.0f, 0.0f, T_liquidus, T_cap};
+    EW(k_ceiling_var, n, stream, H, flags, cp_rho_f, n, vp);
+}
+
+int waam_clamp_enthalpy_floor(float* H, const float* cp_rho_f, const int32_t* flags, int64_t n,
+                              float T_floor, void* stream) {
+    REQUIRE(H && cp_rho_f && flags, "floor: null field");
+    EW(k_floor_var, n, stream, H, cp_rho_f, flags, n, T_floor);
+}
+
+int waam_compute_marangoni_force_variable(const float* T, const float* phi, const float* f_l,
+                                          float* Fx, float* Fy, float* Fz, const int32_t* flags,
+                                          const float* dgamma_f, int nx, int ny, int nz,
+                                          void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "marangoni_variable: bad dims");
+    REQUIRE(T && phi && f_l && Fx && Fy && Fz && flags && dgamma_f,
+            "marangoni_variable: null field");
+    Dims d{nx, ny, nz};
+    EW(k_marangoni, d.n(), stream, d, T, phi, f_l, Fx, Fy, Fz, flags, 0.0f, dgamma_f);
+}
+
+int waam_collide_srt_variable_tau(const float* f_src, float* f_dst, float* rho, float* ux,
+                                  float* uy, float* uz, const float* Fx, const float* Fy,
+                                  const float* Fz, const float* f_l, const int32_t* flags,
+                                  const float* tau_f, int64_t n, float C_darcy, void* stream) {
+    REQUIRE(f_src && f_dst && rho && ux && uy && uz && Fx && Fy && Fz && f_l && flags && tau_f,
+            "collide_srt_variable_tau: null field");
+    REQUIRE(f_src != f_dst, "collide_srt_variable_tau: f_src must not alias f_dst");
+    EW(k_collide<1>, n, stream, f_src, f_dst, rho, ux, uy, uz, Fx, Fy, Fz, f_l, flags, n, 0.0f,
+       0.0f, C_darcy, tau_f);
+}
+
+int waam_remelt_hot_solid(float* T, float* H, float* f_l, float* phi, int32_t* flags,
+                          const float* cp_rho_f, int64_t n, float T_solidus, float T_liquidus,
+                          float L_rho, void* stream) {
+    REQUIRE(T && H && f_l && phi && flags && cp_rho_f, "remelt: null field");
+    EW(k_remelt, n, stream, T, H, f_l, phi, flags, n, 0.0f, T_solidus, T_liquidus, L_rho,
+       cp_rho_f);
+}
+
+int waam_solidify_trailing_pool(float* T, float* H, float* f_l, float* phi, int32_t* flags,
+                                float* ux, float* uy, float* uz, const float* cp_rho_f, int nx,
+                                int ny, int nz, float arc_i, float arc_j, float arc_k, float dir_x,
+                                float dir_y, float dir_z, float lookback, float T_freeze,
+                                float T_solidus, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "trailing: bad dims");
+    REQUIRE(T && H && f_l && phi && flags && ux && uy && uz && cp_rho_f,
+            "trailing: null field");
+    Dims d{nx, ny, nz};
+    EW(k_trailing, d.n(), stream, d, T, H, f_l, phi, flags, ux, uy, uz, 0.0f, arc_i, arc_j, arc_k,
+       dir_x, dir_y, dir_z, lookback, T_freeze, T_solidus, cp_rho_f);
 }
 
 int waam_solidify_cooled_metal(const float* T, float* f_l, float* phi, int32_t* flags, float* ux,

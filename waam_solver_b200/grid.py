@@ -250,7 +250,8 @@ class WAAMGrid:
         """Host copies of every field of the state (for checkpoints and tests)."""
         names = ["rho", "T", "H", "T_max", "f_l", "phi", "dT_dt", "T_prev", "time_above_800_s",
                  "time_above_1100_s", "time_above_solidus_s", "ux", "uy", "uz", "Fx", "Fy",
-                 "Fz", "flags", "f_a", "f_b"]
+                 "Fz", "flags", "f_a", "f_b", "cp_rho_field", "alpha_lu_field",
+                 "dgamma_lu_field", "tau_field"]
         out = {}
         for k in names:
             t = getattr(self, k)

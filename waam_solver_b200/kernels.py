@@ -270,6 +270,133 @@ def apply_thermal_boundary_losses(H, T, flags, T_amb, h_conv, eps_rad, enable_co
           int(enable_rad), float(dt), float(dx), float(sigma_sb), _stream())
 
 
+def apply_thermal_boundary_losses_variable(H, T, flags, cp_rho_field, T_amb, h_conv, eps_rad,
+                                           enable_conv, enable_rad, dt, dx, sigma_sb, FLAG_SOLID,
+                                           FLAG_GAS, nx, ny, nz):
+    """kernels.py:1867-1918: the same loss as apply_thermal_boundary_losses (the
+    q*dt/dx update does not use rho*cp); cp_rho_field is accepted and unused."""
+    apply_thermal_boundary_losses(H, T, flags, T_amb, h_conv, eps_rad, enable_conv, enable_rad,
+                                  0.0, dt, dx, sigma_sb, FLAG_SOLID, FLAG_GAS, nx, ny, nz)
+
+
+# ------------------------------------------------------ material tables ----
+def _host_knots(a):
+    if isinstance(a, torch.Tensor):
+        a = a.detach().cpu()
+    return [float(v) for v in list(a)[:_native.TABLE_KNOTS]]
+
+
+def material_tables_struct(cp_T, cp_V, k_T, k_V, mu_T, mu_V, dgamma_T, dgamma_V, n_cp, n_k, n_mu,
+                           n_dgamma, cp_fallback, k_fallback, mu_fallback, dgamma_fallback):
+    """WaamMaterialTables from knot arrays (lists, numpy arrays or tensors of up
+    to 8 values) and counts (ints or 0-d tensors)."""
+    tb = _native.WaamMaterialTables()
+    for name, arr in (("cp_T", cp_T), ("cp_V", cp_V), ("k_T", k_T), ("k_V", k_V),
+                      ("mu_T", mu_T), ("mu_V", mu_V), ("dgamma_T", dgamma_T),
+                      ("dgamma_V", dgamma_V)):
+        vals = _host_knots(arr)
+        dst = getattr(tb, name)
+        for q, v in enumerate(vals):
+            dst[q] = v
+    for name, v in (("n_cp", n_cp), ("n_k", n_k), ("n_mu", n_mu), ("n_dgamma", n_dgamma)):
+        v = int(v.item() if isinstance(v, torch.Tensor) else v)
+        if not 0 <= v <= _native.TABLE_KNOTS:
+            raise WaamError("%s=%d outside [0, %d]" % (name, v, _native.TABLE_KNOTS))
+        setattr(tb, name, v)
+    tb.cp_fallback, tb.k_fallback = float(cp_fallback), float(k_fallback)
+    tb.mu_fallback, tb.dgamma_fallback = float(mu_fallback), float(dgamma_fallback)
+    return tb
+
+
+def refresh_thermal_properties(T, cp_rho_field, alpha_lu_field, dgamma_lu_field, tau_field, cp_T,
+                               cp_V, k_T, k_V, mu_T, mu_V, dgamma_T, dgamma_V, n_cp, n_k, n_mu,
+                               n_dgamma, rho, dt, dx, cp_fallback, k_fallback, mu_fallback,
+                               dgamma_fallback, force_scale, cp_rho_ref, alpha_lu_ref,
+                               dgamma_lu_ref, tau_ref, marangoni_scale, use_tables, flags,
+                               FLAG_SOLID, FLAG_GAS):
+    """kernels.py:1710-1772.  The knots are read on the host (pass host arrays or
+    a MaterialGPUTables' attributes to keep the call free of device reads)."""
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = T.numel()
+    tb = material_tables_struct(cp_T, cp_V, k_T, k_V, mu_T, mu_V, dgamma_T, dgamma_V, n_cp, n_k,
+                                n_mu, n_dgamma, cp_fallback, k_fallback, mu_fallback,
+                                dgamma_fallback)
+    _call("waam_refresh_thermal_properties", _f(T, n), _f(cp_rho_field, n), _f(alpha_lu_field, n),
+          _f(dgamma_lu_field, n), _f(tau_field, n), _i(flags, n), n, ctypes.byref(tb),
+          float(rho), float(dt), float(dx), float(force_scale), float(cp_rho_ref),
+          float(alpha_lu_ref), float(dgamma_lu_ref), float(tau_ref), float(marangoni_scale),
+          int(use_tables), _stream())
+
+
+def advect_diffuse_temperature_variable(H, T, ux, uy, uz, flags, alpha_lu_field, cp_rho_field, dt,
+                                        FLAG_SOLID, FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    ws, wsb = workspace_for(H)
+    _call("waam_advect_diffuse_temperature_variable", _f(H, n), _f(T, n), _f(ux, n), _f(uy, n),
+          _f(uz, n), _i(flags, n), _f(alpha_lu_field, n), _f(cp_rho_field, n), int(nx), int(ny),
+          int(nz), float(dt), ws, wsb, _stream())
+
+
+def update_phase_variable_cp(H, T, f_l, cp_rho_field, L_rho, T_solidus, T_liquidus, H_sol, H_liq):
+    n = H.numel()
+    _call("waam_update_phase_variable_cp", _f(H, n), _f(T, n), _f(f_l, n), _f(cp_rho_field, n), n,
+          float(L_rho), float(T_solidus), float(T_liquidus), float(H_sol), float(H_liq), _stream())
+
+
+def clamp_enthalpy_ceiling_variable_cp(H, flags, cp_rho_field, H_liq, T_liquidus, T_vapor_cap,
+                                       FLAG_GAS):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = H.numel()
+    _call("waam_clamp_enthalpy_ceiling_variable_cp", _f(H, n), _i(flags, n), _f(cp_rho_field, n),
+          n, float(H_liq), float(T_liquidus), float(T_vapor_cap), _stream())
+
+
+def clamp_enthalpy_floor(H, cp_rho_field, flags, T_floor, FLAG_GAS):
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = H.numel()
+    _call("waam_clamp_enthalpy_floor", _f(H, n), _f(cp_rho_field, n), _i(flags, n), n,
+          float(T_floor), _stream())
+
+
+def compute_marangoni_force_variable(T, phi, f_l, Fx, Fy, Fz, flags, dgamma_lu_field, FLAG_SOLID,
+                                     FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_compute_marangoni_force_variable", _f(T, n), _f(phi, n), _f(f_l, n), _f(Fx, n),
+          _f(Fy, n), _f(Fz, n), _i(flags, n), _f(dgamma_lu_field, n), int(nx), int(ny), int(nz),
+          _stream())
+
+
+def remelt_hot_solid(T, H, f_l, phi, flags, cp_rho_field, T_solidus, T_liquidus, L_rho,
+                     FLAG_SOLID, FLAG_FLUID):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_FLUID=FLAG_FLUID)
+    n = T.numel()
+    _call("waam_remelt_hot_solid", _f(T, n), _f(H, n), _f(f_l, n), _f(phi, n), _i(flags, n),
+          _f(cp_rho_field, n), n, float(T_solidus), float(T_liquidus), float(L_rho), _stream())
+
+
+def solidify_trailing_pool(T, H, f_l, phi, flags, ux, uy, uz, cp_rho_field, arc_i, arc_j, arc_k,
+                           dir_x, dir_y, dir_z, lookback_cells, T_freeze, T_solidus, FLAG_SOLID,
+                           FLAG_FLUID, FLAG_GAS):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_FLUID=FLAG_FLUID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(T)
+    n = T.numel()
+    _call("waam_solidify_trailing_pool", _f(T, n), _f(H, n), _f(f_l, n), _f(phi, n), _i(flags, n),
+          _f(ux, n), _f(uy, n), _f(uz, n), _f(cp_rho_field, n), nx, ny, nz, float(arc_i),
+          float(arc_j), float(arc_k), float(dir_x), float(dir_y), float(dir_z),
+          float(lookback_cells), float(T_freeze), float(T_solidus), _stream())
+
+
+def collide_srt_variable_tau(f_src, f_dst, rho, ux, uy, uz, Fx, Fy, Fz, f_l, flags, tau_field,
+                             C_darcy, FLAG_SOLID, FLAG_GAS, nx, ny, nz):
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_collide_srt_variable_tau", _f(f_src, 19 * n), _f(f_dst, 19 * n), _f(rho, n),
+          _f(ux, n), _f(uy, n), _f(uz, n), _f(Fx, n), _f(Fy, n), _f(Fz, n), _f(f_l, n),
+          _i(flags, n), _f(tau_field, n), n, float(C_darcy), _stream())
+
+
 def update_time_above_T(T, flags, time_above_800, time_above_1100, time_above_solidus, dt, T_800,
                         T_1100, T_solidus, FLAG_GAS):
     _flags_ok(FLAG_GAS=FLAG_GAS)

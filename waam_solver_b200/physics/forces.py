@@ -3,6 +3,7 @@ from .. import kernels
 
 clear_forces = kernels.clear_forces
 compute_marangoni_force = kernels.compute_marangoni_force
+compute_marangoni_force_variable = kernels.compute_marangoni_force_variable
 compute_csf_wetting = kernels.compute_csf_wetting
 add_buoyancy = kernels.add_buoyancy
 add_hydrostatic_gravity = kernels.add_hydrostatic_gravity
@@ -17,6 +18,7 @@ def compute_csf_tension(phi, flags, Fx, Fy, Fz, gamma_lu, FLAG_SOLID, FLAG_GAS, 
 
 
 __all__ = [
-    "clear_forces", "compute_marangoni_force", "compute_csf_tension", "compute_csf_wetting",
+    "clear_forces", "compute_marangoni_force", "compute_marangoni_force_variable",
+    "compute_csf_tension", "compute_csf_wetting",
     "add_buoyancy", "add_hydrostatic_gravity", "apply_arc_pressure",
 ]

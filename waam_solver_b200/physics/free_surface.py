@@ -7,6 +7,7 @@ update_flags_from_phi = kernels.update_flags_from_phi
 sync_phi_liquid_fraction = kernels.sync_phi_liquid_fraction
 surface_height_at = kernels.surface_height_at
 apply_contact_angle_phi_bc = kernels.apply_contact_angle_phi_bc
+remelt_hot_solid = kernels.remelt_hot_solid
 remelt_hot_solid_scalar = kernels.remelt_hot_solid_scalar
 
 
@@ -20,5 +21,5 @@ def solidify_cooled_metal(T, f_l, phi, flags, ux, uy, uz, T_solidus, zero_veloci
 __all__ = [
     "advect_phi", "reinitialize_phi", "update_flags_from_phi", "sync_phi_liquid_fraction",
     "surface_height_at", "solidify_cooled_metal", "apply_contact_angle_phi_bc",
-    "remelt_hot_solid_scalar",
+    "remelt_hot_solid", "remelt_hot_solid_scalar",
 ]

@@ -3,8 +3,8 @@ the step path: construction, derived lattice scalars, reset, step, run,
 run_path, telemetry).
 
 The constructor takes the reference's keyword arguments.  Features outside
-the accelerated path (material tables, vapour recoil, gas shear, moving
-window) raise instead of silently changing the physics.
+the accelerated path (vapour recoil, gas shear, moving window) raise
+instead of silently changing the physics.
 """
 from __future__ import annotations
 
@@ -15,6 +15,7 @@ import torch
 
 from . import kernels
 from .coupled_step import coupled_step
+from .gpu_tables import MaterialGPUTables
 from .grid import WAAMGrid
 from .materials import MaterialProps, load_material
 from .physics.arc import create_heat_source
@@ -58,9 +59,6 @@ class WAAMTwin:
         if enable_moving_window:
             raise NotImplementedError("moving window is not supported by this backend")
         self.mat = material if isinstance(material, MaterialProps) else load_material(material, high_sulphur)
-        if self.mat.has_tables:
-            raise NotImplementedError("temperature-dependent material tables are not supported")
-        self.use_material_tables = False
         self.Q_w = arc_power_W
         self.eta = arc_efficiency
         self.T_amb = T_ambient
@@ -182,7 +180,12 @@ class WAAMTwin:
         self.force_scale = scale_F
         self.dgamma_dT_lu = mat.dgamma_dT * scale_F / g.dx
         self.gamma_lu = mat.gamma_0 * scale_F / g.dx
-        self.H_sol = mat.rho * mat.cp * mat.T_solidus
+        # twin.py:269-273: the table path runs when the material has any table;
+        # H_sol / H_liq use cp at the solidus
+        self.gpu_tables = MaterialGPUTables(mat)
+        self.use_material_tables = self.gpu_tables.enabled
+        cp_sol = mat.cp_at(mat.T_solidus)
+        self.H_sol = mat.rho * cp_sol * mat.T_solidus
         self.H_liq = self.H_sol + self.L_rho
         self.arc_source = create_heat_source(heat_source)
 
@@ -387,5 +390,7 @@ class WAAMTwin:
                     deposited_mass_kg=dep_mass, expected_mass_kg=expected_deposited_mass_kg(self),
                     mass_balance_ratio=dep_mass / max(exp_drop, 1e-12),
                     n_droplets=self._n_droplets_fired,
-                    total_enthalpy_J=float(g.H.double().sum().item()) * g.dx ** 3)
+                    total_enthalpy_J=float(g.H.double().sum().item()) * g.dx ** 3,
+                    material_tables=self.use_material_tables,
+                    variable_tau=self.use_variable_tau and self.use_material_tables)
         return tele
