@@ -73,11 +73,13 @@ def twin_kwargs(w):
     return {k: w[k] for k in keys if k in w}
 
 
-def build_twin(w, device, population_dtype="float32"):
+def build_twin(w, device, population_dtype="float32", tables=None):
     from waam_solver_b200 import WAAMTwin
     from waam_solver_b200.materials import from_constants
     from waam_solver_b200.physics.arc import goldak_from_job_mm
     mat = from_constants("ER70S-6-constants", MATERIAL, contact_angle_deg=w.get("contact_angle_deg", 30.0))
+    if tables is not None:
+        mat.tables = tables
     tw = WAAMTwin(material=mat, nx=w["nx"], ny=w["ny"], nz=w["nz"], dx=w["dx"], max_tracers=1024,
                   device=device, population_dtype=population_dtype, **twin_kwargs(w))
     if w.get("plate_thickness_mm"):
@@ -278,6 +280,43 @@ def run_reference(args, w):
     print(json.dumps(line), flush=True)
 
 
+def _time_variant(tw, w, device, K):
+    """Whole-step time over K device-resident steps after the workload's
+    spin-up, and the stage times of 200 instrumented steps."""
+    import torch
+    g = tw.grid
+    pos = positions(w, g.dt, w["spinup"] + K + 204)
+    s = 0
+    for _ in range(w["spinup"]):
+        tw.step(*pos[s], True)
+        s += 1
+    dev_pos = torch.tensor([[x / g.dx, y / g.dx] for x, y in pos[s:s + K]],
+                           dtype=torch.float32, device=device)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(K):
+        tw._device_position = dev_pos[k]
+        tw.step(*pos[s], True)
+        s += 1
+    e1.record()
+    torch.cuda.synchronize()
+    tw._device_position = None
+    ms = e0.elapsed_time(e1) / K
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(7)] for _ in range(200)]
+    for es in evs:
+        for e in es:
+            e.record()
+    for es in evs:
+        tw._stage_events = es
+        tw.step(*pos[s], True)
+        s += 1
+    torch.cuda.synchronize()
+    tw._stage_events = None
+    stages = [statistics.fmean(es[q].elapsed_time(es[q + 1]) for es in evs) for q in range(6)]
+    return ms, stages
+
+
 def storage_forms(w, device, K, ref_ms):
     """The same workload with 16-bit population storage (float16 / bfloat16
     offsets from the rest weights): whole-step time over K device-resident
@@ -287,35 +326,8 @@ def storage_forms(w, device, K, ref_ms):
     for dtype in ("float16", "bfloat16"):
         tw = build_twin(w, device, population_dtype=dtype)
         g = tw.grid
-        pos = positions(w, g.dt, w["spinup"] + K + 204)
-        s = 0
-        for _ in range(w["spinup"]):
-            tw.step(*pos[s], True)
-            s += 1
-        dev_pos = torch.tensor([[x / g.dx, y / g.dx] for x, y in pos[s:s + K]],
-                               dtype=torch.float32, device=device)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for k in range(K):
-            tw._device_position = dev_pos[k]
-            tw.step(*pos[s], True)
-            s += 1
-        e1.record()
-        torch.cuda.synchronize()
-        tw._device_position = None
-        ms = e0.elapsed_time(e1) / K
-        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(7)] for _ in range(200)]
-        for es in evs:
-            for e in es:
-                e.record()
-        for es in evs:
-            tw._stage_events = es
-            tw.step(*pos[s], True)
-            s += 1
-        torch.cuda.synchronize()
-        tw._stage_events = None
-        stream_ms = statistics.fmean(es[4].elapsed_time(es[5]) for es in evs)
+        ms, stages = _time_variant(tw, w, device, K)
+        stream_ms = stages[4]
         c = census(tw)
         stream_bytes = 4 * c["n"] + 76 * (c["n"] - c["solid"])
         out[dtype] = {"value": g.n_cells / (ms * 1e-3) / 1e6, "unit": "MLUPS", "ms_per_step": ms,
@@ -323,6 +335,36 @@ def storage_forms(w, device, K, ref_ms):
                       "stream_GBps": stream_bytes / (stream_ms * 1e-3) / 1e9, "steps": K}
         del tw, g
         torch.cuda.empty_cache()
+    return out
+
+
+def table_material():
+    """The workload's steel with temperature tables in the layout of a
+    validated material file: cp, k and mu at three knots around the constants
+    and the Sahoo-DebRoy dgamma/dT table (28 ppm S, 8 knots)."""
+    from waam_solver_b200.materials import MaterialTables, build_sahoo_dgamma_table
+    m, Tl = MATERIAL, MATERIAL["T_liquidus"]
+    return MaterialTables(
+        cp=[(300.0, 0.95 * m["cp"]), (1000.0, m["cp"]), (Tl, 1.06 * m["cp"])],
+        k=[(300.0, 0.93 * m["k"]), (1000.0, m["k"]), (Tl, 1.13 * m["k"])],
+        mu=[(300.0, 1.15 * m["mu"]), (Tl, m["mu"]), (Tl + 200.0, 0.85 * m["mu"])],
+        dgamma_dT=build_sahoo_dgamma_table(28.0, Tl, max(Tl + 800.0, 2600.0), n=8))
+
+
+def table_form(w, device, K, ref_ms, ref_stages):
+    """The workload on the material-table path (per-cell properties refreshed
+    from T inside the thermal stage, variable-tau SRT collision)."""
+    import torch
+    tw = build_twin(w, device, tables=table_material())
+    assert tw.use_material_tables
+    ms, stages = _time_variant(tw, w, device, K)
+    out = {"value": tw.grid.n_cells / (ms * 1e-3) / 1e6, "unit": "MLUPS", "ms_per_step": ms,
+           "vs_constants": ref_ms / ms, "thermal_ms": stages[0],
+           "thermal_ms_constants": ref_stages.get("thermal"), "collide_ms": stages[3],
+           "collide_ms_constants": ref_stages.get("collide"), "steps": K,
+           "material": "workload constants + cp/k/mu tables (3 knots) + Sahoo dgamma/dT (8)"}
+    del tw
+    torch.cuda.empty_cache()
     return out
 
 
@@ -456,6 +498,7 @@ def run_b200(args, w):
         line["precision_forms"] = storage_forms(w, device, min(K, 1000), ms / K)
         line["precision_forms"]["storage"] = ("headline value: float32 populations; forms: "
                                               "16-bit offsets f_q - w_q, float32 arithmetic")
+        line["material_tables"] = table_form(w, device, min(K, 1000), ms / K, stage_ms)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:
