@@ -37,7 +37,8 @@ int waam_abi_version(void);
  * step for a grid of n cells (block partial sums and a field-sized scratch). */
 size_t waam_workspace_bytes(int64_t n);
 /* sizeof of the ABI structs, for FFI layout checks: 0 WaamFields,
- * 1 WaamStepParams, 2 WaamMaterialTables (0 for any other value) */
+ * 1 WaamStepParams, 2 WaamMaterialTables, 3 WaamTelemetry, 4 WaamProbeSet
+ * (0 for any other value) */
 size_t waam_struct_size(int which);
 
 /* ---- operator API: one entry per reference Taichi kernel ---------------- */
@@ -348,6 +349,56 @@ int waam_solidify_trailing_pool(float* T, float* H, float* f_l, float* phi, int3
                                 int ny, int nz, float arc_i, float arc_j, float arc_k, float dir_x,
                                 float dir_y, float dir_z, float lookback, float T_freeze,
                                 float T_solidus, void* stream);
+
+/* ---- telemetry (twin.py:706-821; kernels.py:3424-3481) -------------------- */
+
+#define WAAM_TOE_CELLS 16
+/* Pool aggregates written by waam_telemetry_pool into device memory. */
+typedef struct WaamTelemetry {
+    double T_global;        /* max T over all cells, at least 0 */
+    double T_peak;          /* max T over cells with f_l > 0.5, at least 0 */
+    double peak_cool;       /* max -dT/dt over cells with phi > 0.05, at least 0 */
+    double u2_max;          /* max |u|^2 (lattice units) over cells with f_l > 0.5 */
+    double H_sum;           /* sum of H over all cells, FP64, fixed order */
+    int64_t n_liquid;       /* cells with f_l > 0.5 */
+    int64_t i_sum;          /* sum of their i (exact) */
+    int32_t i_min, i_max;   /* their i extent (-1 without liquid) */
+    int32_t i_c;            /* centroid slice round(i_sum / n_liquid) (half to even), clamped; -1 without liquid */
+    int32_t y_min, y_max, z_min; /* extent of f_l > 0.5 in slice i_c (-1 when empty) */
+    int32_t bead_k_max;     /* max k of SOLID cells with k >= nz_solid, -1 if none */
+    int32_t n_tracers_active, n_tracers_trapped; /* porosity tracers with active == 1 / == 2 */
+    int32_t toe_k0, toe_n;  /* toe-angle column (nx/3, ny/2, k0 .. k0 + toe_n - 1) */
+    float toe_phi[WAAM_TOE_CELLS];
+    int32_t toe_flags[WAAM_TOE_CELLS];
+} WaamTelemetry;
+
+/* kernels.py:3424-3468 telemetry_pool_reduce, the centroid slice of
+ * twin.py:723-744 (kernels.py:3471-3481), the tracer counts, the bead height
+ * of physics/electrical_stickout.py:39-50 and the toe column of
+ * physics/bead_geometry.py:13-40, into `out` (device memory): two launches,
+ * deterministic (FP64 enthalpy sum in a fixed order, integer sums exact).
+ * H may be null (H_sum = 0), flags may be null (no bead height, no toe
+ * column), tracer_active may be null (max_tracers ignored). */
+int waam_telemetry_pool(const float* T, const float* f_l, const float* phi, const float* dT_dt,
+                        const float* ux, const float* uy, const float* uz, const float* H,
+                        const int32_t* flags, const int32_t* tracer_active, int max_tracers,
+                        int nx, int ny, int nz, int nz_solid, WaamTelemetry* out,
+                        void* workspace, size_t workspace_bytes, void* stream);
+
+#define WAAM_MAX_PROBES 64
+/* Probe cells (export/probes.py:29-37 resolve on the host; -1 = outside the grid). */
+typedef struct WaamProbeSet {
+    int32_t n_probes;
+    int64_t cell[WAAM_MAX_PROBES];   /* (i * ny + j) * nz + k */
+} WaamProbeSet;
+/* export/probes.py:90-107: row[2p] = T, row[2p+1] = f_l at probe p (NaN outside).
+ * `probes` is a host pointer, `row` device memory (2 * n_probes floats). */
+int waam_probe_sample(const float* T, const float* f_l, const WaamProbeSet* probes, float* row,
+                      void* stream);
+/* physics/electrical_stickout.py:39-50: max k of SOLID cells with k >= nz_solid
+ * into *out (device int32; -1 when there are none). */
+int waam_bead_height(const int32_t* flags, int nx, int ny, int nz, int nz_solid, int32_t* out,
+                     void* stream);
 
 /* ---- fused step: the B200 pipeline of solvers/coupled_step.py:73-464 ----- */
 

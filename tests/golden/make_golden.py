@@ -725,6 +725,56 @@ def table_step_cases():
 
 
 # ---------------------------------------------------------------------------
+# telemetry: the reference's get_telemetry on seeded states
+# ---------------------------------------------------------------------------
+TELEM_FIELDS = ["T", "H", "f_l", "phi", "dT_dt", "ux", "uy", "uz", "flags"]
+
+
+def telemetry_cases():
+    """twin.py:706-821 on three states: a seeded pool with tracers, deposited
+    solid above the plate and wetting on (toe angle); the same state with the
+    pool frozen out (no liquid); the reset state."""
+    nx, ny, nz = 20, 14, 14
+    out = {}
+    for name, seed in (("pool", 31), ("frozen", 32), ("reset", None)):
+        tw = make_twin(nx, ny, nz, enable_wetting=True, droplet_freq_hz=100.0)
+        tw.plate_thickness_mm = 0.8
+        tw.wire_feed_m_s = 0.1
+        tw.reset()
+        tw.enable_force_diagnostics = False
+        g = tw.grid
+        if seed is not None:
+            st = seeded_state(nx, ny, nz, seed=seed, nz_solid=tw.nz_solid)
+            rng = np.random.default_rng(seed)
+            st["dT_dt"] = rng.normal(0.0, 2e4, st["T"].shape).astype(np.float32)
+            if name == "frozen":
+                st["f_l"] = np.minimum(st["f_l"], np.float32(0.4))
+            # a few deposited solid cells above the plate
+            st["flags"][3:6, 5:8, tw.nz_solid:tw.nz_solid + 3] = 1
+            load_state(g, st)
+            act = np.zeros(g.max_tracers, np.int32)
+            act[:30] = 1
+            act[30:41] = 2
+            g.porosity_active.from_numpy(act)
+            tw._deposited_volume_m3 = 3.1e-9
+            tw._n_droplets_fired = 4
+            tw._step_n = 123
+        tele = tw.get_telemetry()
+        tele.pop("force_diagnostics", None)
+        for f in TELEM_FIELDS:
+            out["%s_%s" % (name, f)] = getattr(g, f).to_numpy()
+        out["%s_porosity_active" % name] = g.porosity_active.to_numpy()
+        out["%s_telemetry" % name] = np.array(json.dumps(tele))
+        out["%s_state" % name] = np.array(json.dumps(dict(
+            nz_solid=tw.nz_solid, step=tw._step_n, deposited=tw._deposited_volume_m3,
+            n_drops=tw._n_droplets_fired, material=material_record(tw),
+            twin_kw=dict(nx=nx, ny=ny, nz=nz, enable_wetting=True, droplet_freq_hz=100.0,
+                         use_srt=False, enable_vof=True, wire_feed_m_s=0.1,
+                         plate_thickness_mm=0.8))))
+    save("telemetry.npz", out)
+
+
+# ---------------------------------------------------------------------------
 # known-answer values of the reference validation scripts
 # ---------------------------------------------------------------------------
 def kats():
@@ -748,5 +798,7 @@ if __name__ == "__main__":
         step_cases()
     if "table_steps" in what:
         table_step_cases()
+    if "telemetry" in what:
+        telemetry_cases()
     if "kats" in what:
         kats()

@@ -44,6 +44,24 @@ class WaamMaterialTables(C.Structure):
                                         "dgamma_fallback")])
 
 
+TOE_CELLS = 16
+MAX_PROBES = 64
+
+
+class WaamTelemetry(C.Structure):
+    """Device record of waam_telemetry_pool (see the header)."""
+    _fields_ = ([(n, C.c_double) for n in ("T_global", "T_peak", "peak_cool", "u2_max", "H_sum")]
+                + [(n, C.c_int64) for n in ("n_liquid", "i_sum")]
+                + [(n, C.c_int32) for n in ("i_min", "i_max", "i_c", "y_min", "y_max", "z_min",
+                                            "bead_k_max", "n_tracers_active",
+                                            "n_tracers_trapped", "toe_k0", "toe_n")]
+                + [("toe_phi", C.c_float * TOE_CELLS), ("toe_flags", C.c_int32 * TOE_CELLS)])
+
+
+class WaamProbeSet(C.Structure):
+    _fields_ = [("n_probes", C.c_int32), ("cell", C.c_int64 * MAX_PROBES)]
+
+
 def _params_fields():
     """Field list of WaamStepParams, parsed from the header."""
     src = open(HEADER).read()
@@ -72,6 +90,7 @@ _CTYPES = {
     "const WaamFields*": C.POINTER(WaamFields),
     "const WaamStepParams*": C.POINTER(WaamStepParams), "const char*": C.c_char_p,
     "void* const*": C.c_void_p, "const WaamMaterialTables*": C.POINTER(WaamMaterialTables),
+    "WaamTelemetry*": C.c_void_p, "const WaamProbeSet*": C.POINTER(WaamProbeSet),
 }
 
 

@@ -21,7 +21,7 @@ import torch
 from . import _native, kernels
 from ._native import WaamError
 from .physics import deposition, forces, free_surface, lbm, phase_change, thermal, weld_forces
-from .physics.electrical_stickout import droplet_entry_temperature_K
+from .physics.electrical_stickout import droplet_entry_temperature_K, update_ctwd
 
 T_800 = 800.0 + 273.15
 T_1100 = 1100.0 + 273.15
@@ -151,6 +151,8 @@ def coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=Non
     arc_k = _resolve_arc_k(twin, g, arc_i, arc_j, torch_z_m)
     twin._last_arc_ijk = (float(arc_i), float(arc_j), float(arc_k))
     forces.clear_forces(g.Fx, g.Fy, g.Fz)
+    if twin.enable_ctwd:
+        update_ctwd(twin, g)
     pressure = weld_forces.arc_pressure_peak_pa(twin)
     p_sigma = weld_forces.arc_pressure_sigma_cells(twin)
     if is_welding:
@@ -456,6 +458,9 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     if not _check_fused_supported(twin):
         return coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m)
     g = twin.grid
+    if twin.enable_ctwd:
+        # solvers/coupled_step.py:99-100: bead height from the flags at step start
+        update_ctwd(twin, g)
     arc_i = torch_x_m / g.dx
     arc_j = torch_y_m / g.dx
     p = twin._fused_params

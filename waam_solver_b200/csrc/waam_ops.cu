@@ -705,6 +705,8 @@ size_t waam_struct_size(int which) {
         case 0: return sizeof(WaamFields);
         case 1: return sizeof(WaamStepParams);
         case 2: return sizeof(WaamMaterialTables);
+        case 3: return sizeof(WaamTelemetry);
+        case 4: return sizeof(WaamProbeSet);
         default: return 0;
     }
 }

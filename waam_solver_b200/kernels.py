@@ -788,3 +788,77 @@ def advect_tracers(pos, active, ux, uy, uz, f_l, flags, dx, dt, max_tracers, FLA
         raise WaamError("advect_tracers: pos must be (max_tracers, 3), active (max_tracers,)")
     _call("waam_advect_tracers", _f(pos), _i(active), _f(ux, n), _f(uy, n), _f(uz, n),
           _f(f_l, n), _i(flags, n), nx, ny, nz, float(dx), m, _stream())
+
+
+# ------------------------------------------------------------ telemetry ----
+TELEMETRY_BYTES = ctypes.sizeof(_native.WaamTelemetry)
+
+
+def telemetry_record(device):
+    """Device buffer for one WaamTelemetry record."""
+    return torch.zeros(TELEMETRY_BYTES, dtype=torch.uint8, device=device)
+
+
+def telemetry_pool(T, f_l, phi, dT_dt, ux, uy, uz, H, flags, tracer_active, max_tracers,
+                   nz_solid, record):
+    """Every pool aggregate of get_telemetry into ``record`` (two launches, no sync)."""
+    nx, ny, nz = _dims(T)
+    n = T.numel()
+    if record.numel() < TELEMETRY_BYTES or record.dtype != torch.uint8 or not record.is_cuda:
+        raise WaamError("record must be a CUDA uint8 tensor of %d bytes" % TELEMETRY_BYTES)
+    ws, wsb = workspace_for(T)
+    act = _i(tracer_active) if tracer_active is not None and max_tracers > 0 else None
+    _call("waam_telemetry_pool", _f(T, n), _f(f_l, n), _f(phi, n), _f(dT_dt, n), _f(ux, n),
+          _f(uy, n), _f(uz, n), None if H is None else _f(H, n),
+          None if flags is None else _i(flags, n), act, int(max_tracers), nx, ny, nz,
+          int(nz_solid), record.data_ptr(), ws, wsb, _stream())
+
+
+def read_telemetry(record):
+    """The record as a WaamTelemetry struct (one device-to-host read)."""
+    host = record[:TELEMETRY_BYTES].cpu().numpy().tobytes()
+    return _native.WaamTelemetry.from_buffer_copy(host)
+
+
+def telemetry_pool_reduce(T, f_l, phi, dT_dt, ux, uy, uz, n_buf, T_peak_buf, cool_buf, u2_buf,
+                          i_sum_buf, i_min_buf, i_max_buf, T_global_buf):
+    """kernels.py:3424-3468 with its 0-d output buffers (filled on the device)."""
+    rec = telemetry_record(T.device)
+    telemetry_pool(T, f_l, phi, dT_dt, ux, uy, uz, None, None, None, 0, 0, rec)
+    d = rec[:40].view(torch.float64)
+    q = rec[40:56].view(torch.int64)
+    ints = rec[56:64].view(torch.int32)
+    has = q[0] > 0
+    n_buf.copy_(q[0].to(n_buf.dtype))
+    T_global_buf.copy_(d[0].to(T_global_buf.dtype))
+    T_peak_buf.copy_(d[1].to(T_peak_buf.dtype))
+    cool_buf.copy_(d[2].to(cool_buf.dtype))
+    u2_buf.copy_(d[3].to(u2_buf.dtype))
+    i_sum_buf.copy_(q[1].to(i_sum_buf.dtype))
+    i_min_buf.copy_(torch.where(has, ints[0].to(torch.float64),
+                                torch.full_like(d[0], 1.0e9)).to(i_min_buf.dtype))
+    i_max_buf.copy_(torch.where(has, ints[1].to(torch.float64),
+                                torch.full_like(d[0], -1.0e9)).to(i_max_buf.dtype))
+
+
+def extract_fl_yz_slice(f_l, out, i_slice, ny, nz):
+    """kernels.py:3471-3481."""
+    out.copy_(f_l[int(i_slice)].reshape(out.shape))
+
+
+def probe_sample(T, f_l, cells, row):
+    """T and f_l at cell indices ``cells`` (-1: outside) into ``row`` (device,
+    2 floats per probe), export/probes.py:90-107."""
+    if len(cells) > _native.MAX_PROBES:
+        raise WaamError("at most %d probes" % _native.MAX_PROBES)
+    ps = _native.WaamProbeSet()
+    ps.n_probes = len(cells)
+    for q, c in enumerate(cells):
+        ps.cell[q] = int(c)
+    _call("waam_probe_sample", _f(T), _f(f_l), ctypes.byref(ps), _f(row), _stream())
+
+
+def bead_height_k(flags, nz_solid, out):
+    """Max k of SOLID cells at or above nz_solid into the 0-d int32 ``out`` (-1: none)."""
+    nx, ny, nz = _dims(flags)
+    _call("waam_bead_height", _i(flags), nx, ny, nz, int(nz_solid), _i(out), _stream())

@@ -109,7 +109,7 @@ class MaterialProps:
         return interp_linear(T, self.tables.dgamma_dT, self.dgamma_dT)
 
 
-def from_constants(name: str, c: dict, status: str = "synthetic", **extra) -> MaterialProps:
+def from_constants(name: str, c: dict, status: str = "placeholder", **extra) -> MaterialProps:
     """MaterialProps from a constants dict (keys as the reference YAML ``constants``)."""
     rho, cp, k = float(c["rho"]), float(c["cp"]), float(c["k"])
     return MaterialProps(

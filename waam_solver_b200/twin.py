@@ -19,7 +19,11 @@ from .gpu_tables import MaterialGPUTables
 from .grid import WAAMGrid
 from .materials import MaterialProps, load_material
 from .physics.arc import create_heat_source
-from .physics.deposition_balance import droplet_mass_kg, expected_deposited_mass_kg
+from .physics.bead_geometry import bead_height_m_from_k, toe_angle_from_column
+from .physics.deposition_balance import (droplet_mass_kg, expected_deposited_mass_kg,
+                                         infer_transfer_mode, wire_mass_flux_kg_s)
+from .physics.electrical_stickout import droplet_entry_temperature_K
+from .physics.weld_forces import arc_pressure_peak_pa, droplet_impact_velocity_m_s
 from .torch_path import TorchPathDriver, clamp_torch_to_domain, parse_torch_path
 
 RHO_LATTICE = 1.0
@@ -356,41 +360,109 @@ class WAAMTwin:
             cx, cy = clamp(x, y)
             self.step(cx, cy, is_welding, torch_z_m=z)
 
-    # -- telemetry (twin.py:706-821, pool metrics) -------------------------
-    def get_telemetry(self):
+    # -- telemetry (twin.py:706-821) -----------------------------------------
+    def telemetry_record(self):
+        """Launch the pool reductions into the grid's device record (no sync);
+        ``kernels.read_telemetry(grid.telem_record)`` reads it back later."""
         g = self.grid
-        fl = g.f_l
-        liquid = fl > 0.5
-        n_liquid = int(liquid.sum().item())
-        tele = {"step": self._step_n, "sim_time_s": self._step_n * g.dt, "n_liquid_cells": n_liquid}
-        nongas = g.flags != g.FLAG_GAS
+        rec = getattr(g, "telem_record", None)
+        if rec is None:
+            rec = g.telem_record = kernels.telemetry_record(g.device)
+        kernels.telemetry_pool(g.T, g.f_l, g.phi, g.dT_dt, g.ux, g.uy, g.uz, g.H, g.flags,
+                               g.porosity_active, g.max_tracers, self.nz_solid, rec)
+        return rec
+
+    def get_telemetry(self):
+        """Pool and process telemetry with the reference's keys.
+
+        Every grid aggregate comes from one device record (two launches,
+        deterministic, FP64 enthalpy sum) read back in one small copy; the
+        reference's atomics, f_l slice, tracer, flags and phi copies are not
+        needed.  Force diagnostics (physics/force_diagnostics.py, a telemetry-
+        time re-run of each force operator) are not part of this backend."""
+        g = self.grid
+        r = kernels.read_telemetry(self.telemetry_record())
+        n_liquid = int(r.n_liquid)
         if n_liquid > 0:
-            T_peak = float(torch.where(liquid, g.T, torch.full_like(g.T, -1e30)).max().item())
-            ii = torch.nonzero(liquid)[:, 0].to(torch.float64)
-            i_c = int(round(float(ii.mean().item())))
-            i_c = max(0, min(g.nx - 1, i_c))
-            sect = (fl[i_c] > 0.5).cpu().numpy()
-            if sect.any():
-                y_idx = np.where(sect.any(axis=1))[0]
-                z_idx = np.where(sect.any(axis=0))[0]
-                width = (y_idx[-1] - y_idx[0] + 1) * g.dx
-                depth = max(0, self.nz_solid - z_idx[0]) * g.dx
+            T_peak = float(r.T_peak)
+            if r.y_min >= 0:
+                pool_width_m = (r.y_max - r.y_min + 1) * g.dx
+                pool_depth_m = max(0, self.nz_solid - r.z_min) * g.dx
             else:
-                width = depth = 0.0
-            length = (float(ii.max().item()) - float(ii.min().item()) + 1.0) * g.dx
-            u2 = (g.ux * g.ux + g.uy * g.uy + g.uz * g.uz)[liquid].max().item()
-            u_max = math.sqrt(u2) * g.dx / g.dt
+                pool_width_m = pool_depth_m = 0.0
+            pool_length_m = (float(r.i_max) - float(r.i_min) + 1.0) * g.dx
+            u_max_phys = float(np.sqrt(float(r.u2_max))) * g.dx / g.dt
         else:
-            T_peak = float(torch.where(nongas, g.T, torch.full_like(g.T, -1e30)).max().item())
-            width = depth = length = u_max = 0.0
+            T_peak = float(r.T_global)
+            pool_width_m = pool_depth_m = pool_length_m = u_max_phys = 0.0
+        peak_cool = float(r.peak_cool)
+        n_trapped, n_active = int(r.n_tracers_trapped), int(r.n_tracers_active)
+        porosity_pct = 100.0 * n_trapped / max(n_trapped + n_active, 1)
         dep_mass = self._deposited_volume_m3 * self.mat.rho
-        exp_drop = self._n_droplets_fired * droplet_mass_kg(self)
-        tele.update(T_peak_K=T_peak, pool_width_mm=width * 1e3, pool_depth_mm=depth * 1e3,
-                    pool_length_mm=length * 1e3, u_max_m_s=u_max,
-                    deposited_mass_kg=dep_mass, expected_mass_kg=expected_deposited_mass_kg(self),
-                    mass_balance_ratio=dep_mass / max(exp_drop, 1e-12),
-                    n_droplets=self._n_droplets_fired,
-                    total_enthalpy_J=float(g.H.double().sum().item()) * g.dx ** 3,
-                    material_tables=self.use_material_tables,
-                    variable_tau=self.use_variable_tau and self.use_material_tables)
-        return tele
+        exp_mass = expected_deposited_mass_kg(self)
+        m_drop = droplet_mass_kg(self)
+        exp_drop_mass = self._n_droplets_fired * m_drop
+        mass_ratio = dep_mass / max(exp_drop_mass, 1e-12)
+        bead_h = bead_height_m_from_k(int(r.bead_k_max), self.nz_solid, g.dx) * 1000.0
+        toe_deg = 0.0
+        if self.enable_wetting:
+            toe_deg = toe_angle_from_column(list(r.toe_phi)[: r.toe_n],
+                                            list(r.toe_flags)[: r.toe_n], int(r.toe_k0),
+                                            self.contact_angle_deg, g.dx, g.FLAG_GAS)
+        return {
+            "step": self._step_n,
+            "sim_time_ms": round(self._step_n * g.dt * 1000, 4),
+            "peak_temp_K": round(T_peak, 1),
+            "peak_temp_C": round(T_peak - 273.15, 1),
+            "peak_cooling_rate_Ks": round(peak_cool, 1),
+            "pool_width_mm": round(pool_width_m * 1000, 3),
+            "pool_depth_mm": round(pool_depth_m * 1000, 3),
+            "pool_length_mm": round(pool_length_m * 1000, 3),
+            "n_liquid_cells": n_liquid,
+            "marangoni_vel_ms": round(u_max_phys, 4),
+            "material_status": self.mat.status,
+            "material_name": self.mat.name,
+            "heat_source": self.heat_source_name,
+            "material_tables": self.use_material_tables,
+            "vof_enabled": self.enable_vof,
+            "travel_speed_mm_s": round(self.travel_speed_m_s * 1000, 3),
+            "variable_tau": self.use_variable_tau and self.use_material_tables,
+            "porosity_pct": round(porosity_pct, 3),
+            "n_trapped_tracers": n_trapped,
+            "window_offset_x_mm": round(self._window_offset_x_m * 1000, 3),
+            "deposited_mass_g": round(dep_mass * 1000, 4),
+            "expected_wire_mass_g": round(exp_mass * 1000, 4),
+            "expected_drop_mass_g": round(exp_drop_mass * 1000, 4),
+            "n_droplets_fired": self._n_droplets_fired,
+            "droplet_mass_mg": round(m_drop * 1e6, 3),
+            "droplet_transfer_mode": infer_transfer_mode(self),
+            "droplet_impact_velocity_ms": round(droplet_impact_velocity_m_s(self), 4),
+            "mass_balance_ratio": round(mass_ratio, 3),
+            "wire_mass_flux_g_s": round(wire_mass_flux_kg_s(self) * 1000, 4),
+            "T_vapor_cap_K": self.T_vapor_cap_K,
+            "arc_surface_weighting": self.arc_surface_weighting,
+            "enable_enthalpy_cap": self.enable_enthalpy_cap,
+            "enable_wetting": self.enable_wetting,
+            "enable_hydrostatic_gravity": self.enable_hydrostatic_gravity,
+            "enable_bead_freeze": self.enable_bead_freeze,
+            "enable_ctwd": self.enable_ctwd,
+            "contact_angle_deg": round(self.contact_angle_deg, 1),
+            "bead_height_mm": round(bead_h, 3),
+            "toe_angle_deg": round(toe_deg, 1),
+            "ctwd_mm": round(self.ctwd_m * 1000, 3),
+            "T_drop_K": round(droplet_entry_temperature_K(self), 1),
+            "deposition_overflow_count": self._deposition_overflow,
+            "physics_tier": getattr(self, "physics_tier", "flow"),
+            "strict_mode": bool(getattr(self, "strict_mode", False)),
+            "arc_pressure_model": getattr(self, "arc_pressure_model", "constant"),
+            "arc_pressure_peak_pa": round(arc_pressure_peak_pa(self), 1),
+            "enable_lorentz": self.enable_lorentz,
+            "enable_gas_shear": self.enable_gas_shear,
+            "lorentz_unconverged_count": int(getattr(self, "_lorentz_unconverged", 0) or 0),
+            "lorentz_unconverged_streak": int(getattr(self, "_lorentz_unconverged_streak", 0)
+                                              or 0),
+            "force_diagnostics": {},
+            # additions: the FP64 total enthalpy and the raw pool extents
+            "total_enthalpy_J": float(r.H_sum) * g.dx ** 3,
+            "pool_slice_i": int(r.i_c),
+        }
