@@ -37,8 +37,8 @@ int waam_abi_version(void);
  * step for a grid of n cells (block partial sums and a field-sized scratch). */
 size_t waam_workspace_bytes(int64_t n);
 /* sizeof of the ABI structs, for FFI layout checks: 0 WaamFields,
- * 1 WaamStepParams, 2 WaamMaterialTables, 3 WaamTelemetry, 4 WaamProbeSet
- * (0 for any other value) */
+ * 1 WaamStepParams, 2 WaamMaterialTables, 3 WaamTelemetry, 4 WaamProbeSet,
+ * 5 WaamShiftPlane (0 for any other value) */
 size_t waam_struct_size(int which);
 
 /* ---- operator API: one entry per reference Taichi kernel ---------------- */
@@ -399,6 +399,31 @@ int waam_probe_sample(const float* T, const float* f_l, const WaamProbeSet* prob
  * into *out (device int32; -1 when there are none). */
 int waam_bead_height(const int32_t* flags, int nx, int ny, int nz, int nz_solid, int32_t* out,
                      void* stream);
+
+/* ---- moving window (kernels.py:2620-2723, twin.py:599-631) ---------------- */
+
+#define WAAM_MAX_SHIFT_PLANES 64
+#define WAAM_SHIFT_KEEP 0    /* moved, the right strip keeps its old values */
+#define WAAM_SHIFT_CONST 1   /* moved, the right strip becomes `below` */
+#define WAAM_SHIFT_BY_K 2    /* moved, the right strip becomes `below` for k < nz_solid, else `above` */
+/* One field plane of nx*ny*nz elements (4-byte float / int32 or 16-bit), its
+ * strip reset mode and the reset values as raw element bits. */
+typedef struct WaamShiftPlane {
+    void* ptr;
+    int32_t elem_bytes;
+    int32_t mode;
+    uint32_t below;
+    uint32_t above;
+} WaamShiftPlane;
+/* kernels.py:2620-2723 shift_simulation_window_x over any set of planes in one
+ * launch: plane[i] = plane[i + n_shift] for i < nx - n_shift (the reference's
+ * ascending in-place order), then the strip i >= nx - n_shift is reset per
+ * plane.  `planes` is a host array (n_planes <= WAAM_MAX_SHIFT_PLANES);
+ * n_shift >= 0. */
+int waam_shift_window_x(const WaamShiftPlane* planes, int n_planes, int n_shift, int nx, int ny,
+                        int nz, int nz_solid, void* stream);
+/* twin.py:624-626: pos[:, 0] -= shift_m for every tracer slot */
+int waam_shift_tracers_x(float* pos, int max_tracers, float shift_m, void* stream);
 
 /* ---- fused step: the B200 pipeline of solvers/coupled_step.py:73-464 ----- */
 

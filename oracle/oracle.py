@@ -81,6 +81,8 @@ _SIGS = {
     "wo_solidify_trailing_pool": ([_F] * 4 + [_I] + [_F] * 4 + [_i, _i, _i] + [_f] * 9, None),
     "wo_inject_tracers": ([_F, _I, _I, _i, _f, _f, _f, _f, _i, C.c_uint64], None),
     "wo_advect_tracers": ([_F, _I, _F, _F, _F, _F, _I, _i, _i, _i, _f, _i], None),
+    "wo_shift_simulation_window_x": ([_F] * 6 + [_I] + [_F] * 17 + [_i, _f, _f, _f, _i, _i, _i,
+                                                                    _i], None),
     "wo_num_threads": ([], C.c_int),
     "wo_expf_array": ([_F, _F, _l], None),
     "wo_set_num_threads": ([C.c_int], None),

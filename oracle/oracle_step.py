@@ -50,7 +50,8 @@ class OracleTwin:
             impact_lead_angle_deg=0.0, trailing_solidify_lookback_mm=2.5,
             trailing_solidify_temp_margin_K=35.0, enable_lorentz=False, sigma_liquid_Sm=1.0e6,
             sigma_solid_Sm=1.0e5, lorentz_jacobi_iters=40, lorentz_jacobi_omega=0.85,
-            lorentz_jacobi_tol=1e-4, max_tracers=64, tables=None, use_variable_tau=True)
+            lorentz_jacobi_tol=1e-4, max_tracers=64, tables=None, use_variable_tau=True,
+            enable_moving_window=False)
         unknown = set(kw) - set(self.cfg)
         if unknown:
             raise KeyError("unknown OracleTwin options: %s" % sorted(unknown))
@@ -93,6 +94,7 @@ class OracleTwin:
         self.s = None
         self.lorentz_warm = False
         self.lorentz_iters = []
+        self.window_offset = 0.0
 
     def _setup_tables(self, tables):
         """gpu_tables.py:12-80 (knot upload) and twin.py:269-273 (H_sol / H_liq
@@ -271,16 +273,47 @@ class OracleTwin:
         return min(5.0, sc * max(v_feed, v_grav + pinch) * mt)
 
     # ------------------------------------------------------------------ step --
+    def _maybe_shift_window(self, x_world):
+        """twin.py:599-631 on the oracle state."""
+        s = self.s
+        if x_world - self.window_offset < 0.62 * (self.nx - 8) * self.dx:
+            return
+        n_shift = max(8, self.nx // 10)
+        self.O.call("wo_shift_simulation_window_x", s["f_a"], s["f_b"], s["T"], s["H"], s["f_l"],
+                    s["phi"], s["flags"], s["T_max"], s["T_prev"], s["dT_dt"],
+                    s["time_above_800_s"], s["time_above_1100_s"], s["time_above_solidus_s"],
+                    s["rho"], s["ux"], s["uy"], s["uz"], s["Fx"], s["Fy"], s["Fz"],
+                    s["cp_rho_field"], s["alpha_lu_field"], s["dgamma_lu_field"], s["tau_field"],
+                    n_shift, self.cfg["T_ambient"], self.cp_rho, 1.0, self.nz_solid, self.nx,
+                    self.ny, self.nz)
+        self.window_offset += n_shift * self.dx
+        pos = s["porosity_pos"]
+        pos[:, 0] = pos[:, 0] - self.ft(n_shift * self.dx)
+
     def step(self, x, y, welding=True):
-        c, s, m = self.cfg, self.s, self.mat
-        nx, ny, nz = self.nx, self.ny, self.nz
-        n = nx * ny * nz
+        """One step at torch position (x, y); with the moving window on, x is a
+        world position (twin.py:533-567)."""
+        if self.cfg["enable_moving_window"]:
+            # the direction uses world positions, the physics the window's
+            self._update_dir(x, y)
+            self._maybe_shift_window(x)
+            return self._step(x - self.window_offset, y, welding, dir_done=True)
+        return self._step(x, y, welding)
+
+    def _update_dir(self, x, y):
         if self.last_pos is not None:
             d = (x - self.last_pos[0], y - self.last_pos[1], 0.0 - self.last_pos[2])
             nrm = math.sqrt(sum(v * v for v in d))
             if nrm > 1e-12:
                 self.dir = tuple(v / nrm for v in d)
         self.last_pos = (x, y, 0.0)
+
+    def _step(self, x, y, welding=True, dir_done=False):
+        c, s, m = self.cfg, self.s, self.mat
+        nx, ny, nz = self.nx, self.ny, self.nz
+        n = nx * ny * nz
+        if not dir_done:
+            self._update_dir(x, y)
         self._pos = (x, y)
         arc_i, arc_j = x / self.dx, y / self.dx
         i0 = max(0, min(int(arc_i), nx - 1))

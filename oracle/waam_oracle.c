@@ -1608,3 +1608,60 @@ void wo_solidify_trailing_pool(float* T, float* H, float* f_l, float* phi, int32
                 uz[c] = 0.0f;
             }
 }
+
+/* kernels.py:2620-2723 shift_simulation_window_x: every field moves n_shift
+ * cells towards i = 0 (ascending serial copy per (j, k) column), the right
+ * strip i >= nx - n_shift becomes ambient plate / gas at rest; the property
+ * fields are moved but not reset. */
+void wo_shift_simulation_window_x(float* f_a, float* f_b, float* T, float* H, float* f_l,
+                                  float* phi, int32_t* flags, float* T_max, float* T_prev,
+                                  float* dT_dt, float* t800, float* t1100, float* tsol,
+                                  float* rho, float* ux, float* uy, float* uz, float* Fx,
+                                  float* Fy, float* Fz, float* cp_f, float* alpha_f,
+                                  float* dg_f, float* tau_f, int n_shift, float T_amb,
+                                  float cp_rho, float rho0, int nz_solid, int nx, int ny,
+                                  int nz) {
+    int64_t n = (int64_t)nx * ny * nz;
+    float* fl32[] = {T, H, f_l, phi, T_max, T_prev, dT_dt, t800, t1100, tsol, rho,
+                     ux, uy, uz, Fx, Fy, Fz, cp_f, alpha_f, dg_f, tau_f};
+    const int nf = (int)(sizeof(fl32) / sizeof(fl32[0]));
+    for (int j = 0; j < ny; ++j)
+        for (int k = 0; k < nz; ++k)
+            for (int i = 0; i < nx - n_shift; ++i) {
+                int64_t d = IX(i, j, k), s = IX(i + n_shift, j, k);
+                for (int q = 0; q < nf; ++q) fl32[q][d] = fl32[q][s];
+                flags[d] = flags[s];
+                for (int q = 0; q < 19; ++q) {
+                    f_a[q * n + d] = f_a[q * n + s];
+                    f_b[q * n + d] = f_b[q * n + s];
+                }
+            }
+    int i0 = nx - n_shift;
+    for (int i = i0 < 0 ? 0 : i0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                int64_t c = IX(i, j, k);
+                T[c] = T_amb;
+                H[c] = cp_rho * T_amb;
+                f_l[c] = 0.0f;
+                rho[c] = rho0;
+                ux[c] = uy[c] = uz[c] = 0.0f;
+                Fx[c] = Fy[c] = Fz[c] = 0.0f;
+                T_prev[c] = T_amb;
+                dT_dt[c] = 0.0f;
+                T_max[c] = T_amb;
+                t800[c] = t1100[c] = tsol[c] = 0.0f;
+                if (k < nz_solid) {
+                    flags[c] = SOLID;
+                    phi[c] = 1.0f;
+                } else {
+                    flags[c] = GAS;
+                    phi[c] = 0.0f;
+                }
+                for (int q = 0; q < 19; ++q) {
+                    float feq = WQ(q) * rho0;
+                    f_a[q * n + c] = feq;
+                    f_b[q * n + c] = feq;
+                }
+            }
+}

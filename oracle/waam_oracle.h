@@ -179,6 +179,15 @@ void wo_advect_tracers(float* pos, int32_t* active, const float* ux, const float
                        const float* uz, const float* f_l, const int32_t* flags, int nx, int ny,
                        int nz, float dx, int max_tracers);
 
+/* kernels.py:2620-2723 shift_simulation_window_x */
+void wo_shift_simulation_window_x(float* f_a, float* f_b, float* T, float* H, float* f_l,
+                                  float* phi, int32_t* flags, float* T_max, float* T_prev,
+                                  float* dT_dt, float* t800, float* t1100, float* tsol,
+                                  float* rho, float* ux, float* uy, float* uz, float* Fx,
+                                  float* Fy, float* Fz, float* cp_f, float* alpha_f,
+                                  float* dg_f, float* tau_f, int n_shift, float T_amb,
+                                  float cp_rho, float rho0, int nz_solid, int nx, int ny, int nz);
+
 #ifdef __cplusplus
 }
 #endif

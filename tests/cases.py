@@ -47,14 +47,14 @@ def full_inputs(name):
                 "contact_s5": 5, "forces_wet": 6, "csf": 7, "csf_wet": 8, "collide_srt": 9,
                 "tail": 10, "heat_loss": 11, "surface_height": 12, "deposit": 13,
                 "lorentz": 14, "tracers": 15, "refresh": 16, "thermal_var": 17, "phase_var": 18,
-                "forces_var": 19, "srt_var": 20, "tail_var": 21}
+                "forces_var": 19, "srt_var": 20, "tail_var": 21, "shift": 24}
     grids = [v.shape[-3:] for v in ins.values() if v.ndim >= 3 and v.shape[-1] != 3]
     nx, ny, nz = grids[0] if grids else (13, 11, 12)   # tracer-only cases: the kernel-case grid
     st = state_gen.seeded_state(nx, ny, nz, seed=seed_map.get(name, 0))
     st = {k: (np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v) for k, v in st.items()}
     st["phi_tmp"] = np.zeros_like(st["phi"])
     for f, v in ins.items():
-        if f in st and f != "phi_tmp" and name != "reset":
+        if f in st and f != "phi_tmp" and name not in ("reset", "shift"):
             # the fixture was generated from this very seeded state
             assert np.array_equal(st[f], v), "state_gen drifted from fixture %s (%s)" % (name, f)
         st[f] = v.copy()
@@ -272,6 +272,14 @@ def run_case(be, name, st, a):
                                   st["uy"], st["uz"], st["cp_rho_field"], nx, ny, nz, a["arc_i"],
                                   a["arc_j"], a["arc_k"], 1.0, 0.0, 0.0, a["lookback"],
                                   a["T_freeze"], a["T_solidus_t"])
+    elif name == "shift":
+        be.shift_simulation_window_x(
+            st["f_a"], st["f_b"], st["T"], st["H"], st["f_l"], st["phi"], st["flags"],
+            st["T_max"], st["T_prev"], st["dT_dt"], st["time_above_800_s"],
+            st["time_above_1100_s"], st["time_above_solidus_s"], st["rho"], st["ux"], st["uy"],
+            st["uz"], st["Fx"], st["Fy"], st["Fz"], st["cp_rho_field"], st["alpha_lu_field"],
+            st["dgamma_lu_field"], st["tau_field"], a["n_shift"], a["T_amb"], a["cp_rho"],
+            a["rho0"], a["nz_solid"], nx, ny, nz)
     elif name == "tracers":
         be.advect_tracers(st["porosity_pos"], st["porosity_active"], st["ux"], st["uy"], st["uz"],
                           st["f_l"], st["flags"], nx, ny, nz, a["dx"], a["max_tracers"])
@@ -294,7 +302,7 @@ CASES = ["inject_gauss", "inject_goldak", "ceiling", "thermal", "thermal_s2", "p
          "tmax_cool", "vof", "vof_wet", "contact", "contact_s5", "forces", "forces_wet", "csf",
          "csf_wet", "collide_mrt", "collide_srt", "stream", "tail", "heat_loss",
          "surface_height", "deposit", "lorentz", "tracers", "refresh", "thermal_var",
-         "phase_var", "forces_var", "srt_var", "tail_var", "reset"]
+         "phase_var", "forces_var", "srt_var", "tail_var", "shift", "reset"]
 
 
 def check_case(be, name):

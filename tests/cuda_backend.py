@@ -111,6 +111,20 @@ class CudaBackend:
         for host, t in zip((cp_f, alpha_f, dg_f, tau_f), outs):
             host[...] = t.cpu().numpy()
 
+    def shift_simulation_window_x(self, *args):
+        """Oracle argument order (fields, n_shift, T_amb, cp_rho, rho0, nz_solid,
+        nx, ny, nz) through the reference-signature wrapper."""
+        from waam_solver_b200 import kernels
+        fields = list(args[:24])
+        n_shift, T_amb, cp_rho, rho0, nz_solid, nx, ny, nz = args[24:]
+        dev = [self._up(a) for a in fields]
+        kernels.shift_simulation_window_x(n_shift, *dev, T_amb, cp_rho, rho0, nz_solid, 1, 2, 0,
+                                          nx, ny, nz)
+        torch.cuda.synchronize()
+        self.launched.append("shift_simulation_window_x")
+        for host, t in zip(fields, dev):
+            host[...] = t.cpu().numpy()
+
     def surface_height_at(self, phi, flags, nx, ny, nz, i0, j0, nz_fallback):
         out = torch.zeros((), dtype=torch.float32, device=self.device)
         tp, tf = self._up(phi), self._up(flags)

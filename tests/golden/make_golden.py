@@ -509,6 +509,36 @@ def c_tail_var(tw, g):
     return a
 
 
+SHIFT_FIELDS = ["T", "H", "f_l", "phi", "flags", "T_max", "T_prev", "dT_dt", "time_above_800_s",
+                "time_above_1100_s", "time_above_solidus_s", "rho", "ux", "uy", "uz", "Fx", "Fy",
+                "Fz"] + PROP_FIELDS + ["f_a", "f_b"]
+
+
+def shift_setup(tw, g):
+    """Every shifted field distinct and non-zero (kernels.py:2620-2723 moves 22
+    scalar fields and both population buffers)."""
+    refresh(tw, g)
+    rng = np.random.default_rng(77)
+    for name in ("T_max", "T_prev", "dT_dt", "time_above_800_s", "time_above_1100_s",
+                 "time_above_solidus_s", "Fx", "Fy", "Fz"):
+        fld = getattr(g, name)
+        fld.from_numpy(rng.uniform(-1.0, 2.0, fld.shape).astype(np.float32))
+    fb = g.f_b.to_numpy()
+    g.f_b.from_numpy((fb * rng.uniform(0.9, 1.1, fb.shape)).astype(np.float32))
+
+
+def c_shift(tw, g):
+    a = scal(tw)
+    a.update(n_shift=3, T_amb=300.0, rho0=1.0)
+    K.shift_simulation_window_x(
+        3, g.f_a, g.f_b, g.T, g.H, g.f_l, g.phi, g.flags, g.T_max, g.T_prev, g.dT_dt,
+        g.time_above_800_s, g.time_above_1100_s, g.time_above_solidus_s, g.rho, g.ux, g.uy, g.uz,
+        g.Fx, g.Fy, g.Fz, g.cp_rho_field, g.alpha_lu_field, g.dgamma_lu_field, g.tau_field,
+        300.0, tw.cp_rho, 1.0, tw.nz_solid, g.FLAG_SOLID, g.FLAG_GAS, g.FLAG_FLUID,
+        g.nx, g.ny, g.nz)
+    return a
+
+
 def c_reset(tw, g):
     a = scal(tw)
     tw.reset()
@@ -557,6 +587,7 @@ def kernel_cases():
                 twin_kw=tb, extra_in=props_setup)
     kernel_case("tail_var", c_tail_var, base + ["ux", "uy", "uz"] + PROP_FIELDS, seed=21,
                 twin_kw=tb, extra_in=props_setup)
+    kernel_case("shift", c_shift, SHIFT_FIELDS, seed=24, twin_kw=tb, extra_in=shift_setup)
     kernel_case("reset", c_reset, base + ["rho", "ux", "uy", "uz", "f_a", "f_b", "T_max",
                                           "T_prev", "dT_dt", "time_above_800_s", "Fx", "Fx_snap"])
 

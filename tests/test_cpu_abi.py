@@ -46,9 +46,9 @@ def test_ctypes_struct_layouts_match_the_library():
     lib = _native.lib()
     for which, cls in enumerate((_native.WaamFields, _native.WaamStepParams,
                                  _native.WaamMaterialTables, _native.WaamTelemetry,
-                                 _native.WaamProbeSet)):
+                                 _native.WaamProbeSet, _native.WaamShiftPlane)):
         assert lib.waam_struct_size(which) == ctypes.sizeof(cls), cls.__name__
-    assert lib.waam_struct_size(5) == 0
+    assert lib.waam_struct_size(6) == 0
 
 
 @pytest.mark.parametrize("call", [

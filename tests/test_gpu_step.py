@@ -257,3 +257,38 @@ def test_table_path_operators_equal_fused():
         out.append(tw.grid.state_dict())
     steps.compare_state("operators vs fused (tables)", out[0], out[1],
                         fields=steps.FIELDS + steps.PROP_FIELDS)
+
+
+@pytest.mark.parametrize("kind,tables", [("c1", False), ("c2", True)])
+def test_moving_window_matches_oracle(kind, tables):
+    """enable_moving_window (twin.py:599-631): the torch crosses the trigger, all
+    fields (and the tracers) move back in one launch, the run continues in the
+    window's coordinates; every step against the oracle."""
+    shape = (40, 24, 24)
+    more = dict(enable_moving_window=True)
+    if tables:
+        more.update(material=_table_material(), enable_heat_loss=True)
+    tw, ot, dx = _config_twins(kind, *shape, **more)
+    import state_gen
+    st = state_gen.seeded_state(*shape, seed=13, nz_solid=tw.nz_solid)
+    st["read_is_a"] = True
+    tw.grid.load_state({k: v for k, v in st.items() if k != "nz_solid"})
+    ot.load({k: v for k, v in st.items() if k != "nz_solid"})
+    if kind == "c2":
+        tw._last_droplet_time = -1.0
+        ot.last_drop = -1.0
+    y = (shape[1] // 2) * dx
+    fields = steps.FIELDS + (steps.PROP_FIELDS if tables else [])
+    for s in range(10):
+        x = 19.0 * dx + s * 0.25 * dx
+        tw.step(x, y, True)
+        ot.step(x, y, True)
+        torch.cuda.synchronize()
+        assert tw._window_offset_x_m == pytest.approx(ot.window_offset, abs=1e-15)
+        steps.compare_state("window step %d" % s, tw.grid.state_dict(), ot.s, fields=fields)
+    assert tw._window_offset_x_m > 0.0
+    if kind == "c2":
+        g = tw.grid
+        assert np.array_equal(g.porosity_active.cpu().numpy(), ot.s["porosity_active"])
+        steps.compare("tracers", g.porosity_pos.cpu().numpy(), ot.s["porosity_pos"],
+                      "porosity_pos")

@@ -62,6 +62,15 @@ class WaamProbeSet(C.Structure):
     _fields_ = [("n_probes", C.c_int32), ("cell", C.c_int64 * MAX_PROBES)]
 
 
+MAX_SHIFT_PLANES = 64
+SHIFT_KEEP, SHIFT_CONST, SHIFT_BY_K = 0, 1, 2
+
+
+class WaamShiftPlane(C.Structure):
+    _fields_ = [("ptr", C.c_void_p), ("elem_bytes", C.c_int32), ("mode", C.c_int32),
+                ("below", C.c_uint32), ("above", C.c_uint32)]
+
+
 def _params_fields():
     """Field list of WaamStepParams, parsed from the header."""
     src = open(HEADER).read()
@@ -91,6 +100,7 @@ _CTYPES = {
     "const WaamStepParams*": C.POINTER(WaamStepParams), "const char*": C.c_char_p,
     "void* const*": C.c_void_p, "const WaamMaterialTables*": C.POINTER(WaamMaterialTables),
     "WaamTelemetry*": C.c_void_p, "const WaamProbeSet*": C.POINTER(WaamProbeSet),
+    "const WaamShiftPlane*": C.c_void_p,
 }
 
 

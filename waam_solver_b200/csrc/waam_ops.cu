@@ -707,6 +707,7 @@ size_t waam_struct_size(int which) {
         case 2: return sizeof(WaamMaterialTables);
         case 3: return sizeof(WaamTelemetry);
         case 4: return sizeof(WaamProbeSet);
+        case 5: return sizeof(WaamShiftPlane);
         default: return 0;
     }
 }

@@ -862,3 +862,62 @@ def bead_height_k(flags, nz_solid, out):
     """Max k of SOLID cells at or above nz_solid into the 0-d int32 ``out`` (-1: none)."""
     nx, ny, nz = _dims(flags)
     _call("waam_bead_height", _i(flags), nx, ny, nz, int(nz_solid), _i(out), _stream())
+
+
+# -------------------------------------------------------- moving window ----
+def _f32_bits(v):
+    import numpy as np
+    return int(np.array([v], dtype=np.float32).view(np.uint32)[0])
+
+
+def _pop_reset_bits(t, q, rho0):
+    """Raw bits of the reset population W[q] * rho0 in the storage of ``t``."""
+    import numpy as np
+    feq = np.float32(_W[q]) * np.float32(rho0)
+    if t.dtype == torch.float32:
+        return _f32_bits(feq)
+    off = np.float32(feq - np.float32(_W[q]))
+    h = torch.tensor([float(off)], dtype=torch.float32).to(t.dtype).view(torch.int16)
+    return int(h.item()) & 0xFFFF
+
+
+def shift_simulation_window_x(n_shift, f_a, f_b, T, H, f_l, phi, flags, T_max, T_prev, dT_dt,
+                              time_above_800, time_above_1100, time_above_solidus, rho, ux, uy,
+                              uz, Fx, Fy, Fz, cp_rho_field, alpha_lu_field, dgamma_lu_field,
+                              tau_field, T_amb, cp_rho, rho0, nz_solid, FLAG_SOLID, FLAG_GAS,
+                              FLAG_FLUID, nx, ny, nz):
+    """kernels.py:2620-2723 in one launch (every plane moves in place)."""
+    import numpy as np
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS, FLAG_FLUID=FLAG_FLUID)
+    n = int(nx) * int(ny) * int(nz)
+    planes = []
+
+    def add(t, mode, below=0, above=0, elem=4):
+        planes.append(_native.WaamShiftPlane(t.data_ptr(), elem, mode, below, above))
+
+    C_, K_, B_ = _native.SHIFT_CONST, _native.SHIFT_KEEP, _native.SHIFT_BY_K
+    amb = _f32_bits(T_amb)
+    for t, mode, below, above in (
+            (T, C_, amb, 0), (H, C_, _f32_bits(np.float32(cp_rho) * np.float32(T_amb)), 0),
+            (f_l, C_, 0, 0), (phi, B_, _f32_bits(1.0), 0), (T_max, C_, amb, 0),
+            (T_prev, C_, amb, 0), (dT_dt, C_, 0, 0), (time_above_800, C_, 0, 0),
+            (time_above_1100, C_, 0, 0), (time_above_solidus, C_, 0, 0),
+            (rho, C_, _f32_bits(rho0), 0), (ux, C_, 0, 0), (uy, C_, 0, 0), (uz, C_, 0, 0),
+            (Fx, C_, 0, 0), (Fy, C_, 0, 0), (Fz, C_, 0, 0), (cp_rho_field, K_, 0, 0),
+            (alpha_lu_field, K_, 0, 0), (dgamma_lu_field, K_, 0, 0), (tau_field, K_, 0, 0)):
+        _f(t, n)
+        add(t, mode, below, above)
+    _i(flags, n)
+    add(flags, B_, int(FLAG_SOLID), int(FLAG_GAS))
+    for buf in (f_a, f_b):
+        _pop(buf, 19 * n)
+        elem = buf.element_size()
+        for q in range(19):
+            add(buf[q], C_, _pop_reset_bits(buf, q, rho0), 0, elem)
+    arr = (_native.WaamShiftPlane * len(planes))(*planes)
+    _call("waam_shift_window_x", ctypes.cast(arr, ctypes.c_void_p), len(planes), int(n_shift),
+          int(nx), int(ny), int(nz), int(nz_solid), _stream())
+
+
+def shift_tracers_x(pos, max_tracers, shift_m):
+    _call("waam_shift_tracers_x", _f(pos), int(max_tracers), float(shift_m), _stream())

@@ -9,6 +9,7 @@ surface_height_at = kernels.surface_height_at
 apply_contact_angle_phi_bc = kernels.apply_contact_angle_phi_bc
 remelt_hot_solid = kernels.remelt_hot_solid
 remelt_hot_solid_scalar = kernels.remelt_hot_solid_scalar
+shift_simulation_window_x = kernels.shift_simulation_window_x
 
 
 def solidify_cooled_metal(T, f_l, phi, flags, ux, uy, uz, T_solidus, zero_velocity, FLAG_SOLID,
@@ -21,5 +22,5 @@ def solidify_cooled_metal(T, f_l, phi, flags, ux, uy, uz, T_solidus, zero_veloci
 __all__ = [
     "advect_phi", "reinitialize_phi", "update_flags_from_phi", "sync_phi_liquid_fraction",
     "surface_height_at", "solidify_cooled_metal", "apply_contact_angle_phi_bc",
-    "remelt_hot_solid", "remelt_hot_solid_scalar",
+    "remelt_hot_solid", "remelt_hot_solid_scalar", "shift_simulation_window_x",
 ]

@@ -8,6 +8,7 @@ instead of silently changing the physics.
 """
 from __future__ import annotations
 
+import logging
 import math
 
 import numpy as np
@@ -27,6 +28,7 @@ from .physics.weld_forces import arc_pressure_peak_pa, droplet_impact_velocity_m
 from .torch_path import TorchPathDriver, clamp_torch_to_domain, parse_torch_path
 
 RHO_LATTICE = 1.0
+log = logging.getLogger("waam_solver_b200")
 
 
 class WAAMTwin:
@@ -60,8 +62,6 @@ class WAAMTwin:
             raise ValueError("arc_sigma_mm must be > 0, got %s" % arc_sigma_mm)
         if contact_angle_deg is not None and not 0.0 < contact_angle_deg < 180.0:
             raise ValueError("contact_angle_deg must be in (0, 180), got %s" % contact_angle_deg)
-        if enable_moving_window:
-            raise NotImplementedError("moving window is not supported by this backend")
         self.mat = material if isinstance(material, MaterialProps) else load_material(material, high_sulphur)
         self.Q_w = arc_power_W
         self.eta = arc_efficiency
@@ -162,6 +162,7 @@ class WAAMTwin:
         self._sim_origin_offset_y_m = 0.0
         self._last_torch_pos_m = None
         self._torch_dir_xyz = (1.0, 0.0, 0.0)
+        self._warned_zero_wire_feed = False
         self._last_arc_ijk = None
         self.step_mode = step_mode
         # non-droplet fused steps replay a captured CUDA graph of the step
@@ -277,6 +278,8 @@ class WAAMTwin:
         self._torch_dir_xyz = (1.0, 0.0, 0.0)
         self._lorentz_warm = False
         self._lorentz_unconverged_streak = 0
+        self._bead_height_m = 0.0
+        self._warned_zero_wire_feed = False
         g.deposit_vol_buf.zero_()
         g.deposit_real_buf.zero_()
         g._tracers_live = False
@@ -292,10 +295,38 @@ class WAAMTwin:
             if norm > 1e-12:
                 self._torch_dir_xyz = (d[0] / norm, d[1] / norm, d[2] / norm)
         self._last_torch_pos_m = (torch_x_m, torch_y_m, z_now)
+        if (is_welding and self.droplet_freq > 0 and self.wire_feed_m_s <= 0.0
+                and not self._warned_zero_wire_feed):
+            self._warned_zero_wire_feed = True
+            log.warning("[WAAMTwin] welding step with wire_feed_m_s == 0: no metal will be "
+                        "deposited; set twin.wire_feed_m_s")
+        if self.enable_moving_window:
+            self._maybe_shift_window(torch_x_m)
         sim_x = torch_x_m - self._window_offset_x_m - self._sim_origin_offset_x_m
         sim_y = torch_y_m - self._sim_origin_offset_y_m
         coupled_step(self, sim_x, sim_y, is_welding, torch_z_m)
         self._check_strict_mode()
+
+    def _maybe_shift_window(self, torch_x_world):
+        """twin.py:599-631: once the torch passes 62 % of the window, move every
+        field max(8, nx // 10) cells back (one launch) and the tracers with it."""
+        g = self.grid
+        sim_x = torch_x_world - self._window_offset_x_m
+        if sim_x < 0.62 * (g.nx - 8) * g.dx:
+            return
+        n_shift = max(8, g.nx // 10)
+        kernels.shift_simulation_window_x(
+            n_shift, g.f_a, g.f_b, g.T, g.H, g.f_l, g.phi, g.flags, g.T_max, g.T_prev, g.dT_dt,
+            g.time_above_800_s, g.time_above_1100_s, g.time_above_solidus_s, g.rho, g.ux, g.uy,
+            g.uz, g.Fx, g.Fy, g.Fz, g.cp_rho_field, g.alpha_lu_field, g.dgamma_lu_field,
+            g.tau_field, self.T_amb, self.cp_rho, RHO_LATTICE, self.nz_solid, g.FLAG_SOLID,
+            g.FLAG_GAS, g.FLAG_FLUID, g.nx, g.ny, g.nz)
+        self._window_offset_x_m += n_shift * g.dx
+        kernels.shift_tracers_x(g.porosity_pos, g.max_tracers, n_shift * g.dx)
+        # F may now be non-zero outside the active cells of the fused step
+        g._forces_dirty = True
+        log.info("[WAAMTwin] Moving window shift -%d cells  offset=%.2fmm", n_shift,
+                 self._window_offset_x_m * 1e3)
 
     def _check_strict_mode(self):
         if not self.strict_mode:
