@@ -38,7 +38,7 @@ int waam_abi_version(void);
 size_t waam_workspace_bytes(int64_t n);
 /* sizeof of the ABI structs, for FFI layout checks: 0 WaamFields,
  * 1 WaamStepParams, 2 WaamMaterialTables, 3 WaamTelemetry, 4 WaamProbeSet,
- * 5 WaamShiftPlane (0 for any other value) */
+ * 5 WaamShiftPlane, 6 WaamExportChannel (0 for any other value) */
 size_t waam_struct_size(int which);
 
 /* ---- operator API: one entry per reference Taichi kernel ---------------- */
@@ -424,6 +424,42 @@ int waam_shift_window_x(const WaamShiftPlane* planes, int n_planes, int n_shift,
                         int nz, int nz_solid, void* stream);
 /* twin.py:624-626: pos[:, 0] -= shift_m for every tracer slot */
 int waam_shift_tracers_x(float* pos, int max_tracers, float shift_m, void* stream);
+
+/* ---- export (export/vtk_io.py; kernels.py:3354-3418) ---------------------- */
+
+/* kernels.py:3354-3376 compute_curvature_field: kappa = -div(n) (Brackbill) on
+ * non-gas interior cells with |grad phi| >= 1e-6, else 0 */
+int waam_compute_curvature_field(const float* phi, const int32_t* flags, float* kappa_out, int nx,
+                                 int ny, int nz, void* stream);
+/* kernels.py:3379-3418 compute_vorticity_magnitude: |curl u| / dt [1/s] on
+ * non-gas cells (dx is accepted and unused, as in the reference) */
+int waam_compute_vorticity_magnitude(const float* ux, const float* uy, const float* uz,
+                                     const int32_t* flags, float* vort_out, int nx, int ny, int nz,
+                                     float dx, float dt, void* stream);
+
+#define WAAM_MAX_EXPORT_CHANNELS 48
+/* channel operations, float32 arithmetic in the written order */
+#define WAAM_EXPORT_COPY 0       /* src0 */
+#define WAAM_EXPORT_COPY_I32 1   /* src0 as int32 */
+#define WAAM_EXPORT_ADD 2        /* src0 + a */
+#define WAAM_EXPORT_NEG 3        /* -src0 */
+#define WAAM_EXPORT_LU_VEL 4     /* src0 * a / b            (a = dx, b = dt) */
+#define WAAM_EXPORT_LU_ACC 5     /* src0 * a / b / b */
+#define WAAM_EXPORT_SPEED 6      /* |(src0, src1, src2) * a / b| */
+#define WAAM_EXPORT_ACC_MAG 7    /* |(src0, src1, src2) * a / b / b| */
+#define WAAM_EXPORT_PRESSURE 8   /* (src0 - 1) * a * b * c */
+#define WAAM_EXPORT_MUSHY 9      /* 1 where 0.05 < src0 < 0.95, else 0 */
+typedef struct WaamExportChannel {
+    int32_t op;
+    float a, b, c;
+    const void* src[3];
+} WaamExportChannel;
+/* One launch: channel q of the output (out + q * n, 4-byte elements) holds the
+ * channel's value at every cell in VTK cell order, index i + nx * (j + ny * k).
+ * `channels` is a host array (n_channels <= WAAM_MAX_EXPORT_CHANNELS); `out`
+ * is device memory of n_channels * nx * ny * nz * 4 bytes. */
+int waam_export_pack(const WaamExportChannel* channels, int n_channels, int nx, int ny, int nz,
+                     void* out, void* stream);
 
 /* ---- fused step: the B200 pipeline of solvers/coupled_step.py:73-464 ----- */
 

@@ -83,6 +83,8 @@ _SIGS = {
     "wo_advect_tracers": ([_F, _I, _F, _F, _F, _F, _I, _i, _i, _i, _f, _i], None),
     "wo_shift_simulation_window_x": ([_F] * 6 + [_I] + [_F] * 17 + [_i, _f, _f, _f, _i, _i, _i,
                                                                     _i], None),
+    "wo_compute_curvature_field": ([_F, _I, _F, _i, _i, _i], None),
+    "wo_compute_vorticity_magnitude": ([_F, _F, _F, _I, _F, _i, _i, _i, _f], None),
     "wo_num_threads": ([], C.c_int),
     "wo_expf_array": ([_F, _F, _l], None),
     "wo_set_num_threads": ([C.c_int], None),

@@ -587,6 +587,34 @@ static inline void phi_normal(const float* phi, int nx, int ny, int nz, int i, i
     *g = gm;
 }
 
+/* kernels.py:800-855 _brackbill_curvature_at: -div of the neighbours' unit
+ * normals (the centre normal where a neighbour has no gradient) */
+static float brackbill_kappa(const float* phi, int nx, int ny, int nz, int i, int j, int k,
+                             float* g0) {
+    const float eps = 1e-6f;
+    float n0x, n0y, n0z;
+    phi_normal(phi, nx, ny, nz, i, j, k, &n0x, &n0y, &n0z, g0);
+    float kappa = 0.0f;
+    if (*g0 >= eps) {
+        float a, b, gp, gm, gp2, gm2, gp3, gm3, nxp, nxm, nyp, nym, nzp, nzm;
+        phi_normal(phi, nx, ny, nz, imin(i + 1, nx - 1), j, k, &nxp, &a, &b, &gp);
+        phi_normal(phi, nx, ny, nz, imax(i - 1, 0), j, k, &nxm, &a, &b, &gm);
+        phi_normal(phi, nx, ny, nz, i, imin(j + 1, ny - 1), k, &a, &nyp, &b, &gp2);
+        phi_normal(phi, nx, ny, nz, i, imax(j - 1, 0), k, &a, &nym, &b, &gm2);
+        phi_normal(phi, nx, ny, nz, i, j, imin(k + 1, nz - 1), &a, &b, &nzp, &gp3);
+        phi_normal(phi, nx, ny, nz, i, j, imax(k - 1, 0), &a, &b, &nzm, &gm3);
+        if (gp < eps) nxp = n0x;
+        if (gm < eps) nxm = n0x;
+        if (gp2 < eps) nyp = n0y;
+        if (gm2 < eps) nym = n0y;
+        if (gp3 < eps) nzp = n0z;
+        if (gm3 < eps) nzm = n0z;
+        float div_n = 0.5f * (nxp - nxm) + 0.5f * (nyp - nym) + 0.5f * (nzp - nzm);
+        kappa = -div_n;
+    }
+    return kappa;
+}
+
 /* kernels.py:858-926 compute_csf_tension (+ 681-855 helpers) */
 void wo_compute_csf_tension(const float* phi, const int32_t* flags, float* Fx, float* Fy,
                             float* Fz, int nx, int ny, int nz, float gamma_lu, int wetting,
@@ -600,27 +628,8 @@ void wo_compute_csf_tension(const float* phi, const int32_t* flags, float* Fx, f
                 int64_t c = IX(i, j, k);
                 if (flags[c] == SOLID || flags[c] == GAS) continue;
                 if (i < 1 || j < 1 || k < 1 || i > nx - 2 || j > ny - 2 || k > nz - 2) continue;
-                float n0x, n0y, n0z, g0;
-                phi_normal(phi, nx, ny, nz, i, j, k, &n0x, &n0y, &n0z, &g0);
-                float kappa = 0.0f;
-                if (g0 >= eps) {
-                    float a, b, d, gp, gm, gp2, gm2, gp3, gm3, nxp, nxm, nyp, nym, nzp, nzm;
-                    phi_normal(phi, nx, ny, nz, imin(i + 1, nx - 1), j, k, &nxp, &a, &b, &gp);
-                    phi_normal(phi, nx, ny, nz, imax(i - 1, 0), j, k, &nxm, &a, &b, &gm);
-                    phi_normal(phi, nx, ny, nz, i, imin(j + 1, ny - 1), k, &a, &nyp, &b, &gp2);
-                    phi_normal(phi, nx, ny, nz, i, imax(j - 1, 0), k, &a, &nym, &b, &gm2);
-                    phi_normal(phi, nx, ny, nz, i, j, imin(k + 1, nz - 1), &a, &b, &nzp, &gp3);
-                    phi_normal(phi, nx, ny, nz, i, j, imax(k - 1, 0), &a, &b, &nzm, &gm3);
-                    (void)d;
-                    if (gp < eps) nxp = n0x;
-                    if (gm < eps) nxm = n0x;
-                    if (gp2 < eps) nyp = n0y;
-                    if (gm2 < eps) nym = n0y;
-                    if (gp3 < eps) nzp = n0z;
-                    if (gm3 < eps) nzm = n0z;
-                    float div_n = 0.5f * (nxp - nxm) + 0.5f * (nyp - nym) + 0.5f * (nzp - nzm);
-                    kappa = -div_n;
-                }
+                float g0;
+                float kappa = brackbill_kappa(phi, nx, ny, nz, i, j, k, &g0);
                 float gmag = g0;
                 if (gmag < eps) continue;
                 float dpx = 0.5f * (phi[IX(imin(i + 1, nx - 1), j, k)] - phi[IX(imax(i - 1, 0), j, k)]);
@@ -1663,5 +1672,50 @@ void wo_shift_simulation_window_x(float* f_a, float* f_b, float* T, float* H, fl
                     f_a[q * n + c] = feq;
                     f_b[q * n + c] = feq;
                 }
+            }
+}
+
+/* kernels.py:3354-3376 compute_curvature_field */
+void wo_compute_curvature_field(const float* phi, const int32_t* flags, float* kappa, int nx,
+                                int ny, int nz) {
+#pragma omp parallel for collapse(2)
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                int64_t c = IX(i, j, k);
+                kappa[c] = 0.0f;
+                if (flags[c] == GAS) continue;
+                if (i < 1 || j < 1 || k < 1 || i > nx - 2 || j > ny - 2 || k > nz - 2) continue;
+                float g0;
+                float kv = brackbill_kappa(phi, nx, ny, nz, i, j, k, &g0);
+                if (g0 >= 1e-6f) kappa[c] = kv;
+            }
+}
+
+/* kernels.py:3379-3418 compute_vorticity_magnitude */
+void wo_compute_vorticity_magnitude(const float* ux, const float* uy, const float* uz,
+                                    const int32_t* flags, float* vort, int nx, int ny, int nz,
+                                    float dt) {
+    const float scale = 1.0f / (dt + 1e-12f);
+#pragma omp parallel for collapse(2)
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                int64_t c = IX(i, j, k);
+                vort[c] = 0.0f;
+                if (flags[c] == GAS) continue;
+                int ip = imin(i + 1, nx - 1), im = imax(i - 1, 0);
+                int jp = imin(j + 1, ny - 1), jm = imax(j - 1, 0);
+                int kp = imin(k + 1, nz - 1), km = imax(k - 1, 0);
+                float duz_dy = 0.5f * (uz[IX(i, jp, k)] - uz[IX(i, jm, k)]);
+                float duy_dz = 0.5f * (uy[IX(i, j, kp)] - uy[IX(i, j, km)]);
+                float dux_dz = 0.5f * (ux[IX(i, j, kp)] - ux[IX(i, j, km)]);
+                float duz_dx = 0.5f * (uz[IX(ip, j, k)] - uz[IX(im, j, k)]);
+                float duy_dx = 0.5f * (uy[IX(ip, j, k)] - uy[IX(im, j, k)]);
+                float dux_dy = 0.5f * (ux[IX(i, jp, k)] - ux[IX(i, jm, k)]);
+                float wx = (duz_dy - duy_dz) * scale;
+                float wy = (dux_dz - duz_dx) * scale;
+                float wz = (duy_dx - dux_dy) * scale;
+                vort[c] = sqrtf(wx * wx + wy * wy + wz * wz);
             }
 }

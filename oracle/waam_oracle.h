@@ -188,6 +188,14 @@ void wo_shift_simulation_window_x(float* f_a, float* f_b, float* T, float* H, fl
                                   float* dg_f, float* tau_f, int n_shift, float T_amb,
                                   float cp_rho, float rho0, int nz_solid, int nx, int ny, int nz);
 
+/* kernels.py:3354-3376 compute_curvature_field */
+void wo_compute_curvature_field(const float* phi, const int32_t* flags, float* kappa, int nx,
+                                int ny, int nz);
+/* kernels.py:3379-3418 compute_vorticity_magnitude */
+void wo_compute_vorticity_magnitude(const float* ux, const float* uy, const float* uz,
+                                    const int32_t* flags, float* vort, int nx, int ny, int nz,
+                                    float dt);
+
 #ifdef __cplusplus
 }
 #endif

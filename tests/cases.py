@@ -47,7 +47,7 @@ def full_inputs(name):
                 "contact_s5": 5, "forces_wet": 6, "csf": 7, "csf_wet": 8, "collide_srt": 9,
                 "tail": 10, "heat_loss": 11, "surface_height": 12, "deposit": 13,
                 "lorentz": 14, "tracers": 15, "refresh": 16, "thermal_var": 17, "phase_var": 18,
-                "forces_var": 19, "srt_var": 20, "tail_var": 21, "shift": 24}
+                "forces_var": 19, "srt_var": 20, "tail_var": 21, "shift": 24, "derived": 25}
     grids = [v.shape[-3:] for v in ins.values() if v.ndim >= 3 and v.shape[-1] != 3]
     nx, ny, nz = grids[0] if grids else (13, 11, 12)   # tracer-only cases: the kernel-case grid
     st = state_gen.seeded_state(nx, ny, nz, seed=seed_map.get(name, 0))
@@ -272,6 +272,10 @@ def run_case(be, name, st, a):
                                   st["uy"], st["uz"], st["cp_rho_field"], nx, ny, nz, a["arc_i"],
                                   a["arc_j"], a["arc_k"], 1.0, 0.0, 0.0, a["lookback"],
                                   a["T_freeze"], a["T_solidus_t"])
+    elif name == "derived":
+        be.compute_curvature_field(st["phi"], st["flags"], st["kappa_field"], nx, ny, nz)
+        be.compute_vorticity_magnitude(st["ux"], st["uy"], st["uz"], st["flags"],
+                                       st["vorticity_mag"], nx, ny, nz, a["dt"])
     elif name == "shift":
         be.shift_simulation_window_x(
             st["f_a"], st["f_b"], st["T"], st["H"], st["f_l"], st["phi"], st["flags"],
@@ -302,7 +306,7 @@ CASES = ["inject_gauss", "inject_goldak", "ceiling", "thermal", "thermal_s2", "p
          "tmax_cool", "vof", "vof_wet", "contact", "contact_s5", "forces", "forces_wet", "csf",
          "csf_wet", "collide_mrt", "collide_srt", "stream", "tail", "heat_loss",
          "surface_height", "deposit", "lorentz", "tracers", "refresh", "thermal_var",
-         "phase_var", "forces_var", "srt_var", "tail_var", "shift", "reset"]
+         "phase_var", "forces_var", "srt_var", "tail_var", "shift", "derived", "reset"]
 
 
 def check_case(be, name):

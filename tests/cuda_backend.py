@@ -111,6 +111,11 @@ class CudaBackend:
         for host, t in zip((cp_f, alpha_f, dg_f, tau_f), outs):
             host[...] = t.cpu().numpy()
 
+    def compute_vorticity_magnitude(self, ux, uy, uz, flags, vort, nx, ny, nz, dt):
+        """The C entry also takes dx (unused, as in the reference)."""
+        self._run("compute_vorticity_magnitude", [ux, uy, uz, flags, vort, nx, ny, nz, 0.0, dt],
+                  None)
+
     def shift_simulation_window_x(self, *args):
         """Oracle argument order (fields, n_shift, T_amb, cp_rho, rho0, nz_solid,
         nx, ny, nz) through the reference-signature wrapper."""

@@ -539,6 +539,21 @@ def c_shift(tw, g):
     return a
 
 
+def c_derived(tw, g):
+    a = scal(tw)
+    g.ensure_export_buffers()
+    K.compute_curvature_field(g.phi, g.flags, g.kappa_field, g.FLAG_GAS, g.nx, g.ny, g.nz)
+    K.compute_vorticity_magnitude(g.ux, g.uy, g.uz, g.flags, g.vorticity_mag, g.dx, g.dt,
+                                  g.FLAG_GAS, g.nx, g.ny, g.nz)
+    return a
+
+
+def derived_setup(tw, g):
+    g.ensure_export_buffers()
+    g.kappa_field.from_numpy(np.full((g.nx, g.ny, g.nz), 7.0, np.float32))
+    g.vorticity_mag.from_numpy(np.full((g.nx, g.ny, g.nz), 7.0, np.float32))
+
+
 def c_reset(tw, g):
     a = scal(tw)
     tw.reset()
@@ -588,6 +603,8 @@ def kernel_cases():
     kernel_case("tail_var", c_tail_var, base + ["ux", "uy", "uz"] + PROP_FIELDS, seed=21,
                 twin_kw=tb, extra_in=props_setup)
     kernel_case("shift", c_shift, SHIFT_FIELDS, seed=24, twin_kw=tb, extra_in=shift_setup)
+    kernel_case("derived", c_derived, ["kappa_field", "vorticity_mag"], seed=25,
+                extra_in=derived_setup)
     kernel_case("reset", c_reset, base + ["rho", "ux", "uy", "uz", "f_a", "f_b", "T_max",
                                           "T_prev", "dT_dt", "time_above_800_s", "Fx", "Fx_snap"])
 

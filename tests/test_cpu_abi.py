@@ -46,9 +46,10 @@ def test_ctypes_struct_layouts_match_the_library():
     lib = _native.lib()
     for which, cls in enumerate((_native.WaamFields, _native.WaamStepParams,
                                  _native.WaamMaterialTables, _native.WaamTelemetry,
-                                 _native.WaamProbeSet, _native.WaamShiftPlane)):
+                                 _native.WaamProbeSet, _native.WaamShiftPlane,
+                                 _native.WaamExportChannel)):
         assert lib.waam_struct_size(which) == ctypes.sizeof(cls), cls.__name__
-    assert lib.waam_struct_size(6) == 0
+    assert lib.waam_struct_size(7) == 0
 
 
 @pytest.mark.parametrize("call", [

@@ -71,6 +71,16 @@ class WaamShiftPlane(C.Structure):
                 ("below", C.c_uint32), ("above", C.c_uint32)]
 
 
+MAX_EXPORT_CHANNELS = 48
+(EXPORT_COPY, EXPORT_COPY_I32, EXPORT_ADD, EXPORT_NEG, EXPORT_LU_VEL, EXPORT_LU_ACC, EXPORT_SPEED,
+ EXPORT_ACC_MAG, EXPORT_PRESSURE, EXPORT_MUSHY) = range(10)
+
+
+class WaamExportChannel(C.Structure):
+    _fields_ = [("op", C.c_int32), ("a", C.c_float), ("b", C.c_float), ("c", C.c_float),
+                ("src", C.c_void_p * 3)]
+
+
 def _params_fields():
     """Field list of WaamStepParams, parsed from the header."""
     src = open(HEADER).read()
@@ -100,7 +110,7 @@ _CTYPES = {
     "const WaamStepParams*": C.POINTER(WaamStepParams), "const char*": C.c_char_p,
     "void* const*": C.c_void_p, "const WaamMaterialTables*": C.POINTER(WaamMaterialTables),
     "WaamTelemetry*": C.c_void_p, "const WaamProbeSet*": C.POINTER(WaamProbeSet),
-    "const WaamShiftPlane*": C.c_void_p,
+    "const WaamShiftPlane*": C.c_void_p, "const WaamExportChannel*": C.c_void_p,
 }
 
 

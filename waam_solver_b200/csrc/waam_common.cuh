@@ -479,6 +479,35 @@ __device__ __forceinline__ void phi_normal(const Dims d, const float* __restrict
     g = gm;
 }
 
+// kernels.py:800-855 _brackbill_curvature_at: kappa = -div(n) of the unit
+// normals of the six neighbours (the centre normal where a neighbour has no
+// gradient); g0 = |grad phi| at the cell.  kappa = 0 when g0 < 1e-6.
+__device__ __forceinline__ float brackbill_kappa(const Dims d, const float* __restrict__ phi,
+                                                 int i, int j, int k, float& g0) {
+    const float eps = 1e-6f;
+    float n0x, n0y, n0z;
+    phi_normal(d, phi, i, j, k, n0x, n0y, n0z, g0);
+    float kappa = 0.0f;
+    if (g0 >= eps) {
+        float a, b, gp, gm, gp2, gm2, gp3, gm3, nxp, nxm, nyp, nym, nzp, nzm;
+        phi_normal(d, phi, imin(i + 1, d.nx - 1), j, k, nxp, a, b, gp);
+        phi_normal(d, phi, imax(i - 1, 0), j, k, nxm, a, b, gm);
+        phi_normal(d, phi, i, imin(j + 1, d.ny - 1), k, a, nyp, b, gp2);
+        phi_normal(d, phi, i, imax(j - 1, 0), k, a, nym, b, gm2);
+        phi_normal(d, phi, i, j, imin(k + 1, d.nz - 1), a, b, nzp, gp3);
+        phi_normal(d, phi, i, j, imax(k - 1, 0), a, b, nzm, gm3);
+        if (gp < eps) nxp = n0x;
+        if (gm < eps) nxm = n0x;
+        if (gp2 < eps) nyp = n0y;
+        if (gm2 < eps) nym = n0y;
+        if (gp3 < eps) nzp = n0z;
+        if (gm3 < eps) nzm = n0z;
+        float div_n = 0.5f * (nxp - nxm) + 0.5f * (nyp - nym) + 0.5f * (nzp - nzm);
+        kappa = -div_n;
+    }
+    return kappa;
+}
+
 // Force parameters (solvers/coupled_step.py:298-362)
 struct ForceParams {
     int csf, wetting, welding, hydro;
@@ -501,26 +530,8 @@ __device__ __forceinline__ void cell_forces(const Dims d, const ForceParams& P,
     int64_t c = d.idx(i, j, k);
     // kernels.py:858-926 compute_csf_tension
     if (P.csf && !(i < 1 || j < 1 || k < 1 || i > d.nx - 2 || j > d.ny - 2 || k > d.nz - 2)) {
-        float n0x, n0y, n0z, g0;
-        phi_normal(d, phi, i, j, k, n0x, n0y, n0z, g0);
-        float kappa = 0.0f;
-        if (g0 >= eps) {
-            float a, b, gp, gm, gp2, gm2, gp3, gm3, nxp, nxm, nyp, nym, nzp, nzm;
-            phi_normal(d, phi, imin(i + 1, d.nx - 1), j, k, nxp, a, b, gp);
-            phi_normal(d, phi, imax(i - 1, 0), j, k, nxm, a, b, gm);
-            phi_normal(d, phi, i, imin(j + 1, d.ny - 1), k, a, nyp, b, gp2);
-            phi_normal(d, phi, i, imax(j - 1, 0), k, a, nym, b, gm2);
-            phi_normal(d, phi, i, j, imin(k + 1, d.nz - 1), a, b, nzp, gp3);
-            phi_normal(d, phi, i, j, imax(k - 1, 0), a, b, nzm, gm3);
-            if (gp < eps) nxp = n0x;
-            if (gm < eps) nxm = n0x;
-            if (gp2 < eps) nyp = n0y;
-            if (gm2 < eps) nym = n0y;
-            if (gp3 < eps) nzp = n0z;
-            if (gm3 < eps) nzm = n0z;
-            float div_n = 0.5f * (nxp - nxm) + 0.5f * (nyp - nym) + 0.5f * (nzp - nzm);
-            kappa = -div_n;
-        }
+        float g0;
+        const float kappa = brackbill_kappa(d, phi, i, j, k, g0);
         float gmag = g0;
         if (gmag >= eps) {
             float dpx = 0.5f * (phi[d.idx(imin(i + 1, d.nx - 1), j, k)] - phi[d.idx(imax(i - 1, 0), j, k)]);

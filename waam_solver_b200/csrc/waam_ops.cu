@@ -708,6 +708,7 @@ size_t waam_struct_size(int which) {
         case 3: return sizeof(WaamTelemetry);
         case 4: return sizeof(WaamProbeSet);
         case 5: return sizeof(WaamShiftPlane);
+        case 6: return sizeof(WaamExportChannel);
         default: return 0;
     }
 }

@@ -921,3 +921,39 @@ def shift_simulation_window_x(n_shift, f_a, f_b, T, H, f_l, phi, flags, T_max, T
 
 def shift_tracers_x(pos, max_tracers, shift_m):
     _call("waam_shift_tracers_x", _f(pos), int(max_tracers), float(shift_m), _stream())
+
+
+# --------------------------------------------------------------- export ----
+def compute_curvature_field(phi, flags, kappa_out, FLAG_GAS, nx, ny, nz):
+    """kernels.py:3354-3376."""
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_compute_curvature_field", _f(phi, n), _i(flags, n), _f(kappa_out, n), int(nx),
+          int(ny), int(nz), _stream())
+
+
+def compute_vorticity_magnitude(ux, uy, uz, flags, vort_out, dx, dt, FLAG_GAS, nx, ny, nz):
+    """kernels.py:3379-3418."""
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _call("waam_compute_vorticity_magnitude", _f(ux, n), _f(uy, n), _f(uz, n), _i(flags, n),
+          _f(vort_out, n), int(nx), int(ny), int(nz), float(dx), float(dt), _stream())
+
+
+def export_pack(channels, nx, ny, nz, out):
+    """Pack channels (op, a, b, c, sources) into ``out`` (device, 4-byte
+    elements, len(channels) * nx * ny * nz) in VTK cell order, one launch."""
+    n = int(nx) * int(ny) * int(nz)
+    if len(channels) > _native.MAX_EXPORT_CHANNELS:
+        raise WaamError("at most %d export channels" % _native.MAX_EXPORT_CHANNELS)
+    if out.numel() * out.element_size() < 4 * n * len(channels) or not out.is_cuda:
+        raise WaamError("export staging buffer too small")
+    arr = (_native.WaamExportChannel * max(1, len(channels)))()
+    for q, (op, a, b, c, srcs) in enumerate(channels):
+        arr[q].op, arr[q].a, arr[q].b, arr[q].c = op, a, b, c
+        for s, t in enumerate(srcs):
+            if t.numel() != n or not t.is_contiguous() or t.element_size() != 4 or not t.is_cuda:
+                raise WaamError("export source must be a contiguous 4-byte CUDA field")
+            arr[q].src[s] = t.data_ptr()
+    _call("waam_export_pack", ctypes.cast(arr, ctypes.c_void_p), len(channels), int(nx), int(ny),
+          int(nz), out.data_ptr(), _stream())

@@ -391,6 +391,45 @@ class WAAMTwin:
             cx, cy = clamp(x, y)
             self.step(cx, cy, is_welding, torch_z_m=z)
 
+    # -- export (twin.py:701-869) --------------------------------------------
+    def export_haz_vtk(self, path="haz_map.vti"):
+        from .export import TIER_CORE, export_volume
+        return export_volume(self, path, tiers=(TIER_CORE,), crop_liquid=False)
+
+    def export_vtk(self, path="weld_pool.vti"):
+        return self.export_vtk_full(path, tiers=(0, 3), crop_liquid=False)
+
+    def export_vtk_full(self, path="weld_pool_full.vti", tiers=(0, 1, 2, 3), crop_liquid=False):
+        from .export import TIER_MAP, export_volume
+        return export_volume(self, path, tiers=tuple(TIER_MAP.get(t, t) for t in tiers),
+                             crop_liquid=crop_liquid)
+
+    def export_surface_vtk(self, path="bead_surface.vtp"):
+        from .export import export_surface
+        return export_surface(self, path, include_kappa=True)
+
+    def export_tracers_vtk(self, path="tracers.vtp"):
+        from .export import export_tracers
+        return export_tracers(self, path)
+
+    def export_npz(self, path="state.npz"):
+        from .export import export_npz
+        return export_npz(self, path)
+
+    def export_research_bundle(self, out_dir, tag=None, tiers=(0, 1, 3), include_surface=True,
+                               include_tracers=True, crop_liquid=False):
+        from .export import export_research_bundle
+        return export_research_bundle(self, out_dir, tag=tag, tiers=tiers,
+                                      include_surface=include_surface,
+                                      include_tracers=include_tracers,
+                                      job_path=getattr(self, "_job_path", None),
+                                      crop_liquid=crop_liquid)
+
+    def export_research_sequence(self, *args, **kwargs):
+        from .export import export_research_sequence
+        return export_research_sequence(self, *args, job_path=getattr(self, "_job_path", None),
+                                        **kwargs)
+
     # -- telemetry (twin.py:706-821) -----------------------------------------
     def telemetry_record(self):
         """Launch the pool reductions into the grid's device record (no sync);
