@@ -503,6 +503,15 @@ typedef struct WaamFields {
     float* alpha_f;
     float* dgamma_f;
     float* tau_f;
+    /* adjoint tape of the collision (null: off): for every active cell of
+     * the step, its index (tape_cells[t]) and its 19 pre-collision populations
+     * (tape_f[q * tape_cap + t], float32 storage only); *tape_count receives
+     * the number of active cells.  A step with more than tape_cap active
+     * cells writes none of them and sets *tape_count to -1. */
+    float* tape_f;
+    int32_t* tape_cells;
+    int32_t* tape_count;
+    int64_t tape_cap;
 } WaamFields;
 
 typedef struct WaamStepParams {
@@ -581,6 +590,46 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
 /* Number of kernels the fused stages launch (for launch accounting): stage 0
  * waam_step_pre, 1 waam_step_main, 2 waam_step_main_events. */
 int waam_step_launch_count(const WaamStepParams* p, int stage);
+
+/* ---- adjoint of the coupled step (reverse kernels, one step each) ---------- */
+/* The reverse step runs: waam_adj_stream, waam_adj_collide, waam_adj_combine,
+ * waam_adj_thermal, waam_adj_inject (see waam_solver_b200/adjoint.py).  All
+ * are gathers (no floating-point atomics); parameter sums are FP64 in a fixed
+ * order.  VOF, flags and the active set are the forward trajectory's. */
+
+/* stream transposed: lam_yp (in lam Y', out lam Y' + S^T lam X'), lam_xn (out:
+ * lam X' at SOLID cells, 0 elsewhere); flags of step n + 1 */
+int waam_adj_stream(float* lam_yp, const float* lam_xp, float* lam_xn, const int32_t* flags,
+                    int nx, int ny, int nz, void* stream);
+/* forces + MRT collision + Mach / force clamps at the taped active cells
+ * (WaamFields.tape_*), then the gather of the Marangoni T terms; ctb holds
+ * 6 floats per tape slot, map one int per cell (all -1 on entry and exit) */
+int waam_adj_collide(const WaamStepParams* p, const float* tape_f, const int32_t* tape_cells,
+                     const int32_t* tape_count, int64_t tape_cap, const float* phi,
+                     const float* T, const float* f_l, const int32_t* flags,
+                     const float* scalars, float* lam_yp, float* lam_xn, float* lam_ux,
+                     float* lam_uy, float* lam_uz, float* lam_fl, float* lam_T, float* ctb,
+                     int32_t* map, int nx, int ny, int nz, void* stream);
+/* lam_H += dT/dH lam_T + df_l/dH lam_f_l at H (step n + 1); lam_T = lam_f_l = 0 */
+int waam_adj_combine(const WaamStepParams* p, float* lam_H, float* lam_T, float* lam_fl,
+                     const float* H, const int32_t* flags, const float* phi, int64_t n,
+                     void* stream);
+/* thermal stage transposed: lam_H (step n + 1) -> lam_Hp (post-injection H of
+ * step n); lam_T and the velocity adjoints accumulate step n's terms;
+ * grad_hconv[0] += d/d h_conv (FP64).  mu: one float per cell of scratch. */
+int waam_adj_thermal(const WaamStepParams* p, const float* lam_H, float* lam_Hp, float* mu,
+                     float* lam_T, float* lam_ux, float* lam_uy, float* lam_uz, const float* Hp,
+                     const float* T, const float* ux, const float* uy, const float* uz,
+                     const int32_t* flags, int nx, int ny, int nz, double* grad_hconv,
+                     void* workspace, size_t workspace_bytes, void* stream);
+/* injection + ceiling transposed: lam_Hp -> lam_H (step n); sums[0..10] +=
+ * A, B_{af, ar, b, c, sigma}, D_{af, ar, b, c, sigma} (FP64) */
+int waam_adj_inject(const WaamStepParams* p, float* lam_H, const float* lam_Hp, const float* H,
+                    const float* f_l, const int32_t* flags, const float* scalars, int nx, int ny,
+                    int nz, double* sums, void* workspace, size_t workspace_bytes, void* stream);
+/* lam[cells[t]] += vals[t] for t < count (in order) */
+int waam_adj_scatter_add(float* lam, const int32_t* cells, const float* vals, int count,
+                         void* stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

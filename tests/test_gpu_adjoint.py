@@ -1,0 +1,238 @@
+"""The hand-written adjoint of the coupled step (waam_adjoint.cu, adjoint.py).
+
+* The stream transpose is exact: <lam, S y> = <S^T lam, y> on random data
+  with solid, gas and fluid cells and clamped faces.
+* One reverse step of the thermal chain (injection, advection-diffusion,
+  losses, phase) against central finite differences of one forward step,
+  in a random direction that stays clear of the forward's kinks (phase
+  boundaries, the enthalpy floor and ceiling).
+* The loss gradient (probe misfit + smooth width) for every parameter
+  against central finite differences (relative step 1e-3) of the forward
+  path, from a start state without cells at the kinks; the VOF-frozen
+  approximation reported with VOF on.
+* Determinism, checkpoint independence and the autograd wrapper.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import steps
+
+pytestmark = pytest.mark.gpu
+
+
+def _clean(st, tw, margin=25.0):
+    """Move cold cells of a seeded state clear of the enthalpy floor at T_amb."""
+    from waam_solver_b200 import kernels  # noqa: F401
+    m = steps.MATERIAL
+    cp_rho = m["rho"] * m["cp"]
+    T = st["T"]
+    cold = T < tw.T_amb + margin
+    T = np.where(cold, np.float32(tw.T_amb + margin), T).astype(np.float32)
+    st["T"] = T
+    st["H"] = np.where(cold, (np.float32(cp_rho) * T), st["H"]).astype(np.float32)
+    st["f_l"] = np.where(cold, np.float32(0.0), st["f_l"]).astype(np.float32)
+    return st
+
+
+def _twin(kind="goldak", vof=False, shape=(40, 24, 24), h_conv=3.0e5, clean=True, seed=21):
+    import state_gen
+    from waam_solver_b200 import WAAMTwin
+    from waam_solver_b200.materials import from_constants
+    from waam_solver_b200.physics.arc import Goldak3D
+    dx = 2.5e-4
+    mat = from_constants("m", steps.MATERIAL, contact_angle_deg=30.0)
+    tw = WAAMTwin(material=mat, nx=shape[0], ny=shape[1], nz=shape[2], dx=dx, max_tracers=64,
+                  use_srt=False, enable_vof=vof, travel_speed_m_s=0.008,
+                  heat_source="goldak" if kind == "goldak" else "gaussian2d",
+                  arc_power_W=3000.0, arc_efficiency=0.75, arc_sigma_mm=1.0, droplet_freq_hz=0.0,
+                  enable_heat_loss=True, enable_wetting=True, enable_csf_tension=True,
+                  enable_hydrostatic_gravity=True, h_conv=h_conv)
+    if kind == "goldak":
+        tw.arc_source = Goldak3D(ff=0.6, fr=1.4, a_front=4.0, a_rear=9.0, b=4.0, c=3.0)
+    tw.reset()
+    st = state_gen.seeded_state(*shape, seed=seed, nz_solid=tw.nz_solid)
+    if clean:
+        st = _clean(st, tw)
+    st["read_is_a"] = True
+    tw.grid.load_state({k: v for k, v in st.items() if k != "nz_solid"})
+    return tw, dx
+
+
+def _surface_probes(tw):
+    flags = tw.grid.flags.cpu().numpy()
+    out = []
+    for i, j in ((13, 12), (14, 10), (15, 13), (16, 12)):
+        col = flags[i, j]
+        out.append((i, j, max(k for k in range(tw.grid.nz) if col[k] != 2)))
+    return out
+
+
+def _problem(n_steps=24, kind="goldak", vof=False, checkpoint_every=None, **kw):
+    from waam_solver_b200.adjoint import AdjointProblem
+    tw, dx = _twin(kind=kind, vof=vof, **kw)
+    y = (tw.grid.ny // 2) * dx
+    pos = [(0.3 * tw.grid.nx * dx + s * 0.008 * dx * 0.1, y) for s in range(n_steps)]
+    prob = AdjointProblem(tw, pos, _surface_probes(tw), checkpoint_every=checkpoint_every)
+    base = prob.theta.copy()
+    # targets: the same run at perturbed parameters
+    prob.forward(base * np.array([1.04, 1.3, 1.0, 1.1, 0.9, 1.05, 1.1]))
+    prob.T_target = prob.T_probe.copy()
+    W, _ = prob.width()
+    prob.W_target = W + 0.05
+    prob.w_T, prob.w_W = 1e-3, 10.0
+    return prob, base
+
+
+def test_stream_adjoint_is_the_exact_transpose():
+    from waam_solver_b200 import _native
+    nx, ny, nz = 12, 9, 10
+    n = nx * ny * nz
+    rng = np.random.default_rng(4)
+    flags = rng.choice([0, 1, 2, 4], size=n, p=[0.3, 0.25, 0.35, 0.1]).astype(np.int32)
+    y = rng.normal(size=19 * n).astype(np.float32)
+    lam = rng.normal(size=19 * n).astype(np.float32)
+    dev = lambda a: torch.from_numpy(a).cuda()  # noqa: E731
+    fy, ff = dev(y), dev(flags)
+    fx = torch.zeros(19 * n, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    _native.call("waam_stream", fy.data_ptr(), fx.data_ptr(), ff.data_ptr(), nx, ny, nz, st)
+    lam_xp = dev(lam)
+    lam_yp = torch.zeros(19 * n, device="cuda")
+    lam_xn = torch.zeros(19 * n, device="cuda")
+    _native.call("waam_adj_stream", lam_yp.data_ptr(), lam_xp.data_ptr(), lam_xn.data_ptr(),
+                 ff.data_ptr(), nx, ny, nz, st)
+    torch.cuda.synchronize()
+    solid = np.tile(flags == 1, 19)
+    lhs = float((lam.astype(np.float64) * fx.cpu().numpy().astype(np.float64))[~solid].sum())
+    rhs = float((lam_yp.cpu().numpy().astype(np.float64) * y.astype(np.float64)).sum())
+    assert abs(lhs - rhs) <= 1e-5 * (abs(lhs) + 1.0), (lhs, rhs)
+    # solid cells pass through unchanged (the stream does not write them)
+    assert np.array_equal(lam_xn.cpu().numpy()[solid], lam[solid])
+    assert not lam_xn.cpu().numpy()[~solid].any()
+
+
+def _j(g, lam1):
+    u = torch.stack([g.ux.reshape(-1), g.uy.reshape(-1), g.uz.reshape(-1)])
+    return (float((lam1["H"].double() * g.H.reshape(-1).double()).sum()) +
+            float((lam1["X"].double() * g.f_src.reshape(-1).double()).sum()) +
+            float((lam1["Y"].double() * g.f_dst.reshape(-1).double()).sum()) +
+            float((lam1["u"].double() * u.double()).sum()))
+
+
+def test_one_reverse_step_matches_finite_differences():
+    """<lam_1, d state_1> / eps against <lam_0, d state_0> for a perturbation
+    of H on cells clear of the phase boundaries, the floor and the ceiling."""
+    from waam_solver_b200 import _native, kernels
+    from waam_solver_b200.adjoint import AdjointProblem, _Tape, _ptr, _stream
+    tw, dx = _twin(clean=False)
+    g = tw.grid
+    for s in range(5):                       # a developed velocity field
+        tw.step(12 * dx + s * 1e-6, 12 * dx, True)
+    n = g.n_cells
+    x, y = 12 * dx + 5e-6, 12 * dx
+    prob = AdjointProblem(tw, [(x, y)], [])
+    prob.forward(prob.theta)
+    ck = prob.checkpoints[0]
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    nongas = (g.flags.reshape(-1) != 2).float()
+    lam1 = {"H": torch.randn(n, device="cuda", generator=gen) * nongas * 1e-6,
+            "X": torch.randn(19 * n, device="cuda", generator=gen),
+            "Y": torch.randn(19 * n, device="cuda", generator=gen),
+            "u": torch.randn((3, n), device="cuda", generator=gen)}
+    tape = _Tape(g, 1, n)
+    pre0 = prob._record_segment(0, [0], tape)
+    f32 = dict(dtype=torch.float32, device="cuda")
+    lam = {"H": lam1["H"].clone(), "Hp": torch.zeros(n, **f32), "mu": torch.zeros(n, **f32),
+           "T": torch.zeros(n, **f32), "fl": torch.zeros(n, **f32), "u": lam1["u"].clone()}
+    pops = [lam1["X"].clone(), lam1["Y"].clone(), torch.zeros(19 * n, **f32)]
+    ctb = torch.zeros(6 * n, **f32)
+    amap = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    gh = torch.zeros(1, dtype=torch.float64, device="cuda")
+    inj = torch.zeros(11, dtype=torch.float64, device="cuda")
+    pops = prob._reverse_step(0, 0, pre0, tape, lam, pops, ctb, amap, gh, inj, g.workspace)
+    _native.call("waam_adj_combine", ctypes.byref(prob._params()), _ptr(lam["H"]), _ptr(lam["T"]),
+                 _ptr(lam["fl"]), _ptr(pre0["H"]), _ptr(pre0["flags"]), _ptr(g.phi.reshape(-1)),
+                 n, _stream())
+    # direction: H of solid / liquid cells at least 2e7 J/m^3 (4 K) from every kink
+    H0 = pre0["H"]
+    cp = tw.cp_rho
+    H_sol, H_liq = cp * tw.mat.T_solidus, cp * tw.mat.T_solidus + tw.L_rho
+    away = ((((H_sol - H0) > 2e7) | ((H0 - H_liq) > 2e7)) & (H0 < cp * 3000.0) &
+            ((H0 - cp * tw.T_amb).abs() > 2e7))
+    dH = (torch.rand(n, device="cuda", generator=gen) * 2 - 1) * nongas * away.float() * 2e6
+    adj = float((lam["H"].double() * dH.double()).sum())
+    vals = []
+    tw.use_cuda_graphs = False
+    for sgn in (1, -1):
+        ck.restore(tw)
+        g.H.reshape(-1).add_(sgn * dH)
+        kernels.update_phase(g.H, g.T, g.f_l, tw.cp_rho, tw.L_rho, tw.mat.T_solidus,
+                             tw.mat.T_liquidus)
+        tw.step(x, y, True)
+        torch.cuda.synchronize()
+        vals.append(_j(g, lam1))
+    fd = (vals[0] - vals[1]) / 2.0
+    assert abs(adj - fd) <= 1e-3 * abs(fd), (adj, fd)
+
+
+def _fd(prob, base, rel=1e-3):
+    fd = np.zeros_like(base)
+    for q in range(base.size):
+        if base[q] == 0.0:
+            continue
+        h = rel * abs(base[q])
+        tp, tm = base.copy(), base.copy()
+        tp[q] += h
+        tm[q] -= h
+        fd[q] = (prob.forward(tp) - prob.forward(tm)) / (2 * h)
+    return fd
+
+
+@pytest.mark.parametrize("kind,vof", [("goldak", False), ("gaussian", False), ("goldak", True)])
+def test_adjoint_matches_central_finite_differences(kind, vof):
+    """Float32 forward: the loss moves in steps of its rounding, and cells that
+    cross a phase boundary within the step make the central difference an
+    average of two slopes; 3 % bounds both for this run."""
+    from waam_solver_b200.adjoint import PARAMS
+    prob, base = _problem(kind=kind, vof=vof)
+    L = prob.forward(base)
+    grad = prob.backward()
+    fd = _fd(prob, base)
+    print("%s vof=%s loss %.6e" % (kind, vof, L))
+    for name, g_, f_ in zip(PARAMS, grad, fd):
+        print("  %-18s adjoint % .6e  fd % .6e  rel %.2e" % (
+            name, g_, f_, abs(g_ - f_) / max(abs(f_), 1e-30)))
+    for q, name in enumerate(PARAMS):
+        if base[q] == 0.0 or (kind == "goldak" and name == "arc_sigma_scale"):
+            assert grad[q] == 0.0, name        # structurally zero
+            continue
+        if vof:
+            assert np.sign(grad[q]) == np.sign(fd[q]), name
+            continue
+        assert abs(grad[q] - fd[q]) <= 3e-2 * abs(fd[q]), (name, grad[q], fd[q])
+
+
+def test_adjoint_is_deterministic_and_checkpoint_independent():
+    prob, base = _problem(n_steps=16, checkpoint_every=4)
+    prob.forward(base)
+    g1 = prob.backward()
+    prob.forward(base)
+    g2 = prob.backward()
+    assert np.array_equal(g1, g2)
+    prob2, _ = _problem(n_steps=16, checkpoint_every=16)
+    prob2.forward(base)
+    g3 = prob2.backward()
+    assert np.array_equal(g1, g3)
+
+
+def test_autograd_function():
+    from waam_solver_b200.adjoint import CoupledStepLoss
+    prob, base = _problem(n_steps=8)
+    theta = torch.tensor(base, dtype=torch.float64, requires_grad=True)
+    loss = CoupledStepLoss.apply(theta, prob)
+    loss.backward()
+    assert theta.grad is not None and torch.isfinite(theta.grad).all()
+    assert np.array_equal(theta.grad.numpy(), prob.grad)

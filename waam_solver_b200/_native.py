@@ -29,7 +29,8 @@ class WaamFields(C.Structure):
         "Fz", "step_scalars")] + [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                                   ("tracer_pos", C.c_void_p), ("tracer_active", C.c_void_p),
                                   ("max_tracers", C.c_int)] + [
-        (name, C.c_void_p) for name in ("cp_rho_f", "alpha_f", "dgamma_f", "tau_f")]
+        (name, C.c_void_p) for name in ("cp_rho_f", "alpha_f", "dgamma_f", "tau_f", "tape_f",
+                                        "tape_cells", "tape_count")] + [("tape_cap", C.c_int64)]
 
 
 TABLE_KNOTS = 8
@@ -111,6 +112,7 @@ _CTYPES = {
     "void* const*": C.c_void_p, "const WaamMaterialTables*": C.POINTER(WaamMaterialTables),
     "WaamTelemetry*": C.c_void_p, "const WaamProbeSet*": C.POINTER(WaamProbeSet),
     "const WaamShiftPlane*": C.c_void_p, "const WaamExportChannel*": C.c_void_p,
+    "double*": C.c_void_p,
 }
 
 

@@ -624,6 +624,10 @@ struct CollideArgs {
     float omega, omega_b, C_darcy, u_cap;
     const float* dgamma_f;  // non-null: Marangoni with the per-cell dgamma (table path)
     const float* tau_f;
+    float* tape_f;          // non-null: adjoint tape of the pre-collision populations
+    int32_t* tape_cells;
+    int32_t* tape_count;
+    int64_t tape_cap;
 };
 
 // Body forces + collision + Mach clamp over the active (FLUID/IFACE) cells
@@ -657,6 +661,9 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
     }
     __syncthreads();
     const unsigned cnt = start[kActiveShards];
+    const bool tape = a.tape_f != nullptr && (int64_t)cnt <= a.tape_cap;
+    if (a.tape_f != nullptr && blockIdx.x == 0 && threadIdx.x == 0)
+        *a.tape_count = tape ? (int32_t)cnt : -1;
     ForceParams P = a.P;
     P.arc_k = scalars[kScalarArcK];
     P.arc_i = scalars[kScalarArcI];
@@ -678,6 +685,11 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
         float f[19], o[19];
 #pragma unroll
         for (int q = 0; q < 19; ++q) f[q] = Pop<S>::get(f_src[q * n + c], q);
+        if (tape) {
+            a.tape_cells[t] = c;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) a.tape_f[(int64_t)q * a.tape_cap + t] = f[q];
+        }
         const float tau_c = a.kind == 2 ? a.tau_f[c] : 0.0f;
         if (a.dgamma_f) P.dgamma = a.dgamma_f[c];
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
@@ -1025,6 +1037,12 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
     cl.kind = p->use_tables && p->variable_tau ? 2 : p->collision;
     cl.dgamma_f = p->use_tables ? f->dgamma_f : nullptr;
     cl.tau_f = f->tau_f;
+    cl.tape_f = f->tape_f;
+    cl.tape_cells = f->tape_cells;
+    cl.tape_count = f->tape_count;
+    cl.tape_cap = f->tape_cap;
+    if (f->tape_f && (!f->tape_cells || !f->tape_count || f->tape_cap <= 0))
+        return fail(WAAM_ERR_INVALID, "step_main: incomplete collision tape");
     cl.from_buffer = p->forces_from_buffer;
     cl.omega = p->omega;
     cl.omega_b = p->omega_b;
