@@ -69,7 +69,7 @@ def twin_kwargs(w):
     keys = ("heat_source", "arc_power_W", "arc_efficiency", "droplet_freq_hz", "enable_vof",
             "enable_wetting", "contact_angle_deg", "enable_csf_tension",
             "enable_hydrostatic_gravity", "use_srt", "travel_speed_m_s", "arc_sigma_mm",
-            "wire_diameter_mm")
+            "wire_diameter_mm", "enable_heat_loss")
     return {k: w[k] for k in keys if k in w}
 
 
@@ -368,6 +368,74 @@ def table_form(w, device, K, ref_ms, ref_stages):
     return out
 
 
+ADJOINT_C4 = dict(
+    workload="differentiation 128x64x48 D3Q19, dx 0.25 mm, Goldak 3 kW (a_f 3 / a_r 9 / b 3 / c "
+             "3 mm), 8 mm/s, VOF, heat losses, 2000 steps; loss: 8 surface probe traces + final "
+             "smooth pool width",
+    nx=128, ny=64, nz=48, dx=2.5e-4, heat_source="goldak", arc_power_W=3000.0,
+    arc_efficiency=0.78, goldak_mm=dict(a_front_mm=3.0, a_rear_mm=9.0, b_mm=3.0, c_mm=3.0,
+                                        ff=0.6, fr=1.4),
+    droplet_freq_hz=0.0, enable_vof=True, use_srt=False, travel_speed_m_s=0.008,
+    enable_heat_loss=True, steps=2000)
+
+
+def adjoint_form(device, n_steps=None, fd=True):
+    """Config 4: loss + gradient with the hand-written adjoint (sqrt(N)
+    checkpointing), backward time against forward time (CUDA events), and
+    central finite differences (relative step 1e-3) of every parameter."""
+    import numpy as np
+    import torch
+    from waam_solver_b200.adjoint import PARAMS, AdjointProblem
+    w = dict(ADJOINT_C4)
+    N = int(n_steps or w["steps"])
+    tw = build_twin(w, device)
+    g = tw.grid
+    dx = g.dx
+    x0, yc = 10e-3, (g.ny // 2) * dx
+    pos = [(x0 + s * g.dt * w["travel_speed_m_s"], yc) for s in range(N)]
+    rng = np.random.default_rng(0)
+    probes = []
+    for _ in range(8):
+        off = rng.uniform(2e-3, 6e-3) * (1 if rng.random() < 0.5 else -1)
+        probes.append((int(rng.uniform(x0 - 2e-3, x0 + 3e-3) / dx), int((yc + off) / dx),
+                       tw.nz_solid - 1))
+    prob = AdjointProblem(tw, pos, probes)
+    base = prob.theta.copy()
+    prob.forward(base * np.array([1.05, 1.2, 1.0, 1.1, 0.9, 1.1, 1.1]))
+    prob.T_target = prob.T_probe.copy()
+    prob.W_target, _ = prob.width()
+    prob.W_target += 0.1
+    prob.w_T, prob.w_W = 1e-3, 10.0
+    prob.forward(base)                     # warm-up of both passes
+    prob.backward()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    e[0].record()
+    loss = prob.forward(base)
+    e[1].record()
+    grad = prob.backward()
+    e[2].record()
+    torch.cuda.synchronize()
+    fwd_ms, bwd_ms = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    out = {"config": w["workload"], "steps": N, "checkpoint_every": prob.K,
+           "loss": loss, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+           "backward_over_forward": bwd_ms / fwd_ms,
+           "gradient": {k: float(v) for k, v in zip(PARAMS, grad)}}
+    if fd:
+        rel = {}
+        for q, name in enumerate(PARAMS):
+            if base[q] == 0.0:
+                continue
+            h = 1e-3 * abs(base[q])
+            tp, tm = base.copy(), base.copy()
+            tp[q] += h
+            tm[q] -= h
+            f = (prob.forward(tp) - prob.forward(tm)) / (2 * h)
+            rel[name] = {"fd": f, "rel_diff": abs(grad[q] - f) / max(abs(f), 1e-300)}
+        out["central_fd_rel_step_1e-3"] = rel
+    return out
+
+
 def run_b200(args, w):
     import torch
     from waam_solver_b200 import _native
@@ -499,6 +567,8 @@ def run_b200(args, w):
         line["precision_forms"]["storage"] = ("headline value: float32 populations; forms: "
                                               "16-bit offsets f_q - w_q, float32 arithmetic")
         line["material_tables"] = table_form(w, device, min(K, 1000), ms / K, stage_ms)
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_form(device)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:
@@ -518,6 +588,8 @@ def main():
     ap.add_argument("--no-precision-forms", action="store_true",
                     help="skip the float16 / bfloat16 population-storage timings")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the config-4 adjoint timing and finite-difference check")
     ap.add_argument("--spinup", type=int, default=None,
                     help="steps run before warm-up (default: the workload's spin-up)")
     args = ap.parse_args()
