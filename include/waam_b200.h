@@ -512,6 +512,14 @@ typedef struct WaamFields {
     int32_t* tape_cells;
     int32_t* tape_count;
     int64_t tape_cap;
+    /* current density J (A/m^2) and self field B (T) of the welding current
+     * (physics/weld_forces.py:261-276), solved by the caller between
+     * waam_step_main_stage 0 and 1; when set, the collision adds the J x B
+     * force (kernels.py:1479-1513) after the other body forces and before
+     * their clamp, as the reference's force assembly does
+     * (solvers/coupled_step.py:352-362).  Null: no Lorentz force. */
+    const float* lorentz_J[3];
+    const float* lorentz_B[3];
 } WaamFields;
 
 typedef struct WaamStepParams {
@@ -587,8 +595,17 @@ int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace
 int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* workspace,
                           size_t workspace_bytes, void* const* events, int n_events,
                           void* stream);
+
+/* waam_step_main in two halves around the Lorentz solve, which reads the
+ * liquid fraction and flags of this step and writes the J and B the
+ * collision adds: stage 0 = VOF advection, thermal, phase, flags and the
+ * active-cell list; stage 1 = forces, collision, stream, tracers, tail.
+ * Stage 0 followed by stage 1 equals one waam_step_main. */
+int waam_step_main_stage(const WaamFields* f, const WaamStepParams* p, int stage, void* workspace,
+                         size_t workspace_bytes, void* stream);
 /* Number of kernels the fused stages launch (for launch accounting): stage 0
- * waam_step_pre, 1 waam_step_main, 2 waam_step_main_events. */
+ * waam_step_pre, 1 waam_step_main, 2 waam_step_main_events; the J x B pass
+ * over SOLID cells of a step with WaamFields.lorentz_J set adds one). */
 int waam_step_launch_count(const WaamStepParams* p, int stage);
 
 /* ---- adjoint of the coupled step (reverse kernels, one step each) ---------- */

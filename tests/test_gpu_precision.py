@@ -26,7 +26,7 @@ NON_F = [f for f in steps.FIELDS if f not in ("f_a", "f_b")]
 ULP_BITS = {"float16": 11, "bfloat16": 8}
 
 
-def _c2_twin(dtype, shape=(40, 24, 24)):
+def _c2_twin(dtype, shape=(40, 24, 24), **more):
     from waam_solver_b200 import WAAMTwin
     from waam_solver_b200.materials import from_constants
     from waam_solver_b200.physics.arc import Goldak3D
@@ -35,7 +35,7 @@ def _c2_twin(dtype, shape=(40, 24, 24)):
                   use_srt=False, enable_vof=True, travel_speed_m_s=0.008, heat_source="goldak",
                   arc_power_W=4000.0, arc_efficiency=0.78, arc_sigma_mm=1.0,
                   droplet_freq_hz=100.0, enable_wetting=True, enable_csf_tension=True,
-                  enable_hydrostatic_gravity=True, population_dtype=dtype)
+                  enable_hydrostatic_gravity=True, population_dtype=dtype, **more)
     tw.wire_feed_m_s = 0.1
     tw.droplet_transfer_mode = "pulsed"
     tw.pulse_frequency_hz = 100.0
@@ -45,17 +45,21 @@ def _c2_twin(dtype, shape=(40, 24, 24)):
     return tw
 
 
+@pytest.mark.parametrize("lorentz", [False, True])
 @pytest.mark.parametrize("dtype", ["float16", "bfloat16"])
-def test_one_step_matches_float32_up_to_storage_rounding(dtype):
+def test_one_step_matches_float32_up_to_storage_rounding(dtype, lorentz):
+    """``lorentz``: with the welding current's J x B force (its potential solve,
+    J and B are storage independent and must agree bit for bit too)."""
     import state_gen
     shape = (40, 24, 24)
-    t16 = _c2_twin(dtype, shape)
+    more = dict(enable_lorentz=True, welding_current_A=180.0) if lorentz else {}
+    t16 = _c2_twin(dtype, shape, **more)
     st = state_gen.seeded_state(*shape, seed=5, nz_solid=t16.nz_solid)
     st["read_is_a"] = True
     t16.grid.load_state({k: v for k, v in st.items() if k != "nz_solid"})
     # the float32 twin starts from exactly the populations the 16-bit twin holds
     start = t16.grid.state_dict()
-    t32 = _c2_twin("float32", shape)
+    t32 = _c2_twin("float32", shape, **more)
     t32.grid.load_state(start)
     dx = 2e-4
     for tw in (t16, t32):
@@ -65,6 +69,11 @@ def test_one_step_matches_float32_up_to_storage_rounding(dtype):
     a, b = t16.grid.state_dict(), t32.grid.state_dict()
     for f in NON_F:
         assert np.array_equal(a[f], b[f]), f
+    if lorentz:
+        for f in ("phi_elec", "Jx", "Jy", "Jz", "Bx", "By", "Bz"):
+            assert np.array_equal(getattr(t16.grid, f).cpu().numpy(),
+                                  getattr(t32.grid, f).cpu().numpy()), f
+        assert float(t32.grid.Jz.abs().max()) > 0.0
     w = t32.grid.w.cpu().numpy().reshape(19, 1, 1, 1)
     for f in ("f_a", "f_b"):
         off = np.abs(b[f].astype(np.float64) - w)

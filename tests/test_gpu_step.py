@@ -154,12 +154,14 @@ def test_graph_replay_matches_eager_launches():
 LORENTZ_FIELDS = ("phi_elec", "Jx", "Jy", "Jz", "Bx", "By", "Bz", "elec_rad_bins")
 
 
-def test_lorentz_steps_match_oracle():
+@pytest.mark.parametrize("step_mode", ["fused", "operators"])
+def test_lorentz_steps_match_oracle(step_mode):
     """Welding current on: the potential solve (cold start, then warm), J, B and
-    J x B through the CUDA operators, step by step against the oracle."""
+    J x B, step by step against the oracle -- in the fused step (J x B added
+    inside the collision, before the force clamp) and through the operators."""
     shape = (40, 24, 24)
     tw, ot, dx = _config_twins("c2", *shape, enable_lorentz=True, welding_current_A=180.0,
-                               lorentz_jacobi_iters=40)
+                               lorentz_jacobi_iters=40, step_mode=step_mode)
     import state_gen
     st = state_gen.seeded_state(*shape, seed=9, nz_solid=tw.nz_solid)
     st["read_is_a"] = True

@@ -30,7 +30,8 @@ class WaamFields(C.Structure):
                                   ("tracer_pos", C.c_void_p), ("tracer_active", C.c_void_p),
                                   ("max_tracers", C.c_int)] + [
         (name, C.c_void_p) for name in ("cp_rho_f", "alpha_f", "dgamma_f", "tau_f", "tape_f",
-                                        "tape_cells", "tape_count")] + [("tape_cap", C.c_int64)]
+                                        "tape_cells", "tape_count")] + [("tape_cap", C.c_int64)] + [
+        ("lorentz_J", C.c_void_p * 3), ("lorentz_B", C.c_void_p * 3)]
 
 
 TABLE_KNOTS = 8

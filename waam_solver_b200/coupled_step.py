@@ -356,7 +356,7 @@ def step_params(twin):
 
 
 def _check_fused_supported(twin):
-    supported = not (twin.enable_lorentz or twin.enable_recoil or twin.enable_gas_shear or
+    supported = not (twin.enable_recoil or twin.enable_gas_shear or
                      getattr(twin, "use_torch_z", False))
     if not supported and twin.grid.population_storage:
         raise WaamError("16-bit population storage runs on the fused step only; this "
@@ -406,13 +406,19 @@ def upload_position(twin, arc_i, arc_j):
     ring.upload(g._pos_dst, arc_i, arc_j)
 
 
-def _fields_cached(g):
-    """WaamFields for the current buffer parity (device pointers never move)."""
-    key = (g._read_buf is g.f_a, g._cur)
+def _fields_cached(g, lorentz=False):
+    """WaamFields for the current buffer parity (device pointers never move);
+    ``lorentz``: with the current density and self field the collision adds."""
+    key = (g._read_buf is g.f_a, g._cur, lorentz)
     cache = g.__dict__.setdefault("_fields_cache", {})
     f = cache.get(key)
     if f is None:
         f = cache[key] = _fields(g)
+        if lorentz:
+            for q, t in enumerate((g.Jx, g.Jy, g.Jz)):
+                f.lorentz_J[q] = t.data_ptr()
+            for q, t in enumerate((g.Bx, g.By, g.Bz)):
+                f.lorentz_B[q] = t.data_ptr()
         g._pos_dst = g.step_scalars[4:6]
     return f
 
@@ -454,7 +460,11 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
 
     Steps without a droplet replay a captured CUDA graph of the two stages
     (``twin.use_cuda_graphs``); droplet steps and instrumented steps run the
-    stages eagerly because they read back or record events in between."""
+    stages eagerly because they read back or record events in between.  With
+    the welding current's Lorentz force, waam_step_main runs as its two
+    halves around the potential solve (solvers/coupled_step.py:352-353), whose
+    convergence checks read back; the collision then adds J x B before the
+    force clamp."""
     if not _check_fused_supported(twin):
         return coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m)
     g = twin.grid
@@ -479,8 +489,11 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     twin._last_arc_ijk = _LazyArc(g, arc_i, arc_j)
     events = getattr(twin, "_stage_events", None)
     due = _droplet_due(twin, g, is_welding)
+    lorentz = bool(is_welding and twin.enable_lorentz)
+    if lorentz and events is not None:
+        raise WaamError("stage events are not recorded on steps with the Lorentz force")
     done = False
-    if not due and events is None and getattr(twin, "use_cuda_graphs", True):
+    if not due and not lorentz and events is None and getattr(twin, "use_cuda_graphs", True):
         key = (g._read_buf is g.f_a, g._cur, p.welding, p.clear_forces,
                (dx_, dy_, dz_) if twin.enable_bead_freeze else None)
         done = _run_graph(twin, g, f, p, ws, key)
@@ -495,7 +508,14 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
             f = _fields_cached(g)     # the first droplet switches tracer advection on
             p.forces_from_buffer = 1
             p.clear_forces = 0
-        if events is None:
+        if lorentz:
+            _native.call("waam_step_main_stage", ctypes.byref(f), ctypes.byref(p), 0,
+                         ws.data_ptr(), ws.numel(), stream)
+            arc_k = float(g.step_scalars[0].item())
+            weld_forces.solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=False)
+            _native.call("waam_step_main_stage", ctypes.byref(_fields_cached(g, lorentz=True)),
+                         ctypes.byref(p), 1, ws.data_ptr(), ws.numel(), stream)
+        elif events is None:
             _native.call("waam_step_main", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(),
                          ws.numel(), stream)
         else:
@@ -503,8 +523,9 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
             handles = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
             _native.call("waam_step_main_events", ctypes.byref(f), ctypes.byref(p),
                          ws.data_ptr(), ws.numel(), handles, len(events), stream)
-    # the droplet impact load stays in F outside the active cells until the next step
-    g._forces_dirty = bool(p.forces_from_buffer)
+    # the droplet impact load (and J x B on SOLID cells) stays in F outside the
+    # active cells until the next step
+    g._forces_dirty = bool(p.forces_from_buffer) or lorentz
     g.flip_thermal()
     g.swap_buffers()
     twin._step_n += 1

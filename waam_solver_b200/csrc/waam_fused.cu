@@ -628,7 +628,26 @@ struct CollideArgs {
     int32_t* tape_cells;
     int32_t* tape_count;
     int64_t tape_cap;
+    // non-null: the Lorentz force J x B of the welding current is added after
+    // the other body forces and before their clamp
+    const float* J[3];
+    const float* B[3];
+    float lz_dt, lz_dx, lz_rho;
 };
+
+// kernels.py:1479-1513 apply_lorentz_JxB for one cell (f_l >= 0.05)
+__device__ __forceinline__ void lorentz_add(const float* const* J, const float* const* B, int64_t c,
+                                            float fl, float dt, float dx, float rho_ref,
+                                            float& fx, float& fy, float& fz) {
+    const float jx = J[0][c], jy = J[1][c], jz = J[2][c];
+    const float bx = B[0][c], by = B[1][c], bz = B[2][c];
+    const float fxp = jy * bz - jz * by, fyp = jz * bx - jx * bz, fzp = jx * by - jy * bx;
+    const float flw = fmin_(1.0f, fl);
+    const float scale = flw * dt * dt / (rho_ref * dx);
+    fx += fxp * scale;
+    fy += fyp * scale;
+    fz += fzp * scale;
+}
 
 // Body forces + collision + Mach clamp over the active (FLUID/IFACE) cells
 // listed by k_column, shard after shard (solvers/coupled_step.py:298-402).  Forces stay in
@@ -668,6 +687,9 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
     P.arc_k = scalars[kScalarArcK];
     P.arc_i = scalars[kScalarArcI];
     P.arc_j = scalars[kScalarArcJ];
+    const bool lorentz = a.J[0] != nullptr;
+    const float F_cap = P.F_cap;
+    if (lorentz) P.F_cap = 0.0f;   // clamped below, after J x B
     for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt;
          t += gridDim.x * blockDim.x) {
         int lo = 0, hi = kActiveShards;  // last shard with start <= t
@@ -700,6 +722,20 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
         }
         float fl = f_l[c];
         cell_forces(d, P, phi, T, flags, i, j, k, fl, fx, fy, fz);
+        if (lorentz) {
+            // the reference order: the other forces, J x B, then the clamp
+            // (solvers/coupled_step.py:298-362; kernels.py:3286-3309)
+            if (!(fl < 0.05f)) lorentz_add(a.J, a.B, c, fl, a.lz_dt, a.lz_dx, a.lz_rho, fx, fy, fz);
+            if (F_cap > 0.0f) {
+                const float mag = sqrtf(fx * fx + fy * fy + fz * fz);
+                if (mag > F_cap) {
+                    const float sc = F_cap / (mag + 1e-12f);
+                    fx = fx * sc;
+                    fy = fy * sc;
+                    fz = fz * sc;
+                }
+            }
+        }
         float rr, u, v, w;
         if (a.kind == 0)
             collide_mrt_cell(f, fl, fx, fy, fz, a.omega, a.omega_b, a.C_darcy, o, rr, u, v, w);
@@ -713,6 +749,28 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
         ux[c] = u;
         uy[c] = v;
         uz[c] = w;
+        Fx[c] = fx;
+        Fy[c] = fy;
+        Fz[c] = fz;
+    }
+}
+
+// The J x B force the reference adds to SOLID cells with f_l >= 0.05 (it is
+// part of the force field the step leaves; the collision never reads it).
+__global__ void k_lorentz_solid(int64_t n, const int32_t* __restrict__ flags,
+                                const float* __restrict__ f_l, float* Fx, float* Fy, float* Fz,
+                                const float* Jx, const float* Jy, const float* Jz,
+                                const float* Bx, const float* By, const float* Bz, float dt,
+                                float dx, float rho_ref) {
+    const float* J[3] = {Jx, Jy, Jz};
+    const float* B[3] = {Bx, By, Bz};
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        if (flags[c] != SOLID) continue;
+        const float fl = f_l[c];
+        if (fl < 0.05f) continue;
+        float fx = Fx[c], fy = Fy[c], fz = Fz[c];
+        lorentz_add(J, B, c, fl, dt, dx, rho_ref, fx, fy, fz);
         Fx[c] = fx;
         Fy[c] = fy;
         Fz[c] = fz;
@@ -893,9 +951,13 @@ int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace
     return waam_step_main_events(f, p, workspace, workspace_bytes, nullptr, 0, stream);
 }
 
-int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* workspace,
+}  // extern "C"
+
+namespace waam {
+// stages: bit 0 thermal .. column, bit 1 collide .. tail
+static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* workspace,
                           size_t workspace_bytes, void* const* events, int n_events,
-                          void* stream) {
+                          void* stream, int stages) {
     if (!fields_ok(f) || !p) return fail(WAAM_ERR_INVALID, "step_main: bad fields or params");
     if (!tables_fields_ok(f, p)) return fail(WAAM_ERR_INVALID, "step_main: bad material tables");
     if (p->f_storage < kStoreF32 || p->f_storage > kStoreBF16)
@@ -919,182 +981,219 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
         return fail(WAAM_ERR_INVALID, "step_main: nz too large for the active-cell list");
     const int col_blocks = (int)(((int64_t)d.nx * d.ny * 32 + kThreads - 1) / kThreads);
     cudaStream_t s = STREAM(stream);
+    int e = WAAM_OK;
 
-    ThermalArgs ta;
-    ta.ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
-    ta.cpa = p->cp_rho * p->alpha_lu;
-    ta.dt_lu = 1.0f;
-    ta.inv_dt = 1.0f / (p->dt + 1e-12f);
-    ta.heat_loss = p->heat_loss;
-    ta.conv = p->conv;
-    ta.rad = p->rad;
-    ta.T_amb = p->T_amb;
-    ta.h_conv = p->h_conv;
-    ta.eps_rad = p->eps_rad;
-    ta.dt_phys = p->dt;
-    ta.dx = p->dx;
-    ta.sigma_sb = p->sigma_sb;
-    ta.h_floor = p->cp_rho * p->T_amb;
-    TableArgs tba{};
-    if (p->use_tables) {
-        tba.vp = var_phase(p);
-        tba.tc = TableConsts{p->rho_mat, p->dt, p->dx, p->force_scale_lu, p->marangoni_scale,
-                             p->cp_rho, p->alpha_lu, p->dgamma_lu, p->tau_ref, 1};
-        tba.tb = p->tables;
-        tba.cp_f = f->cp_rho_f;
-        tba.alpha_f = f->alpha_f;
-        tba.dg_f = f->dgamma_f;
-        tba.tau_f = f->tau_f;
-    }
-    // Without stage events, VOF advection (reads phi, u, flags; writes phi_tmp)
-    // runs on a second stream beside the thermal stage (reads H, T, u, flags;
-    // writes the thermal fields and f_l).
-    AuxStream* aux = nullptr;
-    const bool overlap = events == nullptr;
-    if (overlap) {
-        int ea = aux_stream(&aux);
-        if (ea) return ea;
-    }
-    auto fork = [&](int q) {
-        cudaEventRecord(aux->ev[q], s);
-        cudaStreamWaitEvent(aux->s2, aux->ev[q], 0);
-    };
-    auto join = [&](int q) {
-        cudaEventRecord(aux->ev[q], aux->s2);
-        cudaStreamWaitEvent(s, aux->ev[q], 0);
-    };
-    int e;
-    if (overlap && p->vof) {
-        fork(0);
-        k_vof_advect<<<tile_grid(d), tile_block(), 0, aux->s2>>>(d, f->phi, f->phi_tmp, f->ux,
-                                                                  f->uy, f->uz, f->flags);
-        e = check_launch("k_vof_advect");
-        if (e) return e;
-    }
-    mark(0);
-    if (p->use_tables)
-        k_thermal_fused<true><<<tile_grid(d), tile_block(), 0, s>>>(
-            d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
-            f->T_prev, f->dT_dt, active_count, ta, tba);
-    else
-        k_thermal_fused<false><<<tile_grid(d), tile_block(), 0, s>>>(
-            d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
-            f->T_prev, f->dT_dt, active_count, ta, tba);
-    e = check_launch("k_thermal_fused");
-    if (e) return e;
-    mark(1);
-
-    if (p->vof) {
+    if (stages & 1) {
+        ThermalArgs ta;
+        ta.ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
+        ta.cpa = p->cp_rho * p->alpha_lu;
+        ta.dt_lu = 1.0f;
+        ta.inv_dt = 1.0f / (p->dt + 1e-12f);
+        ta.heat_loss = p->heat_loss;
+        ta.conv = p->conv;
+        ta.rad = p->rad;
+        ta.T_amb = p->T_amb;
+        ta.h_conv = p->h_conv;
+        ta.eps_rad = p->eps_rad;
+        ta.dt_phys = p->dt;
+        ta.dx = p->dx;
+        ta.sigma_sb = p->sigma_sb;
+        ta.h_floor = p->cp_rho * p->T_amb;
+        TableArgs tba{};
+        if (p->use_tables) {
+            tba.vp = var_phase(p);
+            tba.tc = TableConsts{p->rho_mat, p->dt, p->dx, p->force_scale_lu, p->marangoni_scale,
+                                 p->cp_rho, p->alpha_lu, p->dgamma_lu, p->tau_ref, 1};
+            tba.tb = p->tables;
+            tba.cp_f = f->cp_rho_f;
+            tba.alpha_f = f->alpha_f;
+            tba.dg_f = f->dgamma_f;
+            tba.tau_f = f->tau_f;
+        }
+        // Without stage events, VOF advection (reads phi, u, flags; writes phi_tmp)
+        // runs on a second stream beside the thermal stage (reads H, T, u, flags;
+        // writes the thermal fields and f_l).
+        AuxStream* aux = nullptr;
+        const bool overlap = events == nullptr;
         if (overlap) {
-            join(1);
-        } else {
-            k_vof_advect<<<tile_grid(d), tile_block(), 0, s>>>(d, f->phi, f->phi_tmp, f->ux,
-                                                                f->uy, f->uz, f->flags);
+            int ea = aux_stream(&aux);
+            if (ea) return ea;
+        }
+        auto fork = [&](int q) {
+            cudaEventRecord(aux->ev[q], s);
+            cudaStreamWaitEvent(aux->s2, aux->ev[q], 0);
+        };
+        auto join = [&](int q) {
+            cudaEventRecord(aux->ev[q], aux->s2);
+            cudaStreamWaitEvent(s, aux->ev[q], 0);
+        };
+        if (overlap && p->vof) {
+            fork(0);
+            k_vof_advect<<<tile_grid(d), tile_block(), 0, aux->s2>>>(d, f->phi, f->phi_tmp, f->ux,
+                                                                      f->uy, f->uz, f->flags);
             e = check_launch("k_vof_advect");
             if (e) return e;
         }
-    }
-    mark(2);
-    ColumnArgs ca;
-    ca.vof = p->vof;
-    ca.wetting = p->wetting;
-    ca.nz_solid = p->nz_solid;
-    ca.cos_t = (float)cos((double)p->theta);
-    ca.sin_t = (float)sin((double)p->theta);
-    ca.dt_phys = p->dt;
-    ca.T800 = p->T800;
-    ca.T1100 = p->T1100;
-    ca.Ts = p->Ts;
-    ca.zero_forces = p->forces_from_buffer ? 0 : 1;
-    ca.clear_all = p->clear_forces;
-    ca.shard_cap = (int)shard_cap;
-    k_column<<<col_blocks, kThreads, 0, s>>>(d, f->phi_tmp, f->phi, f->flags, f->f_l, f->T_next,
-                                             f->t800, f->t1100, f->tsol, f->Fx, f->Fy, f->Fz,
-                                             active_list, active_count, ca);
-    e = check_launch("k_column");
-    if (e) return e;
-    mark(3);
-
-    CollideArgs cl;
-    ForceParams& P = cl.P;
-    P.csf = p->csf;
-    P.wetting = p->wetting;
-    P.welding = p->welding;
-    P.hydro = p->hydro;
-    P.gamma_lu = p->gamma_lu;
-    P.cos_t = (float)cos((double)p->theta);
-    P.sin_t = (float)sin((double)p->theta);
-    P.dgamma = p->dgamma_lu;
-    P.arc_i = P.arc_j = P.arc_k = 0.0f;  // from the device scalars
-    P.p_inv2s2 = 1.0f / (2.0f * p->p_sigma * p->p_sigma + 1e-6f);
-    float Fphys = p->pressure / (p->rho_phys * p->dx);
-    P.p_Flu = Fphys * (p->dt * p->dt) / p->dx;
-    P.g_lu = p->g_lu;
-    P.beta = p->beta;
-    P.T_ref = p->T_ref;
-    P.rho_ref = 1.0f;
-    P.F_cap = p->F_cap;
-    cl.kind = p->use_tables && p->variable_tau ? 2 : p->collision;
-    cl.dgamma_f = p->use_tables ? f->dgamma_f : nullptr;
-    cl.tau_f = f->tau_f;
-    cl.tape_f = f->tape_f;
-    cl.tape_cells = f->tape_cells;
-    cl.tape_count = f->tape_count;
-    cl.tape_cap = f->tape_cap;
-    if (f->tape_f && (!f->tape_cells || !f->tape_count || f->tape_cap <= 0))
-        return fail(WAAM_ERR_INVALID, "step_main: incomplete collision tape");
-    cl.from_buffer = p->forces_from_buffer;
-    cl.omega = p->omega;
-    cl.omega_b = p->omega_b;
-    cl.C_darcy = p->C_darcy;
-    cl.u_cap = p->u_cap;
-#define WAAM_COLLIDE(S)                                                                    \
-    k_collide_list<S><<<kListBlocks, kListThreads, 0, s>>>(                                \
-        d, static_cast<const Pop<S>::T*>(f->f_src), static_cast<Pop<S>::T*>(f->f_dst),           \
-        f->rho, f->ux, f->uy, f->uz, f->Fx, f->Fy, f->Fz, f->phi, f->T_next, f->f_l, f->flags,    \
-        f->step_scalars, active_list, active_count, (int)shard_cap, cl)
-    if (p->f_storage == kStoreF16)
-        WAAM_COLLIDE(kStoreF16);
-    else if (p->f_storage == kStoreBF16)
-        WAAM_COLLIDE(kStoreBF16);
-    else
-        WAAM_COLLIDE(kStoreF32);
-#undef WAAM_COLLIDE
-    e = check_launch("k_collide_list");
-    if (e) return e;
-    mark(4);
-
-    e = launch_stream_stored(d, f->f_dst, f->f_src, f->flags, p->f_storage, s);
-    if (e) return e;
-    if (f->tracer_pos && f->tracer_active && f->max_tracers > 0) {
-        e = launch_advect_tracers(d, f->tracer_pos, f->tracer_active, f->ux, f->uy, f->uz,
-                                  f->f_l, f->flags, p->dx, f->max_tracers, stream);
+        mark(0);
+        if (p->use_tables)
+            k_thermal_fused<true><<<tile_grid(d), tile_block(), 0, s>>>(
+                d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
+                f->T_prev, f->dT_dt, active_count, ta, tba);
+        else
+            k_thermal_fused<false><<<tile_grid(d), tile_block(), 0, s>>>(
+                d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
+                f->T_prev, f->dT_dt, active_count, ta, tba);
+        e = check_launch("k_thermal_fused");
         if (e) return e;
-    }
-    mark(5);
+        mark(1);
 
-    if (p->substrate_growth || p->bead_freeze) {
-        TailArgs t;
-        t.cp_rho = p->cp_rho;
-        t.Ts = p->Ts;
-        t.Tl = p->Tl;
-        t.L_rho = p->L_rho;
-        t.remelt = 1;
-        t.trailing = p->welding && p->bead_freeze;
-        t.cooled = 1;
-        t.dir_x = p->dir_x;
-        t.dir_y = p->dir_y;
-        t.dir_z = p->dir_z;
-        t.lookback = p->lookback;
-        t.T_freeze = p->T_freeze;
-        t.cp_f = p->use_tables ? f->cp_rho_f : nullptr;
-        k_tail<<<tile_grid(d), tile_block(), 0, s>>>(d, f->T_next, f->H_next, f->f_l, f->phi,
-                                                      f->flags, f->ux, f->uy, f->uz,
-                                                      f->step_scalars, t);
-        e = check_launch("k_tail");
+        if (p->vof) {
+            if (overlap) {
+                join(1);
+            } else {
+                k_vof_advect<<<tile_grid(d), tile_block(), 0, s>>>(d, f->phi, f->phi_tmp, f->ux,
+                                                                    f->uy, f->uz, f->flags);
+                e = check_launch("k_vof_advect");
+                if (e) return e;
+            }
+        }
+        mark(2);
+        ColumnArgs ca;
+        ca.vof = p->vof;
+        ca.wetting = p->wetting;
+        ca.nz_solid = p->nz_solid;
+        ca.cos_t = (float)cos((double)p->theta);
+        ca.sin_t = (float)sin((double)p->theta);
+        ca.dt_phys = p->dt;
+        ca.T800 = p->T800;
+        ca.T1100 = p->T1100;
+        ca.Ts = p->Ts;
+        ca.zero_forces = p->forces_from_buffer ? 0 : 1;
+        ca.clear_all = p->clear_forces;
+        ca.shard_cap = (int)shard_cap;
+        k_column<<<col_blocks, kThreads, 0, s>>>(d, f->phi_tmp, f->phi, f->flags, f->f_l, f->T_next,
+                                                 f->t800, f->t1100, f->tsol, f->Fx, f->Fy, f->Fz,
+                                                 active_list, active_count, ca);
+        e = check_launch("k_column");
+        if (e) return e;
+        mark(3);
     }
-    mark(6);
+
+    if (stages & 2) {
+        CollideArgs cl;
+        ForceParams& P = cl.P;
+        P.csf = p->csf;
+        P.wetting = p->wetting;
+        P.welding = p->welding;
+        P.hydro = p->hydro;
+        P.gamma_lu = p->gamma_lu;
+        P.cos_t = (float)cos((double)p->theta);
+        P.sin_t = (float)sin((double)p->theta);
+        P.dgamma = p->dgamma_lu;
+        P.arc_i = P.arc_j = P.arc_k = 0.0f;  // from the device scalars
+        P.p_inv2s2 = 1.0f / (2.0f * p->p_sigma * p->p_sigma + 1e-6f);
+        float Fphys = p->pressure / (p->rho_phys * p->dx);
+        P.p_Flu = Fphys * (p->dt * p->dt) / p->dx;
+        P.g_lu = p->g_lu;
+        P.beta = p->beta;
+        P.T_ref = p->T_ref;
+        P.rho_ref = 1.0f;
+        P.F_cap = p->F_cap;
+        cl.kind = p->use_tables && p->variable_tau ? 2 : p->collision;
+        cl.dgamma_f = p->use_tables ? f->dgamma_f : nullptr;
+        cl.tau_f = f->tau_f;
+        cl.tape_f = f->tape_f;
+        cl.tape_cells = f->tape_cells;
+        cl.tape_count = f->tape_count;
+        cl.tape_cap = f->tape_cap;
+        if (f->tape_f && (!f->tape_cells || !f->tape_count || f->tape_cap <= 0))
+            return fail(WAAM_ERR_INVALID, "step_main: incomplete collision tape");
+        cl.from_buffer = p->forces_from_buffer;
+        cl.omega = p->omega;
+        cl.omega_b = p->omega_b;
+        cl.C_darcy = p->C_darcy;
+        cl.u_cap = p->u_cap;
+        const bool lorentz = f->lorentz_J[0] != nullptr;
+        for (int q = 0; q < 3; ++q) {
+            cl.J[q] = f->lorentz_J[q];
+            cl.B[q] = f->lorentz_B[q];
+            if (lorentz && (!f->lorentz_J[q] || !f->lorentz_B[q]))
+                return fail(WAAM_ERR_INVALID, "step_main: incomplete Lorentz fields");
+        }
+        cl.lz_dt = p->dt;
+        cl.lz_dx = p->dx;
+        cl.lz_rho = p->rho_phys;
+    #define WAAM_COLLIDE(S)                                                                    \
+        k_collide_list<S><<<kListBlocks, kListThreads, 0, s>>>(                                \
+            d, static_cast<const Pop<S>::T*>(f->f_src), static_cast<Pop<S>::T*>(f->f_dst),           \
+            f->rho, f->ux, f->uy, f->uz, f->Fx, f->Fy, f->Fz, f->phi, f->T_next, f->f_l, f->flags,    \
+            f->step_scalars, active_list, active_count, (int)shard_cap, cl)
+        if (p->f_storage == kStoreF16)
+            WAAM_COLLIDE(kStoreF16);
+        else if (p->f_storage == kStoreBF16)
+            WAAM_COLLIDE(kStoreBF16);
+        else
+            WAAM_COLLIDE(kStoreF32);
+    #undef WAAM_COLLIDE
+        e = check_launch("k_collide_list");
+        if (e) return e;
+        if (lorentz) {
+            k_lorentz_solid<<<elem_blocks(d.n()), kThreads, 0, s>>>(
+                d.n(), f->flags, f->f_l, f->Fx, f->Fy, f->Fz, f->lorentz_J[0],
+                f->lorentz_J[1], f->lorentz_J[2], f->lorentz_B[0], f->lorentz_B[1], f->lorentz_B[2],
+                p->dt, p->dx, p->rho_phys);
+            e = check_launch("k_lorentz_solid");
+            if (e) return e;
+        }
+        mark(4);
+
+        e = launch_stream_stored(d, f->f_dst, f->f_src, f->flags, p->f_storage, s);
+        if (e) return e;
+        if (f->tracer_pos && f->tracer_active && f->max_tracers > 0) {
+            e = launch_advect_tracers(d, f->tracer_pos, f->tracer_active, f->ux, f->uy, f->uz,
+                                      f->f_l, f->flags, p->dx, f->max_tracers, stream);
+            if (e) return e;
+        }
+        mark(5);
+
+        if (p->substrate_growth || p->bead_freeze) {
+            TailArgs t;
+            t.cp_rho = p->cp_rho;
+            t.Ts = p->Ts;
+            t.Tl = p->Tl;
+            t.L_rho = p->L_rho;
+            t.remelt = 1;
+            t.trailing = p->welding && p->bead_freeze;
+            t.cooled = 1;
+            t.dir_x = p->dir_x;
+            t.dir_y = p->dir_y;
+            t.dir_z = p->dir_z;
+            t.lookback = p->lookback;
+            t.T_freeze = p->T_freeze;
+            t.cp_f = p->use_tables ? f->cp_rho_f : nullptr;
+            k_tail<<<tile_grid(d), tile_block(), 0, s>>>(d, f->T_next, f->H_next, f->f_l, f->phi,
+                                                          f->flags, f->ux, f->uy, f->uz,
+                                                          f->step_scalars, t);
+            e = check_launch("k_tail");
+        }
+        mark(6);
+    }
     return e;
+}
+}  // namespace waam
+
+extern "C" {
+
+int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* workspace,
+                          size_t workspace_bytes, void* const* events, int n_events,
+                          void* stream) {
+    return step_main_impl(f, p, workspace, workspace_bytes, events, n_events, stream, 3);
+}
+
+int waam_step_main_stage(const WaamFields* f, const WaamStepParams* p, int stage, void* workspace,
+                         size_t workspace_bytes, void* stream) {
+    if (stage != 0 && stage != 1) return fail(WAAM_ERR_INVALID, "step_main_stage: stage 0 or 1");
+    return step_main_impl(f, p, workspace, workspace_bytes, nullptr, 0, stream, 1 << stage);
 }
 
 }  // extern "C"

@@ -29,7 +29,9 @@ def _jacobi_budget(twin, g, cold_start):
     return max_iters
 
 
-def solve_lorentz(twin, g, arc_i, arc_j, arc_k):
+def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True):
+    """``apply_force=False`` leaves J x B to the caller (the fused step adds it
+    inside its collision, before the force clamp)."""
     if not twin.enable_lorentz:
         return
     g.ensure_lorentz_fields()
@@ -88,5 +90,6 @@ def solve_lorentz(twin, g, arc_i, arc_j, arc_k):
     kernels.elec_prefix_bins(g.elec_rad_bins, g.n_elec_bins, g.nz)
     kernels.elec_B_axisymmetric(g.Bx, g.By, g.Bz, g.elec_rad_bins, arc_i, arc_j, g.dx,
                                 bin_dr_cells, MU0, g.n_elec_bins, g.nz)
-    kernels.apply_lorentz_JxB(g.Fx, g.Fy, g.Fz, g.Jx, g.Jy, g.Jz, g.Bx, g.By, g.Bz, g.f_l, g.flags,
-                              g.dt, g.dx, twin.mat.rho, g.FLAG_GAS)
+    if apply_force:
+        kernels.apply_lorentz_JxB(g.Fx, g.Fy, g.Fz, g.Jx, g.Jy, g.Jz, g.Bx, g.By, g.Bz, g.f_l,
+                                  g.flags, g.dt, g.dx, twin.mat.rho, g.FLAG_GAS)

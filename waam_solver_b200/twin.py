@@ -91,9 +91,9 @@ class WAAMTwin:
         self.grid = WAAMGrid(nx, ny, nz, dx, self.mat, max_tracers=max_tracers or 50_000,
                              allocate_lorentz=enable_lorentz, allocate_vof=True, device=device,
                              population_dtype=population_dtype)
-        if self.grid.population_storage and (step_mode != "fused" or enable_lorentz):
+        if self.grid.population_storage and step_mode != "fused":
             raise NotImplementedError("16-bit population storage runs on the fused step only "
-                                      "(step_mode='fused', no Lorentz force)")
+                                      "(step_mode='fused')")
         self.enable_droplet_impact_pressure = enable_droplet_impact_pressure
         self.use_recoil_clausius_clapeyron = use_recoil_clausius_clapeyron
         self.enable_substrate_growth = enable_substrate_growth
