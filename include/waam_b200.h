@@ -231,9 +231,32 @@ int waam_elec_build_sigma(float* sigma, const float* f_l, const int32_t* flags, 
 int waam_elec_inject_arc_source(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
                                 float arc_k, float sigma_cells, float current_A, float dx,
                                 void* stream);
+/* elec_clear_source + elec_inject_arc_source + elec_normalize_source
+ * (kernels.py:1255-1301, as physics/weld_forces.py:206-211 calls them) in two
+ * passes that read nothing: the normalising sum over the source's k slab,
+ * then every cell written once with its scaled value. */
+int waam_elec_arc_source(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
+                         float arc_k, float sigma_cells, float current_A, float dx,
+                         void* workspace, size_t workspace_bytes, void* stream);
 /* kernels.py:1288-1301 elec_normalize_source; the sum is taken in double */
 int waam_elec_normalize_source(float* source, int64_t n, float target_current_A, float dx,
                                void* workspace, size_t workspace_bytes, void* stream);
+/* elec_build_sigma plus a byte mask (fixed[c] = 1) of the cells the Jacobi
+ * sweep holds at 0: GAS, and SOLID at k <= nz_solid (kernels.py:1315-1355) */
+int waam_elec_build_sigma_mask(float* sigma, uint8_t* fixed, const float* f_l,
+                               const int32_t* flags, int nx, int ny, int nz, float sigma_liquid,
+                               float sigma_solid, int nz_solid, void* stream);
+/* n_sweeps elec_jacobi_step sweeps ping-ponging phi_a -> phi_b -> phi_a ...,
+ * the last one with elec_l1_diff of its output against its input into
+ * diff_buf / norm_buf (physics/weld_forces.py:235-245, one check chunk): the
+ * last iterate ends in phi_b for an odd n_sweeps, in phi_a for an even one.
+ * fixed is the mask of waam_elec_build_sigma_mask; the source must be 0
+ * outside the k slab of waam_elec_arc_source for (arc_k, sigma_cells). */
+int waam_elec_jacobi_chunk(float* phi_a, float* phi_b, const float* sigma, const float* source,
+                           const uint8_t* fixed, int nx, int ny, int nz, float dx, float omega_j,
+                           int n_sweeps, float arc_k, float sigma_cells, float* diff_buf,
+                           float* norm_buf, void* workspace, size_t workspace_bytes,
+                           void* stream);
 /* kernels.py:1304-1312 elec_init_ground (phi = 0) */
 int waam_elec_init_ground(float* phi, int64_t n, void* stream);
 /* kernels.py:1315-1355 elec_jacobi_step; phi_in and phi_out must differ */

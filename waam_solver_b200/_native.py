@@ -113,7 +113,7 @@ _CTYPES = {
     "void* const*": C.c_void_p, "const WaamMaterialTables*": C.POINTER(WaamMaterialTables),
     "WaamTelemetry*": C.c_void_p, "const WaamProbeSet*": C.POINTER(WaamProbeSet),
     "const WaamShiftPlane*": C.c_void_p, "const WaamExportChannel*": C.c_void_p,
-    "double*": C.c_void_p,
+    "double*": C.c_void_p, "uint8_t*": C.c_void_p, "const uint8_t*": C.c_void_p,
 }
 
 

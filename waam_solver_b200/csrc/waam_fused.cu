@@ -1137,7 +1137,9 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
     #undef WAAM_COLLIDE
         e = check_launch("k_collide_list");
         if (e) return e;
-        if (lorentz) {
+        // With VOF the column pass has set f_l = 0 on every SOLID cell, below the
+        // 0.05 the force needs: the pass is only run without VOF.
+        if (lorentz && !p->vof) {
             k_lorentz_solid<<<elem_blocks(d.n()), kThreads, 0, s>>>(
                 d.n(), f->flags, f->f_l, f->Fx, f->Fy, f->Fz, f->lorentz_J[0],
                 f->lorentz_J[1], f->lorentz_J[2], f->lorentz_B[0], f->lorentz_B[1], f->lorentz_B[2],

@@ -61,8 +61,10 @@ __device__ __forceinline__ double2 block_sum2(double a, double b) {
     return r;   // valid in thread 0
 }
 
-// Last-block combine of two per-block sums in block order; returns true in the
-// thread that holds the totals.
+// Last-block combine of two per-block sums: every thread of the last block
+// adds a fixed strided subset of the partials in order, then the fixed tree
+// of block_sum2 (the same order on every run).  Returns true in the thread
+// that holds the totals.  Blocks of kTileK x kTileJ threads.
 __device__ bool finish_sum2(Workspace ws, double2 part, double2& total) {
     __shared__ bool last;
     const int t = threadIdx.y * blockDim.x + threadIdx.x;
@@ -76,14 +78,16 @@ __device__ bool finish_sum2(Workspace ws, double2 part, double2& total) {
         last = prev == nb - 1;
     }
     __syncthreads();
-    if (!last || t != 0) return false;
+    if (!last) return false;
     __threadfence();
     double x = 0.0, y = 0.0;
-    for (unsigned q = 0; q < nb; ++q) {
+    for (unsigned q = t; q < nb; q += kTileK * kTileJ) {
         x += ((volatile double*)ws.partials)[q];
         y += ((volatile double*)ws.partials)[nb + q];
     }
-    total = make_double2(x, y);
+    const double2 r = block_sum2(x, y);
+    if (t != 0) return false;
+    total = r;
     *ws.counter = 0u;
     return true;
 }
@@ -98,18 +102,23 @@ __global__ void k_elec_sigma(float* sigma, const float* f_l, const int32_t* flag
     }
 }
 
+// The arc source value of cell (i, j, k) (kernels.py:1261-1284).
+__device__ __forceinline__ float elec_source_value(int i, int j, int k, float arc_i, float arc_j,
+                                                  float arc_k, float inv2s2, float current,
+                                                  float vol_eps, int k_min, int k_max) {
+    if (k < k_min || k > k_max) return 0.0f;
+    float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - arc_k;
+    float r2 = di * di + dj * dj + 0.25f * dk * dk;
+    return current * waam_expf(-r2 * inv2s2) / vol_eps;
+}
+
 // kernels.py:1255-1284 (clear + inject in one pass)
 __global__ void k_elec_source(Dims d, float* src, float arc_i, float arc_j, float arc_k,
                               float inv2s2, float current, float vol_eps, int k_min, int k_max) {
     int i, j, k, c;
     if (!tile_cell(d, i, j, k, c)) return;
-    float v = 0.0f;
-    if (k >= k_min && k <= k_max) {
-        float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - arc_k;
-        float r2 = di * di + dj * dj + 0.25f * dk * dk;
-        v = current * waam_expf(-r2 * inv2s2) / vol_eps;
-    }
-    src[c] = v;
+    src[c] = elec_source_value(i, j, k, arc_i, arc_j, arc_k, inv2s2, current, vol_eps, k_min,
+                               k_max);
 }
 
 // kernels.py:1288-1301, pass 1: sum(source * cell_vol) -> scale in ws scalars
@@ -139,6 +148,43 @@ __global__ void k_elec_source_sum(const float* src, int64_t n, float cell_vol, f
     float total = (float)t;
     ws.scalars[kOpScalarSourceScale] = current / fmax_(total, 1e-12f);
     *ws.counter = 0u;
+}
+
+// Clear + inject + normalise in two passes that read nothing: pass 1 sums
+// value * cell_vol over the slab k_min..k_max (every other cell is 0) in
+// double, fixed order; pass 2 writes value * scale everywhere, the float the
+// reference's in-place scaling leaves.
+__global__ void __launch_bounds__(kTileK* kTileJ)
+    k_elec_source_fused_sum(Dims d, float arc_i, float arc_j, float arc_k, float inv2s2,
+                            float current, float vol_eps, int k_min, int k_max, float cell_vol,
+                            float target, Workspace ws) {
+    double part = 0.0;
+    const int ks = imax(k_min, 0), ke = imin(k_max, d.nz - 1);
+    for (int i = blockIdx.z; i < d.nx; i += gridDim.z)
+        for (int jt = blockIdx.y; jt * kTileJ < d.ny; jt += gridDim.y)
+            for (int kt = blockIdx.x; ks + kt * kTileK <= ke; kt += gridDim.x) {
+                const int k = ks + kt * kTileK + threadIdx.x, j = jt * kTileJ + threadIdx.y;
+                if (k > ke || j >= d.ny) continue;
+                const float v = elec_source_value(i, j, k, arc_i, arc_j, arc_k, inv2s2, current,
+                                                  vol_eps, k_min, k_max);
+                part += (double)(v * cell_vol);
+            }
+    double2 tot;
+    if (finish_sum2(ws, block_sum2(part, 0.0), tot)) {
+        const float total = (float)tot.x;
+        ws.scalars[kOpScalarSourceScale] = target / fmax_(total, 1e-12f);
+    }
+}
+
+__global__ void k_elec_source_fused_write(Dims d, float* src, float arc_i, float arc_j,
+                                          float arc_k, float inv2s2, float current,
+                                          float vol_eps, int k_min, int k_max, Workspace ws) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
+    const float s = ws.scalars[kOpScalarSourceScale];
+    const float v = elec_source_value(i, j, k, arc_i, arc_j, arc_k, inv2s2, current, vol_eps,
+                                      k_min, k_max);
+    src[c] = v * s;
 }
 
 // kernels.py:1288-1301, pass 2
@@ -197,6 +243,72 @@ __global__ void __launch_bounds__(kTileK* kTileJ)
             *norm_out = (float)tot.y;
         }
     }
+}
+
+// The sweep of the fused solve: the same arithmetic as k_elec_jacobi, with
+// the fixed cells (GAS, and SOLID at k <= nz_solid) read from a byte mask
+// built with sigma, and the source read only inside its k slab (it is 0
+// elsewhere).  A tile grid (one cell per thread) for the plain sweeps; the
+// L1 sweep keeps the fixed reduction grid.
+template <bool L1>
+__global__ void __launch_bounds__(kTileK* kTileJ)
+    k_elec_jacobi_m(Dims d, const float* __restrict__ phi_in, float* __restrict__ phi_out,
+                    const float* __restrict__ sigma, const float* __restrict__ src,
+                    const uint8_t* __restrict__ fixed, float dx, float omega_j, int k_src_lo,
+                    int k_src_hi, float* diff_out, float* norm_out, Workspace ws) {
+    const float eps = 1e-12f;
+    const int sx = d.ny * d.nz, sy = d.nz;
+    double dsum = 0.0, nsum = 0.0;
+    const int i_step = L1 ? gridDim.z : d.nx, j_step = L1 ? gridDim.y : d.ny,
+              k_step = L1 ? gridDim.x : d.nz;
+    for (int i = blockIdx.z; i < d.nx; i += i_step)
+        for (int jt = blockIdx.y; jt * kTileJ < d.ny; jt += j_step)
+            for (int kt = blockIdx.x; kt * kTileK < d.nz; kt += k_step) {
+                const int k = kt * kTileK + threadIdx.x, j = jt * kTileJ + threadIdx.y;
+                if (k >= d.nz || j >= d.ny) continue;
+                const int c = (i * d.ny + j) * d.nz + k;
+                const float pin = phi_in[c];
+                float out;
+                if (fixed[c]) {
+                    out = 0.0f;
+                } else {
+                    const int ip = c + (i + 1 < d.nx ? sx : 0), im = c - (i > 0 ? sx : 0);
+                    const int jp = c + (j + 1 < d.ny ? sy : 0), jm = c - (j > 0 ? sy : 0);
+                    const int kp = c + (k + 1 < d.nz ? 1 : 0), km = c - (k > 0 ? 1 : 0);
+                    const float sp = sigma[ip], sm = sigma[im], sn = sigma[jp], ss = sigma[jm];
+                    const float st = sigma[kp], sb = sigma[km];
+                    const float sc = (k >= k_src_lo && k <= k_src_hi) ? src[c] : 0.0f;
+                    const float denom = sp + sm + sn + ss + st + sb + eps;
+                    const float nb = sp * phi_in[ip] + sm * phi_in[im] + sn * phi_in[jp] +
+                                     ss * phi_in[jm] + st * phi_in[kp] + sb * phi_in[km];
+                    const float pn = (nb + sc * dx * dx) / denom;
+                    out = (1.0f - omega_j) * pin + omega_j * pn;
+                }
+                phi_out[c] = out;
+                if (L1) {
+                    dsum += (double)fabsf(out - pin);
+                    nsum += (double)fabsf(pin);
+                }
+            }
+    if (L1) {
+        double2 part = block_sum2(dsum, nsum);
+        double2 tot;
+        if (finish_sum2(ws, part, tot)) {
+            *diff_out = (float)tot.x;
+            *norm_out = (float)tot.y;
+        }
+    }
+}
+
+// kernels.py:1237-1251 elec_build_sigma, plus the byte mask of the cells the
+// Jacobi sweep holds at 0 (kernels.py:1315-1355: GAS, SOLID at k <= nz_solid).
+__global__ void k_elec_sigma_mask(Dims d, float* sigma, uint8_t* fixed, const float* f_l,
+                                  const int32_t* flags, float s_liq, float s_sol, int nz_solid) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
+    const int fl = flags[c];
+    sigma[c] = fl == GAS ? 1e-8f : (f_l[c] > 0.55f ? s_liq : s_sol);
+    fixed[c] = (fl == GAS || (k <= nz_solid && fl == SOLID)) ? 1 : 0;
 }
 
 // kernels.py:1387-1398 elec_l1_diff as an operator
@@ -273,6 +385,64 @@ __global__ void k_elec_bin(Dims d, const float* __restrict__ Jz, double* acc, fl
         if (sbin[b] != 0.0) atomicAdd(&acc[(int64_t)k * n_bins + b], sbin[b]);
 }
 
+// The same sums without atomics: block (kt, ch) is one warp that owns k in
+// [32 kt, 32 kt + 32) of a contiguous chunk of columns and adds each column's
+// Jz dx^2 into its private shared double bins (lane k touches only its own
+// slots), column after column; the loads of 32 columns are in flight at a
+// time, coalesced along k, and lane u finds the bin of the u-th of them.  The
+// per-chunk bins go to partials[ch][b][k]; k_elec_bin_combine adds the chunks
+// in a fixed order, so the bins are the same on every run.
+constexpr int kBinUnroll = 32;
+
+__global__ void __launch_bounds__(32) k_elec_bin_cols(Dims d, const float* __restrict__ Jz,
+                                                      double* __restrict__ partials, float arc_i,
+                                                      float arc_j, float dx2, float bin_dr,
+                                                      int n_bins, int chunk) {
+    extern __shared__ double sacc[];   // [n_bins][32]
+    const int lane = threadIdx.x;
+    const int k = blockIdx.x * 32 + lane;
+    for (int b = 0; b < n_bins; ++b) sacc[b * 32 + lane] = 0.0;
+    const int ncol = d.nx * d.ny;
+    const int c0 = blockIdx.y * chunk, c1 = imin(ncol, c0 + chunk);
+    const bool kin = k < d.nz;
+    for (int col = c0; col < c1; col += kBinUnroll) {
+        float v[kBinUnroll];
+#pragma unroll
+        for (int u = 0; u < kBinUnroll; ++u)
+            v[u] = (kin && col + u < c1) ? Jz[(int64_t)(col + u) * d.nz + k] : 0.0f;
+        int my_bin = 0;
+        if (col + lane < c1) {
+            const int i = (col + lane) / d.ny, j = (col + lane) - i * d.ny;
+            float r;
+            my_bin = radial_bin((float)i - arc_i, (float)j - arc_j, bin_dr, n_bins, r);
+        }
+#pragma unroll
+        for (int u = 0; u < kBinUnroll; ++u) {
+            const int b = __shfl_sync(0xffffffffu, my_bin, u);
+            if (col + u < c1) sacc[b * 32 + lane] += (double)(v[u] * dx2);
+        }
+    }
+    if (!kin) return;
+    double* out = partials + (int64_t)blockIdx.y * n_bins * d.nz;
+    for (int b = 0; b < n_bins; ++b) out[(int64_t)b * d.nz + k] = sacc[b * 32 + lane];
+}
+
+// One warp per bin entry: lane l adds chunks l, l + 32, ... in order, then a
+// fixed shuffle tree.
+__global__ void k_elec_bin_combine(const double* __restrict__ partials, float* bins, int nz,
+                                   int n_bins, int chunks) {
+    const int64_t m = (int64_t)nz * n_bins;
+    const int lane = threadIdx.x & 31;
+    for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < m;
+         q += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int b = (int)(q % n_bins), k = (int)(q / n_bins);
+        double s = 0.0;
+        for (int ch = lane; ch < chunks; ch += 32) s += partials[((int64_t)ch * n_bins + b) * nz + k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) bins[q] = (float)s;
+    }
+}
+
 __global__ void k_elec_bin_store(const double* acc, float* bins, int64_t m) {
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m;
          q += (int64_t)gridDim.x * blockDim.x)
@@ -339,6 +509,13 @@ __global__ void k_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* __re
 
 using namespace waam;
 
+// k slab of the arc current source (kernels.py:1261-1284): cells outside
+// [k_min, k_max] get 0.
+static void source_slab(float arc_k, float sigma_cells, int nz, int& k_min, int& k_max) {
+    k_max = imin(nz, (int)(arc_k + sigma_cells * 4.0f) + 1);
+    k_min = imax(0, (int)(arc_k - sigma_cells));
+}
+
 #define REQUIRE(cond, msg) \
     if (!(cond)) return waam::fail(WAAM_ERR_INVALID, msg)
 
@@ -363,12 +540,42 @@ int waam_elec_inject_arc_source(float* source, int nx, int ny, int nz, float arc
     const float eps = 1e-6f;
     const float inv2s2 = 1.0f / (2.0f * sigma_cells * sigma_cells + eps);
     const float cell_vol = dx * dx * dx;
-    const int k_max = imin(nz, (int)(arc_k + sigma_cells * 4.0f) + 1);
-    const int k_min = imax(0, (int)(arc_k - sigma_cells));
+    int k_min, k_max;
+    source_slab(arc_k, sigma_cells, nz, k_min, k_max);
     Dims d{nx, ny, nz};
     k_elec_source<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
         d, source, arc_i, arc_j, arc_k, inv2s2, current_A, cell_vol + eps, k_min, k_max);
     return check_launch("k_elec_source");
+}
+
+int waam_elec_arc_source(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
+                         float arc_k, float sigma_cells, float current_A, float dx,
+                         void* workspace, size_t workspace_bytes, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_arc_source: bad dims");
+    REQUIRE(source, "elec_arc_source: null field");
+    REQUIRE(std::isfinite(arc_k) && std::isfinite(sigma_cells) && std::fabs(arc_k) < 1e6f &&
+                std::fabs(sigma_cells) < 1e6f,
+            "elec_arc_source: arc k / sigma not finite");
+    Dims d{nx, ny, nz};
+    REQUIRE(workspace_ok(workspace, workspace_bytes, d.n()),
+            "elec_arc_source: workspace too small or misaligned");
+    Workspace ws = Workspace::at(workspace);
+    const float eps = 1e-6f;
+    const float inv2s2 = 1.0f / (2.0f * sigma_cells * sigma_cells + eps);
+    const float cell_vol = dx * dx * dx;
+    int k_min, k_max;
+    source_slab(arc_k, sigma_cells, nz, k_min, k_max);
+    // a fixed grid: the sum order does not depend on the GPU
+    dim3 grid(imin((nz + kTileK - 1) / kTileK, 4), imin((ny + kTileJ - 1) / kTileJ, 16),
+              imin(nx, 64));
+    k_elec_source_fused_sum<<<grid, tile_block(), 0, STREAM(stream)>>>(
+        d, arc_i, arc_j, arc_k, inv2s2, current_A, cell_vol + eps, k_min, k_max, cell_vol,
+        current_A, ws);
+    int rc = check_launch("k_elec_source_fused_sum");
+    if (rc) return rc;
+    k_elec_source_fused_write<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
+        d, source, arc_i, arc_j, arc_k, inv2s2, current_A, cell_vol + eps, k_min, k_max, ws);
+    return check_launch("k_elec_source_fused_write");
 }
 
 int waam_elec_normalize_source(float* source, int64_t n, float target_current_A, float dx,
@@ -424,6 +631,55 @@ int waam_elec_jacobi_step_l1(const float* phi_in, float* phi_out, const float* s
     return check_launch("k_elec_jacobi_l1");
 }
 
+int waam_elec_build_sigma_mask(float* sigma, uint8_t* fixed, const float* f_l,
+                               const int32_t* flags, int nx, int ny, int nz, float sigma_liquid,
+                               float sigma_solid, int nz_solid, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_build_sigma_mask: bad dims");
+    REQUIRE(sigma && fixed && f_l && flags, "elec_build_sigma_mask: null field");
+    Dims d{nx, ny, nz};
+    k_elec_sigma_mask<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
+        d, sigma, fixed, f_l, flags, sigma_liquid, sigma_solid, nz_solid);
+    return check_launch("k_elec_sigma_mask");
+}
+
+int waam_elec_jacobi_chunk(float* phi_a, float* phi_b, const float* sigma, const float* source,
+                           const uint8_t* fixed, int nx, int ny, int nz, float dx, float omega_j,
+                           int n_sweeps, float arc_k, float sigma_cells, float* diff_buf,
+                           float* norm_buf, void* workspace, size_t workspace_bytes,
+                           void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_jacobi_chunk: bad dims");
+    REQUIRE(phi_a && phi_b && sigma && source && fixed && diff_buf && norm_buf && phi_a != phi_b,
+            "elec_jacobi_chunk: null or aliased field");
+    REQUIRE(n_sweeps >= 1, "elec_jacobi_chunk: n_sweeps must be >= 1");
+    REQUIRE(std::isfinite(arc_k) && std::isfinite(sigma_cells) && std::fabs(arc_k) < 1e6f &&
+                std::fabs(sigma_cells) < 1e6f,
+            "elec_jacobi_chunk: arc k / sigma not finite");
+    Dims d{nx, ny, nz};
+    REQUIRE(workspace_ok(workspace, workspace_bytes, d.n()),
+            "elec_jacobi_chunk: workspace too small or misaligned");
+    int k_lo, k_hi;
+    source_slab(arc_k, sigma_cells, nz, k_lo, k_hi);
+    float* in = phi_a;
+    float* out = phi_b;
+    for (int s = 0; s < n_sweeps; ++s) {
+        if (s + 1 < n_sweeps) {
+            k_elec_jacobi_m<false><<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
+                d, in, out, sigma, source, fixed, dx, omega_j, k_lo, k_hi, nullptr, nullptr,
+                Workspace{});
+        } else {
+            k_elec_jacobi_m<true><<<red_tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
+                d, in, out, sigma, source, fixed, dx, omega_j, k_lo, k_hi, diff_buf, norm_buf,
+                Workspace::at(workspace));
+        }
+        int rc = check_launch("k_elec_jacobi_m");
+        if (rc) return rc;
+        float* t = in;
+        in = out;
+        out = t;
+    }
+    return WAAM_OK;
+}
+
 int waam_elec_l1_diff(const float* a, const float* b, float* diff_buf, float* norm_buf, int nx,
                       int ny, int nz, void* workspace, size_t workspace_bytes, void* stream) {
     REQUIRE(dims_ok(nx, ny, nz), "elec_l1_diff: bad dims");
@@ -461,9 +717,29 @@ int waam_elec_bin_axial_current(const float* Jz, float* bins, int nx, int ny, in
             "elec_bin_axial_current: nz * n_bins accumulators exceed the workspace");
     Workspace ws = Workspace::at(workspace);
     double* acc = reinterpret_cast<double*>(ws.field);
+    const int ncol = nx * ny;
+    {
+        // chunked per-warp bins in the field scratch, when they fit
+        const size_t field_bytes = (size_t)(d.n() + kFieldSlack) * sizeof(float);
+        const int ktiles = (nz + 31) / 32;
+        int chunks = imax(1, (148 * 12) / ktiles);
+        chunks = imin(chunks, ncol);
+        chunks = (int)std::min<int64_t>(chunks, (int64_t)(field_bytes / ((size_t)m * sizeof(double))));
+        if (chunks >= 1 && (size_t)n_bins * 32 * sizeof(double) <= 48 * 1024) {
+            const int chunk = (ncol + chunks - 1) / chunks;
+            chunks = (ncol + chunk - 1) / chunk;
+            k_elec_bin_cols<<<dim3(ktiles, chunks), 32, (size_t)n_bins * 32 * sizeof(double),
+                              STREAM(stream)>>>(d, Jz, acc, arc_i, arc_j, dx * dx, bin_dr_cells,
+                                                n_bins, chunk);
+            int rc = check_launch("k_elec_bin_cols");
+            if (rc) return rc;
+            k_elec_bin_combine<<<elem_blocks(m * 32), kThreads, 0, STREAM(stream)>>>(
+                acc, bins, nz, n_bins, chunks);
+            return check_launch("k_elec_bin_combine");
+        }
+    }
     cudaError_t e = cudaMemsetAsync(acc, 0, (size_t)m * sizeof(double), STREAM(stream));
     if (e != cudaSuccess) return fail(WAAM_ERR_CUDA, cudaGetErrorString(e));
-    const int ncol = nx * ny;
     const int strips = imax(1, imin((ncol + kThreads - 1) / kThreads, imax(1, 1184 / nz)));
     k_elec_bin<<<dim3(strips, nz), kThreads, n_bins * sizeof(double), STREAM(stream)>>>(
         d, Jz, acc, arc_i, arc_j, dx * dx, bin_dr_cells, n_bins);

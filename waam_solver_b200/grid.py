@@ -155,6 +155,8 @@ class WAAMGrid:
         self.phi_elec, self.phi_elec_tmp, self.sigma_elec, self.elec_source = mk(), mk(), mk(), mk()
         self.Jx, self.Jy, self.Jz = mk(), mk(), mk()
         self.Bx, self.By, self.Bz = mk(), mk(), mk()
+        # cells the potential solve holds at 0 (GAS, grounded SOLID), one byte each
+        self.elec_fixed = torch.zeros(self._shape3, dtype=torch.uint8, device=self.device)
         self.n_elec_bins = 64
         self.elec_rad_bins = torch.zeros((self.nz, self.n_elec_bins), dtype=torch.float32,
                                          device=self.device)

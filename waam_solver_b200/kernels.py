@@ -667,6 +667,31 @@ def elec_build_sigma(sigma, f_l, flags, sigma_liquid, sigma_solid, FLAG_GAS):
           float(sigma_liquid), float(sigma_solid), _stream())
 
 
+def elec_build_sigma_mask(sigma, fixed, f_l, flags, sigma_liquid, sigma_solid, nz_solid):
+    """elec_build_sigma plus the uint8 mask of the cells the Jacobi sweep holds at 0."""
+    nx, ny, nz = _dims(sigma)
+    if fixed.dtype != torch.uint8 or tuple(fixed.shape) != (nx, ny, nz):
+        raise WaamError("elec_build_sigma_mask: fixed must be uint8 (nx, ny, nz)")
+    n = nx * ny * nz
+    _call("waam_elec_build_sigma_mask", _f(sigma, n), fixed.data_ptr(), _f(f_l, n),
+          _i(flags, n), nx, ny, nz, float(sigma_liquid), float(sigma_solid), int(nz_solid),
+          _stream())
+
+
+def elec_jacobi_chunk(phi_a, phi_b, sigma, source, fixed, dx, omega_j, n_sweeps, arc_k,
+                      sigma_cells, diff_buf, norm_buf):
+    """n_sweeps Jacobi sweeps phi_a -> phi_b -> ..., the last with the L1 check;
+    the last iterate ends in phi_b when n_sweeps is odd, else in phi_a."""
+    nx, ny, nz = _dims(phi_a)
+    if fixed.dtype != torch.uint8 or tuple(fixed.shape) != (nx, ny, nz):
+        raise WaamError("elec_jacobi_chunk: fixed must be uint8 (nx, ny, nz)")
+    n = nx * ny * nz
+    ws, wsb = workspace_for(phi_a)
+    _call("waam_elec_jacobi_chunk", _f(phi_a, n), _f(phi_b, n), _f(sigma, n), _f(source, n),
+          fixed.data_ptr(), nx, ny, nz, float(dx), float(omega_j), int(n_sweeps), float(arc_k),
+          float(sigma_cells), _f(diff_buf, 1), _f(norm_buf, 1), ws, wsb, _stream())
+
+
 def elec_clear_source(source):
     source.zero_()
 
@@ -677,6 +702,14 @@ def elec_inject_arc_source(source, arc_i, arc_j, arc_k, sigma_cells, current_A, 
         raise WaamError("elec_inject_arc_source: nz=%d does not match the field (%d)" % (nz, nz_))
     _call("waam_elec_inject_arc_source", _f(source), nx, ny, nz_, float(arc_i), float(arc_j),
           float(arc_k), float(sigma_cells), float(current_A), float(dx), _stream())
+
+
+def elec_arc_source(source, arc_i, arc_j, arc_k, sigma_cells, current_A, dx):
+    """elec_clear_source + elec_inject_arc_source + elec_normalize_source in one call."""
+    nx, ny, nz = _dims(source)
+    ws, wsb = workspace_for(source)
+    _call("waam_elec_arc_source", _f(source), nx, ny, nz, float(arc_i), float(arc_j),
+          float(arc_k), float(sigma_cells), float(current_A), float(dx), ws, wsb, _stream())
 
 
 def elec_normalize_source(source, target_current_A, dx):

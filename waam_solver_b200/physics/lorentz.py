@@ -6,11 +6,14 @@ electric potential with a relative-L1 convergence check every ten sweeps,
 current density, axisymmetric self field from the enclosed axial current and
 the f_l-weighted J x B body force added to F.
 
-Two differences of form, not of result: the potential ping-pongs between
+Differences of form, not of result: the potential ping-pongs between
 ``phi_elec`` and ``phi_elec_tmp`` instead of copying the new iterate back
 (after the solve ``phi_elec`` holds the last iterate, ``phi_elec_tmp`` the one
-before it), and the L1 change is computed inside the last sweep of each chunk
-of ten -- the only sweep whose L1 the reference reads.
+before it); each chunk of ten sweeps is one native call whose last sweep also
+computes the L1 change -- the only sweep whose L1 the reference reads; the
+sweeps read the fixed cells from a byte mask built with the conductivity map
+and the source only inside its k slab (it is 0 elsewhere); and clearing,
+injecting and normalising the source is one call.
 """
 from __future__ import annotations
 
@@ -35,11 +38,10 @@ def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True):
     if not twin.enable_lorentz:
         return
     g.ensure_lorentz_fields()
-    kernels.elec_build_sigma(g.sigma_elec, g.f_l, g.flags, twin.sigma_liquid_Sm,
-                             twin.sigma_solid_Sm, g.FLAG_GAS)
-    kernels.elec_inject_arc_source(g.elec_source, arc_i, arc_j, arc_k, twin.sigma_cells,
-                                   twin.welding_current_A, g.dx, g.nz)
-    kernels.elec_normalize_source(g.elec_source, twin.welding_current_A, g.dx)
+    kernels.elec_build_sigma_mask(g.sigma_elec, g.elec_fixed, g.f_l, g.flags,
+                                  twin.sigma_liquid_Sm, twin.sigma_solid_Sm, twin.nz_solid)
+    kernels.elec_arc_source(g.elec_source, arc_i, arc_j, arc_k, twin.sigma_cells,
+                            twin.welding_current_A, g.dx)
 
     cold_start = not getattr(twin, "_lorentz_warm", False)
     if cold_start:
@@ -53,19 +55,12 @@ def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True):
     rel = float("inf")
     while iters_done < max_iters:
         chunk = min(check_every, max_iters - iters_done)
-        for c in range(chunk):
-            if c == chunk - 1:
-                kernels.elec_jacobi_step_l1(g.phi_elec, g.phi_elec_tmp, g.sigma_elec,
-                                            g.elec_source, g.flags, g.dx,
-                                            twin.lorentz_jacobi_omega, twin.nz_solid,
-                                            g.elec_res_buf, g.elec_norm_buf)
-            else:
-                kernels.elec_jacobi_step(g.phi_elec, g.phi_elec_tmp, g.sigma_elec,
-                                         g.elec_source, g.flags, g.dx,
-                                         twin.lorentz_jacobi_omega, g.FLAG_GAS, g.FLAG_SOLID,
-                                         twin.nz_solid, g.nx, g.ny, g.nz)
+        kernels.elec_jacobi_chunk(g.phi_elec, g.phi_elec_tmp, g.sigma_elec, g.elec_source,
+                                  g.elec_fixed, g.dx, twin.lorentz_jacobi_omega, chunk, arc_k,
+                                  twin.sigma_cells, g.elec_res_buf, g.elec_norm_buf)
+        if chunk % 2 == 1:
             g.phi_elec, g.phi_elec_tmp = g.phi_elec_tmp, g.phi_elec
-            iters_done += 1
+        iters_done += chunk
         rel = float(g.elec_res_buf.item()) / max(float(g.elec_norm_buf.item()), 1e-30)
         if rel < tol:
             converged = True
