@@ -10,6 +10,15 @@ collision, torch on a straight 40 mm line at 8 mm/s.  Synthetic inputs: the
 run starts from the reference's reset state and spins up (droplets deposit a
 bead) before timing.  One step = one ``WAAMTwin.step``.
 
+``--workload large``: the large FP16-storage case -- 512x256x160 lattice,
+dx = 0.15 mm, float16 population offsets, the same arc, wire and surface
+physics plus the welding current's Lorentz force (140 A) and convective heat
+losses, on a two-layer path of three parallel 60 mm beads (4 mm pitch, 8 mm/s;
+the arc off on the moves between beads; a 5 s dwell; the second layer offset
+2 mm).  ``--compare-steps N`` runs that workload N steps from reset in its own
+storage and in float32 and reports remelt depth, HAZ peak temperature, pool
+width / depth and peak temperature of both.
+
 ``python bench.py [--gpus N] [--steps K] [--warmup W]`` prints one JSON line.
 Under torchrun every rank runs an independent replica (the step has no
 cross-GPU exchange), timing is the max over ranks.
@@ -50,6 +59,23 @@ WORKLOADS = {
         arc_efficiency=0.75, arc_sigma_mm=3.0, droplet_freq_hz=0.0, enable_vof=True,
         plate_thickness_mm=4.0, use_srt=False, travel_speed_m_s=0.008,
         path_mm=((4.0, 4.0), (14.0, 4.0)), spinup=200),
+    "large": dict(
+        workload="two-layer multi-bead 512x256x160 D3Q19, dx 0.15 mm, float16 population "
+                 "storage, Goldak 4 kW, 100 Hz wire droplets, Lorentz force (140 A) + arc "
+                 "pressure, convective heat losses, VOF+wetting 30deg+CSF+Marangoni+buoyancy+"
+                 "gravity, central-moment MRT; 3 x 60 mm beads, pitch 4 mm, 8 mm/s, 5 s dwell, "
+                 "second layer offset 2 mm",
+        nx=512, ny=256, nz=160, dx=1.5e-4, heat_source="goldak", arc_power_W=4000.0,
+        arc_efficiency=0.78, goldak_mm=dict(a_front_mm=3.0, a_rear_mm=9.0, b_mm=3.0, c_mm=3.0,
+                                            ff=0.6, fr=1.4),
+        droplet_freq_hz=100.0, wire_feed_m_s=0.1, wire_diameter_mm=1.2, enable_vof=True,
+        enable_wetting=True, contact_angle_deg=30.0, enable_csf_tension=True,
+        enable_hydrostatic_gravity=True, use_srt=False, travel_speed_m_s=0.008,
+        enable_heat_loss=True, enable_lorentz=True, welding_current_A=140.0,
+        population_dtype="float16",
+        beads=dict(x0_mm=8.4, length_mm=60.0, y0_mm=15.2, pitch_mm=4.0, n=3, layers=2,
+                   layer_offset_mm=2.0, dwell_s=5.0),
+        path_mm=((8.4, 15.2), (68.4, 15.2)), spinup=200),
 }
 
 MATERIAL = dict(k=30.0, rho=7800.0, cp=680.0, T_solidus=1723.0, T_liquidus=1783.0,
@@ -69,17 +95,19 @@ def twin_kwargs(w):
     keys = ("heat_source", "arc_power_W", "arc_efficiency", "droplet_freq_hz", "enable_vof",
             "enable_wetting", "contact_angle_deg", "enable_csf_tension",
             "enable_hydrostatic_gravity", "use_srt", "travel_speed_m_s", "arc_sigma_mm",
-            "wire_diameter_mm", "enable_heat_loss")
+            "wire_diameter_mm", "enable_heat_loss", "enable_lorentz", "welding_current_A")
     return {k: w[k] for k in keys if k in w}
 
 
-def build_twin(w, device, population_dtype="float32", tables=None):
+def build_twin(w, device, population_dtype=None, tables=None):
     from waam_solver_b200 import WAAMTwin
     from waam_solver_b200.materials import from_constants
     from waam_solver_b200.physics.arc import goldak_from_job_mm
     mat = from_constants("ER70S-6-constants", MATERIAL, contact_angle_deg=w.get("contact_angle_deg", 30.0))
     if tables is not None:
         mat.tables = tables
+    if population_dtype is None:
+        population_dtype = w.get("population_dtype", "float32")
     tw = WAAMTwin(material=mat, nx=w["nx"], ny=w["ny"], nz=w["nz"], dx=w["dx"], max_tracers=1024,
                   device=device, population_dtype=population_dtype, **twin_kwargs(w))
     if w.get("plate_thickness_mm"):
@@ -103,6 +131,40 @@ def positions(w, dt, n, start=0):
         d = min(s * dt * w["travel_speed_m_s"], L)
         u = d / L
         out.append((x0 * 1e-3 + u * (x1 - x0) * 1e-3, y0 * 1e-3 + u * (y1 - y0) * 1e-3))
+    return out
+
+
+def path_steps(w, dt, n):
+    """(x, y, welding) of the first n steps.  A workload with ``beads``: bead
+    after bead along +x at the travel speed with the arc on, the moves between
+    beads (back to the next bead's start) at the travel speed with the arc off,
+    the dwell between layers parked with the arc off."""
+    b = w.get("beads")
+    if not b:
+        return [(x, y, True) for x, y in positions(w, dt, n)]
+    v = w["travel_speed_m_s"]
+    segs = []          # (x0, y0, x1, y1, duration_s, welding)
+    for layer in range(b["layers"]):
+        for k in range(b["n"]):
+            y = (b["y0_mm"] + k * b["pitch_mm"] + layer * b["layer_offset_mm"]) * 1e-3
+            x0, x1 = b["x0_mm"] * 1e-3, (b["x0_mm"] + b["length_mm"]) * 1e-3
+            if segs:
+                px, py = segs[-1][2], segs[-1][3]
+                L = math.hypot(x0 - px, y - py)
+                segs.append((px, py, x0, y, L / v, False))
+            segs.append((x0, y, x1, y, (x1 - x0) / v, True))
+        if layer + 1 < b["layers"]:
+            px, py = segs[-1][2], segs[-1][3]
+            segs.append((px, py, px, py, b["dwell_s"], False))
+    out, t, si, t0 = [], 0.0, 0, 0.0
+    for s in range(n):
+        t = s * dt
+        while si < len(segs) - 1 and t >= t0 + segs[si][4]:
+            t0 += segs[si][4]
+            si += 1
+        x0, y0, x1, y1, dur, wl = segs[si]
+        u = min(1.0, (t - t0) / dur) if dur > 0 else 1.0
+        out.append((x0 + u * (x1 - x0), y0 + u * (y1 - y0), wl))
     return out
 
 
@@ -166,7 +228,7 @@ def census(twin):
     return dict(n=n, solid=solid, gas=gas, fluid=n - solid - gas)
 
 
-def algorithmic_bytes(c, tail_on=False):
+def algorithmic_bytes(c, tail_on=False, pop_bytes=4):
     """Compulsory DRAM bytes per launch of each fused stage (FP32 fields, int32
     flags), from the cell census; each field element read or written once.
 
@@ -178,6 +240,7 @@ def algorithmic_bytes(c, tail_on=False):
       column     phi_tmp, phi, flags r+w, f_l: n; T, 3 time-above r+w: ng; list: na
       collide    list, f_l, phi, T, flags, 19 f reads, 19 f writes, rho, u (3), F (3): na
       stream     flags: n; 19 f reads + 19 f writes: ns
+    (populations of pop_bytes each: 4 for float32, 2 for the 16-bit forms)
       tail       flags: n; T, phi, f_l: ng (only when remelt / solidify run)
     Neighbour reads of the stencils are cache hits and are not counted.
     """
@@ -187,8 +250,8 @@ def algorithmic_bytes(c, tail_on=False):
         "thermal": 20 * n + 24 * ng + 12 * na,
         "vof_advect": 12 * n + 12 * na,
         "column": 20 * n + 28 * ng + 4 * na,
-        "collide": 200 * na,
-        "stream": 4 * n + 152 * ns,
+        "collide": (48 + 38 * pop_bytes) * na,
+        "stream": 4 * n + 38 * pop_bytes * ns,
         "tail": (4 * n + 12 * ng) if tail_on else 0,
     }
 
@@ -436,6 +499,114 @@ def adjoint_form(device, n_steps=None, fd=True):
     return out
 
 
+def jacobi_timing(tw, reps=10):
+    """The potential solve's sweep as the step runs it: 10-sweep chunks over the
+    live-cell list of the twin's current state (the production entry point),
+    timed with CUDA events on copies of the potential buffers."""
+    import torch
+    from waam_solver_b200 import kernels
+    g = tw.grid
+    a, b = g.phi_elec.clone(), g.phi_elec_tmp.clone()
+    res, nrm = torch.zeros((), device=a.device), torch.zeros((), device=a.device)
+    arc_k = float(g.step_scalars[0].item())
+    call = lambda: kernels.elec_jacobi_live(  # noqa: E731
+        a, b, g.sigma_elec, g.elec_source, g.elec_live, g.elec_zero, g.elec_counts, g.dx,
+        tw.lorentz_jacobi_omega, 10, False, arc_k, tw.sigma_cells, res, nrm)
+    call()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / (10 * reps)
+    live = int(g.elec_counts[0].item())
+    # per live cell: phi in, phi out, sigma (4 B each) and its list entry (4 B),
+    # the source (4 B) inside its k slab; neighbour reads are cache hits
+    nbytes = 20 * live
+    return {"sweeps_per_step": int(tw._lorentz_last_iters), "live_cells": live,
+            "ms_per_sweep": ms, "bytes_per_sweep": nbytes,
+            "sweep_GBps": nbytes / (ms * 1e-3) / 1e9,
+            "timing": "10-sweep chunks over the live-cell list of the state after the "
+                      "stage-timing steps, CUDA events, %d repetitions" % reps}
+
+
+def melt_metrics(tw):
+    """Remelt depth, HAZ peak temperature and pool size from the step's fields.
+
+    remelt depth: how far below the original plate top (k = nz_solid - 1) the
+    metal reached the solidus (T_max >= T_s); HAZ T_max: the highest T_max in
+    the substrate plane 1 mm below the deepest remelted cell; pool width /
+    depth: extent of f_l > 0.5 across y and down from the top of the pool in
+    the x section through the pool's centroid."""
+    import numpy as np
+    g = tw.grid
+    Ts = tw.mat.T_solidus
+    tmax = g.T_max.cpu().numpy().astype(np.float64)
+    flags = g.flags.cpu().numpy()
+    fl = g.f_l.cpu().numpy() > 0.5
+    nzs = tw.nz_solid
+    sub = tmax[:, :, :nzs]
+    melted = np.nonzero((sub >= Ts).any(axis=(0, 1)))[0]
+    k_melt = int(melted.min()) if melted.size else nzs
+    depth_cells = nzs - k_melt
+    k_haz = max(0, min(nzs - 1, k_melt - int(round(1e-3 / g.dx))))
+    out = {"remelt_depth_mm": depth_cells * g.dx * 1e3, "remelt_depth_cells": depth_cells,
+           "haz_plane_k": k_haz, "haz_T_max_K": float(tmax[:, :, k_haz].max()),
+           "T_max_peak_K": float(tmax[flags != 2].max()) if (flags != 2).any() else None,
+           "pool_width_cells": 0, "pool_depth_cells": 0,
+           "H_total_J": float(g.H.double().sum().item()) * g.dx ** 3}
+    if fl.any():
+        ii = np.nonzero(fl)[0]
+        sect = fl[int(round(ii.mean()))]
+        ys, zs = np.nonzero(sect.any(axis=1))[0], np.nonzero(sect.any(axis=0))[0]
+        if ys.size:
+            out["pool_width_cells"] = int(ys[-1] - ys[0] + 1)
+            out["pool_depth_cells"] = int(zs[-1] - zs[0] + 1)
+    return out
+
+
+def storage_comparison(w, device, n_steps):
+    """The workload from reset for n_steps in its own population storage and
+    in float32: sustained MLUPS of each run (CUDA events around all steps) and
+    the melt metrics of both."""
+    import torch
+    out = {"steps": n_steps}
+    forms = [w.get("population_dtype", "float32")]
+    if forms[0] != "float32":
+        forms.append("float32")
+    for dtype in forms:
+        tw = build_twin(w, device, population_dtype=dtype)
+        g = tw.grid
+        path = path_steps(w, g.dt, n_steps)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for x, y, wl in path:
+            tw.step(x, y, wl)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / n_steps
+        m = melt_metrics(tw)
+        m.update(ms_per_step=ms, MLUPS=g.n_cells / (ms * 1e-3) / 1e6,
+                 droplets=tw._n_droplets_fired, lorentz_unconverged=tw._lorentz_unconverged)
+        out[dtype] = m
+        del tw, g
+        torch.cuda.empty_cache()
+    if len(forms) == 2:
+        a, b = out[forms[0]], out["float32"]
+        out["difference"] = {
+            "remelt_depth_cells": a["remelt_depth_cells"] - b["remelt_depth_cells"],
+            "haz_T_max_rel": (a["haz_T_max_K"] - b["haz_T_max_K"]) / b["haz_T_max_K"],
+            "T_max_peak_rel": (a["T_max_peak_K"] - b["T_max_peak_K"]) / b["T_max_peak_K"],
+            "pool_width_cells": a["pool_width_cells"] - b["pool_width_cells"],
+            "pool_depth_cells": a["pool_depth_cells"] - b["pool_depth_cells"],
+            "H_total_rel": (a["H_total_J"] - b["H_total_J"]) / b["H_total_J"],
+            "speedup": b["ms_per_step"] / a["ms_per_step"]}
+    return out
+
+
 def run_b200(args, w):
     import torch
     from waam_solver_b200 import _native
@@ -445,16 +616,18 @@ def run_b200(args, w):
     g = tw.grid
     cells = g.n_cells
     total = w["spinup"] + args.warmup + 2 * args.steps + min(args.steps, 400) + 4
-    pos = positions(w, g.dt, total)
+    pos = path_steps(w, g.dt, total)
+    lorentz = bool(w.get("enable_lorentz"))
+    pb = 2 if g.population_storage else 4
     s = 0
     for _ in range(w["spinup"] + args.warmup):
-        tw.step(*pos[s], True)
+        tw.step(*pos[s])
         s += 1
     torch.cuda.synchronize()
 
     # ---- device-resident run (value): positions staged on the device ----
     K = args.steps
-    dev_pos_all = torch.tensor([[x / g.dx, y / g.dx] for x, y in pos[s:s + K]],
+    dev_pos_all = torch.tensor([[x / g.dx, y / g.dx] for x, y, _ in pos[s:s + K]],
                                dtype=torch.float32, device=device)
     dev_pos = [dev_pos_all[k] for k in range(K)]
     drops0 = tw._n_droplets_fired
@@ -467,7 +640,7 @@ def run_b200(args, w):
         start.record()
         for k in range(K):
             tw._device_position = dev_pos[k]
-            tw.step(*pos[s], True)
+            tw.step(*pos[s])
             s += 1
         stop.record()
         host_ms = (time.perf_counter() - t_host) * 1e3 / K
@@ -482,32 +655,56 @@ def run_b200(args, w):
     Ks = min(K, 400)
     ev_sets = [[torch.cuda.Event(enable_timing=True) for _ in range(7)] for _ in range(Ks)]
     ev_pre = [torch.cuda.Event(enable_timing=True) for _ in range(Ks)]
+    ev_lz = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+             for _ in range(Ks)]
     for es in ev_sets:
         for e in es:
             e.record()
+    for es in ev_lz:
+        for e in es:
+            e.record()
     torch.cuda.synchronize()
-    pre_steps = []
+    pre_steps, lz_steps = [], []
     for k in range(Ks):
         tw._stage_events = ev_sets[k]
+        tw._lorentz_events = ev_lz[k] if lorentz else None
         due = tw._n_droplets_fired
         ev_pre[k].record()
-        tw.step(*pos[s], True)
+        x, y, wl = pos[s]
+        tw.step(x, y, wl)
         if tw._n_droplets_fired == due:
             pre_steps.append(k)     # the pre stage of droplet steps includes the deposition
+        if lorentz and wl:
+            lz_steps.append(k)
         s += 1
     torch.cuda.synchronize()
     tw._stage_events = None
+    tw._lorentz_events = None
     stage_ms = {"pre": statistics.fmean(ev_pre[k].elapsed_time(ev_sets[k][0]) for k in pre_steps)}
     for i, name in enumerate(STAGES):
         stage_ms[name] = statistics.fmean(es[i].elapsed_time(es[i + 1]) for es in ev_sets)
+    lz_info = None
+    if lz_steps:
+        # the potential solve runs between the column pass and the collision
+        lz_ms = statistics.fmean(ev_lz[k][0].elapsed_time(ev_lz[k][1]) for k in lz_steps)
+        stage_ms["lorentz_solve"] = lz_ms
+        stage_ms["collide"] = statistics.fmean(
+            ev_sets[k][3].elapsed_time(ev_sets[k][4]) - ev_lz[k][0].elapsed_time(ev_lz[k][1])
+            for k in lz_steps)
+        lz_info = jacobi_timing(tw)
     c = census(tw)
-    algo = algorithmic_bytes(c, tw.enable_bead_freeze or tw.enable_substrate_growth)
+    algo = algorithmic_bytes(c, tw.enable_bead_freeze or tw.enable_substrate_growth, pb)
     hbm, hbm_src = peaks()
     dom = max(("stream", "collide", "thermal", "column", "vof_advect"),
               key=lambda k: stage_ms[k])
-    achieved = algo[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    dom_ms, dom_bytes, kernel = stage_ms[dom], algo[dom], "k_" + dom
+    if lz_info and lz_info["ms_per_sweep"] * tw._lorentz_last_iters > dom_ms:
+        dom, kernel = "jacobi", "k_elec_jacobi_live"
+        dom_ms, dom_bytes = lz_info["ms_per_sweep"], lz_info["bytes_per_sweep"]
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic_%s.json" % dom)
+    tpath = os.path.join(ROOT, "profiles", "traffic_%s%s.json" % (
+        dom, "_f16" if pb == 2 and dom in ("stream", "collide") else ""))
     if os.path.exists(tpath):
         with open(tpath) as fh:
             t = json.load(fh)
@@ -519,6 +716,10 @@ def run_b200(args, w):
     pre = lib.waam_step_launch_count(tw._fused_params, 0)
     launches_graph = pre + lib.waam_step_launch_count(tw._fused_params, 1)
     launches_events = pre + lib.waam_step_launch_count(tw._fused_params, 2)
+    if lorentz:
+        # sigma + mask, source (2), the sweeps, J, bins (2), prefix, B
+        launches_graph += 8 + tw._lorentz_last_iters
+        launches_events += 8 + tw._lorentz_last_iters
 
     # ---- end-to-end run through the public API with host inputs / outputs ----
     probe = (g.nx // 2) * g.ny * g.nz + (g.ny // 2) * g.nz + tw.nz_solid - 1
@@ -529,7 +730,7 @@ def run_b200(args, w):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for k in range(K):
-        tw.step(*pos[s], True)           # torch position from the host (pinned H2D, 8 B)
+        tw.step(*pos[s])                 # torch position from the host (pinned H2D, 8 B)
         s += 1
         host_out[k:k + 1].copy_(g.T.view(-1)[probe:probe + 1], non_blocking=True)  # D2H, 4 B
     e1.record()
@@ -546,12 +747,13 @@ def run_b200(args, w):
         "data": "synthetic (reference reset state + %d spin-up steps)" % w["spinup"],
         "config": {"workload": w["workload"], "cells": cells, "global_batch": world,
                    "parallelism": "replicas x%d" % world, "l2": "inputs larger than L2 "
-                   "(populations %.0f MB)" % (2 * 19 * cells * 4 / 1e6),
+                   "(populations %.0f MB)" % (2 * 19 * cells * pb / 1e6),
+                   "population_storage": "float16" if pb == 2 else "float32",
                    "droplets_in_timed_region": drops},
-        "roofline": {"bound": "hbm", "kernel": "k_" + ("stream" if dom == "stream" else dom),
+        "roofline": {"bound": "hbm", "kernel": kernel,
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "peak_source": hbm_src,
-                     "algorithmic_bytes_per_launch": algo[dom]},
+                     "algorithmic_bytes_per_launch": dom_bytes},
         "stages_ms": stage_ms,
         "step_algorithmic_GBps": step_bytes / (ms / K * 1e-3) / 1e9,
         "host_enqueue_ms_per_step": host_ms,
@@ -559,17 +761,24 @@ def run_b200(args, w):
         "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 4},
         "gpu_launches": int(launches_graph * 2 * K + launches_events * Ks),
         "stage_timing": "events between the fused kernels over %d instrumented steps "
-                        "(eager launches); value/e2e steps replay CUDA graphs" % Ks,
+                        "(eager launches); value/e2e steps %s" % (
+                            Ks, "run eagerly (the potential solve reads back its convergence "
+                            "checks)" if lorentz else "replay CUDA graphs"),
         "clocks": clocks.summary(),
     }
-    if world == 1 and not args.no_precision_forms:
+    if lz_info:
+        line["lorentz"] = lz_info
+    standard = "beads" not in w
+    if world == 1 and args.compare_steps:
+        line["storage_comparison"] = storage_comparison(w, device, args.compare_steps)
+    if world == 1 and standard and not args.no_precision_forms:
         line["precision_forms"] = storage_forms(w, device, min(K, 1000), ms / K)
         line["precision_forms"]["storage"] = ("headline value: float32 populations; forms: "
                                               "16-bit offsets f_q - w_q, float32 arithmetic")
         line["material_tables"] = table_form(w, device, min(K, 1000), ms / K, stage_ms)
-    if world == 1 and not args.no_adjoint:
+    if world == 1 and standard and not args.no_adjoint:
         line["adjoint"] = adjoint_form(device)
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and standard and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -590,6 +799,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the config-4 adjoint timing and finite-difference check")
+    ap.add_argument("--compare-steps", type=int, default=0,
+                    help="run the workload this many steps from reset in its own population "
+                         "storage and in float32; report remelt depth, HAZ T_max, pool W/D")
     ap.add_argument("--spinup", type=int, default=None,
                     help="steps run before warm-up (default: the workload's spin-up)")
     args = ap.parse_args()

@@ -257,6 +257,30 @@ int waam_elec_jacobi_chunk(float* phi_a, float* phi_b, const float* sigma, const
                            int n_sweeps, float arc_k, float sigma_cells, float* diff_buf,
                            float* norm_buf, void* workspace, size_t workspace_bytes,
                            void* stream);
+/* The potential solve over its live cells (those the sweep does not hold at
+ * 0: neither GAS nor SOLID at k <= nz_solid).  waam_elec_prepare writes sigma
+ * (elec_build_sigma) and the fixed-cell mask, zeroes phi_b at cells that
+ * became fixed since the mask was last built (an all-zero mask: every fixed
+ * cell), lists those cells (zero_list) and the live cells (live_list, in a
+ * fixed order; counts[0] = live, counts[1] = newly fixed; counts has
+ * waam_elec_counts_len entries).  waam_elec_jacobi_live runs n_sweeps sweeps
+ * phi_a -> phi_b -> ... over the live list, the last with the L1 check; with
+ * first_chunk set (the first call of a solve, phi_a its input) it also zeroes
+ * the newly fixed cells of phi_a after the first sweep.  Exact against the
+ * full-grid sweeps as long as both buffers are only written by these calls
+ * (and elec_init_ground) between mask builds: the fixed cells of both then
+ * hold 0, which is what every sweep writes there. */
+int64_t waam_elec_counts_len(int nx, int ny, int nz);
+int waam_elec_prepare(float* sigma, uint8_t* fixed, float* phi_b, const float* f_l,
+                      const int32_t* flags, int nx, int ny, int nz, float sigma_liquid,
+                      float sigma_solid, int nz_solid, int32_t* live_list, int32_t* zero_list,
+                      int32_t* counts, int64_t counts_len, void* stream);
+int waam_elec_jacobi_live(float* phi_a, float* phi_b, const float* sigma, const float* source,
+                          const int32_t* live_list, const int32_t* zero_list,
+                          const int32_t* counts, int nx, int ny, int nz, float dx,
+                          float omega_j, int n_sweeps, int first_chunk, float arc_k,
+                          float sigma_cells, float* diff_buf, float* norm_buf, void* workspace,
+                          size_t workspace_bytes, void* stream);
 /* kernels.py:1304-1312 elec_init_ground (phi = 0) */
 int waam_elec_init_ground(float* phi, int64_t n, void* stream);
 /* kernels.py:1315-1355 elec_jacobi_step; phi_in and phi_out must differ */
@@ -623,9 +647,12 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
  * liquid fraction and flags of this step and writes the J and B the
  * collision adds: stage 0 = VOF advection, thermal, phase, flags and the
  * active-cell list; stage 1 = forces, collision, stream, tracers, tail.
- * Stage 0 followed by stage 1 equals one waam_step_main. */
+ * Stage 0 followed by stage 1 equals one waam_step_main.  events: null, or
+ * the 7 handles of waam_step_main_events given to both calls (stage 0
+ * records 0..3, stage 1 records 4..6). */
 int waam_step_main_stage(const WaamFields* f, const WaamStepParams* p, int stage, void* workspace,
-                         size_t workspace_bytes, void* stream);
+                         size_t workspace_bytes, void* const* events, int n_events,
+                         void* stream);
 /* Number of kernels the fused stages launch (for launch accounting): stage 0
  * waam_step_pre, 1 waam_step_main, 2 waam_step_main_events; the J x B pass
  * over SOLID cells of a step with WaamFields.lorentz_J set adds one). */

@@ -141,3 +141,60 @@ def test_jacobi_chunk_matches_single_sweeps(n_sweeps):
     assert torch.equal(a, last)
     assert math.isclose(float(d1.item()), float(d2.item()), rel_tol=1e-6)
     assert math.isclose(float(n1.item()), float(n2.item()), rel_tol=1e-6)
+
+
+def test_live_list_solve_matches_full_grid_sweeps():
+    """Three solves of 20 sweeps (chunks of 10) with the flags changing between
+    them -- metal cells turning to gas and gas to metal -- on the live list and
+    on full-grid sweeps: the potential in both buffers is equal bit for bit and
+    the L1 sums of every chunk agree."""
+    K = _k()
+    dev = torch.device("cuda", 0)
+    nx, ny, nz, nzs = 40, 32, 28, 8
+    rng = np.random.default_rng(21)
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
+    n = nx * ny * nz
+    fixed = torch.zeros((nx, ny, nz), dtype=torch.uint8, device=dev)
+    fixed_full = torch.zeros_like(fixed)
+    live = torch.zeros(n, dtype=torch.int32, device=dev)
+    zero = torch.zeros(n, dtype=torch.int32, device=dev)
+    counts = torch.zeros(int(_native_counts_len(nx, ny, nz)), dtype=torch.int32, device=dev)
+    # garbage in the buffers before the first solve (cold start zeroes only a)
+    a_l, b_l = t(rng.uniform(0, 1, (nx, ny, nz)).astype(np.float32)), \
+        t(rng.uniform(0, 1, (nx, ny, nz)).astype(np.float32))
+    a_l.zero_()
+    a_f, b_f = a_l.clone(), b_l.clone()
+    sig_l, sig_f = torch.zeros_like(a_l), torch.zeros_like(a_l)
+    src = torch.zeros_like(a_l)
+    for solve in range(3):
+        flags = np.full((nx, ny, nz), 2, np.int32)
+        flags[:, :, :nzs] = 1
+        flags[:, :, nzs] = 4
+        x0 = 8 + 4 * solve
+        flags[x0:x0 + 12, 10:22, nzs:nzs + 4 + solve] = 0
+        flags[5:7, 5:7, nzs + 3] = 1
+        fl = np.where(flags == 0, 0.9, 0.0).astype(np.float32)
+        F, FL = t(flags), t(fl)
+        arc = (x0 + 6.0, 16.0, float(nzs + 2))
+        K.elec_arc_source(src, *arc, 3.0, 150.0, 2e-4)
+        K.elec_prepare(sig_l, fixed, b_l, FL, F, 1e6, 1e5, nzs, live, zero, counts)
+        K.elec_build_sigma_mask(sig_f, fixed_full, FL, F, 1e6, 1e5, nzs)
+        for chunk in range(2):
+            d1, n1 = torch.zeros((), device=dev), torch.zeros((), device=dev)
+            d2, n2 = torch.zeros((), device=dev), torch.zeros((), device=dev)
+            K.elec_jacobi_live(a_l, b_l, sig_l, src, live, zero, counts, 2e-4, 0.85, 10,
+                               chunk == 0, arc[2], 3.0, d1, n1)
+            K.elec_jacobi_chunk(a_f, b_f, sig_f, src, fixed_full, 2e-4, 0.85, 10, arc[2], 3.0,
+                                d2, n2)
+            torch.cuda.synchronize()
+            assert math.isclose(float(d1.item()), float(d2.item()), rel_tol=1e-6)
+            assert math.isclose(float(n1.item()), float(n2.item()), rel_tol=1e-6)
+        assert torch.equal(sig_l, sig_f)
+        assert torch.equal(fixed, fixed_full)
+        assert torch.equal(a_l, a_f), solve
+        assert torch.equal(b_l, b_f), solve
+
+
+def _native_counts_len(nx, ny, nz):
+    from waam_solver_b200 import _native
+    return _native.lib().waam_elec_counts_len(nx, ny, nz)

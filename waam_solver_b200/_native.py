@@ -123,7 +123,8 @@ def parse_header(path: str = HEADER):
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     src = re.sub(r"typedef struct \w+ \{.*?\} \w+;", "", src, flags=re.S)
     decls = {}
-    for m in re.finditer(r"(const char\*|int|size_t)\s+(waam_\w+)\s*\(([^)]*)\)\s*;", src):
+    for m in re.finditer(r"(const char\*|int64_t|int|size_t)\s+(waam_\w+)\s*\(([^)]*)\)\s*;",
+                         src):
         ret, name, args = m.group(1), m.group(2), m.group(3)
         types = []
         args = args.strip()

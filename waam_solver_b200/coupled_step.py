@@ -490,8 +490,6 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     events = getattr(twin, "_stage_events", None)
     due = _droplet_due(twin, g, is_welding)
     lorentz = bool(is_welding and twin.enable_lorentz)
-    if lorentz and events is not None:
-        raise WaamError("stage events are not recorded on steps with the Lorentz force")
     done = False
     if not due and not lorentz and events is None and getattr(twin, "use_cuda_graphs", True):
         key = (g._read_buf is g.f_a, g._cur, p.welding, p.clear_forces,
@@ -509,12 +507,23 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
             p.forces_from_buffer = 1
             p.clear_forces = 0
         if lorentz:
+            # stage events (if any) go to both halves; _lorentz_events, if set,
+            # bracket the potential solve between them
+            handles, n_ev = None, 0
+            if events is not None:
+                handles = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
+                n_ev = len(events)
             _native.call("waam_step_main_stage", ctypes.byref(f), ctypes.byref(p), 0,
-                         ws.data_ptr(), ws.numel(), stream)
+                         ws.data_ptr(), ws.numel(), handles, n_ev, stream)
+            lz_events = getattr(twin, "_lorentz_events", None)
+            if lz_events is not None:
+                lz_events[0].record()
             arc_k = float(g.step_scalars[0].item())
             weld_forces.solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=False)
+            if lz_events is not None:
+                lz_events[1].record()
             _native.call("waam_step_main_stage", ctypes.byref(_fields_cached(g, lorentz=True)),
-                         ctypes.byref(p), 1, ws.data_ptr(), ws.numel(), stream)
+                         ctypes.byref(p), 1, ws.data_ptr(), ws.numel(), handles, n_ev, stream)
         elif events is None:
             _native.call("waam_step_main", ctypes.byref(f), ctypes.byref(p), ws.data_ptr(),
                          ws.numel(), stream)

@@ -1193,9 +1193,11 @@ int waam_step_main_events(const WaamFields* f, const WaamStepParams* p, void* wo
 }
 
 int waam_step_main_stage(const WaamFields* f, const WaamStepParams* p, int stage, void* workspace,
-                         size_t workspace_bytes, void* stream) {
+                         size_t workspace_bytes, void* const* events, int n_events,
+                         void* stream) {
     if (stage != 0 && stage != 1) return fail(WAAM_ERR_INVALID, "step_main_stage: stage 0 or 1");
-    return step_main_impl(f, p, workspace, workspace_bytes, nullptr, 0, stream, 1 << stage);
+    return step_main_impl(f, p, workspace, workspace_bytes, events, n_events, stream,
+                          1 << stage);
 }
 
 }  // extern "C"

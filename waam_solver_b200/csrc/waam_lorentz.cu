@@ -300,6 +300,155 @@ __global__ void __launch_bounds__(kTileK* kTileJ)
     }
 }
 
+// One cell of the masked sweep from its neighbour values, in the reference's
+// expression order (kernels.py:1315-1355).
+__device__ __forceinline__ float jacobi_cell(float pin, float sp, float sm, float sn, float ss,
+                                            float st, float sb, float pp, float pm, float pn_,
+                                            float ps, float pt, float pb, float sc, float dx,
+                                            float omega_j) {
+    const float eps = 1e-12f;
+    const float denom = sp + sm + sn + ss + st + sb + eps;
+    const float nb = sp * pp + sm * pm + sn * pn_ + ss * ps + st * pt + sb * pb;
+    const float pn = (nb + sc * dx * dx) / denom;
+    return (1.0f - omega_j) * pin + omega_j * pn;
+}
+
+// ---- the potential solve over its live cells ---------------------------------
+// Only the cells the sweep does not hold at 0 (metal above the grounded
+// plate) change: the sweeps walk a list of them.  The fixed cells stay exact
+// because both potential buffers hold 0 at every fixed cell: k_elec_prepare
+// zeroes the output buffer of the first sweep at cells that became fixed
+// since the previous solve (old mask 0, new mask 1), the zero list zeroes the
+// other buffer after that sweep, and every later sweep writes 0 there in the
+// reference anyway.  Fixed cells then add exactly 0 to the L1 sums of every
+// sweep after the first.  counts: [0] live cells, [1] newly fixed cells,
+// [2 + b] live cells of tile block b, then (after the scan) its list offset.
+constexpr int kCntLive = 0, kCntZero = 1, kCntBlocks = 2;
+constexpr int kLiveBlocks = 148 * 8;
+
+__device__ __forceinline__ int tile_block_linear() {
+    return (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+}
+
+__global__ void __launch_bounds__(kTileK* kTileJ)
+    k_elec_prepare(Dims d, float* __restrict__ sigma, uint8_t* __restrict__ fixed,
+                   float* __restrict__ phi_b, const float* __restrict__ f_l,
+                   const int32_t* __restrict__ flags, float s_liq, float s_sol, int nz_solid,
+                   int* __restrict__ zero_list, int* __restrict__ counts) {
+    int i, j, k, c;
+    const bool ok = tile_cell(d, i, j, k, c);
+    bool live = false, newly = false;
+    if (ok) {
+        const int fl = flags[c];
+        sigma[c] = fl == GAS ? 1e-8f : (f_l[c] > 0.55f ? s_liq : s_sol);
+        const uint8_t nf = (fl == GAS || (k <= nz_solid && fl == SOLID)) ? 1 : 0;
+        const uint8_t of = fixed[c];
+        if (nf != of) fixed[c] = nf;
+        newly = nf && !of;
+        if (newly) phi_b[c] = 0.0f;
+        live = !nf;
+    }
+    // newly fixed cells: one atomic per warp
+    const unsigned m = __ballot_sync(0xffffffffu, newly);
+    const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+    int base = 0;
+    if (m && lane == 0) base = atomicAdd(&counts[kCntZero], __popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (newly) zero_list[base + __popc(m & ((1u << lane) - 1u))] = c;
+    const int nlive = __syncthreads_count(live);
+    if (threadIdx.x == 0 && threadIdx.y == 0) counts[kCntBlocks + tile_block_linear()] = nlive;
+}
+
+// Exclusive scan of the per-block live counts (one block of 1024 threads).
+__global__ void __launch_bounds__(1024) k_elec_scan(int* counts, int nb) {
+    __shared__ int part[1024];
+    const int t = threadIdx.x, T = blockDim.x;
+    const int per = (nb + T - 1) / T;
+    const int b0 = imin(nb, t * per), b1 = imin(nb, b0 + per);
+    int sum = 0;
+    for (int b = b0; b < b1; ++b) sum += counts[kCntBlocks + b];
+    part[t] = sum;
+    __syncthreads();
+    for (int off = 1; off < T; off <<= 1) {
+        const int v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int run = part[t] - sum;
+    for (int b = b0; b < b1; ++b) {
+        const int cb = counts[kCntBlocks + b];
+        counts[kCntBlocks + b] = run;
+        run += cb;
+    }
+    if (t == T - 1) counts[kCntLive] = part[T - 1];
+}
+
+// The live list in tile-block order (a fixed order).
+__global__ void __launch_bounds__(kTileK* kTileJ)
+    k_elec_list(Dims d, const uint8_t* __restrict__ fixed, const int* __restrict__ counts,
+                int* __restrict__ live_list) {
+    int i, j, k, c;
+    const bool ok = tile_cell(d, i, j, k, c);
+    const bool live = ok && !fixed[c];
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    const int lane = t & 31, w = t >> 5;
+    const unsigned m = __ballot_sync(0xffffffffu, live);
+    __shared__ int wc[kTileK * kTileJ / 32];
+    if (lane == 0) wc[w] = __popc(m);
+    __syncthreads();
+    int base = counts[kCntBlocks + tile_block_linear()];
+    for (int q = 0; q < w; ++q) base += wc[q];
+    if (live) live_list[base + __popc(m & ((1u << lane) - 1u))] = c;
+}
+
+// One sweep over the live list (a fixed grid: the L1 sums in a fixed order).
+template <bool L1>
+__global__ void __launch_bounds__(256)
+    k_elec_jacobi_live(Dims d, const float* __restrict__ phi_in, float* __restrict__ phi_out,
+                       const float* __restrict__ sigma, const float* __restrict__ src,
+                       const int* __restrict__ live_list, const int* __restrict__ counts,
+                       float dx, float omega_j, int k_src_lo, int k_src_hi, float* diff_out,
+                       float* norm_out, Workspace ws) {
+    const int cnt = counts[kCntLive];
+    const int sx = d.ny * d.nz, sy = d.nz;
+    double dsum = 0.0, nsum = 0.0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+        const int c = live_list[t];
+        const int k = c % d.nz;
+        const int r = c / d.nz;
+        const int j = r % d.ny, i = r / d.ny;
+        const int ip = c + (i + 1 < d.nx ? sx : 0), im = c - (i > 0 ? sx : 0);
+        const int jp = c + (j + 1 < d.ny ? sy : 0), jm = c - (j > 0 ? sy : 0);
+        const int kp = c + (k + 1 < d.nz ? 1 : 0), km = c - (k > 0 ? 1 : 0);
+        const float pin = phi_in[c];
+        const float sc = (k >= k_src_lo && k <= k_src_hi) ? src[c] : 0.0f;
+        const float out = jacobi_cell(pin, sigma[ip], sigma[im], sigma[jp], sigma[jm], sigma[kp],
+                                      sigma[km], phi_in[ip], phi_in[im], phi_in[jp], phi_in[jm],
+                                      phi_in[kp], phi_in[km], sc, dx, omega_j);
+        phi_out[c] = out;
+        if (L1) {
+            dsum += (double)fabsf(out - pin);
+            nsum += (double)fabsf(pin);
+        }
+    }
+    if (L1) {
+        double2 part = block_sum2(dsum, nsum);
+        double2 tot;
+        if (finish_sum2(ws, part, tot)) {
+            *diff_out = (float)tot.x;
+            *norm_out = (float)tot.y;
+        }
+    }
+}
+
+__global__ void k_elec_zero_list(const int* __restrict__ zero_list, const int* __restrict__ counts,
+                                 float* phi) {
+    const int cnt = counts[kCntZero];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x)
+        phi[zero_list[t]] = 0.0f;
+}
+
 // kernels.py:1237-1251 elec_build_sigma, plus the byte mask of the cells the
 // Jacobi sweep holds at 0 (kernels.py:1315-1355: GAS, SOLID at k <= nz_solid).
 __global__ void k_elec_sigma_mask(Dims d, float* sigma, uint8_t* fixed, const float* f_l,
@@ -673,6 +822,84 @@ int waam_elec_jacobi_chunk(float* phi_a, float* phi_b, const float* sigma, const
         }
         int rc = check_launch("k_elec_jacobi_m");
         if (rc) return rc;
+        float* t = in;
+        in = out;
+        out = t;
+    }
+    return WAAM_OK;
+}
+
+int64_t waam_elec_counts_len(int nx, int ny, int nz) {
+    if (!dims_ok(nx, ny, nz)) return 0;
+    const dim3 g = tile_grid(Dims{nx, ny, nz});
+    return (int64_t)kCntBlocks + (int64_t)g.x * g.y * g.z;
+}
+
+int waam_elec_prepare(float* sigma, uint8_t* fixed, float* phi_b, const float* f_l,
+                      const int32_t* flags, int nx, int ny, int nz, float sigma_liquid,
+                      float sigma_solid, int nz_solid, int32_t* live_list, int32_t* zero_list,
+                      int32_t* counts, int64_t counts_len, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_prepare: bad dims");
+    REQUIRE(sigma && fixed && phi_b && f_l && flags && live_list && zero_list && counts,
+            "elec_prepare: null field");
+    REQUIRE(counts_len >= waam_elec_counts_len(nx, ny, nz), "elec_prepare: counts too short");
+    Dims d{nx, ny, nz};
+    const dim3 g = tile_grid(d);
+    const int nb = (int)(g.x * g.y * g.z);
+    cudaError_t e = cudaMemsetAsync(counts, 0, kCntBlocks * sizeof(int32_t), STREAM(stream));
+    if (e != cudaSuccess) return fail(WAAM_ERR_CUDA, cudaGetErrorString(e));
+    k_elec_prepare<<<g, tile_block(), 0, STREAM(stream)>>>(d, sigma, fixed, phi_b, f_l, flags,
+                                                           sigma_liquid, sigma_solid, nz_solid,
+                                                           zero_list, counts);
+    int rc = check_launch("k_elec_prepare");
+    if (rc) return rc;
+    k_elec_scan<<<1, 1024, 0, STREAM(stream)>>>(counts, nb);
+    rc = check_launch("k_elec_scan");
+    if (rc) return rc;
+    k_elec_list<<<g, tile_block(), 0, STREAM(stream)>>>(d, fixed, counts, live_list);
+    return check_launch("k_elec_list");
+}
+
+int waam_elec_jacobi_live(float* phi_a, float* phi_b, const float* sigma, const float* source,
+                          const int32_t* live_list, const int32_t* zero_list,
+                          const int32_t* counts, int nx, int ny, int nz, float dx,
+                          float omega_j, int n_sweeps, int first_chunk, float arc_k,
+                          float sigma_cells, float* diff_buf, float* norm_buf, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "elec_jacobi_live: bad dims");
+    REQUIRE(phi_a && phi_b && sigma && source && live_list && zero_list && counts && diff_buf &&
+                norm_buf && phi_a != phi_b,
+            "elec_jacobi_live: null or aliased field");
+    REQUIRE(n_sweeps >= 1, "elec_jacobi_live: n_sweeps must be >= 1");
+    REQUIRE(!first_chunk || n_sweeps >= 2,
+            "elec_jacobi_live: the first chunk of a solve needs at least 2 sweeps");
+    REQUIRE(std::isfinite(arc_k) && std::isfinite(sigma_cells) && std::fabs(arc_k) < 1e6f &&
+                std::fabs(sigma_cells) < 1e6f,
+            "elec_jacobi_live: arc k / sigma not finite");
+    Dims d{nx, ny, nz};
+    REQUIRE(workspace_ok(workspace, workspace_bytes, d.n()),
+            "elec_jacobi_live: workspace too small or misaligned");
+    int k_lo, k_hi;
+    source_slab(arc_k, sigma_cells, nz, k_lo, k_hi);
+    float* in = phi_a;
+    float* out = phi_b;
+    for (int s = 0; s < n_sweeps; ++s) {
+        if (s + 1 < n_sweeps)
+            k_elec_jacobi_live<false><<<kLiveBlocks, 256, 0, STREAM(stream)>>>(
+                d, in, out, sigma, source, live_list, counts, dx, omega_j, k_lo, k_hi, nullptr,
+                nullptr, Workspace{});
+        else
+            k_elec_jacobi_live<true><<<kLiveBlocks, 256, 0, STREAM(stream)>>>(
+                d, in, out, sigma, source, live_list, counts, dx, omega_j, k_lo, k_hi, diff_buf,
+                norm_buf, Workspace::at(workspace));
+        int rc = check_launch("k_elec_jacobi_live");
+        if (rc) return rc;
+        if (first_chunk && s == 0) {
+            // the input of the first sweep: its newly fixed cells become 0
+            k_elec_zero_list<<<kLiveBlocks, 256, 0, STREAM(stream)>>>(zero_list, counts, in);
+            rc = check_launch("k_elec_zero_list");
+            if (rc) return rc;
+        }
         float* t = in;
         in = out;
         out = t;

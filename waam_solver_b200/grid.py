@@ -155,8 +155,15 @@ class WAAMGrid:
         self.phi_elec, self.phi_elec_tmp, self.sigma_elec, self.elec_source = mk(), mk(), mk(), mk()
         self.Jx, self.Jy, self.Jz = mk(), mk(), mk()
         self.Bx, self.By, self.Bz = mk(), mk(), mk()
-        # cells the potential solve holds at 0 (GAS, grounded SOLID), one byte each
+        # cells the potential solve holds at 0 (GAS, grounded SOLID), one byte
+        # each, and the lists of its live and newly fixed cells
         self.elec_fixed = torch.zeros(self._shape3, dtype=torch.uint8, device=self.device)
+        n = self.nx * self.ny * self.nz
+        self.elec_live = torch.zeros(n, dtype=torch.int32, device=self.device)
+        self.elec_zero = torch.zeros(n, dtype=torch.int32, device=self.device)
+        from . import _native
+        m = int(_native.lib().waam_elec_counts_len(self.nx, self.ny, self.nz))
+        self.elec_counts = torch.zeros(m, dtype=torch.int32, device=self.device)
         self.n_elec_bins = 64
         self.elec_rad_bins = torch.zeros((self.nz, self.n_elec_bins), dtype=torch.float32,
                                          device=self.device)
@@ -266,6 +273,10 @@ class WAAMGrid:
     def load_state(self, st):
         """Inverse of state_dict (numpy arrays or tensors)."""
         self._forces_dirty = True
+        if self._has_lorentz:
+            # the potential buffers may now hold anything at fixed cells: the
+            # next solve treats every fixed cell as newly fixed
+            self.elec_fixed.zero_()
         for k, v in st.items():
             if k == "read_is_a":
                 self._read_buf, self._write_buf = (self.f_a, self.f_b) if v else (self.f_b, self.f_a)

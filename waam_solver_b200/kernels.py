@@ -692,6 +692,34 @@ def elec_jacobi_chunk(phi_a, phi_b, sigma, source, fixed, dx, omega_j, n_sweeps,
           float(sigma_cells), _f(diff_buf, 1), _f(norm_buf, 1), ws, wsb, _stream())
 
 
+def elec_prepare(sigma, fixed, phi_b, f_l, flags, sigma_liquid, sigma_solid, nz_solid, live,
+                 zero, counts):
+    """Conductivity map, fixed-cell mask and the live / newly fixed cell lists of
+    one potential solve (zeroes phi_b at the newly fixed cells)."""
+    nx, ny, nz = _dims(sigma)
+    n = nx * ny * nz
+    for t, name in ((live, "live"), (zero, "zero"), (counts, "counts")):
+        if t.dtype != torch.int32 or not t.is_contiguous():
+            raise WaamError("elec_prepare: %s must be contiguous int32" % name)
+    if live.numel() < n or zero.numel() < n:
+        raise WaamError("elec_prepare: live / zero lists need nx*ny*nz entries")
+    _call("waam_elec_prepare", _f(sigma, n), fixed.data_ptr(), _f(phi_b, n), _f(f_l, n),
+          _i(flags, n), nx, ny, nz, float(sigma_liquid), float(sigma_solid), int(nz_solid),
+          live.data_ptr(), zero.data_ptr(), counts.data_ptr(), counts.numel(), _stream())
+
+
+def elec_jacobi_live(phi_a, phi_b, sigma, source, live, zero, counts, dx, omega_j, n_sweeps,
+                     first_chunk, arc_k, sigma_cells, diff_buf, norm_buf):
+    """n_sweeps sweeps over the live cells (see waam_elec_jacobi_live)."""
+    nx, ny, nz = _dims(phi_a)
+    n = nx * ny * nz
+    ws, wsb = workspace_for(phi_a)
+    _call("waam_elec_jacobi_live", _f(phi_a, n), _f(phi_b, n), _f(sigma, n), _f(source, n),
+          live.data_ptr(), zero.data_ptr(), counts.data_ptr(), nx, ny, nz, float(dx),
+          float(omega_j), int(n_sweeps), 1 if first_chunk else 0, float(arc_k),
+          float(sigma_cells), _f(diff_buf, 1), _f(norm_buf, 1), ws, wsb, _stream())
+
+
 def elec_clear_source(source):
     source.zero_()
 

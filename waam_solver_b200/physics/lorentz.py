@@ -11,9 +11,10 @@ Differences of form, not of result: the potential ping-pongs between
 (after the solve ``phi_elec`` holds the last iterate, ``phi_elec_tmp`` the one
 before it); each chunk of ten sweeps is one native call whose last sweep also
 computes the L1 change -- the only sweep whose L1 the reference reads; the
-sweeps read the fixed cells from a byte mask built with the conductivity map
-and the source only inside its k slab (it is 0 elsewhere); and clearing,
-injecting and normalising the source is one call.
+sweeps visit only the live cells -- those not held at 0 (GAS, grounded
+SOLID), listed when the conductivity map is built -- while both buffers keep
+exact zeros at the fixed cells; and clearing, injecting and normalising the
+source is one call.
 """
 from __future__ import annotations
 
@@ -38,8 +39,10 @@ def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True):
     if not twin.enable_lorentz:
         return
     g.ensure_lorentz_fields()
-    kernels.elec_build_sigma_mask(g.sigma_elec, g.elec_fixed, g.f_l, g.flags,
-                                  twin.sigma_liquid_Sm, twin.sigma_solid_Sm, twin.nz_solid)
+    # phi_elec is the first sweep's input, phi_elec_tmp its output
+    kernels.elec_prepare(g.sigma_elec, g.elec_fixed, g.phi_elec_tmp, g.f_l, g.flags,
+                         twin.sigma_liquid_Sm, twin.sigma_solid_Sm, twin.nz_solid, g.elec_live,
+                         g.elec_zero, g.elec_counts)
     kernels.elec_arc_source(g.elec_source, arc_i, arc_j, arc_k, twin.sigma_cells,
                             twin.welding_current_A, g.dx)
 
@@ -55,9 +58,10 @@ def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True):
     rel = float("inf")
     while iters_done < max_iters:
         chunk = min(check_every, max_iters - iters_done)
-        kernels.elec_jacobi_chunk(g.phi_elec, g.phi_elec_tmp, g.sigma_elec, g.elec_source,
-                                  g.elec_fixed, g.dx, twin.lorentz_jacobi_omega, chunk, arc_k,
-                                  twin.sigma_cells, g.elec_res_buf, g.elec_norm_buf)
+        kernels.elec_jacobi_live(g.phi_elec, g.phi_elec_tmp, g.sigma_elec, g.elec_source,
+                                 g.elec_live, g.elec_zero, g.elec_counts, g.dx,
+                                 twin.lorentz_jacobi_omega, chunk, iters_done == 0, arc_k,
+                                 twin.sigma_cells, g.elec_res_buf, g.elec_norm_buf)
         if chunk % 2 == 1:
             g.phi_elec, g.phi_elec_tmp = g.phi_elec_tmp, g.phi_elec
         iters_done += chunk
