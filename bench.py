@@ -508,10 +508,9 @@ def jacobi_timing(tw, reps=10):
     g = tw.grid
     a, b = g.phi_elec.clone(), g.phi_elec_tmp.clone()
     res, nrm = torch.zeros((), device=a.device), torch.zeros((), device=a.device)
-    arc_k = float(g.step_scalars[0].item())
     call = lambda: kernels.elec_jacobi_live(  # noqa: E731
         a, b, g.sigma_elec, g.elec_source, g.elec_live, g.elec_zero, g.elec_counts, g.dx,
-        tw.lorentz_jacobi_omega, 10, False, arc_k, tw.sigma_cells, res, nrm)
+        tw.lorentz_jacobi_omega, 10, False, g.step_scalars[0:1], tw.sigma_cells, res, nrm)
     call()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()

@@ -238,6 +238,10 @@ int waam_elec_inject_arc_source(float* source, int nx, int ny, int nz, float arc
 int waam_elec_arc_source(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
                          float arc_k, float sigma_cells, float current_A, float dx,
                          void* workspace, size_t workspace_bytes, void* stream);
+/* waam_elec_arc_source with the arc height read from device memory */
+int waam_elec_arc_source_dev(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
+                             const float* arc_k_dev, float sigma_cells, float current_A,
+                             float dx, void* workspace, size_t workspace_bytes, void* stream);
 /* kernels.py:1288-1301 elec_normalize_source; the sum is taken in double */
 int waam_elec_normalize_source(float* source, int64_t n, float target_current_A, float dx,
                                void* workspace, size_t workspace_bytes, void* stream);
@@ -269,7 +273,9 @@ int waam_elec_jacobi_chunk(float* phi_a, float* phi_b, const float* sigma, const
  * the newly fixed cells of phi_a after the first sweep.  Exact against the
  * full-grid sweeps as long as both buffers are only written by these calls
  * (and elec_init_ground) between mask builds: the fixed cells of both then
- * hold 0, which is what every sweep writes there. */
+ * hold 0, which is what every sweep writes there.  The source's k slab
+ * comes from the arc height at arc_k_dev (device memory, e.g. the fused
+ * step's scalar 0), so the solve needs no host copy of it. */
 int64_t waam_elec_counts_len(int nx, int ny, int nz);
 int waam_elec_prepare(float* sigma, uint8_t* fixed, float* phi_b, const float* f_l,
                       const int32_t* flags, int nx, int ny, int nz, float sigma_liquid,
@@ -278,7 +284,7 @@ int waam_elec_prepare(float* sigma, uint8_t* fixed, float* phi_b, const float* f
 int waam_elec_jacobi_live(float* phi_a, float* phi_b, const float* sigma, const float* source,
                           const int32_t* live_list, const int32_t* zero_list,
                           const int32_t* counts, int nx, int ny, int nz, float dx,
-                          float omega_j, int n_sweeps, int first_chunk, float arc_k,
+                          float omega_j, int n_sweeps, int first_chunk, const float* arc_k_dev,
                           float sigma_cells, float* diff_buf, float* norm_buf, void* workspace,
                           size_t workspace_bytes, void* stream);
 /* kernels.py:1304-1312 elec_init_ground (phi = 0) */
@@ -311,6 +317,13 @@ int waam_elec_prefix_bins(float* bins, int n_bins, int nz, void* stream);
 int waam_elec_B_axisymmetric(float* Bx, float* By, float* Bz, const float* bins, int nx, int ny,
                              int nz, float arc_i, float arc_j, float dx, float bin_dr_cells,
                              float mu0, int n_bins, void* stream);
+/* After the potential solve (physics/weld_forces.py:261-276): elec_compute_J,
+ * elec_bin_axial_current, elec_prefix_bins, elec_B_axisymmetric in one call */
+int waam_elec_fields(float* Jx, float* Jy, float* Jz, float* Bx, float* By, float* Bz,
+                     float* bins, const float* phi, const float* sigma, const int32_t* flags,
+                     int nx, int ny, int nz, float arc_i, float arc_j, float dx,
+                     float bin_dr_cells, float mu0, int n_bins, void* workspace,
+                     size_t workspace_bytes, void* stream);
 /* kernels.py:1479-1513 apply_lorentz_JxB */
 int waam_apply_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* Jx, const float* Jy,
                            const float* Jz, const float* Bx, const float* By, const float* Bz,

@@ -143,14 +143,16 @@ def test_jacobi_chunk_matches_single_sweeps(n_sweeps):
     assert math.isclose(float(n1.item()), float(n2.item()), rel_tol=1e-6)
 
 
-def test_live_list_solve_matches_full_grid_sweeps():
+@pytest.mark.parametrize("shape", [(40, 32, 28, 8), (70, 80, 40, 10)])
+def test_live_list_solve_matches_full_grid_sweeps(shape):
     """Three solves of 20 sweeps (chunks of 10) with the flags changing between
     them -- metal cells turning to gas and gas to metal -- on the live list and
     on full-grid sweeps: the potential in both buffers is equal bit for bit and
-    the L1 sums of every chunk agree."""
+    the L1 sums of every chunk agree.  The second grid has more than 1024 tile
+    blocks (two levels of the list's offset scan)."""
     K = _k()
     dev = torch.device("cuda", 0)
-    nx, ny, nz, nzs = 40, 32, 28, 8
+    nx, ny, nz, nzs = shape
     rng = np.random.default_rng(21)
     t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
     n = nx * ny * nz
@@ -183,7 +185,7 @@ def test_live_list_solve_matches_full_grid_sweeps():
             d1, n1 = torch.zeros((), device=dev), torch.zeros((), device=dev)
             d2, n2 = torch.zeros((), device=dev), torch.zeros((), device=dev)
             K.elec_jacobi_live(a_l, b_l, sig_l, src, live, zero, counts, 2e-4, 0.85, 10,
-                               chunk == 0, arc[2], 3.0, d1, n1)
+                               chunk == 0, torch.tensor([arc[2]], device=dev), 3.0, d1, n1)
             K.elec_jacobi_chunk(a_f, b_f, sig_f, src, fixed_full, 2e-4, 0.85, 10, arc[2], 3.0,
                                 d2, n2)
             torch.cuda.synchronize()

@@ -518,8 +518,8 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
             lz_events = getattr(twin, "_lorentz_events", None)
             if lz_events is not None:
                 lz_events[0].record()
-            arc_k = float(g.step_scalars[0].item())
-            weld_forces.solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=False)
+            weld_forces.solve_lorentz(twin, g, arc_i, arc_j, None, apply_force=False,
+                                      arc_k_dev=g.step_scalars[0:1])
             if lz_events is not None:
                 lz_events[1].record()
             _native.call("waam_step_main_stage", ctypes.byref(_fields_cached(g, lorentz=True)),

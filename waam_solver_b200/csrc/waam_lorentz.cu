@@ -29,6 +29,14 @@ constexpr int kRedGridMax = kWsMaxPartials / 2;   // two sums share the partials
 constexpr int kMaxBins = 1024;
 constexpr int kOpScalarSourceScale = 16;          // ws.scalars slot of the source scale
 
+// k slab of the arc current source (kernels.py:1261-1284): cells outside
+// [k_min, k_max] get 0.  The same float arithmetic on host and device.
+__host__ __device__ __forceinline__ void source_slab(float arc_k, float sigma_cells, int nz,
+                                                     int& k_min, int& k_max) {
+    k_max = imin(nz, (int)(arc_k + sigma_cells * 4.0f) + 1);
+    k_min = imax(0, (int)(arc_k - sigma_cells));
+}
+
 // Reduction tiles: the 32 x 8 (k, j) tiles with loops over the tiles and i,
 // so the grid stays at <= kRedGridMax blocks (one partial per block).
 inline dim3 red_tile_grid(const Dims& d) {
@@ -155,9 +163,12 @@ __global__ void k_elec_source_sum(const float* src, int64_t n, float cell_vol, f
 // double, fixed order; pass 2 writes value * scale everywhere, the float the
 // reference's in-place scaling leaves.
 __global__ void __launch_bounds__(kTileK* kTileJ)
-    k_elec_source_fused_sum(Dims d, float arc_i, float arc_j, float arc_k, float inv2s2,
-                            float current, float vol_eps, int k_min, int k_max, float cell_vol,
-                            float target, Workspace ws) {
+    k_elec_source_fused_sum(Dims d, float arc_i, float arc_j, float arc_k, const float* arc_k_dev,
+                            float sigma_cells, float inv2s2, float current, float vol_eps,
+                            float cell_vol, float target, Workspace ws) {
+    if (arc_k_dev) arc_k = *arc_k_dev;
+    int k_min, k_max;
+    source_slab(arc_k, sigma_cells, d.nz, k_min, k_max);
     double part = 0.0;
     const int ks = imax(k_min, 0), ke = imin(k_max, d.nz - 1);
     for (int i = blockIdx.z; i < d.nx; i += gridDim.z)
@@ -177,10 +188,14 @@ __global__ void __launch_bounds__(kTileK* kTileJ)
 }
 
 __global__ void k_elec_source_fused_write(Dims d, float* src, float arc_i, float arc_j,
-                                          float arc_k, float inv2s2, float current,
-                                          float vol_eps, int k_min, int k_max, Workspace ws) {
+                                          float arc_k, const float* arc_k_dev, float sigma_cells,
+                                          float inv2s2, float current, float vol_eps,
+                                          Workspace ws) {
     int i, j, k, c;
     if (!tile_cell(d, i, j, k, c)) return;
+    if (arc_k_dev) arc_k = *arc_k_dev;
+    int k_min, k_max;
+    source_slab(arc_k, sigma_cells, d.nz, k_min, k_max);
     const float s = ws.scalars[kOpScalarSourceScale];
     const float v = elec_source_value(i, j, k, arc_i, arc_j, arc_k, inv2s2, current, vol_eps,
                                       k_min, k_max);
@@ -322,9 +337,19 @@ __device__ __forceinline__ float jacobi_cell(float pin, float sp, float sm, floa
 // other buffer after that sweep, and every later sweep writes 0 there in the
 // reference anyway.  Fixed cells then add exactly 0 to the L1 sums of every
 // sweep after the first.  counts: [0] live cells, [1] newly fixed cells,
-// [2 + b] live cells of tile block b, then (after the scan) its list offset.
+// [2 + b] live cells of tile block b, then (after the scan) its list offset;
+// after those the per-block live bitmaps (one word per warp) and the totals
+// of the scan's 1024-block groups.
 constexpr int kCntLive = 0, kCntZero = 1, kCntBlocks = 2;
 constexpr int kLiveBlocks = 148 * 8;
+constexpr int kWarpsPerTile = kTileK * kTileJ / 32;
+constexpr int kScanGroup = 1024;
+
+inline int64_t counts_bitmap_offset(int64_t nb) { return kCntBlocks + nb; }
+inline int64_t counts_group_offset(int64_t nb) { return kCntBlocks + nb + nb * kWarpsPerTile; }
+inline int64_t counts_total_len(int64_t nb) {
+    return counts_group_offset(nb) + (nb + kScanGroup - 1) / kScanGroup;
+}
 
 __device__ __forceinline__ int tile_block_linear() {
     return (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
@@ -334,7 +359,8 @@ __global__ void __launch_bounds__(kTileK* kTileJ)
     k_elec_prepare(Dims d, float* __restrict__ sigma, uint8_t* __restrict__ fixed,
                    float* __restrict__ phi_b, const float* __restrict__ f_l,
                    const int32_t* __restrict__ flags, float s_liq, float s_sol, int nz_solid,
-                   int* __restrict__ zero_list, int* __restrict__ counts) {
+                   int* __restrict__ zero_list, int* __restrict__ counts,
+                   unsigned* __restrict__ bitmaps) {
     int i, j, k, c;
     const bool ok = tile_cell(d, i, j, k, c);
     bool live = false, newly = false;
@@ -355,51 +381,93 @@ __global__ void __launch_bounds__(kTileK* kTileJ)
     if (m && lane == 0) base = atomicAdd(&counts[kCntZero], __popc(m));
     base = __shfl_sync(0xffffffffu, base, 0);
     if (newly) zero_list[base + __popc(m & ((1u << lane) - 1u))] = c;
+    const unsigned lm = __ballot_sync(0xffffffffu, live);
+    const int b = tile_block_linear();
+    if (lane == 0) bitmaps[(int64_t)b * kWarpsPerTile + ((threadIdx.y * blockDim.x) >> 5)] = lm;
     const int nlive = __syncthreads_count(live);
-    if (threadIdx.x == 0 && threadIdx.y == 0) counts[kCntBlocks + tile_block_linear()] = nlive;
+    if (threadIdx.x == 0 && threadIdx.y == 0) counts[kCntBlocks + b] = nlive;
 }
 
-// Exclusive scan of the per-block live counts (one block of 1024 threads).
-__global__ void __launch_bounds__(1024) k_elec_scan(int* counts, int nb) {
-    __shared__ int part[1024];
-    const int t = threadIdx.x, T = blockDim.x;
-    const int per = (nb + T - 1) / T;
-    const int b0 = imin(nb, t * per), b1 = imin(nb, b0 + per);
-    int sum = 0;
-    for (int b = b0; b < b1; ++b) sum += counts[kCntBlocks + b];
-    part[t] = sum;
+// Exclusive scan of the per-block live counts in two levels: each block of
+// 1024 threads scans a group of 1024 counts (coalesced) and leaves the group
+// total; k_elec_scan_groups scans the totals; k_elec_list adds both.
+__device__ __forceinline__ int block_exclusive_scan_1024(int v, int& total) {
+    __shared__ int warp_sums[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_sums[w] = incl;
     __syncthreads();
-    for (int off = 1; off < T; off <<= 1) {
-        const int v = t >= off ? part[t - off] : 0;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
+    if (w == 0) {
+        int ws_ = warp_sums[lane], wincl = ws_;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, wincl, o);
+            if (lane >= o) wincl += y;
+        }
+        warp_sums[lane] = wincl - ws_;
+        if (lane == 31) total = wincl;
     }
-    int run = part[t] - sum;
-    for (int b = b0; b < b1; ++b) {
-        const int cb = counts[kCntBlocks + b];
-        counts[kCntBlocks + b] = run;
-        run += cb;
-    }
-    if (t == T - 1) counts[kCntLive] = part[T - 1];
+    __syncthreads();
+    const int out = warp_sums[w] + incl - v;
+    return out;
 }
 
-// The live list in tile-block order (a fixed order).
-__global__ void __launch_bounds__(kTileK* kTileJ)
-    k_elec_list(Dims d, const uint8_t* __restrict__ fixed, const int* __restrict__ counts,
+__global__ void __launch_bounds__(kScanGroup) k_elec_scan(int* counts, int nb, int* groups) {
+    const int b = blockIdx.x * kScanGroup + threadIdx.x;
+    const int v = b < nb ? counts[kCntBlocks + b] : 0;
+    int t = 0;
+    const int ex = block_exclusive_scan_1024(v, t);
+    if (b < nb) counts[kCntBlocks + b] = ex;
+    if (threadIdx.x == 31) groups[blockIdx.x] = t;   // thread 31 holds the group total
+}
+
+// Exclusive scan of the group totals (one block), total live count to counts[0].
+__global__ void __launch_bounds__(kScanGroup) k_elec_scan_groups(int* counts, int* groups,
+                                                                 int n_groups) {
+    int running = 0;
+    for (int g0 = 0; g0 < n_groups; g0 += kScanGroup) {
+        const int g = g0 + threadIdx.x;
+        const int v = g < n_groups ? groups[g] : 0;
+        __shared__ int tot;
+        int t = 0;
+        const int ex = block_exclusive_scan_1024(v, t);
+        if (threadIdx.x == 31) tot = t;
+        __syncthreads();
+        if (g < n_groups) groups[g] = running + ex;
+        running += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) counts[kCntLive] = running;
+}
+
+// The live list in tile-block order (a fixed order), from the blocks' bitmaps:
+// one warp per tile block (grid-stride), which leaves at once when the block
+// has no live cells.
+__global__ void __launch_bounds__(256)
+    k_elec_list(Dims d, const int* __restrict__ counts, const unsigned* __restrict__ bitmaps,
+                const int* __restrict__ groups, int nb, int gx, int gy,
                 int* __restrict__ live_list) {
-    int i, j, k, c;
-    const bool ok = tile_cell(d, i, j, k, c);
-    const bool live = ok && !fixed[c];
-    const int t = threadIdx.y * blockDim.x + threadIdx.x;
-    const int lane = t & 31, w = t >> 5;
-    const unsigned m = __ballot_sync(0xffffffffu, live);
-    __shared__ int wc[kTileK * kTileJ / 32];
-    if (lane == 0) wc[w] = __popc(m);
-    __syncthreads();
-    int base = counts[kCntBlocks + tile_block_linear()];
-    for (int q = 0; q < w; ++q) base += wc[q];
-    if (live) live_list[base + __popc(m & ((1u << lane) - 1u))] = c;
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += nwarps) {
+        const int off = counts[kCntBlocks + b] + groups[b / kScanGroup];
+        const int next = b + 1 < nb ? counts[kCntBlocks + b + 1] + groups[(b + 1) / kScanGroup]
+                                    : counts[kCntLive];
+        if (next == off) continue;
+        const int bx = b % gx, by = (b / gx) % gy, i = b / (gx * gy);
+        int base = off;
+        for (int w = 0; w < kWarpsPerTile; ++w) {
+            const unsigned m = bitmaps[(int64_t)b * kWarpsPerTile + w];
+            if ((m >> lane) & 1u) {
+                const int k = bx * kTileK + lane, j = by * kTileJ + w;
+                live_list[base + __popc(m & ((1u << lane) - 1u))] = (i * d.ny + j) * d.nz + k;
+            }
+            base += __popc(m);
+        }
+    }
 }
 
 // One sweep over the live list (a fixed grid: the L1 sums in a fixed order).
@@ -408,9 +476,11 @@ __global__ void __launch_bounds__(256)
     k_elec_jacobi_live(Dims d, const float* __restrict__ phi_in, float* __restrict__ phi_out,
                        const float* __restrict__ sigma, const float* __restrict__ src,
                        const int* __restrict__ live_list, const int* __restrict__ counts,
-                       float dx, float omega_j, int k_src_lo, int k_src_hi, float* diff_out,
-                       float* norm_out, Workspace ws) {
+                       float dx, float omega_j, const float* __restrict__ arc_k_dev,
+                       float sigma_cells, float* diff_out, float* norm_out, Workspace ws) {
     const int cnt = counts[kCntLive];
+    int k_src_lo, k_src_hi;
+    source_slab(*arc_k_dev, sigma_cells, d.nz, k_src_lo, k_src_hi);
     const int sx = d.ny * d.nz, sy = d.nz;
     double dsum = 0.0, nsum = 0.0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
@@ -658,12 +728,6 @@ __global__ void k_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* __re
 
 using namespace waam;
 
-// k slab of the arc current source (kernels.py:1261-1284): cells outside
-// [k_min, k_max] get 0.
-static void source_slab(float arc_k, float sigma_cells, int nz, int& k_min, int& k_max) {
-    k_max = imin(nz, (int)(arc_k + sigma_cells * 4.0f) + 1);
-    k_min = imax(0, (int)(arc_k - sigma_cells));
-}
 
 #define REQUIRE(cond, msg) \
     if (!(cond)) return waam::fail(WAAM_ERR_INVALID, msg)
@@ -697,9 +761,10 @@ int waam_elec_inject_arc_source(float* source, int nx, int ny, int nz, float arc
     return check_launch("k_elec_source");
 }
 
-int waam_elec_arc_source(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
-                         float arc_k, float sigma_cells, float current_A, float dx,
-                         void* workspace, size_t workspace_bytes, void* stream) {
+static int arc_source_impl(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
+                           float arc_k, const float* arc_k_dev, float sigma_cells,
+                           float current_A, float dx, void* workspace, size_t workspace_bytes,
+                           void* stream) {
     REQUIRE(dims_ok(nx, ny, nz), "elec_arc_source: bad dims");
     REQUIRE(source, "elec_arc_source: null field");
     REQUIRE(std::isfinite(arc_k) && std::isfinite(sigma_cells) && std::fabs(arc_k) < 1e6f &&
@@ -712,19 +777,33 @@ int waam_elec_arc_source(float* source, int nx, int ny, int nz, float arc_i, flo
     const float eps = 1e-6f;
     const float inv2s2 = 1.0f / (2.0f * sigma_cells * sigma_cells + eps);
     const float cell_vol = dx * dx * dx;
-    int k_min, k_max;
-    source_slab(arc_k, sigma_cells, nz, k_min, k_max);
     // a fixed grid: the sum order does not depend on the GPU
     dim3 grid(imin((nz + kTileK - 1) / kTileK, 4), imin((ny + kTileJ - 1) / kTileJ, 16),
               imin(nx, 64));
     k_elec_source_fused_sum<<<grid, tile_block(), 0, STREAM(stream)>>>(
-        d, arc_i, arc_j, arc_k, inv2s2, current_A, cell_vol + eps, k_min, k_max, cell_vol,
-        current_A, ws);
+        d, arc_i, arc_j, arc_k, arc_k_dev, sigma_cells, inv2s2, current_A, cell_vol + eps,
+        cell_vol, current_A, ws);
     int rc = check_launch("k_elec_source_fused_sum");
     if (rc) return rc;
     k_elec_source_fused_write<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
-        d, source, arc_i, arc_j, arc_k, inv2s2, current_A, cell_vol + eps, k_min, k_max, ws);
+        d, source, arc_i, arc_j, arc_k, arc_k_dev, sigma_cells, inv2s2, current_A,
+        cell_vol + eps, ws);
     return check_launch("k_elec_source_fused_write");
+}
+
+int waam_elec_arc_source(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
+                         float arc_k, float sigma_cells, float current_A, float dx,
+                         void* workspace, size_t workspace_bytes, void* stream) {
+    return arc_source_impl(source, nx, ny, nz, arc_i, arc_j, arc_k, nullptr, sigma_cells,
+                           current_A, dx, workspace, workspace_bytes, stream);
+}
+
+int waam_elec_arc_source_dev(float* source, int nx, int ny, int nz, float arc_i, float arc_j,
+                             const float* arc_k_dev, float sigma_cells, float current_A,
+                             float dx, void* workspace, size_t workspace_bytes, void* stream) {
+    REQUIRE(arc_k_dev, "elec_arc_source_dev: null arc k");
+    return arc_source_impl(source, nx, ny, nz, arc_i, arc_j, 0.0f, arc_k_dev, sigma_cells,
+                           current_A, dx, workspace, workspace_bytes, stream);
 }
 
 int waam_elec_normalize_source(float* source, int64_t n, float target_current_A, float dx,
@@ -832,7 +911,7 @@ int waam_elec_jacobi_chunk(float* phi_a, float* phi_b, const float* sigma, const
 int64_t waam_elec_counts_len(int nx, int ny, int nz) {
     if (!dims_ok(nx, ny, nz)) return 0;
     const dim3 g = tile_grid(Dims{nx, ny, nz});
-    return (int64_t)kCntBlocks + (int64_t)g.x * g.y * g.z;
+    return counts_total_len((int64_t)g.x * g.y * g.z);
 }
 
 int waam_elec_prepare(float* sigma, uint8_t* fixed, float* phi_b, const float* f_l,
@@ -848,22 +927,29 @@ int waam_elec_prepare(float* sigma, uint8_t* fixed, float* phi_b, const float* f
     const int nb = (int)(g.x * g.y * g.z);
     cudaError_t e = cudaMemsetAsync(counts, 0, kCntBlocks * sizeof(int32_t), STREAM(stream));
     if (e != cudaSuccess) return fail(WAAM_ERR_CUDA, cudaGetErrorString(e));
+    unsigned* bitmaps = reinterpret_cast<unsigned*>(counts + counts_bitmap_offset(nb));
+    int* groups = counts + counts_group_offset(nb);
+    const int n_groups = (nb + kScanGroup - 1) / kScanGroup;
     k_elec_prepare<<<g, tile_block(), 0, STREAM(stream)>>>(d, sigma, fixed, phi_b, f_l, flags,
                                                            sigma_liquid, sigma_solid, nz_solid,
-                                                           zero_list, counts);
+                                                           zero_list, counts, bitmaps);
     int rc = check_launch("k_elec_prepare");
     if (rc) return rc;
-    k_elec_scan<<<1, 1024, 0, STREAM(stream)>>>(counts, nb);
+    k_elec_scan<<<n_groups, kScanGroup, 0, STREAM(stream)>>>(counts, nb, groups);
     rc = check_launch("k_elec_scan");
     if (rc) return rc;
-    k_elec_list<<<g, tile_block(), 0, STREAM(stream)>>>(d, fixed, counts, live_list);
+    k_elec_scan_groups<<<1, kScanGroup, 0, STREAM(stream)>>>(counts, groups, n_groups);
+    rc = check_launch("k_elec_scan_groups");
+    if (rc) return rc;
+    k_elec_list<<<kLiveBlocks, 256, 0, STREAM(stream)>>>(d, counts, bitmaps, groups, nb,
+                                                         (int)g.x, (int)g.y, live_list);
     return check_launch("k_elec_list");
 }
 
 int waam_elec_jacobi_live(float* phi_a, float* phi_b, const float* sigma, const float* source,
                           const int32_t* live_list, const int32_t* zero_list,
                           const int32_t* counts, int nx, int ny, int nz, float dx,
-                          float omega_j, int n_sweeps, int first_chunk, float arc_k,
+                          float omega_j, int n_sweeps, int first_chunk, const float* arc_k_dev,
                           float sigma_cells, float* diff_buf, float* norm_buf, void* workspace,
                           size_t workspace_bytes, void* stream) {
     REQUIRE(dims_ok(nx, ny, nz), "elec_jacobi_live: bad dims");
@@ -873,25 +959,22 @@ int waam_elec_jacobi_live(float* phi_a, float* phi_b, const float* sigma, const 
     REQUIRE(n_sweeps >= 1, "elec_jacobi_live: n_sweeps must be >= 1");
     REQUIRE(!first_chunk || n_sweeps >= 2,
             "elec_jacobi_live: the first chunk of a solve needs at least 2 sweeps");
-    REQUIRE(std::isfinite(arc_k) && std::isfinite(sigma_cells) && std::fabs(arc_k) < 1e6f &&
-                std::fabs(sigma_cells) < 1e6f,
-            "elec_jacobi_live: arc k / sigma not finite");
+    REQUIRE(arc_k_dev && std::isfinite(sigma_cells) && std::fabs(sigma_cells) < 1e6f,
+            "elec_jacobi_live: null arc k or sigma not finite");
     Dims d{nx, ny, nz};
     REQUIRE(workspace_ok(workspace, workspace_bytes, d.n()),
             "elec_jacobi_live: workspace too small or misaligned");
-    int k_lo, k_hi;
-    source_slab(arc_k, sigma_cells, nz, k_lo, k_hi);
     float* in = phi_a;
     float* out = phi_b;
     for (int s = 0; s < n_sweeps; ++s) {
         if (s + 1 < n_sweeps)
             k_elec_jacobi_live<false><<<kLiveBlocks, 256, 0, STREAM(stream)>>>(
-                d, in, out, sigma, source, live_list, counts, dx, omega_j, k_lo, k_hi, nullptr,
-                nullptr, Workspace{});
+                d, in, out, sigma, source, live_list, counts, dx, omega_j, arc_k_dev,
+                sigma_cells, nullptr, nullptr, Workspace{});
         else
             k_elec_jacobi_live<true><<<kLiveBlocks, 256, 0, STREAM(stream)>>>(
-                d, in, out, sigma, source, live_list, counts, dx, omega_j, k_lo, k_hi, diff_buf,
-                norm_buf, Workspace::at(workspace));
+                d, in, out, sigma, source, live_list, counts, dx, omega_j, arc_k_dev,
+                sigma_cells, diff_buf, norm_buf, Workspace::at(workspace));
         int rc = check_launch("k_elec_jacobi_live");
         if (rc) return rc;
         if (first_chunk && s == 0) {
@@ -992,6 +1075,22 @@ int waam_elec_B_axisymmetric(float* Bx, float* By, float* Bz, const float* bins,
     k_elec_B<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(d, Bx, By, Bz, bins, arc_i, arc_j,
                                                                dx, bin_dr_cells, mu0, n_bins);
     return check_launch("k_elec_B");
+}
+
+int waam_elec_fields(float* Jx, float* Jy, float* Jz, float* Bx, float* By, float* Bz,
+                     float* bins, const float* phi, const float* sigma, const int32_t* flags,
+                     int nx, int ny, int nz, float arc_i, float arc_j, float dx,
+                     float bin_dr_cells, float mu0, int n_bins, void* workspace,
+                     size_t workspace_bytes, void* stream) {
+    int rc = waam_elec_compute_J(Jx, Jy, Jz, phi, sigma, flags, nx, ny, nz, dx, stream);
+    if (rc) return rc;
+    rc = waam_elec_bin_axial_current(Jz, bins, nx, ny, nz, arc_i, arc_j, dx, bin_dr_cells,
+                                     n_bins, workspace, workspace_bytes, stream);
+    if (rc) return rc;
+    rc = waam_elec_prefix_bins(bins, n_bins, nz, stream);
+    if (rc) return rc;
+    return waam_elec_B_axisymmetric(Bx, By, Bz, bins, nx, ny, nz, arc_i, arc_j, dx, bin_dr_cells,
+                                    mu0, n_bins, stream);
 }
 
 int waam_apply_lorentz_JxB(float* Fx, float* Fy, float* Fz, const float* Jx, const float* Jy,

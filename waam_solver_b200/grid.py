@@ -164,6 +164,7 @@ class WAAMGrid:
         from . import _native
         m = int(_native.lib().waam_elec_counts_len(self.nx, self.ny, self.nz))
         self.elec_counts = torch.zeros(m, dtype=torch.int32, device=self.device)
+        self.elec_arc_k = torch.zeros(1, dtype=torch.float32, device=self.device)
         self.n_elec_bins = 64
         self.elec_rad_bins = torch.zeros((self.nz, self.n_elec_bins), dtype=torch.float32,
                                          device=self.device)

@@ -709,14 +709,15 @@ def elec_prepare(sigma, fixed, phi_b, f_l, flags, sigma_liquid, sigma_solid, nz_
 
 
 def elec_jacobi_live(phi_a, phi_b, sigma, source, live, zero, counts, dx, omega_j, n_sweeps,
-                     first_chunk, arc_k, sigma_cells, diff_buf, norm_buf):
-    """n_sweeps sweeps over the live cells (see waam_elec_jacobi_live)."""
+                     first_chunk, arc_k_dev, sigma_cells, diff_buf, norm_buf):
+    """n_sweeps sweeps over the live cells (see waam_elec_jacobi_live); arc_k_dev:
+    a one-element float32 device tensor holding the arc height in cells."""
     nx, ny, nz = _dims(phi_a)
     n = nx * ny * nz
     ws, wsb = workspace_for(phi_a)
     _call("waam_elec_jacobi_live", _f(phi_a, n), _f(phi_b, n), _f(sigma, n), _f(source, n),
           live.data_ptr(), zero.data_ptr(), counts.data_ptr(), nx, ny, nz, float(dx),
-          float(omega_j), int(n_sweeps), 1 if first_chunk else 0, float(arc_k),
+          float(omega_j), int(n_sweeps), 1 if first_chunk else 0, _f(arc_k_dev, 1),
           float(sigma_cells), _f(diff_buf, 1), _f(norm_buf, 1), ws, wsb, _stream())
 
 
@@ -738,6 +739,28 @@ def elec_arc_source(source, arc_i, arc_j, arc_k, sigma_cells, current_A, dx):
     ws, wsb = workspace_for(source)
     _call("waam_elec_arc_source", _f(source), nx, ny, nz, float(arc_i), float(arc_j),
           float(arc_k), float(sigma_cells), float(current_A), float(dx), ws, wsb, _stream())
+
+
+def elec_arc_source_dev(source, arc_i, arc_j, arc_k_dev, sigma_cells, current_A, dx):
+    """elec_arc_source with the arc height in a one-element device tensor."""
+    nx, ny, nz = _dims(source)
+    ws, wsb = workspace_for(source)
+    _call("waam_elec_arc_source_dev", _f(source), nx, ny, nz, float(arc_i), float(arc_j),
+          _f(arc_k_dev, 1), float(sigma_cells), float(current_A), float(dx), ws, wsb, _stream())
+
+
+def elec_fields(Jx, Jy, Jz, Bx, By, Bz, bins, phi, sigma, flags, arc_i, arc_j, dx, bin_dr_cells,
+                mu0, n_bins):
+    """elec_compute_J, elec_bin_axial_current, elec_prefix_bins, elec_B_axisymmetric."""
+    nx, ny, nz = _dims(phi)
+    n = nx * ny * nz
+    if tuple(bins.shape) != (nz, int(n_bins)):
+        raise WaamError("elec_fields: bins must be (nz, n_bins)")
+    ws, wsb = workspace_for(phi)
+    _call("waam_elec_fields", _f(Jx, n), _f(Jy, n), _f(Jz, n), _f(Bx, n), _f(By, n), _f(Bz, n),
+          _f(bins, nz * int(n_bins)), _f(phi, n), _f(sigma, n), _i(flags, n), nx, ny, nz,
+          float(arc_i), float(arc_j), float(dx), float(bin_dr_cells), float(mu0), int(n_bins),
+          ws, wsb, _stream())
 
 
 def elec_normalize_source(source, target_current_A, dx):

@@ -33,18 +33,23 @@ def _jacobi_budget(twin, g, cold_start):
     return max_iters
 
 
-def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True):
+def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True, arc_k_dev=None):
     """``apply_force=False`` leaves J x B to the caller (the fused step adds it
-    inside its collision, before the force clamp)."""
+    inside its collision, before the force clamp).  ``arc_k_dev``: the arc
+    height as a one-element device tensor (the fused step's scalar), used
+    instead of ``arc_k`` so that nothing is read back before the solve."""
     if not twin.enable_lorentz:
         return
     g.ensure_lorentz_fields()
+    if arc_k_dev is None:
+        g.elec_arc_k.fill_(float(arc_k))
+        arc_k_dev = g.elec_arc_k
     # phi_elec is the first sweep's input, phi_elec_tmp its output
     kernels.elec_prepare(g.sigma_elec, g.elec_fixed, g.phi_elec_tmp, g.f_l, g.flags,
                          twin.sigma_liquid_Sm, twin.sigma_solid_Sm, twin.nz_solid, g.elec_live,
                          g.elec_zero, g.elec_counts)
-    kernels.elec_arc_source(g.elec_source, arc_i, arc_j, arc_k, twin.sigma_cells,
-                            twin.welding_current_A, g.dx)
+    kernels.elec_arc_source_dev(g.elec_source, arc_i, arc_j, arc_k_dev, twin.sigma_cells,
+                                twin.welding_current_A, g.dx)
 
     cold_start = not getattr(twin, "_lorentz_warm", False)
     if cold_start:
@@ -60,7 +65,7 @@ def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True):
         chunk = min(check_every, max_iters - iters_done)
         kernels.elec_jacobi_live(g.phi_elec, g.phi_elec_tmp, g.sigma_elec, g.elec_source,
                                  g.elec_live, g.elec_zero, g.elec_counts, g.dx,
-                                 twin.lorentz_jacobi_omega, chunk, iters_done == 0, arc_k,
+                                 twin.lorentz_jacobi_omega, chunk, iters_done == 0, arc_k_dev,
                                  twin.sigma_cells, g.elec_res_buf, g.elec_norm_buf)
         if chunk % 2 == 1:
             g.phi_elec, g.phi_elec_tmp = g.phi_elec_tmp, g.phi_elec
@@ -81,14 +86,10 @@ def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True):
         twin._lorentz_unconverged_streak = 0
     twin._lorentz_last_iters = iters_done
 
-    kernels.elec_compute_J(g.Jx, g.Jy, g.Jz, g.phi_elec, g.sigma_elec, g.flags, g.dx, g.FLAG_GAS,
-                           g.nx, g.ny, g.nz)
     bin_dr_cells = max(float(max(g.nx, g.ny)) / (2.0 * g.n_elec_bins), 0.5)
-    kernels.elec_bin_axial_current(g.Jz, g.elec_rad_bins, arc_i, arc_j, g.dx, bin_dr_cells,
-                                   g.n_elec_bins, g.nz)
-    kernels.elec_prefix_bins(g.elec_rad_bins, g.n_elec_bins, g.nz)
-    kernels.elec_B_axisymmetric(g.Bx, g.By, g.Bz, g.elec_rad_bins, arc_i, arc_j, g.dx,
-                                bin_dr_cells, MU0, g.n_elec_bins, g.nz)
+    kernels.elec_fields(g.Jx, g.Jy, g.Jz, g.Bx, g.By, g.Bz, g.elec_rad_bins, g.phi_elec,
+                        g.sigma_elec, g.flags, arc_i, arc_j, g.dx, bin_dr_cells, MU0,
+                        g.n_elec_bins)
     if apply_force:
         kernels.apply_lorentz_JxB(g.Fx, g.Fy, g.Fz, g.Jx, g.Jy, g.Jz, g.Bx, g.By, g.Bz, g.f_l,
                                   g.flags, g.dt, g.dx, twin.mat.rho, g.FLAG_GAS)

@@ -105,7 +105,8 @@ def apply_gas_shear(twin, g, arc_i, arc_j, arc_k):
         raise WaamError("shielding-gas shear is not supported by this backend")
 
 
-def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True):
+def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True, arc_k_dev=None):
     if twin.enable_lorentz:
         from . import lorentz
-        lorentz.solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=apply_force)
+        lorentz.solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=apply_force,
+                              arc_k_dev=arc_k_dev)
