@@ -538,7 +538,11 @@ def melt_metrics(tw):
     metal reached the solidus (T_max >= T_s); HAZ T_max: the highest T_max in
     the substrate plane 1 mm below the deepest remelted cell; pool width /
     depth: extent of f_l > 0.5 across y and down from the top of the pool in
-    the x section through the pool's centroid."""
+    the x section through the pool's centroid.  Also whether H is finite and
+    the largest |rho - 1| of the FLUID/IFACE cells: the reference's LBM moves
+    no populations into collided cells (streamed values land in the buffer
+    the next collision overwrites), so a liquid cell under a steady force
+    gathers momentum step after step and its density eventually diverges."""
     import numpy as np
     g = tw.grid
     Ts = tw.mat.T_solidus
@@ -551,7 +555,11 @@ def melt_metrics(tw):
     k_melt = int(melted.min()) if melted.size else nzs
     depth_cells = nzs - k_melt
     k_haz = max(0, min(nzs - 1, k_melt - int(round(1e-3 / g.dx))))
-    out = {"remelt_depth_mm": depth_cells * g.dx * 1e3, "remelt_depth_cells": depth_cells,
+    act = (flags == 0) | (flags == 4)
+    rho = g.rho.cpu().numpy().astype(np.float64)
+    out = {"finite": bool(np.isfinite(g.H.cpu().numpy()).all()),
+           "rho_dev_max_active": float(np.abs(rho[act] - 1.0).max()) if act.any() else 0.0,
+           "remelt_depth_mm": depth_cells * g.dx * 1e3, "remelt_depth_cells": depth_cells,
            "haz_plane_k": k_haz, "haz_T_max_K": float(tmax[:, :, k_haz].max()),
            "T_max_peak_K": float(tmax[flags != 2].max()) if (flags != 2).any() else None,
            "pool_width_cells": 0, "pool_depth_cells": 0,

@@ -144,6 +144,17 @@ struct ArcParams {
     int enable;
 };
 
+// The spatial factor of one cell's arc weight (the Gaussian exponential or the
+// Goldak pdf), before the depth weight.
+__device__ __forceinline__ float arc_cell_shape(const ArcParams& p, int i, int j, int k) {
+    float di = (float)i - p.arc_i, dj = (float)j - p.arc_j, dk = (float)k - p.arc_k;
+    if (p.kind == 0) {
+        float r2 = di * di + dj * dj + dk * dk * 0.25f;
+        return waam_expf(-r2 * p.inv2s2);
+    }
+    return goldak_w(di, dj, dk, p.sign, p.ff, p.fr, p.a_f, p.a_r, p.b, p.c);
+}
+
 // Weight of one cell before normalisation (0 for skipped cells).
 __device__ __forceinline__ float arc_cell_weight(const ArcParams& p, int i, int j, int k, int flag,
                                                  float fl) {

@@ -27,6 +27,7 @@ constexpr int kMainEvents = 7;
 constexpr int kMaxDevices = 64;
 constexpr int kTileRedBlocks = 592;   // <= kWsMaxPartials; a fixed grid keeps the sum order fixed
 constexpr int kListThreads = 128;
+constexpr int kArcTableMax = 1024;    // nz up to which the arc depth weights come from a table
 constexpr int kListBlocks = 148 * 6;
 
 
@@ -305,15 +306,20 @@ __device__ double tile_block_sum(double v) {
 // Arc weight sum over 32x8 tiles (pass 1 of kernels.py:443-510 / 548-622),
 // deterministic: fixed tile-to-block assignment, double partials, the last
 // block sums them in order.  Writes the weight sum and the energy per weight.
+// The depth weight of a cell that is not liquid depends on k alone: it comes
+// from a per-block table of the nz values (kArcTableMax at most; larger nz
+// computes it per cell).  The spatial factor of every weighted cell is left
+// in `shape` for the injection pass, which then needs no exponential.
 __global__ void __launch_bounds__(256) k_arc_norm_tiles(Dims d, const int32_t* __restrict__ flags,
                                                         const float* __restrict__ f_l,
                                                         const float* __restrict__ phi, int nz_solid,
                                                         ArcParams p, float* scalars,
                                                         float arc_k_offset, float Qe_dt, float dx3,
-                                                        Workspace ws) {
+                                                        Workspace ws, float* __restrict__ shape) {
     // every block finds the arc k itself (one warp scans the torch column), so
     // the surface query needs no launch of its own; block 0 publishes it
     __shared__ float s_arc_k;
+    __shared__ float s_wd[kArcTableMax];
     if (threadIdx.y == 0) {
         const float kf = surface_arc_k(d, phi, flags, scalars, nz_solid);
         if (threadIdx.x == 0) {
@@ -325,6 +331,11 @@ __global__ void __launch_bounds__(256) k_arc_norm_tiles(Dims d, const int32_t* _
     p.arc_k = s_arc_k + arc_k_offset;
     p.arc_i = scalars[kScalarArcI];
     p.arc_j = scalars[kScalarArcJ];
+    const bool table = d.nz <= kArcTableMax;
+    if (table)
+        for (int k = threadIdx.y * kTileK + threadIdx.x; k < d.nz; k += kTileK * kTileJ)
+            s_wd[k] = arc_weight(k, p.arc_k, 0.0f, p.pen, p.enable);
+    __syncthreads();
     const int kt = (d.nz + kTileK - 1) / kTileK, jt = (d.ny + kTileJ - 1) / kTileJ;
     const int tiles = kt * jt * d.nx;
     // four tiles per pass: their flags and liquid fractions are all requested
@@ -349,8 +360,16 @@ __global__ void __launch_bounds__(256) k_arc_norm_tiles(Dims d, const int32_t* _
             ck[u] = k;
         }
 #pragma unroll
-        for (int u = 0; u < kU; ++u)
-            if (fg[u] != GAS) part += (double)arc_cell_weight(p, ci[u], cj[u], ck[u], fg[u], fl[u]);
+        for (int u = 0; u < kU; ++u) {
+            if (fg[u] == GAS) continue;
+            // arc_cell_weight (waam_common.cuh) with the depth weight from the table
+            const float wd = !table ? arc_weight(ck[u], p.arc_k, fl[u], p.pen, p.enable)
+                                    : (fl[u] > 0.55f ? 1.0f : s_wd[ck[u]]);
+            if (wd < 1e-6f) continue;
+            const float sh = arc_cell_shape(p, ci[u], cj[u], ck[u]);
+            shape[(ci[u] * d.ny + cj[u]) * d.nz + ck[u]] = sh;
+            part += (double)(sh * wd);
+        }
     }
     part = tile_block_sum(part);
     __shared__ bool last;
@@ -388,20 +407,37 @@ __global__ void __launch_bounds__(256) k_arc_inject_tiles(Dims d, float* __restr
                                                           float arc_k_offset, int cap,
                                                           PhaseParams ph,
                                                           const float* __restrict__ cp_f,
-                                                          VarPhase vp) {
+                                                          VarPhase vp,
+                                                          const float* __restrict__ shape) {
     int i, j, k, c;
-    if (!tile_cell(d, i, j, k, c)) return;
+    const bool ok = tile_cell(d, i, j, k, c);
     // the device scalars and the flag are requested together, then f_l and H
     p.arc_k = scalars[kScalarArcK] + arc_k_offset;
     p.arc_i = scalars[kScalarArcI];
     p.arc_j = scalars[kScalarArcJ];
+    // depth weights of the block's 32 k values (non-liquid cells)
+    __shared__ float s_wd[kTileK];
+    if (threadIdx.y == 0)
+        s_wd[threadIdx.x] = arc_weight(blockIdx.x * kTileK + threadIdx.x, p.arc_k, 0.0f, p.pen,
+                                       p.enable);
+    __syncthreads();
+    if (!ok) return;
     const float epw = scalars[kScalarEpw];
     const int flag = flags[c];
     const float fl = f_l[c];           // requested with the flag (ignored for gas cells)
     float h = cap ? H[c] : 0.0f;
     if (flag == GAS) return;
-    float dh;
-    const bool hit = arc_cell_heat(p, epw, i, j, k, flag, fl, dh);
+    // arc_cell_heat (waam_common.cuh) with the spatial factor the weight-sum
+    // pass left in `shape` and the depth weight from the table
+    float dh = 0.0f;
+    bool hit = false;
+    if (epw > 0.0f) {
+        const float wd = fl > 0.55f ? 1.0f : s_wd[threadIdx.x];
+        if (!(wd < 1e-6f)) {
+            dh = epw * shape[c] * wd;
+            hit = true;
+        }
+    }
     if (!hit && !cap) return;
     if (!cap) h = H[c];
     if (hit) h = h + dh;
@@ -936,13 +972,13 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     const int blocks = tiles < kTileRedBlocks ? tiles : kTileRedBlocks;
     k_arc_norm_tiles<<<blocks, tile_block(), 0, STREAM(stream)>>>(
         d, f->flags, f->f_l, f->phi, p->nz_solid, a, f->step_scalars, p->arc_k_offset, Qe_dt,
-        p->dx3, ws);
+        p->dx3, ws, ws.field);
     int e = check_launch("k_arc_norm_tiles");
     if (e) return e;
     PhaseParams ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
     k_arc_inject_tiles<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
         d, f->H, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, p->cap_enabled, ph,
-        p->use_tables ? f->cp_rho_f : nullptr, var_phase(p));
+        p->use_tables ? f->cp_rho_f : nullptr, var_phase(p), ws.field);
     return check_launch("k_arc_inject_tiles");
 }
 
