@@ -580,6 +580,14 @@ typedef struct WaamFields {
      * (solvers/coupled_step.py:352-362).  Null: no Lorentz force. */
     const float* lorentz_J[3];
     const float* lorentz_B[3];
+    /* flag copies for the pipelined stream (null: none): waam_step_main's
+     * column pass writes the step's flags also to flags_copy_w, and the
+     * pending stream of the previous step (WaamStepParams.stream_prev) reads
+     * flags_copy_r, the copy that step wrote -- so it may run on while the
+     * column pass rewrites the flags, and is joined only before the
+     * collision.  The caller alternates two buffers from step to step. */
+    int32_t* flags_copy_w;
+    const int32_t* flags_copy_r;
 } WaamFields;
 
 typedef struct WaamStepParams {
@@ -633,6 +641,19 @@ typedef struct WaamStepParams {
     float H_sol_t, H_liq_t; /* rho * cp(T_solidus) * T_solidus, H_sol_t + L_rho */
     float tau_ref;          /* grid tau (SOLID / GAS cells) */
     WaamMaterialTables tables;
+    /* pipelined stream: the stream of step n reads and writes only population
+     * buffers, and step n + 1 touches them again only from its column pass on
+     * (the collision writes the buffer the stream of step n writes), while
+     * its arc, thermal and VOF stages only read the flags the stream reads.
+     * defer_stream = 1: waam_step_main leaves this step's stream pending;
+     * stream_prev = 1: it is pending from the step before -- waam_step_pre
+     * starts it on a library stream beside the arc, thermal and VOF stages and
+     * waam_step_main joins it before the column pass.  A caller that reads or
+     * writes populations between steps runs the pending stream first with
+     * waam_step_stream.  defer_stream needs the remelt / solidify tail off
+     * (it writes flags after the stream). */
+    int stream_prev;
+    int defer_stream;
 } WaamStepParams;
 
 /* Stages of one fused step.  waam_step_pre runs the surface-height query,
@@ -648,6 +669,10 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
                   size_t workspace_bytes, void* stream);
 int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace,
                    size_t workspace_bytes, void* stream);
+/* The stream left pending by the previous step (WaamStepParams.defer_stream),
+ * for fields that describe the step after it (buffers swapped): reads f_src,
+ * writes f_dst, with the flags of that step. */
+int waam_step_stream(const WaamFields* f, const WaamStepParams* p, void* stream);
 /* waam_step_main that also records events[0..6] (cudaEvent_t handles) on the
  * stream at the stage boundaries: before thermal, after thermal, after VOF
  * advection, after the column pass, after collide, after stream, after the

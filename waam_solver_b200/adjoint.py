@@ -54,6 +54,7 @@ class _Checkpoint:
 
     def __init__(self, tw):
         g = tw.grid
+        g.flush_stream()
         self.t = {k: getattr(g, k).clone() for k in _FIELDS}
         self.t["_H"] = [h.clone() for h in g._H]
         self.t["_T"] = [x.clone() for x in g._T]
@@ -63,6 +64,7 @@ class _Checkpoint:
 
     def restore(self, tw):
         g = tw.grid
+        g._stream_pending = False       # the checkpoint holds a streamed state
         for k in _FIELDS:
             getattr(g, k).copy_(self.t[k])
         for dst, src in zip(g._H, self.t["_H"]):
@@ -380,6 +382,9 @@ def _taped_step(tw, x, y, tape, slot):
     p = tw._fused_params
     if p is None:
         p = tw._fused_params = step_params(tw)
+    g.flush_stream()
+    p.stream_prev = 0
+    p.defer_stream = 0
     arc_i, arc_j = sim_x / g.dx, sim_y / g.dx
     p.arc_i, p.arc_j = arc_i, arc_j
     p.welding = 1

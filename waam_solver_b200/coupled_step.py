@@ -295,6 +295,11 @@ def _fields(g):
         f.max_tracers = g.max_tracers
     f.cp_rho_f, f.alpha_f = g.cp_rho_field.data_ptr(), g.alpha_lu_field.data_ptr()
     f.dgamma_f, f.tau_f = g.dgamma_lu_field.data_ptr(), g.tau_field.data_ptr()
+    copies = getattr(g, "flags_copies", None)
+    if copies is not None:
+        w = getattr(g, "_flags_copy_i", 0)
+        f.flags_copy_w = copies[w].data_ptr()
+        f.flags_copy_r = copies[1 - w].data_ptr()
     return f
 
 
@@ -409,7 +414,7 @@ def upload_position(twin, arc_i, arc_j):
 def _fields_cached(g, lorentz=False):
     """WaamFields for the current buffer parity (device pointers never move);
     ``lorentz``: with the current density and self field the collision adds."""
-    key = (g._read_buf is g.f_a, g._cur, lorentz)
+    key = (g._read_buf is g.f_a, g._cur, lorentz, getattr(g, "_flags_copy_i", 0))
     cache = g.__dict__.setdefault("_fields_cache", {})
     f = cache.get(key)
     if f is None:
@@ -421,6 +426,18 @@ def _fields_cached(g, lorentz=False):
                 f.lorentz_B[q] = t.data_ptr()
         g._pos_dst = g.step_scalars[4:6]
     return f
+
+
+def flush_stream(g):
+    """Run the stream a pipelined step left pending (WaamStepParams.defer_stream),
+    so that the population buffers hold the step's result.  A no-op otherwise."""
+    if not getattr(g, "_stream_pending", False):
+        return
+    g._stream_pending = False
+    p = _native.WaamStepParams()
+    p.f_storage = g.population_storage
+    _native.call("waam_step_stream", ctypes.byref(_fields_cached(g)), ctypes.byref(p),
+                 torch.cuda.current_stream().cuda_stream)
 
 
 def _droplet_due(twin, g, is_welding):
@@ -466,6 +483,7 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     convergence checks read back; the collision then adds J x B before the
     force clamp."""
     if not _check_fused_supported(twin):
+        flush_stream(twin.grid)
         return coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m)
     g = twin.grid
     if twin.enable_ctwd:
@@ -483,6 +501,11 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     p.clear_forces = 1 if getattr(g, "_forces_dirty", True) else 0
     dx_, dy_, dz_ = getattr(twin, "_torch_dir_xyz", (1.0, 0.0, 0.0))
     p.dir_x, p.dir_y, p.dir_z = dx_, dy_, dz_
+    if getattr(g, "flags_copies", None) is None:
+        # the flags of each step, copied by its column pass, for its pending stream
+        g.flags_copies = (torch.zeros_like(g.flags), torch.zeros_like(g.flags))
+        g._flags_copy_i = 0
+        g.__dict__.pop("_fields_cache", None)
     f = _fields_cached(g)
     ws = g.workspace
     upload_position(twin, arc_i, arc_j)
@@ -490,9 +513,18 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     events = getattr(twin, "_stage_events", None)
     due = _droplet_due(twin, g, is_welding)
     lorentz = bool(is_welding and twin.enable_lorentz)
+    # Pipelined stream: this step's stream is left to run beside the next
+    # step's first stages.  Droplet steps (the deposition writes populations),
+    # instrumented steps and the remelt / solidify tail run it in order.
+    if due or events is not None:
+        flush_stream(g)
+    p.stream_prev = 1 if getattr(g, "_stream_pending", False) else 0
+    p.defer_stream = 1 if (getattr(twin, "pipeline_stream", True) and events is None and
+                           not (twin.enable_bead_freeze or twin.enable_substrate_growth)) else 0
     done = False
     if not due and not lorentz and events is None and getattr(twin, "use_cuda_graphs", True):
-        key = (g._read_buf is g.f_a, g._cur, p.welding, p.clear_forces,
+        key = (g._read_buf is g.f_a, g._cur, p.welding, p.clear_forces, p.stream_prev,
+               p.defer_stream, g._flags_copy_i,
                (dx_, dy_, dz_) if twin.enable_bead_freeze else None)
         done = _run_graph(twin, g, f, p, ws, key)
     if not done:
@@ -535,6 +567,8 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     # the droplet impact load (and J x B on SOLID cells) stays in F outside the
     # active cells until the next step
     g._forces_dirty = bool(p.forces_from_buffer) or lorentz
+    g._stream_pending = bool(p.defer_stream)
+    g._flags_copy_i = 1 - g._flags_copy_i    # this step's copy is read by the next step
     g.flip_thermal()
     g.swap_buffers()
     twin._step_n += 1

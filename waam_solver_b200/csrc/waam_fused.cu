@@ -212,10 +212,9 @@ __device__ __forceinline__ int stream_source(const Dims& d, bool interior, int i
 // T is the stored element: streaming moves stored values unchanged, whatever
 // the population storage.
 template <typename T>
-__global__ void __launch_bounds__(256) k_stream(Dims d, const __grid_constant__ StreamPtrs<T> P,
-                                                const int32_t* __restrict__ flags) {
-    int i, j, k, c;
-    if (!tile_cell(d, i, j, k, c)) return;
+__device__ __forceinline__ void stream_cell(const Dims& d, const StreamPtrs<T>& P,
+                                            const int32_t* __restrict__ flags, int i, int j,
+                                            int k, int c) {
     const int flag = flags[c];
     if (flag == SOLID) return;
     const bool interior = i > 0 && i < d.nx - 1 && j > 0 && j < d.ny - 1 && k > 0 && k < d.nz - 1;
@@ -235,6 +234,15 @@ __global__ void __launch_bounds__(256) k_stream(Dims d, const __grid_constant__ 
 #pragma unroll
     for (int q = 0; q < 19; ++q) P.dst[q][c] = v[q];
 }
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_stream(Dims d, const __grid_constant__ StreamPtrs<T> P,
+                                                const int32_t* __restrict__ flags) {
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
+    stream_cell(d, P, flags, i, j, k, c);
+}
+
 
 template <typename T>
 static void launch_stream_t(const Dims& d, const void* f_src, void* f_dst, const int32_t* flags,
@@ -605,6 +613,7 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
                                                 float* __restrict__ Fy, float* __restrict__ Fz,
                                                 int* __restrict__ active_list,
                                                 unsigned* __restrict__ active_count,
+                                                int32_t* __restrict__ flags_copy,
                                                 ColumnArgs a) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (warp >= d.nx * d.ny) return;
@@ -638,6 +647,7 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
                                Fz[c] = 0.0f;
                            }
                        }
+                       if (valid && flags_copy) flags_copy[c] = flag;
                        bool act = valid && is_active(flag);
                        unsigned m = __ballot_sync(0xffffffffu, act);
                        if (m) {
@@ -893,9 +903,15 @@ static ArcParams arc_params(const WaamStepParams* p) {
 // (created on the first step on that device, which should not be inside a
 // stream capture).  Calls on different host threads share them; every fork is
 // ordered by its own event record, so sharing only serialises.
+// hi: the stages of the step (highest priority); s2: VOF advection beside the
+// thermal stage (highest priority); s3: the pending stream of the previous
+// step (lowest priority), so that its blocks fill what the latency-bound arc,
+// thermal and VOF kernels leave free instead of being placed before them.
 struct AuxStream {
+    cudaStream_t hi = nullptr;
     cudaStream_t s2 = nullptr;
-    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaStream_t s3 = nullptr;
+    cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 static int aux_stream(AuxStream** out) {
@@ -908,8 +924,15 @@ static int aux_stream(AuxStream** out) {
     std::lock_guard<std::mutex> lock(mu);
     AuxStream& a = table[dev];
     if (!a.s2) {
-        e = cudaStreamCreateWithFlags(&a.s2, cudaStreamNonBlocking);
-        for (int q = 0; q < 2 && e == cudaSuccess; ++q)
+        int least = 0, greatest = 0;
+        e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (e == cudaSuccess)
+            e = cudaStreamCreateWithPriority(&a.hi, cudaStreamNonBlocking, greatest);
+        if (e == cudaSuccess)
+            e = cudaStreamCreateWithPriority(&a.s2, cudaStreamNonBlocking, greatest);
+        if (e == cudaSuccess)
+            e = cudaStreamCreateWithPriority(&a.s3, cudaStreamNonBlocking, least);
+        for (int q = 0; q < 8 && e == cudaSuccess; ++q)
             e = cudaEventCreateWithFlags(&a.ev[q], cudaEventDisableTiming);
         if (e != cudaSuccess) {
             a.s2 = nullptr;
@@ -919,6 +942,29 @@ static int aux_stream(AuxStream** out) {
     *out = &a;
     return WAAM_OK;
 }
+
+// The stages of a call run on the library's high-priority stream, forked from
+// and joined back into the caller's stream (events ev[fork], ev[fork + 1]).
+struct WorkStream {
+    cudaStream_t caller = nullptr, s = nullptr;
+    AuxStream* aux = nullptr;
+    int slot = 0;
+    int err = WAAM_OK;
+    WorkStream(cudaStream_t c, bool use_hi, int fork_slot) : caller(c), s(c), slot(fork_slot) {
+        if (!use_hi) return;
+        err = aux_stream(&aux);
+        if (err) return;
+        cudaEventRecord(aux->ev[slot], caller);
+        cudaStreamWaitEvent(aux->hi, aux->ev[slot], 0);
+        s = aux->hi;
+    }
+    ~WorkStream() {
+        if (aux && s != caller) {
+            cudaEventRecord(aux->ev[slot + 1], s);
+            cudaStreamWaitEvent(caller, aux->ev[slot + 1], 0);
+        }
+    }
+};
 
 static bool fields_ok(const WaamFields* f) {
     return f && f->f_src && f->f_dst && f->rho && f->ux && f->uy && f->uz && f->T && f->T_next &&
@@ -946,9 +992,10 @@ extern "C" {
 
 int waam_step_launch_count(const WaamStepParams* p, int stage) {
     if (!p) return 0;
-    if (stage == 0) return p->welding ? 2 : 1;
-    // thermal, [vof], column, collide, stream (tracers counted by the caller)
-    int n = 1 + (p->vof ? 1 : 0) + 1 + 1 + 1;
+    // the pending stream of the previous step is launched by waam_step_pre
+    if (stage == 0) return (p->welding ? 2 : 1) + (p->stream_prev ? 1 : 0);
+    // thermal, [vof], column, collide, [stream] (tracers counted by the caller)
+    int n = 1 + (p->vof ? 1 : 0) + 1 + 1 + (p->defer_stream ? 0 : 1);
     if (p->substrate_growth || p->bead_freeze) n += 1;
     return n;
 }
@@ -961,8 +1008,26 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     if (!workspace_ok(workspace, workspace_bytes, d.n()))
         return fail(WAAM_ERR_INVALID, "step_pre: workspace too small or misaligned");
     Workspace ws = Workspace::at(workspace);
+    WorkStream W(STREAM(stream), true, 4);
+    if (W.err) return W.err;
+    const cudaStream_t s = W.s;
+    if (p->stream_prev) {
+        // the previous step's stream, beside this step's stages up to the
+        // column pass (waam_step_main joins it there)
+        AuxStream* aux = nullptr;
+        int ea = aux_stream(&aux);
+        if (ea) return ea;
+        cudaEventRecord(aux->ev[2], s);
+        cudaStreamWaitEvent(aux->s3, aux->ev[2], 0);
+        // the flags it streams with: the previous step's copy if there is one
+        // (then the column pass may rewrite the flags meanwhile)
+        const int32_t* sf = f->flags_copy_r ? f->flags_copy_r : f->flags;
+        ea = launch_stream_stored(d, f->f_src, f->f_dst, sf, p->f_storage, aux->s3);
+        if (ea) return ea;
+        cudaEventRecord(aux->ev[3], aux->s3);
+    }
     if (!p->welding) {
-        k_surface_arc<<<1, 32, 0, STREAM(stream)>>>(d, f->phi, f->flags, f->step_scalars,
+        k_surface_arc<<<1, 32, 0, s>>>(d, f->phi, f->flags, f->step_scalars,
                                                     p->nz_solid);
         return check_launch("k_surface_arc");
     }
@@ -970,16 +1035,24 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     float Qe_dt = p->Q_w * p->eta * p->dt;
     const int tiles = (int)tile_grid(d).x * (int)tile_grid(d).y * d.nx;
     const int blocks = tiles < kTileRedBlocks ? tiles : kTileRedBlocks;
-    k_arc_norm_tiles<<<blocks, tile_block(), 0, STREAM(stream)>>>(
+    k_arc_norm_tiles<<<blocks, tile_block(), 0, s>>>(
         d, f->flags, f->f_l, f->phi, p->nz_solid, a, f->step_scalars, p->arc_k_offset, Qe_dt,
         p->dx3, ws, ws.field);
     int e = check_launch("k_arc_norm_tiles");
     if (e) return e;
     PhaseParams ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
-    k_arc_inject_tiles<<<tile_grid(d), tile_block(), 0, STREAM(stream)>>>(
+    k_arc_inject_tiles<<<tile_grid(d), tile_block(), 0, s>>>(
         d, f->H, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, p->cap_enabled, ph,
         p->use_tables ? f->cp_rho_f : nullptr, var_phase(p), ws.field);
     return check_launch("k_arc_inject_tiles");
+}
+
+int waam_step_stream(const WaamFields* f, const WaamStepParams* p, void* stream) {
+    if (!fields_ok(f) || !p) return fail(WAAM_ERR_INVALID, "step_stream: bad fields or params");
+    if (p->f_storage < kStoreF32 || p->f_storage > kStoreBF16)
+        return fail(WAAM_ERR_INVALID, "step_stream: bad f_storage");
+    Dims d{f->nx, f->ny, f->nz};
+    return launch_stream_stored(d, f->f_src, f->f_dst, f->flags, p->f_storage, STREAM(stream));
 }
 
 int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace,
@@ -1000,6 +1073,8 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         return fail(WAAM_ERR_INVALID, "step_main: f_storage must be 0 (f32), 1 (f16) or 2 (bf16)");
     if (events && n_events < kMainEvents)
         return fail(WAAM_ERR_INVALID, "step_main: need 7 events");
+    if (p->defer_stream && (p->substrate_growth || p->bead_freeze))
+        return fail(WAAM_ERR_INVALID, "step_main: defer_stream needs the remelt/solidify tail off");
     for (int q = 0; events && q < kMainEvents; ++q)
         if (!events[q]) return fail(WAAM_ERR_INVALID, "step_main: null event handle");
     auto mark = [&](int i) {
@@ -1016,7 +1091,10 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
     if (shard_cap * kActiveShards > d.n() + kFieldSlack || shard_cap > INT32_MAX)
         return fail(WAAM_ERR_INVALID, "step_main: nz too large for the active-cell list");
     const int col_blocks = (int)(((int64_t)d.nx * d.ny * 32 + kThreads - 1) / kThreads);
-    cudaStream_t s = STREAM(stream);
+    // without stage events the stages run on the library's high-priority stream
+    WorkStream W(STREAM(stream), events == nullptr, 6);
+    if (W.err) return W.err;
+    cudaStream_t s = W.s;
     int e = WAAM_OK;
 
     if (stages & 1) {
@@ -1094,6 +1172,14 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
             }
         }
         mark(2);
+        if (p->stream_prev && !f->flags_copy_r) {
+            // the previous step's stream (started by waam_step_pre) ends here:
+            // the column pass writes the flags it reads
+            AuxStream* sa = nullptr;
+            int ea = aux_stream(&sa);
+            if (ea) return ea;
+            cudaStreamWaitEvent(s, sa->ev[3], 0);
+        }
         ColumnArgs ca;
         ca.vof = p->vof;
         ca.wetting = p->wetting;
@@ -1109,13 +1195,21 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         ca.shard_cap = (int)shard_cap;
         k_column<<<col_blocks, kThreads, 0, s>>>(d, f->phi_tmp, f->phi, f->flags, f->f_l, f->T_next,
                                                  f->t800, f->t1100, f->tsol, f->Fx, f->Fy, f->Fz,
-                                                 active_list, active_count, ca);
+                                                 active_list, active_count, f->flags_copy_w, ca);
         e = check_launch("k_column");
         if (e) return e;
         mark(3);
     }
 
     if (stages & 2) {
+        if (p->stream_prev && f->flags_copy_r) {
+            // the previous step's stream ends here: the collision writes the
+            // populations of the active cells into the buffer it writes
+            AuxStream* sa = nullptr;
+            int ea = aux_stream(&sa);
+            if (ea) return ea;
+            cudaStreamWaitEvent(s, sa->ev[3], 0);
+        }
         CollideArgs cl;
         ForceParams& P = cl.P;
         P.csf = p->csf;
@@ -1185,11 +1279,15 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         }
         mark(4);
 
-        e = launch_stream_stored(d, f->f_dst, f->f_src, f->flags, p->f_storage, s);
-        if (e) return e;
+        if (!p->defer_stream) {
+            e = launch_stream_stored(d, f->f_dst, f->f_src, f->flags, p->f_storage, s);
+            if (e) return e;
+        }
+        // tracers read u, f_l and flags only (they follow the stream in the
+        // reference order; nothing of theirs depends on it)
         if (f->tracer_pos && f->tracer_active && f->max_tracers > 0) {
             e = launch_advect_tracers(d, f->tracer_pos, f->tracer_active, f->ux, f->uy, f->uz,
-                                      f->f_l, f->flags, p->dx, f->max_tracers, stream);
+                                      f->f_l, f->flags, p->dx, f->max_tracers, s);
             if (e) return e;
         }
         mark(5);

@@ -229,14 +229,22 @@ class WAAMGrid:
             w = self._w_col = self.w.view(Q, 1, 1, 1)
         return w
 
+    def flush_stream(self):
+        """Run the stream a pipelined step left pending (see coupled_step)."""
+        if getattr(self, "_stream_pending", False):
+            from .coupled_step import flush_stream
+            flush_stream(self)
+
     def populations(self, t):
         """float32 f_q of population buffer ``t`` (f_a, f_b, f_src or f_dst)."""
+        self.flush_stream()
         if t.dtype == torch.float32:
             return t
         return t.float() + self._rest_weights()
 
     def store_populations(self, dst, f):
         """Write float32 f_q into population buffer ``dst`` in its storage."""
+        self.flush_stream()
         f = torch.as_tensor(f, device=self.device).to(torch.float32).reshape(dst.shape)
         if dst.dtype == torch.float32:
             dst.copy_(f)
@@ -258,6 +266,7 @@ class WAAMGrid:
 
     def state_dict(self):
         """Host copies of every field of the state (for checkpoints and tests)."""
+        self.flush_stream()
         names = ["rho", "T", "H", "T_max", "f_l", "phi", "dT_dt", "T_prev", "time_above_800_s",
                  "time_above_1100_s", "time_above_solidus_s", "ux", "uy", "uz", "Fx", "Fy",
                  "Fz", "flags", "f_a", "f_b", "cp_rho_field", "alpha_lu_field",
@@ -273,6 +282,7 @@ class WAAMGrid:
 
     def load_state(self, st):
         """Inverse of state_dict (numpy arrays or tensors)."""
+        self.flush_stream()
         self._forces_dirty = True
         if self._has_lorentz:
             # the potential buffers may now hold anything at fixed cells: the

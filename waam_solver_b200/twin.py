@@ -165,6 +165,9 @@ class WAAMTwin:
         self._warned_zero_wire_feed = False
         self._last_arc_ijk = None
         self.step_mode = step_mode
+        # leave each step's LBM stream running beside the next step's first
+        # stages (results identical; see coupled_step.coupled_step_fused)
+        self.pipeline_stream = True
         # non-droplet fused steps replay a captured CUDA graph of the step
         self.use_cuda_graphs = True
         self._fused_params = None
@@ -253,6 +256,7 @@ class WAAMTwin:
             self.nz_solid = self.resolve_nz_solid(False)
             nz_solid = self.nz_solid
             i0, i1, j0, j1 = self.resolve_plate_ij()
+        g._stream_pending = False          # the state is rebuilt below
         f_a, f_b = g.f_a, g.f_b
         if g.population_storage:   # initialise and stream in float32, then store offsets
             f_a, f_b = torch.empty(f_a.shape, device=g.device), torch.empty(f_b.shape,
@@ -315,6 +319,8 @@ class WAAMTwin:
         if sim_x < 0.62 * (g.nx - 8) * g.dx:
             return
         n_shift = max(8, g.nx // 10)
+        from .coupled_step import flush_stream
+        flush_stream(g)
         kernels.shift_simulation_window_x(
             n_shift, g.f_a, g.f_b, g.T, g.H, g.f_l, g.phi, g.flags, g.T_max, g.T_prev, g.dT_dt,
             g.time_above_800_s, g.time_above_1100_s, g.time_above_solidus_s, g.rho, g.ux, g.uy,
