@@ -518,6 +518,24 @@ typedef struct WaamExportChannel {
  * channel's value at every cell in VTK cell order, index i + nx * (j + ny * k).
  * `channels` is a host array (n_channels <= WAAM_MAX_EXPORT_CHANNELS); `out`
  * is device memory of n_channels * nx * ny * nz * 4 bytes. */
+/* export/vtk_io.py:180-224 (the phi = 0.5 surface).  waam_cell_to_point:
+ * values at the (nx+1)(ny+1)(nz+1) cell corners, each the mean of the cells
+ * sharing it, for up to four fields (c1..c3 may be null; point index
+ * (I * (ny+1) + J) * (nz+1) + K).  waam_isosurface: marching tetrahedra of
+ * iso_points at `iso` (six tetrahedra per cube around its 0-7 diagonal);
+ * per triangle vertex the edge key keys[3t + v] (lower point index times
+ * the point count plus the upper one) and vals[(3t + v) * 6 + ..] = x, y, z
+ * (origin + spacing * lattice position) and a0..a2 interpolated (null: 0);
+ * order[t] = cube * 16 + tetrahedron * 2 + part restores a fixed order;
+ * *count receives the triangle total (rows past `capacity` are not written).
+ * Triangles face from above iso to below. */
+int waam_cell_to_point(const float* c0, const float* c1, const float* c2, const float* c3,
+                       float* p0, float* p1, float* p2, float* p3, int nx, int ny, int nz,
+                       void* stream);
+int waam_isosurface(const float* iso_points, const float* a0, const float* a1, const float* a2,
+                    int nx, int ny, int nz, float iso, float spacing, float ox, float oy,
+                    float oz, int64_t* keys, float* vals, int64_t* order,
+                    unsigned long long* count, int64_t capacity, void* stream);
 int waam_export_pack(const WaamExportChannel* channels, int n_channels, int nx, int ny, int nz,
                      void* out, void* stream);
 

@@ -115,7 +115,9 @@ def test_gpu_research_bundle_and_sequence(tmp_path):
     for s in range(3):
         tw.step(8 * dx, 8 * dx, True)
     paths = tw.export_research_bundle(tmp_path / "b")
-    assert set(paths) == {"volume", "tracers", "telemetry", "meta", "probes"}
+    assert set(paths) == {"volume", "surface", "tracers", "telemetry", "meta", "probes"}
+    surf = E.read_vtk_xml(paths["surface"])
+    assert surf["Points"].shape[0] > 0 and np.all(surf["phi"] == np.float32(0.5))
     meta = json.loads(open(paths["meta"]).read())
     assert meta["grid"]["nx"] == 24 and meta["step"] == 3
     assert meta["telemetry"]["n_droplets_fired"] == 1

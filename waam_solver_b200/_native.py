@@ -115,6 +115,7 @@ _CTYPES = {
     "WaamTelemetry*": C.c_void_p, "const WaamProbeSet*": C.POINTER(WaamProbeSet),
     "const WaamShiftPlane*": C.c_void_p, "const WaamExportChannel*": C.c_void_p,
     "double*": C.c_void_p, "uint8_t*": C.c_void_p, "const uint8_t*": C.c_void_p,
+    "int64_t*": C.c_void_p, "unsigned long long*": C.c_void_p,
 }
 
 

@@ -12,10 +12,14 @@ VTK cell order (x fastest) by one ``waam_export_pack`` launch into a staging
 buffer, and reaches the host in a single copy.  ``read_vtk_xml`` reads the
 files back (tests, post-processing without VTK).
 
-Not built: the phi = 0.5 surface (``export_surface``; the reference contours
-with PyVista's marching cubes) and ``crop_liquid`` thresholding (an
-unstructured grid).  ``export_npz`` writes the raw state instead, for
-Python post-processing.
+The phi = 0.5 surface (``export_surface``) is contoured on the device: cell
+values averaged to the cell corners (as VTK's cell_data_to_point_data) and
+cut by marching tetrahedra (the reference calls PyVista's contour filter, a
+different triangulation of the same isosurface); triangle vertices are merged
+by lattice edge on the host and written as PolyData.  ``crop_liquid`` keeps
+the cells with a liquid fraction of at least 0.05 (the reference's threshold)
+as an UnstructuredGrid of voxels (``.vtu``).  ``export_npz`` writes the raw
+state for Python post-processing.
 """
 from __future__ import annotations
 
@@ -208,6 +212,71 @@ def write_vtp_points(path, points, point_arrays):
     return _write_vtk(path, lines, app)
 
 
+def write_vtp_triangles(path, points, tris, point_arrays):
+    """PolyData of triangles (tris: (T, 3) vertex indices)."""
+    pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+    tris = np.ascontiguousarray(tris, dtype=np.int64).reshape(-1, 3)
+    app = _Appended()
+    lines = ['<?xml version="1.0"?>',
+             '<VTKFile type="PolyData" version="1.0" byte_order="LittleEndian" '
+             'header_type="UInt64">',
+             "  <PolyData>",
+             '    <Piece NumberOfPoints="%d" NumberOfVerts="0" NumberOfLines="0" '
+             'NumberOfStrips="0" NumberOfPolys="%d">' % (pts.shape[0], tris.shape[0]),
+             "      <PointData>"]
+    for name, arr in point_arrays.items():
+        lines.append("        " + _array_tag(name, arr, app))
+    lines += ["      </PointData>", "      <Points>",
+              "        " + _array_tag("Points", pts, app, ncomp=3), "      </Points>",
+              "      <Polys>",
+              "        " + _array_tag("connectivity", tris.reshape(-1), app),
+              "        " + _array_tag("offsets", 3 * np.arange(1, tris.shape[0] + 1,
+                                                           dtype=np.int64), app),
+              "      </Polys>", "    </Piece>", "  </PolyData>"]
+    return _write_vtk(path, lines, app)
+
+
+VTK_VOXEL = 11
+
+
+def write_vtu_voxels(path, nx, ny, nz, spacing, origin, cell_ids, cell_arrays):
+    """UnstructuredGrid of the voxels cell_ids (VTK cell order of an nx*ny*nz
+    ImageData), points shared, arrays given per kept cell."""
+    cell_ids = np.asarray(cell_ids, dtype=np.int64)
+    i = cell_ids % nx
+    j = (cell_ids // nx) % ny
+    k = cell_ids // (nx * ny)
+    # voxel corner order: x fastest, then y, then z
+    di = np.array([0, 1, 0, 1, 0, 1, 0, 1])
+    dj = np.array([0, 0, 1, 1, 0, 0, 1, 1])
+    dk = np.array([0, 0, 0, 0, 1, 1, 1, 1])
+    corner = ((i[:, None] + di) + (nx + 1) * ((j[:, None] + dj) + (ny + 1) * (k[:, None] + dk)))
+    uniq, inv = np.unique(corner.reshape(-1), return_inverse=True)
+    I = uniq % (nx + 1)
+    J = (uniq // (nx + 1)) % (ny + 1)
+    K = uniq // ((nx + 1) * (ny + 1))
+    pts = np.stack([origin[0] + spacing[0] * I, origin[1] + spacing[1] * J,
+                    origin[2] + spacing[2] * K], axis=1).astype(np.float32)
+    nc = cell_ids.shape[0]
+    app = _Appended()
+    lines = ['<?xml version="1.0"?>',
+             '<VTKFile type="UnstructuredGrid" version="1.0" byte_order="LittleEndian" '
+             'header_type="UInt64">',
+             "  <UnstructuredGrid>",
+             '    <Piece NumberOfPoints="%d" NumberOfCells="%d">' % (pts.shape[0], nc),
+             "      <CellData>"]
+    for name, arr in cell_arrays.items():
+        lines.append("        " + _array_tag(name, arr, app))
+    lines += ["      </CellData>", "      <Points>",
+              "        " + _array_tag("Points", pts, app, ncomp=3), "      </Points>",
+              "      <Cells>",
+              "        " + _array_tag("connectivity", inv.astype(np.int64), app),
+              "        " + _array_tag("offsets", 8 * np.arange(1, nc + 1, dtype=np.int64), app),
+              "        " + _array_tag("types", np.full(nc, VTK_VOXEL, dtype=np.uint8), app),
+              "      </Cells>", "    </Piece>", "  </UnstructuredGrid>"]
+    return _write_vtk(path, lines, app)
+
+
 def read_vtk_xml(path):
     """Arrays of a raw-appended VTK XML file written here: {name: array}, plus
     "_attrs" with the dataset element's attributes."""
@@ -227,21 +296,95 @@ def read_vtk_xml(path):
 
 # ---- reference export entry points -----------------------------------------
 def export_volume(twin, path, tiers=(TIER_CORE, TIER_DERIVED), crop_liquid=False):
-    """vtk_io.py:82-166."""
-    if crop_liquid:
-        raise NotImplementedError("crop_liquid (an unstructured threshold grid) is not "
-                                  "supported; export the full volume")
+    """vtk_io.py:82-166.  crop_liquid: only the cells with Liquid_Fraction >= 0.05
+    (vtk_io.py:170-171), written as an UnstructuredGrid (``.vtu``; the
+    reference's threshold output is unstructured too, which its ``.vti`` name
+    does not fit).  Returns None when no cell qualifies."""
     g = twin.grid
     arrays = gather_volume(twin, tiers)
+    spacing = (g.dx * 1000.0,) * 3
+    origin = (twin._window_offset_x_m * 1000.0, 0.0, 0.0)
+    if crop_liquid and "Liquid_Fraction" in arrays:
+        keep = np.nonzero(arrays["Liquid_Fraction"] >= np.float32(0.05))[0]
+        if keep.size == 0:
+            return None
+        out = str(pathlib.Path(vtk_imagedata_path(path)).with_suffix(".vtu"))
+        return write_vtu_voxels(out, g.nx, g.ny, g.nz, spacing, origin, keep,
+                                {k: np.ascontiguousarray(v[keep]) for k, v in arrays.items()})
     out = vtk_imagedata_path(path)
-    write_vti(out, g.nx, g.ny, g.nz, (g.dx * 1000.0,) * 3,
-              (twin._window_offset_x_m * 1000.0, 0.0, 0.0), arrays)
+    write_vti(out, g.nx, g.ny, g.nz, spacing, origin, arrays)
     return out
 
 
+def isosurface(g, iso_cells, attr_cells, iso=0.5, spacing=1.0, origin=(0.0, 0.0, 0.0)):
+    """Marching-tetrahedra isosurface of a cell field at ``iso`` after the
+    cell-to-corner averaging: (points (V, 3), triangles (T, 3), interpolated
+    attributes (V, len(attr_cells))), vertices merged by lattice edge, order
+    fixed.  None when the surface is empty."""
+    nx, ny, nz = g.nx, g.ny, g.nz
+    npts = (nx + 1) * (ny + 1) * (nz + 1)
+    fields = [iso_cells] + list(attr_cells)
+    if len(fields) > 4:
+        raise ValueError("isosurface: at most three attributes")
+    pts = torch.empty((len(fields), npts), dtype=torch.float32, device=g.device)
+    cptr = [t.data_ptr() for t in fields] + [None] * (4 - len(fields))
+    pptr = [pts[m].data_ptr() for m in range(len(fields))] + [None] * (4 - len(fields))
+    st = torch.cuda.current_stream().cuda_stream
+    N.call("waam_cell_to_point", *cptr, *pptr, nx, ny, nz, st)
+    count = torch.zeros(1, dtype=torch.int64, device=g.device)
+    cap = max(1 << 16, 4 * (nx * ny + ny * nz + nx * nz))
+    na = len(attr_cells)
+    aptr = [pts[1 + m].data_ptr() for m in range(na)] + [None] * (3 - na)
+    while True:
+        keys = torch.empty(3 * cap, dtype=torch.int64, device=g.device)
+        vals = torch.empty((3 * cap, 6), dtype=torch.float32, device=g.device)
+        order = torch.empty(cap, dtype=torch.int64, device=g.device)
+        N.call("waam_isosurface", pts[0].data_ptr(), *aptr, nx, ny, nz, float(iso),
+               float(spacing), float(origin[0]), float(origin[1]), float(origin[2]),
+               keys.data_ptr(), vals.data_ptr(), order.data_ptr(), count.data_ptr(), cap, st)
+        n_tri = int(count.item())
+        if n_tri <= cap:
+            break
+        cap = n_tri
+    if n_tri == 0:
+        return None
+    order_h = order[:n_tri].cpu().numpy()
+    perm = np.argsort(order_h, kind="stable")
+    keys_h = keys[:3 * n_tri].cpu().numpy().reshape(n_tri, 3)[perm].reshape(-1)
+    vals_h = vals[:3 * n_tri].cpu().numpy().reshape(n_tri, 3, 6)[perm].reshape(-1, 6)
+    uniq, first, inv = np.unique(keys_h, return_index=True, return_inverse=True)
+    verts = vals_h[first]
+    return verts[:, :3], inv.reshape(n_tri, 3), verts[:, 3:3 + na]
+
+
 def export_surface(twin, path, include_kappa=True):
-    """vtk_io.py:169-224 contours phi = 0.5 with PyVista; not part of this
-    backend (returns None, as the reference does without PyVista)."""
+    """vtk_io.py:180-224: the phi = 0.5 surface (the bead's free surface), or the
+    f_l = 0.5 surface when phi has none, as PolyData with the corner-averaged
+    phi, Liquid_Fraction, Temperature_K (and Curvature_kappa) interpolated to
+    its vertices.  Returns None when neither surface exists."""
+    g = twin.grid
+    if include_kappa:
+        g.ensure_export_buffers()
+        kernels.compute_curvature_field(g.phi, g.flags, g.kappa_field, g.FLAG_GAS, g.nx, g.ny,
+                                        g.nz)
+    names = {"phi": g.phi, "Liquid_Fraction": g.f_l, "Temperature_K": g.T}
+    if include_kappa:
+        names["Curvature_kappa"] = g.kappa_field
+    h = g.dx * 1000.0
+    origin = (twin._window_offset_x_m * 1000.0, 0.0, 0.0)
+    for scalar in ("phi", "Liquid_Fraction"):
+        others = [k for k in names if k != scalar]
+        surf = isosurface(g, names[scalar], [names[k] for k in others], 0.5, h, origin)
+        if surf is None:
+            continue
+        verts, tris, attrs = surf
+        point_arrays = {}
+        for k in names:
+            if k == scalar:
+                point_arrays[k] = np.full(verts.shape[0], 0.5, dtype=np.float32)
+            else:
+                point_arrays[k] = np.ascontiguousarray(attrs[:, others.index(k)])
+        return write_vtp_triangles(path, verts, tris, point_arrays)
     return None
 
 
