@@ -672,6 +672,21 @@ typedef struct WaamStepParams {
      * (it writes flags after the stream). */
     int stream_prev;
     int defer_stream;
+    /* pipelined collision: the collision of step n (with the tracers) needs
+     * the column pass of step n, and step n + 1 needs its velocities only
+     * from its thermal and VOF stages on, while its arc stage reads flags, f_l
+     * and phi and writes H.  defer_collide = 1 (needs defer_stream = 1, no
+     * force buffer, no collision tape, no Lorentz fields): waam_step_main
+     * stops after the column pass and leaves collision, tracers and stream
+     * pending; collide_prev = 1: they are pending from the step before
+     * (welding flag collide_prev_welding) -- waam_step_pre runs the collision
+     * beside the arc stage and the stream after it, and waam_step_main waits
+     * for the collision before its thermal and VOF stages.  A caller that
+     * reads populations, density, velocity, forces or tracers between steps
+     * runs the pending work first with waam_step_finish. */
+    int collide_prev;
+    int collide_prev_welding;
+    int defer_collide;
 } WaamStepParams;
 
 /* Stages of one fused step.  waam_step_pre runs the surface-height query,
@@ -691,6 +706,12 @@ int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace
  * for fields that describe the step after it (buffers swapped): reads f_src,
  * writes f_dst, with the flags of that step. */
 int waam_step_stream(const WaamFields* f, const WaamStepParams* p, void* stream);
+/* The collision, tracers and stream left pending by the previous step
+ * (WaamStepParams.defer_collide; p->collide_prev_welding is that step's
+ * welding flag), for fields that describe the step after it (buffers
+ * swapped, thermal fields flipped). */
+int waam_step_finish(const WaamFields* f, const WaamStepParams* p, void* workspace,
+                     size_t workspace_bytes, void* stream);
 /* waam_step_main that also records events[0..6] (cudaEvent_t handles) on the
  * stream at the stage boundaries: before thermal, after thermal, after VOF
  * advection, after the column pass, after collide, after stream, after the

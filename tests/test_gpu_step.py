@@ -159,20 +159,28 @@ def test_pipelined_stream_matches_in_order_stream(lorentz):
     Lorentz split step; the state read-out runs the pending stream."""
     states = []
     more = dict(enable_lorentz=True, welding_current_A=180.0) if lorentz else {}
-    for pipelined in (False, True):
+    for mode in ("in_order", "stream", "stream_collide"):
         tw, ot, dx = _config_twins("c2", 40, 24, 24, **more)
-        tw.pipeline_stream = pipelined
+        tw.pipeline_stream = mode != "in_order"
+        tw.pipeline_collide = mode == "stream_collide"
         tw._last_droplet_time = -1.0
         for s in range(24):
-            tw.step(0.3 * 40 * dx + s * 1e-6, 12 * dx, True)
-        if pipelined:
-            assert tw.grid._stream_pending
+            # a non-welding stretch switches the arc off and on
+            tw.step(0.3 * 40 * dx + s * 1e-6, 12 * dx, not 10 <= s < 13)
+        g = tw.grid
+        if mode != "in_order":
+            assert g._stream_pending
+        if mode == "stream_collide" and not lorentz:
+            assert g._collide_pending
+            u = g.ux.clone()              # reading a collision output runs the pending work
+            assert not g._collide_pending and not g._stream_pending
         torch.cuda.synchronize()
-        states.append(tw.grid.state_dict())
+        states.append(g.state_dict())
         assert tw._n_droplets_fired >= 1
-    for k, v in states[0].items():
-        if isinstance(v, np.ndarray):
-            assert np.array_equal(v, states[1][k]), k
+    for other in states[1:]:
+        for k, v in states[0].items():
+            if isinstance(v, np.ndarray):
+                assert np.array_equal(v, other[k]), k
 
 
 LORENTZ_FIELDS = ("phi_elec", "Jx", "Jy", "Jz", "Bx", "By", "Bz", "elec_rad_bins")

@@ -65,6 +65,7 @@ class _Checkpoint:
     def restore(self, tw):
         g = tw.grid
         g._stream_pending = False       # the checkpoint holds a streamed state
+        g._collide_pending = False
         for k in _FIELDS:
             getattr(g, k).copy_(self.t[k])
         for dst, src in zip(g._H, self.t["_H"]):
@@ -385,6 +386,8 @@ def _taped_step(tw, x, y, tape, slot):
     g.flush_stream()
     p.stream_prev = 0
     p.defer_stream = 0
+    p.collide_prev = 0
+    p.defer_collide = 0
     arc_i, arc_j = sim_x / g.dx, sim_y / g.dx
     p.arc_i, p.arc_j = arc_i, arc_j
     p.welding = 1

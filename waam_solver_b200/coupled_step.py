@@ -21,6 +21,7 @@ import torch
 from . import _native, kernels
 from ._native import WaamError
 from .physics import deposition, forces, free_surface, lbm, phase_change, thermal, weld_forces
+from .grid import raw_field
 from .physics.electrical_stickout import droplet_entry_temperature_K, update_ctwd
 
 T_800 = 800.0 + 273.15
@@ -281,17 +282,20 @@ def coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=Non
 def _fields(g):
     f = _native.WaamFields()
     g.ensure_vof_buffers()
-    for name, t in (("f_src", g.f_src), ("f_dst", g.f_dst), ("rho", g.rho), ("ux", g.ux),
-                    ("uy", g.uy), ("uz", g.uz), ("T", g.T), ("T_next", g.T_next), ("H", g.H),
+    r = lambda name: raw_field(g, name)  # noqa: E731  (no flush of pending work)
+    for name, t in (("f_src", g.f_src), ("f_dst", g.f_dst), ("rho", r("rho")), ("ux", r("ux")),
+                    ("uy", r("uy")), ("uz", r("uz")), ("T", g.T), ("T_next", g.T_next), ("H", g.H),
                     ("H_next", g.H_next), ("f_l", g.f_l), ("phi", g.phi),
                     ("phi_tmp", g.phi_tmp), ("flags", g.flags), ("T_max", g.T_max),
                     ("T_prev", g.T_prev), ("dT_dt", g.dT_dt), ("t800", g.time_above_800_s),
                     ("t1100", g.time_above_1100_s), ("tsol", g.time_above_solidus_s),
-                    ("Fx", g.Fx), ("Fy", g.Fy), ("Fz", g.Fz), ("step_scalars", g.step_scalars)):
+                    ("Fx", r("Fx")), ("Fy", r("Fy")), ("Fz", r("Fz")),
+                    ("step_scalars", g.step_scalars)):
         setattr(f, name, t.data_ptr())
     f.nx, f.ny, f.nz = g.nx, g.ny, g.nz
     if getattr(g, "_tracers_live", False):   # advected once the first droplet spawned some
-        f.tracer_pos, f.tracer_active = g.porosity_pos.data_ptr(), g.porosity_active.data_ptr()
+        f.tracer_pos = r("porosity_pos").data_ptr()
+        f.tracer_active = r("porosity_active").data_ptr()
         f.max_tracers = g.max_tracers
     f.cp_rho_f, f.alpha_f = g.cp_rho_field.data_ptr(), g.alpha_lu_field.data_ptr()
     f.dgamma_f, f.tau_f = g.dgamma_lu_field.data_ptr(), g.tau_field.data_ptr()
@@ -429,15 +433,23 @@ def _fields_cached(g, lorentz=False):
 
 
 def flush_stream(g):
-    """Run the stream a pipelined step left pending (WaamStepParams.defer_stream),
-    so that the population buffers hold the step's result.  A no-op otherwise."""
-    if not getattr(g, "_stream_pending", False):
+    """Run the work a pipelined step left pending (WaamStepParams.defer_stream /
+    defer_collide), so that populations, density, velocity, forces and tracers
+    hold the step's result.  A no-op otherwise."""
+    collide = g.__dict__.get("_collide_pending", False)
+    if not (collide or g.__dict__.get("_stream_pending", False)):
         return
     g._stream_pending = False
+    g._collide_pending = False
+    st = torch.cuda.current_stream().cuda_stream
+    if collide:
+        p = g._pending_params
+        _native.call("waam_step_finish", ctypes.byref(_fields_cached(g)), ctypes.byref(p),
+                     g.workspace.data_ptr(), g.workspace.numel(), st)
+        return
     p = _native.WaamStepParams()
     p.f_storage = g.population_storage
-    _native.call("waam_step_stream", ctypes.byref(_fields_cached(g)), ctypes.byref(p),
-                 torch.cuda.current_stream().cuda_stream)
+    _native.call("waam_step_stream", ctypes.byref(_fields_cached(g)), ctypes.byref(p), st)
 
 
 def _droplet_due(twin, g, is_welding):
@@ -516,15 +528,24 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     # Pipelined stream: this step's stream is left to run beside the next
     # step's first stages.  Droplet steps (the deposition writes populations),
     # instrumented steps and the remelt / solidify tail run it in order.
+    # Pipelined collision: a step that may leave its stream pending also
+    # leaves its collision and tracers pending, to run beside the next step's
+    # arc stage -- except droplet steps (force buffer) and Lorentz steps.
     if due or events is not None:
         flush_stream(g)
-    p.stream_prev = 1 if getattr(g, "_stream_pending", False) else 0
+    collide_prev = bool(g.__dict__.get("_collide_pending", False))
+    p.collide_prev = 1 if collide_prev else 0
+    p.collide_prev_welding = g.__dict__.get("_pending_welding", 0) if collide_prev else 0
+    p.stream_prev = 1 if (collide_prev or g.__dict__.get("_stream_pending", False)) else 0
     p.defer_stream = 1 if (getattr(twin, "pipeline_stream", True) and events is None and
                            not (twin.enable_bead_freeze or twin.enable_substrate_growth)) else 0
+    p.defer_collide = 1 if (p.defer_stream and not due and not lorentz and
+                            getattr(twin, "pipeline_collide", True)) else 0
     done = False
     if not due and not lorentz and events is None and getattr(twin, "use_cuda_graphs", True):
         key = (g._read_buf is g.f_a, g._cur, p.welding, p.clear_forces, p.stream_prev,
-               p.defer_stream, g._flags_copy_i,
+               p.defer_stream, p.collide_prev, p.collide_prev_welding, p.defer_collide,
+               g._flags_copy_i,
                (dx_, dy_, dz_) if twin.enable_bead_freeze else None)
         done = _run_graph(twin, g, f, p, ws, key)
     if not done:
@@ -568,6 +589,12 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     # active cells until the next step
     g._forces_dirty = bool(p.forces_from_buffer) or lorentz
     g._stream_pending = bool(p.defer_stream)
+    g._collide_pending = bool(p.defer_collide)
+    if p.defer_collide:
+        q = _native.WaamStepParams.from_buffer_copy(p)
+        q.collide_prev, q.collide_prev_welding = 1, p.welding
+        g._pending_params = q
+        g._pending_welding = p.welding
     g._flags_copy_i = 1 - g._flags_copy_i    # this step's copy is read by the next step
     g.flip_thermal()
     g.swap_buffers()

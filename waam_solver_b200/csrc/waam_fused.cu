@@ -614,8 +614,14 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
                                                 int* __restrict__ active_list,
                                                 unsigned* __restrict__ active_count,
                                                 int32_t* __restrict__ flags_copy,
+                                                float* __restrict__ scalars,
                                                 ColumnArgs a) {
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        scalars[kScalarCollideArcK] = scalars[kScalarArcK];
+        scalars[kScalarCollideArcI] = scalars[kScalarArcI];
+        scalars[kScalarCollideArcJ] = scalars[kScalarArcJ];
+    }
     if (warp >= d.nx * d.ny) return;
     const int lane = threadIdx.x & 31;
     int i = warp / d.ny, j = warp % d.ny;
@@ -730,9 +736,9 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
     if (a.tape_f != nullptr && blockIdx.x == 0 && threadIdx.x == 0)
         *a.tape_count = tape ? (int32_t)cnt : -1;
     ForceParams P = a.P;
-    P.arc_k = scalars[kScalarArcK];
-    P.arc_i = scalars[kScalarArcI];
-    P.arc_j = scalars[kScalarArcJ];
+    P.arc_k = scalars[kScalarCollideArcK];
+    P.arc_i = scalars[kScalarCollideArcI];
+    P.arc_j = scalars[kScalarCollideArcJ];
     const bool lorentz = a.J[0] != nullptr;
     const float F_cap = P.F_cap;
     if (lorentz) P.F_cap = 0.0f;   // clamped below, after J x B
@@ -911,7 +917,7 @@ struct AuxStream {
     cudaStream_t hi = nullptr;
     cudaStream_t s2 = nullptr;
     cudaStream_t s3 = nullptr;
-    cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev[10] = {};
 };
 
 static int aux_stream(AuxStream** out) {
@@ -932,7 +938,7 @@ static int aux_stream(AuxStream** out) {
             e = cudaStreamCreateWithPriority(&a.s2, cudaStreamNonBlocking, greatest);
         if (e == cudaSuccess)
             e = cudaStreamCreateWithPriority(&a.s3, cudaStreamNonBlocking, least);
-        for (int q = 0; q < 8 && e == cudaSuccess; ++q)
+        for (int q = 0; q < 10 && e == cudaSuccess; ++q)
             e = cudaEventCreateWithFlags(&a.ev[q], cudaEventDisableTiming);
         if (e != cudaSuccess) {
             a.s2 = nullptr;
@@ -988,14 +994,20 @@ static VarPhase var_phase(const WaamStepParams* p) {
 
 }  // namespace waam
 
+namespace waam {
+static int launch_collide_tracers(const WaamFields* f, const WaamStepParams* p, const Dims& d,
+                                  Workspace ws, const void* pop_in, void* pop_out,
+                                  const float* T_cur, int welding, cudaStream_t s);
+}  // namespace waam
+
 extern "C" {
 
 int waam_step_launch_count(const WaamStepParams* p, int stage) {
     if (!p) return 0;
     // the pending stream of the previous step is launched by waam_step_pre
-    if (stage == 0) return (p->welding ? 2 : 1) + (p->stream_prev ? 1 : 0);
-    // thermal, [vof], column, collide, [stream] (tracers counted by the caller)
-    int n = 1 + (p->vof ? 1 : 0) + 1 + 1 + (p->defer_stream ? 0 : 1);
+    if (stage == 0) return (p->welding ? 2 : 1) + (p->stream_prev ? 1 : 0) + (p->collide_prev ? 1 : 0);
+    // thermal, [vof], column, [collide], [stream] (tracers counted by the caller)
+    int n = 1 + (p->vof ? 1 : 0) + 1 + (p->defer_collide ? 0 : 1) + (p->defer_stream ? 0 : 1);
     if (p->substrate_growth || p->bead_freeze) n += 1;
     return n;
 }
@@ -1011,14 +1023,28 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     WorkStream W(STREAM(stream), true, 4);
     if (W.err) return W.err;
     const cudaStream_t s = W.s;
+    if (p->collide_prev) {
+        // the previous step's collision and tracers, beside this step's arc
+        // stage (waam_step_main waits for them before its thermal stage)
+        AuxStream* aux = nullptr;
+        int ea = aux_stream(&aux);
+        if (ea) return ea;
+        cudaEventRecord(aux->ev[8], s);
+        cudaStreamWaitEvent(aux->s2, aux->ev[8], 0);
+        ea = launch_collide_tracers(f, p, d, ws, f->f_dst, f->f_src, f->T, p->collide_prev_welding,
+                                    aux->s2);
+        if (ea) return ea;
+        cudaEventRecord(aux->ev[9], aux->s2);
+    }
     if (p->stream_prev) {
         // the previous step's stream, beside this step's stages up to the
-        // column pass (waam_step_main joins it there)
+        // column pass (waam_step_main joins it there); after its collision
         AuxStream* aux = nullptr;
         int ea = aux_stream(&aux);
         if (ea) return ea;
         cudaEventRecord(aux->ev[2], s);
         cudaStreamWaitEvent(aux->s3, aux->ev[2], 0);
+        if (p->collide_prev) cudaStreamWaitEvent(aux->s3, aux->ev[9], 0);
         // the flags it streams with: the previous step's copy if there is one
         // (then the column pass may rewrite the flags meanwhile)
         const int32_t* sf = f->flags_copy_r ? f->flags_copy_r : f->flags;
@@ -1033,17 +1059,18 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     }
     ArcParams a = arc_params(p);
     float Qe_dt = p->Q_w * p->eta * p->dt;
+    float* shape = reinterpret_cast<float*>(static_cast<char*>(workspace) + ws_shape_offset(d.n()));
     const int tiles = (int)tile_grid(d).x * (int)tile_grid(d).y * d.nx;
     const int blocks = tiles < kTileRedBlocks ? tiles : kTileRedBlocks;
     k_arc_norm_tiles<<<blocks, tile_block(), 0, s>>>(
         d, f->flags, f->f_l, f->phi, p->nz_solid, a, f->step_scalars, p->arc_k_offset, Qe_dt,
-        p->dx3, ws, ws.field);
+        p->dx3, ws, shape);
     int e = check_launch("k_arc_norm_tiles");
     if (e) return e;
     PhaseParams ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
     k_arc_inject_tiles<<<tile_grid(d), tile_block(), 0, s>>>(
         d, f->H, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, p->cap_enabled, ph,
-        p->use_tables ? f->cp_rho_f : nullptr, var_phase(p), ws.field);
+        p->use_tables ? f->cp_rho_f : nullptr, var_phase(p), shape);
     return check_launch("k_arc_inject_tiles");
 }
 
@@ -1055,6 +1082,22 @@ int waam_step_stream(const WaamFields* f, const WaamStepParams* p, void* stream)
     return launch_stream_stored(d, f->f_src, f->f_dst, f->flags, p->f_storage, STREAM(stream));
 }
 
+int waam_step_finish(const WaamFields* f, const WaamStepParams* p, void* workspace,
+                     size_t workspace_bytes, void* stream) {
+    if (!fields_ok(f) || !p) return fail(WAAM_ERR_INVALID, "step_finish: bad fields or params");
+    if (p->f_storage < kStoreF32 || p->f_storage > kStoreBF16)
+        return fail(WAAM_ERR_INVALID, "step_finish: bad f_storage");
+    Dims d{f->nx, f->ny, f->nz};
+    if (!workspace_ok(workspace, workspace_bytes, d.n()))
+        return fail(WAAM_ERR_INVALID, "step_finish: workspace too small or misaligned");
+    Workspace ws = Workspace::at(workspace);
+    cudaStream_t s = STREAM(stream);
+    int e = launch_collide_tracers(f, p, d, ws, f->f_dst, f->f_src, f->T, p->collide_prev_welding,
+                                   s);
+    if (e) return e;
+    return launch_stream_stored(d, f->f_src, f->f_dst, f->flags, p->f_storage, s);
+}
+
 int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace,
                    size_t workspace_bytes, void* stream) {
     return waam_step_main_events(f, p, workspace, workspace_bytes, nullptr, 0, stream);
@@ -1063,6 +1106,94 @@ int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace
 }  // extern "C"
 
 namespace waam {
+// Collision (forces in registers, Lorentz J x B when the fields carry J and B),
+// J x B on solid cells without VOF, then the tracers, over the active list of
+// the workspace: populations pop_in -> pop_out, temperature T_cur.
+static int launch_collide_tracers(const WaamFields* f, const WaamStepParams* p, const Dims& d,
+                                  Workspace ws, const void* pop_in, void* pop_out,
+                                  const float* T_cur, int welding, cudaStream_t s) {
+    unsigned* active_count = ws.counter + kActiveShardSlot;
+    int* active_list = reinterpret_cast<int*>(ws.field);
+    const int64_t shard_cap =
+        ((int64_t)d.nx * d.ny + kActiveShards - 1) / kActiveShards * (int64_t)d.nz;
+    int e = WAAM_OK;
+    CollideArgs cl;
+    ForceParams& P = cl.P;
+    P.csf = p->csf;
+    P.wetting = p->wetting;
+    P.welding = welding;
+    P.hydro = p->hydro;
+    P.gamma_lu = p->gamma_lu;
+    P.cos_t = (float)cos((double)p->theta);
+    P.sin_t = (float)sin((double)p->theta);
+    P.dgamma = p->dgamma_lu;
+    P.arc_i = P.arc_j = P.arc_k = 0.0f;  // from the device scalars
+    P.p_inv2s2 = 1.0f / (2.0f * p->p_sigma * p->p_sigma + 1e-6f);
+    float Fphys = p->pressure / (p->rho_phys * p->dx);
+    P.p_Flu = Fphys * (p->dt * p->dt) / p->dx;
+    P.g_lu = p->g_lu;
+    P.beta = p->beta;
+    P.T_ref = p->T_ref;
+    P.rho_ref = 1.0f;
+    P.F_cap = p->F_cap;
+    cl.kind = p->use_tables && p->variable_tau ? 2 : p->collision;
+    cl.dgamma_f = p->use_tables ? f->dgamma_f : nullptr;
+    cl.tau_f = f->tau_f;
+    cl.tape_f = f->tape_f;
+    cl.tape_cells = f->tape_cells;
+    cl.tape_count = f->tape_count;
+    cl.tape_cap = f->tape_cap;
+    if (f->tape_f && (!f->tape_cells || !f->tape_count || f->tape_cap <= 0))
+        return fail(WAAM_ERR_INVALID, "collide: incomplete collision tape");
+    cl.from_buffer = p->forces_from_buffer;
+    cl.omega = p->omega;
+    cl.omega_b = p->omega_b;
+    cl.C_darcy = p->C_darcy;
+    cl.u_cap = p->u_cap;
+    const bool lorentz = f->lorentz_J[0] != nullptr;
+    for (int q = 0; q < 3; ++q) {
+        cl.J[q] = f->lorentz_J[q];
+        cl.B[q] = f->lorentz_B[q];
+        if (lorentz && (!f->lorentz_J[q] || !f->lorentz_B[q]))
+            return fail(WAAM_ERR_INVALID, "collide: incomplete Lorentz fields");
+    }
+    cl.lz_dt = p->dt;
+    cl.lz_dx = p->dx;
+    cl.lz_rho = p->rho_phys;
+#define WAAM_COLLIDE(S)                                                                    \
+    k_collide_list<S><<<kListBlocks, kListThreads, 0, s>>>(                                \
+        d, static_cast<const Pop<S>::T*>(pop_in), static_cast<Pop<S>::T*>(pop_out),              \
+        f->rho, f->ux, f->uy, f->uz, f->Fx, f->Fy, f->Fz, f->phi, T_cur, f->f_l, f->flags,        \
+        f->step_scalars, active_list, active_count, (int)shard_cap, cl)
+    if (p->f_storage == kStoreF16)
+        WAAM_COLLIDE(kStoreF16);
+    else if (p->f_storage == kStoreBF16)
+        WAAM_COLLIDE(kStoreBF16);
+    else
+        WAAM_COLLIDE(kStoreF32);
+#undef WAAM_COLLIDE
+    e = check_launch("k_collide_list");
+    if (e) return e;
+    // With VOF the column pass has set f_l = 0 on every SOLID cell, below the
+    // 0.05 the force needs: the pass is only run without VOF.
+    if (lorentz && !p->vof) {
+        k_lorentz_solid<<<elem_blocks(d.n()), kThreads, 0, s>>>(
+            d.n(), f->flags, f->f_l, f->Fx, f->Fy, f->Fz, f->lorentz_J[0],
+            f->lorentz_J[1], f->lorentz_J[2], f->lorentz_B[0], f->lorentz_B[1], f->lorentz_B[2],
+            p->dt, p->dx, p->rho_phys);
+        e = check_launch("k_lorentz_solid");
+        if (e) return e;
+    }
+    // tracers read u, f_l and flags only (they follow the stream in the
+    // reference order; nothing of theirs depends on it)
+    if (f->tracer_pos && f->tracer_active && f->max_tracers > 0) {
+        e = launch_advect_tracers(d, f->tracer_pos, f->tracer_active, f->ux, f->uy, f->uz,
+                                  f->f_l, f->flags, p->dx, f->max_tracers, s);
+        if (e) return e;
+    }
+    return WAAM_OK;
+}
+
 // stages: bit 0 thermal .. column, bit 1 collide .. tail
 static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* workspace,
                           size_t workspace_bytes, void* const* events, int n_events,
@@ -1075,6 +1206,11 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         return fail(WAAM_ERR_INVALID, "step_main: need 7 events");
     if (p->defer_stream && (p->substrate_growth || p->bead_freeze))
         return fail(WAAM_ERR_INVALID, "step_main: defer_stream needs the remelt/solidify tail off");
+    if (p->defer_collide && (!p->defer_stream || p->forces_from_buffer || f->tape_f ||
+                             f->lorentz_J[0]))
+        return fail(WAAM_ERR_INVALID,
+                    "step_main: defer_collide needs defer_stream and no force buffer, tape or "
+                    "Lorentz fields");
     for (int q = 0; events && q < kMainEvents; ++q)
         if (!events[q]) return fail(WAAM_ERR_INVALID, "step_main: null event handle");
     auto mark = [&](int i) {
@@ -1098,6 +1234,14 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
     int e = WAAM_OK;
 
     if (stages & 1) {
+        if (p->collide_prev) {
+            // the previous step's collision (started by waam_step_pre) writes
+            // the velocities the thermal and VOF stages read
+            AuxStream* sa = nullptr;
+            int ea = aux_stream(&sa);
+            if (ea) return ea;
+            cudaStreamWaitEvent(s, sa->ev[9], 0);
+        }
         ThermalArgs ta;
         ta.ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
         ta.cpa = p->cp_rho * p->alpha_lu;
@@ -1195,7 +1339,8 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         ca.shard_cap = (int)shard_cap;
         k_column<<<col_blocks, kThreads, 0, s>>>(d, f->phi_tmp, f->phi, f->flags, f->f_l, f->T_next,
                                                  f->t800, f->t1100, f->tsol, f->Fx, f->Fy, f->Fz,
-                                                 active_list, active_count, f->flags_copy_w, ca);
+                                                 active_list, active_count, f->flags_copy_w,
+                                                 f->step_scalars, ca);
         e = check_launch("k_column");
         if (e) return e;
         mark(3);
@@ -1210,85 +1355,14 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
             if (ea) return ea;
             cudaStreamWaitEvent(s, sa->ev[3], 0);
         }
-        CollideArgs cl;
-        ForceParams& P = cl.P;
-        P.csf = p->csf;
-        P.wetting = p->wetting;
-        P.welding = p->welding;
-        P.hydro = p->hydro;
-        P.gamma_lu = p->gamma_lu;
-        P.cos_t = (float)cos((double)p->theta);
-        P.sin_t = (float)sin((double)p->theta);
-        P.dgamma = p->dgamma_lu;
-        P.arc_i = P.arc_j = P.arc_k = 0.0f;  // from the device scalars
-        P.p_inv2s2 = 1.0f / (2.0f * p->p_sigma * p->p_sigma + 1e-6f);
-        float Fphys = p->pressure / (p->rho_phys * p->dx);
-        P.p_Flu = Fphys * (p->dt * p->dt) / p->dx;
-        P.g_lu = p->g_lu;
-        P.beta = p->beta;
-        P.T_ref = p->T_ref;
-        P.rho_ref = 1.0f;
-        P.F_cap = p->F_cap;
-        cl.kind = p->use_tables && p->variable_tau ? 2 : p->collision;
-        cl.dgamma_f = p->use_tables ? f->dgamma_f : nullptr;
-        cl.tau_f = f->tau_f;
-        cl.tape_f = f->tape_f;
-        cl.tape_cells = f->tape_cells;
-        cl.tape_count = f->tape_count;
-        cl.tape_cap = f->tape_cap;
-        if (f->tape_f && (!f->tape_cells || !f->tape_count || f->tape_cap <= 0))
-            return fail(WAAM_ERR_INVALID, "step_main: incomplete collision tape");
-        cl.from_buffer = p->forces_from_buffer;
-        cl.omega = p->omega;
-        cl.omega_b = p->omega_b;
-        cl.C_darcy = p->C_darcy;
-        cl.u_cap = p->u_cap;
-        const bool lorentz = f->lorentz_J[0] != nullptr;
-        for (int q = 0; q < 3; ++q) {
-            cl.J[q] = f->lorentz_J[q];
-            cl.B[q] = f->lorentz_B[q];
-            if (lorentz && (!f->lorentz_J[q] || !f->lorentz_B[q]))
-                return fail(WAAM_ERR_INVALID, "step_main: incomplete Lorentz fields");
-        }
-        cl.lz_dt = p->dt;
-        cl.lz_dx = p->dx;
-        cl.lz_rho = p->rho_phys;
-    #define WAAM_COLLIDE(S)                                                                    \
-        k_collide_list<S><<<kListBlocks, kListThreads, 0, s>>>(                                \
-            d, static_cast<const Pop<S>::T*>(f->f_src), static_cast<Pop<S>::T*>(f->f_dst),           \
-            f->rho, f->ux, f->uy, f->uz, f->Fx, f->Fy, f->Fz, f->phi, f->T_next, f->f_l, f->flags,    \
-            f->step_scalars, active_list, active_count, (int)shard_cap, cl)
-        if (p->f_storage == kStoreF16)
-            WAAM_COLLIDE(kStoreF16);
-        else if (p->f_storage == kStoreBF16)
-            WAAM_COLLIDE(kStoreBF16);
-        else
-            WAAM_COLLIDE(kStoreF32);
-    #undef WAAM_COLLIDE
-        e = check_launch("k_collide_list");
-        if (e) return e;
-        // With VOF the column pass has set f_l = 0 on every SOLID cell, below the
-        // 0.05 the force needs: the pass is only run without VOF.
-        if (lorentz && !p->vof) {
-            k_lorentz_solid<<<elem_blocks(d.n()), kThreads, 0, s>>>(
-                d.n(), f->flags, f->f_l, f->Fx, f->Fy, f->Fz, f->lorentz_J[0],
-                f->lorentz_J[1], f->lorentz_J[2], f->lorentz_B[0], f->lorentz_B[1], f->lorentz_B[2],
-                p->dt, p->dx, p->rho_phys);
-            e = check_launch("k_lorentz_solid");
+        if (!p->defer_collide) {
+            e = launch_collide_tracers(f, p, d, ws, f->f_src, f->f_dst, f->T_next, p->welding, s);
             if (e) return e;
-        }
-        mark(4);
-
-        if (!p->defer_stream) {
-            e = launch_stream_stored(d, f->f_dst, f->f_src, f->flags, p->f_storage, s);
-            if (e) return e;
-        }
-        // tracers read u, f_l and flags only (they follow the stream in the
-        // reference order; nothing of theirs depends on it)
-        if (f->tracer_pos && f->tracer_active && f->max_tracers > 0) {
-            e = launch_advect_tracers(d, f->tracer_pos, f->tracer_active, f->ux, f->uy, f->uz,
-                                      f->f_l, f->flags, p->dx, f->max_tracers, s);
-            if (e) return e;
+            mark(4);
+            if (!p->defer_stream) {
+                e = launch_stream_stored(d, f->f_dst, f->f_src, f->flags, p->f_storage, s);
+                if (e) return e;
+            }
         }
         mark(5);
 

@@ -18,6 +18,7 @@ constexpr int kRedBlocks = 592;           // fixed so reduction order never depe
 //   [1024, 132096)      double partial sums, one per reduction block (<= 16384)
 //   [132096, ...)       one field-sized scratch (n + kFieldSlack elements): a float
 //                       snapshot (operator API) or the int32 active-cell list (fused step)
+//   [ws_shape_offset(n), +4n)  the fused step's arc shape factors
 constexpr size_t kWsScalarsOffset = 512;
 constexpr size_t kWsPartialsOffset = 1024;
 constexpr int kWsMaxPartials = 16384;
@@ -25,9 +26,17 @@ constexpr size_t kWsFieldOffset = kWsPartialsOffset + kWsMaxPartials * sizeof(do
 constexpr int64_t kFieldSlack = 65536;
 constexpr int kActiveShards = 64;     // power of two
 
-inline size_t ws_total_bytes(int64_t n) {
+inline size_t ws_field_bytes(int64_t n) {
     size_t field = (size_t)((n > 0 ? n : 0) + kFieldSlack) * sizeof(float);
-    return kWsFieldOffset + ((field + 255) & ~(size_t)255);
+    return (field + 255) & ~(size_t)255;
+}
+// a second field-sized region after the first: the arc pass's per-cell shape
+// factors (so they never share memory with the active-cell list a pending
+// collision still reads)
+inline size_t ws_shape_offset(int64_t n) { return kWsFieldOffset + ws_field_bytes(n); }
+inline size_t ws_total_bytes(int64_t n) {
+    size_t shape = ((size_t)(n > 0 ? n : 0) * sizeof(float) + 255) & ~(size_t)255;
+    return ws_shape_offset(n) + shape;
 }
 constexpr int kActiveShardSlot = 64;  // first shard counter in the counter block
 
@@ -57,6 +66,12 @@ constexpr int kScalarWsum = 1;   // arc weight sum
 constexpr int kScalarEpw = 2;    // energy per unit weight
 constexpr int kScalarArcI = 4;   // torch x in cells (copied in by the host every step)
 constexpr int kScalarArcJ = 5;   // torch y in cells
+// the arc position of the step as its collision sees it, copied by the column
+// pass: a collision left pending for the next step's first stages must not
+// see that step's position (slots 0, 4, 5 are rewritten by then)
+constexpr int kScalarCollideArcK = 8;
+constexpr int kScalarCollideArcI = 9;
+constexpr int kScalarCollideArcJ = 10;
 
 struct Workspace {
     unsigned* counter;        // counter[0]: reduction, counter[kActiveCountSlot]: active cells

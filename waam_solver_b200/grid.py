@@ -230,8 +230,9 @@ class WAAMGrid:
         return w
 
     def flush_stream(self):
-        """Run the stream a pipelined step left pending (see coupled_step)."""
-        if getattr(self, "_stream_pending", False):
+        """Run the work a pipelined step left pending -- its stream, or its
+        collision, tracers and stream (see coupled_step)."""
+        if getattr(self, "_stream_pending", False) or getattr(self, "_collide_pending", False):
             from .coupled_step import flush_stream
             flush_stream(self)
 
@@ -302,6 +303,35 @@ class WAAMGrid:
                 self.store_populations(dst, v)
                 continue
             dst.copy_(torch.as_tensor(v).to(dst.dtype).reshape(dst.shape))
+
+
+# The fields a pending collision (WaamStepParams.defer_collide) still has to
+# write: reading one through the grid runs the pending work first.
+_COLLIDE_OUTPUTS = ("rho", "ux", "uy", "uz", "Fx", "Fy", "Fz", "porosity_pos",
+                    "porosity_active")
+
+
+def _collide_output(name):
+    key = "_pf_" + name
+
+    def get(self):
+        if self.__dict__.get("_collide_pending", False):
+            self.flush_stream()
+        return self.__dict__[key]
+
+    def put(self, value):
+        self.__dict__[key] = value
+
+    return property(get, put, doc="%s (runs a pending collision first)" % name)
+
+
+for _name in _COLLIDE_OUTPUTS:
+    setattr(WAAMGrid, _name, _collide_output(_name))
+
+
+def raw_field(g, name):
+    """A collision output without running pending work (the step's own use)."""
+    return g.__dict__["_pf_" + name] if name in _COLLIDE_OUTPUTS else getattr(g, name)
 
 
 def cells_of(mm, dx):

@@ -168,6 +168,8 @@ class WAAMTwin:
         # leave each step's LBM stream running beside the next step's first
         # stages (results identical; see coupled_step.coupled_step_fused)
         self.pipeline_stream = True
+        # and its collision and tracers beside the next step's arc stage
+        self.pipeline_collide = True
         # non-droplet fused steps replay a captured CUDA graph of the step
         self.use_cuda_graphs = True
         self._fused_params = None
@@ -257,6 +259,7 @@ class WAAMTwin:
             nz_solid = self.nz_solid
             i0, i1, j0, j1 = self.resolve_plate_ij()
         g._stream_pending = False          # the state is rebuilt below
+        g._collide_pending = False
         f_a, f_b = g.f_a, g.f_b
         if g.population_storage:   # initialise and stream in float32, then store offsets
             f_a, f_b = torch.empty(f_a.shape, device=g.device), torch.empty(f_b.shape,
