@@ -127,6 +127,21 @@ int waam_compute_marangoni_force(const float* T, const float* phi, const float* 
                                  float* Fy, float* Fz, const int32_t* flags, int nx, int ny,
                                  int nz, float dgamma, void* stream);
 /* kernels.py:3038-3083 apply_arc_pressure (physics/forces.py:110) */
+/* kernels.py:1094-1141 apply_gas_shear_stress (its arc_k argument is unused) */
+int waam_apply_gas_shear_stress(float* Fx, float* Fy, const float* phi, const int32_t* flags,
+                                int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                                float tau_peak_pa, float dt, float dx, float rho_ref,
+                                void* stream);
+/* kernels.py:995-1028 apply_vapor_recoil (T-ratio form) */
+int waam_apply_vapor_recoil(float* Fz, const float* T, const float* phi, const int32_t* flags,
+                            int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                            float recoil_pa, float T_ref, float dt, float dx, float rho_ref,
+                            void* stream);
+/* kernels.py:1046-1091 apply_vapor_recoil_clausius_clapeyron */
+int waam_apply_vapor_recoil_cc(float* Fz, const float* T, const float* phi, const int32_t* flags,
+                               int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                               float P_ref, float T_boil, float L_vap, float R_spec, float C_acc,
+                               float dt, float dx, float rho_ref, void* stream);
 int waam_apply_arc_pressure(float* Fz, const int32_t* flags, const float* phi, int nx, int ny,
                             int nz, float arc_i, float arc_j, float arc_k, float sigma,
                             float pressure, float dt, float dx, float rho_ref, void* stream);
@@ -687,6 +702,15 @@ typedef struct WaamStepParams {
     int collide_prev;
     int collide_prev_welding;
     int defer_collide;
+    /* shielding-gas shear and vapour recoil in the force assembly while
+     * welding (physics/weld_forces.py:137-193): gas_shear on/off with the
+     * peak shear stress; recoil 0 off, 1 T-ratio form (recoil_pa, recoil_T_ref),
+     * 2 Clausius-Clapeyron form (P_ref, T_boil, L_vap, R_spec, C_acc); both
+     * over the Gaussian of width weld_sigma (cells) around the torch */
+    int gas_shear;
+    float gs_tau_pa;
+    int recoil;
+    float recoil_pa, recoil_T_ref, P_ref, T_boil, L_vap, R_spec, C_acc, weld_sigma;
 } WaamStepParams;
 
 /* Stages of one fused step.  waam_step_pre runs the surface-height query,

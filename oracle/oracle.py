@@ -44,6 +44,9 @@ _SIGS = {
     "wo_compute_csf_tension": ([_F, _I, _F, _F, _F, _i, _i, _i, _f, _i, _f], None),
     "wo_compute_marangoni_force": ([_F, _F, _F, _F, _F, _F, _I, _i, _i, _i, _f], None),
     "wo_apply_arc_pressure": ([_F, _I, _F, _i, _i, _i] + [_f] * 8, None),
+    "wo_apply_gas_shear_stress": ([_F, _F, _F, _I, _i, _i, _i] + [_f] * 7, None),
+    "wo_apply_vapor_recoil": ([_F, _F, _F, _I, _i, _i, _i] + [_f] * 8, None),
+    "wo_apply_vapor_recoil_cc": ([_F, _F, _F, _I, _i, _i, _i] + [_f] * 11, None),
     "wo_add_hydrostatic_gravity": ([_F, _F, _I, _l, _f, _f], None),
     "wo_add_buoyancy": ([_F, _F, _F, _I, _l, _f, _f, _f, _f], None),
     "wo_clamp_body_force_magnitude": ([_F, _F, _F, _I, _l, _f], None),

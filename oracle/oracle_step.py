@@ -51,7 +51,10 @@ class OracleTwin:
             trailing_solidify_temp_margin_K=35.0, enable_lorentz=False, sigma_liquid_Sm=1.0e6,
             sigma_solid_Sm=1.0e5, lorentz_jacobi_iters=40, lorentz_jacobi_omega=0.85,
             lorentz_jacobi_tol=1e-4, max_tracers=64, tables=None, use_variable_tau=True,
-            enable_moving_window=False)
+            enable_moving_window=False, enable_recoil=False, enable_gas_shear=False,
+            use_recoil_clausius_clapeyron=True, recoil_pressure_pa=5000.0, T_boiling_K=3100.0,
+            P_vapor_ref_Pa=101325.0, L_vapor_J_kg=6.0e6, R_spec_vapor_J_kgK=450.0,
+            gas_jet_velocity_m_s=12.0, gas_shear_coeff=1.0)
         unknown = set(kw) - set(self.cfg)
         if unknown:
             raise KeyError("unknown OracleTwin options: %s" % sorted(unknown))
@@ -392,10 +395,28 @@ class OracleTwin:
         else:
             self.O.call("wo_compute_marangoni_force", s["T"], s["phi"], s["f_l"], s["Fx"],
                         s["Fy"], s["Fz"], s["flags"], nx, ny, nz, self.dgamma_dT_lu)
+        sig = self.arc_sigma_m / self.dx
+        if welding and c["enable_gas_shear"]:
+            # physics/weld_forces.py:126-131 gas_shear_tau_pa, 180-193
+            v = c["gas_jet_velocity_m_s"]
+            tau = min(0.5 * 1.6 * v * v * c["gas_shear_coeff"], 5000.0)
+            self.O.call("wo_apply_gas_shear_stress", s["Fx"], s["Fy"], s["phi"], s["flags"], nx,
+                        ny, nz, arc_i, arc_j, sig, tau, self.dt, self.dx, m["rho"])
         if welding:
             self.O.call("wo_apply_arc_pressure", s["Fz"], s["flags"], s["phi"], nx, ny, nz, arc_i,
                    arc_j, arc_k, self.arc_sigma_m / self.dx, c["arc_pressure_pa"], self.dt,
                    self.dx, m["rho"])
+        if welding and c["enable_recoil"]:
+            # physics/weld_forces.py:134-158
+            if c["use_recoil_clausius_clapeyron"]:
+                self.O.call("wo_apply_vapor_recoil_cc", s["Fz"], s["T"], s["phi"], s["flags"],
+                            nx, ny, nz, arc_i, arc_j, sig, c["P_vapor_ref_Pa"], c["T_boiling_K"],
+                            c["L_vapor_J_kg"], c["R_spec_vapor_J_kgK"], 0.54, self.dt, self.dx,
+                            m["rho"])
+            else:
+                self.O.call("wo_apply_vapor_recoil", s["Fz"], s["T"], s["phi"], s["flags"], nx,
+                            ny, nz, arc_i, arc_j, sig, c["recoil_pressure_pa"], Tl, self.dt,
+                            self.dx, m["rho"])
         if c["enable_hydrostatic_gravity"]:
             self.O.call("wo_add_hydrostatic_gravity", s["Fz"], s["f_l"], s["flags"], n, 1.0, self.g_lu)
         self.O.call("wo_add_buoyancy", s["T"], s["Fz"], s["f_l"], s["flags"], n, self.g_lu,

@@ -761,6 +761,90 @@ void wo_apply_arc_pressure(float* Fz, const int32_t* flags, const float* phi, in
             }
 }
 
+/* kernels.py:1094-1141 apply_gas_shear_stress (arc_k is not used there) */
+void wo_apply_gas_shear_stress(float* Fx, float* Fy, const float* phi, const int32_t* flags,
+                               int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                               float tau_peak_pa, float dt, float dx, float rho_ref) {
+    const float eps = 1e-6f;
+    const float inv2s2 = 1.0f / (2.0f * sigma * sigma + eps);
+    const float F_scale = 1.0f / (rho_ref * dx) * dt * dt / dx;
+#pragma omp parallel for collapse(2)
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                int64_t c = IX(i, j, k);
+                if (flags[c] == SOLID || flags[c] == GAS) continue;
+                float dpx = 0.5f * (phi[IX(imin(i + 1, nx - 1), j, k)] - phi[IX(imax(i - 1, 0), j, k)]);
+                float dpy = 0.5f * (phi[IX(i, imin(j + 1, ny - 1), k)] - phi[IX(i, imax(j - 1, 0), k)]);
+                float dpz = 0.5f * (phi[IX(i, j, imin(k + 1, nz - 1))] - phi[IX(i, j, imax(k - 1, 0))]);
+                float gmag = sqrtf(dpx * dpx + dpy * dpy + dpz * dpz);
+                if (gmag < 0.08f) continue;
+                float di = (float)i - arc_i, dj = (float)j - arc_j;
+                float r2 = di * di + dj * dj;
+                float r = sqrtf(r2 + eps);
+                float rx = di / r, ry = dj / r;
+                float nxn = dpx / gmag, nyn = dpy / gmag;
+                float rdotn = rx * nxn + ry * nyn;
+                float tx = rx - rdotn * nxn, ty = ry - rdotn * nyn;
+                float tmag = sqrtf(tx * tx + ty * ty + eps);
+                tx = tx / tmag;
+                ty = ty / tmag;
+                float tau = tau_peak_pa * waam_expf(-r2 * inv2s2);
+                float Fmag = tau * F_scale;
+                Fx[c] += Fmag * tx;
+                Fy[c] += Fmag * ty;
+            }
+}
+
+/* kernels.py:995-1028 apply_vapor_recoil (T-ratio form) */
+void wo_apply_vapor_recoil(float* Fz, const float* T, const float* phi, const int32_t* flags,
+                           int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                           float recoil_pa, float T_ref, float dt, float dx, float rho_ref) {
+    const float eps = 1e-6f;
+    const float inv2s2 = 1.0f / (2.0f * sigma * sigma + eps);
+    const float F_peak = (recoil_pa / (rho_ref * dx)) * dt * dt / dx;
+#pragma omp parallel for collapse(2)
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                int64_t c = IX(i, j, k);
+                if (flags[c] == SOLID || flags[c] == GAS) continue;
+                float dpz = phi[IX(i, j, imin(k + 1, nz - 1))] - phi[IX(i, j, imax(k - 1, 0))];
+                if (fabsf(dpz) < 0.05f) continue;
+                float di = (float)i - arc_i, dj = (float)j - arc_j;
+                float r2 = di * di + dj * dj;
+                float t_ratio = fminf_(T[c] / (T_ref + eps), 3.0f);
+                Fz[c] += -F_peak * t_ratio * waam_expf(-r2 * inv2s2);
+            }
+}
+
+/* kernels.py:1046-1091 apply_vapor_recoil_clausius_clapeyron */
+void wo_apply_vapor_recoil_cc(float* Fz, const float* T, const float* phi, const int32_t* flags,
+                              int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                              float P_ref, float T_boil, float L_vap, float R_spec, float C_acc,
+                              float dt, float dx, float rho_ref) {
+    const float eps = 1e-6f;
+    const float inv2s2 = 1.0f / (2.0f * sigma * sigma + eps);
+#pragma omp parallel for collapse(2)
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                int64_t c = IX(i, j, k);
+                if (flags[c] == SOLID || flags[c] == GAS) continue;
+                float dpz = phi[IX(i, j, imin(k + 1, nz - 1))] - phi[IX(i, j, imax(k - 1, 0))];
+                if (fabsf(dpz) < 0.05f) continue;
+                float Tc = T[c];
+                if (Tc <= T_boil) continue;
+                float ex = (L_vap / (R_spec + eps)) * (1.0f / (T_boil + eps) - 1.0f / (Tc + eps));
+                ex = fminf_(ex, 12.0f);
+                float P_vap = C_acc * P_ref * waam_expf(ex);
+                float F_peak = P_vap / (rho_ref * dx) * dt * dt / dx;
+                float di = (float)i - arc_i, dj = (float)j - arc_j;
+                float r2 = di * di + dj * dj;
+                Fz[c] += -F_peak * waam_expf(-r2 * inv2s2);
+            }
+}
+
 /* kernels.py:2756-2772 add_hydrostatic_gravity */
 void wo_add_hydrostatic_gravity(float* Fz, const float* f_l, const int32_t* flags, int64_t n,
                                 float rho_ref, float g_lu) {

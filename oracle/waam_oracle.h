@@ -69,6 +69,16 @@ void wo_compute_csf_tension(const float* phi, const int32_t* flags, float* Fx, f
 void wo_compute_marangoni_force(const float* T, const float* phi, const float* f_l, float* Fx,
                                 float* Fy, float* Fz, const int32_t* flags, int nx, int ny, int nz,
                                 float dgamma);
+void wo_apply_gas_shear_stress(float* Fx, float* Fy, const float* phi, const int32_t* flags,
+                               int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                               float tau_peak_pa, float dt, float dx, float rho_ref);
+void wo_apply_vapor_recoil(float* Fz, const float* T, const float* phi, const int32_t* flags,
+                           int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                           float recoil_pa, float T_ref, float dt, float dx, float rho_ref);
+void wo_apply_vapor_recoil_cc(float* Fz, const float* T, const float* phi, const int32_t* flags,
+                              int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                              float P_ref, float T_boil, float L_vap, float R_spec, float C_acc,
+                              float dt, float dx, float rho_ref);
 void wo_apply_arc_pressure(float* Fz, const int32_t* flags, const float* phi, int nx, int ny,
                            int nz, float arc_i, float arc_j, float arc_k, float sigma,
                            float pressure, float dt, float dx, float rho_ref);

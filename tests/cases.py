@@ -47,14 +47,15 @@ def full_inputs(name):
                 "contact_s5": 5, "forces_wet": 6, "csf": 7, "csf_wet": 8, "collide_srt": 9,
                 "tail": 10, "heat_loss": 11, "surface_height": 12, "deposit": 13,
                 "lorentz": 14, "tracers": 15, "refresh": 16, "thermal_var": 17, "phase_var": 18,
-                "forces_var": 19, "srt_var": 20, "tail_var": 21, "shift": 24, "derived": 25}
+                "forces_var": 19, "srt_var": 20, "tail_var": 21, "shift": 24, "derived": 25,
+                "weld_forces": 26}
     grids = [v.shape[-3:] for v in ins.values() if v.ndim >= 3 and v.shape[-1] != 3]
     nx, ny, nz = grids[0] if grids else (13, 11, 12)   # tracer-only cases: the kernel-case grid
     st = state_gen.seeded_state(nx, ny, nz, seed=seed_map.get(name, 0))
     st = {k: (np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v) for k, v in st.items()}
     st["phi_tmp"] = np.zeros_like(st["phi"])
     for f, v in ins.items():
-        if f in st and f != "phi_tmp" and name not in ("reset", "shift"):
+        if f in st and f != "phi_tmp" and name not in ("reset", "shift", "weld_forces"):
             # the fixture was generated from this very seeded state
             assert np.array_equal(st[f], v), "state_gen drifted from fixture %s (%s)" % (name, f)
         st[f] = v.copy()
@@ -143,6 +144,17 @@ def run_case(be, name, st, a):
         be.add_buoyancy(st["T"], st["Fz"], st["f_l"], st["flags"], n, a["g_lu"], a["beta"],
                         a["T_liquidus"], 1.0)
         be.clamp_body_force_magnitude(st["Fx"], st["Fy"], st["Fz"], st["flags"], n, a["F_cap"])
+    elif name == "weld_forces":
+        be.apply_gas_shear_stress(st["Fx"], st["Fy"], st["phi"], st["flags"], nx, ny, nz,
+                                  a["arc_i"], a["arc_j"], a["sigma"], a["tau_pa"], a["dt"],
+                                  a["dx"], a["rho_ref"])
+        be.apply_vapor_recoil(st["Fz"], st["T"], st["phi"], st["flags"], nx, ny, nz, a["arc_i"],
+                              a["arc_j"], a["sigma"], a["recoil_pa"], a["T_ref"], a["dt"],
+                              a["dx"], a["rho_ref"])
+        be.apply_vapor_recoil_cc(st["Fz"], st["T"], st["phi"], st["flags"], nx, ny, nz,
+                                 a["arc_i"], a["arc_j"], a["sigma"], a["P_ref"], a["T_boil"],
+                                 a["L_vap"], a["R_spec"], a["C_acc"], a["dt"], a["dx"],
+                                 a["rho_ref"])
     elif name in ("csf", "csf_wet"):
         be.compute_csf_tension(st["phi"], st["flags"], st["Fx"], st["Fy"], st["Fz"], nx, ny, nz,
                                a["gamma_lu"], a["wetting"], a["theta"])
@@ -303,7 +315,8 @@ def run_case(be, name, st, a):
 
 
 CASES = ["inject_gauss", "inject_goldak", "ceiling", "thermal", "thermal_s2", "phase",
-         "tmax_cool", "vof", "vof_wet", "contact", "contact_s5", "forces", "forces_wet", "csf",
+         "tmax_cool", "vof", "vof_wet", "contact", "contact_s5", "forces", "forces_wet",
+         "weld_forces", "csf",
          "csf_wet", "collide_mrt", "collide_srt", "stream", "tail", "heat_loss",
          "surface_height", "deposit", "lorentz", "tracers", "refresh", "thermal_var",
          "phase_var", "forces_var", "srt_var", "tail_var", "shift", "derived", "reset"]

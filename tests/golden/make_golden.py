@@ -376,6 +376,39 @@ LORENTZ_FIELDS = ["sigma_elec", "elec_source", "phi_elec", "phi_elec_tmp", "Jx",
                   "Bx", "By", "Bz", "elec_rad_bins", "Fx", "Fy", "Fz"]
 
 
+def weld_forces_setup(tw, g):
+    """Some interface cells above the boiling point (the Clausius-Clapeyron
+    recoil acts only there) and non-zero starting forces."""
+    T = g.T.to_numpy()
+    rng = np.random.default_rng(41)
+    hot = rng.uniform(0.0, 1.0, T.shape) < 0.35
+    T = np.where(hot, rng.uniform(3000.0, 3600.0, T.shape), T).astype(np.float32)
+    g.T.from_numpy(T)
+    for name in ("Fx", "Fy", "Fz"):
+        fld = getattr(g, name)
+        fld.from_numpy(rng.normal(0.0, 1e-3, fld.shape).astype(np.float32))
+
+
+def c_weld_forces(tw, g):
+    """kernels.py:995-1141: shielding-gas shear, vapour recoil (T-ratio form) and
+    vapour recoil (Clausius-Clapeyron form), added to F one after the other."""
+    a = scal(tw)
+    a.update(arc_i=6.3, arc_j=5.4, arc_k=float(tw.nz_solid + 1), sigma=2.5, tau_pa=115.2,
+             recoil_pa=5000.0, T_ref=tw.mat.T_liquidus, P_ref=101325.0, T_boil=3100.0,
+             L_vap=6.0e6, R_spec=450.0, C_acc=0.54, rho_ref=tw.mat.rho)
+    K.apply_gas_shear_stress(g.Fx, g.Fy, g.phi, g.flags, a["arc_i"], a["arc_j"], a["arc_k"],
+                             a["sigma"], a["tau_pa"], g.dt, g.dx, a["rho_ref"], g.FLAG_SOLID,
+                             g.FLAG_GAS)
+    K.apply_vapor_recoil(g.Fz, g.T, g.phi, g.flags, a["arc_i"], a["arc_j"], a["arc_k"],
+                         a["sigma"], a["recoil_pa"], a["T_ref"], g.dt, g.dx, a["rho_ref"],
+                         g.FLAG_SOLID, g.FLAG_GAS)
+    K.apply_vapor_recoil_clausius_clapeyron(g.Fz, g.T, g.phi, g.flags, a["arc_i"], a["arc_j"],
+                                            a["arc_k"], a["sigma"], a["P_ref"], a["T_boil"],
+                                            a["L_vap"], a["R_spec"], a["C_acc"], g.dt, g.dx,
+                                            a["rho_ref"], g.FLAG_SOLID, g.FLAG_GAS)
+    return a
+
+
 def lorentz_setup(tw, g):
     g.ensure_lorentz_fields()
     rng = np.random.default_rng(31)
@@ -588,6 +621,8 @@ def kernel_cases():
     kernel_case("surface_height", c_surface_height, ["phi"], seed=12)
     kernel_case("deposit", c_deposit, base + ["rho", "f_a", "ux", "uy", "uz", "Fz"], seed=13)
     kernel_case("lorentz", c_lorentz, LORENTZ_FIELDS, seed=14, extra_in=lorentz_setup)
+    kernel_case("weld_forces", c_weld_forces, ["T", "Fx", "Fy", "Fz"], seed=26,
+                extra_in=weld_forces_setup)
     kernel_case("tracers", c_tracers, ["porosity_pos", "porosity_active"], seed=15,
                 extra_in=tracer_setup)
     tb = dict(tables=True)

@@ -151,6 +151,32 @@ def test_graph_replay_matches_eager_launches():
             assert np.array_equal(v, states[1][k]), k
 
 
+@pytest.mark.parametrize("step_mode", ["fused", "operators"])
+@pytest.mark.parametrize("cc", [True, False])
+def test_recoil_and_gas_shear_steps_match_oracle(step_mode, cc):
+    """Vapour recoil (Clausius-Clapeyron or T-ratio form) and shielding-gas shear
+    on: steps from a seeded hot pool against the oracle, in the fused step (both
+    terms inside the collision's force assembly) and through the operators."""
+    import state_gen
+    shape = (40, 24, 24)
+    tw, ot, dx = _config_twins("c2", *shape, enable_recoil=True, enable_gas_shear=True,
+                               use_recoil_clausius_clapeyron=cc, step_mode=step_mode)
+    st = state_gen.seeded_state(*shape, seed=9, nz_solid=tw.nz_solid)
+    T = st["T"]
+    hot = (st["flags"] == 4) | (st["flags"] == 0)
+    st["T"] = np.where(hot, np.maximum(T, 3150.0), T).astype(np.float32)
+    st["read_is_a"] = True
+    tw.grid.load_state({k: v for k, v in st.items() if k != "nz_solid"})
+    ot.load({k: v for k, v in st.items() if k != "nz_solid"})
+    y = (shape[1] // 2) * dx
+    for s in range(4):
+        x = 0.3 * shape[0] * dx + s * 0.008 * dx * 0.1
+        tw.step(x, y, True)
+        ot.step(x, y, True)
+        torch.cuda.synchronize()
+        steps.compare_state("recoil step %d" % s, tw.grid.state_dict(), ot.s)
+
+
 @pytest.mark.parametrize("lorentz", [False, True])
 def test_pipelined_stream_matches_in_order_stream(lorentz):
     """Each step's stream left to run beside the next step's arc, thermal and VOF

@@ -361,12 +361,20 @@ def step_params(twin):
     p.H_sol_t, p.H_liq_t = twin.H_sol, twin.H_liq
     p.tau_ref = g.tau
     p.tables = twin.gpu_tables.struct
+    # shielding-gas shear and vapour recoil (physics/weld_forces.py:126-193)
+    p.gas_shear = 1 if twin.enable_gas_shear else 0
+    p.gs_tau_pa = weld_forces.gas_shear_tau_pa(twin)
+    p.recoil = (2 if twin.use_recoil_clausius_clapeyron else 1) if twin.enable_recoil else 0
+    p.recoil_pa, p.recoil_T_ref = twin.recoil_pressure_pa, m.T_liquidus
+    p.P_ref, p.T_boil = twin.P_vapor_ref_Pa, twin.T_boiling_K
+    p.L_vap, p.R_spec = twin.L_vapor_J_kg, twin.R_spec_vapor_J_kgK
+    p.C_acc = weld_forces.recoil_accommodation(twin)
+    p.weld_sigma = twin.sigma_cells
     return p
 
 
 def _check_fused_supported(twin):
-    supported = not (twin.enable_recoil or twin.enable_gas_shear or
-                     getattr(twin, "use_torch_z", False))
+    supported = not getattr(twin, "use_torch_z", False)
     if not supported and twin.grid.population_storage:
         raise WaamError("16-bit population storage runs on the fused step only; this "
                         "configuration needs the operator path")

@@ -650,6 +650,7 @@ int waam_adj_collide(const WaamStepParams* p, const float* tape_f, const int32_t
             "collision with constant material properties");
     AdjCollideArgs a;
     ForceParams& P = a.P;
+    P.W = WeldForceParams{};
     P.csf = p->csf;
     P.wetting = p->wetting;
     P.welding = p->welding;

@@ -520,7 +520,97 @@ __device__ __forceinline__ float brackbill_kappa(const Dims d, const float* __re
 }
 
 // Force parameters (solvers/coupled_step.py:298-362)
+// Shielding-gas shear and vapour recoil (kernels.py:995-1141): the constants
+// the reference computes per kernel call, prepared on the host in its float
+// order.  recoil: 0 off, 1 the T-ratio form, 2 the Clausius-Clapeyron form.
+struct WeldForceParams {
+    int gas_shear;
+    float gs_tau, gs_scale, gs_inv2s2;        // tau_peak, F(1 Pa), 1 / (2 sigma^2 + eps)
+    int recoil;
+    float rc_inv2s2;
+    float rc_Fpeak, rc_Tref;                  // T-ratio form: F_peak_lu, T_ref
+    float rc_LR, rc_invTb, rc_Tboil, rc_CP;   // CC form: L / (R + eps), 1 / (T_boil + eps),
+    float rc_rhodx, rc_dt, rc_dx;             //   T_boil, C_acc * P_ref, rho * dx, dt, dx
+};
+
+// The constants in the reference's float order (kernels.py:1015, 1033-1035,
+// 1072-1086, 1117-1119).
+__host__ inline WeldForceParams weld_force_params(int gas_shear, float tau_peak_pa, int recoil,
+                                                  float recoil_pa, float T_ref, float P_ref,
+                                                  float T_boil, float L_vap, float R_spec,
+                                                  float C_acc, float sigma, float dt, float dx,
+                                                  float rho_ref) {
+    const float eps = 1e-6f;
+    WeldForceParams W{};
+    W.gas_shear = gas_shear;
+    W.gs_tau = tau_peak_pa;
+    W.gs_scale = 1.0f / (rho_ref * dx) * dt * dt / dx;
+    W.gs_inv2s2 = 1.0f / (2.0f * sigma * sigma + eps);
+    W.recoil = recoil;
+    W.rc_inv2s2 = W.gs_inv2s2;
+    W.rc_Fpeak = (recoil_pa / (rho_ref * dx)) * dt * dt / dx;
+    W.rc_Tref = T_ref;
+    W.rc_LR = L_vap / (R_spec + eps);
+    W.rc_invTb = 1.0f / (T_boil + eps);
+    W.rc_Tboil = T_boil;
+    W.rc_CP = C_acc * P_ref;
+    W.rc_rhodx = rho_ref * dx;
+    W.rc_dt = dt;
+    W.rc_dx = dx;
+    return W;
+}
+
+// kernels.py:1094-1141 apply_gas_shear_stress for one non-solid non-gas cell.
+__device__ __forceinline__ void gas_shear_cell(const Dims& d, const float* __restrict__ phi,
+                                               int i, int j, int k, float arc_i, float arc_j,
+                                               const WeldForceParams& W, float& fx, float& fy) {
+    const float eps = 1e-6f;
+    const float dpx = 0.5f * (phi[d.idx(imin(i + 1, d.nx - 1), j, k)] - phi[d.idx(imax(i - 1, 0), j, k)]);
+    const float dpy = 0.5f * (phi[d.idx(i, imin(j + 1, d.ny - 1), k)] - phi[d.idx(i, imax(j - 1, 0), k)]);
+    const float dpz = 0.5f * (phi[d.idx(i, j, imin(k + 1, d.nz - 1))] - phi[d.idx(i, j, imax(k - 1, 0))]);
+    const float gmag = sqrtf(dpx * dpx + dpy * dpy + dpz * dpz);
+    if (gmag < 0.08f) return;
+    const float di = (float)i - arc_i, dj = (float)j - arc_j;
+    const float r2 = di * di + dj * dj;
+    const float r = sqrtf(r2 + eps);
+    const float rx = di / r, ry = dj / r;
+    const float nxn = dpx / gmag, nyn = dpy / gmag;
+    const float rdotn = rx * nxn + ry * nyn;
+    float tx = rx - rdotn * nxn, ty = ry - rdotn * nyn;
+    const float tmag = sqrtf(tx * tx + ty * ty + eps);
+    tx = tx / tmag;
+    ty = ty / tmag;
+    const float tau = W.gs_tau * waam_expf(-r2 * W.gs_inv2s2);
+    const float Fmag = tau * W.gs_scale;
+    fx += Fmag * tx;
+    fy += Fmag * ty;
+}
+
+// kernels.py:995-1028 (recoil 1) and 1046-1091 (recoil 2) for one non-solid
+// non-gas cell with temperature Tc.
+__device__ __forceinline__ void recoil_cell(const Dims& d, const float* __restrict__ phi, float Tc,
+                                            int i, int j, int k, float arc_i, float arc_j,
+                                            const WeldForceParams& W, float& fz) {
+    const float eps = 1e-6f;
+    const float dpz = phi[d.idx(i, j, imin(k + 1, d.nz - 1))] - phi[d.idx(i, j, imax(k - 1, 0))];
+    if (fabsf(dpz) < 0.05f) return;
+    const float di = (float)i - arc_i, dj = (float)j - arc_j;
+    const float r2 = di * di + dj * dj;
+    if (W.recoil == 1) {
+        const float t_ratio = fmin_(Tc / (W.rc_Tref + eps), 3.0f);
+        fz += -W.rc_Fpeak * t_ratio * waam_expf(-r2 * W.rc_inv2s2);
+    } else {
+        if (Tc <= W.rc_Tboil) return;
+        float ex = W.rc_LR * (W.rc_invTb - 1.0f / (Tc + eps));
+        ex = fmin_(ex, 12.0f);
+        const float P_vap = W.rc_CP * waam_expf(ex);
+        const float F_peak = P_vap / W.rc_rhodx * W.rc_dt * W.rc_dt / W.rc_dx;
+        fz += -F_peak * waam_expf(-r2 * W.rc_inv2s2);
+    }
+}
+
 struct ForceParams {
+    WeldForceParams W;
     int csf, wetting, welding, hydro;
     float gamma_lu, cos_t, sin_t;
     float dgamma;
@@ -529,8 +619,8 @@ struct ForceParams {
     float F_cap;
 };
 
-// Body force of one non-solid non-gas cell (CSF -> Marangoni -> arc pressure
-// -> hydrostatic -> buoyancy -> clamp), accumulated on (fx, fy, fz) in the
+// Body force of one non-solid non-gas cell (CSF -> Marangoni -> gas shear ->
+// arc pressure -> recoil -> hydrostatic -> buoyancy -> clamp), accumulated on (fx, fy, fz) in the
 // reference order (solvers/coupled_step.py:298-362).
 __device__ __forceinline__ void cell_forces(const Dims d, const ForceParams& P,
                                             const float* __restrict__ phi,
@@ -622,6 +712,8 @@ __device__ __forceinline__ void cell_forces(const Dims d, const ForceParams& P,
             fz += scale * sz;
         }
     }
+    // physics/weld_forces.py:161-193 apply_gas_shear (solvers/coupled_step.py:325-326)
+    if (P.welding && P.W.gas_shear) gas_shear_cell(d, phi, i, j, k, P.arc_i, P.arc_j, P.W, fx, fy);
     // kernels.py:3038-3083 apply_arc_pressure
     if (P.welding) {
         float dpz = phi[d.idx(i, j, imin(k + 1, d.nz - 1))] - phi[d.idx(i, j, imax(k - 1, 0))];
@@ -631,6 +723,8 @@ __device__ __forceinline__ void cell_forces(const Dims d, const ForceParams& P,
             fz += -P.p_Flu * waam_expf(-r2 * P.p_inv2s2);
         }
     }
+    // physics/weld_forces.py:137-158 apply_recoil (solvers/coupled_step.py:334)
+    if (P.welding && P.W.recoil) recoil_cell(d, phi, T[c], i, j, k, P.arc_i, P.arc_j, P.W, fz);
     // kernels.py:2756-2772 add_hydrostatic_gravity
     if (P.hydro && fl > 0.0f) fz += -P.rho_ref * P.g_lu * fl;
     // kernels.py:2729-2753 add_buoyancy

@@ -1119,6 +1119,9 @@ static int launch_collide_tracers(const WaamFields* f, const WaamStepParams* p, 
     int e = WAAM_OK;
     CollideArgs cl;
     ForceParams& P = cl.P;
+    P.W = weld_force_params(p->gas_shear, p->gs_tau_pa, p->recoil, p->recoil_pa, p->recoil_T_ref,
+                            p->P_ref, p->T_boil, p->L_vap, p->R_spec, p->C_acc, p->weld_sigma,
+                            p->dt, p->dx, p->rho_phys);
     P.csf = p->csf;
     P.wetting = p->wetting;
     P.welding = welding;

@@ -434,6 +434,34 @@ __global__ void k_marangoni(Dims d, const float* T, const float* phi, const floa
     }
 }
 
+// kernels.py:1094-1141 apply_gas_shear_stress / 995-1091 apply_vapor_recoil(_cc)
+__global__ void k_gas_shear(Dims d, float* Fx, float* Fy, const int32_t* flags, const float* phi,
+                            float arc_i, float arc_j, WeldForceParams W) {
+    GRID_LOOP(c, d.n()) {
+        int flag = flags[c];
+        if (flag == SOLID || flag == GAS) continue;
+        int i, j, k;
+        d.ijk(c, i, j, k);
+        float fx = Fx[c], fy = Fy[c];
+        gas_shear_cell(d, phi, i, j, k, arc_i, arc_j, W, fx, fy);
+        Fx[c] = fx;
+        Fy[c] = fy;
+    }
+}
+
+__global__ void k_recoil(Dims d, float* Fz, const float* T, const int32_t* flags, const float* phi,
+                         float arc_i, float arc_j, WeldForceParams W) {
+    GRID_LOOP(c, d.n()) {
+        int flag = flags[c];
+        if (flag == SOLID || flag == GAS) continue;
+        int i, j, k;
+        d.ijk(c, i, j, k);
+        float fz = Fz[c];
+        recoil_cell(d, phi, T[c], i, j, k, arc_i, arc_j, W, fz);
+        Fz[c] = fz;
+    }
+}
+
 __global__ void k_arc_pressure(Dims d, float* Fz, const int32_t* flags, const float* phi,
                                float arc_i, float arc_j, float arc_k, float inv2s2, float Flu) {
     int64_t n = d.n();
@@ -915,6 +943,42 @@ int waam_compute_marangoni_force(const float* T, const float* phi, const float* 
     REQUIRE(T && phi && f_l && Fx && Fy && Fz && flags, "marangoni: null field");
     Dims d{nx, ny, nz};
     EW(k_marangoni, d.n(), stream, d, T, phi, f_l, Fx, Fy, Fz, flags, dgamma, nullptr);
+}
+
+int waam_apply_gas_shear_stress(float* Fx, float* Fy, const float* phi, const int32_t* flags,
+                                int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                                float tau_peak_pa, float dt, float dx, float rho_ref,
+                                void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "gas_shear: bad dims");
+    REQUIRE(Fx && Fy && flags && phi, "gas_shear: null field");
+    Dims d{nx, ny, nz};
+    WeldForceParams W = weld_force_params(1, tau_peak_pa, 0, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f,
+                                          0.0f, sigma, dt, dx, rho_ref);
+    EW(k_gas_shear, d.n(), stream, d, Fx, Fy, flags, phi, arc_i, arc_j, W);
+}
+
+int waam_apply_vapor_recoil(float* Fz, const float* T, const float* phi, const int32_t* flags,
+                            int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                            float recoil_pa, float T_ref, float dt, float dx, float rho_ref,
+                            void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "vapor_recoil: bad dims");
+    REQUIRE(Fz && T && flags && phi, "vapor_recoil: null field");
+    Dims d{nx, ny, nz};
+    WeldForceParams W = weld_force_params(0, 0.0f, 1, recoil_pa, T_ref, 0.0f, 0.0f, 0.0f, 0.0f,
+                                          0.0f, sigma, dt, dx, rho_ref);
+    EW(k_recoil, d.n(), stream, d, Fz, T, flags, phi, arc_i, arc_j, W);
+}
+
+int waam_apply_vapor_recoil_cc(float* Fz, const float* T, const float* phi, const int32_t* flags,
+                               int nx, int ny, int nz, float arc_i, float arc_j, float sigma,
+                               float P_ref, float T_boil, float L_vap, float R_spec, float C_acc,
+                               float dt, float dx, float rho_ref, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "vapor_recoil_cc: bad dims");
+    REQUIRE(Fz && T && flags && phi, "vapor_recoil_cc: null field");
+    Dims d{nx, ny, nz};
+    WeldForceParams W = weld_force_params(0, 0.0f, 2, 0.0f, 0.0f, P_ref, T_boil, L_vap, R_spec,
+                                          C_acc, sigma, dt, dx, rho_ref);
+    EW(k_recoil, d.n(), stream, d, Fz, T, flags, phi, arc_i, arc_j, W);
 }
 
 int waam_apply_arc_pressure(float* Fz, const int32_t* flags, const float* phi, int nx, int ny,

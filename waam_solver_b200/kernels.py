@@ -493,6 +493,41 @@ def compute_marangoni_force(T, phi, f_l, Fx, Fy, Fz, flags, dgamma_dT, dx, FLAG_
           _f(Fz, n), _i(flags, n), int(nx), int(ny), int(nz), float(dgamma_dT), _stream())
 
 
+def apply_gas_shear_stress(Fx, Fy, phi, flags, arc_i, arc_j, arc_k, sigma, tau_peak_pa, dt, dx,
+                           rho_ref, FLAG_SOLID, FLAG_GAS):
+    """kernels.py:1094-1141 (arc_k is not used by the reference either)."""
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(Fx)
+    n = Fx.numel()
+    _call("waam_apply_gas_shear_stress", _f(Fx, n), _f(Fy, n), _f(phi, n), _i(flags, n), nx, ny,
+          nz, float(arc_i), float(arc_j), float(sigma), float(tau_peak_pa), float(dt), float(dx),
+          float(rho_ref), _stream())
+
+
+def apply_vapor_recoil(Fz, T, phi, flags, arc_i, arc_j, arc_k, sigma, recoil_pa, T_ref, dt, dx,
+                       rho_ref, FLAG_SOLID, FLAG_GAS):
+    """kernels.py:995-1028."""
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(Fz)
+    n = Fz.numel()
+    _call("waam_apply_vapor_recoil", _f(Fz, n), _f(T, n), _f(phi, n), _i(flags, n), nx, ny, nz,
+          float(arc_i), float(arc_j), float(sigma), float(recoil_pa), float(T_ref), float(dt),
+          float(dx), float(rho_ref), _stream())
+
+
+def apply_vapor_recoil_clausius_clapeyron(Fz, T, phi, flags, arc_i, arc_j, arc_k, sigma, P_ref_Pa,
+                                          T_boil_K, L_vapor_J_kg, R_spec_J_kgK, C_acc, dt, dx,
+                                          rho_ref, FLAG_SOLID, FLAG_GAS):
+    """kernels.py:1046-1091."""
+    _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)
+    nx, ny, nz = _dims(Fz)
+    n = Fz.numel()
+    _call("waam_apply_vapor_recoil_cc", _f(Fz, n), _f(T, n), _f(phi, n), _i(flags, n), nx, ny,
+          nz, float(arc_i), float(arc_j), float(sigma), float(P_ref_Pa), float(T_boil_K),
+          float(L_vapor_J_kg), float(R_spec_J_kgK), float(C_acc), float(dt), float(dx),
+          float(rho_ref), _stream())
+
+
 def apply_arc_pressure(Fz, flags, phi, arc_i, arc_j, arc_k, sigma, pressure_pa, dt, dx, rho_ref,
                        FLAG_SOLID, FLAG_GAS):
     _flags_ok(FLAG_SOLID=FLAG_SOLID, FLAG_GAS=FLAG_GAS)

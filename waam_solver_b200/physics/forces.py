@@ -8,6 +8,7 @@ compute_csf_wetting = kernels.compute_csf_wetting
 add_buoyancy = kernels.add_buoyancy
 add_hydrostatic_gravity = kernels.add_hydrostatic_gravity
 apply_arc_pressure = kernels.apply_arc_pressure
+apply_vapor_recoil = kernels.apply_vapor_recoil
 
 
 def compute_csf_tension(phi, flags, Fx, Fy, Fz, gamma_lu, FLAG_SOLID, FLAG_GAS, nx, ny, nz,
@@ -20,5 +21,5 @@ def compute_csf_tension(phi, flags, Fx, Fy, Fz, gamma_lu, FLAG_SOLID, FLAG_GAS, 
 __all__ = [
     "clear_forces", "compute_marangoni_force", "compute_marangoni_force_variable",
     "compute_csf_tension", "compute_csf_wetting",
-    "add_buoyancy", "add_hydrostatic_gravity", "apply_arc_pressure",
+    "add_buoyancy", "add_hydrostatic_gravity", "apply_arc_pressure", "apply_vapor_recoil",
 ]

@@ -95,14 +95,40 @@ def apply_droplet_impact(twin, g, arc_i, arc_j, arc_k, drop_r, drop_mass_kg=None
             twin.mat.rho, g.FLAG_SOLID, g.FLAG_GAS)
 
 
+def gas_shear_tau_pa(twin):
+    """physics/weld_forces.py:126-131: dynamic shear of the argon jet, capped."""
+    rho_gas = 1.6
+    v = twin.gas_jet_velocity_m_s
+    tau = 0.5 * rho_gas * v * v * twin.gas_shear_coeff
+    return min(tau, 5000.0)
+
+
+def recoil_accommodation(twin):
+    return float(getattr(twin, "recoil_accommodation", 0.54))
+
+
 def apply_recoil(twin, g, arc_i, arc_j, arc_k):
-    if twin.enable_recoil:
-        raise WaamError("vapour recoil is not supported by this backend")
+    """physics/weld_forces.py:134-158."""
+    if not twin.enable_recoil:
+        return
+    if twin.use_recoil_clausius_clapeyron:
+        kernels.apply_vapor_recoil_clausius_clapeyron(
+            g.Fz, g.T, g.phi, g.flags, arc_i, arc_j, arc_k, twin.sigma_cells,
+            twin.P_vapor_ref_Pa, twin.T_boiling_K, twin.L_vapor_J_kg, twin.R_spec_vapor_J_kgK,
+            recoil_accommodation(twin), g.dt, g.dx, twin.mat.rho, g.FLAG_SOLID, g.FLAG_GAS)
+    else:
+        kernels.apply_vapor_recoil(g.Fz, g.T, g.phi, g.flags, arc_i, arc_j, arc_k,
+                                   twin.sigma_cells, twin.recoil_pressure_pa, twin.mat.T_liquidus,
+                                   g.dt, g.dx, twin.mat.rho, g.FLAG_SOLID, g.FLAG_GAS)
 
 
 def apply_gas_shear(twin, g, arc_i, arc_j, arc_k):
-    if twin.enable_gas_shear:
-        raise WaamError("shielding-gas shear is not supported by this backend")
+    """physics/weld_forces.py:180-193."""
+    if not twin.enable_gas_shear:
+        return
+    kernels.apply_gas_shear_stress(g.Fx, g.Fy, g.phi, g.flags, arc_i, arc_j, arc_k,
+                                   twin.sigma_cells, gas_shear_tau_pa(twin), g.dt, g.dx,
+                                   twin.mat.rho, g.FLAG_SOLID, g.FLAG_GAS)
 
 
 def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True, arc_k_dev=None):
