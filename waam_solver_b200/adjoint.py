@@ -121,6 +121,10 @@ class AdjointProblem:
     def __init__(self, twin, positions, probes, T_target=None, W_target=None, w_T=1.0,
                  w_W=1.0, beta=20.0, checkpoint_every=None):
         self.tw = twin
+        # every forward changes the twin's parameters and restores a checkpoint,
+        # which drops its captured step graphs: plain launches cost less than
+        # capturing them again for each forward
+        twin.use_cuda_graphs = False
         self.positions = [(float(x), float(y)) for x, y in positions]
         self.N = len(self.positions)
         g = twin.grid
