@@ -442,16 +442,14 @@ ADJOINT_C4 = dict(
     enable_heat_loss=True, steps=2000)
 
 
-def adjoint_form(device, n_steps=None, fd=True):
-    """Config 4: loss + gradient with the hand-written adjoint (sqrt(N)
-    checkpointing), backward time against forward time (CUDA events), and
-    central finite differences (relative step 1e-3) of every parameter."""
+def _c4_problem(device, N, h_conv_scale=1.0):
+    """The config-4 adjoint problem: probe targets from a run at perturbed
+    parameters, the width target 0.1 mm above the base run's width."""
     import numpy as np
-    import torch
-    from waam_solver_b200.adjoint import PARAMS, AdjointProblem
+    from waam_solver_b200.adjoint import AdjointProblem
     w = dict(ADJOINT_C4)
-    N = int(n_steps or w["steps"])
     tw = build_twin(w, device)
+    tw.h_conv = tw.h_conv * h_conv_scale
     g = tw.grid
     dx = g.dx
     x0, yc = 10e-3, (g.ny // 2) * dx
@@ -469,6 +467,26 @@ def adjoint_form(device, n_steps=None, fd=True):
     prob.W_target, _ = prob.width()
     prob.W_target += 0.1
     prob.w_T, prob.w_W = 1e-3, 10.0
+    return prob, base
+
+
+def _central_fd(prob, base, q, step):
+    h = step * abs(base[q])
+    tp, tm = base.copy(), base.copy()
+    tp[q] += h
+    tm[q] -= h
+    return (prob.forward(tp) - prob.forward(tm)) / (2 * h)
+
+
+def adjoint_form(device, n_steps=None, fd=True):
+    """Config 4: loss + gradient with the hand-written adjoint (sqrt(N)
+    checkpointing), backward time against forward time (CUDA events), and
+    central finite differences (relative step 1e-3) of every parameter."""
+    import torch
+    from waam_solver_b200.adjoint import PARAMS
+    w = dict(ADJOINT_C4)
+    N = int(n_steps or w["steps"])
+    prob, base = _c4_problem(device, N)
     prob.forward(base)                     # warm-up of both passes
     prob.backward()
     e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
@@ -493,13 +511,26 @@ def adjoint_form(device, n_steps=None, fd=True):
             for q, name in enumerate(PARAMS):
                 if base[q] == 0.0:
                     continue
-                h = step * abs(base[q])
-                tp, tm = base.copy(), base.copy()
-                tp[q] += h
-                tm[q] -= h
-                f = (prob.forward(tp) - prob.forward(tm)) / (2 * h)
+                f = _central_fd(prob, base, q, step)
                 rel[name] = {"fd": f, "rel_diff": abs(grad[q] - f) / max(abs(f), 1e-300)}
             out[key] = rel
+        # At h_conv 25 W/m^2K one step's convective loss from a surface cell
+        # is a few float32 ULPs of its enthalpy (dt 25 us, H ~ 4e9 J/m^3, ULP
+        # 256), so a 1 % change of the factor moves H_next by ~0.05 ULP and the
+        # float32 forward answers it through rounding.  The same problem with
+        # h_conv x1000 resolves the term: there the difference measures the
+        # adjoint's heat-loss derivative itself.
+        del prob
+        torch.cuda.empty_cache()
+        q = PARAMS.index("heat_loss_factor")
+        prob, base = _c4_problem(device, N, h_conv_scale=1000.0)
+        prob.forward(base)
+        g_hl = float(prob.backward()[q])
+        chk = {"h_conv_W_m2K": prob.tw.h_conv, "gradient": g_hl}
+        for step in (1e-3, 1e-2):
+            f = _central_fd(prob, base, q, step)
+            chk["central_fd_rel_step_%g" % step] = {"fd": f, "rel_diff": abs(g_hl - f) / abs(f)}
+        out["heat_loss_factor_at_h_conv_x1000"] = chk
     return out
 
 
