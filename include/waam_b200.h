@@ -62,11 +62,14 @@ int waam_inject_goldak_heat(float* H, const int32_t* flags, const float* f_l, fl
                             float Q_w, float dt, float dx3, float eta, float sign, float ff,
                             float fr, float a_f, float a_r, float b, float c, float pen,
                             int enable, void* workspace, size_t workspace_bytes, void* stream);
-/* Same operation and result as waam_inject_goldak_heat, for callers that
- * cannot allocate device memory (an FFI host without a CUDA allocator, or a
- * step loop under a fixed device-memory budget): its reduction scratch is a
- * static device array inside the library, so it takes no workspace.  No
- * counterpart in the reference.  Grids above 16,777,216 cells are rejected
+/* The operation of waam_inject_goldak_heat, for callers that cannot allocate
+ * device memory (an FFI host without a CUDA allocator, or a step loop under a
+ * fixed device-memory budget): its reduction scratch is a static device array
+ * inside the library, so it takes no workspace.  The result equals
+ * waam_inject_goldak_heat's to rounding: its double weight sum is split over
+ * ceil(n / 2048) blocks instead of the workspace path's fixed block count, so
+ * the float32 weight sum can differ in the last bit.  No counterpart in the
+ * reference.  Grids above 16,777,216 cells are rejected
  * with WAAM_ERR_INVALID; calls that overlap on the GPU race on the shared
  * scratch; the first call on a device resolves the scratch address and
  * should come before any stream capture. */
@@ -204,6 +207,21 @@ int waam_feed_wire_surface(float* f_src, int32_t* flags, float* f_l, float* phi,
                            float arc_k, float foot_r, float drop_r, float target_vol,
                            float T_drop, float cp_rho, float L_rho, float rho0, float* vol_acc,
                            float* real_acc, float cell_vol, void* stream);
+/* kernels.py:177-242 feed_wire (physics/deposition.py:22): the older droplet
+ * feed -- GAS cells inside the droplet sphere or the column above the arc
+ * become liquid metal while the volume budget *vol_acc (device float) is below
+ * target_vol, in serial lexicographic order.  f_src holds populations in the
+ * storage f_storage (as WaamStepParams.f_storage).  One CTA per call. */
+int waam_feed_wire(void* f_src, int f_storage, int32_t* flags, float* f_l, float* phi, float* H,
+                   float* T, float* rho, int nx, int ny, int nz, float arc_i, float arc_j,
+                   float arc_k, float drop_r, float target_vol, float T_drop, float cp_rho,
+                   float L_rho, float rho0, float* vol_acc, float cell_vol, void* stream);
+/* kernels.py:644-676 feed_wire_momentum (physics/deposition.py:24):
+ * uz = min(uz + vz_lu, 0.15) for the non-gas cells with f_l >= 0.5 of the
+ * droplet's column. */
+int waam_feed_wire_momentum(float* uz, const int32_t* flags, const float* f_l, int nx, int ny,
+                            int nz, float arc_i, float arc_j, float arc_k, float drop_r,
+                            float vz_lu, void* stream);
 /* The droplet's whole deposition, solvers/coupled_step.py:126-151: attempt t
  * is feed_wire_surface with footprint radius foot_radii[t]; attempt 0 starts
  * from *vol_acc / *real_acc, attempt t > 0 runs only while the converted

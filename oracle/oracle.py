@@ -60,6 +60,8 @@ _SIGS = {
     "wo_solidify_trailing_pool_scalar": ([_F, _F, _F, _F, _I, _F, _F, _F, _i, _i, _i] + [_f] * 10, None),
     "wo_solidify_cooled_metal": ([_F, _F, _F, _I, _F, _F, _F, _l, _f, _i], None),
     "wo_surface_height_at": ([_F, _I, _i, _i, _i, _i, _i, _i], C.c_float),
+    "wo_feed_wire": ([_F, _I, _F, _F, _F, _F, _F, _i, _i, _i] + [_f] * 9 + [_F, _f], None),
+    "wo_feed_wire_momentum": ([_F, _I, _F, _i, _i, _i] + [_f] * 5, None),
     "wo_feed_wire_surface": ([_F, _I, _F, _F, _F, _F, _F, _i, _i, _i] + [_f] * 10 + [_F, _F, _f], None),
     "wo_feed_wire_momentum_impact": ([_F, _F, _F, _F, _F, _I, _F, _i, _i, _i] + [_f] * 7, None),
     "wo_apply_droplet_impact_pressure": ([_F, _I, _F, _F, _i, _i, _i] + [_f] * 8, None),

@@ -174,6 +174,9 @@ class OracleTwin:
 
     # ---------------------------------------------------------------- state --
     def reset(self):
+        # twin.py:486-531 also forgets the torch position and direction
+        self.last_pos = None
+        self.dir = (1.0, 0.0, 0.0)
         nx, ny, nz = self.nx, self.ny, self.nz
         sh = (nx, ny, nz)
         z = lambda: np.zeros(sh, self.ft)  # noqa: E731
@@ -293,23 +296,27 @@ class OracleTwin:
         pos = s["porosity_pos"]
         pos[:, 0] = pos[:, 0] - self.ft(n_shift * self.dx)
 
-    def step(self, x, y, welding=True):
-        """One step at torch position (x, y); with the moving window on, x is a
+    def step(self, x, y, welding=True, z=None):
+        """One step at torch position (x, y) and torch height z (None: 0, used
+        for the travel direction only); with the moving window on, x is a
         world position (twin.py:533-567)."""
         if self.cfg["enable_moving_window"]:
             # the direction uses world positions, the physics the window's
-            self._update_dir(x, y)
+            self._update_dir(x, y, z)
             self._maybe_shift_window(x)
             return self._step(x - self.window_offset, y, welding, dir_done=True)
-        return self._step(x, y, welding)
+        self._update_dir(x, y, z)
+        return self._step(x, y, welding, dir_done=True)
 
-    def _update_dir(self, x, y):
+    def _update_dir(self, x, y, z=None):
+        """twin.py:540-546: the unit vector from the previous torch position."""
+        z = 0.0 if z is None else float(z)
         if self.last_pos is not None:
-            d = (x - self.last_pos[0], y - self.last_pos[1], 0.0 - self.last_pos[2])
+            d = (x - self.last_pos[0], y - self.last_pos[1], z - self.last_pos[2])
             nrm = math.sqrt(sum(v * v for v in d))
             if nrm > 1e-12:
                 self.dir = tuple(v / nrm for v in d)
-        self.last_pos = (x, y, 0.0)
+        self.last_pos = (x, y, z)
 
     def _step(self, x, y, welding=True, dir_done=False):
         c, s, m = self.cfg, self.s, self.mat

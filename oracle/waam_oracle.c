@@ -1202,6 +1202,58 @@ static void deposit_cell(float* f_src, int32_t* flags, float* f_l, float* phi, f
     for (int q = 0; q < 19; ++q) f_src[q * n + c] = WQ(q) * rho0;
 }
 
+/* kernels.py:177-242 feed_wire -- serial lexicographic order of the
+ * reserve-then-commit budget over the droplet sphere and the column above
+ * the arc. */
+void wo_feed_wire(float* f_src, int32_t* flags, float* f_l, float* phi, float* H, float* T,
+                  float* rho, int nx, int ny, int nz, float arc_i, float arc_j, float arc_k,
+                  float drop_r, float target_vol, float T_drop, float cp_rho, float L_rho,
+                  float rho0, float* vol_acc, float cell_vol) {
+    int64_t n = (int64_t)nx * ny * nz;
+    float search_r = fmaxf_(drop_r * 2.5f, drop_r + 2.0f);
+    int i0 = imax(0, (int)(arc_i - search_r)), i1 = imin(nx, (int)(arc_i + search_r) + 1);
+    int j0 = imax(0, (int)(arc_j - search_r)), j1 = imin(ny, (int)(arc_j + search_r) + 1);
+    int k0 = imax(0, (int)(arc_k + 1.0f)), k1 = imin(nz, (int)(arc_k + search_r * 3.0f) + 1);
+    float drop_cz = arc_k + drop_r + 1.0f;
+    for (int i = i0; i < i1; ++i)
+        for (int j = j0; j < j1; ++j)
+            for (int k = k0; k < k1; ++k) {
+                if (*vol_acc >= target_vol) continue;
+                float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - drop_cz;
+                float r2 = di * di + dj * dj + dk * dk;
+                float rij2 = di * di + dj * dj;
+                int in_sphere = r2 <= drop_r * drop_r;
+                int in_column = rij2 <= search_r * search_r && (float)k >= arc_k + 1.0f;
+                int64_t c = IX(i, j, k);
+                if (!((in_sphere || in_column) && flags[c] == GAS)) continue;
+                float reserved = *vol_acc;
+                *vol_acc = reserved + cell_vol;
+                if (reserved >= target_vol)
+                    *vol_acc = *vol_acc - cell_vol;
+                else
+                    deposit_cell(f_src, flags, f_l, phi, H, T, rho, n, c, T_drop, cp_rho, L_rho,
+                                 rho0);
+            }
+}
+
+/* kernels.py:644-676 feed_wire_momentum */
+void wo_feed_wire_momentum(float* uz, const int32_t* flags, const float* f_l, int nx, int ny,
+                           int nz, float arc_i, float arc_j, float arc_k, float drop_r,
+                           float vz_lu) {
+    int i0 = imax(0, (int)(arc_i - drop_r)), i1 = imin(nx, (int)(arc_i + drop_r) + 1);
+    int j0 = imax(0, (int)(arc_j - drop_r)), j1 = imin(ny, (int)(arc_j + drop_r) + 1);
+    int k0 = imax(0, (int)arc_k), k1 = imin(nz, (int)(arc_k + drop_r * 2.0f) + 1);
+    for (int i = i0; i < i1; ++i)
+        for (int j = j0; j < j1; ++j)
+            for (int k = k0; k < k1; ++k) {
+                int64_t c = IX(i, j, k);
+                if (flags[c] == GAS) continue;
+                if (f_l[c] < 0.5f) continue;
+                float di = (float)i - arc_i, dj = (float)j - arc_j;
+                if (di * di + dj * dj <= drop_r * drop_r) uz[c] = fminf_(uz[c] + vz_lu, 0.15f);
+            }
+}
+
 /* kernels.py:278-400 feed_wire_surface -- serial lexicographic order of the
  * reserve-then-commit budget. */
 void wo_feed_wire_surface(float* f_src, int32_t* flags, float* f_l, float* phi, float* H,

@@ -113,6 +113,13 @@ void wo_solidify_cooled_metal(const float* T, float* f_l, float* phi, int32_t* f
                               float* uy, float* uz, int64_t n, float Ts, int zero_velocity);
 float wo_surface_height_at(const float* phi, const int32_t* flags, int nx, int ny, int nz, int i0,
                            int j0, int nz_fallback);
+void wo_feed_wire(float* f_src, int32_t* flags, float* f_l, float* phi, float* H, float* T,
+                  float* rho, int nx, int ny, int nz, float arc_i, float arc_j, float arc_k,
+                  float drop_r, float target_vol, float T_drop, float cp_rho, float L_rho,
+                  float rho0, float* vol_acc, float cell_vol);
+void wo_feed_wire_momentum(float* uz, const int32_t* flags, const float* f_l, int nx, int ny,
+                           int nz, float arc_i, float arc_j, float arc_k, float drop_r,
+                           float vz_lu);
 void wo_feed_wire_surface(float* f_src, int32_t* flags, float* f_l, float* phi, float* H,
                           float* T, float* rho, int nx, int ny, int nz, float arc_i, float arc_j,
                           float arc_k, float foot_r, float drop_r, float target_vol, float T_drop,

@@ -48,7 +48,7 @@ def full_inputs(name):
                 "tail": 10, "heat_loss": 11, "surface_height": 12, "deposit": 13,
                 "lorentz": 14, "tracers": 15, "refresh": 16, "thermal_var": 17, "phase_var": 18,
                 "forces_var": 19, "srt_var": 20, "tail_var": 21, "shift": 24, "derived": 25,
-                "weld_forces": 26}
+                "weld_forces": 26, "feed_wire": 27, "feed_wire_momentum": 28}
     grids = [v.shape[-3:] for v in ins.values() if v.ndim >= 3 and v.shape[-1] != 3]
     nx, ny, nz = grids[0] if grids else (13, 11, 12)   # tracer-only cases: the kernel-case grid
     st = state_gen.seeded_state(nx, ny, nz, seed=seed_map.get(name, 0))
@@ -217,6 +217,18 @@ def run_case(be, name, st, a):
                                          a["arc_i"], a["arc_j"], a["arc_k"], a["drop_r"],
                                          a["impact_pa"], a["dt"], a["dx"], 7800.0)
         return placed
+    elif name == "feed_wire":
+        acc, accs = 0.0, []
+        for arc_k, drop_r in zip(a["arc_ks"], a["drop_rs"]):
+            acc = be.feed_wire(st["f_a"], st["flags"], st["f_l"], st["phi"], st["H"], st["T"],
+                               st["rho"], nx, ny, nz, a["arc_i"], a["arc_j"], arc_k, drop_r,
+                               a["target_vol"], a["T_drop"], a["cp_rho"], a["L_rho"], a["rho0"],
+                               acc, a["cell_vol"])
+            accs.append(acc)
+        return accs
+    elif name == "feed_wire_momentum":
+        be.feed_wire_momentum(st["uz"], st["flags"], st["f_l"], nx, ny, nz, a["arc_i"], a["arc_j"],
+                              a["arc_k"], a["drop_r"], a["vz_lu"])
     elif name == "lorentz":
         rng = np.random.default_rng(31)
         for f in ("sigma_elec", "elec_source", "phi_elec_tmp", "Jx", "Jy", "Jz", "Bx", "By", "Bz"):
@@ -318,7 +330,7 @@ CASES = ["inject_gauss", "inject_goldak", "ceiling", "thermal", "thermal_s2", "p
          "tmax_cool", "vof", "vof_wet", "contact", "contact_s5", "forces", "forces_wet",
          "weld_forces", "csf",
          "csf_wet", "collide_mrt", "collide_srt", "stream", "tail", "heat_loss",
-         "surface_height", "deposit", "lorentz", "tracers", "refresh", "thermal_var",
+         "surface_height", "deposit", "feed_wire", "feed_wire_momentum", "lorentz", "tracers", "refresh", "thermal_var",
          "phase_var", "forces_var", "srt_var", "tail_var", "shift", "derived", "reset"]
 
 
@@ -335,6 +347,10 @@ def check_case(be, name):
         for got, ref in zip(extra, a["l1"]):
             for g_, r_ in zip(got, ref):
                 assert abs(g_ - r_) <= RTOL * abs(r_), (extra, a["l1"])
+    if name == "feed_wire":
+        # the budget accumulator is float32 in both: equal to the bit
+        assert [np.float32(v) for v in extra] == [np.float32(v) for v in a["vol_acc_after"]], (
+            extra, a["vol_acc_after"])
     if name == "deposit":
         for got, ref in zip(extra, a["placed"]):
             assert abs(got[1] - ref[1]) <= 1e-6 * max(ref[1], 1e-30) + 1e-30, (extra, a["placed"])
@@ -370,6 +386,13 @@ class OracleBackend:
 
     def elec_bins(self, Jz, bins, nx, ny, nz, arc_i, arc_j, dx, bin_dr, n_bins):
         self.O.call("wo_elec_bins", Jz, bins, nx, ny, nz, arc_i, arc_j, dx, bin_dr, n_bins)
+
+    def feed_wire(self, *args):
+        args = list(args)
+        acc = np.array([args[19]], dtype=np.float32)
+        args[19] = acc
+        self.O.call("wo_feed_wire", *args)
+        return float(acc[0])
 
     def feed_wire_surface(self, *args):
         args = list(args)

@@ -137,6 +137,15 @@ class CudaBackend:
                      ny, nz, i0, j0, nz_fallback, torch.cuda.current_stream().cuda_stream)
         return float(out.item())
 
+    def feed_wire(self, *args):
+        """waam_feed_wire on float32 populations (storage code 0)."""
+        args = list(args)
+        acc = np.array([args[19]], dtype=np.float32)
+        args[19] = acc
+        args.insert(1, 0)
+        self._run("feed_wire", args, None)
+        return float(acc[0])
+
     def feed_wire_surface(self, *args):
         args = list(args)
         vol = np.array([args[20]], dtype=np.float32).reshape(())

@@ -1,9 +1,13 @@
 """Generate the golden fixtures in this folder from the waam_twin reference.
 
 TEST INFRASTRUCTURE ONLY.  Run in a container that has the reference
-checkout (``WAAM_REFERENCE_ROOT``, default ``/root/reference``)::
+checkout, named by ``WAAM_REFERENCE_ROOT``::
 
-    python tests/golden/make_golden.py
+    WAAM_REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py [what ...]
+
+``what``: ``kernels``, ``kernel=<name>``, ``steps``, ``table_steps``,
+``telemetry``, ``run_path``, ``kat_materials``, ``kats`` or ``kat=<script>`` (one validation script, merged
+into the existing ``kat_reference.json``).
 
 Every fixture is produced by the reference's own, unmodified Taichi kernels
 (kernels.py, cumulant_kernel.py) or its own ``WAAMTwin.step`` /
@@ -17,8 +21,9 @@ semantics documented there.  Inputs are seeded synthetic states from
 * ``step_<case>.npz``: a short ``WAAMTwin.step`` run -- the full state before
   each step and after the last one (``s<n>_<field>``), the torch positions and
   the twin's derived scalars.
-* ``kat_<case>.json``: known-answer values of the reference's validation
-  scripts executed on the stand-in (Poiseuille, VOF mass, Goldak energy).
+* ``kat_reference.json``: known-answer values of the reference's validation
+  scripts executed on the stand-in (Poiseuille, VOF mass, Goldak energy,
+  Stefan, thermal diffusion, lid cavity, Rosenthal far field).
 """
 from __future__ import annotations
 
@@ -372,6 +377,32 @@ def c_deposit(tw, g):
     return a
 
 
+def c_feed_wire(tw, g):
+    """feed_wire (kernels.py:177-242) twice: the second call starts from the
+    budget the first one left, so the cut falls inside its box."""
+    a = scal(tw)
+    a.update(arc_i=6.3, arc_j=5.2, arc_k=float(tw.nz_solid), drop_rs=[0.6, 1.7],
+             arc_ks=[float(g.nz - 2), float(tw.nz_solid)], cell_vol=g.dx ** 3,
+             T_drop=tw.mat.T_liquidus + 500.0, rho0=1.0)
+    a["target_vol"] = 40.0 * g.dx ** 3
+    acc = []
+    for arc_k, drop_r in zip(a["arc_ks"], a["drop_rs"]):
+        K.feed_wire(g.f_a, g.flags, g.f_l, g.phi, g.H, g.T, g.rho, a["arc_i"], a["arc_j"], arc_k,
+                    drop_r, a["target_vol"], a["T_drop"], tw.cp_rho, tw.L_rho, a["rho0"],
+                    g.deposit_vol_buf, a["cell_vol"], g.FLAG_GAS, g.FLAG_FLUID, g.nx, g.ny, g.nz)
+        acc.append(float(g.deposit_vol_buf[None]))
+    a["vol_acc_after"] = acc
+    return a
+
+
+def c_feed_wire_momentum(tw, g):
+    a = scal(tw)
+    a.update(arc_i=5.6, arc_j=4.4, arc_k=float(tw.nz_solid - 2), drop_r=3.3, vz_lu=0.021)
+    K.feed_wire_momentum(g.ux, g.uy, g.uz, g.flags, g.f_l, a["arc_i"], a["arc_j"], a["arc_k"],
+                         a["drop_r"], a["vz_lu"], g.FLAG_GAS, g.nx, g.ny, g.nz)
+    return a
+
+
 LORENTZ_FIELDS = ["sigma_elec", "elec_source", "phi_elec", "phi_elec_tmp", "Jx", "Jy", "Jz",
                   "Bx", "By", "Bz", "elec_rad_bins", "Fx", "Fy", "Fz"]
 
@@ -620,6 +651,8 @@ def kernel_cases():
     kernel_case("heat_loss", c_heat_loss, ["H"], seed=11)
     kernel_case("surface_height", c_surface_height, ["phi"], seed=12)
     kernel_case("deposit", c_deposit, base + ["rho", "f_a", "ux", "uy", "uz", "Fz"], seed=13)
+    kernel_case("feed_wire", c_feed_wire, base + ["rho", "f_a"], seed=27)
+    kernel_case("feed_wire_momentum", c_feed_wire_momentum, ["ux", "uy", "uz"], seed=28)
     kernel_case("lorentz", c_lorentz, LORENTZ_FIELDS, seed=14, extra_in=lorentz_setup)
     kernel_case("weld_forces", c_weld_forces, ["T", "Fx", "Fy", "Fz"], seed=26,
                 extra_in=weld_forces_setup)
@@ -860,21 +893,101 @@ def telemetry_cases():
 # ---------------------------------------------------------------------------
 # known-answer values of the reference validation scripts
 # ---------------------------------------------------------------------------
-def kats():
-    import importlib
+def kat_materials():
+    """The material the validation scripts load (materials/placeholders/
+    ER70S-6.yaml through the reference's load_material), as a record."""
+    from waam_twin.materials import load_material
+    m = load_material("materials/placeholders/ER70S-6.yaml")
+    rec = {k: float(getattr(m, k)) for k in (
+        "k", "rho", "cp", "alpha", "T_solidus", "T_liquidus", "L_fusion", "gamma_0",
+        "dgamma_dT", "T_ref_gamma", "mu", "beta_T")}
+    rec = dict(constants=rec, name=m.name, status=m.status,
+               contact_angle_deg=float(m.contact_angle_deg),
+               tables={k: [list(map(float, r)) for r in getattr(m.tables, k)]
+                       for k in ("cp", "k", "mu", "dgamma_dT")})
+    with open(os.path.join(HERE, "kat_materials.json"), "w") as fh:
+        json.dump({"ER70S-6-placeholder": rec}, fh, indent=1, sort_keys=True)
+    print("kat materials", rec)
+
+
+class _PathRecorder:
+    """Stands in for a twin in the reference's ``WAAMTwin.run_path``: the
+    attributes that method reads, and a ``step`` that records its call."""
+
+    def __init__(self, nx, ny, dx, travel, interpass_attr=0, window_offset=0.0):
+        import types
+        self.grid = types.SimpleNamespace(nx=nx, ny=ny, dx=dx, dt=dx * 0.05 / 0.5)
+        self.travel_speed_m_s = travel
+        self._interpass_cooling_steps = interpass_attr
+        self._window_offset_x_m = window_offset
+        self._torch_dir_xyz = (1.0, 0.0, 0.0)
+        self.calls = []
+
+    def step(self, x, y, is_welding=True, torch_z_m=None):
+        self.calls.append([float(x), float(y), bool(is_welding), torch_z_m])
+
+
+RUN_PATH_CASES = {
+    # name: (job given as, n_steps, interpass argument, interpass attribute, window offset)
+    "yaml_interpass": ("yaml", 180, 7, 0, 0.0),
+    "yaml_attr_interpass": ("yaml", 150, 0, 5, 0.0),
+    "dict_default_steps": ("dict", None, 0, 0, 0.0),
+    "dict_window": ("dict", 120, 3, 0, 1.5e-3),
+    "empty_path": ("empty", 40, 0, 0, 0.0),
+}
+
+
+def run_path_cases():
+    """The reference's run_path (twin.py:632-704) on the recorder: every step
+    call (x, y, welding, z) and the seeded torch direction, for a job YAML, a
+    job dict, and a job without a path (tests/golden/job_path.yaml)."""
+    import yaml
+    job_file = os.path.join(HERE, "job_path.yaml")
+    with open(job_file) as fh:
+        job = yaml.safe_load(fh)
     out = {}
-    for name, kw in [("test_vof_mass", {}), ("test_goldak_energy", {}),
-                     ("test_lbm_poiseuille", {}), ("test_stefan_solidification", {})]:
+    for name, (kind, n, ip_arg, ip_attr, off) in RUN_PATH_CASES.items():
+        rec = _PathRecorder(48, 32, 2.5e-4, 2.5, ip_attr, off)
+        arg = {"yaml": job_file, "dict": job, "empty": {"job_name": "no_path"}}[kind]
+        wt.WAAMTwin.run_path(rec, arg, n_steps=n, interpass_steps=ip_arg)
+        out[name] = dict(calls=rec.calls, torch_dir=list(rec._torch_dir_xyz),
+                         nx=48, ny=32, dx=2.5e-4, travel=2.5, n_steps=n,
+                         interpass_steps=ip_arg, interpass_attr=ip_attr, window_offset=off,
+                         job=kind)
+        print("run_path", name, len(rec.calls), "steps")
+    with open(os.path.join(HERE, "run_path_reference.json"), "w") as fh:
+        json.dump(out, fh)
+
+
+KAT_SCRIPTS = ["test_vof_mass", "test_goldak_energy", "test_lbm_poiseuille",
+               "test_stefan_solidification", "test_thermal_diffusion", "test_lbm_cavity",
+               "test_rosenthal_farfield"]
+
+
+def kats(names=None):
+    """Run validation scripts of the reference (their own ``run()`` with its
+    default arguments) and merge their returned values into
+    kat_reference.json."""
+    import importlib
+    import time
+    path = os.path.join(HERE, "kat_reference.json")
+    out = {}
+    if os.path.exists(path):
+        with open(path) as fh:
+            out = json.load(fh)
+    for name in names or KAT_SCRIPTS:
+        t0 = time.time()
         mod = importlib.import_module("waam_twin.validation." + name)
-        out[name] = float(mod.run(**kw))
-    with open(os.path.join(HERE, "kat_reference.json"), "w") as fh:
-        json.dump(out, fh, indent=1, sort_keys=True)
-    print("kats", out)
+        out[name] = float(mod.run())
+        print("kat", name, out[name], "%.0f s" % (time.time() - t0), flush=True)
+        with open(path, "w") as fh:
+            json.dump(out, fh, indent=1, sort_keys=True)
 
 
 if __name__ == "__main__":
     what = sys.argv[1:] or ["kernels", "steps", "kats"]
     ONLY.update(w.split("=", 1)[1] for w in what if w.startswith("kernel="))
+    KAT_ONLY = [w.split("=", 1)[1] for w in what if w.startswith("kat=")]
     if "kernels" in what or ONLY:
         kernel_cases()
     if "steps" in what:
@@ -883,5 +996,9 @@ if __name__ == "__main__":
         table_step_cases()
     if "telemetry" in what:
         telemetry_cases()
-    if "kats" in what:
-        kats()
+    if "run_path" in what:
+        run_path_cases()
+    if "kat_materials" in what:
+        kat_materials()
+    if "kats" in what or KAT_ONLY:
+        kats(KAT_ONLY or None)

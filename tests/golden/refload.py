@@ -11,11 +11,17 @@ import sys
 import types
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE_ROOT = os.environ.get("WAAM_REFERENCE_ROOT", "/root/reference")
+REFERENCE_ROOT = os.environ.get("WAAM_REFERENCE_ROOT", "")
 
 
 def load():
-    """Return the imported reference package ``waam_twin`` (shim-backed)."""
+    """Return the imported reference package ``waam_twin`` (shim-backed).
+
+    ``WAAM_REFERENCE_ROOT`` names the reference checkout (the folder that
+    holds ``kernels.py`` and ``twin.py``)."""
+    if not REFERENCE_ROOT or not os.path.isfile(os.path.join(REFERENCE_ROOT, "kernels.py")):
+        raise RuntimeError("set WAAM_REFERENCE_ROOT to the waam_twin reference checkout "
+                           "(the folder with kernels.py); got %r" % REFERENCE_ROOT)
     shim = os.path.join(HERE, "taichi_shim")
     if shim not in sys.path:
         sys.path.insert(0, shim)

@@ -352,3 +352,33 @@ def test_moving_window_matches_oracle(kind, tables):
         assert np.array_equal(g.porosity_active.cpu().numpy(), ot.s["porosity_active"])
         steps.compare("tracers", g.porosity_pos.cpu().numpy(), ot.s["porosity_pos"],
                       "porosity_pos")
+
+
+def test_operator_calls_after_pipelined_steps_see_streamed_populations():
+    """After fused steps that leave their stream (and collision) pending, the
+    kept operator API reads g.f_src / g.f_dst through the grid, which runs the
+    pending work first: an operator-API collide + stream + swap after the
+    steps gives, bit for bit, the state of the same calls after in-order
+    steps."""
+    from waam_solver_b200.physics import lbm
+    states = []
+    for pipelined in (False, True):
+        tw, ot, dx = _config_twins("c2", 40, 24, 24)
+        tw.pipeline_stream = tw.pipeline_collide = pipelined
+        tw._last_droplet_time = -1.0
+        for s in range(9):
+            tw.step(0.3 * 40 * dx + s * 1e-6, 12 * dx, True)
+        g = tw.grid
+        if pipelined:
+            assert g._stream_pending and g._collide_pending
+        lbm.collide_mrt(g.f_src, g.f_dst, g.rho, g.ux, g.uy, g.uz, g.Fx, g.Fy, g.Fz, g.f_l,
+                        g.flags, g.ex, g.ey, g.ez, g.w, g.opp, tw.omega, tw.omega_bulk,
+                        tw.C_darcy, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+        assert not g._stream_pending and not g._collide_pending
+        lbm.stream(g.f_dst, g.f_src, g.flags, g.FLAG_SOLID, g.FLAG_GAS, g.nx, g.ny, g.nz)
+        g.swap_buffers()
+        torch.cuda.synchronize()
+        states.append(g.state_dict())
+    for k, v in states[0].items():
+        if isinstance(v, np.ndarray):
+            assert np.array_equal(v, states[1][k]), k

@@ -283,7 +283,7 @@ def _fields(g):
     f = _native.WaamFields()
     g.ensure_vof_buffers()
     r = lambda name: raw_field(g, name)  # noqa: E731  (no flush of pending work)
-    for name, t in (("f_src", g.f_src), ("f_dst", g.f_dst), ("rho", r("rho")), ("ux", r("ux")),
+    for name, t in (("f_src", r("f_src")), ("f_dst", r("f_dst")), ("rho", r("rho")), ("ux", r("ux")),
                     ("uy", r("uy")), ("uz", r("uz")), ("T", g.T), ("T_next", g.T_next), ("H", g.H),
                     ("H_next", g.H_next), ("f_l", g.f_l), ("phi", g.phi),
                     ("phi_tmp", g.phi_tmp), ("flags", g.flags), ("T_max", g.T_max),
@@ -426,7 +426,7 @@ def upload_position(twin, arc_i, arc_j):
 def _fields_cached(g, lorentz=False):
     """WaamFields for the current buffer parity (device pointers never move);
     ``lorentz``: with the current density and self field the collision adds."""
-    key = (g._read_buf is g.f_a, g._cur, lorentz, getattr(g, "_flags_copy_i", 0))
+    key = (g._read_buf is raw_field(g, "f_a"), g._cur, lorentz, getattr(g, "_flags_copy_i", 0))
     cache = g.__dict__.setdefault("_fields_cache", {})
     f = cache.get(key)
     if f is None:
@@ -551,7 +551,7 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
                             getattr(twin, "pipeline_collide", True)) else 0
     done = False
     if not due and not lorentz and events is None and getattr(twin, "use_cuda_graphs", True):
-        key = (g._read_buf is g.f_a, g._cur, p.welding, p.clear_forces, p.stream_prev,
+        key = (g._read_buf is raw_field(g, "f_a"), g._cur, p.welding, p.clear_forces, p.stream_prev,
                p.defer_stream, p.collide_prev, p.collide_prev_welding, p.defer_collide,
                g._flags_copy_i,
                (dx_, dy_, dz_) if twin.enable_bead_freeze else None)

@@ -691,6 +691,121 @@ __global__ void k_momentum_impact(Dims d, void* f_src, int storage, const float*
     }
 }
 
+// Block-wide exclusive scan of one 0/1 value per thread (blockDim.x a multiple
+// of 32, at most 1024); returns the thread's prefix, *total the block's sum.
+__device__ __forceinline__ unsigned block_scan01(unsigned v, unsigned* total) {
+    __shared__ unsigned warp_sum[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned m = __ballot_sync(0xffffffffu, v != 0u);
+    const unsigned in_warp = __popc(m & ((1u << lane) - 1u));
+    if (lane == 0) warp_sum[warp] = __popc(m);
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    unsigned before = 0, all = 0;
+    for (int w = 0; w < nw; ++w) {
+        const unsigned s = warp_sum[w];
+        before += w < warp ? s : 0u;
+        all += s;
+    }
+    __syncthreads();   // warp_sum is reused by the next call
+    *total = all;
+    return before + in_warp;
+}
+
+// kernels.py:177-242 feed_wire: in the box around the arc, a GAS cell inside
+// the droplet sphere or the column above the arc becomes liquid metal while
+// the volume budget lasts.  Serially (lexicographic i, j, k) each eligible
+// cell is taken while the float32 accumulator is below the target, so the
+// cells taken are the first `take` eligible cells in that order: one thread
+// replays the accumulation to find `take`, then the block converts the first
+// `take` eligible cells chunk by chunk with a block scan.  One CTA.
+__global__ void __launch_bounds__(1024) k_feed_wire(
+    Dims d, void* f_src, int storage, int32_t* flags, float* f_l, float* phi, float* H, float* T,
+    float* rho, float arc_i, float arc_j, float arc_k, float drop_r, float search_r,
+    float target_vol, float T_drop, float cp_rho, float L_rho, float rho0, float* vol_acc,
+    float cell_vol, int i0, int i1, int j0, int j1, int k0, int k1) {
+    const int nj = j1 - j0, nk = k1 - k0;
+    const int64_t m = (int64_t)(i1 - i0) * nj * nk;
+    const int64_t n = d.n();
+    const float drop_cz = arc_k + drop_r + 1.0f;
+    auto cell_of = [&](int64_t t) -> int64_t {
+        const int k = k0 + (int)(t % nk);
+        const int j = j0 + (int)((t / nk) % nj);
+        const int i = i0 + (int)(t / ((int64_t)nk * nj));
+        return d.idx(i, j, k);
+    };
+    auto eligible = [&](int64_t t) -> bool {
+        const int k = k0 + (int)(t % nk);
+        const int j = j0 + (int)((t / nk) % nj);
+        const int i = i0 + (int)(t / ((int64_t)nk * nj));
+        const float di = (float)i - arc_i, dj = (float)j - arc_j, dk = (float)k - drop_cz;
+        const float r2 = di * di + dj * dj + dk * dk;
+        const float rij2 = di * di + dj * dj;
+        const bool in_sphere = r2 <= drop_r * drop_r;
+        const bool in_column = rij2 <= search_r * search_r && (float)k >= arc_k + 1.0f;
+        return (in_sphere || in_column) && flags[d.idx(i, j, k)] == GAS;
+    };
+    __shared__ unsigned s_take;
+    unsigned total = 0, local = 0;
+    for (int64_t t = threadIdx.x; t < m; t += blockDim.x) local += eligible(t) ? 1u : 0u;
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+    __shared__ unsigned warp_tot[32];
+    if ((threadIdx.x & 31) == 0) warp_tot[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) total += warp_tot[w];
+        float acc = *vol_acc;
+        unsigned take = 0;
+        while (take < total && acc < target_vol) {
+            acc = acc + cell_vol;
+            ++take;
+        }
+        *vol_acc = acc;
+        s_take = take;
+    }
+    __syncthreads();
+    const unsigned take = s_take;
+    unsigned base = 0;
+    for (int64_t t0 = 0; t0 < m && base < take; t0 += blockDim.x) {
+        const int64_t t = t0 + threadIdx.x;
+        const bool e = t < m && eligible(t);
+        unsigned chunk = 0;
+        const unsigned rank = block_scan01(e ? 1u : 0u, &chunk);
+        if (e && base + rank < take) {
+            const int64_t c = cell_of(t);
+            flags[c] = FLUID;
+            f_l[c] = 1.0f;
+            phi[c] = 1.0f;
+            T[c] = T_drop;
+            H[c] = cp_rho * T_drop + L_rho;
+            rho[c] = rho0;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) pop_store(f_src, q * n + c, q, wq(q) * rho0, storage);
+        }
+        base += chunk;
+    }
+}
+
+// kernels.py:644-676 feed_wire_momentum: downward droplet momentum for the
+// liquid (f_l >= 0.5), non-gas cells of the column under the droplet.
+__global__ void k_feed_wire_momentum(Dims d, float* uz, const int32_t* flags, const float* f_l,
+                                     float arc_i, float arc_j, float drop_r, float vz_lu, int i0,
+                                     int i1, int j0, int j1, int k0, int k1) {
+    const int nj = j1 - j0, nk = k1 - k0;
+    const int64_t m = (int64_t)(i1 - i0) * nj * nk;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int k = k0 + (int)(t % nk);
+        const int j = j0 + (int)((t / nk) % nj);
+        const int i = i0 + (int)(t / ((int64_t)nk * nj));
+        const int64_t c = d.idx(i, j, k);
+        if (flags[c] == GAS) continue;
+        if (f_l[c] < 0.5f) continue;
+        const float di = (float)i - arc_i, dj = (float)j - arc_j;
+        if (di * di + dj * dj <= drop_r * drop_r) uz[c] = fmin_(uz[c] + vz_lu, 0.15f);
+    }
+}
+
 __global__ void k_impact_pressure(Dims d, float* Fz, const int32_t* flags, const float* phi,
                                   const float* f_l, float arc_i, float arc_j, float arc_k,
                                   float drop_r, float inv2s2, float Flu) {
@@ -1262,6 +1377,51 @@ int waam_feed_wire_momentum_impact(float* f_src, const float* rho, float* ux, fl
     return waam_feed_wire_momentum_impact_stored(f_src, waam::kStoreF32, rho, ux, uy, uz, flags,
                                                  f_l, nx, ny, nz, arc_i, arc_j, arc_k, drop_r, vx,
                                                  vy, vz, stream);
+}
+
+int waam_feed_wire(void* f_src, int f_storage, int32_t* flags, float* f_l, float* phi, float* H,
+                   float* T, float* rho, int nx, int ny, int nz, float arc_i, float arc_j,
+                   float arc_k, float drop_r, float target_vol, float T_drop, float cp_rho,
+                   float L_rho, float rho0, float* vol_acc, float cell_vol, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "feed_wire: bad dims");
+    REQUIRE(f_src && flags && f_l && phi && H && T && rho && vol_acc, "feed_wire: null field");
+    REQUIRE(f_storage >= waam::kStoreF32 && f_storage <= waam::kStoreBF16,
+            "feed_wire: f_storage must be 0, 1 or 2");
+    REQUIRE(std::isfinite(arc_i) && std::isfinite(arc_j) && std::isfinite(arc_k) &&
+                std::isfinite(drop_r) && drop_r >= 0.0f && fabsf(arc_i) < 1e7f &&
+                fabsf(arc_j) < 1e7f && fabsf(arc_k) < 1e7f && drop_r < 1e6f,
+            "feed_wire: arc position or droplet radius out of range");
+    // kernels.py:211-217: the search box (ti.cast truncates toward zero)
+    const float search_r = fmax_(drop_r * 2.5f, drop_r + 2.0f);
+    const int i0 = imax(0, (int)(arc_i - search_r)), i1 = imin(nx, (int)(arc_i + search_r) + 1);
+    const int j0 = imax(0, (int)(arc_j - search_r)), j1 = imin(ny, (int)(arc_j + search_r) + 1);
+    const int k0 = imax(0, (int)(arc_k + 1.0f)), k1 = imin(nz, (int)(arc_k + search_r * 3.0f) + 1);
+    if (i1 <= i0 || j1 <= j0 || k1 <= k0) return WAAM_OK;
+    k_feed_wire<<<1, 1024, 0, STREAM(stream)>>>(Dims{nx, ny, nz}, f_src, f_storage, flags, f_l,
+                                                 phi, H, T, rho, arc_i, arc_j, arc_k, drop_r,
+                                                 search_r, target_vol, T_drop, cp_rho, L_rho,
+                                                 rho0, vol_acc, cell_vol, i0, i1, j0, j1, k0, k1);
+    return waam::check_launch("k_feed_wire");
+}
+
+int waam_feed_wire_momentum(float* uz, const int32_t* flags, const float* f_l, int nx, int ny,
+                            int nz, float arc_i, float arc_j, float arc_k, float drop_r,
+                            float vz_lu, void* stream) {
+    REQUIRE(dims_ok(nx, ny, nz), "feed_wire_momentum: bad dims");
+    REQUIRE(uz && flags && f_l, "feed_wire_momentum: null field");
+    REQUIRE(std::isfinite(arc_i) && std::isfinite(arc_j) && std::isfinite(arc_k) &&
+                std::isfinite(drop_r) && fabsf(arc_i) < 1e7f && fabsf(arc_j) < 1e7f &&
+                fabsf(arc_k) < 1e7f && fabsf(drop_r) < 1e6f,
+            "feed_wire_momentum: arc position or droplet radius out of range");
+    // kernels.py:662-667
+    const int i0 = imax(0, (int)(arc_i - drop_r)), i1 = imin(nx, (int)(arc_i + drop_r) + 1);
+    const int j0 = imax(0, (int)(arc_j - drop_r)), j1 = imin(ny, (int)(arc_j + drop_r) + 1);
+    const int k0 = imax(0, (int)arc_k), k1 = imin(nz, (int)(arc_k + drop_r * 2.0f) + 1);
+    if (i1 <= i0 || j1 <= j0 || k1 <= k0) return WAAM_OK;
+    const int64_t m = (int64_t)(i1 - i0) * (j1 - j0) * (k1 - k0);
+    k_feed_wire_momentum<<<waam::elem_blocks(m), kThreads, 0, STREAM(stream)>>>(
+        Dims{nx, ny, nz}, uz, flags, f_l, arc_i, arc_j, drop_r, vz_lu, i0, i1, j0, j1, k0, k1);
+    return waam::check_launch("k_feed_wire_momentum");
 }
 
 int waam_apply_droplet_impact_pressure(float* Fz, const int32_t* flags, const float* phi,

@@ -216,10 +216,14 @@ class WAAMGrid:
 
     @property
     def f_src(self):
+        """The buffer the next collision reads (runs pending step work first)."""
+        self.flush_stream()
         return self._read_buf
 
     @property
     def f_dst(self):
+        """The buffer the next collision writes (runs pending step work first)."""
+        self.flush_stream()
         return self._write_buf
 
     # -- population storage -------------------------------------------------
@@ -232,7 +236,8 @@ class WAAMGrid:
     def flush_stream(self):
         """Run the work a pipelined step left pending -- its stream, or its
         collision, tracers and stream (see coupled_step)."""
-        if getattr(self, "_stream_pending", False) or getattr(self, "_collide_pending", False):
+        d = self.__dict__
+        if d.get("_stream_pending", False) or d.get("_collide_pending", False):
             from .coupled_step import flush_stream
             flush_stream(self)
 
@@ -329,9 +334,38 @@ for _name in _COLLIDE_OUTPUTS:
     setattr(WAAMGrid, _name, _collide_output(_name))
 
 
+# The population buffers: a pipelined step leaves its stream (and possibly its
+# collision) pending, so reading f_a / f_b / f_src / f_dst through the grid
+# runs that work first and the caller sees the step's streamed populations.
+_POPULATIONS = ("f_a", "f_b")
+
+
+def _population(name):
+    key = "_pf_" + name
+
+    def get(self):
+        self.flush_stream()
+        return self.__dict__[key]
+
+    def put(self, value):
+        self.__dict__[key] = value
+
+    return property(get, put, doc="%s (runs pending step work first)" % name)
+
+
+for _name in _POPULATIONS:
+    setattr(WAAMGrid, _name, _population(_name))
+
+
 def raw_field(g, name):
-    """A collision output without running pending work (the step's own use)."""
-    return g.__dict__["_pf_" + name] if name in _COLLIDE_OUTPUTS else getattr(g, name)
+    """A field without running pending step work (the step's own use)."""
+    if name in _COLLIDE_OUTPUTS or name in _POPULATIONS:
+        return g.__dict__["_pf_" + name]
+    if name == "f_src":
+        return g._read_buf
+    if name == "f_dst":
+        return g._write_buf
+    return getattr(g, name)
 
 
 def cells_of(mm, dx):

@@ -162,6 +162,33 @@ def surface_height_at(phi, flags, out, i0, j0, nz_fallback, FLAG_GAS, nz):
 
 
 # ---------------------------------------------------------- deposition ----
+def feed_wire(f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j, arc_k, droplet_radius, target_vol,
+              T_drop, cp_rho, L_rho, rho0, vol_acc, cell_vol, FLAG_GAS, FLAG_FLUID, nx, ny, nz):
+    """kernels.py:177-242: GAS cells in the droplet sphere or the column above
+    the arc become liquid metal while ``vol_acc`` (0-d device float) is below
+    ``target_vol``, in serial lexicographic order."""
+    _flags_ok(FLAG_GAS=FLAG_GAS, FLAG_FLUID=FLAG_FLUID)
+    n = int(nx) * int(ny) * int(nz)
+    fp, storage = _pop(f_src, 19 * n)
+    _call("waam_feed_wire", fp, storage, _i(flags, n), _f(f_l, n), _f(phi, n), _f(H, n), _f(T, n),
+          _f(rho, n), int(nx), int(ny), int(nz), float(arc_i), float(arc_j), float(arc_k),
+          float(droplet_radius), float(target_vol), float(T_drop), float(cp_rho), float(L_rho),
+          float(rho0), _f(vol_acc, 1), float(cell_vol), _stream())
+
+
+def feed_wire_momentum(ux, uy, uz, flags, f_l, arc_i, arc_j, arc_k, droplet_radius, vz_lu,
+                       FLAG_GAS, nx, ny, nz):
+    """kernels.py:644-676: uz = min(uz + vz_lu, 0.15) for the liquid, non-gas
+    cells of the droplet's column (ux and uy are not touched)."""
+    _flags_ok(FLAG_GAS=FLAG_GAS)
+    n = int(nx) * int(ny) * int(nz)
+    _f(ux, n)
+    _f(uy, n)
+    _call("waam_feed_wire_momentum", _f(uz, n), _i(flags, n), _f(f_l, n), int(nx), int(ny),
+          int(nz), float(arc_i), float(arc_j), float(arc_k), float(droplet_radius), float(vz_lu),
+          _stream())
+
+
 def feed_wire_surface(f_src, flags, f_l, phi, H, T, rho, arc_i, arc_j, arc_k, footprint_r,
                       droplet_radius, target_vol, T_drop, cp_rho, L_rho, rho0, vol_acc, real_acc,
                       cell_vol, FLAG_GAS, FLAG_FLUID, FLAG_SOLID, nx, ny, nz):

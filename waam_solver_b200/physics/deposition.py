@@ -13,7 +13,9 @@ from .deposition_balance import (  # noqa: F401
     wire_mass_flux_kg_s,
 )
 
+feed_wire = kernels.feed_wire
 feed_wire_surface = kernels.feed_wire_surface
+feed_wire_momentum = kernels.feed_wire_momentum
 
 
 def deposition_footprint_cells(twin, drop_r=None) -> float:
@@ -23,7 +25,7 @@ def deposition_footprint_cells(twin, drop_r=None) -> float:
 
 
 __all__ = [
-    "feed_wire_surface", "deposition_footprint_cells", "droplet_mass_for_interval_kg",
-    "wire_mass_flux_kg_s", "droplet_mass_kg", "droplet_period_s", "droplet_radius_cells",
+    "feed_wire", "feed_wire_surface", "feed_wire_momentum", "deposition_footprint_cells",
+    "droplet_mass_for_interval_kg", "wire_mass_flux_kg_s", "droplet_mass_kg", "droplet_period_s", "droplet_radius_cells",
     "droplet_radius_cells_from_mass_kg", "expected_deposited_mass_kg", "infer_transfer_mode",
 ]

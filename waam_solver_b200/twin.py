@@ -25,7 +25,7 @@ from .physics.deposition_balance import (droplet_mass_kg, expected_deposited_mas
                                          infer_transfer_mode, wire_mass_flux_kg_s)
 from .physics.electrical_stickout import droplet_entry_temperature_K
 from .physics.weld_forces import arc_pressure_peak_pa, droplet_impact_velocity_m_s
-from .torch_path import TorchPathDriver, clamp_torch_to_domain, parse_torch_path
+from .torch_path import plan_path, run_path
 
 RHO_LATTICE = 1.0
 log = logging.getLogger("waam_solver_b200")
@@ -358,47 +358,14 @@ class WAAMTwin:
             self.step(torch_x_m, torch_y_m, is_welding)
 
     def path_positions(self, job, n_steps=None):
-        """(x, y, z) torch positions of run_path, as a list (twin.py:632-704)."""
-        waypoints = parse_torch_path(job) if isinstance(job, dict) else list(job)
-        g = self.grid
-        if not waypoints:
-            waypoints = [(0.01, (g.ny // 2) * g.dx, 0.0)]
-        driver = TorchPathDriver(waypoints, self.travel_speed_m_s)
-        if n_steps is None:
-            n_steps = max(400, int(driver.total_length / max(self.travel_speed_m_s * g.dt, 1e-12)))
-        if driver.segments:
-            s0 = driver.segments[0]
-            d = (s0.x1 - s0.x0, s0.y1 - s0.y0, s0.z1 - s0.z0)
-            norm = math.sqrt(sum(v * v for v in d))
-            if norm > 1e-12:
-                self._torch_dir_xyz = tuple(v / norm for v in d)
-        out = []
-        for step, x, y, z in driver.positions_for_steps(n_steps, g.dt):
-            seg = driver.segment_index_at_distance(driver.distance_at_step(step, g.dt))
-            out.append((step, seg, x, y, z))
-        return driver, out
+        """(driver, [(step, segment, x, y, z), ...]) of run_path (twin.py:632-704);
+        ``job``: a job dict, a job YAML path or a sequence of (x, y, z) [m]."""
+        return plan_path(self, job, n_steps)
 
     def run_path(self, job, n_steps=None, is_welding=True, interpass_steps=0):
-        """Follow the job's torch path at travel speed, with interpass parking."""
-        driver, pos = self.path_positions(job, n_steps)
-        g = self.grid
-        interpass = int(interpass_steps) if interpass_steps else int(self._interpass_cooling_steps or 0)
-        prev_seg = -1
-
-        def clamp(x, y):
-            off = self._window_offset_x_m
-            cx, cy = clamp_torch_to_domain(x - off, y, g.nx, g.ny, g.dx)
-            return cx + off, cy
-
-        for step, seg, x, y, z in pos:
-            if interpass > 0 and seg > prev_seg >= 0:
-                park = driver.segment_end(prev_seg) or (x, y, z)
-                for _ in range(interpass):
-                    cx, cy = clamp(park[0], park[1])
-                    self.step(cx, cy, is_welding=False, torch_z_m=park[2])
-            prev_seg = seg
-            cx, cy = clamp(x, y)
-            self.step(cx, cy, is_welding, torch_z_m=z)
+        """Follow the job's torch path at travel speed, with interpass parking
+        (twin.py:632-704); ``job`` as in ``path_positions``."""
+        run_path(self, job, n_steps, is_welding, interpass_steps)
 
     # -- export (twin.py:701-869) --------------------------------------------
     def export_haz_vtk(self, path="haz_map.vti"):
