@@ -51,7 +51,7 @@ WORKLOADS = {
         droplet_freq_hz=100.0, wire_feed_m_s=0.1, wire_diameter_mm=1.2, enable_vof=True,
         enable_wetting=True, contact_angle_deg=30.0, enable_csf_tension=True,
         enable_hydrostatic_gravity=True, use_srt=False, travel_speed_m_s=0.008,
-        path_mm=((5.6, 12.8), (45.6, 12.8)), spinup=1200),
+        path_mm=((5.6, 12.8), (45.6, 12.8)), spinup=200),
     "small": dict(
         workload="bead-on-plate 64x32x32 D3Q19, dx 0.25 mm, Gaussian 3 kW r 3 mm, no wire, VOF, "
                  "central-moment MRT",
@@ -201,22 +201,29 @@ class ClockSampler:
             self.lines = [ln for ln in out.splitlines() if ln.strip()]
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
+        """Median SM clock of the samples taken under load (power draw at least
+        half of the run's maximum), the maximum clock, and every throttle
+        reason seen in any sample of the run."""
+        rows, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in getattr(self, "lines", []):
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
+                sm_mhz, smax, pw = float(parts[1]), float(parts[2]), float(parts[3])
             except ValueError:
                 continue
+            rows.append((sm_mhz, pw))
             for nm, val in zip(names, parts[5:9]):
                 if val.lower() == "active":
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        pmax = max((pw for _, pw in rows), default=0.0)
+        load = [m for m, pw in rows if pw >= 0.5 * pmax]
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(rows), "samples_under_load": len(load),
+                "coverage": "the whole run: spin-up, timed steps, stage timing, end-to-end "
+                            "and droplet-period timing (nvidia-smi every 200 ms)"}
 
 
 def census(twin):
@@ -290,7 +297,8 @@ def barrier():
 
 def cpu_baseline(w, budget_s=15.0, max_steps=400):
     """The CPU oracle (C restatement, OpenMP on all host cores) on the same
-    workload: reset, then as many full steps as fit the time budget."""
+    workload and state as the GPU arm: reset, the workload's spin-up steps on
+    the same torch path, then as many full steps as fit the time budget."""
     from oracle.oracle_step import OracleTwin
     from oracle import oracle as O
     threads = os.cpu_count() or 1
@@ -313,18 +321,25 @@ def cpu_baseline(w, budget_s=15.0, max_steps=400):
     mat = dict(MATERIAL, contact_angle_deg=w.get("contact_angle_deg", 30.0))
     ot = OracleTwin(w["nx"], w["ny"], w["nz"], w["dx"], mat, goldak=g, **kw, **extra)
     ot.reset()
-    pos = positions(w, ot.dt, max_steps + 1)
-    ot.step(*pos[0], True)  # warm-up (page-in, thread pool)
+    spin = int(w["spinup"])
+    pos = path_steps(w, ot.dt, spin + max_steps)
+    t_spin = time.perf_counter()
+    for x, y, wl in pos[:spin]:
+        ot.step(x, y, wl)
+    t_spin = time.perf_counter() - t_spin
+    d0 = ot.n_drops
     t0 = time.perf_counter()
     n = 0
     while n < max_steps and (time.perf_counter() - t0) < budget_s:
-        ot.step(*pos[n + 1], True)
+        ot.step(*pos[spin + n])
         n += 1
     el = time.perf_counter() - t0
     cells = w["nx"] * w["ny"] * w["nz"]
     return {"value": cells * n / el / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
-            "sample": "%d full steps of the %dx%dx%d workload after reset (%.1f s)" % (
-                n, w["nx"], w["ny"], w["nz"], el)}
+            "droplets": ot.n_drops - d0,
+            "sample": "%d full steps of the %dx%dx%d workload after reset and the same %d "
+                      "spin-up steps as the GPU arm (spin-up %.1f s, timed %.1f s)" % (
+                          n, w["nx"], w["ny"], w["nz"], spin, t_spin, el)}
 
 
 def run_reference(args, w):
@@ -337,7 +352,8 @@ def run_reference(args, w):
     line = {"impl": "reference", "metric": "coupled step throughput (MLUPS)", "value": cb["value"],
             "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": w["workload"]}, "cpu_baseline": cb,
+            "data": "synthetic (reference reset state + %d spin-up steps)" % w["spinup"],
+            "config": bench_config(w, world, 4, cb["droplets"]), "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -649,15 +665,59 @@ def storage_comparison(w, device, n_steps):
     return out
 
 
+def bench_config(w, world, pb, drops):
+    """The workload record both arms print (identical keys and values)."""
+    cells = w["nx"] * w["ny"] * w["nz"]
+    return {"workload": w["workload"], "cells": cells, "global_batch": world,
+            "parallelism": "replicas x%d" % world,
+            "l2": "inputs larger than L2 (populations %.0f MB)" % (2 * 19 * cells * pb / 1e6),
+            "population_storage": "float16" if pb == 2 else "float32",
+            "spinup_steps": w["spinup"], "droplets_in_timed_region": drops}
+
+
+def droplet_period_steps(tw):
+    """Steps per droplet of the twin's schedule (None without wire droplets)."""
+    from waam_solver_b200.physics import deposition
+    if tw.droplet_freq <= 0 or tw.wire_feed_m_s <= 0:
+        return None
+    return max(1, int(math.ceil(deposition.droplet_period_s(tw) / tw.grid.dt)))
+
+
+def droplet_period_timing(tw, pos, s, period, device):
+    """Whole-step time over one droplet period (the droplet step included),
+    CUDA events around all steps, positions staged on the device."""
+    import torch
+    g = tw.grid
+    dev_pos = torch.tensor([[x / g.dx, y / g.dx] for x, y, _ in pos[s:s + period]],
+                           dtype=torch.float32, device=device)
+    d0 = tw._n_droplets_fired
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(period):
+        tw._device_position = dev_pos[k]
+        tw.step(*pos[s + k])
+    e1.record()
+    torch.cuda.synchronize()
+    tw._device_position = None
+    ms = e0.elapsed_time(e1) / period
+    return {"steps": period, "droplets": tw._n_droplets_fired - d0, "ms_per_step": ms,
+            "value": g.n_cells / (ms * 1e-3) / 1e6, "unit": "MLUPS",
+            "deposited_m3": tw._deposited_volume_m3}
+
+
 def run_b200(args, w):
     import torch
     from waam_solver_b200 import _native
     world, rank, local = dist_setup()
     device = torch.device("cuda", local)
+    clocks = ClockSampler(local).__enter__()     # sampled over the whole run
     tw = build_twin(w, device)
     g = tw.grid
     cells = g.n_cells
-    total = w["spinup"] + args.warmup + 2 * args.steps + min(args.steps, 400) + 4
+    period = droplet_period_steps(tw)
+    total = (w["spinup"] + args.warmup + 2 * args.steps + min(args.steps, 400) + 4 +
+             (period or 0))
     pos = path_steps(w, g.dt, total)
     lorentz = bool(w.get("enable_lorentz"))
     pb = 2 if g.population_storage else 4
@@ -677,16 +737,15 @@ def run_b200(args, w):
     barrier()
     torch.cuda.synchronize()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        t_host = time.perf_counter()
-        start.record()
-        for k in range(K):
-            tw._device_position = dev_pos[k]
-            tw.step(*pos[s])
-            s += 1
-        stop.record()
-        host_ms = (time.perf_counter() - t_host) * 1e3 / K
-        torch.cuda.synchronize()
+    t_host = time.perf_counter()
+    start.record()
+    for k in range(K):
+        tw._device_position = dev_pos[k]
+        tw.step(*pos[s])
+        s += 1
+    stop.record()
+    host_ms = (time.perf_counter() - t_host) * 1e3 / K
+    torch.cuda.synchronize()
     tw._device_position = None
     barrier()
     ms_local = start.elapsed_time(stop)
@@ -780,6 +839,14 @@ def run_b200(args, w):
     barrier()
     ms_e2e = dist_max(e0.elapsed_time(e1))
 
+    # ---- one droplet period, droplet step included (it runs eagerly and reads
+    # back the placed volume); device-resident positions as for `value` ----
+    drop_info = None
+    if period:
+        drop_info = droplet_period_timing(tw, pos, s, period, device)
+        s += period
+    clocks.__exit__(None, None, None)
+
     value = world * cells * K / (ms * 1e-3) / 1e6
     e2e = world * cells * K / (ms_e2e * 1e-3) / 1e6
     line = {
@@ -787,11 +854,7 @@ def run_b200(args, w):
         "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (reference reset state + %d spin-up steps)" % w["spinup"],
-        "config": {"workload": w["workload"], "cells": cells, "global_batch": world,
-                   "parallelism": "replicas x%d" % world, "l2": "inputs larger than L2 "
-                   "(populations %.0f MB)" % (2 * 19 * cells * pb / 1e6),
-                   "population_storage": "float16" if pb == 2 else "float32",
-                   "droplets_in_timed_region": drops},
+        "config": bench_config(w, world, pb, drops),
         "roofline": {"bound": "hbm", "kernel": kernel,
                      "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "peak_source": hbm_src,
@@ -810,6 +873,8 @@ def run_b200(args, w):
                             "checks)" if lorentz else "replay CUDA graphs"),
         "clocks": clocks.summary(),
     }
+    if drop_info:
+        line["droplet_period"] = drop_info
     if lz_info:
         line["lorentz"] = lz_info
     standard = "beads" not in w

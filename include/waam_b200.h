@@ -639,7 +639,18 @@ typedef struct WaamFields {
      * collision.  The caller alternates two buffers from step to step. */
     int32_t* flags_copy_w;
     const int32_t* flags_copy_r;
+    /* health word of the fused step (null: off), device uint32 that the
+     * kernels OR bits into (WAAM_HEALTH_*): the thermal stage when a non-gas
+     * cell's enthalpy is not finite, the collision when an active cell's
+     * density or velocity is not finite or its density lies outside
+     * [WaamStepParams.rho_lo, rho_hi].  Nothing clears it; the caller reads
+     * it where it synchronises anyway and zeroes it when it wants. */
+    uint32_t* status;
 } WaamFields;
+
+#define WAAM_HEALTH_NONFINITE_H 1u   /* H of a non-gas cell is NaN or infinite */
+#define WAAM_HEALTH_NONFINITE_LBM 2u /* density or velocity of an active cell not finite */
+#define WAAM_HEALTH_RHO_RANGE 4u     /* density of an active cell outside [rho_lo, rho_hi] */
 
 typedef struct WaamStepParams {
     /* torch position (solvers/coupled_step.py:92-94); the kernels read it from
@@ -729,6 +740,9 @@ typedef struct WaamStepParams {
     float gs_tau_pa;
     int recoil;
     float recoil_pa, recoil_T_ref, P_ref, T_boil, L_vap, R_spec, C_acc, weld_sigma;
+    /* density band of the health word's WAAM_HEALTH_RHO_RANGE bit (the check
+     * is off when rho_hi <= rho_lo) */
+    float rho_lo, rho_hi;
 } WaamStepParams;
 
 /* Stages of one fused step.  waam_step_pre runs the surface-height query,

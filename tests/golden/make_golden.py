@@ -967,21 +967,30 @@ KAT_SCRIPTS = ["test_vof_mass", "test_goldak_energy", "test_lbm_poiseuille",
 def kats(names=None):
     """Run validation scripts of the reference (their own ``run()`` with its
     default arguments) and merge their returned values into
-    kat_reference.json."""
+    kat_reference.json.  A script's pass/fail threshold is set to infinity so
+    that it returns its value even where the reference itself misses its own
+    threshold; the value does not depend on it, and the tests apply the
+    thresholds."""
     import importlib
+    import inspect
     import time
     path = os.path.join(HERE, "kat_reference.json")
     out = {}
-    if os.path.exists(path):
-        with open(path) as fh:
-            out = json.load(fh)
     for name in names or KAT_SCRIPTS:
         t0 = time.time()
         mod = importlib.import_module("waam_twin.validation." + name)
-        out[name] = float(mod.run())
+        params = inspect.signature(mod.run).parameters
+        kw = {p: float("inf") for p in ("threshold", "threshold_pct") if p in params}
+        out[name] = float(mod.run(**kw))
         print("kat", name, out[name], "%.0f s" % (time.time() - t0), flush=True)
+        # merge into the file as it is now (another run may have added values)
+        cur = {}
+        if os.path.exists(path):
+            with open(path) as fh:
+                cur = json.load(fh)
+        cur[name] = out[name]
         with open(path, "w") as fh:
-            json.dump(out, fh, indent=1, sort_keys=True)
+            json.dump(cur, fh, indent=1, sort_keys=True)
 
 
 if __name__ == "__main__":

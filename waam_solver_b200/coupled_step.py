@@ -304,6 +304,7 @@ def _fields(g):
         w = getattr(g, "_flags_copy_i", 0)
         f.flags_copy_w = copies[w].data_ptr()
         f.flags_copy_r = copies[1 - w].data_ptr()
+    f.status = g.step_status.data_ptr()
     return f
 
 
@@ -370,6 +371,7 @@ def step_params(twin):
     p.L_vap, p.R_spec = twin.L_vapor_J_kg, twin.R_spec_vapor_J_kgK
     p.C_acc = weld_forces.recoil_accommodation(twin)
     p.weld_sigma = twin.sigma_cells
+    p.rho_lo, p.rho_hi = getattr(twin, "health_rho_band", (0.5, 2.0))
     return p
 
 
@@ -562,6 +564,7 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
                      ws.numel(), stream)
         if due:
             arc_k = float(g.step_scalars[0].item())
+            twin._synced_this_step = True
             forces.clear_forces(g.Fx, g.Fy, g.Fz)
             _droplet(twin, g, arc_i, arc_j, arc_k, torch_x_m, torch_y_m, device_retries=True)
             f = _fields_cached(g)     # the first droplet switches tracer advection on

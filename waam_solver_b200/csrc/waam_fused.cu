@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(256) k_thermal_fused(
     float* __restrict__ T_next, float* __restrict__ f_l, const float* __restrict__ ux,
     const float* __restrict__ uy, const float* __restrict__ uz, const int32_t* __restrict__ flags,
     float* __restrict__ T_max, float* __restrict__ T_prev, float* __restrict__ dT_dt,
-    unsigned* active_count, ThermalArgs a, TableArgs tba) {
+    unsigned* active_count, ThermalArgs a, TableArgs tba, uint32_t* status) {
     if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
         const int t = threadIdx.y * kTileK + threadIdx.x;
         if (t < kActiveShards) active_count[t] = 0u;
@@ -538,6 +538,7 @@ __global__ void __launch_bounds__(256) k_thermal_fused(
             if (h < h_floor) h = h_floor;
         }
         if (a.ph.cap_enabled) h = TABLES ? cap_h_var(tba.vp, pr.cp_rho, h) : cap_h(a.ph, h);
+        if (status != nullptr && !isfinite(h)) atomicOr(status, WAAM_HEALTH_NONFINITE_H);
     }
     float t, fl;
     if (TABLES)
@@ -685,6 +686,8 @@ struct CollideArgs {
     const float* J[3];
     const float* B[3];
     float lz_dt, lz_dx, lz_rho;
+    uint32_t* status;       // health word (null: off)
+    float rho_lo, rho_hi;   // density band of WAAM_HEALTH_RHO_RANGE (off when hi <= lo)
 };
 
 // kernels.py:1479-1513 apply_lorentz_JxB for one cell (f_l >= 0.05)
@@ -797,6 +800,12 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
 #pragma unroll
         for (int q = 0; q < 19; ++q) f_dst[q * n + c] = Pop<S>::put(o[q], q);
         if (a.u_cap > 0.0f) clamp_mach(u, v, w, a.u_cap);
+        if (a.status != nullptr) {
+            if (!(isfinite(rr) && isfinite(u) && isfinite(v) && isfinite(w)))
+                atomicOr(a.status, WAAM_HEALTH_NONFINITE_LBM);
+            else if (a.rho_hi > a.rho_lo && !(rr >= a.rho_lo && rr <= a.rho_hi))
+                atomicOr(a.status, WAAM_HEALTH_RHO_RANGE);
+        }
         rho[c] = rr;
         ux[c] = u;
         uy[c] = v;
@@ -1163,6 +1172,9 @@ static int launch_collide_tracers(const WaamFields* f, const WaamStepParams* p, 
     cl.lz_dt = p->dt;
     cl.lz_dx = p->dx;
     cl.lz_rho = p->rho_phys;
+    cl.status = f->status;
+    cl.rho_lo = p->rho_lo;
+    cl.rho_hi = p->rho_hi;
 #define WAAM_COLLIDE(S)                                                                    \
     k_collide_list<S><<<kListBlocks, kListThreads, 0, s>>>(                                \
         d, static_cast<const Pop<S>::T*>(pop_in), static_cast<Pop<S>::T*>(pop_out),              \
@@ -1299,11 +1311,11 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         if (p->use_tables)
             k_thermal_fused<true><<<tile_grid(d), tile_block(), 0, s>>>(
                 d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
-                f->T_prev, f->dT_dt, active_count, ta, tba);
+                f->T_prev, f->dT_dt, active_count, ta, tba, f->status);
         else
             k_thermal_fused<false><<<tile_grid(d), tile_block(), 0, s>>>(
                 d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
-                f->T_prev, f->dT_dt, active_count, ta, tba);
+                f->T_prev, f->dT_dt, active_count, ta, tba, f->status);
         e = check_launch("k_thermal_fused");
         if (e) return e;
         mark(1);

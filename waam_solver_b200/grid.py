@@ -115,6 +115,8 @@ class WAAMGrid:
         self.deposit_real_buf = torch.zeros((), **f32)
         self.arc_norm_buf = torch.zeros((), **f32)
         self.step_scalars = torch.zeros(16, **f32)
+        # health word of the fused step (WAAM_HEALTH_* bits, see WAAMTwin.health)
+        self.step_status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.telem_fl_slice = torch.zeros((self.ny, self.nz), **f32)
         self.porosity_pos = torch.zeros((self.max_tracers, 3), **f32)
         self.porosity_active = torch.zeros(self.max_tracers, dtype=torch.int32, device=dev)

@@ -337,9 +337,39 @@ class WAAMTwin:
         log.info("[WAAMTwin] Moving window shift -%d cells  offset=%.2fmm", n_shift,
                  self._window_offset_x_m * 1e3)
 
+    HEALTH_BITS = {"nonfinite_enthalpy": 1, "nonfinite_lbm": 2, "rho_out_of_band": 4}
+
+    def health(self, clear=False):
+        """The fused step's device health word since it was last cleared: a
+        non-gas cell's enthalpy not finite, an active cell's density or
+        velocity not finite, an active cell's density outside
+        ``health_rho_band`` (default (0.5, 2.0)).  Reading it synchronises
+        with the device (4 bytes)."""
+        g = self.grid
+        g.flush_stream()
+        word = int(g.step_status.item())
+        if clear:
+            g.step_status.zero_()
+        out = {k: bool(word & b) for k, b in self.HEALTH_BITS.items()}
+        out["word"] = word
+        return out
+
+    def _check_health(self):
+        """strict_mode on a step that already synchronised with the device: raise
+        when the health word reports non-finite values (the reference's
+        NaN/Inf check of its force diagnostics, twin.py:578-585, at the points
+        where it can be read without an extra synchronisation)."""
+        h = self.health()
+        if h["nonfinite_enthalpy"] or h["nonfinite_lbm"]:
+            raise RuntimeError("[strict_mode] NaN/Inf in the fused step (health word %d: %s) "
+                               "after step %d" % (h["word"], ", ".join(
+                                   k for k in self.HEALTH_BITS if h[k]), self._step_n))
+
     def _check_strict_mode(self):
         if not self.strict_mode:
             return
+        if self.__dict__.pop("_synced_this_step", False):
+            self._check_health()
         streak = int(getattr(self, "_lorentz_unconverged_streak", 0) or 0)
         if self.enable_lorentz and streak > 50:
             raise RuntimeError("[strict_mode] Lorentz Jacobi failed to converge for %d "
@@ -428,6 +458,8 @@ class WAAMTwin:
         time re-run of each force operator) are not part of this backend."""
         g = self.grid
         r = kernels.read_telemetry(self.telemetry_record())
+        if self.strict_mode:
+            self._check_health()    # the telemetry read has synchronised already
         n_liquid = int(r.n_liquid)
         if n_liquid > 0:
             T_peak = float(r.T_peak)
