@@ -486,6 +486,74 @@ def _c4_problem(device, N, h_conv_scale=1.0):
     return prob, base
 
 
+FD64_FIXTURE = os.path.join(ROOT, "tests", "golden", "adjoint_fd64.npz")
+
+
+def fd64_problem(device, variant):
+    """The config-4 problem of ``oracle/adjoint_fd64.py`` (variant ``c4`` from
+    reset, ``c4_pool`` from its seeded molten pool) on the GPU, with the FP64
+    run's targets: (problem, fixture metadata, FP64 probe temperatures at the
+    base parameters)."""
+    import numpy as np
+    from waam_solver_b200.adjoint import AdjointProblem
+    z = np.load(FD64_FIXTURE)
+    meta = json.loads(str(z[variant + "_meta"]))
+    tw = build_twin(dict(ADJOINT_C4), device)
+    g = tw.grid
+    yc = (g.ny // 2) * g.dx
+    if variant == "c4_pool":
+        tests = os.path.join(ROOT, "tests")
+        if tests not in sys.path:
+            sys.path.insert(0, tests)
+        import state_gen
+        st = state_gen.seeded_state(g.nx, g.ny, g.nz, seed=meta["pool_seed"],
+                                    nz_solid=tw.nz_solid,
+                                    hot=(meta["x0"] / g.dx + 2.0, yc / g.dx, tw.nz_solid + 1.0))
+        st = {k: v for k, v in st.items() if k != "nz_solid"}
+        st["read_is_a"] = True
+        g.load_state(st)
+    pos = [(meta["x0"] + s * g.dt * meta["travel"], yc) for s in range(meta["steps"])]
+    prob = AdjointProblem(tw, pos, [tuple(p) for p in meta["probes"]],
+                          T_target=z[variant + "_T_target"], W_target=meta["W_target"],
+                          w_T=meta["w_T"], w_W=meta["w_W"], beta=meta["beta"])
+    assert np.allclose(prob.theta, meta["theta"], rtol=1e-12, atol=0.0), (prob.theta, meta)
+    return prob, meta, z[variant + "_T_base"]
+
+
+def adjoint_fd64(device):
+    """The adjoint's gradient against central differences (relative step
+    1e-3) of the FP64 oracle forward (``oracle/adjoint_fd64.py``): config 4
+    from reset and from a seeded molten pool (non-zero width term)."""
+    import numpy as np
+    if not os.path.exists(FD64_FIXTURE):
+        return None
+    from waam_solver_b200.adjoint import PARAMS
+    out = {}
+    with np.load(FD64_FIXTURE) as z:
+        variants = [k[:-5] for k in z.files if k.endswith("_meta")]
+    for variant in variants:
+        prob, meta, T64 = fd64_problem(device, variant)
+        loss = prob.forward(prob.theta)
+        grad = prob.backward()
+        rel = {}
+        for q, name in enumerate(PARAMS):
+            if name not in meta["fd"]:
+                rel[name] = {"adjoint": float(grad[q]), "fd_fp64": 0.0,
+                             "note": "structural zero (nothing of this configuration reads it)"}
+                continue
+            f = meta["fd"][name]
+            rel[name] = {"adjoint": float(grad[q]), "fd_fp64": f,
+                         "rel_diff": abs(grad[q] - f) / max(abs(f), 1e-300)}
+        out[variant] = {"steps": meta["steps"], "loss_float32": loss,
+                        "loss_fp64": meta["loss_base"], "width_mm": prob.width()[0],
+                        "probe_T_max_abs_diff_vs_fp64": float(np.abs(prob.T_probe - T64).max()),
+                        "gradient": rel}
+        del prob
+        import torch
+        torch.cuda.empty_cache()
+    return out
+
+
 def _central_fd(prob, base, q, step):
     h = step * abs(base[q])
     tp, tm = base.copy(), base.copy()
@@ -887,6 +955,9 @@ def run_b200(args, w):
         line["material_tables"] = table_form(w, device, min(K, 1000), ms / K, stage_ms)
     if world == 1 and standard and not args.no_adjoint:
         line["adjoint"] = adjoint_form(device)
+        fd64 = adjoint_fd64(device)
+        if fd64:
+            line["adjoint"]["fd_fp64"] = fd64
     if world == 1 and standard and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:

@@ -646,6 +646,23 @@ typedef struct WaamFields {
      * [WaamStepParams.rho_lo, rho_hi].  Nothing clears it; the caller reads
      * it where it synchronises anyway and zeroes it when it wants. */
     uint32_t* status;
+    /* quiet-tile skipping of the fused step (all null: every tile is worked).
+     * Tiles are the 32 (k) x 8 (j) cell blocks of one x plane, numbered
+     * t = (i * ceil(ny / 8) + j / 8) * ceil(nz / 32) + k / 32; a chunk is the
+     * 32 cells of one (i, j) column inside a tile (column-chunk number
+     * (i * ny + j) * ceil(nz / 32) + k / 32).  With WaamStepParams.tile_skip
+     * set, waam_step_pre marks as quiet every tile whose cells and every cell
+     * within two lattice steps of them are GAS, and that was all GAS at the
+     * step before; the arc, thermal, VOF and column stages leave quiet tiles
+     * alone (they are exact no-ops there).  The caller owns and zero-fills:
+     *   tile_bits: ceil(nz/32) * nx * ny chunk bytes, then one byte per tile;
+     *   tile_list: 1 + tiles int32 (count, then the tiles to work);
+     *   tile_part: tiles doubles (per-tile arc weight sums).
+     * They carry state from step to step: after changing the fields any
+     * other way, run the next step with tile_skip = 0. */
+    uint8_t* tile_bits;
+    int32_t* tile_list;
+    double* tile_part;
 } WaamFields;
 
 #define WAAM_HEALTH_NONFINITE_H 1u   /* H of a non-gas cell is NaN or infinite */
@@ -743,6 +760,11 @@ typedef struct WaamStepParams {
     /* density band of the health word's WAAM_HEALTH_RHO_RANGE bit (the check
      * is off when rho_hi <= rho_lo) */
     float rho_lo, rho_hi;
+    /* quiet-tile skipping (needs WaamFields.tile_*): 1 skips the quiet tiles
+     * of this step; 0 works every tile and restarts the tile history (the
+     * step after a state change, a droplet deposition, a force clear, or
+     * with the remelt / solidify tail on) */
+    int tile_skip;
 } WaamStepParams;
 
 /* Stages of one fused step.  waam_step_pre runs the surface-height query,

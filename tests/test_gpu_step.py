@@ -382,3 +382,53 @@ def test_operator_calls_after_pipelined_steps_see_streamed_populations():
     for k, v in states[0].items():
         if isinstance(v, np.ndarray):
             assert np.array_equal(v, states[1][k]), k
+
+
+def test_quiet_tile_skipping_matches_working_every_tile():
+    """Quiet-tile skipping (the default) against every tile worked, bit for bit,
+    on a grid tall enough for quiet tiles (nz = 96: three 32-cell k tiles over
+    a 19-cell plate), through droplet steps (the tile history restarts),
+    graph replays and the pipelined stream and collision; the skipping
+    really skips (the work list is shorter than the tile count)."""
+    states, counts = [], []
+    for skip in (False, True):
+        tw, ot, dx = _config_twins("c2", 40, 32, 96)
+        tw.skip_quiet_tiles = skip
+        tw._last_droplet_time = -1.0
+        g = tw.grid
+        n_tiles = g.tile_list.numel() - 1
+        for s in range(40):
+            tw.step(0.3 * 40 * dx + s * 1e-6, 16 * dx, not 25 <= s < 28)
+            if s == 35:
+                torch.cuda.synchronize()
+                counts.append(int(g.tile_list[0].item()))
+        torch.cuda.synchronize()
+        states.append(g.state_dict())
+    assert counts[0] == n_tiles and 0 < counts[1] < n_tiles, (counts, n_tiles)
+    for k, v in states[0].items():
+        if isinstance(v, np.ndarray):
+            assert np.array_equal(v, states[1][k]), k
+
+
+def test_quiet_tile_history_restarts_after_operator_calls():
+    """An operator-API call that writes flags / phi / f_l / H / T between fused
+    steps (here update_flags_from_phi) restarts the quiet-tile history: the
+    next step works every tile; so do load_state and invalidate()."""
+    from waam_solver_b200 import kernels
+    tw, ot, dx = _config_twins("c2", 40, 32, 96)
+    g = tw.grid
+    for s in range(4):
+        tw.step(0.3 * 40 * dx + s * 1e-6, 16 * dx, True)
+    assert tw._fused_params.tile_skip == 1
+    kernels.update_flags_from_phi(g.phi, g.f_l, g.flags, tw.nz_solid, 0, 1, 2, 4)
+    tw.step(0.3 * 40 * dx + 5e-6, 16 * dx, True)
+    assert tw._fused_params.tile_skip == 0
+    tw.step(0.3 * 40 * dx + 6e-6, 16 * dx, True)
+    assert tw._fused_params.tile_skip == 1
+    g.load_state(g.state_dict())
+    tw.step(0.3 * 40 * dx + 7e-6, 16 * dx, True)
+    assert tw._fused_params.tile_skip == 0
+    tw.step(0.3 * 40 * dx + 8e-6, 16 * dx, True)
+    tw.invalidate()
+    tw.step(0.3 * 40 * dx + 9e-6, 16 * dx, True)
+    assert tw._fused_params.tile_skip == 0

@@ -305,6 +305,9 @@ def _fields(g):
         f.flags_copy_w = copies[w].data_ptr()
         f.flags_copy_r = copies[1 - w].data_ptr()
     f.status = g.step_status.data_ptr()
+    f.tile_bits = g.tile_bits.data_ptr()
+    f.tile_list = g.tile_list.data_ptr()
+    f.tile_part = g.tile_part.data_ptr()
     return f
 
 
@@ -451,6 +454,7 @@ def flush_stream(g):
         return
     g._stream_pending = False
     g._collide_pending = False
+    kernels.PENDING_GRIDS.discard(g)
     st = torch.cuda.current_stream().cuda_stream
     if collide:
         p = g._pending_params
@@ -551,11 +555,18 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
                            not (twin.enable_bead_freeze or twin.enable_substrate_growth)) else 0
     p.defer_collide = 1 if (p.defer_stream and not due and not lorentz and
                             getattr(twin, "pipeline_collide", True)) else 0
+    # quiet tiles: skipped only while the tile history is the fused step's own
+    # (no droplet deposition in the middle of this step, no force clear, no
+    # remelt / solidify tail rewriting flags, nothing changed the state since)
+    p.tile_skip = 1 if (getattr(twin, "skip_quiet_tiles", True) and g._tiles_valid and
+                        g.__dict__.get("_tile_epoch") == kernels.STATE_EPOCH[0] and not due and
+                        not p.clear_forces and
+                        not (twin.enable_bead_freeze or twin.enable_substrate_growth)) else 0
     done = False
     if not due and not lorentz and events is None and getattr(twin, "use_cuda_graphs", True):
         key = (g._read_buf is raw_field(g, "f_a"), g._cur, p.welding, p.clear_forces, p.stream_prev,
                p.defer_stream, p.collide_prev, p.collide_prev_welding, p.defer_collide,
-               g._flags_copy_i,
+               g._flags_copy_i, p.tile_skip,
                (dx_, dy_, dz_) if twin.enable_bead_freeze else None)
         done = _run_graph(twin, g, f, p, ws, key)
     if not done:
@@ -601,12 +612,16 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     g._forces_dirty = bool(p.forces_from_buffer) or lorentz
     g._stream_pending = bool(p.defer_stream)
     g._collide_pending = bool(p.defer_collide)
+    if p.defer_stream:
+        kernels.PENDING_GRIDS.add(g)
     if p.defer_collide:
         q = _native.WaamStepParams.from_buffer_copy(p)
         q.collide_prev, q.collide_prev_welding = 1, p.welding
         g._pending_params = q
         g._pending_welding = p.welding
     g._flags_copy_i = 1 - g._flags_copy_i    # this step's copy is read by the next step
+    g._tiles_valid = True                    # this step's column pass wrote the chunk bits
+    g._tile_epoch = kernels.STATE_EPOCH[0]
     g.flip_thermal()
     g.swap_buffers()
     twin._step_n += 1
@@ -633,9 +648,14 @@ class _LazyArc(tuple):
 
 def coupled_step(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     if getattr(twin, "step_mode", "fused") == "operators":
+        flush_stream(twin.grid)
         coupled_step_operators(twin, torch_x_m, torch_y_m, is_welding, torch_z_m)
     else:
-        coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m)
+        kernels.IN_FUSED_STEP[0] = True
+        try:
+            coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m)
+        finally:
+            kernels.IN_FUSED_STEP[0] = False
     rec = getattr(twin, "probe_recorder", None)
     if rec is not None:
         rec.record_step(twin)

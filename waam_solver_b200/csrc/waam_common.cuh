@@ -415,6 +415,43 @@ __device__ __forceinline__ float thermal_dh(const Dims d, const float* __restric
     return dH;
 }
 
+// thermal_dh with neighbour offsets instead of clamped coordinates (same
+// values): a clamped neighbour is the cell itself (non-gas: the centre
+// value), and a clamped second neighbour is the first one, whose masked value
+// it then takes either way.  Tc = T[c].
+__device__ __forceinline__ float thermal_dh_offsets(const Dims& d, const float* __restrict__ Hs,
+                                                    const float* __restrict__ T,
+                                                    const int32_t* __restrict__ flags, float u,
+                                                    float v, float w, int i, int j, int k, int c,
+                                                    int flag, float Hc, float Tc, float cpa,
+                                                    float dt) {
+    const int sx = d.ny * d.nz, sy = d.nz;
+    const bool mxm = i > 0 && flags[c - sx] != GAS, mxp = i < d.nx - 1 && flags[c + sx] != GAS;
+    const bool mym = j > 0 && flags[c - sy] != GAS, myp = j < d.ny - 1 && flags[c + sy] != GAS;
+    const bool mzm = k > 0 && flags[c - 1] != GAS, mzp = k < d.nz - 1 && flags[c + 1] != GAS;
+    const float Tim = mxm ? T[c - sx] : Tc, Tip = mxp ? T[c + sx] : Tc;
+    const float Tjm = mym ? T[c - sy] : Tc, Tjp = myp ? T[c + sy] : Tc;
+    const float Tkm = mzm ? T[c - 1] : Tc, Tkp = mzp ? T[c + 1] : Tc;
+    float lap = Tip + Tim + Tjp + Tjm + Tkp + Tkm - 6.0f * Tc;
+    float dH = cpa * lap * dt;
+    if (flag != SOLID) {
+        const float Him = mxm ? Hs[c - sx] : Hc, Hip = mxp ? Hs[c + sx] : Hc;
+        const float Hjm = mym ? Hs[c - sy] : Hc, Hjp = myp ? Hs[c + sy] : Hc;
+        const float Hkm = mzm ? Hs[c - 1] : Hc, Hkp = mzp ? Hs[c + 1] : Hc;
+        const float Himm = (i >= 2 && flags[c - 2 * sx] != GAS) ? Hs[c - 2 * sx] : Him;
+        const float Hipp = (i <= d.nx - 3 && flags[c + 2 * sx] != GAS) ? Hs[c + 2 * sx] : Hip;
+        const float Hjmm = (j >= 2 && flags[c - 2 * sy] != GAS) ? Hs[c - 2 * sy] : Hjm;
+        const float Hjpp = (j <= d.ny - 3 && flags[c + 2 * sy] != GAS) ? Hs[c + 2 * sy] : Hjp;
+        const float Hkmm = (k >= 2 && flags[c - 2] != GAS) ? Hs[c - 2] : Hkm;
+        const float Hkpp = (k <= d.nz - 3 && flags[c + 2] != GAS) ? Hs[c + 2] : Hkp;
+        float gx = upwind_grad(u, Himm, Him, Hc, Hip, Hipp);
+        float gy = upwind_grad(v, Hjmm, Hjm, Hc, Hjp, Hjpp);
+        float gz = upwind_grad(w, Hkmm, Hkm, Hc, Hkp, Hkpp);
+        dH -= (u * gx + v * gy + w * gz) * dt;
+    }
+    return dH;
+}
+
 // kernels.py:2275-2317 _vof_face_flux
 __device__ __forceinline__ float vof_flux(const Dims d, const float* __restrict__ phi,
                                           const float* __restrict__ vel,

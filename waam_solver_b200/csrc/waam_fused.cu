@@ -28,6 +28,7 @@ constexpr int kMaxDevices = 64;
 constexpr int kTileRedBlocks = 592;   // <= kWsMaxPartials; a fixed grid keeps the sum order fixed
 constexpr int kListThreads = 128;
 constexpr int kArcTableMax = 1024;    // nz up to which the arc depth weights come from a table
+constexpr int kArcAxisMax = 3072;     // nx + ny + nz up to which the arc shape uses axis tables
 constexpr int kListBlocks = 148 * 6;
 
 
@@ -82,16 +83,26 @@ __device__ __forceinline__ float contact_rules(const ContactConst& cc, float sta
 // Runs the column pass for one warp; `emit(k, c, value, flag_old, valid)` is
 // called by every lane of every chunk (convergent), value = final phi (snap
 // for solid cells).
-template <class Emit>
+// skip(k0): the chunk at k0 is a quiet all-GAS chunk (warp-uniform); it is
+// left alone and the next chunk starts from a GAS cell below with phi < 0.55
+// and no ghost value, which is what its cells would see.
+template <class Emit, class Skip>
 __device__ __forceinline__ void contact_column(const Dims d, const float* __restrict__ snap,
                                                const int32_t* __restrict__ flags, int i, int j,
-                                               bool wetting, const ContactConst& cc, Emit emit) {
+                                               bool wetting, const ContactConst& cc, Emit emit,
+                                               Skip skip) {
     const int lane = threadIdx.x & 31;
     int carry_flag = SOLID;      // old flag of the cell below the chunk
     float carry_final = 0.0f;    // final phi of the cell below the chunk
     float carry_ghost = -1.0f;   // ghost value written into the chunk's first cell (<0: none)
     const int sx = d.ny * d.nz;
     for (int k0 = 0; k0 < d.nz; k0 += 32) {
+        if (skip(k0)) {
+            carry_flag = GAS;
+            carry_final = 0.0f;
+            carry_ghost = -1.0f;
+            continue;
+        }
         int k = k0 + lane;
         bool valid = k < d.nz;
         int c = d.idx(i, j, valid ? k : d.nz - 1);
@@ -155,7 +166,7 @@ __global__ void k_contact_op(Dims d, const float* __restrict__ snap, float* __re
     ContactConst cc = contact_const(cos_t, sin_t);
     contact_column(d, snap, flags, i, j, true, cc, [&](int k, int c, float v, int flag, bool valid) {
         if (valid && flag != SOLID) phi[c] = v;
-    });
+    }, [](int) { return false; });
 }
 
 int launch_contact_columns(Dims d, const float* snap, float* phi, const int32_t* flags,
@@ -406,31 +417,202 @@ __global__ void __launch_bounds__(256) k_arc_norm_tiles(Dims d, const int32_t* _
     }
 }
 
-// Pass 2: H += epw * weight (non-gas cells), then the enthalpy ceiling
-// (solvers/coupled_step.py:107-108).
-__global__ void __launch_bounds__(256) k_arc_inject_tiles(Dims d, float* __restrict__ H,
-                                                          const int32_t* __restrict__ flags,
-                                                          const float* __restrict__ f_l,
-                                                          ArcParams p, const float* scalars,
-                                                          float arc_k_offset, int cap,
-                                                          PhaseParams ph,
-                                                          const float* __restrict__ cp_f,
-                                                          VarPhase vp,
-                                                          const float* __restrict__ shape) {
-    int i, j, k, c;
-    const bool ok = tile_cell(d, i, j, k, c);
-    // the device scalars and the flag are requested together, then f_l and H
-    p.arc_k = scalars[kScalarArcK] + arc_k_offset;
+// Quiet-tile classification (WaamFields.tile_bits): one thread per tile.  A
+// tile is quiet when its columns were all GAS in the last two column passes
+// (chunk bits 0 and 1) and every cell within two lattice steps of it is GAS:
+// the chunks of the 5 x (8 + 4) columns around it at the same k are all GAS
+// (bit 0), the top two cells of the chunks below (bit 2) and the bottom two
+// of the chunks above (bit 3) too -- x periodic, y and z out of range count
+// as GAS.  Writes one work byte per tile and appends the work tiles to the
+// list (count in list[0], zeroed before the launch).
+__global__ void k_classify_tiles(Dims d, const uint8_t* __restrict__ chunk,
+                                 uint8_t* __restrict__ work, int32_t* __restrict__ list,
+                                 int skip) {
+    const int KT = tiles_k(d), JT = tiles_j(d);
+    const int64_t T = tile_total(d);
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool w = true;
+    int kt = 0, jt = 0, i = 0;
+    if (t < T) {
+        kt = (int)(t % KT);
+        const int r = (int)(t / KT);
+        jt = r % JT;
+        i = r / JT;
+        if (skip) {
+            const int j0 = jt * kTileJ, j1 = imin(j0 + kTileJ, d.ny);
+            auto cb = [&](int ii, int jj, int kk) -> unsigned {
+                return chunk[((int64_t)ii * d.ny + jj) * KT + kk];
+            };
+            // every load is issued before any is tested (no early exit), so the
+            // tile costs a few round trips, not one per chunk
+            unsigned core = 3u;
+#pragma unroll
+            for (int dj = 0; dj < kTileJ; ++dj)
+                if (j0 + dj < j1) core &= cb(i, j0 + dj, kt);
+            unsigned box = 1u;
+#pragma unroll
+            for (int di = -2; di <= 2; ++di) {
+                const int ii = ((i + di) % d.nx + d.nx) % d.nx;
+#pragma unroll
+                for (int dj = -2; dj < kTileJ + 2; ++dj) {
+                    const int jj = j0 + dj;
+                    if (jj < 0 || jj >= imin(d.ny, j1 + 2)) continue;
+                    unsigned b = cb(ii, jj, kt);
+                    if (kt > 0) b &= cb(ii, jj, kt - 1) >> 2;
+                    if (kt + 1 < KT) b &= cb(ii, jj, kt + 1) >> 3;
+                    box &= b;
+                }
+            }
+            w = !((core & 3u) == 3u && (box & 1u));
+        }
+        work[t] = w ? 1 : 0;
+    }
+    const bool app = t < T && w;
+    const unsigned m = __ballot_sync(0xffffffffu, app);
+    if (m) {
+        const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
+        int base = 0;
+        if (lane == lead) base = atomicAdd(&list[0], __popc(m));
+        base = __shfl_sync(0xffffffffu, base, lead);
+        if (app) list[1 + base + __popc(m & ((1u << lane) - 1u))] = pack_tile(i, jt, kt);
+    }
+}
+
+// The arc weight sum over the tiles of the work list (quiet tiles are all GAS
+// and weigh nothing).  Each listed tile's sum goes to its own slot of
+// tile_part; the last block adds the slots in tile order, so the total does
+// not depend on the list's order.  Otherwise as k_arc_norm_tiles.
+__global__ void __launch_bounds__(256) k_arc_norm_list(Dims d, const int32_t* __restrict__ flags,
+                                                       const float* __restrict__ f_l,
+                                                       const float* __restrict__ phi,
+                                                       int nz_solid, ArcParams p, float* scalars,
+                                                       float arc_k_offset, float Qe_dt, float dx3,
+                                                       Workspace ws, float* __restrict__ shape,
+                                                       const int32_t* __restrict__ list,
+                                                       const uint8_t* __restrict__ tile_work,
+                                                       double* __restrict__ tile_part, int tiles) {
+    __shared__ float s_arc_k;
+    __shared__ float s_wd[kArcTableMax];
+    if (threadIdx.y == 0) {
+        const float kf = surface_arc_k(d, phi, flags, scalars, nz_solid);
+        if (threadIdx.x == 0) {
+            s_arc_k = kf;
+            if (blockIdx.x == 0) scalars[kScalarArcK] = kf;
+        }
+    }
+    __syncthreads();
+    p.arc_k = s_arc_k + arc_k_offset;
     p.arc_i = scalars[kScalarArcI];
     p.arc_j = scalars[kScalarArcJ];
-    // depth weights of the block's 32 k values (non-liquid cells)
-    __shared__ float s_wd[kTileK];
-    if (threadIdx.y == 0)
-        s_wd[threadIdx.x] = arc_weight(blockIdx.x * kTileK + threadIdx.x, p.arc_k, 0.0f, p.pen,
-                                       p.enable);
+    const bool table = d.nz <= kArcTableMax;
+    if (table)
+        for (int k = threadIdx.y * kTileK + threadIdx.x; k < d.nz; k += kTileK * kTileJ)
+            s_wd[k] = arc_weight(k, p.arc_k, 0.0f, p.pen, p.enable);
+    // The spatial factor's exponent is a sum of an i, a j and a k term
+    // (Gaussian: di^2 + dj^2 + dk^2 / 4; Goldak: xt^2 / a^2 + dj^2 / b^2 +
+    // dk^2 / c^2, waam_common.cuh arc_cell_shape); each term is tabulated once
+    // per block with the per-cell expression and added in the same order, so
+    // a cell costs one exponential and no division.
+    __shared__ float s_axis[kArcAxisMax];
+    const bool axes = d.nx + d.ny + d.nz <= kArcAxisMax;
+    if (axes) {
+        const float eps = 1e-6f;
+        for (int t = threadIdx.y * kTileK + threadIdx.x; t < d.nx + d.ny + d.nz;
+             t += kTileK * kTileJ) {
+            float v;
+            if (t < d.nx) {
+                const float di = (float)t - p.arc_i;
+                if (p.kind == 0) {
+                    v = di * di;
+                } else {
+                    const float xt = di * p.sign;
+                    const float a = xt >= 0.0f ? p.a_f : p.a_r;
+                    v = (xt * xt) / (a * a + eps);
+                }
+            } else if (t < d.nx + d.ny) {
+                const float dj = (float)(t - d.nx) - p.arc_j;
+                v = p.kind == 0 ? dj * dj : (dj * dj) / (p.b * p.b + eps);
+            } else {
+                const float dk = (float)(t - d.nx - d.ny) - p.arc_k;
+                v = p.kind == 0 ? dk * dk * 0.25f : (dk * dk) / (p.c * p.c + eps);
+            }
+            s_axis[t] = v;
+        }
+    }
     __syncthreads();
-    if (!ok) return;
-    const float epw = scalars[kScalarEpw];
+    auto shape_of = [&](int i, int j, int k) -> float {
+        if (!axes) return arc_cell_shape(p, i, j, k);
+        const float sum = (s_axis[i] + s_axis[d.nx + j]) + s_axis[d.nx + d.ny + k];
+        if (p.kind == 0) return waam_expf(-sum * p.inv2s2);
+        const float xt = ((float)i - p.arc_i) * p.sign;
+        return (xt >= 0.0f ? p.ff : p.fr) * waam_expf(-3.0f * sum);
+    };
+    const int tid = threadIdx.y * kTileK + threadIdx.x;
+    const int cnt = imin(list[0], tiles);
+    constexpr int kU = 4;
+    for (int e0 = blockIdx.x; e0 < cnt; e0 += kU * gridDim.x) {
+        int fg[kU], ci[kU], cj[kU], ck[kU], tt[kU];
+        float fl[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int e = e0 + u * gridDim.x;
+            const int ent = e < cnt ? list[1 + e] : -1;
+            tt[u] = ent >= 0 ? (int)tile_index(d, ent) : -1;
+            int i = 0, j = 0, k = 0, c = 0;
+            const bool ok = ent >= 0 && list_tile_cell(d, ent, i, j, k, c);
+            fg[u] = ok ? flags[c] : GAS;
+            fl[u] = ok ? f_l[c] : 0.0f;
+            ci[u] = i;
+            cj[u] = j;
+            ck[u] = k;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            double v = 0.0;
+            if (fg[u] != GAS) {
+                const float wd = !table ? arc_weight(ck[u], p.arc_k, fl[u], p.pen, p.enable)
+                                        : (fl[u] > 0.55f ? 1.0f : s_wd[ck[u]]);
+                if (!(wd < 1e-6f)) {
+                    const float sh = shape_of(ci[u], cj[u], ck[u]);
+                    shape[(ci[u] * d.ny + cj[u]) * d.nz + ck[u]] = sh;
+                    v = (double)(sh * wd);
+                }
+            }
+            const double sum = tile_block_sum(v);
+            if (tid == 0 && tt[u] >= 0) tile_part[tt[u]] = sum;
+        }
+    }
+    __shared__ bool last;
+    if (tid == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(ws.counter, 1u);
+        last = prev == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double acc = 0.0;
+    for (int t = tid; t < tiles; t += kTileK * kTileJ)
+        acc += tile_work[t] ? ((volatile double*)tile_part)[t] : 0.0;
+    const double tot = tile_block_sum(acc);
+    if (tid == 0) {
+        *ws.counter = 0u;
+        const float w_total = (float)tot;
+        float epw = 0.0f;
+        if (w_total > 1e-9f) epw = Qe_dt / (w_total * dx3);
+        scalars[kScalarWsum] = w_total;
+        scalars[kScalarEpw] = epw;
+    }
+}
+
+// Pass 2 for one cell: H += epw * weight (non-gas cells), then the enthalpy
+// ceiling (solvers/coupled_step.py:107-108); wd_dry is the depth weight of
+// the cell's k for a cell that is not liquid.
+__device__ __forceinline__ void inject_cell(float* __restrict__ H, const int32_t* __restrict__ flags,
+                                            const float* __restrict__ f_l, float epw, int cap,
+                                            const PhaseParams& ph, const float* __restrict__ cp_f,
+                                            const VarPhase& vp, const float* __restrict__ shape,
+                                            float wd_dry, int c) {
     const int flag = flags[c];
     const float fl = f_l[c];           // requested with the flag (ignored for gas cells)
     float h = cap ? H[c] : 0.0f;
@@ -440,7 +622,7 @@ __global__ void __launch_bounds__(256) k_arc_inject_tiles(Dims d, float* __restr
     float dh = 0.0f;
     bool hit = false;
     if (epw > 0.0f) {
-        const float wd = fl > 0.55f ? 1.0f : s_wd[threadIdx.x];
+        const float wd = fl > 0.55f ? 1.0f : wd_dry;
         if (!(wd < 1e-6f)) {
             dh = epw * shape[c] * wd;
             hit = true;
@@ -453,6 +635,58 @@ __global__ void __launch_bounds__(256) k_arc_inject_tiles(Dims d, float* __restr
     // (kernels.py:1988-2010)
     if (cap) h = cp_f ? cap_h_var(vp, cp_f[c], h) : cap_h(ph, h);
     H[c] = h;
+}
+
+__global__ void __launch_bounds__(256) k_arc_inject_tiles(Dims d, float* __restrict__ H,
+                                                          const int32_t* __restrict__ flags,
+                                                          const float* __restrict__ f_l,
+                                                          ArcParams p, const float* scalars,
+                                                          float arc_k_offset, int cap,
+                                                          PhaseParams ph,
+                                                          const float* __restrict__ cp_f,
+                                                          VarPhase vp,
+                                                          const float* __restrict__ shape) {
+    int i, j, k, c;
+    const bool ok = tile_cell(d, i, j, k, c);
+    p.arc_k = scalars[kScalarArcK] + arc_k_offset;
+    // depth weights of the block's 32 k values (non-liquid cells)
+    __shared__ float s_wd[kTileK];
+    if (threadIdx.y == 0)
+        s_wd[threadIdx.x] = arc_weight(blockIdx.x * kTileK + threadIdx.x, p.arc_k, 0.0f, p.pen,
+                                       p.enable);
+    __syncthreads();
+    if (!ok) return;
+    inject_cell(H, flags, f_l, scalars[kScalarEpw], cap, ph, cp_f, vp, shape, s_wd[threadIdx.x], c);
+}
+
+// The injection over the tiles of the work list (quiet tiles are all GAS, so
+// the injection and the ceiling leave them unchanged).
+__global__ void __launch_bounds__(256) k_arc_inject_list(Dims d, float* __restrict__ H,
+                                                         const int32_t* __restrict__ flags,
+                                                         const float* __restrict__ f_l,
+                                                         ArcParams p, const float* scalars,
+                                                         float arc_k_offset, int cap,
+                                                         PhaseParams ph,
+                                                         const float* __restrict__ cp_f,
+                                                         VarPhase vp,
+                                                         const float* __restrict__ shape,
+                                                         const int32_t* __restrict__ list,
+                                                         int tiles) {
+    p.arc_k = scalars[kScalarArcK] + arc_k_offset;
+    __shared__ float s_wd[kArcTableMax];
+    const bool table = d.nz <= kArcTableMax;
+    if (table)
+        for (int k = threadIdx.y * kTileK + threadIdx.x; k < d.nz; k += kTileK * kTileJ)
+            s_wd[k] = arc_weight(k, p.arc_k, 0.0f, p.pen, p.enable);
+    __syncthreads();
+    const float epw = scalars[kScalarEpw];
+    const int cnt = imin(list[0], tiles);
+    for (int e = blockIdx.x; e < cnt; e += gridDim.x) {
+        int i, j, k, c;
+        if (!list_tile_cell(d, list[1 + e], i, j, k, c)) continue;
+        const float wd = table ? s_wd[k] : arc_weight(k, p.arc_k, 0.0f, p.pen, p.enable);
+        inject_cell(H, flags, f_l, epw, cap, ph, cp_f, vp, shape, wd, c);
+    }
 }
 
 struct ThermalArgs {
@@ -484,18 +718,13 @@ struct TableArgs {
 // clamp_enthalpy_floor and update_phase_variable_cp / the variable ceiling
 // (kernels.py:1710-1863, 1922-1935, 1988-2010) instead of the scalar forms.
 template <bool TABLES>
-__global__ void __launch_bounds__(256) k_thermal_fused(
-    Dims d, const float* __restrict__ H, float* __restrict__ H_next, const float* __restrict__ T,
-    float* __restrict__ T_next, float* __restrict__ f_l, const float* __restrict__ ux,
-    const float* __restrict__ uy, const float* __restrict__ uz, const int32_t* __restrict__ flags,
-    float* __restrict__ T_max, float* __restrict__ T_prev, float* __restrict__ dT_dt,
-    unsigned* active_count, ThermalArgs a, TableArgs tba, uint32_t* status) {
-    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
-        const int t = threadIdx.y * kTileK + threadIdx.x;
-        if (t < kActiveShards) active_count[t] = 0u;
-    }
-    int i, j, k, c;
-    if (!tile_cell(d, i, j, k, c)) return;
+__device__ __forceinline__ void thermal_cell(
+    const Dims& d, const float* __restrict__ H, float* __restrict__ H_next,
+    const float* __restrict__ T, float* __restrict__ T_next, float* __restrict__ f_l,
+    const float* __restrict__ ux, const float* __restrict__ uy, const float* __restrict__ uz,
+    const int32_t* __restrict__ flags, float* __restrict__ T_max, float* __restrict__ T_prev,
+    float* __restrict__ dT_dt, const ThermalArgs& a, const TableArgs& tba, uint32_t* status,
+    int i, int j, int k, int c) {
     const int flag = flags[c];
     float h = H[c];
     CellProps pr{};
@@ -514,7 +743,8 @@ __global__ void __launch_bounds__(256) k_thermal_fused(
             w = uz[c];
         }
         const float cpa = TABLES ? pr.cp_rho * pr.alpha : a.cpa;
-        h = h + thermal_dh(d, H, T, flags, u, v, w, i, j, k, flag, h, cpa, a.dt_lu);
+        h = h + thermal_dh_offsets(d, H, T, flags, u, v, w, i, j, k, c, flag, h, T[c], cpa,
+                                   a.dt_lu);
         if (a.heat_loss) {
             int ne = 0;
             const int sx = d.ny * d.nz;
@@ -556,9 +786,103 @@ __global__ void __launch_bounds__(256) k_thermal_fused(
     }
 }
 
+template <bool TABLES>
+__global__ void __launch_bounds__(256) k_thermal_fused(
+    Dims d, const float* __restrict__ H, float* __restrict__ H_next, const float* __restrict__ T,
+    float* __restrict__ T_next, float* __restrict__ f_l, const float* __restrict__ ux,
+    const float* __restrict__ uy, const float* __restrict__ uz, const int32_t* __restrict__ flags,
+    float* __restrict__ T_max, float* __restrict__ T_prev, float* __restrict__ dT_dt,
+    unsigned* active_count, ThermalArgs a, TableArgs tba, uint32_t* status) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
+        const int t = threadIdx.y * kTileK + threadIdx.x;
+        if (t < kActiveShards) active_count[t] = 0u;
+    }
+    int i, j, k, c;
+    if (!tile_cell(d, i, j, k, c)) return;
+    thermal_cell<TABLES>(d, H, H_next, T, T_next, f_l, ux, uy, uz, flags, T_max, T_prev, dT_dt, a,
+                         tba, status, i, j, k, c);
+}
+
+// The thermal stage over the tiles of the work list.  A quiet tile was all
+// GAS in the flags of this step and of the step before, so the previous
+// step already left both enthalpy / temperature buffers equal there and its
+// column pass left f_l = 0 (GAS): the stage would rewrite the same values.
+template <bool TABLES>
+__global__ void __launch_bounds__(256) k_thermal_list(
+    Dims d, const float* __restrict__ H, float* __restrict__ H_next, const float* __restrict__ T,
+    float* __restrict__ T_next, float* __restrict__ f_l, const float* __restrict__ ux,
+    const float* __restrict__ uy, const float* __restrict__ uz, const int32_t* __restrict__ flags,
+    float* __restrict__ T_max, float* __restrict__ T_prev, float* __restrict__ dT_dt,
+    unsigned* active_count, ThermalArgs a, TableArgs tba, uint32_t* status,
+    const int32_t* __restrict__ list, int tiles) {
+    if (blockIdx.x == 0) {
+        const int t = threadIdx.y * kTileK + threadIdx.x;
+        if (t < kActiveShards) active_count[t] = 0u;
+    }
+    const int cnt = imin(list[0], tiles);
+    for (int e = blockIdx.x; e < cnt; e += gridDim.x) {
+        int i, j, k, c;
+        if (!list_tile_cell(d, list[1 + e], i, j, k, c)) continue;
+        thermal_cell<TABLES>(d, H, H_next, T, T_next, f_l, ux, uy, uz, flags, T_max, T_prev, dT_dt,
+                             a, tba, status, i, j, k, c);
+    }
+}
+
 // VOF advection + reinitialisation (kernels.py:2320-2391) -> phi_tmp.  A gas
 // cell whose six face neighbours are gas (or outside y/z) has zero velocity on
 // every face, so all fluxes vanish and phi_tmp = reinit(phi) exactly.
+__device__ __forceinline__ void vof_cell(const Dims& d, const float* __restrict__ phi,
+                                         float* __restrict__ phi_tmp,
+                                         const float* __restrict__ ux,
+                                         const float* __restrict__ uy,
+                                         const float* __restrict__ uz,
+                                         const int32_t* __restrict__ flags, int i, int j, int k,
+                                         int c) {
+    const int flag = flags[c];
+    const float p0 = phi[c];
+    float p = p0;
+    if (flag != SOLID) {
+        // kernels.py:2320-2361 for one non-solid cell: donor-cell fluxes through
+        // the six faces (x periodic, no flux through y / z domain faces or into
+        // SOLID cells, GAS cells at rest).  The six neighbour flags are loaded
+        // once for the quiet-gas test and the fluxes.
+        const int sx = d.ny * d.nz, sy = d.nz;
+        const int cw = i > 0 ? c - sx : c + (d.nx - 1) * sx;
+        const int ce = i < d.nx - 1 ? c + sx : c - (d.nx - 1) * sx;
+        const bool hs = j > 0, hn = j < d.ny - 1, hb = k > 0, ht = k < d.nz - 1;
+        const int fw = flags[cw], fe = flags[ce];
+        const int fs = hs ? flags[c - sy] : GAS, fn = hn ? flags[c + sy] : GAS;
+        const int fb = hb ? flags[c - 1] : GAS, ft = ht ? flags[c + 1] : GAS;
+        // a GAS cell whose six face neighbours are GAS (or outside y / z) has zero
+        // velocity on every face: phi_tmp = reinit(phi) exactly
+        const bool quiet = flag == GAS && ((fw == GAS) & (fe == GAS) & (fs == GAS) & (fn == GAS) &
+                                           (fb == GAS) & (ft == GAS));
+        if (!quiet) {
+            const bool moving = flag != GAS;
+            const float vx = moving ? ux[c] : 0.0f, vy = moving ? uy[c] : 0.0f;
+            const float vz = moving ? uz[c] : 0.0f;
+            // flux through the face between this cell and neighbour cn (flag fn_):
+            // face velocity = mean of the lower and upper cell, upwind phi
+            auto flux = [&](bool exists, int fn_, int cn, const float* vel, float v_own,
+                            bool own_lower) -> float {
+                if (!exists || fn_ == SOLID) return 0.0f;
+                const float vn = fn_ != GAS ? vel[cn] : 0.0f;
+                const float uf = own_lower ? 0.5f * (v_own + vn) : 0.5f * (vn + v_own);
+                if (uf > 0.0f) return uf * (own_lower ? p0 : phi[cn]);
+                return uf * (own_lower ? phi[cn] : p0);
+            };
+            const float Fe = flux(true, fe, ce, ux, vx, true);
+            const float Fw = flux(true, fw, cw, ux, vx, false);
+            const float Fn = flux(hn, fn, c + sy, uy, vy, true);
+            const float Fs = flux(hs, fs, c - sy, uy, vy, false);
+            const float Ft = flux(ht, ft, c + 1, uz, vz, true);
+            const float Fb = flux(hb, fb, c - 1, uz, vz, false);
+            p = p0 - (Fe - Fw) - (Fn - Fs) - (Ft - Fb);
+        }
+    }
+    phi_tmp[c] = reinit_phi(p, flag);
+}
+
 __global__ void __launch_bounds__(256) k_vof_advect(Dims d, const float* __restrict__ phi,
                                                     float* __restrict__ phi_tmp,
                                                     const float* __restrict__ ux,
@@ -567,23 +891,27 @@ __global__ void __launch_bounds__(256) k_vof_advect(Dims d, const float* __restr
                                                     const int32_t* __restrict__ flags) {
     int i, j, k, c;
     if (!tile_cell(d, i, j, k, c)) return;
-    const int flag = flags[c];
-    float p = phi[c];
-    if (flag == GAS) {
-        const int sx = d.ny * d.nz;
-        int im = i > 0 ? c - sx : c + (d.nx - 1) * sx;
-        int ip = i < d.nx - 1 ? c + sx : c - (d.nx - 1) * sx;
-        // all six loads issued together (no short-circuit chain of dependent loads)
-        const int fa = flags[im], fb = flags[ip];
-        const int fc = j > 0 ? flags[c - d.nz] : GAS, fd = j < d.ny - 1 ? flags[c + d.nz] : GAS;
-        const int fe = k > 0 ? flags[c - 1] : GAS, ff = k < d.nz - 1 ? flags[c + 1] : GAS;
-        const bool quiet = ((fa == GAS) & (fb == GAS) & (fc == GAS) & (fd == GAS) & (fe == GAS) &
-                            (ff == GAS)) != 0;
-        if (!quiet) p = advect_phi_cell(d, phi, ux, uy, uz, flags, i, j, k, flag);
-    } else if (flag != SOLID) {
-        p = advect_phi_cell(d, phi, ux, uy, uz, flags, i, j, k, flag);
+    vof_cell(d, phi, phi_tmp, ux, uy, uz, flags, i, j, k, c);
+}
+
+// VOF advection over the tiles of the work list.  In a quiet tile every cell
+// within two lattice steps is GAS: all face velocities vanish and phi is
+// already reinitialised, so phi_tmp would equal phi; the column pass skips
+// those tiles, and a worked cell next to one only compares its phi_tmp (<=
+// phi < 0.05 there) against 0.55.
+__global__ void __launch_bounds__(256) k_vof_list(Dims d, const float* __restrict__ phi,
+                                                  float* __restrict__ phi_tmp,
+                                                  const float* __restrict__ ux,
+                                                  const float* __restrict__ uy,
+                                                  const float* __restrict__ uz,
+                                                  const int32_t* __restrict__ flags,
+                                                  const int32_t* __restrict__ list, int tiles) {
+    const int cnt = imin(list[0], tiles);
+    for (int e = blockIdx.x; e < cnt; e += gridDim.x) {
+        int i, j, k, c;
+        if (!list_tile_cell(d, list[1 + e], i, j, k, c)) continue;
+        vof_cell(d, phi, phi_tmp, ux, uy, uz, flags, i, j, k, c);
     }
-    phi_tmp[c] = reinit_phi(p, flag);
 }
 
 struct ColumnArgs {
@@ -593,6 +921,10 @@ struct ColumnArgs {
     int zero_forces;  // keep F == 0 outside the active cells (see k_collide_list)
     int clear_all;    // the previous step left forces outside the active set
     int shard_cap;    // list slots per shard: ceil(nx*ny / kActiveShards) * nz
+    // quiet tiles (null: none): work byte per tile, chunk bits per column chunk
+    const uint8_t* tile_work;
+    uint8_t* chunk_bits;
+    int tile_history;  // 1: chunk bit 1 takes the previous bit 0; 0: history restarts
 };
 
 __device__ __forceinline__ bool is_active(int flag) { return flag == FLUID || flag == IFACE; }
@@ -628,6 +960,11 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
     int i = warp / d.ny, j = warp % d.ny;
     ContactConst cc = contact_const(a.cos_t, a.sin_t);
     const float* src = a.vof ? phi_tmp : phi;
+    const int KT = tiles_k(d), JT = tiles_j(d);
+    auto skip = [&](int k0) -> bool {
+        return a.tile_work != nullptr &&
+               a.tile_work[((int64_t)i * JT + j / kTileJ) * KT + k0 / kTileK] == 0;
+    };
     contact_column(d, src, flags, i, j, a.vof && a.wetting, cc,
                    [&](int k, int c, float v, int flag_old, bool valid) {
                        int flag = flag_old;
@@ -655,6 +992,20 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
                            }
                        }
                        if (valid && flags_copy) flags_copy[c] = flag;
+                       if (a.chunk_bits != nullptr) {
+                           // chunk bits: all GAS, that of the previous pass, top and
+                           // bottom two cells GAS (cells beyond nz count as GAS)
+                           const unsigned gm = __ballot_sync(0xffffffffu, !valid || flag == GAS);
+                           if (lane == 0) {
+                               uint8_t* cbp = a.chunk_bits + ((int64_t)i * d.ny + j) * KT + (k >> 5);
+                               const unsigned old = *cbp;
+                               unsigned nb = gm == 0xffffffffu ? 1u : 0u;
+                               if (a.tile_history && (old & 1u)) nb |= 2u;
+                               if ((gm >> 30) == 3u) nb |= 4u;
+                               if ((gm & 3u) == 3u) nb |= 8u;
+                               *cbp = (uint8_t)nb;
+                           }
+                       }
                        bool act = valid && is_active(flag);
                        unsigned m = __ballot_sync(0xffffffffu, act);
                        if (m) {
@@ -668,7 +1019,7 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
                                active_list[(int64_t)shard * a.shard_cap + base +
                                            __popc(m & ((1u << lane) - 1u))] = c;
                        }
-                   });
+                   }, skip);
 }
 
 struct CollideArgs {
@@ -997,6 +1348,12 @@ static bool tables_fields_ok(const WaamFields* f, const WaamStepParams* p) {
     return f->cp_rho_f && f->alpha_f && f->dgamma_f && f->tau_f;
 }
 
+static bool tiles_on(const WaamFields* f) {
+    return f->tile_bits != nullptr && f->tile_list != nullptr && f->tile_part != nullptr &&
+           tiles_packable(Dims{f->nx, f->ny, f->nz});
+}
+constexpr int kTileListBlocks = 148 * 6;   // persistent grid of the work-list kernels
+
 static VarPhase var_phase(const WaamStepParams* p) {
     return VarPhase{p->H_sol_t, p->H_liq_t, p->L_rho, p->Ts, p->Tl, p->T_cap};
 }
@@ -1032,6 +1389,9 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     WorkStream W(STREAM(stream), true, 4);
     if (W.err) return W.err;
     const cudaStream_t s = W.s;
+    const bool tl = tiles_on(f);
+    const int64_t n_tiles = tile_total(d);
+    const uint8_t* tile_work = tl ? f->tile_bits + (int64_t)tiles_k(d) * d.nx * d.ny : nullptr;
     if (p->collide_prev) {
         // the previous step's collision and tracers, beside this step's arc
         // stage (waam_step_main waits for them before its thermal stage)
@@ -1061,6 +1421,16 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
         if (ea) return ea;
         cudaEventRecord(aux->ev[3], aux->s3);
     }
+    if (tl) {
+        // the step's work tiles, from the chunk bits the previous column pass left
+        cudaMemsetAsync(f->tile_list, 0, sizeof(int32_t), s);
+        // one warp per block: a tile's check is ~190 independent byte loads,
+        // so the grid should reach every SM
+        k_classify_tiles<<<(int)((n_tiles + 31) / 32), 32, 0, s>>>(
+            d, f->tile_bits, const_cast<uint8_t*>(tile_work), f->tile_list, p->tile_skip);
+        int e = check_launch("k_classify_tiles");
+        if (e) return e;
+    }
     if (!p->welding) {
         k_surface_arc<<<1, 32, 0, s>>>(d, f->phi, f->flags, f->step_scalars,
                                                     p->nz_solid);
@@ -1071,12 +1441,25 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     float* shape = reinterpret_cast<float*>(static_cast<char*>(workspace) + ws_shape_offset(d.n()));
     const int tiles = (int)tile_grid(d).x * (int)tile_grid(d).y * d.nx;
     const int blocks = tiles < kTileRedBlocks ? tiles : kTileRedBlocks;
+    PhaseParams ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
+    if (tl) {
+        k_arc_norm_list<<<blocks, tile_block(), 0, s>>>(
+            d, f->flags, f->f_l, f->phi, p->nz_solid, a, f->step_scalars, p->arc_k_offset, Qe_dt,
+            p->dx3, ws, shape, f->tile_list, tile_work, f->tile_part, (int)n_tiles);
+        int e = check_launch("k_arc_norm_list");
+        if (e) return e;
+        const int lb = (int)(n_tiles < kTileListBlocks ? n_tiles : kTileListBlocks);
+        k_arc_inject_list<<<lb, tile_block(), 0, s>>>(
+            d, f->H, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, p->cap_enabled, ph,
+            p->use_tables ? f->cp_rho_f : nullptr, var_phase(p), shape, f->tile_list,
+            (int)n_tiles);
+        return check_launch("k_arc_inject_list");
+    }
     k_arc_norm_tiles<<<blocks, tile_block(), 0, s>>>(
         d, f->flags, f->f_l, f->phi, p->nz_solid, a, f->step_scalars, p->arc_k_offset, Qe_dt,
         p->dx3, ws, shape);
     int e = check_launch("k_arc_norm_tiles");
     if (e) return e;
-    PhaseParams ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
     k_arc_inject_tiles<<<tile_grid(d), tile_block(), 0, s>>>(
         d, f->H, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, p->cap_enabled, ph,
         p->use_tables ? f->cp_rho_f : nullptr, var_phase(p), shape);
@@ -1300,15 +1683,34 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
             cudaEventRecord(aux->ev[q], aux->s2);
             cudaStreamWaitEvent(s, aux->ev[q], 0);
         };
+        // the work tiles waam_step_pre listed (quiet tiles skipped), or every tile
+        const bool tl = tiles_on(f);
+        const int n_tiles = (int)tile_total(d);
+        const int lb = n_tiles < kTileListBlocks ? n_tiles : kTileListBlocks;
+        auto launch_vof = [&](cudaStream_t st) {
+            if (tl)
+                k_vof_list<<<lb, tile_block(), 0, st>>>(d, f->phi, f->phi_tmp, f->ux, f->uy, f->uz,
+                                                        f->flags, f->tile_list, n_tiles);
+            else
+                k_vof_advect<<<tile_grid(d), tile_block(), 0, st>>>(d, f->phi, f->phi_tmp, f->ux,
+                                                                     f->uy, f->uz, f->flags);
+            return check_launch("k_vof_advect");
+        };
         if (overlap && p->vof) {
             fork(0);
-            k_vof_advect<<<tile_grid(d), tile_block(), 0, aux->s2>>>(d, f->phi, f->phi_tmp, f->ux,
-                                                                      f->uy, f->uz, f->flags);
-            e = check_launch("k_vof_advect");
+            e = launch_vof(aux->s2);
             if (e) return e;
         }
         mark(0);
-        if (p->use_tables)
+        if (tl && p->use_tables)
+            k_thermal_list<true><<<lb, tile_block(), 0, s>>>(
+                d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
+                f->T_prev, f->dT_dt, active_count, ta, tba, f->status, f->tile_list, n_tiles);
+        else if (tl)
+            k_thermal_list<false><<<lb, tile_block(), 0, s>>>(
+                d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
+                f->T_prev, f->dT_dt, active_count, ta, tba, f->status, f->tile_list, n_tiles);
+        else if (p->use_tables)
             k_thermal_fused<true><<<tile_grid(d), tile_block(), 0, s>>>(
                 d, f->H, f->H_next, f->T, f->T_next, f->f_l, f->ux, f->uy, f->uz, f->flags, f->T_max,
                 f->T_prev, f->dT_dt, active_count, ta, tba, f->status);
@@ -1324,9 +1726,7 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
             if (overlap) {
                 join(1);
             } else {
-                k_vof_advect<<<tile_grid(d), tile_block(), 0, s>>>(d, f->phi, f->phi_tmp, f->ux,
-                                                                    f->uy, f->uz, f->flags);
-                e = check_launch("k_vof_advect");
+                e = launch_vof(s);
                 if (e) return e;
             }
         }
@@ -1352,6 +1752,9 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         ca.zero_forces = p->forces_from_buffer ? 0 : 1;
         ca.clear_all = p->clear_forces;
         ca.shard_cap = (int)shard_cap;
+        ca.tile_work = tl ? f->tile_bits + (int64_t)tiles_k(d) * d.nx * d.ny : nullptr;
+        ca.chunk_bits = tl ? f->tile_bits : nullptr;
+        ca.tile_history = p->tile_skip ? 1 : 0;
         k_column<<<col_blocks, kThreads, 0, s>>>(d, f->phi_tmp, f->phi, f->flags, f->f_l, f->T_next,
                                                  f->t800, f->t1100, f->tsol, f->Fx, f->Fy, f->Fz,
                                                  active_list, active_count, f->flags_copy_w,

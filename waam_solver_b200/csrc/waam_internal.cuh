@@ -60,6 +60,37 @@ __device__ __forceinline__ bool tile_cell(const Dims& d, int& i, int& j, int& k,
     return true;
 }
 
+// Tile numbering of the quiet-tile lists: t = (i * tiles_j + j / kTileJ) *
+// tiles_k + k / kTileK (WaamFields.tile_bits / tile_list).
+__host__ __device__ inline int tiles_k(const Dims& d) { return (d.nz + kTileK - 1) / kTileK; }
+__host__ __device__ inline int tiles_j(const Dims& d) { return (d.ny + kTileJ - 1) / kTileJ; }
+__host__ __device__ inline int64_t tile_total(const Dims& d) {
+    return (int64_t)tiles_k(d) * tiles_j(d) * d.nx;
+}
+
+// Work-list entries pack a tile as (i << 16) | (j / kTileJ << 6) | k / kTileK, so
+// the list kernels decode them with shifts; quiet-tile skipping therefore
+// needs tiles_k <= 64 and tiles_j <= 1024 (nz <= 2048, ny <= 8192).
+__host__ __device__ inline bool tiles_packable(const Dims& d) {
+    return tiles_k(d) <= 64 && tiles_j(d) <= 1024 && d.nx <= 65535;
+}
+__host__ __device__ inline int pack_tile(int i, int jt, int kt) { return (i << 16) | (jt << 6) | kt; }
+__host__ __device__ inline int64_t tile_index(const Dims& d, int e) {
+    return ((int64_t)(e >> 16) * tiles_j(d) + ((e >> 6) & 1023)) * tiles_k(d) + (e & 63);
+}
+
+// The cell of this thread (threadIdx.x along k, threadIdx.y along j) in the
+// tile of packed work-list entry e.
+__device__ __forceinline__ bool list_tile_cell(const Dims& d, int e, int& i, int& j, int& k,
+                                               int& c) {
+    k = (e & 63) * kTileK + threadIdx.x;
+    j = ((e >> 6) & 1023) * kTileJ + threadIdx.y;
+    i = e >> 16;
+    if (k >= d.nz || j >= d.ny) return false;
+    c = (i * d.ny + j) * d.nz + k;
+    return true;
+}
+
 // Slots of the fused step's device scalars (WaamFields::step_scalars).
 constexpr int kScalarArcK = 0;   // resolved arc k (written by the surface query)
 constexpr int kScalarWsum = 1;   // arc weight sum

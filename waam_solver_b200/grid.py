@@ -117,6 +117,15 @@ class WAAMGrid:
         self.step_scalars = torch.zeros(16, **f32)
         # health word of the fused step (WAAM_HEALTH_* bits, see WAAMTwin.health)
         self.step_status = torch.zeros(1, dtype=torch.int32, device=dev)
+        # quiet-tile skipping of the fused step (WaamFields.tile_*): column-chunk
+        # bits then one work byte per 32 x 8 tile, the work-tile list, per-tile
+        # arc weight sums; their history is valid while _tiles_valid holds
+        kt, jt = (self.nz + 31) // 32, (self.ny + 7) // 8
+        n_tiles = kt * jt * self.nx
+        self.tile_bits = torch.zeros(kt * self.nx * self.ny + n_tiles, dtype=torch.uint8, device=dev)
+        self.tile_list = torch.zeros(1 + n_tiles, dtype=torch.int32, device=dev)
+        self.tile_part = torch.zeros(n_tiles, dtype=torch.float64, device=dev)
+        self._tiles_valid = False
         self.telem_fl_slice = torch.zeros((self.ny, self.nz), **f32)
         self.porosity_pos = torch.zeros((self.max_tracers, 3), **f32)
         self.porosity_active = torch.zeros(self.max_tracers, dtype=torch.int32, device=dev)
@@ -292,6 +301,7 @@ class WAAMGrid:
         """Inverse of state_dict (numpy arrays or tensors)."""
         self.flush_stream()
         self._forces_dirty = True
+        self._tiles_valid = False
         if self._has_lorentz:
             # the potential buffers may now hold anything at fixed cells: the
             # next solve treats every fixed cell as newly fixed

@@ -12,6 +12,7 @@ raises.
 from __future__ import annotations
 
 import ctypes
+import weakref
 import math
 
 import torch
@@ -90,7 +91,42 @@ def workspace_for(t):
     return ws.data_ptr(), ws.numel()
 
 
+# Entry points that can change flags, phi, f_l, H, T or the material-property
+# fields.  The fused step keeps a history of all-GAS tiles from step to step
+# (quiet-tile skipping); a grid trusts it only while STATE_EPOCH is the value
+# it saw at its last step.
+_TILE_STATE_WRITERS = frozenset({
+    "waam_advect_diffuse_temperature", "waam_advect_diffuse_temperature_variable",
+    "waam_advect_phi", "waam_apply_contact_angle_phi_bc", "waam_apply_thermal_boundary_losses",
+    "waam_clamp_enthalpy_ceiling_scalar", "waam_clamp_enthalpy_ceiling_variable_cp",
+    "waam_clamp_enthalpy_floor", "waam_clamp_enthalpy_floor_scalar", "waam_deposit_droplet",
+    "waam_feed_wire", "waam_feed_wire_surface", "waam_init_grid", "waam_inject_arc_heat",
+    "waam_inject_goldak_heat", "waam_refresh_thermal_properties", "waam_reinitialize_phi",
+    "waam_remelt_hot_solid", "waam_remelt_hot_solid_scalar", "waam_shift_window_x",
+    "waam_solidify_cooled_metal", "waam_solidify_trailing_pool",
+    "waam_solidify_trailing_pool_scalar", "waam_sync_phi_liquid_fraction",
+    "waam_update_flags_from_phi", "waam_update_phase", "waam_update_phase_variable_cp"})
+STATE_EPOCH = [0]
+# Grids whose last fused step left work pending (its stream, or its collision,
+# tracers and stream): a state-writing operator call runs that work first,
+# since the pending collision reads phi, T, f_l and flags.  IN_FUSED_STEP
+# marks the fused step's own operator calls.
+PENDING_GRIDS = weakref.WeakSet()
+IN_FUSED_STEP = [False]
+
+
+def state_changed():
+    """Record a change of flags / phi / f_l / H / T made outside the fused step,
+    after running the work a pipelined step left pending."""
+    if not IN_FUSED_STEP[0]:
+        for g in list(PENDING_GRIDS):
+            g.flush_stream()
+    STATE_EPOCH[0] += 1
+
+
 def _call(name, *args):
+    if name in _TILE_STATE_WRITERS:
+        state_changed()
     return _native.call(name, *args)
 
 
@@ -632,6 +668,7 @@ def stream(f_src, f_dst, flags, FLAG_SOLID, FLAG_GAS, nx, ny, nz):
 # (kernels.py:2085-2155, 3089-3179); they are set-up code, not step code.
 def init_poiseuille_channel(f, rho, ux, uy, uz, f_l, phi, flags, rho0, ny, nz, fx_lu, nu_lu,
                             FLAG_FLUID, FLAG_SOLID):
+    state_changed()
     nx = rho.shape[0]
     dev = rho.device
     j = torch.arange(ny, device=dev).view(1, ny, 1).expand(nx, ny, nz)
@@ -665,6 +702,7 @@ def set_uniform_Fx(Fx, Fy, Fz, fx_lu, flags, FLAG_FLUID):
 
 
 def prescribe_gaussian_pulse(T, H, f_l, flags, T_bg, A, sigma_m, cx, cy, cz, dx, cp_rho, FLAG_GAS):
+    state_changed()
     nx, ny, nz = T.shape
     dev = T.device
     f32 = dict(dtype=torch.float32, device=dev)
@@ -682,11 +720,13 @@ def prescribe_gaussian_pulse(T, H, f_l, flags, T_bg, A, sigma_m, cx, cy, cz, dx,
 
 
 def sync_T_from_H(H, T, cp_rho):
+    state_changed()
     T.copy_(H / float(cp_rho))
 
 
 def init_stefan_liquid_column(T, H, f_l, phi, flags, nz_solid, T_amb, T_init, cp_rho, L_rho,
                               T_solidus, T_liquidus, FLAG_FLUID, FLAG_SOLID):
+    state_changed()
     nx, ny, nz = T.shape
     k = torch.arange(nz, device=T.device).view(1, 1, nz).expand(nx, ny, nz)
     sol = k < int(nz_solid)
@@ -702,6 +742,7 @@ def init_stefan_liquid_column(T, H, f_l, phi, flags, nz_solid, T_amb, T_init, cp
 
 
 def clamp_substrate_enthalpy(H, T, f_l, flags, nz_solid, T_amb, cp_rho, FLAG_SOLID):
+    state_changed()
     nx, ny, nz = T.shape
     k = torch.arange(nz, device=T.device).view(1, 1, nz).expand(nx, ny, nz)
     m = (k < int(nz_solid)) & (flags == FLAG_SOLID)
