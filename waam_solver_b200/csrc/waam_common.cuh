@@ -416,9 +416,10 @@ __device__ __forceinline__ float thermal_dh(const Dims d, const float* __restric
 }
 
 // thermal_dh with neighbour offsets instead of clamped coordinates (same
-// values): a clamped neighbour is the cell itself (non-gas: the centre
-// value), and a clamped second neighbour is the first one, whose masked value
-// it then takes either way.  Tc = T[c].
+// values): a neighbour outside the domain clamps to the cell itself
+// (non-gas: the centre value) and a second neighbour outside it to the first
+// one.  Every value and its flag are loaded unconditionally and the GAS
+// fallback is applied afterwards, so no load waits on another.  Tc = T[c].
 __device__ __forceinline__ float thermal_dh_offsets(const Dims& d, const float* __restrict__ Hs,
                                                     const float* __restrict__ T,
                                                     const int32_t* __restrict__ flags, float u,
@@ -426,24 +427,34 @@ __device__ __forceinline__ float thermal_dh_offsets(const Dims& d, const float* 
                                                     int flag, float Hc, float Tc, float cpa,
                                                     float dt) {
     const int sx = d.ny * d.nz, sy = d.nz;
-    const bool mxm = i > 0 && flags[c - sx] != GAS, mxp = i < d.nx - 1 && flags[c + sx] != GAS;
-    const bool mym = j > 0 && flags[c - sy] != GAS, myp = j < d.ny - 1 && flags[c + sy] != GAS;
-    const bool mzm = k > 0 && flags[c - 1] != GAS, mzp = k < d.nz - 1 && flags[c + 1] != GAS;
-    const float Tim = mxm ? T[c - sx] : Tc, Tip = mxp ? T[c + sx] : Tc;
-    const float Tjm = mym ? T[c - sy] : Tc, Tjp = myp ? T[c + sy] : Tc;
-    const float Tkm = mzm ? T[c - 1] : Tc, Tkp = mzp ? T[c + 1] : Tc;
+    const int cxm = i > 0 ? c - sx : c, cxp = i < d.nx - 1 ? c + sx : c;
+    const int cym = j > 0 ? c - sy : c, cyp = j < d.ny - 1 ? c + sy : c;
+    const int czm = k > 0 ? c - 1 : c, czp = k < d.nz - 1 ? c + 1 : c;
+    const bool gxm = flags[cxm] == GAS, gxp = flags[cxp] == GAS, gym = flags[cym] == GAS;
+    const bool gyp = flags[cyp] == GAS, gzm = flags[czm] == GAS, gzp = flags[czp] == GAS;
+    const float tim = T[cxm], tip = T[cxp], tjm = T[cym], tjp = T[cyp], tkm = T[czm], tkp = T[czp];
+    const float Tim = gxm ? Tc : tim, Tip = gxp ? Tc : tip;
+    const float Tjm = gym ? Tc : tjm, Tjp = gyp ? Tc : tjp;
+    const float Tkm = gzm ? Tc : tkm, Tkp = gzp ? Tc : tkp;
     float lap = Tip + Tim + Tjp + Tjm + Tkp + Tkm - 6.0f * Tc;
     float dH = cpa * lap * dt;
     if (flag != SOLID) {
-        const float Him = mxm ? Hs[c - sx] : Hc, Hip = mxp ? Hs[c + sx] : Hc;
-        const float Hjm = mym ? Hs[c - sy] : Hc, Hjp = myp ? Hs[c + sy] : Hc;
-        const float Hkm = mzm ? Hs[c - 1] : Hc, Hkp = mzp ? Hs[c + 1] : Hc;
-        const float Himm = (i >= 2 && flags[c - 2 * sx] != GAS) ? Hs[c - 2 * sx] : Him;
-        const float Hipp = (i <= d.nx - 3 && flags[c + 2 * sx] != GAS) ? Hs[c + 2 * sx] : Hip;
-        const float Hjmm = (j >= 2 && flags[c - 2 * sy] != GAS) ? Hs[c - 2 * sy] : Hjm;
-        const float Hjpp = (j <= d.ny - 3 && flags[c + 2 * sy] != GAS) ? Hs[c + 2 * sy] : Hjp;
-        const float Hkmm = (k >= 2 && flags[c - 2] != GAS) ? Hs[c - 2] : Hkm;
-        const float Hkpp = (k <= d.nz - 3 && flags[c + 2] != GAS) ? Hs[c + 2] : Hkp;
+        const int cxmm = i >= 2 ? c - 2 * sx : cxm, cxpp = i <= d.nx - 3 ? c + 2 * sx : cxp;
+        const int cymm = j >= 2 ? c - 2 * sy : cym, cypp = j <= d.ny - 3 ? c + 2 * sy : cyp;
+        const int czmm = k >= 2 ? c - 2 : czm, czpp = k <= d.nz - 3 ? c + 2 : czp;
+        const float him = Hs[cxm], hip = Hs[cxp], hjm = Hs[cym], hjp = Hs[cyp];
+        const float hkm = Hs[czm], hkp = Hs[czp];
+        const float himm = Hs[cxmm], hipp = Hs[cxpp], hjmm = Hs[cymm], hjpp = Hs[cypp];
+        const float hkmm = Hs[czmm], hkpp = Hs[czpp];
+        const bool gxmm = flags[cxmm] == GAS, gxpp = flags[cxpp] == GAS;
+        const bool gymm = flags[cymm] == GAS, gypp = flags[cypp] == GAS;
+        const bool gzmm = flags[czmm] == GAS, gzpp = flags[czpp] == GAS;
+        const float Him = gxm ? Hc : him, Hip = gxp ? Hc : hip;
+        const float Hjm = gym ? Hc : hjm, Hjp = gyp ? Hc : hjp;
+        const float Hkm = gzm ? Hc : hkm, Hkp = gzp ? Hc : hkp;
+        const float Himm = gxmm ? Him : himm, Hipp = gxpp ? Hip : hipp;
+        const float Hjmm = gymm ? Hjm : hjmm, Hjpp = gypp ? Hjp : hjpp;
+        const float Hkmm = gzmm ? Hkm : hkmm, Hkpp = gzpp ? Hkp : hkpp;
         float gx = upwind_grad(u, Himm, Him, Hc, Hip, Hipp);
         float gy = upwind_grad(v, Hjmm, Hjm, Hc, Hjp, Hjpp);
         float gz = upwind_grad(w, Hkmm, Hkm, Hc, Hkp, Hkpp);
@@ -774,6 +785,202 @@ __device__ __forceinline__ void cell_forces(const Dims d, const ForceParams& P,
             fx = fx * s;
             fy = fy * s;
             fz = fz * s;
+        }
+    }
+}
+
+// cell_forces with every stencil value requested before any is used: the six
+// face neighbours of phi, T and flags (clamped at the domain faces, as
+// cell_forces clamps them) and, for a CSF cell, the twelve further phi
+// values the six neighbour normals of its curvature need.  The expressions,
+// operands and order are cell_forces' own, so the forces are identical; the
+// loads no longer wait on the branches that consume them (one memory round
+// trip instead of one per force term).  c = d.idx(i, j, k).
+__device__ __forceinline__ void cell_forces_preloaded(const Dims d, const ForceParams& P,
+                                                      const float* __restrict__ phi,
+                                                      const float* __restrict__ T,
+                                                      const int32_t* __restrict__ flags, int i,
+                                                      int j, int k, int c, float fl, float& fx,
+                                                      float& fy, float& fz) {
+    const float eps = 1e-6f;
+    const int sx = d.ny * d.nz, sy = d.nz;
+    // face neighbours, clamped to the domain (imin / imax of cell_forces)
+    const int cxm = i > 0 ? c - sx : c, cxp = i < d.nx - 1 ? c + sx : c;
+    const int cym = j > 0 ? c - sy : c, cyp = j < d.ny - 1 ? c + sy : c;
+    const int czm = k > 0 ? c - 1 : c, czp = k < d.nz - 1 ? c + 1 : c;
+    const float Pxm = phi[cxm], Pxp = phi[cxp], Pym = phi[cym], Pyp = phi[cyp];
+    const float Pzm = phi[czm], Pzp = phi[czp];
+    const float Txm = T[cxm], Txp = T[cxp], Tym = T[cym], Typ = T[cyp], Tzm = T[czm], Tzp = T[czp];
+    const float Tc = T[c];
+    const bool csf = P.csf && !(i < 1 || j < 1 || k < 1 || i > d.nx - 2 || j > d.ny - 2 ||
+                                k > d.nz - 2);
+    // the curvature's second ring (CSF cells are interior: the first ring is
+    // unclamped, the second clamps at the domain faces)
+    float P0 = 0.0f, Pxpp = 0.0f, Pxmm = 0.0f, Pypp = 0.0f, Pymm = 0.0f, Pzpp = 0.0f, Pzmm = 0.0f;
+    float Pxpyp = 0.0f, Pxpym = 0.0f, Pxmyp = 0.0f, Pxmym = 0.0f, Pxpzp = 0.0f, Pxpzm = 0.0f;
+    float Pxmzp = 0.0f, Pxmzm = 0.0f, Pypzp = 0.0f, Pypzm = 0.0f, Pymzp = 0.0f, Pymzm = 0.0f;
+    int fxm = FLUID, fxp = FLUID, fym = FLUID, fyp = FLUID, fzm = FLUID, fzp = FLUID;
+    if (csf) {
+        P0 = phi[c];
+        Pxpp = phi[i + 2 <= d.nx - 1 ? c + 2 * sx : c + sx];
+        Pxmm = phi[i - 2 >= 0 ? c - 2 * sx : c - sx];
+        Pypp = phi[j + 2 <= d.ny - 1 ? c + 2 * sy : c + sy];
+        Pymm = phi[j - 2 >= 0 ? c - 2 * sy : c - sy];
+        Pzpp = phi[k + 2 <= d.nz - 1 ? c + 2 : c + 1];
+        Pzmm = phi[k - 2 >= 0 ? c - 2 : c - 1];
+        Pxpyp = phi[c + sx + sy];
+        Pxpym = phi[c + sx - sy];
+        Pxmyp = phi[c - sx + sy];
+        Pxmym = phi[c - sx - sy];
+        Pxpzp = phi[c + sx + 1];
+        Pxpzm = phi[c + sx - 1];
+        Pxmzp = phi[c - sx + 1];
+        Pxmzm = phi[c - sx - 1];
+        Pypzp = phi[c + sy + 1];
+        Pypzm = phi[c + sy - 1];
+        Pymzp = phi[c - sy + 1];
+        Pymzm = phi[c - sy - 1];
+        if (P.wetting != 0) {
+            fxm = flags[c - sx];
+            fxp = flags[c + sx];
+            fym = flags[c - sy];
+            fyp = flags[c + sy];
+            fzm = flags[c - 1];
+            fzp = flags[c + 1];
+        }
+    }
+    // kernels.py:858-926 compute_csf_tension
+    if (csf) {
+        // _phi_unit_normal_at of the cell and of its six neighbours (phi_normal)
+        auto gmag3 = [](float a, float b, float cc) { return sqrtf(a * a + b * b + cc * cc); };
+        const float d0x = 0.5f * (Pxp - Pxm), d0y = 0.5f * (Pyp - Pym), d0z = 0.5f * (Pzp - Pzm);
+        const float g0 = gmag3(d0x, d0y, d0z);
+        float kappa = 0.0f;
+        if (g0 >= eps) {
+            const float n0x = d0x / g0, n0y = d0y / g0, n0z = d0z / g0;
+            // x neighbours: x component of their normal
+            float ax = 0.5f * (Pxpp - P0), ay = 0.5f * (Pxpyp - Pxpym), az = 0.5f * (Pxpzp - Pxpzm);
+            float g = gmag3(ax, ay, az);
+            const float nxp = g < eps ? n0x : ax / g;
+            ax = 0.5f * (P0 - Pxmm); ay = 0.5f * (Pxmyp - Pxmym); az = 0.5f * (Pxmzp - Pxmzm);
+            g = gmag3(ax, ay, az);
+            const float nxm = g < eps ? n0x : ax / g;
+            // y neighbours: y component
+            ax = 0.5f * (Pxpyp - Pxmyp); ay = 0.5f * (Pypp - P0); az = 0.5f * (Pypzp - Pypzm);
+            g = gmag3(ax, ay, az);
+            const float nyp = g < eps ? n0y : ay / g;
+            ax = 0.5f * (Pxpym - Pxmym); ay = 0.5f * (P0 - Pymm); az = 0.5f * (Pymzp - Pymzm);
+            g = gmag3(ax, ay, az);
+            const float nym = g < eps ? n0y : ay / g;
+            // z neighbours: z component
+            ax = 0.5f * (Pxpzp - Pxmzp); ay = 0.5f * (Pypzp - Pymzp); az = 0.5f * (Pzpp - P0);
+            g = gmag3(ax, ay, az);
+            const float nzp = g < eps ? n0z : az / g;
+            ax = 0.5f * (Pxpzm - Pxmzm); ay = 0.5f * (Pypzm - Pymzm); az = 0.5f * (P0 - Pzmm);
+            g = gmag3(ax, ay, az);
+            const float nzm = g < eps ? n0z : az / g;
+            const float div_n = 0.5f * (nxp - nxm) + 0.5f * (nyp - nym) + 0.5f * (nzp - nzm);
+            kappa = -div_n;
+        }
+        const float gmag = g0;
+        if (gmag >= eps) {
+            const float dpx = 0.5f * (Pxp - Pxm), dpy = 0.5f * (Pyp - Pym), dpz = 0.5f * (Pzp - Pzm);
+            float sx_ = P.gamma_lu * kappa * dpx;
+            float sy_ = P.gamma_lu * kappa * dpy;
+            float sz_ = P.gamma_lu * kappa * dpz;
+            if (P.wetting != 0) {
+                float wx = 0.0f, wy = 0.0f, wz = 0.0f;
+                int has_wall = 0;
+                if (fxm == SOLID) { wx += 1.0f; has_wall = 1; }
+                if (fxp == SOLID) { wx -= 1.0f; has_wall = 1; }
+                if (fym == SOLID) { wy += 1.0f; has_wall = 1; }
+                if (fyp == SOLID) { wy -= 1.0f; has_wall = 1; }
+                if (fzm == SOLID) { wz += 1.0f; has_wall = 1; }
+                if (fzp == SOLID) { wz -= 1.0f; has_wall = 1; }
+                float wmag = sqrtf(wx * wx + wy * wy + wz * wz);
+                if (wmag > 1e-8f) {
+                    wx /= wmag;
+                    wy /= wmag;
+                    wz /= wmag;
+                }
+                if (has_wall != 0) {
+                    float nxn = dpx / gmag, nyn = dpy / gmag, nzn = dpz / gmag;
+                    // kernels.py:723-766 _correct_normal_contact_angle
+                    float dot = nxn * wx + nyn * wy + nzn * wz;
+                    float tx = nxn - dot * wx, ty = nyn - dot * wy, tz = nzn - dot * wz;
+                    float tmag = sqrtf(tx * tx + ty * ty + tz * tz);
+                    float ncx = 0.0f, ncy = 0.0f, ncz = 0.0f;
+                    if (tmag > 1e-8f) {
+                        ncx = P.cos_t * wx + P.sin_t * tx / tmag;
+                        ncy = P.cos_t * wy + P.sin_t * ty / tmag;
+                        ncz = P.cos_t * wz + P.sin_t * tz / tmag;
+                    } else if (fabsf(wz) > 0.5f) {
+                        ncx = P.sin_t; ncy = 0.0f; ncz = P.cos_t;
+                    } else if (fabsf(wx) > 0.5f) {
+                        ncx = P.cos_t; ncy = P.sin_t; ncz = 0.0f;
+                    } else {
+                        ncx = P.cos_t * wx + P.sin_t; ncy = P.cos_t * wy; ncz = P.cos_t * wz;
+                    }
+                    float cmag = sqrtf(ncx * ncx + ncy * ncy + ncz * ncz);
+                    if (cmag > 1e-8f) {
+                        ncx /= cmag;
+                        ncy /= cmag;
+                        ncz /= cmag;
+                    }
+                    sx_ = P.gamma_lu * kappa * ncx * gmag;
+                    sy_ = P.gamma_lu * kappa * ncy * gmag;
+                    sz_ = P.gamma_lu * kappa * ncz * gmag;
+                }
+            }
+            fx += sx_;
+            fy += sy_;
+            fz += sz_;
+        }
+    }
+    // kernels.py:2158-2217 compute_marangoni_force
+    if (!(fl < 0.05f)) {
+        float dx_ = 0.5f * (Pxp - Pxm);
+        float dy_ = 0.5f * (Pyp - Pym);
+        float dz_ = 0.5f * (Pzp - Pzm);
+        float g = sqrtf(dx_ * dx_ + dy_ * dy_ + dz_ * dz_);
+        if (!(g < 1e-6f)) {
+            float nxn = dx_ / g, nyn = dy_ / g, nzn = dz_ / g;
+            float tx = 0.5f * (Txp - Txm);
+            float ty = 0.5f * (Typ - Tym);
+            float tz = 0.5f * (Tzp - Tzm);
+            float nd = nxn * tx + nyn * ty + nzn * tz;
+            float sx_ = tx - nd * nxn, sy_ = ty - nd * nyn, sz_ = tz - nd * nzn;
+            float scale = P.dgamma * g;
+            fx += scale * sx_;
+            fy += scale * sy_;
+            fz += scale * sz_;
+        }
+    }
+    // physics/weld_forces.py:161-193 apply_gas_shear (solvers/coupled_step.py:325-326)
+    if (P.welding && P.W.gas_shear) gas_shear_cell(d, phi, i, j, k, P.arc_i, P.arc_j, P.W, fx, fy);
+    // kernels.py:3038-3083 apply_arc_pressure
+    if (P.welding) {
+        float dpz = Pzp - Pzm;
+        if (fabsf(dpz) > 0.05f) {
+            float di = (float)i - P.arc_i, dj = (float)j - P.arc_j, dk = (float)k - P.arc_k;
+            float r2 = di * di + dj * dj + dk * dk * 0.1f;
+            fz += -P.p_Flu * waam_expf(-r2 * P.p_inv2s2);
+        }
+    }
+    // physics/weld_forces.py:137-158 apply_recoil (solvers/coupled_step.py:334)
+    if (P.welding && P.W.recoil) recoil_cell(d, phi, Tc, i, j, k, P.arc_i, P.arc_j, P.W, fz);
+    // kernels.py:2756-2772 add_hydrostatic_gravity
+    if (P.hydro && fl > 0.0f) fz += -P.rho_ref * P.g_lu * fl;
+    // kernels.py:2729-2753 add_buoyancy
+    if (fl > 0.0f) fz += P.rho_ref * P.g_lu * P.beta * (Tc - P.T_ref) * fl;
+    // kernels.py:3286-3309 clamp_body_force_magnitude
+    if (P.F_cap > 0.0f) {
+        float mag = sqrtf(fx * fx + fy * fy + fz * fz);
+        if (mag > P.F_cap) {
+            float s_ = P.F_cap / (mag + 1e-12f);
+            fx = fx * s_;
+            fy = fy * s_;
+            fz = fz * s_;
         }
     }
 }

@@ -591,9 +591,11 @@ __global__ void __launch_bounds__(256) k_arc_norm_list(Dims d, const int32_t* __
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // the slots come from other blocks (fenced before their arrival count):
+    // read them from L2 (__ldcg), independent loads that can all be in flight
     double acc = 0.0;
     for (int t = tid; t < tiles; t += kTileK * kTileJ)
-        acc += tile_work[t] ? ((volatile double*)tile_part)[t] : 0.0;
+        acc += tile_work[t] ? __ldcg(tile_part + t) : 0.0;
     const double tot = tile_block_sum(acc);
     if (tid == 0) {
         *ws.counter = 0u;
@@ -1127,7 +1129,7 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
             fz = Fz[c];
         }
         float fl = f_l[c];
-        cell_forces(d, P, phi, T, flags, i, j, k, fl, fx, fy, fz);
+        cell_forces_preloaded(d, P, phi, T, flags, i, j, k, c, fl, fx, fy, fz);
         if (lorentz) {
             // the reference order: the other forces, J x B, then the clamp
             // (solvers/coupled_step.py:298-362; kernels.py:3286-3309)
