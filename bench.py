@@ -967,6 +967,20 @@ def run_b200(args, w):
         dist.destroy_process_group()
 
 
+def profile_run(w, n):
+    """The workload's first n steps from reset, pending work flushed -- the small
+    case that kernel captures under ncu select launches from (-k, -s, -c)."""
+    import torch
+    tw = build_twin(w, torch.device("cuda", 0))
+    for x, y, welding in path_steps(w, tw.grid.dt, n):
+        tw.step(x, y, welding)
+    tw.grid.flush_stream()
+    torch.cuda.synchronize()
+    g = tw.grid
+    print("profile run: %d steps, %d of %d tiles worked at the last step"
+          % (n, int(g.tile_list[0].item()), g.tile_list.numel() - 1))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -984,13 +998,18 @@ def main():
                          "storage and in float32; report remelt depth, HAZ T_max, pool W/D")
     ap.add_argument("--spinup", type=int, default=None,
                     help="steps run before warm-up (default: the workload's spin-up)")
+    ap.add_argument("--profile", type=int, default=None, metavar="N",
+                    help="run N steps of the workload from reset on cuda:0 and exit, no timing "
+                         "and no JSON line (the case of the kernel captures under ncu)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     w = dict(WORKLOADS[args.workload])
     if args.spinup is not None:
         w["spinup"] = args.spinup
-    if args.impl == "reference":
+    if args.profile is not None:
+        profile_run(w, args.profile)
+    elif args.impl == "reference":
         run_reference(args, w)
     else:
         run_b200(args, w)

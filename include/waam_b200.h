@@ -636,7 +636,8 @@ typedef struct WaamFields {
      * pending stream of the previous step (WaamStepParams.stream_prev) reads
      * flags_copy_r, the copy that step wrote -- so it may run on while the
      * column pass rewrites the flags, and is joined only before the
-     * collision.  The caller alternates two buffers from step to step. */
+     * collision.  The caller alternates two buffers from step to step (three
+     * with flags_copy_rr).  Quiet tiles' cells are written too (GAS). */
     int32_t* flags_copy_w;
     const int32_t* flags_copy_r;
     /* health word of the fused step (null: off), device uint32 that the
@@ -663,6 +664,10 @@ typedef struct WaamFields {
     uint8_t* tile_bits;
     int32_t* tile_list;
     double* tile_part;
+    /* the flag copy of the step before the one flags_copy_r holds, for the
+     * lagged stream (WaamStepParams.hold_stream / stream_lag); with it the
+     * caller rotates three buffers (w, r, rr) from step to step */
+    const int32_t* flags_copy_rr;
 } WaamFields;
 
 #define WAAM_HEALTH_NONFINITE_H 1u   /* H of a non-gas cell is NaN or infinite */
@@ -765,6 +770,21 @@ typedef struct WaamStepParams {
      * step after a state change, a droplet deposition, a force clear, or
      * with the remelt / solidify tail on) */
     int tile_skip;
+    /* lagged stream.  The collision of step n + 1 overwrites every population
+     * of its active cells in the buffer the stream of step n writes, and
+     * reads the buffer that stream reads, so the stream of step n needs to
+     * visit only the other cells -- and then depends on neither the
+     * collision of step n + 1 nor anything of step n + 1 but its column
+     * pass.  hold_stream = 1 (needs stream_prev = 1, defer_collide = 1 and
+     * the three flag copies): waam_step_pre does not run the previous step's
+     * pending stream; it stays pending, and the next step runs it with
+     * stream_lag = 1: waam_step_pre starts it at once beside the pending
+     * collision (which must be pending: collide_prev = 1), skipping the cells
+     * active in flags_copy_r, with the flags of flags_copy_rr; waam_step_main
+     * joins it after the column pass.  waam_step_finish with stream_lag = 1
+     * runs it before the pending collision. */
+    int stream_lag;
+    int hold_stream;
 } WaamStepParams;
 
 /* Stages of one fused step.  waam_step_pre runs the surface-height query,

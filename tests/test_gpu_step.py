@@ -181,14 +181,18 @@ def test_recoil_and_gas_shear_steps_match_oracle(step_mode, cc):
 def test_pipelined_stream_matches_in_order_stream(lorentz):
     """Each step's stream left to run beside the next step's arc, thermal and VOF
     stages (joined before the column pass) gives the same states, bit for bit,
-    as the stream run in order -- over droplet steps, graph replays and the
-    Lorentz split step; the state read-out runs the pending stream."""
+    as the stream run in order -- and so does the collision left pending as
+    well, and the stream held back one more step to run beside the next
+    collision on the cells it does not write (lagged) -- over droplet steps,
+    graph replays and the Lorentz split step; the state read-out runs the
+    pending work."""
     states = []
     more = dict(enable_lorentz=True, welding_current_A=180.0) if lorentz else {}
-    for mode in ("in_order", "stream", "stream_collide"):
+    for mode in ("in_order", "stream", "stream_collide", "lagged"):
         tw, ot, dx = _config_twins("c2", 40, 24, 24, **more)
         tw.pipeline_stream = mode != "in_order"
-        tw.pipeline_collide = mode == "stream_collide"
+        tw.pipeline_collide = mode in ("stream_collide", "lagged")
+        tw.pipeline_lag_stream = mode == "lagged"
         tw._last_droplet_time = -1.0
         for s in range(24):
             # a non-welding stretch switches the arc off and on
@@ -196,10 +200,12 @@ def test_pipelined_stream_matches_in_order_stream(lorentz):
         g = tw.grid
         if mode != "in_order":
             assert g._stream_pending
-        if mode == "stream_collide" and not lorentz:
+        if mode in ("stream_collide", "lagged") and not lorentz:
             assert g._collide_pending
+            assert g.__dict__.get("_lag_pending", False) == (mode == "lagged")
             u = g.ux.clone()              # reading a collision output runs the pending work
             assert not g._collide_pending and not g._stream_pending
+            assert not g._lag_pending
         torch.cuda.synchronize()
         states.append(g.state_dict())
         assert tw._n_droplets_fired >= 1
@@ -385,15 +391,18 @@ def test_operator_calls_after_pipelined_steps_see_streamed_populations():
 
 
 def test_quiet_tile_skipping_matches_working_every_tile():
-    """Quiet-tile skipping (the default) against every tile worked, bit for bit,
-    on a grid tall enough for quiet tiles (nz = 96: three 32-cell k tiles over
-    a 19-cell plate), through droplet steps (the tile history restarts),
-    graph replays and the pipelined stream and collision; the skipping
-    really skips (the work list is shorter than the tile count)."""
+    """Quiet-tile skipping with the lagged stream (the defaults) against every
+    tile worked and the stream run one step later, bit for bit, on a grid
+    tall enough for quiet tiles (nz = 96: three 32-cell k tiles over a
+    19-cell plate), through droplet steps (the tile history restarts), graph
+    replays and the pipelined stream and collision -- the lagged stream
+    reads flag copies that quiet tiles must still write; the skipping really
+    skips (the work list is shorter than the tile count)."""
     states, counts = [], []
     for skip in (False, True):
         tw, ot, dx = _config_twins("c2", 40, 32, 96)
         tw.skip_quiet_tiles = skip
+        tw.pipeline_lag_stream = skip
         tw._last_droplet_time = -1.0
         g = tw.grid
         n_tiles = g.tile_list.numel() - 1

@@ -33,7 +33,8 @@ class WaamFields(C.Structure):
                                         "tape_cells", "tape_count")] + [("tape_cap", C.c_int64)] + [
         ("lorentz_J", C.c_void_p * 3), ("lorentz_B", C.c_void_p * 3),
         ("flags_copy_w", C.c_void_p), ("flags_copy_r", C.c_void_p), ("status", C.c_void_p),
-        ("tile_bits", C.c_void_p), ("tile_list", C.c_void_p), ("tile_part", C.c_void_p)]
+        ("tile_bits", C.c_void_p), ("tile_list", C.c_void_p), ("tile_part", C.c_void_p),
+        ("flags_copy_rr", C.c_void_p)]
 
 
 TABLE_KNOTS = 8

@@ -66,6 +66,7 @@ class _Checkpoint:
         g = tw.grid
         g._stream_pending = False       # the checkpoint holds a streamed state
         g._collide_pending = False
+        g._lag_pending = False
         g._tiles_valid = False          # the quiet-tile history is not the checkpoint's
         for k in _FIELDS:
             getattr(g, k).copy_(self.t[k])

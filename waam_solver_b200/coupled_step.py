@@ -301,9 +301,12 @@ def _fields(g):
     f.dgamma_f, f.tau_f = g.dgamma_lu_field.data_ptr(), g.tau_field.data_ptr()
     copies = getattr(g, "flags_copies", None)
     if copies is not None:
+        # rotation of three: this step writes w, the step before wrote r, the
+        # one before that rr
         w = getattr(g, "_flags_copy_i", 0)
         f.flags_copy_w = copies[w].data_ptr()
-        f.flags_copy_r = copies[1 - w].data_ptr()
+        f.flags_copy_r = copies[(w + 2) % 3].data_ptr()
+        f.flags_copy_rr = copies[(w + 1) % 3].data_ptr()
     f.status = g.step_status.data_ptr()
     f.tile_bits = g.tile_bits.data_ptr()
     f.tile_list = g.tile_list.data_ptr()
@@ -454,6 +457,7 @@ def flush_stream(g):
         return
     g._stream_pending = False
     g._collide_pending = False
+    g._lag_pending = False      # a held stream is pending only with a collision (_pending_params)
     kernels.PENDING_GRIDS.discard(g)
     st = torch.cuda.current_stream().cuda_stream
     if collide:
@@ -528,8 +532,9 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     dx_, dy_, dz_ = getattr(twin, "_torch_dir_xyz", (1.0, 0.0, 0.0))
     p.dir_x, p.dir_y, p.dir_z = dx_, dy_, dz_
     if getattr(g, "flags_copies", None) is None:
-        # the flags of each step, copied by its column pass, for its pending stream
-        g.flags_copies = (torch.zeros_like(g.flags), torch.zeros_like(g.flags))
+        # the flags of each step, copied by its column pass, for its pending
+        # stream -- kept for two steps, for the lagged stream
+        g.flags_copies = tuple(torch.zeros_like(g.flags) for _ in range(3))
         g._flags_copy_i = 0
         g.__dict__.pop("_fields_cache", None)
     f = _fields_cached(g)
@@ -555,6 +560,12 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
                            not (twin.enable_bead_freeze or twin.enable_substrate_growth)) else 0
     p.defer_collide = 1 if (p.defer_stream and not due and not lorentz and
                             getattr(twin, "pipeline_collide", True)) else 0
+    # Lagged stream: a step that leaves its collision pending also holds back
+    # the previous step's stream, which the next step runs beside that
+    # collision, on the cells that collision does not write
+    p.stream_lag = 1 if g.__dict__.get("_lag_pending", False) else 0
+    p.hold_stream = 1 if (p.stream_prev and p.defer_collide and
+                          getattr(twin, "pipeline_lag_stream", True)) else 0
     # quiet tiles: skipped only while the tile history is the fused step's own
     # (no droplet deposition in the middle of this step, no force clear, no
     # remelt / solidify tail rewriting flags, nothing changed the state since)
@@ -566,7 +577,7 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     if not due and not lorentz and events is None and getattr(twin, "use_cuda_graphs", True):
         key = (g._read_buf is raw_field(g, "f_a"), g._cur, p.welding, p.clear_forces, p.stream_prev,
                p.defer_stream, p.collide_prev, p.collide_prev_welding, p.defer_collide,
-               g._flags_copy_i, p.tile_skip,
+               g._flags_copy_i, p.tile_skip, p.stream_lag, p.hold_stream,
                (dx_, dy_, dz_) if twin.enable_bead_freeze else None)
         done = _run_graph(twin, g, f, p, ws, key)
     if not done:
@@ -612,14 +623,16 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     g._forces_dirty = bool(p.forces_from_buffer) or lorentz
     g._stream_pending = bool(p.defer_stream)
     g._collide_pending = bool(p.defer_collide)
+    g._lag_pending = bool(p.hold_stream)
     if p.defer_stream:
         kernels.PENDING_GRIDS.add(g)
     if p.defer_collide:
         q = _native.WaamStepParams.from_buffer_copy(p)
         q.collide_prev, q.collide_prev_welding = 1, p.welding
+        q.stream_lag, q.hold_stream = p.hold_stream, 0
         g._pending_params = q
         g._pending_welding = p.welding
-    g._flags_copy_i = 1 - g._flags_copy_i    # this step's copy is read by the next step
+    g._flags_copy_i = (g._flags_copy_i + 1) % 3    # this step's copy is read by the next two
     g._tiles_valid = True                    # this step's column pass wrote the chunk bits
     g._tile_epoch = kernels.STATE_EPOCH[0]
     g.flip_thermal()

@@ -246,33 +246,44 @@ __device__ __forceinline__ void stream_cell(const Dims& d, const StreamPtrs<T>& 
     for (int q = 0; q < 19; ++q) P.dst[q][c] = v[q];
 }
 
+__device__ __forceinline__ bool is_active(int flag) { return flag == FLUID || flag == IFACE; }
+
+// next_flags (null: none): the flags of the step after the streamed one.
+// Cells active there (FLUID / IFACE) are left alone: that step's collision
+// writes all 19 populations of each of them into the buffer the stream
+// writes, and nothing reads that buffer between the two (the lagged stream
+// of WaamStepParams.hold_stream).
 template <typename T>
 __global__ void __launch_bounds__(256) k_stream(Dims d, const __grid_constant__ StreamPtrs<T> P,
-                                                const int32_t* __restrict__ flags) {
+                                                const int32_t* __restrict__ flags,
+                                                const int32_t* __restrict__ next_flags) {
     int i, j, k, c;
     if (!tile_cell(d, i, j, k, c)) return;
+    if (next_flags != nullptr && is_active(next_flags[c])) return;
     stream_cell(d, P, flags, i, j, k, c);
 }
 
 
 template <typename T>
 static void launch_stream_t(const Dims& d, const void* f_src, void* f_dst, const int32_t* flags,
-                            cudaStream_t s) {
-    k_stream<T><<<tile_grid(d), tile_block(), 0, s>>>(d, stream_ptrs<T>(d, f_src, f_dst), flags);
+                            const int32_t* next_flags, cudaStream_t s) {
+    k_stream<T><<<tile_grid(d), tile_block(), 0, s>>>(d, stream_ptrs<T>(d, f_src, f_dst), flags,
+                                                       next_flags);
 }
 
 int launch_stream(Dims d, const float* f_src, float* f_dst, const int32_t* flags, void* stream) {
-    launch_stream_t<float>(d, f_src, f_dst, flags, STREAM(stream));
+    launch_stream_t<float>(d, f_src, f_dst, flags, nullptr, STREAM(stream));
     return check_launch("k_stream");
 }
 
 // The fused step's stream: 4-byte or 2-byte stored populations.
 static int launch_stream_stored(Dims d, const void* f_src, void* f_dst, const int32_t* flags,
-                                int storage, cudaStream_t s) {
+                                int storage, cudaStream_t s,
+                                const int32_t* next_flags = nullptr) {
     if (storage == kStoreF32)
-        launch_stream_t<float>(d, f_src, f_dst, flags, s);
+        launch_stream_t<float>(d, f_src, f_dst, flags, next_flags, s);
     else
-        launch_stream_t<uint16_t>(d, f_src, f_dst, flags, s);
+        launch_stream_t<uint16_t>(d, f_src, f_dst, flags, next_flags, s);
     return check_launch("k_stream");
 }
 
@@ -929,8 +940,6 @@ struct ColumnArgs {
     int tile_history;  // 1: chunk bit 1 takes the previous bit 0; 0: history restarts
 };
 
-__device__ __forceinline__ bool is_active(int flag) { return flag == FLUID || flag == IFACE; }
-
 // Column pass: contact-angle BC (kernels.py:933-991) on phi_tmp, flags from
 // phi (2394-2419), phi/f_l sync (3484-3504) and time-above-T (3261-3283,
 // which runs after collide/stream in the reference but only reads T and the
@@ -963,9 +972,15 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
     ContactConst cc = contact_const(a.cos_t, a.sin_t);
     const float* src = a.vof ? phi_tmp : phi;
     const int KT = tiles_k(d), JT = tiles_j(d);
+    // a quiet chunk keeps its (GAS) flags; its flag copy is still written, so
+    // that every copy holds the whole step's flags however old its last
+    // worked pass is
     auto skip = [&](int k0) -> bool {
-        return a.tile_work != nullptr &&
-               a.tile_work[((int64_t)i * JT + j / kTileJ) * KT + k0 / kTileK] == 0;
+        const bool quiet = a.tile_work != nullptr &&
+                           a.tile_work[((int64_t)i * JT + j / kTileJ) * KT + k0 / kTileK] == 0;
+        if (quiet && flags_copy != nullptr && k0 + lane < d.nz)
+            flags_copy[d.idx(i, j, k0 + lane)] = GAS;
+        return quiet;
     };
     contact_column(d, src, flags, i, j, a.vof && a.wetting, cc,
                    [&](int k, int c, float v, int flag_old, bool valid) {
@@ -1350,6 +1365,23 @@ static bool tables_fields_ok(const WaamFields* f, const WaamStepParams* p) {
     return f->cp_rho_f && f->alpha_f && f->dgamma_f && f->tau_f;
 }
 
+// waam_step_pre starts a pending stream on the library's low-priority stream
+static bool stream_work(const WaamStepParams* p) {
+    return p->stream_lag || (p->stream_prev && !p->hold_stream);
+}
+
+// The lagged stream leaves to the pending collision the cells that collision
+// writes, and reads the flags of two steps from their copies.
+static const char* lag_error(const WaamFields* f, const WaamStepParams* p) {
+    if (p->stream_lag && (!p->collide_prev || !f->flags_copy_r || !f->flags_copy_rr ||
+                          f->flags_copy_rr == f->flags_copy_r))
+        return "stream_lag needs collide_prev and two distinct flag copies";
+    if (p->hold_stream && (!p->stream_prev || !p->defer_collide || !f->flags_copy_r ||
+                           !f->flags_copy_w || !f->flags_copy_rr))
+        return "hold_stream needs stream_prev, defer_collide and three flag copies";
+    return nullptr;
+}
+
 static bool tiles_on(const WaamFields* f) {
     return f->tile_bits != nullptr && f->tile_list != nullptr && f->tile_part != nullptr &&
            tiles_packable(Dims{f->nx, f->ny, f->nz});
@@ -1373,7 +1405,9 @@ extern "C" {
 int waam_step_launch_count(const WaamStepParams* p, int stage) {
     if (!p) return 0;
     // the pending stream of the previous step is launched by waam_step_pre
-    if (stage == 0) return (p->welding ? 2 : 1) + (p->stream_prev ? 1 : 0) + (p->collide_prev ? 1 : 0);
+    if (stage == 0)
+        return (p->welding ? 2 : 1) + (p->stream_lag ? 1 : 0) +
+               (p->stream_prev && !p->hold_stream ? 1 : 0) + (p->collide_prev ? 1 : 0);
     // thermal, [vof], column, [collide], [stream] (tracers counted by the caller)
     int n = 1 + (p->vof ? 1 : 0) + 1 + (p->defer_collide ? 0 : 1) + (p->defer_stream ? 0 : 1);
     if (p->substrate_growth || p->bead_freeze) n += 1;
@@ -1384,6 +1418,7 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
                   size_t workspace_bytes, void* stream) {
     if (!fields_ok(f) || !p) return fail(WAAM_ERR_INVALID, "step_pre: bad fields or params");
     if (!tables_fields_ok(f, p)) return fail(WAAM_ERR_INVALID, "step_pre: bad material tables");
+    if (const char* le = lag_error(f, p)) return fail(WAAM_ERR_INVALID, le);
     Dims d{f->nx, f->ny, f->nz};
     if (!workspace_ok(workspace, workspace_bytes, d.n()))
         return fail(WAAM_ERR_INVALID, "step_pre: workspace too small or misaligned");
@@ -1407,20 +1442,33 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
         if (ea) return ea;
         cudaEventRecord(aux->ev[9], aux->s2);
     }
-    if (p->stream_prev) {
-        // the previous step's stream, beside this step's stages up to the
-        // column pass (waam_step_main joins it there); after its collision
+    if (p->stream_lag || (p->stream_prev && !p->hold_stream)) {
         AuxStream* aux = nullptr;
         int ea = aux_stream(&aux);
         if (ea) return ea;
         cudaEventRecord(aux->ev[2], s);
         cudaStreamWaitEvent(aux->s3, aux->ev[2], 0);
-        if (p->collide_prev) cudaStreamWaitEvent(aux->s3, aux->ev[9], 0);
-        // the flags it streams with: the previous step's copy if there is one
-        // (then the column pass may rewrite the flags meanwhile)
-        const int32_t* sf = f->flags_copy_r ? f->flags_copy_r : f->flags;
-        ea = launch_stream_stored(d, f->f_src, f->f_dst, sf, p->f_storage, aux->s3);
-        if (ea) return ea;
+        if (p->stream_lag) {
+            // the stream of the step before the previous one, held back by
+            // the previous step: beside the previous step's collision, from
+            // the buffer that collision reads into the one it writes, leaving
+            // alone the cells that collision writes (active in the previous
+            // step's flags); its own flags are the older copy
+            ea = launch_stream_stored(d, f->f_dst, f->f_src, f->flags_copy_rr, p->f_storage,
+                                      aux->s3, f->flags_copy_r);
+            if (ea) return ea;
+        }
+        if (p->stream_prev && !p->hold_stream) {
+            // the previous step's stream, after its collision
+            if (p->collide_prev) cudaStreamWaitEvent(aux->s3, aux->ev[9], 0);
+            // the flags it streams with: the previous step's copy if there is
+            // one (then the column pass may rewrite the flags meanwhile)
+            const int32_t* sf = f->flags_copy_r ? f->flags_copy_r : f->flags;
+            ea = launch_stream_stored(d, f->f_src, f->f_dst, sf, p->f_storage, aux->s3);
+            if (ea) return ea;
+        }
+        // waam_step_main joins them before the column pass (without flag
+        // copies) or after it
         cudaEventRecord(aux->ev[3], aux->s3);
     }
     if (tl) {
@@ -1484,10 +1532,17 @@ int waam_step_finish(const WaamFields* f, const WaamStepParams* p, void* workspa
     Dims d{f->nx, f->ny, f->nz};
     if (!workspace_ok(workspace, workspace_bytes, d.n()))
         return fail(WAAM_ERR_INVALID, "step_finish: workspace too small or misaligned");
+    if (const char* le = lag_error(f, p)) return fail(WAAM_ERR_INVALID, le);
     Workspace ws = Workspace::at(workspace);
     cudaStream_t s = STREAM(stream);
-    int e = launch_collide_tracers(f, p, d, ws, f->f_dst, f->f_src, f->T, p->collide_prev_welding,
-                                   s);
+    int e = WAAM_OK;
+    if (p->stream_lag) {
+        // the stream held back by the previous step, then its collision
+        e = launch_stream_stored(d, f->f_dst, f->f_src, f->flags_copy_rr, p->f_storage, s,
+                                 f->flags_copy_r);
+        if (e) return e;
+    }
+    e = launch_collide_tracers(f, p, d, ws, f->f_dst, f->f_src, f->T, p->collide_prev_welding, s);
     if (e) return e;
     return launch_stream_stored(d, f->f_src, f->f_dst, f->flags, p->f_storage, s);
 }
@@ -1600,6 +1655,7 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
                           void* stream, int stages) {
     if (!fields_ok(f) || !p) return fail(WAAM_ERR_INVALID, "step_main: bad fields or params");
     if (!tables_fields_ok(f, p)) return fail(WAAM_ERR_INVALID, "step_main: bad material tables");
+    if (const char* le = lag_error(f, p)) return fail(WAAM_ERR_INVALID, le);
     if (p->f_storage < kStoreF32 || p->f_storage > kStoreBF16)
         return fail(WAAM_ERR_INVALID, "step_main: f_storage must be 0 (f32), 1 (f16) or 2 (bf16)");
     if (events && n_events < kMainEvents)
@@ -1733,7 +1789,7 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
             }
         }
         mark(2);
-        if (p->stream_prev && !f->flags_copy_r) {
+        if (stream_work(p) && !f->flags_copy_r) {
             // the previous step's stream (started by waam_step_pre) ends here:
             // the column pass writes the flags it reads
             AuxStream* sa = nullptr;
@@ -1767,9 +1823,9 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
     }
 
     if (stages & 2) {
-        if (p->stream_prev && f->flags_copy_r) {
-            // the previous step's stream ends here: the collision writes the
-            // populations of the active cells into the buffer it writes
+        if (stream_work(p) && f->flags_copy_r) {
+            // the streams waam_step_pre started end here: the collision writes
+            // the populations of the active cells into the buffer they write
             AuxStream* sa = nullptr;
             int ea = aux_stream(&sa);
             if (ea) return ea;

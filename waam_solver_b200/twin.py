@@ -170,6 +170,9 @@ class WAAMTwin:
         self.pipeline_stream = True
         # and its collision and tracers beside the next step's arc stage
         self.pipeline_collide = True
+        # and hold each stream back one more step, to run beside the next
+        # collision on the cells that collision does not write
+        self.pipeline_lag_stream = True
         # non-droplet fused steps replay a captured CUDA graph of the step
         self.use_cuda_graphs = True
         self._fused_params = None
@@ -263,6 +266,7 @@ class WAAMTwin:
             i0, i1, j0, j1 = self.resolve_plate_ij()
         g._stream_pending = False          # the state is rebuilt below
         g._collide_pending = False
+        g._lag_pending = False
         f_a, f_b = g.f_a, g.f_b
         if g.population_storage:   # initialise and stream in float32, then store offsets
             f_a, f_b = torch.empty(f_a.shape, device=g.device), torch.empty(f_b.shape,
