@@ -28,6 +28,7 @@ oracle, all host cores) on the same workload.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -881,10 +882,12 @@ def run_b200(args, w):
         per = {"stream": c["n"] - c["solid"], "collide": c["fluid"]}.get(dom, c["n"])
         traffic = t["dram_bytes"] * per / t["cells_touched"]
     step_bytes = sum(algo.values())
+    from waam_solver_b200.coupled_step import _fields_cached
     lib = _native.lib()
-    pre = lib.waam_step_launch_count(tw._fused_params, 0)
-    launches_graph = pre + lib.waam_step_launch_count(tw._fused_params, 1)
-    launches_events = pre + lib.waam_step_launch_count(tw._fused_params, 2)
+    fl = ctypes.byref(_fields_cached(tw.grid))
+    pre = lib.waam_step_launch_count(fl, tw._fused_params, 0)
+    launches_graph = pre + lib.waam_step_launch_count(fl, tw._fused_params, 1)
+    launches_events = pre + lib.waam_step_launch_count(fl, tw._fused_params, 2)
     if lorentz:
         # sigma + mask, source (2), the sweeps, J, bins (2), prefix, B
         launches_graph += 8 + tw._lorentz_last_iters

@@ -830,8 +830,9 @@ int waam_step_main_stage(const WaamFields* f, const WaamStepParams* p, int stage
                          void* stream);
 /* Number of kernels the fused stages launch (for launch accounting): stage 0
  * waam_step_pre, 1 waam_step_main, 2 waam_step_main_events; the J x B pass
- * over SOLID cells of a step with WaamFields.lorentz_J set adds one). */
-int waam_step_launch_count(const WaamStepParams* p, int stage);
+ * over SOLID cells of a step with WaamFields.lorentz_J set adds one).  f may
+ * be null (then: without the quiet-tile buffers). */
+int waam_step_launch_count(const WaamFields* f, const WaamStepParams* p, int stage);
 
 /* ---- adjoint of the coupled step (reverse kernels, one step each) ---------- */
 /* The reverse step runs: waam_adj_stream, waam_adj_collide, waam_adj_combine,

@@ -275,7 +275,8 @@ def test_rosenthal_far_field_tail():
     (reference defaults: SRT, Gaussian arc, 50 Hz droplet schedule without
     wire) for 1200 steps at 5 mm/s; the substrate temperature 2, 3 and 4 mm
     behind the torch against the Rosenthal thick-plate tail
-    (validation/rosenthal.py:7-61), mean error (%) below 55 %."""
+    (validation/rosenthal.py:7-61), mean error (%) -- the script's gate is
+    55 %, which the reference itself misses here; the test pins the value."""
     travel, Q, eta, T0 = 0.005, 2800.0, 0.72, 300.0
     tw = _twin(nx=80, ny=40, nz=32, dx=2.5e-4, arc_power_W=Q, arc_efficiency=eta,
                travel_speed_m_s=travel, enable_heat_loss=False, C_darcy=1.6e5,
@@ -304,6 +305,9 @@ def test_rosenthal_far_field_tail():
             errs.append(abs(Ts - Ta) / (Ta - T0) * 100.0)
     assert errs
     err = float(np.mean(errs))
-    assert err < 55.0
+    # The unmodified script misses its own 55 % gate on this case (96.63 % on
+    # the stand-in): the tail runs hotter than the thick-plate solution.  The
+    # drop-in reproduces the reference's value, not the gate.
     ref = _kat("test_rosenthal_farfield", err)
+    assert ref > 55.0
     assert abs(err - ref) <= 1e-3 * ref, (err, ref)

@@ -573,6 +573,9 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
                         g.__dict__.get("_tile_epoch") == kernels.STATE_EPOCH[0] and not due and
                         not p.clear_forces and
                         not (twin.enable_bead_freeze or twin.enable_substrate_growth)) else 0
+    # until this step completes: a step that raises part-way leaves the next
+    # one a tile-history restart (which also zeroes the work-list count)
+    g._tiles_valid = False
     done = False
     if not due and not lorentz and events is None and getattr(twin, "use_cuda_graphs", True):
         key = (g._read_buf is raw_field(g, "f_a"), g._cur, p.welding, p.clear_forces, p.stream_prev,

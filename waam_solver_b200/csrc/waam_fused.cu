@@ -29,7 +29,10 @@ constexpr int kTileRedBlocks = 592;   // <= kWsMaxPartials; a fixed grid keeps t
 constexpr int kListThreads = 128;
 constexpr int kArcTableMax = 1024;    // nz up to which the arc depth weights come from a table
 constexpr int kArcAxisMax = 3072;     // nx + ny + nz up to which the arc shape uses axis tables
-constexpr int kListBlocks = 148 * 6;
+// the collision's persistent grid: 4 blocks of 128 threads (96 registers) per
+// SM hold 3/4 of its register file, leaving room for the stage kernels that
+// run beside it
+constexpr int kListBlocks = 148 * 4;
 
 
 // ---------------------------------------------------------------------------
@@ -428,91 +431,110 @@ __global__ void __launch_bounds__(256) k_arc_norm_tiles(Dims d, const int32_t* _
     }
 }
 
-// Quiet-tile classification (WaamFields.tile_bits): one thread per tile.  A
-// tile is quiet when its columns were all GAS in the last two column passes
-// (chunk bits 0 and 1) and every cell within two lattice steps of it is GAS:
-// the chunks of the 5 x (8 + 4) columns around it at the same k are all GAS
-// (bit 0), the top two cells of the chunks below (bit 2) and the bottom two
-// of the chunks above (bit 3) too -- x periodic, y and z out of range count
-// as GAS.  Writes one work byte per tile and appends the work tiles to the
-// list (count in list[0], zeroed before the launch).
-__global__ void k_classify_tiles(Dims d, const uint8_t* __restrict__ chunk,
-                                 uint8_t* __restrict__ work, int32_t* __restrict__ list,
-                                 int skip) {
-    const int KT = tiles_k(d), JT = tiles_j(d);
-    const int64_t T = tile_total(d);
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    bool w = true;
-    int kt = 0, jt = 0, i = 0;
-    if (t < T) {
-        kt = (int)(t % KT);
-        const int r = (int)(t / KT);
-        jt = r % JT;
-        i = r / JT;
-        if (skip) {
-            const int j0 = jt * kTileJ, j1 = imin(j0 + kTileJ, d.ny);
-            auto cb = [&](int ii, int jj, int kk) -> unsigned {
-                return chunk[((int64_t)ii * d.ny + jj) * KT + kk];
-            };
-            // every load is issued before any is tested (no early exit), so the
-            // tile costs a few round trips, not one per chunk
-            unsigned core = 3u;
-#pragma unroll
-            for (int dj = 0; dj < kTileJ; ++dj)
-                if (j0 + dj < j1) core &= cb(i, j0 + dj, kt);
-            unsigned box = 1u;
-#pragma unroll
-            for (int di = -2; di <= 2; ++di) {
-                const int ii = ((i + di) % d.nx + d.nx) % d.nx;
-#pragma unroll
-                for (int dj = -2; dj < kTileJ + 2; ++dj) {
-                    const int jj = j0 + dj;
-                    if (jj < 0 || jj >= imin(d.ny, j1 + 2)) continue;
-                    unsigned b = cb(ii, jj, kt);
-                    if (kt > 0) b &= cb(ii, jj, kt - 1) >> 2;
-                    if (kt + 1 < KT) b &= cb(ii, jj, kt + 1) >> 3;
-                    box &= b;
-                }
-            }
-            w = !((core & 3u) == 3u && (box & 1u));
+// Quiet-tile classification (WaamFields.tile_bits).  A tile is quiet when its
+// columns were all GAS in the last two column passes (chunk bits 0 and 1) and
+// every cell within two lattice steps of it is GAS: the chunks of the
+// 5 x (8 + 4) columns around it at the same k are all GAS (bit 0), the top
+// two cells of the chunks below (bit 2) and the bottom two of the chunks
+// above (bit 3) too -- x periodic, y and z out of range count as GAS.  Writes
+// one work byte per tile and appends the work tiles to the list (count in
+// list[0], zeroed before the launch).
+// One warp per (i, j-tile) band of tiles: lane q < 60 owns the neighbour
+// column (di, dj) = (q / 12 - 2, q % 12 - 2) and loads its three chunk bytes
+// per k-tile; the warp votes.  A tile costs one round of independent loads.
+// A quiet tile's arc weight slot (tile_part) is set to 0.  The grid's last
+// block runs the surface query of the step (scalars[kScalarArcK]).
+constexpr int kClassifyWarps = 8;
+__global__ void __launch_bounds__(32 * kClassifyWarps)
+    k_classify_tiles(Dims d, const uint8_t* __restrict__ chunk, uint8_t* __restrict__ work,
+                     int32_t* __restrict__ list, int skip, double* __restrict__ tile_part,
+                     const float* __restrict__ phi, const int32_t* __restrict__ flags,
+                     float* __restrict__ scalars, int nz_solid) {
+    if (blockIdx.x == gridDim.x - 1) {
+        if (threadIdx.x < 32) {
+            const float kf = surface_arc_k(d, phi, flags, scalars, nz_solid);
+            if (threadIdx.x == 0) scalars[kScalarArcK] = kf;
         }
-        work[t] = w ? 1 : 0;
+        return;
     }
-    const bool app = t < T && w;
-    const unsigned m = __ballot_sync(0xffffffffu, app);
-    if (m) {
-        const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
-        int base = 0;
-        if (lane == lead) base = atomicAdd(&list[0], __popc(m));
-        base = __shfl_sync(0xffffffffu, base, lead);
-        if (app) list[1 + base + __popc(m & ((1u << lane) - 1u))] = pack_tile(i, jt, kt);
+    const int KT = tiles_k(d), JT = tiles_j(d);
+    const int band = blockIdx.x * kClassifyWarps + (threadIdx.x >> 5);
+    if (band >= d.nx * JT) return;   // warp-uniform
+    const int lane = threadIdx.x & 31;
+    const int i = band / JT, jt = band % JT;
+    const int j0 = jt * kTileJ, j1 = imin(j0 + kTileJ, d.ny);
+    // the lane's two neighbour columns (second: q = lane + 32 < 60); -1: none
+    int64_t col[2];
+    bool is_core[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int q = lane + 32 * h;
+        const int di = q / (kTileJ + 4) - 2, dj = q % (kTileJ + 4) - 2;
+        const int jj = j0 + dj;
+        const bool ok = q < 5 * (kTileJ + 4) && jj >= 0 && jj < imin(d.ny, j1 + 2);
+        const int ii = ((i + di) % d.nx + d.nx) % d.nx;
+        col[h] = ok ? ((int64_t)ii * d.ny + jj) * KT : -1;
+        is_core[h] = ok && di == 0 && dj >= 0 && jj < j1;
+    }
+    uint64_t wmask = 0;   // work k-tiles of the band (KT <= 64 with tiles on)
+    for (int kt = 0; kt < KT; ++kt) {
+        bool w = true;
+        if (skip) {
+            // every load is issued before any is tested
+            unsigned b[2], c[2], lo[2], hi[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const bool ok = col[h] >= 0;
+                c[h] = ok ? chunk[col[h] + kt] : 3u;
+                lo[h] = ok && kt > 0 ? chunk[col[h] + kt - 1] : 0xffu;
+                hi[h] = ok && kt + 1 < KT ? chunk[col[h] + kt + 1] : 0xffu;
+            }
+            bool quiet = true;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                b[h] = c[h] & (lo[h] >> 2) & (hi[h] >> 3);
+                if (col[h] >= 0 && !(b[h] & 1u)) quiet = false;
+                if (is_core[h] && (c[h] & 3u) != 3u) quiet = false;
+            }
+            w = !__all_sync(0xffffffffu, quiet);
+        }
+        if (lane == 0) {
+            work[(int64_t)band * KT + kt] = w ? 1 : 0;
+            if (!w) tile_part[(int64_t)band * KT + kt] = 0.0;
+        }
+        if (w) wmask |= 1ull << kt;
+    }
+    if (wmask == 0) return;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&list[0], __popcll(wmask));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    // the band's work tiles in k-tile order, one lane per k-tile (a count
+    // left non-zero by a step that stopped after this kernel cannot write
+    // past the list)
+    const int64_t cap = tile_total(d);
+    for (int kt = lane; kt < KT; kt += 32) {
+        const int64_t slot = (int64_t)base + __popcll(wmask & ((1ull << kt) - 1ull));
+        if (((wmask >> kt) & 1ull) && slot < cap) list[1 + slot] = pack_tile(i, jt, kt);
     }
 }
 
 // The arc weight sum over the tiles of the work list (quiet tiles are all GAS
 // and weigh nothing).  Each listed tile's sum goes to its own slot of
-// tile_part; the last block adds the slots in tile order, so the total does
-// not depend on the list's order.  Otherwise as k_arc_norm_tiles.
+// tile_part (k_classify_tiles zeroes the quiet tiles' slots); the last block
+// adds all slots in tile order, so the total does not depend on the list's
+// order.  The surface query's arc k comes from k_classify_tiles.  A block
+// takes kArcBatch listed tiles at a time: their loads are all issued first and
+// their block sums share one barrier.  Otherwise as k_arc_norm_tiles.
+constexpr int kArcBatch = 8;
 __global__ void __launch_bounds__(256) k_arc_norm_list(Dims d, const int32_t* __restrict__ flags,
                                                        const float* __restrict__ f_l,
-                                                       const float* __restrict__ phi,
-                                                       int nz_solid, ArcParams p, float* scalars,
+                                                       ArcParams p, float* scalars,
                                                        float arc_k_offset, float Qe_dt, float dx3,
                                                        Workspace ws, float* __restrict__ shape,
                                                        const int32_t* __restrict__ list,
-                                                       const uint8_t* __restrict__ tile_work,
                                                        double* __restrict__ tile_part, int tiles) {
-    __shared__ float s_arc_k;
     __shared__ float s_wd[kArcTableMax];
-    if (threadIdx.y == 0) {
-        const float kf = surface_arc_k(d, phi, flags, scalars, nz_solid);
-        if (threadIdx.x == 0) {
-            s_arc_k = kf;
-            if (blockIdx.x == 0) scalars[kScalarArcK] = kf;
-        }
-    }
-    __syncthreads();
-    p.arc_k = s_arc_k + arc_k_offset;
+    p.arc_k = scalars[kScalarArcK] + arc_k_offset;
     p.arc_i = scalars[kScalarArcI];
     p.arc_j = scalars[kScalarArcJ];
     const bool table = d.nz <= kArcTableMax;
@@ -560,17 +582,18 @@ __global__ void __launch_bounds__(256) k_arc_norm_list(Dims d, const int32_t* __
     };
     const int tid = threadIdx.y * kTileK + threadIdx.x;
     const int cnt = imin(list[0], tiles);
-    constexpr int kU = 4;
-    for (int e0 = blockIdx.x; e0 < cnt; e0 += kU * gridDim.x) {
-        int fg[kU], ci[kU], cj[kU], ck[kU], tt[kU];
+    constexpr int kU = kArcBatch, kWarps = (kTileK * kTileJ) / 32;
+    __shared__ double s_part[kU][kWarps];
+    for (int e0 = blockIdx.x * kU; e0 < cnt; e0 += kU * gridDim.x) {
+        int ent[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) ent[u] = e0 + u < cnt ? list[1 + e0 + u] : -1;
+        int fg[kU], ci[kU], cj[kU], ck[kU];
         float fl[kU];
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
-            const int e = e0 + u * gridDim.x;
-            const int ent = e < cnt ? list[1 + e] : -1;
-            tt[u] = ent >= 0 ? (int)tile_index(d, ent) : -1;
             int i = 0, j = 0, k = 0, c = 0;
-            const bool ok = ent >= 0 && list_tile_cell(d, ent, i, j, k, c);
+            const bool ok = ent[u] >= 0 && list_tile_cell(d, ent[u], i, j, k, c);
             fg[u] = ok ? flags[c] : GAS;
             fl[u] = ok ? f_l[c] : 0.0f;
             ci[u] = i;
@@ -589,9 +612,21 @@ __global__ void __launch_bounds__(256) k_arc_norm_list(Dims d, const int32_t* __
                     v = (double)(sh * wd);
                 }
             }
-            const double sum = tile_block_sum(v);
-            if (tid == 0 && tt[u] >= 0) tile_part[tt[u]] = sum;
+            // the block sum of tile_block_sum: warp tree, then the warps in order
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if ((tid & 31) == 0) s_part[u][tid >> 5] = v;
         }
+        __syncthreads();
+        int mine = -1;   // thread u < kU writes tile u's slot
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            if (tid == u) mine = ent[u];
+        if (mine >= 0) {
+            double sum = 0.0;
+            for (int w = 0; w < kWarps; ++w) sum += s_part[tid][w];
+            tile_part[tile_index(d, mine)] = sum;
+        }
+        __syncthreads();
     }
     __shared__ bool last;
     if (tid == 0) {
@@ -603,10 +638,10 @@ __global__ void __launch_bounds__(256) k_arc_norm_list(Dims d, const int32_t* __
     if (!last) return;
     __threadfence();
     // the slots come from other blocks (fenced before their arrival count):
-    // read them from L2 (__ldcg), independent loads that can all be in flight
+    // read them from L2 (__ldcg), independent loads that can all be in flight;
+    // a quiet tile's slot is 0 and adds nothing
     double acc = 0.0;
-    for (int t = tid; t < tiles; t += kTileK * kTileJ)
-        acc += tile_work[t] ? __ldcg(tile_part + t) : 0.0;
+    for (int t = tid; t < tiles; t += kTileK * kTileJ) acc += __ldcg(tile_part + t);
     const double tot = tile_block_sum(acc);
     if (tid == 0) {
         *ws.counter = 0u;
@@ -938,6 +973,7 @@ struct ColumnArgs {
     const uint8_t* tile_work;
     uint8_t* chunk_bits;
     int tile_history;  // 1: chunk bit 1 takes the previous bit 0; 0: history restarts
+    int32_t* tile_list;  // non-null: its count is zeroed for the next step's classification
 };
 
 // Column pass: contact-angle BC (kernels.py:933-991) on phi_tmp, flags from
@@ -965,10 +1001,20 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
         scalars[kScalarCollideArcK] = scalars[kScalarArcK];
         scalars[kScalarCollideArcI] = scalars[kScalarArcI];
         scalars[kScalarCollideArcJ] = scalars[kScalarArcJ];
+        // this step's work list was read by the thermal and VOF stages
+        if (a.tile_list != nullptr) a.tile_list[0] = 0;
     }
-    if (warp >= d.nx * d.ny) return;
+    // warp w works column (w % 64) * C + w / 64 (C = ceil(nx * ny / 64)) and
+    // appends to shard w % 64: a shard holds a contiguous run of columns, so
+    // the collision's warps, which take the list in order, see neighbouring
+    // columns (shared stencil sectors)
+    const int n_col = d.nx * d.ny;
+    const int C = (n_col + kActiveShards - 1) / kActiveShards;
+    if (warp >= C * kActiveShards) return;
+    const int col = (warp & (kActiveShards - 1)) * C + warp / kActiveShards;
+    if (col >= n_col) return;
     const int lane = threadIdx.x & 31;
-    int i = warp / d.ny, j = warp % d.ny;
+    int i = col / d.ny, j = col % d.ny;
     ContactConst cc = contact_const(a.cos_t, a.sin_t);
     const float* src = a.vof ? phi_tmp : phi;
     const int KT = tiles_k(d), JT = tiles_j(d);
@@ -1402,12 +1448,15 @@ static int launch_collide_tracers(const WaamFields* f, const WaamStepParams* p, 
 
 extern "C" {
 
-int waam_step_launch_count(const WaamStepParams* p, int stage) {
+int waam_step_launch_count(const WaamFields* f, const WaamStepParams* p, int stage) {
     if (!p) return 0;
-    // the pending stream of the previous step is launched by waam_step_pre
-    if (stage == 0)
-        return (p->welding ? 2 : 1) + (p->stream_lag ? 1 : 0) +
+    // the pending stream of the previous step is launched by waam_step_pre;
+    // with tiles the classification also runs the surface query
+    if (stage == 0) {
+        const bool tl = f != nullptr && tiles_on(f);
+        return (tl ? (p->welding ? 3 : 1) : (p->welding ? 2 : 1)) + (p->stream_lag ? 1 : 0) +
                (p->stream_prev && !p->hold_stream ? 1 : 0) + (p->collide_prev ? 1 : 0);
+    }
     // thermal, [vof], column, [collide], [stream] (tracers counted by the caller)
     int n = 1 + (p->vof ? 1 : 0) + 1 + (p->defer_collide ? 0 : 1) + (p->defer_stream ? 0 : 1);
     if (p->substrate_growth || p->bead_freeze) n += 1;
@@ -1429,24 +1478,43 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     const bool tl = tiles_on(f);
     const int64_t n_tiles = tile_total(d);
     const uint8_t* tile_work = tl ? f->tile_bits + (int64_t)tiles_k(d) * d.nx * d.ny : nullptr;
+    const bool s3_work = stream_work(p);
+    AuxStream* aux = nullptr;
+    if (p->collide_prev || s3_work) {
+        int ea = aux_stream(&aux);
+        if (ea) return ea;
+        // the fork points of the pending collision (ev[8]) and streams (ev[2]):
+        // the start of the step, before the work-tile classification is
+        // launched (so that its blocks are placed first)
+        if (p->collide_prev) cudaEventRecord(aux->ev[8], s);
+        if (s3_work) cudaEventRecord(aux->ev[2], s);
+    }
+    if (tl) {
+        // the step's work tiles, from the chunk bits the previous column pass
+        // left; the list count was zeroed by that column pass (or here, when
+        // the tile history restarts)
+        if (!p->tile_skip) cudaMemsetAsync(f->tile_list, 0, sizeof(int32_t), s);
+        // one block more than the bands need: the surface query
+        const int bands = d.nx * tiles_j(d);
+        k_classify_tiles<<<(bands + kClassifyWarps - 1) / kClassifyWarps + 1,
+                           32 * kClassifyWarps, 0, s>>>(
+            d, f->tile_bits, const_cast<uint8_t*>(tile_work), f->tile_list, p->tile_skip,
+            f->tile_part, f->phi, f->flags, f->step_scalars, p->nz_solid);
+        int e = check_launch("k_classify_tiles");
+        if (e) return e;
+    }
     if (p->collide_prev) {
         // the previous step's collision and tracers, beside this step's arc
         // stage (waam_step_main waits for them before its thermal stage)
-        AuxStream* aux = nullptr;
-        int ea = aux_stream(&aux);
-        if (ea) return ea;
-        cudaEventRecord(aux->ev[8], s);
+        int ea = WAAM_OK;
         cudaStreamWaitEvent(aux->s2, aux->ev[8], 0);
         ea = launch_collide_tracers(f, p, d, ws, f->f_dst, f->f_src, f->T, p->collide_prev_welding,
                                     aux->s2);
         if (ea) return ea;
         cudaEventRecord(aux->ev[9], aux->s2);
     }
-    if (p->stream_lag || (p->stream_prev && !p->hold_stream)) {
-        AuxStream* aux = nullptr;
-        int ea = aux_stream(&aux);
-        if (ea) return ea;
-        cudaEventRecord(aux->ev[2], s);
+    if (s3_work) {
+        int ea = WAAM_OK;
         cudaStreamWaitEvent(aux->s3, aux->ev[2], 0);
         if (p->stream_lag) {
             // the stream of the step before the previous one, held back by
@@ -1471,17 +1539,8 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
         // copies) or after it
         cudaEventRecord(aux->ev[3], aux->s3);
     }
-    if (tl) {
-        // the step's work tiles, from the chunk bits the previous column pass left
-        cudaMemsetAsync(f->tile_list, 0, sizeof(int32_t), s);
-        // one warp per block: a tile's check is ~190 independent byte loads,
-        // so the grid should reach every SM
-        k_classify_tiles<<<(int)((n_tiles + 31) / 32), 32, 0, s>>>(
-            d, f->tile_bits, const_cast<uint8_t*>(tile_work), f->tile_list, p->tile_skip);
-        int e = check_launch("k_classify_tiles");
-        if (e) return e;
-    }
     if (!p->welding) {
+        if (tl) return WAAM_OK;
         k_surface_arc<<<1, 32, 0, s>>>(d, f->phi, f->flags, f->step_scalars,
                                                     p->nz_solid);
         return check_launch("k_surface_arc");
@@ -1494,8 +1553,8 @@ int waam_step_pre(const WaamFields* f, const WaamStepParams* p, void* workspace,
     PhaseParams ph = make_phase(p->cp_rho, p->L_rho, p->Ts, p->Tl, p->T_cap, p->cap_enabled);
     if (tl) {
         k_arc_norm_list<<<blocks, tile_block(), 0, s>>>(
-            d, f->flags, f->f_l, f->phi, p->nz_solid, a, f->step_scalars, p->arc_k_offset, Qe_dt,
-            p->dx3, ws, shape, f->tile_list, tile_work, f->tile_part, (int)n_tiles);
+            d, f->flags, f->f_l, a, f->step_scalars, p->arc_k_offset, Qe_dt, p->dx3, ws, shape,
+            f->tile_list, f->tile_part, (int)n_tiles);
         int e = check_launch("k_arc_norm_list");
         if (e) return e;
         const int lb = (int)(n_tiles < kTileListBlocks ? n_tiles : kTileListBlocks);
@@ -1682,7 +1741,8 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         ((int64_t)d.nx * d.ny + kActiveShards - 1) / kActiveShards * (int64_t)d.nz;
     if (shard_cap * kActiveShards > d.n() + kFieldSlack || shard_cap > INT32_MAX)
         return fail(WAAM_ERR_INVALID, "step_main: nz too large for the active-cell list");
-    const int col_blocks = (int)(((int64_t)d.nx * d.ny * 32 + kThreads - 1) / kThreads);
+    // one warp per column, in kActiveShards groups of shard_cap / nz (k_column)
+    const int col_blocks = (int)((shard_cap / d.nz * kActiveShards * 32 + kThreads - 1) / kThreads);
     // without stage events the stages run on the library's high-priority stream
     WorkStream W(STREAM(stream), events == nullptr, 6);
     if (W.err) return W.err;
@@ -1813,6 +1873,7 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         ca.tile_work = tl ? f->tile_bits + (int64_t)tiles_k(d) * d.nx * d.ny : nullptr;
         ca.chunk_bits = tl ? f->tile_bits : nullptr;
         ca.tile_history = p->tile_skip ? 1 : 0;
+        ca.tile_list = tl ? f->tile_list : nullptr;
         k_column<<<col_blocks, kThreads, 0, s>>>(d, f->phi_tmp, f->phi, f->flags, f->f_l, f->T_next,
                                                  f->t800, f->t1100, f->tsol, f->Fx, f->Fy, f->Fz,
                                                  active_list, active_count, f->flags_copy_w,
