@@ -979,9 +979,8 @@ def profile_run(w, n):
         tw.step(x, y, welding)
     tw.grid.flush_stream()
     torch.cuda.synchronize()
-    g = tw.grid
     print("profile run: %d steps, %d of %d tiles worked at the last step"
-          % (n, int(g.tile_list[0].item()), g.tile_list.numel() - 1))
+          % ((n,) + tw.grid.worked_tiles()))
 
 
 def main():

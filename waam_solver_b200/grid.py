@@ -126,6 +126,7 @@ class WAAMGrid:
         self.tile_list = torch.zeros(1 + n_tiles, dtype=torch.int32, device=dev)
         self.tile_part = torch.zeros(n_tiles, dtype=torch.float64, device=dev)
         self._tiles_valid = False
+        self._n_chunk_bytes = kt * self.nx * self.ny
         self.telem_fl_slice = torch.zeros((self.ny, self.nz), **f32)
         self.porosity_pos = torch.zeros((self.max_tracers, 3), **f32)
         self.porosity_active = torch.zeros(self.max_tracers, dtype=torch.int32, device=dev)
@@ -222,6 +223,12 @@ class WAAMGrid:
         return self._snap[2] if self._separate_snapshot else self.Fz
 
     # -- ping-pong populations (grid.py:268-278) --------------------------
+    def worked_tiles(self):
+        """(worked, total) 32 x 8 tiles of the last fused step (its work bytes;
+        the list count itself is zeroed for the next step).  Synchronises."""
+        work = self.tile_bits[self._n_chunk_bytes:]
+        return int(work.sum(dtype=torch.int64).item()), int(work.numel())
+
     def swap_buffers(self):
         self._read_buf, self._write_buf = self._write_buf, self._read_buf
 
