@@ -502,7 +502,7 @@ def fd64_problem(device, variant):
     tw = build_twin(dict(ADJOINT_C4), device)
     g = tw.grid
     yc = (g.ny // 2) * g.dx
-    if variant == "c4_pool":
+    if variant.split("@")[0] == "c4_pool":   # "<variant>@<step>": another difference step
         tests = os.path.join(ROOT, "tests")
         if tests not in sys.path:
             sys.path.insert(0, tests)
@@ -545,7 +545,7 @@ def adjoint_fd64(device):
             f = meta["fd"][name]
             rel[name] = {"adjoint": float(grad[q]), "fd_fp64": f,
                          "rel_diff": abs(grad[q] - f) / max(abs(f), 1e-300)}
-        out[variant] = {"steps": meta["steps"], "loss_float32": loss,
+        out[variant] = {"steps": meta["steps"], "fd_step": meta["fd_step"], "loss_float32": loss,
                         "loss_fp64": meta["loss_base"], "width_mm": prob.width()[0],
                         "probe_T_max_abs_diff_vs_fp64": float(np.abs(prob.T_probe - T64).max()),
                         "gradient": rel}

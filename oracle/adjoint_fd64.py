@@ -23,7 +23,7 @@ perturbed parameters base x (1.05, 1.2, 1.0, 1.1, 0.9, 1.1, 1.1), W* = W +
 molten pool (tests/state_gen.py) so that the width term is not identically
 zero.
 
-    python oracle/adjoint_fd64.py c4 [steps]       (minutes to hours of CPU)
+    python oracle/adjoint_fd64.py c4 [steps [fd_step]]   (minutes to hours of CPU)
 """
 from __future__ import annotations
 
@@ -138,9 +138,13 @@ def width(f_l, dx):
     return float(dx * 1e3 * s.sum())
 
 
-def run(variant, n_steps):
+def run(variant, n_steps, fd_step=FD_STEP):
+    """Differences at relative step fd_step; a step other than FD_STEP is
+    stored under the key ``<variant>@<fd_step>`` (a second step size shows
+    how far the differences themselves depend on it)."""
     t0 = time.time()
     pb = Problem(variant, n_steps)
+    key = variant if fd_step == FD_STEP else "%s@%g" % (variant, fd_step)
     T_t, W_t = pb.forward(pb.base * np.array(PERTURB))
     T0, W0 = pb.forward(pb.base)
     W_target = W0 + W_OFFSET_MM
@@ -149,7 +153,7 @@ def run(variant, n_steps):
     for q, name in enumerate(PARAMS):
         if name == "arc_sigma_scale":
             continue    # structural zero: no kernel of this configuration reads it
-        h = FD_STEP * abs(pb.base[q])
+        h = fd_step * abs(pb.base[q])
         tp, tm = pb.base.copy(), pb.base.copy()
         tp[q] += h
         tm[q] -= h
@@ -159,20 +163,21 @@ def run(variant, n_steps):
         print(variant, name, fd[name], "%.0f s" % (time.time() - t0), flush=True)
     meta = dict(variant=variant, steps=pb.N, params=PARAMS, theta=pb.base.tolist(),
                 probes=pb.probes, x0=C4["x0"], travel=C4["travel"], w_T=W_T, w_W=W_W,
-                beta=BETA, fd_step=FD_STEP, W_target=W_target, W_base=W0, loss_base=L0,
+                beta=BETA, fd_step=fd_step, W_target=W_target, W_base=W0, loss_base=L0,
                 fd=fd, pool_seed=POOL_SEED if variant == "c4_pool" else None,
                 seconds=time.time() - t0)
     payload = {}
     if os.path.exists(OUT):
         with np.load(OUT) as z:
             payload = {k: z[k] for k in z.files}
-    payload[variant + "_T_target"] = T_t
-    payload[variant + "_T_base"] = T0
-    payload[variant + "_meta"] = np.array(json.dumps(meta))
+    payload[key + "_T_target"] = T_t
+    payload[key + "_T_base"] = T0
+    payload[key + "_meta"] = np.array(json.dumps(meta))
     np.savez_compressed(OUT, **payload)
     print(json.dumps(meta), flush=True)
 
 
 if __name__ == "__main__":
     run(sys.argv[1] if len(sys.argv) > 1 else "c4",
-        int(sys.argv[2]) if len(sys.argv) > 2 else 2000)
+        int(sys.argv[2]) if len(sys.argv) > 2 else 2000,
+        float(sys.argv[3]) if len(sys.argv) > 3 else FD_STEP)

@@ -394,6 +394,12 @@ def _taped_step(tw, x, y, tape, slot):
     p.defer_stream = 0
     p.collide_prev = 0
     p.defer_collide = 0
+    p.stream_lag = 0
+    p.hold_stream = 0
+    # taped steps follow checkpoint restores: every tile worked, and the next
+    # fused step restarts the tile history too
+    p.tile_skip = 0
+    g._tiles_valid = False
     arc_i, arc_j = sim_x / g.dx, sim_y / g.dx
     p.arc_i, p.arc_j = arc_i, arc_j
     p.welding = 1
