@@ -247,12 +247,14 @@ def test_config4_gradient_matches_fp64_central_differences(variant):
     the adjoint's own error.  ``c4``: from reset, 2000 steps -- every
     parameter within 1e-3 (measured: at most 2.6e-4).  ``c4_pool``: from a
     seeded molten pool, 500 steps, where the final-width term of the loss is
-    not zero and the pool's phase boundary, the surface-weighting switch
-    (f_l > 0.55) and the interface move with the parameters: the adjoint
-    keeps them at the forward trajectory's (its stated approximation), the
-    differences see them switch, so only the signs agree for the parameters
-    that move the pool (measured relative differences 0.1 to 10); the
-    heat-loss factor and a_front, which barely do, agree to 1e-3 / 2e-2."""
+    not zero.  There the pool's phase boundary, the surface-weighting switch
+    (f_l > 0.55) and the interface move with the parameters; the loss
+    switches with them, and the FP64 differences themselves depend on the
+    step (1e-3 against 1e-2: eta -31.5 / -46.0, a_rear 0.40 / 0.74, c 0.09 /
+    1.01).  The adjoint keeps the switches at the forward trajectory's (its
+    stated approximation) and gives the smooth part: it must have the
+    differences' sign and lie inside the band the two steps span, widened
+    by 15 % of its far end."""
     import os
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -269,7 +271,12 @@ def test_config4_gradient_matches_fp64_central_differences(variant):
     # the float32 forward follows the FP64 one (the same problem, set up alike)
     assert abs(loss - meta["loss_base"]) <= 1e-3 * abs(meta["loss_base"]), (loss, meta)
     assert np.abs(prob.T_probe - T64).max() < 0.05
-    bound = FD64_BOUND[variant]
+    other = None     # the same differences at the second step, if the fixture has them
+    with np.load(bench.FD64_FIXTURE) as z:
+        keys = [k[:-5] for k in z.files if k.startswith(variant + "@") and k.endswith("_meta")]
+        if keys:
+            import json
+            other = json.loads(str(z[keys[0] + "_meta"]))["fd"]
     for q, name in enumerate(PARAMS):
         if name not in meta["fd"]:
             assert grad[q] == 0.0, name      # structurally zero in this configuration
@@ -277,13 +284,15 @@ def test_config4_gradient_matches_fp64_central_differences(variant):
         f = meta["fd"][name]
         rel = abs(grad[q] - f) / abs(f)
         print("%s %-18s adjoint % .6e  fd64 % .6e  rel %.2e" % (variant, name, grad[q], f, rel))
-        lim = bound.get(name, bound["*"])
         assert np.sign(grad[q]) == np.sign(f), (variant, name, grad[q], f)
-        if lim is not None:
-            assert rel <= lim, (variant, name, grad[q], f, rel)
+        if variant == "c4":
+            assert rel <= FD64_REL, (variant, name, grad[q], f, rel)
+        else:
+            assert other is not None, "the pool variant needs differences at two steps"
+            lo, hi = min(f, other[name]), max(f, other[name])
+            slack = FD64_BAND * max(abs(lo), abs(hi))
+            assert lo - slack <= grad[q] <= hi + slack, (name, grad[q], f, other[name])
 
 
-# relative bounds of the FP64 comparison, per variant ("*": every other
-# parameter; None: the signs only)
-FD64_BOUND = {"c4": {"*": 1e-3},
-              "c4_pool": {"heat_loss_factor": 1e-3, "a_front": 2e-2, "*": None}}
+FD64_REL = 1e-3      # config 4 from reset: relative bound against the FP64 differences
+FD64_BAND = 0.15     # pool variant: widening of the two-step band (of its far end)

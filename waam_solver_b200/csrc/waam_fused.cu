@@ -1004,17 +1004,9 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
         // this step's work list was read by the thermal and VOF stages
         if (a.tile_list != nullptr) a.tile_list[0] = 0;
     }
-    // warp w works column (w % 64) * C + w / 64 (C = ceil(nx * ny / 64)) and
-    // appends to shard w % 64: a shard holds a contiguous run of columns, so
-    // the collision's warps, which take the list in order, see neighbouring
-    // columns (shared stencil sectors)
-    const int n_col = d.nx * d.ny;
-    const int C = (n_col + kActiveShards - 1) / kActiveShards;
-    if (warp >= C * kActiveShards) return;
-    const int col = (warp & (kActiveShards - 1)) * C + warp / kActiveShards;
-    if (col >= n_col) return;
+    if (warp >= d.nx * d.ny) return;
     const int lane = threadIdx.x & 31;
-    int i = col / d.ny, j = col % d.ny;
+    int i = warp / d.ny, j = warp % d.ny;
     ContactConst cc = contact_const(a.cos_t, a.sin_t);
     const float* src = a.vof ? phi_tmp : phi;
     const int KT = tiles_k(d), JT = tiles_j(d);
@@ -1741,8 +1733,7 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         ((int64_t)d.nx * d.ny + kActiveShards - 1) / kActiveShards * (int64_t)d.nz;
     if (shard_cap * kActiveShards > d.n() + kFieldSlack || shard_cap > INT32_MAX)
         return fail(WAAM_ERR_INVALID, "step_main: nz too large for the active-cell list");
-    // one warp per column, in kActiveShards groups of shard_cap / nz (k_column)
-    const int col_blocks = (int)((shard_cap / d.nz * kActiveShards * 32 + kThreads - 1) / kThreads);
+    const int col_blocks = (int)(((int64_t)d.nx * d.ny * 32 + kThreads - 1) / kThreads);
     // without stage events the stages run on the library's high-priority stream
     WorkStream W(STREAM(stream), events == nullptr, 6);
     if (W.err) return W.err;
