@@ -1010,14 +1010,23 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
     ContactConst cc = contact_const(a.cos_t, a.sin_t);
     const float* src = a.vof ? phi_tmp : phi;
     const int KT = tiles_k(d), JT = tiles_j(d);
-    // a quiet chunk keeps its (GAS) flags; its flag copy is still written, so
-    // that every copy holds the whole step's flags however old its last
-    // worked pass is
+    // A quiet chunk keeps its (GAS) flags.  Its flag copy is still written
+    // until the last three passes have all written GAS copies of it (chunk
+    // bits 4-5 count them), so that each of the three rotating copies holds
+    // the whole step's flags however old its last worked pass is.
     auto skip = [&](int k0) -> bool {
         const bool quiet = a.tile_work != nullptr &&
                            a.tile_work[((int64_t)i * JT + j / kTileJ) * KT + k0 / kTileK] == 0;
-        if (quiet && flags_copy != nullptr && k0 + lane < d.nz)
-            flags_copy[d.idx(i, j, k0 + lane)] = GAS;
+        if (quiet && flags_copy != nullptr) {
+            uint8_t* cbp = a.chunk_bits + ((int64_t)i * d.ny + j) * KT + (k0 >> 5);
+            const unsigned old = *cbp;   // same address for the warp
+            const unsigned cnt = (old >> 4) & 3u;
+            if (cnt < 3u) {
+                if (k0 + lane < d.nz) flags_copy[d.idx(i, j, k0 + lane)] = GAS;
+                __syncwarp();
+                if (lane == 0) *cbp = (uint8_t)((old & 0xcfu) | ((cnt + 1u) << 4));
+            }
+        }
         return quiet;
     };
     contact_column(d, src, flags, i, j, a.vof && a.wetting, cc,
@@ -1058,7 +1067,11 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
                                if (a.tile_history && (old & 1u)) nb |= 2u;
                                if ((gm >> 30) == 3u) nb |= 4u;
                                if ((gm & 3u) == 3u) nb |= 8u;
-                               *cbp = (uint8_t)nb;
+                               // bits 4-5: consecutive passes (at most 3) whose
+                               // flag copies of the chunk were all GAS
+                               unsigned cnt = a.tile_history ? (old >> 4) & 3u : 0u;
+                               cnt = (nb & 1u) && flags_copy ? (cnt < 3u ? cnt + 1u : 3u) : 0u;
+                               *cbp = (uint8_t)(nb | (cnt << 4));
                            }
                        }
                        bool act = valid && is_active(flag);
