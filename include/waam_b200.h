@@ -656,8 +656,12 @@ typedef struct WaamFields {
      * within two lattice steps of them are GAS, and that was all GAS at the
      * step before; the arc, thermal, VOF and column stages leave quiet tiles
      * alone (they are exact no-ops there).  The caller owns and zero-fills:
-     *   tile_bits: ceil(nz/32) * nx * ny chunk bytes, then one byte per tile;
-     *   tile_list: 1 + tiles int32 (count, then the tiles to work);
+     *   tile_bits: ceil(nz/32) * nx * ny chunk bytes (bit 0: all GAS, 1: all
+     *     GAS the pass before, 2 / 3: top / bottom two cells GAS, 4-5: passes
+     *     in a row whose flag copies of the chunk were all GAS), then one work
+     *     byte per tile;
+     *   tile_list: 1 + tiles int32 (count, then the tiles to work; the
+     *     column pass zeroes the count for the next step);
      *   tile_part: tiles doubles (per-tile arc weight sums).
      * They carry state from step to step: after changing the fields any
      * other way, run the next step with tile_skip = 0. */
