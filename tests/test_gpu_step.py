@@ -390,17 +390,21 @@ def test_operator_calls_after_pipelined_steps_see_streamed_populations():
             assert np.array_equal(v, states[1][k]), k
 
 
-def test_quiet_tile_skipping_matches_working_every_tile():
+@pytest.mark.parametrize("lorentz", [False, True])
+def test_quiet_tile_skipping_matches_working_every_tile(lorentz):
     """Quiet-tile skipping with the lagged stream (the defaults) against every
     tile worked and the stream run one step earlier, bit for bit, on a grid
     tall enough for quiet tiles (nz = 96: three 32-cell k tiles over a
     19-cell plate), through droplet steps (the tile history restarts), graph
     replays and the pipelined stream and collision -- the lagged stream
     reads flag copies that quiet tiles must still write; the skipping really
-    skips (the work list is shorter than the tile count)."""
+    skips (the work list is shorter than the tile count).  With the welding
+    current's Lorentz force (and VOF, so J x B stays on the active cells) the
+    tiles are skipped on the split steps as well."""
     states, counts = [], []
+    more = dict(enable_lorentz=True, welding_current_A=180.0) if lorentz else {}
     for skip in (False, True):
-        tw, ot, dx = _config_twins("c2", 40, 32, 96)
+        tw, ot, dx = _config_twins("c2", 40, 32, 96, **more)
         tw.skip_quiet_tiles = skip
         tw.pipeline_lag_stream = skip
         tw._last_droplet_time = -1.0

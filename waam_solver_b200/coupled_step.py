@@ -308,9 +308,12 @@ def _fields(g):
         f.flags_copy_r = copies[(w + 2) % 3].data_ptr()
         f.flags_copy_rr = copies[(w + 1) % 3].data_ptr()
     f.status = g.step_status.data_ptr()
-    f.tile_bits = g.tile_bits.data_ptr()
-    f.tile_list = g.tile_list.data_ptr()
-    f.tile_part = g.tile_part.data_ptr()
+    if g.nz > 32:
+        # quiet tiles need a k tile above the plate's: with one 32-cell k tile
+        # every tile holds metal, and the list would only add a kernel
+        f.tile_bits = g.tile_bits.data_ptr()
+        f.tile_list = g.tile_list.data_ptr()
+        f.tile_part = g.tile_part.data_ptr()
     return f
 
 
@@ -621,9 +624,9 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
             handles = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
             _native.call("waam_step_main_events", ctypes.byref(f), ctypes.byref(p),
                          ws.data_ptr(), ws.numel(), handles, len(events), stream)
-    # the droplet impact load (and J x B on SOLID cells) stays in F outside the
-    # active cells until the next step
-    g._forces_dirty = bool(p.forces_from_buffer) or lorentz
+    # the droplet impact load (and J x B on SOLID cells, which only runs
+    # without VOF) stays in F outside the active cells until the next step
+    g._forces_dirty = bool(p.forces_from_buffer) or (lorentz and not twin.enable_vof)
     g._stream_pending = bool(p.defer_stream)
     g._collide_pending = bool(p.defer_collide)
     g._lag_pending = bool(p.hold_stream)

@@ -728,13 +728,12 @@ __global__ void __launch_bounds__(256) k_arc_inject_list(Dims d, float* __restri
             s_wd[k] = arc_weight(k, p.arc_k, 0.0f, p.pen, p.enable);
     __syncthreads();
     const float epw = scalars[kScalarEpw];
-    const int cnt = imin(list[0], tiles);
-    for (int e = blockIdx.x; e < cnt; e += gridDim.x) {
+    for_list_tiles(list, imin(list[0], tiles), [&](int ent) {
         int i, j, k, c;
-        if (!list_tile_cell(d, list[1 + e], i, j, k, c)) continue;
+        if (!list_tile_cell(d, ent, i, j, k, c)) return;
         const float wd = table ? s_wd[k] : arc_weight(k, p.arc_k, 0.0f, p.pen, p.enable);
         inject_cell(H, flags, f_l, epw, cap, ph, cp_f, vp, shape, wd, c);
-    }
+    });
 }
 
 struct ThermalArgs {
@@ -867,13 +866,12 @@ __global__ void __launch_bounds__(256) k_thermal_list(
         const int t = threadIdx.y * kTileK + threadIdx.x;
         if (t < kActiveShards) active_count[t] = 0u;
     }
-    const int cnt = imin(list[0], tiles);
-    for (int e = blockIdx.x; e < cnt; e += gridDim.x) {
+    for_list_tiles(list, imin(list[0], tiles), [&](int ent) {
         int i, j, k, c;
-        if (!list_tile_cell(d, list[1 + e], i, j, k, c)) continue;
+        if (!list_tile_cell(d, ent, i, j, k, c)) return;
         thermal_cell<TABLES>(d, H, H_next, T, T_next, f_l, ux, uy, uz, flags, T_max, T_prev, dT_dt,
                              a, tba, status, i, j, k, c);
-    }
+    });
 }
 
 // VOF advection + reinitialisation (kernels.py:2320-2391) -> phi_tmp.  A gas
@@ -954,12 +952,11 @@ __global__ void __launch_bounds__(256) k_vof_list(Dims d, const float* __restric
                                                   const float* __restrict__ uz,
                                                   const int32_t* __restrict__ flags,
                                                   const int32_t* __restrict__ list, int tiles) {
-    const int cnt = imin(list[0], tiles);
-    for (int e = blockIdx.x; e < cnt; e += gridDim.x) {
+    for_list_tiles(list, imin(list[0], tiles), [&](int ent) {
         int i, j, k, c;
-        if (!list_tile_cell(d, list[1 + e], i, j, k, c)) continue;
+        if (!list_tile_cell(d, ent, i, j, k, c)) return;
         vof_cell(d, phi, phi_tmp, ux, uy, uz, flags, i, j, k, c);
-    }
+    });
 }
 
 struct ColumnArgs {
@@ -1010,16 +1007,35 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
     ContactConst cc = contact_const(a.cos_t, a.sin_t);
     const float* src = a.vof ? phi_tmp : phi;
     const int KT = tiles_k(d), JT = tiles_j(d);
+    // The column's work bytes and chunk bits, all requested at once (lane kt
+    // holds chunk kt and kt + 32; KT <= 64 with tiles on), so that no chunk
+    // waits for a load of its own before its cells are requested.
+    uint64_t quiet_mask = 0;
+    unsigned cb_lo = 0u, cb_hi = 0u;
+    if (a.tile_work != nullptr) {
+        const int64_t tw0 = ((int64_t)i * JT + j / kTileJ) * KT;
+        const int64_t cb0 = ((int64_t)i * d.ny + j) * KT;
+        const bool in0 = lane < KT, in1 = lane + 32 < KT;
+        const unsigned w0 = in0 ? a.tile_work[tw0 + lane] : 1u;
+        const unsigned w1 = in1 ? a.tile_work[tw0 + lane + 32] : 1u;
+        cb_lo = in0 ? a.chunk_bits[cb0 + lane] : 0u;
+        cb_hi = in1 ? a.chunk_bits[cb0 + lane + 32] : 0u;
+        quiet_mask = (uint64_t)__ballot_sync(0xffffffffu, w0 == 0u) |
+                     ((uint64_t)__ballot_sync(0xffffffffu, w1 == 0u) << 32);
+    }
+    // chunk kc's bits as they were before this pass (warp-uniform kc)
+    auto old_bits = [&](int kc) -> unsigned {
+        return __shfl_sync(0xffffffffu, kc < 32 ? cb_lo : cb_hi, kc & 31);
+    };
     // A quiet chunk keeps its (GAS) flags.  Its flag copy is still written
     // until the last three passes have all written GAS copies of it (chunk
     // bits 4-5 count them), so that each of the three rotating copies holds
     // the whole step's flags however old its last worked pass is.
     auto skip = [&](int k0) -> bool {
-        const bool quiet = a.tile_work != nullptr &&
-                           a.tile_work[((int64_t)i * JT + j / kTileJ) * KT + k0 / kTileK] == 0;
+        const bool quiet = (quiet_mask >> (k0 >> 5)) & 1ull;
         if (quiet && flags_copy != nullptr) {
             uint8_t* cbp = a.chunk_bits + ((int64_t)i * d.ny + j) * KT + (k0 >> 5);
-            const unsigned old = *cbp;   // same address for the warp
+            const unsigned old = old_bits(k0 >> 5);
             const unsigned cnt = (old >> 4) & 3u;
             if (cnt < 3u) {
                 if (k0 + lane < d.nz) flags_copy[d.idx(i, j, k0 + lane)] = GAS;
@@ -1060,9 +1076,9 @@ __global__ void __launch_bounds__(256) k_column(Dims d, const float* __restrict_
                            // chunk bits: all GAS, that of the previous pass, top and
                            // bottom two cells GAS (cells beyond nz count as GAS)
                            const unsigned gm = __ballot_sync(0xffffffffu, !valid || flag == GAS);
+                           const unsigned old = old_bits(k >> 5);
                            if (lane == 0) {
                                uint8_t* cbp = a.chunk_bits + ((int64_t)i * d.ny + j) * KT + (k >> 5);
-                               const unsigned old = *cbp;
                                unsigned nb = gm == 0xffffffffu ? 1u : 0u;
                                if (a.tile_history && (old & 1u)) nb |= 2u;
                                if ((gm >> 30) == 3u) nb |= 4u;

@@ -91,6 +91,22 @@ __device__ __forceinline__ bool list_tile_cell(const Dims& d, int e, int& i, int
     return true;
 }
 
+// This block's share of the first cnt work-list entries (blockIdx.x, then every
+// gridDim.x-th), handed to f(entry) one after the other; the next entry is
+// requested before f works the current one, so that its load overlaps.
+template <class F>
+__device__ __forceinline__ void for_list_tiles(const int32_t* __restrict__ list, int cnt, F f) {
+    int e = blockIdx.x;
+    int ent = e < cnt ? list[1 + e] : -1;
+    while (e < cnt) {
+        const int e2 = e + (int)gridDim.x;
+        const int ent2 = e2 < cnt ? list[1 + e2] : -1;
+        f(ent);
+        e = e2;
+        ent = ent2;
+    }
+}
+
 // Slots of the fused step's device scalars (WaamFields::step_scalars).
 constexpr int kScalarArcK = 0;   // resolved arc k (written by the surface query)
 constexpr int kScalarWsum = 1;   // arc weight sum
