@@ -294,8 +294,6 @@ static int launch_stream_stored(Dims d, const void* f_src, void* f_dst, const in
 // Fused step kernels
 // ---------------------------------------------------------------------------
 
-// Surface height at the torch column + the arc-k fallback of
-// solvers/coupled_step.py:34-59 -> scalars[kScalarArcK].
 // Top metal cell of the torch column and the arc-k fallback of
 // solvers/coupled_step.py:34-59, computed by one warp (every lane returns it).
 __device__ __forceinline__ float surface_arc_k(const Dims& d, const float* phi,
