@@ -81,7 +81,7 @@ def _config_twins(kind, nx, ny, nz, material=None, **more):
     if goldak:
         tw.arc_source = Goldak3D(**goldak)
     tw.reset()
-    okw = {k: v for k, v in kw.items() if k != "step_mode"}
+    okw = {k: v for k, v in kw.items() if k not in ("step_mode", "population_dtype")}
     ot = OracleTwin(nx, ny, nz, dx, omat, goldak=goldak, tables=otables, contact_angle_deg=30.0,
                     **okw, **host)
     ot.reset()
@@ -177,17 +177,19 @@ def test_recoil_and_gas_shear_steps_match_oracle(step_mode, cc):
         steps.compare_state("recoil step %d" % s, tw.grid.state_dict(), ot.s)
 
 
+@pytest.mark.parametrize("dtype", ["float32", "float16"])
 @pytest.mark.parametrize("lorentz", [False, True])
-def test_pipelined_stream_matches_in_order_stream(lorentz):
+def test_pipelined_stream_matches_in_order_stream(lorentz, dtype):
     """Each step's stream left to run beside the next step's arc, thermal and VOF
     stages (joined before the column pass) gives the same states, bit for bit,
     as the stream run in order -- and so does the collision left pending as
     well, and the stream held back one more step to run beside the next
     collision on the cells it does not write (lagged) -- over droplet steps,
-    graph replays and the Lorentz split step; the state read-out runs the
-    pending work."""
+    graph replays and the Lorentz split step, in float32 and 16-bit population
+    storage; the state read-out runs the pending work."""
     states = []
     more = dict(enable_lorentz=True, welding_current_A=180.0) if lorentz else {}
+    more["population_dtype"] = dtype
     for mode in ("in_order", "stream", "stream_collide", "lagged"):
         tw, ot, dx = _config_twins("c2", 40, 24, 24, **more)
         tw.pipeline_stream = mode != "in_order"
