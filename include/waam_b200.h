@@ -736,7 +736,8 @@ typedef struct WaamStepParams {
      * defer_stream = 1: waam_step_main leaves this step's stream pending;
      * stream_prev = 1: it is pending from the step before -- waam_step_pre
      * starts it on a library stream beside the arc, thermal and VOF stages and
-     * waam_step_main joins it before the column pass.  A caller that reads or
+     * waam_step_main joins it before the column pass, or after it when the
+     * stream reads the flag copies (WaamFields.flags_copy_r).  A caller that reads or
      * writes populations between steps runs the pending stream first with
      * waam_step_stream.  defer_stream needs the remelt / solidify tail off
      * (it writes flags after the stream). */
