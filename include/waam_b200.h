@@ -672,6 +672,25 @@ typedef struct WaamFields {
      * lagged stream (WaamStepParams.hold_stream / stream_lag); with it the
      * caller rotates three buffers (w, r, rr) from step to step */
     const int32_t* flags_copy_rr;
+    /* Compact copy of the collision's output (all null: off).  Under the
+     * reference's buffer order (collide f_src -> f_dst at the active cells,
+     * stream f_dst -> f_src, swap) a cell active in two consecutive steps
+     * reads in the second exactly the populations its first collision wrote,
+     * so each collision also writes them, in stored form, to a slot of
+     * pop_cache_dst, and the next collision reads them from pop_cache_src
+     * (WaamStepParams.cache_read) in three or six 16-byte loads instead of
+     * 19 scattered ones.  Slot: ((i*ny + j) * ceil(nz/32) + k/32) * 2 + the
+     * cell's rank among the active cells of its 32-cell column chunk in k
+     * order (ranks 0 and 1; the others go without); 96 bytes (4-byte
+     * storage: 19 populations, cell index, stamp, pad) or 48 bytes (2-byte
+     * storage: 19 populations, 2 bytes pad, cell index, stamp); a slot counts
+     * only if its cell index and stamp match.  The caller allocates two
+     * buffers of nx*ny*ceil(nz/32)*2 slots, each filled with 0xff bytes, and
+     * swaps them with f_src / f_dst; pop_cache_stamp is one zeroed device
+     * word that the thermal stage counts up once per step. */
+    void* pop_cache_src;
+    void* pop_cache_dst;
+    uint32_t* pop_cache_stamp;
 } WaamFields;
 
 #define WAAM_HEALTH_NONFINITE_H 1u   /* H of a non-gas cell is NaN or infinite */
@@ -790,6 +809,13 @@ typedef struct WaamStepParams {
      * runs it before the pending collision. */
     int stream_lag;
     int hold_stream;
+    /* 1: the collision takes the populations of the cells whose slot in
+     * WaamFields.pop_cache_src holds their index and the previous step's
+     * stamp from that slot.  Only when nothing but the fused step's own
+     * collision and stream has written the populations since the previous
+     * collision (not after a droplet deposition, a state load, the moving
+     * window or an operator call). */
+    int cache_read;
 } WaamStepParams;
 
 /* Stages of one fused step.  waam_step_pre runs the surface-height query,

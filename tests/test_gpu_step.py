@@ -448,3 +448,90 @@ def test_quiet_tile_history_restarts_after_operator_calls():
     tw.invalidate()
     tw.step(0.3 * 40 * dx + 9e-6, 16 * dx, True)
     assert tw._fused_params.tile_skip == 0
+
+
+def _cache_slots(g):
+    """(cell index, stamp, stored populations as integers) of every slot of the
+    compact copy that goes with the buffer the next collision reads."""
+    from waam_solver_b200.grid import raw_field
+    a_first = g._read_buf is raw_field(g, "f_a")
+    cache = g.pop_caches[0 if a_first else 1]
+    if g.population_storage == 0:
+        w = cache.view(torch.int32).view(-1, 24)
+        return w[:, 19], w[:, 20], w[:, :19]
+    w = cache.view(torch.int32).view(-1, 12)
+    pops = cache.view(torch.int16).view(-1, 24)[:, :19].to(torch.int32)
+    return w[:, 10], w[:, 11], pops
+
+
+@pytest.mark.parametrize("dtype,lorentz", [("float32", False), ("float16", False),
+                                           ("bfloat16", False), ("float32", True)])
+def test_population_cache_matches_plane_reads(dtype, lorentz):
+    """The collision's compact copy of its output, read back by the next
+    collision for the cells active in both steps, against the 19 population
+    planes read every step (no copy), bit for bit, through droplet steps, graph
+    replays, the pipelined and lagged stream and (with the welding current)
+    the Lorentz split step, in float32 and 16-bit population storage.  The
+    copy really is read (cache_read on the regular steps) and every slot the
+    last collision wrote holds its cell's stored populations."""
+    states = []
+    more = dict(enable_lorentz=True, welding_current_A=180.0) if lorentz else {}
+    more["population_dtype"] = dtype
+    for cached in (False, True):
+        tw, ot, dx = _config_twins("c2", 40, 32, 96, **more)
+        tw.population_cache = cached
+        tw._last_droplet_time = -1.0
+        g = tw.grid
+        reads = 0
+        for s in range(40):
+            tw.step(0.3 * 40 * dx + s * 1e-6, 16 * dx, not 25 <= s < 28)
+            reads += tw._fused_params.cache_read
+        torch.cuda.synchronize()
+        states.append(g.state_dict())
+        assert tw._n_droplets_fired >= 1
+        if not cached:
+            assert getattr(g, "pop_caches", None) is None and reads == 0
+            continue
+        assert reads >= 30
+        tag, stamp, pops = _cache_slots(g)
+        live = (stamp == int(g.pop_cache_stamp.item())) & (tag >= 0)
+        cells = tag[live].long()
+        assert cells.numel() >= 40 * 32      # two plate-top cells per column, at least
+        f = g._read_buf.reshape(19, -1)
+        stored = f.view(torch.int32) if g.population_storage == 0 else f.view(torch.int16)
+        assert torch.equal(stored[:, cells].T.to(torch.int32), pops[live])
+    for k, v in states[0].items():
+        if isinstance(v, np.ndarray):
+            assert np.array_equal(v, states[1][k]), k
+
+
+def test_population_cache_read_stops_after_other_population_writes():
+    """The next collision reads the compact copy only when nothing but the
+    fused step wrote the populations since the previous collision: not on a
+    droplet step (the deposition writes them before its collision), nor
+    after an operator-API stream call, a state load or invalidate()."""
+    from waam_solver_b200 import kernels
+    tw, ot, dx = _config_twins("c2", 40, 32, 96)
+    g = tw.grid
+    x = lambda s: 0.3 * 40 * dx + s * 1e-6   # noqa: E731
+    for s in range(4):
+        tw.step(x(s), 16 * dx, True)
+    assert tw._fused_params.cache_read == 1
+    kernels.stream(g.f_src, g.f_dst, g.flags, 1, 2, g.nx, g.ny, g.nz)
+    tw.step(x(4), 16 * dx, True)
+    assert tw._fused_params.cache_read == 0
+    tw.step(x(5), 16 * dx, True)
+    assert tw._fused_params.cache_read == 1
+    g.load_state(g.state_dict())
+    tw.step(x(6), 16 * dx, True)
+    assert tw._fused_params.cache_read == 0
+    tw.step(x(7), 16 * dx, True)
+    tw.invalidate()
+    tw.step(x(8), 16 * dx, True)
+    assert tw._fused_params.cache_read == 0
+    tw._last_droplet_time = -1.0
+    n0 = tw._n_droplets_fired
+    tw.step(x(9), 16 * dx, True)
+    assert tw._n_droplets_fired == n0 + 1 and tw._fused_params.cache_read == 0
+    tw.step(x(10), 16 * dx, True)
+    assert tw._fused_params.cache_read == 1

@@ -34,7 +34,8 @@ class WaamFields(C.Structure):
         ("lorentz_J", C.c_void_p * 3), ("lorentz_B", C.c_void_p * 3),
         ("flags_copy_w", C.c_void_p), ("flags_copy_r", C.c_void_p), ("status", C.c_void_p),
         ("tile_bits", C.c_void_p), ("tile_list", C.c_void_p), ("tile_part", C.c_void_p),
-        ("flags_copy_rr", C.c_void_p)]
+        ("flags_copy_rr", C.c_void_p), ("pop_cache_src", C.c_void_p),
+        ("pop_cache_dst", C.c_void_p), ("pop_cache_stamp", C.c_void_p)]
 
 
 TABLE_KNOTS = 8

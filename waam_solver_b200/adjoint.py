@@ -399,6 +399,7 @@ def _taped_step(tw, x, y, tape, slot):
     # taped steps follow checkpoint restores: every tile worked, and the next
     # fused step restarts the tile history too
     p.tile_skip = 0
+    p.cache_read = 0
     g._tiles_valid = False
     arc_i, arc_j = sim_x / g.dx, sim_y / g.dx
     p.arc_i, p.arc_j = arc_i, arc_j

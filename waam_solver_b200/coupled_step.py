@@ -308,6 +308,13 @@ def _fields(g):
         f.flags_copy_r = copies[(w + 2) % 3].data_ptr()
         f.flags_copy_rr = copies[(w + 1) % 3].data_ptr()
     f.status = g.step_status.data_ptr()
+    caches = getattr(g, "pop_caches", None)
+    if caches is not None:
+        # each compact copy goes with its population buffer
+        a_first = g._read_buf is raw_field(g, "f_a")
+        f.pop_cache_src = caches[0 if a_first else 1].data_ptr()
+        f.pop_cache_dst = caches[1 if a_first else 0].data_ptr()
+        f.pop_cache_stamp = g.pop_cache_stamp.data_ptr()
     if g.nz > 32:
         # quiet tiles need a k tile above the plate's: with one 32-cell k tile
         # every tile holds metal, and the list would only add a kernel
@@ -540,6 +547,16 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
         g.flags_copies = tuple(torch.zeros_like(g.flags) for _ in range(3))
         g._flags_copy_i = 0
         g.__dict__.pop("_fields_cache", None)
+    if getattr(g, "pop_caches", None) is None and getattr(twin, "population_cache", True):
+        # the compact copies of the collision's output (WaamFields.pop_cache_*):
+        # two slots per 32-cell column chunk, 96 or 48 bytes each, filled with
+        # 0xff bytes (a cell index no cell has)
+        slot = 96 if g.population_storage == 0 else 48
+        nbytes = g.nx * g.ny * ((g.nz + 31) // 32) * 2 * slot
+        g.pop_caches = tuple(torch.full((nbytes,), 255, dtype=torch.uint8, device=g.device)
+                             for _ in range(2))
+        g.pop_cache_stamp = torch.zeros(1, dtype=torch.int32, device=g.device)
+        g.__dict__.pop("_fields_cache", None)
     f = _fields_cached(g)
     ws = g.workspace
     upload_position(twin, arc_i, arc_j)
@@ -576,6 +593,14 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
                         g.__dict__.get("_tile_epoch") == kernels.STATE_EPOCH[0] and not due and
                         not p.clear_forces and
                         not (twin.enable_bead_freeze or twin.enable_substrate_growth)) else 0
+    # population cache: read only while nothing but the fused step has written
+    # the populations since the previous collision (the conditions of the
+    # tile history that concern them: no state change since the previous
+    # fused step completed, no droplet deposition before this collision)
+    p.cache_read = 1 if (getattr(g, "pop_caches", None) is not None and
+                         getattr(twin, "population_cache", True) and g._tiles_valid and
+                         g.__dict__.get("_tile_epoch") == kernels.STATE_EPOCH[0] and
+                         not due) else 0
     # until this step completes: a step that raises part-way leaves the next
     # one a tile-history restart (which also zeroes the work-list count)
     g._tiles_valid = False
@@ -583,7 +608,7 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     if not due and not lorentz and events is None and getattr(twin, "use_cuda_graphs", True):
         key = (g._read_buf is raw_field(g, "f_a"), g._cur, p.welding, p.clear_forces, p.stream_prev,
                p.defer_stream, p.collide_prev, p.collide_prev_welding, p.defer_collide,
-               g._flags_copy_i, p.tile_skip, p.stream_lag, p.hold_stream,
+               g._flags_copy_i, p.tile_skip, p.stream_lag, p.hold_stream, p.cache_read,
                (dx_, dy_, dz_) if twin.enable_bead_freeze else None)
         done = _run_graph(twin, g, f, p, ws, key)
     if not done:

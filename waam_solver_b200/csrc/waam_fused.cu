@@ -739,6 +739,7 @@ struct ThermalArgs {
     float cpa, dt_lu, inv_dt;
     int heat_loss, conv, rad;
     float T_amb, h_conv, eps_rad, dt_phys, dx, sigma_sb, h_floor;
+    uint32_t* cache_stamp;  // counted up once per step (null: no population cache)
 };
 
 // Table path of the thermal stage: the property refresh (kernels.py:1710-1772)
@@ -841,6 +842,7 @@ __global__ void __launch_bounds__(256) k_thermal_fused(
     if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
         const int t = threadIdx.y * kTileK + threadIdx.x;
         if (t < kActiveShards) active_count[t] = 0u;
+        if (t == 0 && a.cache_stamp) *a.cache_stamp += 1u;
     }
     int i, j, k, c;
     if (!tile_cell(d, i, j, k, c)) return;
@@ -865,6 +867,7 @@ __global__ void __launch_bounds__(256, TABLES ? 1 : 6) k_thermal_list(
     if (blockIdx.x == 0) {
         const int t = threadIdx.y * kTileK + threadIdx.x;
         if (t < kActiveShards) active_count[t] = 0u;
+        if (t == 0 && a.cache_stamp) *a.cache_stamp += 1u;
     }
     for_list_tiles(list, imin(list[0], tiles), [&](int ent) {
         int i, j, k, c;
@@ -1124,6 +1127,86 @@ struct CollideArgs {
     float lz_dt, lz_dx, lz_rho;
     uint32_t* status;       // health word (null: off)
     float rho_lo, rho_hi;   // density band of WAAM_HEALTH_RHO_RANGE (off when hi <= lo)
+    // population cache (cache_out null: off; cache_in null: not read this step)
+    const void* cache_in;
+    void* cache_out;
+    const uint32_t* stamp;
+};
+
+// Compact copy of the collision's output (WaamFields.pop_cache_*).  Slot
+// (column * ceil(nz/32) + k/32) * kCacheDepth + rank, rank = the cell's place
+// among the active cells of its 32-cell column chunk (the column pass lists
+// them one after another in k order, so the rank comes from the list entries
+// just before the cell's); cells of rank kCacheDepth and above go without.
+// A slot holds the cell's 19 stored populations (4-byte storage: one word
+// each; 2-byte storage: two per word, the last half-word zero), then the
+// cell index and the stamp of the step that wrote it: 24 or 12 words, read
+// and written as 16-byte vectors.
+constexpr int kCacheDepth = 2;
+
+__device__ __forceinline__ uint32_t pop_bits(float v) { return __float_as_uint(v); }
+__device__ __forceinline__ uint32_t pop_bits(__half v) { return __half_as_ushort(v); }
+__device__ __forceinline__ uint32_t pop_bits(__nv_bfloat16 v) { return __bfloat16_as_ushort(v); }
+template <typename T>
+__device__ __forceinline__ T pop_of_bits(uint32_t b);
+template <>
+__device__ __forceinline__ float pop_of_bits<float>(uint32_t b) { return __uint_as_float(b); }
+template <>
+__device__ __forceinline__ __half pop_of_bits<__half>(uint32_t b) {
+    return __ushort_as_half((unsigned short)b);
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 pop_of_bits<__nv_bfloat16>(uint32_t b) {
+    return __ushort_as_bfloat16((unsigned short)b);
+}
+
+template <int S>
+struct PopCache {
+    typedef typename Pop<S>::T T;
+    static constexpr int kWords = S == kStoreF32 ? 24 : 12;
+    static constexpr int kTag = S == kStoreF32 ? 19 : 10;   // cell index, then stamp
+
+    // f = the slot's populations if it holds cell c with this stamp
+    __device__ static __forceinline__ bool load(const void* cache, int slot, int c,
+                                                uint32_t stamp, float* f) {
+        const uint4* v = reinterpret_cast<const uint4*>(cache) + (int64_t)slot * (kWords / 4);
+        uint32_t w[kWords];
+#pragma unroll
+        for (int u = 0; u < kWords / 4; ++u) {
+            const uint4 x = v[u];
+            w[4 * u] = x.x;
+            w[4 * u + 1] = x.y;
+            w[4 * u + 2] = x.z;
+            w[4 * u + 3] = x.w;
+        }
+        if (w[kTag] != (uint32_t)c || w[kTag + 1] != stamp) return false;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const uint32_t b = S == kStoreF32 ? w[q] : (w[q >> 1] >> (16 * (q & 1))) & 0xffffu;
+            f[q] = Pop<S>::get(pop_of_bits<T>(b), q);
+        }
+        return true;
+    }
+
+    __device__ static __forceinline__ void store(void* cache, int slot, int c, uint32_t stamp,
+                                                 const T* o) {
+        uint32_t w[kWords];
+#pragma unroll
+        for (int u = 0; u < kWords; ++u) w[u] = 0u;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            if (S == kStoreF32)
+                w[q] = pop_bits(o[q]);
+            else
+                w[q >> 1] |= pop_bits(o[q]) << (16 * (q & 1));
+        }
+        w[kTag] = (uint32_t)c;
+        w[kTag + 1] = stamp;
+        uint4* v = reinterpret_cast<uint4*>(cache) + (int64_t)slot * (kWords / 4);
+#pragma unroll
+        for (int u = 0; u < kWords / 4; ++u)
+            v[u] = make_uint4(w[4 * u], w[4 * u + 1], w[4 * u + 2], w[4 * u + 3]);
+    }
 };
 
 // kernels.py:1479-1513 apply_lorentz_JxB for one cell (f_l >= 0.05)
@@ -1181,6 +1264,8 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
     const bool lorentz = a.J[0] != nullptr;
     const float F_cap = P.F_cap;
     if (lorentz) P.F_cap = 0.0f;   // clamped below, after J x B
+    // the stamp of this step (slots of the previous step carry stamp - 1)
+    const uint32_t stamp = a.cache_out != nullptr ? *a.stamp : 0u;
     for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt;
          t += gridDim.x * blockDim.x) {
         int lo = 0, hi = kActiveShards;  // last shard with start <= t
@@ -1188,16 +1273,37 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
             int mid = (lo + hi) >> 1;
             if (start[mid] <= t) lo = mid; else hi = mid;
         }
-        const int c = active_list[(int64_t)lo * shard_cap + (t - start[lo])];
+        const int64_t at = (int64_t)lo * shard_cap + (t - start[lo]);
+        const int c = active_list[at];
         const int k = c % d.nz;
         const int r = c / d.nz;
         const int j = r % d.ny;
         const int i = r / d.ny;
+        int slot = -1;
+        if (a.cache_out != nullptr) {
+            // rank in the chunk: the entries before it in this shard that lie
+            // in the same chunk below it (cells c - (k % 32) .. c - 1)
+            const int chunk_lo = c - (k & 31);
+            const unsigned pos = t - start[lo];
+            int rk = 0;
+            while (rk < kCacheDepth && (unsigned)rk < pos) {
+                const int e = active_list[at - 1 - rk];
+                if (e < chunk_lo || e >= c) break;
+                ++rk;
+            }
+            if (rk < kCacheDepth) slot = (r * ((d.nz + 31) >> 5) + (k >> 5)) * kCacheDepth + rk;
+        }
         // the populations (DRAM) are requested first so that their latency
-        // overlaps the force stencil (cache-resident phi, T, flags)
+        // overlaps the force stencil (cache-resident phi, T, flags): from the
+        // cache slot when it holds this cell from the previous step, else
+        // from the 19 population planes
         float f[19], o[19];
+        const bool hit = a.cache_in != nullptr && slot >= 0 &&
+                         PopCache<S>::load(a.cache_in, slot, c, stamp - 1u, f);
+        if (!hit) {
 #pragma unroll
-        for (int q = 0; q < 19; ++q) f[q] = Pop<S>::get(f_src[q * n + c], q);
+            for (int q = 0; q < 19; ++q) f[q] = Pop<S>::get(f_src[q * n + c], q);
+        }
         if (tape) {
             a.tape_cells[t] = c;
 #pragma unroll
@@ -1233,8 +1339,13 @@ __global__ void __launch_bounds__(kListThreads) k_collide_list(
         else  // kernels.py:2889-2965: omega = 1 / (tau + 1e-6) per cell
             collide_srt_cell(f, fl, fx, fy, fz, a.kind == 2 ? 1.0f / (tau_c + 1e-6f) : a.omega,
                              a.C_darcy, o, rr, u, v, w);
+        typename Pop<S>::T so[19];
 #pragma unroll
-        for (int q = 0; q < 19; ++q) f_dst[q * n + c] = Pop<S>::put(o[q], q);
+        for (int q = 0; q < 19; ++q) {
+            so[q] = Pop<S>::put(o[q], q);
+            f_dst[q * n + c] = so[q];
+        }
+        if (slot >= 0) PopCache<S>::store(a.cache_out, slot, c, stamp, so);
         if (a.u_cap > 0.0f) clamp_mach(u, v, w, a.u_cap);
         if (a.status != nullptr) {
             if (!(isfinite(rr) && isfinite(u) && isfinite(v) && isfinite(w)))
@@ -1447,6 +1558,13 @@ static const char* lag_error(const WaamFields* f, const WaamStepParams* p) {
     if (p->hold_stream && (!p->stream_prev || !p->defer_collide || !f->flags_copy_r ||
                            !f->flags_copy_w || !f->flags_copy_rr))
         return "hold_stream needs stream_prev, defer_collide and three flag copies";
+    const bool any = f->pop_cache_src || f->pop_cache_dst || f->pop_cache_stamp;
+    const bool all = f->pop_cache_src && f->pop_cache_dst && f->pop_cache_stamp;
+    if (any && (!all || f->pop_cache_src == f->pop_cache_dst ||
+                (reinterpret_cast<uintptr_t>(f->pop_cache_src) |
+                 reinterpret_cast<uintptr_t>(f->pop_cache_dst)) % 16 != 0))
+        return "population cache needs two distinct 16-byte aligned buffers and the stamp";
+    if (p->cache_read && !all) return "cache_read needs the population cache";
     return nullptr;
 }
 
@@ -1696,6 +1814,18 @@ static int launch_collide_tracers(const WaamFields* f, const WaamStepParams* p, 
     cl.status = f->status;
     cl.rho_lo = p->rho_lo;
     cl.rho_hi = p->rho_hi;
+    // the population cache: pop_in is f_src (this step's collision) or f_dst
+    // (the previous step's, after the buffer swap); each cache buffer goes
+    // with its population buffer
+    cl.cache_in = nullptr;
+    cl.cache_out = nullptr;
+    cl.stamp = nullptr;
+    if (f->pop_cache_dst) {
+        const bool fwd = pop_in == f->f_src;
+        cl.cache_out = fwd ? f->pop_cache_dst : f->pop_cache_src;
+        if (p->cache_read) cl.cache_in = fwd ? f->pop_cache_src : f->pop_cache_dst;
+        cl.stamp = f->pop_cache_stamp;
+    }
 #define WAAM_COLLIDE(S)                                                                    \
     k_collide_list<S><<<kListBlocks, kListThreads, 0, s>>>(                                \
         d, static_cast<const Pop<S>::T*>(pop_in), static_cast<Pop<S>::T*>(pop_out),              \
@@ -1794,6 +1924,7 @@ static int step_main_impl(const WaamFields* f, const WaamStepParams* p, void* wo
         ta.dx = p->dx;
         ta.sigma_sb = p->sigma_sb;
         ta.h_floor = p->cp_rho * p->T_amb;
+        ta.cache_stamp = f->pop_cache_dst ? f->pop_cache_stamp : nullptr;
         TableArgs tba{};
         if (p->use_tables) {
             tba.vp = var_phase(p);

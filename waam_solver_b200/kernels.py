@@ -106,6 +106,11 @@ _TILE_STATE_WRITERS = frozenset({
     "waam_solidify_cooled_metal", "waam_solidify_trailing_pool",
     "waam_solidify_trailing_pool_scalar", "waam_sync_phi_liquid_fraction",
     "waam_update_flags_from_phi", "waam_update_phase", "waam_update_phase_variable_cp"})
+# Entry points that write populations (besides those above): they end the
+# fused step's population cache as well.
+_POPULATION_WRITERS = frozenset({
+    "waam_collide_mrt", "waam_collide_srt", "waam_collide_srt_variable_tau", "waam_stream",
+    "waam_feed_wire_momentum", "waam_feed_wire_momentum_impact_stored"})
 STATE_EPOCH = [0]
 # Grids whose last fused step left work pending (its stream, or its collision,
 # tracers and stream): a state-writing operator call runs that work first,
@@ -125,7 +130,7 @@ def state_changed():
 
 
 def _call(name, *args):
-    if name in _TILE_STATE_WRITERS:
+    if name in _TILE_STATE_WRITERS or name in _POPULATION_WRITERS:
         state_changed()
     return _native.call(name, *args)
 

@@ -268,8 +268,10 @@ class WAAMTwin:
         g._collide_pending = False
         g._lag_pending = False
         f_a, f_b = g.f_a, g.f_b
-        if g.population_storage:   # initialise and stream in float32, then store offsets
-            f_a, f_b = torch.empty(f_a.shape, device=g.device), torch.empty(f_b.shape,
+        if g.population_storage:
+            # initialise and stream in float32, then store offsets; zeroed like
+            # the float32 buffers, since the stream leaves SOLID cells alone
+            f_a, f_b = torch.zeros(f_a.shape, device=g.device), torch.zeros(f_b.shape,
                                                                               device=g.device)
         kernels.init_grid(f_a, g.rho, g.ux, g.uy, g.uz, g.T, g.H, g.f_l, g.phi, g.flags, T0,
                           RHO_LATTICE, self.cp_rho, nz_solid, i0, i1, j0, j1, g.FLAG_FLUID,
