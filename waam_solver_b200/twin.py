@@ -205,8 +205,9 @@ class WAAMTwin:
     # -- configuration ----------------------------------------------------
     def invalidate(self):
         """Drop cached step parameters after changing a twin attribute, and the
-        fused step's quiet-tile history -- call it after writing grid fields
-        (flags, phi, f_l, H, T) directly, outside this package's operators."""
+        fused step's quiet-tile history and population copy -- call it after
+        writing grid fields (flags, phi, f_l, H, T, populations) directly,
+        outside this package's operators."""
         self._fused_params = None
         self.grid.__dict__.pop("_fields_cache", None)
         self.grid._tiles_valid = False
