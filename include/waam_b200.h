@@ -816,6 +816,9 @@ typedef struct WaamStepParams {
      * collision (not after a droplet deposition, a state load, the moving
      * window or an operator call). */
     int cache_read;
+    /* cache_read of the pending collision (collide_prev = 1): the previous
+     * step's own cache_read */
+    int collide_prev_cache_read;
 } WaamStepParams;
 
 /* Stages of one fused step.  waam_step_pre runs the surface-height query,
@@ -836,8 +839,9 @@ int waam_step_main(const WaamFields* f, const WaamStepParams* p, void* workspace
  * writes f_dst, with the flags of that step. */
 int waam_step_stream(const WaamFields* f, const WaamStepParams* p, void* stream);
 /* The collision, tracers and stream left pending by the previous step
- * (WaamStepParams.defer_collide; p->collide_prev_welding is that step's
- * welding flag), for fields that describe the step after it (buffers
+ * (WaamStepParams.defer_collide; p->collide_prev_welding and
+ * p->collide_prev_cache_read are that step's welding flag and cache_read),
+ * for fields that describe the step after it (buffers
  * swapped, thermal fields flipped). */
 int waam_step_finish(const WaamFields* f, const WaamStepParams* p, void* workspace,
                      size_t workspace_bytes, void* stream);

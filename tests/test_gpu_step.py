@@ -535,3 +535,33 @@ def test_population_cache_read_stops_after_other_population_writes():
     assert tw._n_droplets_fired == n0 + 1 and tw._fused_params.cache_read == 0
     tw.step(x(10), 16 * dx, True)
     assert tw._fused_params.cache_read == 1
+
+
+def test_population_cache_after_reloading_an_older_state():
+    """Back to an older state (as the adjoint's checkpoints and FD probes do):
+    the first collision after the reload, left pending by its step, must not
+    read the copy the newer state's last collision wrote -- the pending
+    collision reads as its own step decided (collide_prev_cache_read), not as
+    the step that runs it.  Against the same sequence without the copy."""
+    states = []
+    for cached in (False, True):
+        tw, ot, dx = _config_twins("c2", 40, 32, 96)
+        tw.population_cache = cached
+        g = tw.grid
+        x = lambda s: 0.3 * 40 * dx + s * 1e-6   # noqa: E731
+        for s in range(6):
+            tw.step(x(s), 16 * dx, True)
+        older = g.state_dict()
+        for s in range(6, 16):
+            tw.step(x(s), 16 * dx, True)
+        g.load_state(older)
+        reads = []
+        for s in range(6, 14):
+            tw.step(x(s), 16 * dx, True)
+            reads.append(tw._fused_params.cache_read)
+        assert reads[0] == 0 and (sum(reads[1:]) > 0) == cached
+        torch.cuda.synchronize()
+        states.append(g.state_dict())
+    for k, v in states[0].items():
+        if isinstance(v, np.ndarray):
+            assert np.array_equal(v, states[1][k]), k

@@ -400,6 +400,7 @@ def _taped_step(tw, x, y, tape, slot):
     # fused step restarts the tile history too
     p.tile_skip = 0
     p.cache_read = 0
+    p.collide_prev_cache_read = 0
     g._tiles_valid = False
     arc_i, arc_j = sim_x / g.dx, sim_y / g.dx
     p.arc_i, p.arc_j = arc_i, arc_j

@@ -575,6 +575,8 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     collide_prev = bool(g.__dict__.get("_collide_pending", False))
     p.collide_prev = 1 if collide_prev else 0
     p.collide_prev_welding = g.__dict__.get("_pending_welding", 0) if collide_prev else 0
+    # the pending collision reads the population copy as its own step decided
+    p.collide_prev_cache_read = g.__dict__.get("_pending_cache_read", 0) if collide_prev else 0
     p.stream_prev = 1 if (collide_prev or g.__dict__.get("_stream_pending", False)) else 0
     p.defer_stream = 1 if (getattr(twin, "pipeline_stream", True) and events is None and
                            not (twin.enable_bead_freeze or twin.enable_substrate_growth)) else 0
@@ -607,7 +609,8 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     done = False
     if not due and not lorentz and events is None and getattr(twin, "use_cuda_graphs", True):
         key = (g._read_buf is raw_field(g, "f_a"), g._cur, p.welding, p.clear_forces, p.stream_prev,
-               p.defer_stream, p.collide_prev, p.collide_prev_welding, p.defer_collide,
+               p.defer_stream, p.collide_prev, p.collide_prev_welding,
+               p.collide_prev_cache_read, p.defer_collide,
                g._flags_copy_i, p.tile_skip, p.stream_lag, p.hold_stream, p.cache_read,
                (dx_, dy_, dz_) if twin.enable_bead_freeze else None)
         done = _run_graph(twin, g, f, p, ws, key)
@@ -660,9 +663,11 @@ def coupled_step_fused(twin, torch_x_m, torch_y_m, is_welding, torch_z_m=None):
     if p.defer_collide:
         q = _native.WaamStepParams.from_buffer_copy(p)
         q.collide_prev, q.collide_prev_welding = 1, p.welding
+        q.collide_prev_cache_read = p.cache_read
         q.stream_lag, q.hold_stream = p.hold_stream, 0
         g._pending_params = q
         g._pending_welding = p.welding
+        g._pending_cache_read = p.cache_read
     g._flags_copy_i = (g._flags_copy_i + 1) % 3    # this step's copy is read by the next two
     g._tiles_valid = True                    # this step's column pass wrote the chunk bits
     g._tile_epoch = kernels.STATE_EPOCH[0]

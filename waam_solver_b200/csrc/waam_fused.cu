@@ -1564,7 +1564,8 @@ static const char* lag_error(const WaamFields* f, const WaamStepParams* p) {
                 (reinterpret_cast<uintptr_t>(f->pop_cache_src) |
                  reinterpret_cast<uintptr_t>(f->pop_cache_dst)) % 16 != 0))
         return "population cache needs two distinct 16-byte aligned buffers and the stamp";
-    if (p->cache_read && !all) return "cache_read needs the population cache";
+    if ((p->cache_read || p->collide_prev_cache_read) && !all)
+        return "cache_read needs the population cache";
     return nullptr;
 }
 
@@ -1823,7 +1824,8 @@ static int launch_collide_tracers(const WaamFields* f, const WaamStepParams* p, 
     if (f->pop_cache_dst) {
         const bool fwd = pop_in == f->f_src;
         cl.cache_out = fwd ? f->pop_cache_dst : f->pop_cache_src;
-        if (p->cache_read) cl.cache_in = fwd ? f->pop_cache_src : f->pop_cache_dst;
+        if (fwd ? p->cache_read : p->collide_prev_cache_read)
+            cl.cache_in = fwd ? f->pop_cache_src : f->pop_cache_dst;
         cl.stamp = f->pop_cache_stamp;
     }
 #define WAAM_COLLIDE(S)                                                                    \
