@@ -919,6 +919,7 @@ def run_b200(args, w):
         drop_info = droplet_period_timing(tw, pos, s, period, device)
         s += period
     clocks.__exit__(None, None, None)
+    health = tw.health()
 
     value = world * cells * K / (ms * 1e-3) / 1e6
     e2e = world * cells * K / (ms_e2e * 1e-3) / 1e6
@@ -945,6 +946,12 @@ def run_b200(args, w):
                             Ks, "run eagerly (the potential solve reads back its convergence "
                             "checks)" if lorentz else "replay CUDA graphs"),
         "clocks": clocks.summary(),
+        # the fused step's health word over the whole run (non-finite enthalpy,
+        # density or velocity, density out of band): the numbers above hold
+        # for a state that stayed finite (the standard workload from reset
+        # leaves its finite window after about 9,000 steps, oracle and GPU alike)
+        "health": {"word": health["word"], "steps_run": tw._step_n,
+                   "finite": not (health["nonfinite_enthalpy"] or health["nonfinite_lbm"])},
     }
     if drop_info:
         line["droplet_period"] = drop_info

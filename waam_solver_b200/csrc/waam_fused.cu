@@ -29,10 +29,12 @@ constexpr int kTileRedBlocks = 592;   // <= kWsMaxPartials; a fixed grid keeps t
 constexpr int kListThreads = 128;
 constexpr int kArcTableMax = 1024;    // nz up to which the arc depth weights come from a table
 constexpr int kArcAxisMax = 3072;     // nx + ny + nz up to which the arc shape uses axis tables
-// the collision's persistent grid: 2 blocks of 128 threads (96 registers) per
-// SM hold 3/8 of its register file, leaving room for the stage kernels that
-// run beside it (measured: 2 per SM beat 3, 4 and 6)
-constexpr int kListBlocks = 148 * 2;
+// the collision's persistent grid: 4 blocks of 128 threads (96 registers) per
+// SM, 75,776 threads, one pass over the ~66 k active cells of the standard
+// workload (measured with the population copy: 0.2132 against 0.2154 ms per
+// droplet period for 2 per SM, 0.2150 for 3; no change on the 512x256x160
+// and 64x32x32 workloads; without the copy 2 per SM had been best)
+constexpr int kListBlocks = 148 * 4;
 
 
 // ---------------------------------------------------------------------------
