@@ -180,8 +180,11 @@ class WAAMGrid:
         self.n_elec_bins = 64
         self.elec_rad_bins = torch.zeros((self.nz, self.n_elec_bins), dtype=torch.float32,
                                          device=self.device)
-        self.elec_res_buf = torch.zeros((), dtype=torch.float32, device=self.device)
-        self.elec_norm_buf = torch.zeros((), dtype=torch.float32, device=self.device)
+        # the Jacobi check's L1 change and norm, side by side so that one
+        # device-to-host copy reads both
+        self.elec_res_norm = torch.zeros(2, dtype=torch.float32, device=self.device)
+        self.elec_res_buf = self.elec_res_norm[0]
+        self.elec_norm_buf = self.elec_res_norm[1]
         self._has_lorentz = True
 
     def ensure_export_buffers(self):

@@ -70,7 +70,8 @@ def solve_lorentz(twin, g, arc_i, arc_j, arc_k, apply_force=True, arc_k_dev=None
         if chunk % 2 == 1:
             g.phi_elec, g.phi_elec_tmp = g.phi_elec_tmp, g.phi_elec
         iters_done += chunk
-        rel = float(g.elec_res_buf.item()) / max(float(g.elec_norm_buf.item()), 1e-30)
+        res, norm = g.elec_res_norm.tolist()
+        rel = res / max(norm, 1e-30)
         if rel < tol:
             converged = True
             break
