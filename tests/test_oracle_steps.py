@@ -69,3 +69,29 @@ def test_oracle_trajectory_matches_reference(name, monkeypatch):
         ot.step(x, y, True)
     steps.compare_state("%s trajectory" % name, ot.s, states[-1],
                         fields=steps.fields_for(name), reference=True)
+
+
+def test_trajectory_fixture_is_complete_and_consistent():
+    """tests/golden/trajectory_standard.json (make_trajectory.py): one record
+    every 500 steps, droplets counted up by one per 100 Hz period, the state
+    finite through step 9,000, and the hash helper the GPU test shares is the
+    SHA-1 of the float32 bytes."""
+    import hashlib
+    import json
+    import os
+    import sys
+
+    import numpy as np
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    from make_trajectory import FIELDS, field_hash
+    with open(os.path.join(here, "golden", "trajectory_standard.json")) as fh:
+        fix = json.load(fh)
+    recs = fix["records"]
+    assert [r["step"] for r in recs] == list(range(500, fix["n_steps"] + 1, 500))
+    finite = [r for r in recs if r["nonfinite_T"] == 0]
+    assert finite[-1]["step"] >= 9000 and all(r["nonfinite_T"] == 0 for r in recs[:len(finite)])
+    assert all(b["drops"] - a["drops"] == 1 for a, b in zip(recs, recs[1:]))
+    assert all(len(r[k]) == 12 for r in recs for k in FIELDS)
+    a = np.arange(10, dtype=np.float64)
+    assert field_hash(a) == hashlib.sha1(a.astype(np.float32).tobytes()).hexdigest()[:12]
