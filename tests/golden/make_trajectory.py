@@ -1,16 +1,17 @@
-"""Full-size trajectory fixture: field hashes of the standard bench workload
-(256x128x96 D3Q19 bead-on-plate, Goldak 4 kW, 100 Hz droplets, VOF, wetting,
-CSF, Marangoni, buoyancy, gravity, central-moment MRT) every ``every`` steps
-from the reference reset state, computed by the CPU oracle.
+"""Full-size trajectory fixtures: field hashes of a bench workload every
+``every`` steps from the reference reset state, computed by the CPU oracle --
+the standard workload (256x128x96 D3Q19 bead-on-plate, Goldak 4 kW, 100 Hz
+droplets, VOF, wetting, CSF, Marangoni, buoyancy, gravity, central-moment
+MRT) and the small one (64x32x32, Gaussian 3 kW, no wire, VOF).
 
 TEST INFRASTRUCTURE ONLY.  The GPU test (tests/test_gpu_trajectory.py)
 runs the same steps through WAAMTwin and compares the hashes bit for bit::
 
-    python tests/golden/make_trajectory.py [n_steps] [every]
+    python tests/golden/make_trajectory.py [workload] [n_steps] [every]
 
-(about 40 minutes on 8 host cores for 10,000 steps).  The oracle twin is
-built as bench.py's CPU baseline builds it, on the torch path of
-bench.path_steps.
+(standard: about 40 minutes on 8 host cores for 10,000 steps; small: a few
+seconds for 2,000).  The oracle twin is built as bench.py's CPU baseline
+builds it, on the torch path of bench.path_steps.
 """
 from __future__ import annotations
 
@@ -24,7 +25,6 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-OUT = os.path.join(HERE, "trajectory_standard.json")
 FIELDS = ("T", "phi", "f_l", "flags", "ux", "f_a", "f_b")
 
 
@@ -55,21 +55,32 @@ def oracle_twin(w):
     O.call("wo_set_num_threads", os.cpu_count() or 1)
     kw = bench.twin_kwargs(w)
     kw.pop("wire_diameter_mm", None)
-    gm, dxmm = w["goldak_mm"], w["dx"] * 1e3
-    goldak = dict(ff=gm["ff"], fr=gm["fr"], a_front=gm["a_front_mm"] / dxmm,
-                  a_rear=gm["a_rear_mm"] / dxmm, b=gm["b_mm"] / dxmm, c=gm["c_mm"] / dxmm)
-    extra = dict(wire_feed_m_s=w["wire_feed_m_s"], droplet_transfer_mode="pulsed",
-                 pulse_frequency_hz=w["droplet_freq_hz"], droplet_size_jitter=0.0)
+    goldak = None
+    if w.get("goldak_mm"):
+        gm, dxmm = w["goldak_mm"], w["dx"] * 1e3
+        goldak = dict(ff=gm["ff"], fr=gm["fr"], a_front=gm["a_front_mm"] / dxmm,
+                      a_rear=gm["a_rear_mm"] / dxmm, b=gm["b_mm"] / dxmm,
+                      c=gm["c_mm"] / dxmm)
+    extra = {}
+    if w.get("wire_feed_m_s"):
+        extra = dict(wire_feed_m_s=w["wire_feed_m_s"], droplet_transfer_mode="pulsed",
+                     pulse_frequency_hz=w["droplet_freq_hz"], droplet_size_jitter=0.0)
+    if w.get("plate_thickness_mm"):
+        extra["plate_thickness_mm"] = w["plate_thickness_mm"]
     mat = dict(bench.MATERIAL, contact_angle_deg=w.get("contact_angle_deg", 30.0))
     ot = OracleTwin(w["nx"], w["ny"], w["nz"], w["dx"], mat, goldak=goldak, **kw, **extra)
     ot.reset()
     return ot
 
 
-def main(n_steps=10000, every=500):
+def fixture_path(workload):
+    return os.path.join(HERE, "trajectory_%s.json" % workload)
+
+
+def main(workload="standard", n_steps=10000, every=500):
     sys.path.insert(0, ROOT)
     import bench
-    w = dict(bench.WORKLOADS["standard"])
+    w = dict(bench.WORKLOADS[workload])
     ot = oracle_twin(w)
     pos = bench.path_steps(w, ot.dt, n_steps)
     recs, t0 = [], time.time()
@@ -78,11 +89,12 @@ def main(n_steps=10000, every=500):
         if (s + 1) % every == 0:
             recs.append(record(s + 1, ot.s, ot.n_drops))
             print(json.dumps(recs[-1]), "%.0f s" % (time.time() - t0), flush=True)
-    with open(OUT, "w") as fh:
+    with open(fixture_path(workload), "w") as fh:
         json.dump({"workload": w["workload"], "every": every, "n_steps": n_steps,
                    "generator": "CPU oracle (oracle/oracle_step.py), tests/golden/make_trajectory.py",
                    "records": recs}, fh, indent=1)
 
 
 if __name__ == "__main__":
-    main(*(int(a) for a in sys.argv[1:3]))
+    main(sys.argv[1] if len(sys.argv) > 1 else "standard",
+         *(int(a) for a in sys.argv[2:4]))

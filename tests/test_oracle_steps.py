@@ -73,7 +73,7 @@ def test_oracle_trajectory_matches_reference(name, monkeypatch):
 
 def test_trajectory_fixture_is_complete_and_consistent():
     """tests/golden/trajectory_standard.json (make_trajectory.py): one record
-    every 500 steps, droplets counted up by one per 100 Hz period, the state
+    every 500 steps (the small workload's every 250 through 2,000), droplets counted up by one per 100 Hz period, the state
     finite through step 9,000, and the hash helper the GPU test shares is the
     SHA-1 of the float32 bytes."""
     import hashlib
@@ -84,9 +84,13 @@ def test_trajectory_fixture_is_complete_and_consistent():
     import numpy as np
     here = os.path.dirname(os.path.abspath(__file__))
     sys.path.insert(0, os.path.join(here, "golden"))
-    from make_trajectory import FIELDS, field_hash
-    with open(os.path.join(here, "golden", "trajectory_standard.json")) as fh:
+    from make_trajectory import FIELDS, field_hash, fixture_path
+    with open(fixture_path("standard")) as fh:
         fix = json.load(fh)
+    with open(fixture_path("small")) as fh:
+        small = json.load(fh)
+    assert [r["step"] for r in small["records"]] == list(range(250, 2001, 250))
+    assert all(r["nonfinite_T"] == 0 for r in small["records"])
     recs = fix["records"]
     assert [r["step"] for r in recs] == list(range(500, fix["n_steps"] + 1, 500))
     finite = [r for r in recs if r["nonfinite_T"] == 0]
