@@ -761,7 +761,8 @@ struct TableArgs {
 // 2030-2082 + 1937-1950 (losses, floor), 1519-1556 twice around the ceiling
 // 1953-1984 (only the second update_phase is observable), 3016-3032 (T_max),
 // 2013-2027 (cooling rate).  H and T are double-buffered so neighbour reads
-// see the pre-stage values.  Also resets the active-cell shard counters of the step.
+// see the pre-stage values.  Also resets the active-cell shard counters of the step and
+// counts up the population copy's stamp (one thermal stage between two collisions).
 // TABLES: refresh_thermal_properties, advect_diffuse_temperature_variable,
 // clamp_enthalpy_floor and update_phase_variable_cp / the variable ceiling
 // (kernels.py:1710-1863, 1922-1935, 1988-2010) instead of the scalar forms.
