@@ -1,6 +1,6 @@
 /* waam_b200 -- C ABI of the B200 (sm_100a) coupled melt-pool step.
  *
- * Drop-in native backend for the waam_twin operator API (physics/*.py) and
+ * Drop-in native backend for the waam_twin operator API (the physics modules) and
  * its step driver (solvers/coupled_step.py:73-464) of THEDARKDEACON/waam_solver.
  * All pointers are DEVICE pointers to memory owned by the caller (torch
  * tensors in the Python host); the library never allocates or frees on these
